@@ -1,0 +1,142 @@
+/*
+ * riv_gpu.h -- C ABI of the B200 riv2 P-frame encoder (drop-in for reitero_encode).
+ *
+ * Each declaration names the reference interface it replaces (paths relative to the
+ * reference project root; enc/ = reitero_video/reitero_encode/src/).  A Rust caller
+ * binds these through an `extern "C"` block; Python binds them
+ * with ctypes (riv2_b200/encoder.py).  No CUDA or torch types appear here: buffers
+ * are plain pointers and sizes.
+ *
+ * Threading: one encoder per host thread.  riv_encode_frame may keep up to
+ * `pipeline_depth` frames in flight (GPU work and host entropy coding overlap across
+ * frames); records still reach the writer strictly in frame order, and riv_finish
+ * flushes everything.  With pipeline_depth == 0 every call returns only after its own
+ * record has been handed to the writer, exactly like Encoder::encode_frame.
+ */
+#ifndef RIV_GPU_H
+#define RIV_GPU_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* EncodeError variants (enc/error.rs:4-20) plus device-side failures. */
+typedef enum {
+    RIV_OK = 0,
+    RIV_ERR_IO = 1,               /* EncodeError::Io -- a writer callback failed */
+    RIV_ERR_INVALID_CONFIG = 2,   /* EncodeError::InvalidConfig */
+    RIV_ERR_ENCODING_FAILED = 3,  /* EncodeError::EncodingFailed */
+    RIV_ERR_UNSUPPORTED_CODEC = 4,/* EncodeError::UnsupportedCodec (never produced) */
+    RIV_ERR_FRAME = 5,            /* EncodeError::FrameError -- bad dimensions / sizes */
+    RIV_ERR_CUDA = 6,             /* a CUDA runtime call failed */
+    RIV_ERR_DEVICE_TIMEOUT = 7    /* a bounded device-side wait expired */
+} riv_status;
+
+/* KeyframeInterval (enc/config.rs:5-19): AllIntra, Automatic (= fixed 30), Fixed(n). */
+typedef enum { RIV_KEYFRAME_ALL_INTRA = 0, RIV_KEYFRAME_AUTOMATIC = 1, RIV_KEYFRAME_FIXED = 2 } riv_keyframe_mode;
+
+/* EncoderConfig (enc/config.rs:24-53).  The trailing device fields never change bits. */
+typedef struct {
+    uint32_t display_width, display_height;
+    uint32_t storage_width, storage_height;
+    uint32_t fps;
+    uint32_t keyframe_mode;     /* riv_keyframe_mode */
+    uint64_t keyframe_interval; /* for RIV_KEYFRAME_FIXED */
+    uint8_t intra_quality, inter_quality, search_range, mv_deflate_level, skip_threshold;
+    uint8_t _pad[3];
+    int64_t me_zero_mv_threshold, me_predictor_threshold;
+    double rdo_lambda_mult;
+    float inter_dead_zone;
+    /* device / host-runtime tuning */
+    int32_t device;          /* CUDA device ordinal */
+    uint32_t pipeline_depth; /* frames in flight (0 = synchronous, like the reference) */
+    uint32_t entropy_threads;/* host threads for the DCT-coefficient rANS coder (0 = auto) */
+    uint32_t _pad2[2];
+} riv_config;
+
+/* EncoderConfig::new (enc/config.rs:56-77): defaults, storage rounded up to 16. */
+void riv_config_default(riv_config* cfg, uint32_t width, uint32_t height, uint32_t fps);
+
+/* VideoWriter (enc/writer.rs:5-18).  Callbacks return 0 on success. */
+typedef struct {
+    int (*write)(void* user, const uint8_t* data, size_t len);
+    uint64_t (*position)(void* user);
+    int (*seek)(void* user, uint64_t pos);
+    int (*flush)(void* user);
+    void* user;
+} riv_writer_vtable;
+
+/* A subset of EncodeFrameStats (enc/encoder.rs:58-124). */
+typedef struct {
+    uint64_t frame_index, timestamp_ms;
+    uint32_t frame_type; /* 1 = intra, 2 = inter (FrameType, com/format.rs:12-20) */
+    uint32_t total_bytes, mv_bytes, residual_bytes;
+    uint32_t storage_width, storage_height;
+    uint32_t blocks_total, blocks_skipped, rdo_blocks_selected_skip;
+    uint32_t mv_mode_counts[7];
+    uint32_t mv_new_base_counts[5];
+    uint32_t mv_new_blocks;
+    int32_t mv_bias_dx, mv_bias_dy;
+    double rdo_lambda;
+} riv_frame_stats;
+
+typedef struct riv_encoder riv_encoder;
+
+/* Encoder::new (enc/encoder.rs:162-188): validates, writes the 36-byte header now. */
+riv_status riv_encoder_new(const riv_config* cfg, const riv_writer_vtable* writer, riv_encoder** out);
+/* Encoder::encode_frame / encode_frame_with_stats (enc/encoder.rs:229-256): RGB24,
+ * display size, row-major, no padding; `rgb` is only read during the call.
+ * `stats` (nullable) forces this frame to complete before returning. */
+riv_status riv_encode_frame(riv_encoder* enc, const uint8_t* rgb, uint32_t width, uint32_t height,
+                            uint64_t timestamp_ms, riv_frame_stats* stats);
+/* Same input already resident in device memory (display-size RGB24). */
+riv_status riv_encode_frame_device(riv_encoder* enc, const void* d_rgb, uint64_t timestamp_ms, riv_frame_stats* stats);
+/* Test hook: storage-size YUV 4:2:0 planes (the input of the path after RGB->YUV). */
+riv_status riv_encode_frame_yuv(riv_encoder* enc, const uint8_t* y, const uint8_t* u, const uint8_t* v,
+                                uint64_t timestamp_ms, riv_frame_stats* stats);
+/* Encoder::finish (enc/encoder.rs:950-961): drains, rewrites frame_count, flushes. */
+riv_status riv_finish(riv_encoder* enc);
+void riv_encoder_free(riv_encoder* enc);
+/* Message of the last failure ("" if none). */
+const char* riv_last_error(const riv_encoder* enc);
+uint64_t riv_frame_count(const riv_encoder* enc);
+
+/* Reconstruction (deblocked reference) of the last frame whose GPU work finished;
+ * storage-size planes.  Synchronises the device. */
+riv_status riv_last_recon(riv_encoder* enc, uint8_t* y, uint8_t* u, uint8_t* v);
+/* Per-frame GPU timing of the last completed frame, microseconds:
+ * [0] rgb->yuv [1] search [2] predict [3] aq [4] residual [5] deblock [6] compact [7] total */
+riv_status riv_last_kernel_times(riv_encoder* enc, float* us8);
+
+/* In-memory writer (VecWriter, enc/writer.rs:20-69). */
+typedef struct riv_memwriter riv_memwriter;
+riv_memwriter* riv_memwriter_new(void);
+void riv_memwriter_vtable(riv_memwriter* w, riv_writer_vtable* out);
+size_t riv_memwriter_size(const riv_memwriter* w);
+const uint8_t* riv_memwriter_data(const riv_memwriter* w);
+void riv_memwriter_free(riv_memwriter* w);
+
+/* ---- Stage entry points (one kernel each, host buffers in/out) for parity tests ---- */
+/* Yuv420Frame::from_rgb after pad_rgb24 (com/yuv.rs:41-74, enc/encoder.rs:1049-1096). */
+riv_status riv_stage_rgb_to_yuv(const uint8_t* rgb, uint32_t dw, uint32_t dh, uint32_t sw, uint32_t sh,
+                                uint8_t* yuv_out);
+/* deblock_yuv420 (com/deblock.rs:189-202); mask: one byte per MB or NULL. */
+riv_status riv_stage_deblock(uint8_t* yuv, uint32_t w, uint32_t h, int level, int intra, const uint8_t* mask);
+/* glibc-exact logf (which=0) / exp2f (which=1) on the device over n inputs. */
+riv_status riv_stage_libm(int which, const float* in, float* out, size_t n);
+/* Test hook: device state left by the most recent frame (synchronises the device; meant
+ * for pipeline_depth == 0).  what: 0 per-MB search/mode output (20 B/MB), 1 AQ steps
+ * (f32/MB), 2 prediction (YUV), 3 converted input (YUV), 4 quantised coefficients
+ * (384 x i16 per MB), 5 optimized skip (u8/MB).  Returns RIV_ERR_FRAME if `size` is short. */
+riv_status riv_debug_frame_state(riv_encoder* enc, int what, void* out, size_t size);
+/* Number of glibc fix-up entries loaded for logf / exp2f. */
+riv_status riv_libm_fixup_counts(uint32_t* nlog, uint32_t* nexp);
+/* The DCT bases the device uses (T16[i][j], T8[i][j]: sample i, frequency j). */
+void riv_dct_tables(int32_t* t16, int32_t* t8);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

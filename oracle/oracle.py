@@ -1,0 +1,269 @@
+"""ctypes binding of the CPU oracle (test infrastructure only).
+
+The oracle is a single-threaded C++ restatement of the reference riv2 encoder path
+(reitero_encode + reitero_residual + reitero_dct + reitero_video_common) and of its
+decoder (reitero_decode); see riv_oracle.cpp for the file:line citations.  Only the
+test suite, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` may
+use it, and only as the checker -- the product never routes through it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+
+
+class OracleConfig(C.Structure):
+    """Mirror of ``oracle_config`` (riv_oracle.h) == reitero_encode::EncoderConfig."""
+
+    _fields_ = [
+        ("display_width", C.c_uint32), ("display_height", C.c_uint32),
+        ("storage_width", C.c_uint32), ("storage_height", C.c_uint32),
+        ("fps", C.c_uint32), ("keyframe_mode", C.c_uint32), ("keyframe_interval", C.c_uint64),
+        ("intra_quality", C.c_uint8), ("inter_quality", C.c_uint8), ("search_range", C.c_uint8),
+        ("mv_deflate_level", C.c_uint8), ("skip_threshold", C.c_uint8), ("_pad", C.c_uint8 * 3),
+        ("me_zero_mv_threshold", C.c_int64), ("me_predictor_threshold", C.c_int64),
+        ("rdo_lambda_mult", C.c_double), ("inter_dead_zone", C.c_float), ("_pad2", C.c_uint32),
+    ]
+
+
+def build() -> str:
+    """Compile liboracle.so with the committed Makefile (idempotent)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        P, U8, I8, I16, I64, F32 = (C.c_void_p, C.POINTER(C.c_uint8), C.POINTER(C.c_int8),
+                                     C.POINTER(C.c_int16), C.POINTER(C.c_int64), C.POINTER(C.c_float))
+        L.oracle_config_default.argtypes = [C.POINTER(OracleConfig), C.c_uint32, C.c_uint32, C.c_uint32]
+        L.oracle_enc_new.restype = P
+        L.oracle_enc_new.argtypes = [C.POINTER(OracleConfig), C.POINTER(C.c_int)]
+        L.oracle_enc_frame_rgb.argtypes = [P, U8, C.c_uint32, C.c_uint32, C.c_uint64]
+        L.oracle_enc_frame_yuv.argtypes = [P, U8, U8, U8, C.c_uint64]
+        L.oracle_enc_finish.argtypes = [P]
+        L.oracle_enc_bytes.restype = C.c_size_t
+        L.oracle_enc_bytes.argtypes = [P, C.POINTER(U8)]
+        L.oracle_enc_free.argtypes = [P]
+        L.oracle_enc_last_type.argtypes = [P]
+        for n in ("recon", "recon_pre", "curr", "pred"):
+            getattr(L, f"oracle_enc_last_{n}").argtypes = [P, U8, U8, U8]
+        L.oracle_enc_last_mvs.argtypes = [P, I8, I8, I64]
+        L.oracle_enc_last_side.argtypes = [P, U8]
+        L.oracle_enc_last_qsteps.argtypes = [P, F32]
+        L.oracle_enc_last_coeffs.argtypes = [P, I16]
+        L.oracle_enc_last_bias.argtypes = [P, I8]
+        L.oracle_enc_last_record.restype = C.c_size_t
+        L.oracle_enc_last_record.argtypes = [P, C.POINTER(U8)]
+        L.oracle_dec_new.restype = P
+        L.oracle_dec_new.argtypes = [U8, C.c_size_t, C.POINTER(C.c_int)]
+        L.oracle_dec_next.argtypes = [P, U8, U8, U8]
+        L.oracle_dec_dims.argtypes = [P, C.POINTER(C.c_uint32)]
+        L.oracle_dec_free.argtypes = [P]
+        L.oracle_rgb_to_yuv420.argtypes = [U8, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, U8, U8, U8]
+        L.oracle_deblock.argtypes = [U8, U8, U8, C.c_uint32, C.c_uint32, C.c_int, C.c_int, U8]
+        L.oracle_deblock_level.argtypes = [C.c_uint8]
+        L.oracle_quant_step.restype = C.c_float
+        L.oracle_quant_step.argtypes = [C.c_uint8]
+        for n in ("oracle_build_predicted", "oracle_reference_build_predicted"):
+            getattr(L, n).argtypes = [U8, U8, U8, C.c_uint32, C.c_uint32, I8, U8, U8, U8]
+        L.oracle_motion_search.argtypes = [U8, U8, C.c_uint32, C.c_uint32, C.c_uint8, I8, C.c_int64, C.c_int64,
+                                           C.c_double, I8, I64]
+        for n in ("oracle_sad_int", "oracle_sad_halfpel"):
+            getattr(L, n).restype = C.c_int64
+            getattr(L, n).argtypes = [U8, U8, C.c_uint32, C.c_uint32, C.c_int, C.c_int, C.c_int, C.c_int,
+                                      C.c_int64, C.c_int]
+        L.oracle_aq_steps.argtypes = [U8, C.c_uint32, C.c_uint32, C.c_float, F32]
+        L.oracle_rdo_lambda.restype = C.c_double
+        L.oracle_rdo_lambda.argtypes = [C.c_uint8, C.c_double]
+        for n in ("oracle_fdct16_quant", "oracle_fdct8_quant"):
+            getattr(L, n).argtypes = [I16, C.c_float, C.c_float, I16]
+        for n in ("oracle_idct16_aq", "oracle_idct8_aq"):
+            getattr(L, n).argtypes = [I16, C.c_float, I16]
+        L.oracle_rans_roundtrip.restype = C.c_size_t
+        L.oracle_rans_roundtrip.argtypes = [U8, U8, C.c_size_t, U8, U8, C.c_size_t]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray, ct):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+def u8(a):
+    return _p(a, C.c_uint8)
+
+
+def i8(a):
+    return _p(a, C.c_int8)
+
+
+def i16(a):
+    return _p(a, C.c_int16)
+
+
+def default_config(w: int, h: int, fps: int = 30) -> OracleConfig:
+    c = OracleConfig()
+    lib().oracle_config_default(C.byref(c), w, h, fps)
+    return c
+
+
+class Frames:
+    """YUV 4:2:0 planes of one frame."""
+
+    def __init__(self, w: int, h: int):
+        self.w, self.h = w, h
+        self.y = np.zeros((h, w), np.uint8)
+        self.u = np.zeros((h // 2, w // 2), np.uint8)
+        self.v = np.zeros((h // 2, w // 2), np.uint8)
+
+    def ptrs(self):
+        return u8(self.y), u8(self.u), u8(self.v)
+
+    def equal(self, o) -> bool:
+        return (np.array_equal(self.y, o.y) and np.array_equal(self.u, o.u) and np.array_equal(self.v, o.v))
+
+
+class OracleEncoder:
+    """Oracle encoder: Encoder::new / encode_frame / finish over an in-memory writer."""
+
+    def __init__(self, cfg: OracleConfig):
+        st = C.c_int(0)
+        self.cfg = cfg
+        self.h = lib().oracle_enc_new(C.byref(cfg), C.byref(st))
+        if not self.h:
+            raise ValueError(f"oracle config rejected (status {st.value})")
+        self.sw, self.sh = cfg.storage_width, cfg.storage_height
+        self.mbs = (self.sw // 16) * (self.sh // 16)
+
+    def encode_rgb(self, rgb: np.ndarray, ts: int) -> int:
+        rgb = np.ascontiguousarray(rgb, dtype=np.uint8)
+        return lib().oracle_enc_frame_rgb(self.h, u8(rgb), self.cfg.display_width, self.cfg.display_height, ts)
+
+    def encode_yuv(self, f: Frames, ts: int) -> int:
+        return lib().oracle_enc_frame_yuv(self.h, *f.ptrs(), ts)
+
+    def finish(self) -> bytes:
+        lib().oracle_enc_finish(self.h)
+        return self.bytes()
+
+    def bytes(self) -> bytes:
+        p = C.POINTER(C.c_uint8)()
+        n = lib().oracle_enc_bytes(self.h, C.byref(p))
+        return C.string_at(p, n)
+
+    def last_record(self) -> bytes:
+        p = C.POINTER(C.c_uint8)()
+        n = lib().oracle_enc_last_record(self.h, C.byref(p))
+        return C.string_at(p, n)
+
+    def last(self, what: str) -> Frames:
+        f = Frames(self.sw, self.sh)
+        getattr(lib(), f"oracle_enc_last_{what}")(self.h, *f.ptrs())
+        return f
+
+    def last_type(self) -> int:
+        return lib().oracle_enc_last_type(self.h)
+
+    def last_mvs(self):
+        raw = np.zeros((self.mbs, 4), np.int8)
+        coded = np.zeros((self.mbs, 4), np.int8)
+        sad = np.zeros(self.mbs, np.int64)
+        lib().oracle_enc_last_mvs(self.h, i8(raw), i8(coded), _p(sad, C.c_int64))
+        return raw, coded, sad
+
+    def last_side(self) -> np.ndarray:
+        s = np.zeros((self.mbs, 8), np.uint8)
+        lib().oracle_enc_last_side(self.h, u8(s))
+        return s
+
+    def last_qsteps(self) -> np.ndarray:
+        q = np.zeros(self.mbs, np.float32)
+        lib().oracle_enc_last_qsteps(self.h, _p(q, C.c_float))
+        return q
+
+    def last_coeffs(self) -> np.ndarray:
+        c = np.zeros((self.mbs, 384), np.int16)
+        lib().oracle_enc_last_coeffs(self.h, i16(c))
+        return c
+
+    def last_bias(self):
+        b = np.zeros(2, np.int8)
+        lib().oracle_enc_last_bias(self.h, i8(b))
+        return int(b[0]), int(b[1])
+
+    def close(self):
+        if self.h:
+            lib().oracle_enc_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class OracleDecoder:
+    def __init__(self, stream: bytes):
+        self._buf = np.frombuffer(stream, np.uint8).copy()
+        st = C.c_int(0)
+        self.h = lib().oracle_dec_new(u8(self._buf), len(stream), C.byref(st))
+        if not self.h:
+            raise ValueError("bad .riv header")
+        d = (C.c_uint32 * 6)()
+        lib().oracle_dec_dims(self.h, d)
+        self.dw, self.dh, self.sw, self.sh, self.fps, self.frame_count = list(d)
+
+    def next(self):
+        f = Frames(self.sw, self.sh)
+        t = lib().oracle_dec_next(self.h, *f.ptrs())
+        return t, f
+
+    def close(self):
+        if self.h:
+            lib().oracle_dec_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def rgb_to_yuv(rgb: np.ndarray, dw: int, dh: int, sw: int, sh: int) -> Frames:
+    f = Frames(sw, sh)
+    rgb = np.ascontiguousarray(rgb, dtype=np.uint8)
+    lib().oracle_rgb_to_yuv420(u8(rgb), dw, dh, sw, sh, *f.ptrs())
+    return f
+
+
+def deblock(f: Frames, level: int, intra: bool, mask=None) -> Frames:
+    o = Frames(f.w, f.h)
+    o.y[:], o.u[:], o.v[:] = f.y, f.u, f.v
+    m = None if mask is None else u8(np.ascontiguousarray(mask, dtype=np.uint8))
+    lib().oracle_deblock(*o.ptrs(), f.w, f.h, level, int(intra), m)
+    return o
+
+
+def build_predicted(prev: Frames, mvs4: np.ndarray, reference: bool = False) -> Frames:
+    o = Frames(prev.w, prev.h)
+    m = np.ascontiguousarray(mvs4, dtype=np.int8)
+    fn = lib().oracle_reference_build_predicted if reference else lib().oracle_build_predicted
+    fn(*prev.ptrs(), prev.w, prev.h, i8(m), *o.ptrs())
+    return o

@@ -1,0 +1,69 @@
+// riv_entropy.h -- host-side entropy coders of the riv2 bitstream (byte-exact with the
+// reference): adaptive binary rANS (com/rans.rs), the DCT-coefficient coder
+// (res/rans.rs) and the motion-vector coder (res/mv_rans/encoder.rs).  They consume the
+// per-MB side info and compacted coefficients produced by the GPU.
+#pragma once
+#include <cstdint>
+#include <tuple>
+#include <unordered_map>
+#include <vector>
+
+namespace riv {
+
+void entropy_init();
+
+struct BinProb {
+    uint16_t packed = 0x0101;
+};
+
+// Binary rANS writer with the reference's buffering (BATCH = 16386 symbols per drain,
+// two interleaved states, 8-bit scale, RANS_L = 2^16, u16 emission).
+class RansWriter {
+public:
+    explicit RansWriter(std::vector<uint8_t>* sink);
+    inline void put(bool bit, BinProb& ctx);
+    inline void put_bypass(bool bit);
+    void finish();
+
+private:
+    void drain();
+    std::vector<uint8_t>* sink_;
+    std::vector<uint16_t> stack_;  // entry = p | bit << 8; stack_[BATCH-1] is the oldest
+    std::vector<uint16_t> words_;
+    int sp_;
+};
+
+// One MB's coefficients in the GPU's compact layout: Y[256], U[64], V[64] plus the last
+// non-zero index of each plane block.
+void encode_residual_frame(const int16_t* packed, const uint8_t* eobs, int nblocks, bool intra,
+                           std::vector<uint8_t>& out);
+
+enum MvMode { M_ZERO = 0, M_NEAREST = 1, M_NEAR = 2, M_TOPRIGHT = 3, M_TOPLEFT = 4, M_NEW = 5, M_TEMPORAL = 6 };
+enum Subpel { SP_ZERO = 0, SP_PLUS = 1, SP_MINUS = 2 };
+
+struct MvCodedBlock {  // res/mv_rans.rs:65-78
+    uint8_t mode, new_base;
+    int8_t dx, dy;
+    uint8_t spx, spy;
+    bool skip;
+};
+
+class MvCoder {  // res/mv_rans/encoder.rs:60-412
+public:
+    void reset();
+    void encode_frame(const std::vector<MvCodedBlock>& blocks, int bw, std::vector<uint8_t>& out);
+
+private:
+    void update(const std::vector<MvCodedBlock>& blocks);
+    BinProb skip_, m_new_[4], m_nz_[4], m_near_[4], m_tmp_[4], m_tr_[4], m_tl_[4], b_nearest_[4], b_near_[4],
+        b_tr_[4], b_tl_[4], cls_x_[4], cls_y_[4], sign_x_, sign_y_, mag_x_[10], mag_y_[10], sub_x_, sub_y_,
+        hit_[3], cidx_[4];
+    std::vector<uint32_t> cands_;  // packed keys
+    std::unordered_map<uint32_t, uint32_t> counts_;
+    uint32_t total_ = 0;
+};
+
+// compute_delta_bias_for_new (enc/encoder.rs:984-1048) from per-axis histograms.
+void compute_delta_bias(const std::vector<std::pair<int8_t, int8_t>>& deltas, int8_t& bx, int8_t& by);
+
+}  // namespace riv

@@ -1,0 +1,1014 @@
+// riv_host.cpp -- the C-ABI encoder (include/riv_gpu.h): device buffers, the per-frame
+// kernel sequence, the frame pipeline and the host entropy stage.
+//
+// Per P-frame (one CUDA stream):  rgb->yuv -> search/mode wavefront -> predict+variance
+// -> AQ -> residual/DCT/quant/recon -> deblock -> compaction; a copy stream brings the
+// per-MB side info and the coded MBs' coefficients back; the host runs the motion-vector
+// rANS coder (ordered, contexts persist across frames), the DCT-coefficient rANS coder
+// (fresh contexts per frame, so frames code in parallel on a thread pool) and writes the
+// records in frame order.  Reference: enc/encoder.rs:258-947 (enc/ =
+// reitero_video/reitero_encode/src/).
+#include <cuda_runtime.h>
+#include <dlfcn.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <functional>
+#include <future>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/riv_gpu.h"
+#include "riv_entropy.h"
+#include "riv_internal.h"
+
+extern "C" int riv_upload_dct_tables(const int32_t* t16, const int32_t* t8);
+
+namespace {
+
+using namespace riv;
+
+// ---------------------------------------------------------------------------------
+// Small utilities
+// ---------------------------------------------------------------------------------
+struct CudaError {
+    cudaError_t e;
+    const char* where;
+};
+#define CK(x)                                                   \
+    do {                                                        \
+        cudaError_t e_ = (cudaError_t)(x);                      \
+        if (e_ != cudaSuccess) throw CudaError{e_, #x};         \
+    } while (0)
+
+class ThreadPool {
+public:
+    explicit ThreadPool(unsigned n) {
+        for (unsigned i = 0; i < n; i++) workers_.emplace_back([this] { run(); });
+    }
+    ~ThreadPool() {
+        {
+            std::lock_guard<std::mutex> g(m_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : workers_) t.join();
+    }
+    std::future<void> submit(std::function<void()> f) {
+        auto task = std::make_shared<std::packaged_task<void()>>(std::move(f));
+        std::future<void> fut = task->get_future();
+        {
+            std::lock_guard<std::mutex> g(m_);
+            q_.push_back([task] { (*task)(); });
+        }
+        cv_.notify_one();
+        return fut;
+    }
+
+private:
+    void run() {
+        for (;;) {
+            std::function<void()> f;
+            {
+                std::unique_lock<std::mutex> l(m_);
+                cv_.wait(l, [this] { return stop_ || !q_.empty(); });
+                if (stop_ && q_.empty()) return;
+                f = std::move(q_.front());
+                q_.pop_front();
+            }
+            f();
+        }
+    }
+    std::vector<std::thread> workers_;
+    std::deque<std::function<void()>> q_;
+    std::mutex m_;
+    std::condition_variable cv_;
+    bool stop_ = false;
+};
+
+// DCT bases from their definition: T[i][j] = round(2^18 * c_j * cos((2i+1) j pi / 2N)),
+// c_0 = sqrt(1/N), c_j = sqrt(2/N) -- equal to the reference's tables
+// (dct/dct16.rs:7-145, dct/dct8.rs:6-25; checked against tests/golden).
+static int32_t round_half_away(double v) { return (int32_t)(v >= 0 ? floor(v + 0.5) : -floor(-v + 0.5)); }
+static void dct_tables(int32_t* t16, int32_t* t8) {
+    const double PI = 3.14159265358979323846;
+    for (int i = 0; i < 16; i++)
+        for (int j = 0; j < 16; j++)
+            t16[i * 16 + j] = round_half_away(262144.0 * (j == 0 ? sqrt(1.0 / 16) : sqrt(2.0 / 16)) *
+                                              cos((2 * i + 1) * j * PI / 32));
+    for (int i = 0; i < 8; i++)
+        for (int j = 0; j < 8; j++)
+            t8[i * 8 + j] = round_half_away(262144.0 * (j == 0 ? sqrt(1.0 / 8) : 0.5) * cos((2 * i + 1) * j * PI / 16));
+}
+
+// quant_step_from_quality (res/residual.rs:13-23)
+static float quant_step(uint8_t q) {
+    if (q == 100) return 1.0f;
+    if (q == 1) return 112.0f;
+    return 1.0f + (100.0f - (float)q) / 99.0f * (112.0f - 1.0f);
+}
+// deblock_level_from_quant_step / thresholds (com/deblock.rs:34-58)
+static int deblock_level(float qs) {
+    float v = roundf(qs * 0.6f);
+    v = v < 0.0f ? 0.0f : (v > 63.0f ? 63.0f : v);
+    return (int)v;
+}
+static void deblock_thresholds(int level, bool intra, int& E, int& I, int& H) {
+    I = std::max(level, 1);
+    E = (level + 2) * 2 + I;
+    if (intra) H = level >= 40 ? 2 : (level >= 15 ? 1 : 0);
+    else H = level >= 40 ? 3 : (level >= 20 ? 2 : (level >= 15 ? 1 : 0));
+}
+// build_intra_{y,uv}_quant_table (res/residual.rs:58-96)
+static const float JPEG_LUMA[64] = {16, 11, 10, 16, 24,  40,  51,  61,  12, 12, 14, 19, 26,  58,  60,  55,
+                                    14, 13, 16, 24, 40,  57,  69,  56,  14, 17, 22, 29, 51,  87,  80,  62,
+                                    18, 22, 37, 56, 68,  109, 103, 77,  24, 35, 55, 64, 81,  104, 113, 92,
+                                    49, 64, 78, 87, 103, 121, 120, 101, 72, 92, 95, 98, 112, 100, 103, 99};
+static const float JPEG_CHROMA[64] = {17, 18, 24, 47, 99, 99, 99, 99, 18, 21, 26, 66, 99, 99, 99, 99,
+                                      24, 26, 56, 99, 99, 99, 99, 99, 47, 66, 99, 99, 99, 99, 99, 99,
+                                      99, 99, 99, 99, 99, 99, 99, 99, 99, 99, 99, 99, 99, 99, 99, 99,
+                                      99, 99, 99, 99, 99, 99, 99, 99, 99, 99, 99, 99, 99, 99, 99, 99};
+static uint16_t round_max1_u16(float s) {
+    float r = roundf(s);
+    if (r < 1.0f) r = 1.0f;
+    return r >= 65535.0f ? 65535 : (uint16_t)r;
+}
+static void intra_tables(float qs, uint16_t* yt, uint16_t* ct) {
+    for (int v = 0; v < 16; v++)
+        for (int u = 0; u < 16; u++) {
+            float fx = (float)u * 7.0f / 15.0f, fy = (float)v * 7.0f / 15.0f;
+            int x0 = (int)fx, y0 = (int)fy, x1 = std::min(x0 + 1, 7), y1 = std::min(y0 + 1, 7);
+            float dx = fx - (float)x0, dy = fy - (float)y0;
+            float val = JPEG_LUMA[y0 * 8 + x0] * (1.0f - dx) * (1.0f - dy) + JPEG_LUMA[y0 * 8 + x1] * dx * (1.0f - dy) +
+                        JPEG_LUMA[y1 * 8 + x0] * (1.0f - dx) * dy + JPEG_LUMA[y1 * 8 + x1] * dx * dy;
+            yt[v * 16 + u] = round_max1_u16((val / JPEG_LUMA[0]) * qs);
+        }
+    for (int i = 0; i < 64; i++) ct[i] = round_max1_u16((JPEG_CHROMA[i] / JPEG_CHROMA[0]) * qs);
+}
+// LambdaEntry::for_quality (enc/rdo.rs:23-48, 75-86)
+struct Lambda {
+    double lambda, ret, slope, icpt, skip_bits, keep_bits;
+};
+static Lambda lambda_for(uint8_t quality, double mult) {
+    quality = (uint8_t)std::min(std::max((int)quality, 1), 100);
+    int qp = (int)round((double)(100u - quality) * 0.6);
+    qp = std::min(std::max(qp, 0), 60);
+    Lambda L;
+    L.lambda = mult * pow(2.0, ((double)qp - 12.0) / 3.0);
+    double nq = (double)quality / 100.0, q = (double)quant_step(quality);
+    L.slope = 0.5 / q;
+    L.icpt = 5.0 + 0.56 * q;
+    L.ret = 0.15 + ((q - 1.0) / 111.0) * 0.55;
+    L.skip_bits = 0.55 - nq * 0.15;
+    L.keep_bits = 1.20 + nq * 0.35;
+    return L;
+}
+static int64_t f64_as_i64(double d) {
+    if (std::isnan(d)) return 0;
+    if (d <= -9223372036854775808.0) return INT64_MIN;
+    if (d >= 9223372036854775807.0) return INT64_MAX;
+    return (int64_t)d;
+}
+
+static void put_le(std::vector<uint8_t>& b, uint64_t v, int n) {
+    for (int i = 0; i < n; i++) b.push_back((uint8_t)(v >> (8 * i)));
+}
+// VideoHeader::to_bytes (com/format.rs:64-88)
+static std::vector<uint8_t> header_bytes(const riv_config& c, uint64_t frame_count) {
+    std::vector<uint8_t> b = {'R', 'I', 'V', 0};
+    put_le(b, 5, 4);
+    put_le(b, c.display_width, 4);
+    put_le(b, c.display_height, 4);
+    put_le(b, c.storage_width, 4);
+    put_le(b, c.storage_height, 4);
+    put_le(b, c.fps, 4);
+    put_le(b, frame_count, 8);
+    return b;
+}
+
+// glibc logf/exp2f fix-up tables, generated next to the library at build time.
+struct LibmFix {
+    std::vector<uint32_t> logf, exp2f;  // (in, out) pairs
+    bool ok = false;
+    std::string err;
+};
+static LibmFix& libm_fix() {
+    static LibmFix F;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        Dl_info info;
+        std::string dir = ".";
+        if (dladdr((void*)&libm_fix, &info) && info.dli_fname) {
+            dir = info.dli_fname;
+            size_t k = dir.rfind('/');
+            dir = k == std::string::npos ? "." : dir.substr(0, k);
+        }
+        std::string path = dir + "/libm_fixups.bin";
+        FILE* f = fopen(path.c_str(), "rb");
+        if (!f) { F.err = "missing " + path; return; }
+        char magic[8];
+        uint32_t n[2];
+        if (fread(magic, 1, 8, f) != 8 || memcmp(magic, "RIVLIBM1", 8) || fread(n, 4, 2, f) != 2) {
+            F.err = "bad " + path;
+            fclose(f);
+            return;
+        }
+        F.logf.resize(2 * (size_t)n[0]);
+        F.exp2f.resize(2 * (size_t)n[1]);
+        bool good = fread(F.logf.data(), 4, F.logf.size(), f) == F.logf.size() &&
+                    fread(F.exp2f.data(), 4, F.exp2f.size(), f) == F.exp2f.size();
+        fclose(f);
+        if (!good) { F.err = "short " + path; return; }
+        F.ok = true;
+    });
+    return F;
+}
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t bytes) {
+        n = bytes;
+        CK(cudaMalloc(&p, bytes ? bytes : 1));
+    }
+    void zero(cudaStream_t s) { CK(cudaMemsetAsync(p, 0, n ? n : 1, s)); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+    template <class T>
+    T* as() const { return (T*)p; }
+};
+struct HostBuf {
+    void* p = nullptr;
+    void alloc(size_t bytes) { CK(cudaMallocHost(&p, bytes ? bytes : 1)); }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+    }
+    template <class T>
+    T* as() const { return (T*)p; }
+};
+
+enum { EV_START, EV_YUV, EV_SEARCH, EV_PRED, EV_AQ, EV_RES, EV_DEBLOCK, EV_COMPACT, EV_N };
+
+struct Slot {
+    DevBuf rgb, side, index, packed, peobs, count;
+    HostBuf h_side, h_count, h_packed, h_peobs, h_status;
+    cudaEvent_t ev_h2d = nullptr, ev_gpu = nullptr, ev_side = nullptr, ev_coef = nullptr;
+    cudaEvent_t ev_k[EV_N] = {};
+};
+
+struct Job {
+    uint64_t index = 0, ts = 0;
+    int type = 0, slot = 0;
+    int state = 0;  // 0 submitted, 1 entropy running
+    uint32_t count = 0;
+    std::future<void> fut;
+    std::vector<uint8_t> res_bytes, mv_bytes;
+    int8_t bias[2] = {0, 0};
+    riv_frame_stats stats{};
+    float times[8] = {0};
+};
+
+}  // namespace
+
+struct riv_encoder {
+    riv_config cfg;
+    riv_writer_vtable wr;
+    std::string err;
+    bool poisoned = false;
+    uint64_t header_pos = 0, frame_count = 0, submitted = 0;
+    int W = 0, H = 0, BW = 0, BH = 0, NMB = 0;
+    size_t yuv_bytes = 0;
+    cudaStream_t S = nullptr, C = nullptr;
+    // device state
+    DevBuf cur, ref[2], pred, mbout, coded[2], rec, varsum, lnv, qs, coeffs, opt_skip, fmask, eobs, status;
+    DevBuf mvbits, logfix, expfix, ytab, ctab;
+    int ref_cur = 0, coded_cur = 0;
+    bool has_ref = false, has_prev_mvs = false;
+    unsigned tag = 0;
+    int search_grid = 0;
+    Lambda L{};
+    int inter_E = 0, inter_I = 0, inter_H = 0, inter_level = 0;
+    int intra_E = 0, intra_I = 0, intra_H = 0, intra_level = 0;
+    float inter_base = 0.0f;
+    int nlog = 0, nexp = 0;
+    std::vector<Slot> slots;
+    std::deque<Job> jobs;
+    MvCoder mvc;
+    std::unique_ptr<ThreadPool> pool;
+    float last_times[8] = {0};
+    bool have_times = false;
+    riv_frame_stats last_stats{};
+};
+
+namespace {
+
+static riv_status fail(riv_encoder* e, riv_status s, const std::string& msg) {
+    e->err = msg;
+    if (s == RIV_ERR_CUDA || s == RIV_ERR_DEVICE_TIMEOUT) e->poisoned = true;
+    return s;
+}
+
+static riv_status validate(const riv_config& c, std::string& msg) {  // enc/config.rs:129-164
+    if (c.display_width == 0 || c.display_height == 0) { msg = "Width and height must be greater than 0"; return RIV_ERR_INVALID_CONFIG; }
+    if (c.storage_width < c.display_width || c.storage_height < c.display_height) {
+        msg = "Storage dimensions must be >= display dimensions";
+        return RIV_ERR_INVALID_CONFIG;
+    }
+    if (c.fps == 0) { msg = "FPS must be greater than 0"; return RIV_ERR_INVALID_CONFIG; }
+    if (c.search_range > 127) { msg = "search_range must be <= 127 for current MV encoding"; return RIV_ERR_INVALID_CONFIG; }
+    if (c.mv_deflate_level > 10) { msg = "mv_deflate_level must be in 0..=10"; return RIV_ERR_INVALID_CONFIG; }
+    if (c.keyframe_mode == RIV_KEYFRAME_FIXED && c.keyframe_interval == 0) {
+        msg = "Keyframe interval must be greater than 0";
+        return RIV_ERR_INVALID_CONFIG;
+    }
+    if (c.keyframe_mode > 2) { msg = "unknown keyframe mode"; return RIV_ERR_INVALID_CONFIG; }
+    if (c.storage_width % 16 || c.storage_height % 16) { msg = "storage dimensions must be multiples of 16"; return RIV_ERR_INVALID_CONFIG; }
+    return RIV_OK;
+}
+
+static void setup_device(riv_encoder* e) {
+    const riv_config& c = e->cfg;
+    CK(cudaSetDevice(c.device));
+    e->W = (int)c.storage_width; e->H = (int)c.storage_height;
+    e->BW = e->W / 16; e->BH = e->H / 16; e->NMB = e->BW * e->BH;
+    e->yuv_bytes = (size_t)e->W * e->H * 3 / 2;
+    CK(cudaStreamCreateWithFlags(&e->S, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&e->C, cudaStreamNonBlocking));
+    int32_t t16[256], t8[64];
+    dct_tables(t16, t8);
+    CK(riv_upload_dct_tables(t16, t8));
+    const int N = e->NMB;
+    e->cur.alloc(e->yuv_bytes);
+    e->ref[0].alloc(e->yuv_bytes);
+    e->ref[1].alloc(e->yuv_bytes);
+    e->pred.alloc(e->yuv_bytes);
+    e->mbout.alloc((size_t)N * sizeof(MbOut));
+    e->coded[0].alloc((size_t)N * 4);
+    e->coded[1].alloc((size_t)N * 4);
+    e->rec.alloc((size_t)N * sizeof(MbRec));
+    e->varsum.alloc((size_t)N * sizeof(uint2));
+    e->lnv.alloc((size_t)N * sizeof(float));
+    e->qs.alloc((size_t)N * sizeof(float));
+    e->coeffs.alloc((size_t)N * 384 * sizeof(int16_t));
+    e->opt_skip.alloc(N);
+    e->fmask.alloc(N);
+    e->eobs.alloc((size_t)N * 3);
+    e->status.alloc(sizeof(unsigned));
+    e->rec.zero(e->S);
+    e->status.zero(e->S);
+    // search cost tables (enc/motion/scalar.rs:503-541): b(0)=1, b(d)=2*log2(d)+2
+    double bits[256];
+    bits[0] = 1.0;
+    for (int d = 1; d < 256; d++) bits[d] = 2.0 * log2((double)d) + 2.0;
+    e->mvbits.alloc(sizeof(bits));
+    CK(cudaMemcpy(e->mvbits.p, bits, sizeof(bits), cudaMemcpyHostToDevice));
+    LibmFix& F = libm_fix();
+    if (!F.ok) throw std::runtime_error("glibc fix-up table: " + F.err);
+    e->nlog = (int)(F.logf.size() / 2);
+    e->nexp = (int)(F.exp2f.size() / 2);
+    e->logfix.alloc(F.logf.size() * 4);
+    e->expfix.alloc(F.exp2f.size() * 4);
+    CK(cudaMemcpy(e->logfix.p, F.logf.data(), F.logf.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(e->expfix.p, F.exp2f.data(), F.exp2f.size() * 4, cudaMemcpyHostToDevice));
+    uint16_t yt[256], ct[64];
+    intra_tables(quant_step(c.intra_quality), yt, ct);
+    e->ytab.alloc(sizeof(yt));
+    e->ctab.alloc(sizeof(ct));
+    CK(cudaMemcpy(e->ytab.p, yt, sizeof(yt), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(e->ctab.p, ct, sizeof(ct), cudaMemcpyHostToDevice));
+    int g = 0;
+    CK(search_max_grid(c.search_range, &g));
+    if (g <= 0) throw std::runtime_error("search kernel cannot be made resident");
+    e->search_grid = std::min(g, e->BH);
+    // frame constants
+    e->L = lambda_for(c.inter_quality, c.rdo_lambda_mult);
+    e->inter_base = quant_step(c.inter_quality);
+    e->inter_level = deblock_level(quant_step(c.inter_quality));
+    deblock_thresholds(e->inter_level, false, e->inter_E, e->inter_I, e->inter_H);
+    e->intra_level = deblock_level(quant_step(c.intra_quality));
+    deblock_thresholds(e->intra_level, true, e->intra_E, e->intra_I, e->intra_H);
+    // pipeline slots
+    int nslots = std::max(1u, c.pipeline_depth);
+    e->slots.resize(nslots);
+    size_t rgb_bytes = (size_t)c.display_width * c.display_height * 3;
+    for (auto& s : e->slots) {
+        s.rgb.alloc(rgb_bytes);
+        s.side.alloc((size_t)N * 4);
+        s.index.alloc((size_t)N * 4);
+        s.packed.alloc((size_t)N * 384 * 2);
+        s.peobs.alloc((size_t)N * 3);
+        s.count.alloc(4);
+        s.h_side.alloc((size_t)N * 4);
+        s.h_count.alloc(4);
+        s.h_packed.alloc((size_t)N * 384 * 2);
+        s.h_peobs.alloc((size_t)N * 3);
+        s.h_status.alloc(4);
+        CK(cudaEventCreateWithFlags(&s.ev_h2d, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&s.ev_gpu, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&s.ev_side, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&s.ev_coef, cudaEventDisableTiming));
+        for (int k = 0; k < EV_N; k++) CK(cudaEventCreate(&s.ev_k[k]));
+    }
+    unsigned nt = c.entropy_threads;
+    if (nt == 0) nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency() > 1 ? std::thread::hardware_concurrency() - 1 : 1u));
+    e->pool.reset(new ThreadPool(nt));
+    CK(cudaStreamSynchronize(e->S));
+}
+
+// Enqueue the GPU work of one frame.  `src` = 0 host RGB, 1 device RGB, 2 host YUV.
+static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const void* b, const void* c3) {
+    const riv_config& c = e->cfg;
+    Slot& s = e->slots[j.slot];
+    const int W = e->W, H = e->H, N = e->NMB;
+    cudaStream_t S = e->S;
+    CK(cudaEventRecord(s.ev_k[EV_START], S));
+    if (src == 0) {
+        CK(cudaMemcpyAsync(s.rgb.p, a, (size_t)c.display_width * c.display_height * 3, cudaMemcpyHostToDevice, e->C));
+        CK(cudaEventRecord(s.ev_h2d, e->C));
+        CK(cudaStreamWaitEvent(S, s.ev_h2d, 0));
+        CK(launch_rgb_to_yuv((const uint8_t*)s.rgb.p, (int)c.display_width, (int)c.display_height, e->cur.as<uint8_t>(), W, H, S));
+    } else if (src == 1) {
+        CK(launch_rgb_to_yuv((const uint8_t*)a, (int)c.display_width, (int)c.display_height, e->cur.as<uint8_t>(), W, H, S));
+    } else {
+        uint8_t* d = e->cur.as<uint8_t>();
+        size_t ys = (size_t)W * H, cs = ys / 4;
+        CK(cudaMemcpyAsync(d, a, ys, cudaMemcpyHostToDevice, e->C));
+        CK(cudaMemcpyAsync(d + ys, b, cs, cudaMemcpyHostToDevice, e->C));
+        CK(cudaMemcpyAsync(d + ys + cs, c3, cs, cudaMemcpyHostToDevice, e->C));
+        CK(cudaEventRecord(s.ev_h2d, e->C));
+        CK(cudaStreamWaitEvent(S, s.ev_h2d, 0));
+    }
+    CK(cudaEventRecord(s.ev_k[EV_YUV], S));
+    const int nxt = e->ref_cur ^ 1;
+    uint8_t* recon = e->ref[nxt].as<uint8_t>();
+    ResidualParams rp{};
+    rp.cur = e->cur.as<uint8_t>();
+    rp.pred = e->pred.as<uint8_t>();
+    rp.recon = recon;
+    rp.coeffs = e->coeffs.as<int16_t>();
+    rp.opt_skip = e->opt_skip.as<uint8_t>();
+    rp.fmask = e->fmask.as<uint8_t>();
+    rp.eobs = e->eobs.as<uint8_t>();
+    rp.dead_zone = c.inter_dead_zone;
+    rp.W = W; rp.H = H; rp.BW = e->BW;
+    if (j.type == 1) {
+        rp.intra = 1;
+        rp.intra_ytab = e->ytab.as<uint16_t>();
+        rp.intra_ctab = e->ctab.as<uint16_t>();
+        CK(cudaEventRecord(s.ev_k[EV_SEARCH], S));
+        CK(cudaEventRecord(s.ev_k[EV_PRED], S));
+        CK(cudaEventRecord(s.ev_k[EV_AQ], S));
+        CK(launch_residual(rp, N, S));
+        CK(cudaEventRecord(s.ev_k[EV_RES], S));
+        if (e->intra_level > 0) CK(launch_deblock(recon, W, H, e->intra_E, e->intra_I, e->intra_H, nullptr, S));
+        CK(cudaEventRecord(s.ev_k[EV_DEBLOCK], S));
+        CK(launch_compact(e->opt_skip.as<uint8_t>(), e->mbout.as<MbOut>(), e->coeffs.as<int16_t>(), e->eobs.as<uint8_t>(), N, 1,
+                          s.side.as<uint32_t>(), s.index.as<int32_t>(), s.packed.as<int16_t>(), s.peobs.as<uint8_t>(),
+                          s.count.as<uint32_t>(), S));
+        e->has_prev_mvs = false;
+    } else {
+        SearchParams sp{};
+        sp.ref_y = e->ref[e->ref_cur].as<uint8_t>();
+        sp.cur_y = e->cur.as<uint8_t>();
+        sp.W = W; sp.H = H; sp.BW = e->BW; sp.BH = e->BH; sp.sr = c.search_range;
+        sp.prev_coded = e->has_prev_mvs ? e->coded[e->coded_cur].as<int8_t>() : nullptr;
+        sp.zthr = c.me_zero_mv_threshold;
+        sp.pthr = c.me_predictor_threshold;
+        double lam = e->L.lambda;
+        sp.lam2 = lam * 2.0;
+        sp.c15 = f64_as_i64(lam * 2.0 * 1.5);
+        sp.c05 = f64_as_i64(lam * 2.0 * 0.5);
+        sp.lambda_zero = lam == 0.0;
+        sp.mvbits = e->mvbits.as<double>();
+        sp.rdo_lambda = lam;
+        sp.rdo_skip_bits = e->L.skip_bits;
+        sp.rdo_keep_bits = e->L.keep_bits;
+        sp.rdo_icpt = e->L.icpt;
+        sp.rdo_slope = e->L.slope;
+        sp.rdo_ret = e->L.ret;
+        sp.rdo_guard = 768.0 * (double)c.skip_threshold;
+        sp.rdo_allow = c.skip_threshold > 0;
+        sp.rec = e->rec.as<MbRec>();
+        e->tag = (e->tag + 1) & 0xffffu;
+        if (e->tag == 0) e->tag = 1;
+        sp.tag = e->tag;
+        sp.out = e->mbout.as<MbOut>();
+        sp.status = e->status.as<unsigned>();
+        sp.spin_limit = 1ll << 22;  // ~ a few seconds, far above any legitimate wait
+        CK(launch_search(sp, e->search_grid, S));
+        CK(cudaEventRecord(s.ev_k[EV_SEARCH], S));
+        // coded MVs of this frame become next frame's temporal predictors
+        const int cn = e->coded_cur ^ 1;
+        CK(cudaMemcpy2DAsync(e->coded[cn].p, 4, (const char*)e->mbout.p + offsetof(MbOut, coded), sizeof(MbOut), 4, N,
+                             cudaMemcpyDeviceToDevice, S));
+        CK(launch_predict(e->ref[e->ref_cur].as<uint8_t>(), e->mbout.as<MbOut>(), e->pred.as<uint8_t>(), e->varsum.as<uint2>(), W, H, S));
+        CK(cudaEventRecord(s.ev_k[EV_PRED], S));
+        CK(launch_aq(e->varsum.as<uint2>(), N, e->inter_base, e->logfix.as<uint32_t>(), e->nlog, e->expfix.as<uint32_t>(),
+                     e->nexp, e->lnv.as<float>(), e->qs.as<float>(), S));
+        CK(cudaEventRecord(s.ev_k[EV_AQ], S));
+        rp.intra = 0;
+        rp.mb = e->mbout.as<MbOut>();
+        rp.qs = e->qs.as<float>();
+        CK(launch_residual(rp, N, S));
+        CK(cudaEventRecord(s.ev_k[EV_RES], S));
+        if (e->inter_level > 0) CK(launch_deblock(recon, W, H, e->inter_E, e->inter_I, e->inter_H, e->fmask.as<uint8_t>(), S));
+        CK(cudaEventRecord(s.ev_k[EV_DEBLOCK], S));
+        CK(launch_compact(e->opt_skip.as<uint8_t>(), e->mbout.as<MbOut>(), e->coeffs.as<int16_t>(), e->eobs.as<uint8_t>(), N, 0,
+                          s.side.as<uint32_t>(), s.index.as<int32_t>(), s.packed.as<int16_t>(), s.peobs.as<uint8_t>(),
+                          s.count.as<uint32_t>(), S));
+        e->coded_cur = cn;
+        e->has_prev_mvs = true;
+    }
+    CK(cudaEventRecord(s.ev_k[EV_COMPACT], S));
+    CK(cudaEventRecord(s.ev_gpu, S));
+    e->ref_cur = nxt;
+    e->has_ref = true;
+    CK(cudaStreamWaitEvent(e->C, s.ev_gpu, 0));
+    CK(cudaMemcpyAsync(s.h_side.p, s.side.p, (size_t)N * 4, cudaMemcpyDeviceToHost, e->C));
+    CK(cudaMemcpyAsync(s.h_count.p, s.count.p, 4, cudaMemcpyDeviceToHost, e->C));
+    CK(cudaMemcpyAsync(s.h_status.p, e->status.p, 4, cudaMemcpyDeviceToHost, e->C));
+    CK(cudaEventRecord(s.ev_side, e->C));
+}
+
+// Host part of a frame after its side info is back: coefficient copy, MV coding
+// (ordered), then the DCT coder on the pool.
+static riv_status retire(riv_encoder* e, Job& j) {
+    Slot& s = e->slots[j.slot];
+    CK(cudaEventSynchronize(s.ev_side));
+    unsigned st = *s.h_status.as<unsigned>();
+    if (st) {
+        return fail(e, (st & ST_WAIT_TIMEOUT) ? RIV_ERR_DEVICE_TIMEOUT : RIV_ERR_ENCODING_FAILED,
+                    (st & ST_WAIT_TIMEOUT) ? "device-side wavefront wait timed out" : "device search iteration cap hit");
+    }
+    j.count = *s.h_count.as<uint32_t>();
+    if (j.count) {
+        CK(cudaMemcpyAsync(s.h_packed.p, s.packed.p, (size_t)j.count * 768, cudaMemcpyDeviceToHost, e->C));
+        CK(cudaMemcpyAsync(s.h_peobs.p, s.peobs.p, (size_t)j.count * 3, cudaMemcpyDeviceToHost, e->C));
+        CK(cudaEventRecord(s.ev_coef, e->C));
+        CK(cudaEventSynchronize(s.ev_coef));
+    }
+    float t[8] = {0};
+    for (int k = 0; k < 7; k++) cudaEventElapsedTime(&t[k], s.ev_k[k], s.ev_k[k + 1]);
+    cudaEventElapsedTime(&t[7], s.ev_k[EV_START], s.ev_k[EV_COMPACT]);
+    for (int k = 0; k < 8; k++) j.times[k] = t[k] * 1000.0f;
+    const int N = e->NMB;
+    riv_frame_stats& S = j.stats;
+    memset(&S, 0, sizeof(S));
+    S.frame_index = j.index;
+    S.timestamp_ms = j.ts;
+    S.frame_type = (uint32_t)j.type;
+    S.storage_width = (uint32_t)e->W;
+    S.storage_height = (uint32_t)e->H;
+    S.blocks_total = (uint32_t)N;
+    if (j.type == 2) {
+        const uint32_t* side = s.h_side.as<uint32_t>();
+        std::vector<std::pair<int8_t, int8_t>> nd;
+        nd.reserve(N);
+        for (int i = 0; i < N; i++)
+            if ((side[i] & 7) == M_NEW) nd.emplace_back((int8_t)(side[i] >> 8), (int8_t)(side[i] >> 16));
+        compute_delta_bias(nd, j.bias[0], j.bias[1]);
+        // MvCodedBlock assembly (enc/encoder.rs:774-818)
+        std::vector<MvCodedBlock> blocks(N);
+        for (int i = 0; i < N; i++) {
+            uint32_t v = side[i];
+            MvCodedBlock& b = blocks[i];
+            b.mode = (uint8_t)(v & 7);
+            b.new_base = (uint8_t)((v >> 3) & 7);
+            b.skip = (v >> 24) & 1;
+            b.dx = b.dy = 0;
+            b.spx = b.spy = SP_ZERO;
+            if (b.mode == M_NEW) {
+                b.dx = (int8_t)std::min(std::max((int)(int8_t)(v >> 8) - j.bias[0], -128), 127);
+                b.dy = (int8_t)std::min(std::max((int)(int8_t)(v >> 16) - j.bias[1], -128), 127);
+                b.spx = ((v >> 6) & 1) ? SP_PLUS : SP_ZERO;
+                b.spy = ((v >> 7) & 1) ? SP_PLUS : SP_ZERO;
+                S.mv_new_blocks++;
+                S.mv_new_base_counts[std::min<int>(b.new_base, 4)]++;
+            }
+            S.mv_mode_counts[b.mode]++;
+            if (b.skip) S.blocks_skipped++;
+        }
+        e->mvc.encode_frame(blocks, e->BW, j.mv_bytes);
+        S.mv_bias_dx = j.bias[0];
+        S.mv_bias_dy = j.bias[1];
+        S.rdo_lambda = e->L.lambda;
+    } else {
+        e->mvc.reset();  // key frame: MV entropy contexts restart (enc/encoder.rs:335-337)
+    }
+    const int16_t* packed = s.h_packed.as<int16_t>();
+    const uint8_t* peobs = s.h_peobs.as<uint8_t>();
+    Job* jp = &j;
+    uint32_t count = j.count;
+    bool intra = j.type == 1;
+    j.fut = e->pool->submit([jp, packed, peobs, count, intra] {
+        encode_residual_frame(packed, peobs, (int)count, intra, jp->res_bytes);
+    });
+    j.state = 1;
+    return RIV_OK;
+}
+
+// PackedFrame::to_bytes (com/format.rs:171-207) and the writer call.
+static riv_status write_job(riv_encoder* e, Job& j) {
+    j.fut.get();
+    const riv_config& c = e->cfg;
+    std::vector<uint8_t> rec;
+    rec.reserve(32 + j.mv_bytes.size() + j.res_bytes.size());
+    put_le(rec, j.ts, 8);
+    if (j.type == 1) {
+        rec.push_back(1);
+        rec.push_back(c.intra_quality);
+        put_le(rec, j.res_bytes.size(), 4);
+        rec.insert(rec.end(), j.res_bytes.begin(), j.res_bytes.end());
+    } else {
+        rec.push_back(2);
+        rec.push_back(c.inter_quality);
+        rec.push_back((uint8_t)j.bias[0]);
+        rec.push_back((uint8_t)j.bias[1]);
+        rec.push_back(0);
+        put_le(rec, j.mv_bytes.size(), 4);
+        rec.insert(rec.end(), j.mv_bytes.begin(), j.mv_bytes.end());
+        put_le(rec, j.res_bytes.size(), 4);
+        rec.insert(rec.end(), j.res_bytes.begin(), j.res_bytes.end());
+    }
+    j.stats.total_bytes = (uint32_t)rec.size();
+    j.stats.mv_bytes = (uint32_t)j.mv_bytes.size();
+    j.stats.residual_bytes = (uint32_t)j.res_bytes.size();
+    if (e->wr.write(e->wr.user, rec.data(), rec.size()) != 0) return fail(e, RIV_ERR_IO, "writer.write failed");
+    e->frame_count++;
+    memcpy(e->last_times, j.times, sizeof(j.times));
+    e->have_times = true;
+    e->last_stats = j.stats;
+    return RIV_OK;
+}
+
+// Advance the pipeline.  Frames are retired strictly in order (the MV coder's contexts
+// carry across frames) and written strictly in order.  With `block_front` the oldest
+// frame is driven to completion; everything else only advances if already possible.
+static riv_status pump(riv_encoder* e, bool block_front) {
+    bool block = block_front;
+    for (auto& j : e->jobs) {
+        if (j.state != 0) continue;
+        if (!block) {
+            cudaError_t q = cudaEventQuery(e->slots[j.slot].ev_side);
+            if (q == cudaErrorNotReady) break;
+            if (q != cudaSuccess) throw CudaError{q, "cudaEventQuery"};
+        }
+        riv_status st = retire(e, j);
+        if (st) return st;
+        block = false;
+    }
+    block = block_front;
+    while (!e->jobs.empty()) {
+        Job& f = e->jobs.front();
+        if (f.state != 1) break;
+        if (!block && f.fut.wait_for(std::chrono::seconds(0)) != std::future_status::ready) break;
+        riv_status st = write_job(e, f);
+        if (st) return st;
+        e->jobs.pop_front();
+        block = false;
+    }
+    return RIV_OK;
+}
+
+static riv_status drain_all(riv_encoder* e) {
+    while (!e->jobs.empty()) {
+        riv_status st = pump(e, true);
+        if (st) return st;
+    }
+    return RIV_OK;
+}
+
+static riv_status encode_common(riv_encoder* e, int src, const void* a, const void* b, const void* c3,
+                                uint64_t ts, riv_frame_stats* stats) {
+    if (e->poisoned) return fail(e, RIV_ERR_ENCODING_FAILED, "encoder unusable after an earlier device failure: " + e->err);
+    try {
+        CK(cudaSetDevice(e->cfg.device));
+        size_t cap = e->slots.size();
+        while (e->jobs.size() >= cap) {
+            riv_status st = pump(e, true);
+            if (st) return st;
+        }
+        // frame type (enc/encoder.rs:265-291)
+        const riv_config& c = e->cfg;
+        bool intra;
+        uint64_t n = e->submitted;
+        if (c.keyframe_mode == RIV_KEYFRAME_ALL_INTRA) intra = true;
+        else if (c.keyframe_mode == RIV_KEYFRAME_AUTOMATIC) intra = n % 30 == 0;
+        else intra = n % c.keyframe_interval == 0;
+        if (!e->has_ref) intra = true;
+        e->jobs.emplace_back();
+        Job& j = e->jobs.back();
+        j.index = n;
+        j.ts = ts;
+        j.type = intra ? 1 : 2;
+        j.slot = (int)(n % cap);
+        submit_gpu(e, j, src, a, b, c3);
+        e->submitted++;
+        if (src == 0 || src == 2) CK(cudaEventSynchronize(e->slots[j.slot].ev_h2d));  // caller buffer reusable
+        if (e->cfg.pipeline_depth == 0 || stats) {
+            riv_status st = drain_all(e);
+            if (st) return st;
+            if (stats) *stats = e->last_stats;  // this frame was the last one written
+        } else {
+            riv_status st = pump(e, false);
+            if (st) return st;
+        }
+    } catch (const CudaError& ce) {
+        return fail(e, RIV_ERR_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
+    } catch (const std::exception& ex) {
+        return fail(e, RIV_ERR_ENCODING_FAILED, ex.what());
+    }
+    return RIV_OK;
+}
+
+}  // namespace
+
+// =====================================================================================
+// C ABI
+// =====================================================================================
+extern "C" {
+
+void riv_config_default(riv_config* c, uint32_t w, uint32_t h, uint32_t fps) {
+    memset(c, 0, sizeof(*c));
+    c->display_width = w;
+    c->display_height = h;
+    c->storage_width = (w + 15) / 16 * 16;
+    c->storage_height = (h + 15) / 16 * 16;
+    c->fps = fps;
+    c->keyframe_mode = RIV_KEYFRAME_FIXED;
+    c->keyframe_interval = 30;
+    c->intra_quality = 90;
+    c->inter_quality = 35;
+    c->search_range = 12;
+    c->mv_deflate_level = 6;
+    c->skip_threshold = 3;
+    c->rdo_lambda_mult = 0.49;
+    c->inter_dead_zone = 0.75f;
+    c->device = 0;
+    c->pipeline_depth = 0;
+    c->entropy_threads = 0;
+}
+
+riv_status riv_encoder_new(const riv_config* cfg, const riv_writer_vtable* writer, riv_encoder** out) {
+    if (!cfg || !writer || !out || !writer->write || !writer->position || !writer->seek || !writer->flush)
+        return RIV_ERR_INVALID_CONFIG;
+    *out = nullptr;
+    std::string msg;
+    riv_status st = validate(*cfg, msg);
+    if (st) return st;
+    entropy_init();
+    riv_encoder* e = new riv_encoder();
+    e->cfg = *cfg;
+    e->wr = *writer;
+    try {
+        setup_device(e);
+    } catch (const CudaError& ce) {
+        std::string m = std::string(ce.where) + ": " + cudaGetErrorString(ce.e);
+        fprintf(stderr, "riv_encoder_new: %s\n", m.c_str());
+        riv_encoder_free(e);
+        return RIV_ERR_CUDA;
+    } catch (const std::exception& ex) {
+        fprintf(stderr, "riv_encoder_new: %s\n", ex.what());
+        riv_encoder_free(e);
+        return RIV_ERR_ENCODING_FAILED;
+    }
+    e->header_pos = e->wr.position(e->wr.user);
+    std::vector<uint8_t> h = header_bytes(e->cfg, 0);
+    if (e->wr.write(e->wr.user, h.data(), h.size()) != 0) {
+        riv_encoder_free(e);
+        return RIV_ERR_IO;
+    }
+    *out = e;
+    return RIV_OK;
+}
+
+riv_status riv_encode_frame(riv_encoder* e, const uint8_t* rgb, uint32_t w, uint32_t h, uint64_t ts,
+                            riv_frame_stats* stats) {
+    if (!e) return RIV_ERR_INVALID_CONFIG;
+    if (w != e->cfg.display_width || h != e->cfg.display_height) {  // enc/encoder.rs:237-242
+        char buf[160];
+        snprintf(buf, sizeof(buf), "Frame dimensions (%u, %u) do not match config (%u, %u)", w, h,
+                 e->cfg.display_width, e->cfg.display_height);
+        return fail(e, RIV_ERR_FRAME, buf);
+    }
+    if (!rgb) return fail(e, RIV_ERR_FRAME, "null frame data");
+    riv_frame_stats tmp;
+    riv_status st = encode_common(e, 0, rgb, nullptr, nullptr, ts, stats ? &tmp : nullptr);
+    if (st == RIV_OK && stats) *stats = tmp;
+    return st;
+}
+
+riv_status riv_encode_frame_device(riv_encoder* e, const void* d_rgb, uint64_t ts, riv_frame_stats* stats) {
+    if (!e || !d_rgb) return RIV_ERR_FRAME;
+    riv_frame_stats tmp;
+    riv_status st = encode_common(e, 1, d_rgb, nullptr, nullptr, ts, stats ? &tmp : nullptr);
+    if (st == RIV_OK && stats) *stats = tmp;
+    return st;
+}
+
+riv_status riv_encode_frame_yuv(riv_encoder* e, const uint8_t* y, const uint8_t* u, const uint8_t* v, uint64_t ts,
+                                riv_frame_stats* stats) {
+    if (!e || !y || !u || !v) return RIV_ERR_FRAME;
+    riv_frame_stats tmp;
+    riv_status st = encode_common(e, 2, y, u, v, ts, stats ? &tmp : nullptr);
+    if (st == RIV_OK && stats) *stats = tmp;
+    return st;
+}
+
+riv_status riv_finish(riv_encoder* e) {  // enc/encoder.rs:950-961
+    if (!e) return RIV_ERR_INVALID_CONFIG;
+    try {
+        CK(cudaSetDevice(e->cfg.device));
+        riv_status st = drain_all(e);
+        if (st) return st;
+    } catch (const CudaError& ce) {
+        return fail(e, RIV_ERR_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
+    }
+    uint64_t end = e->wr.position(e->wr.user);
+    if (e->wr.seek(e->wr.user, e->header_pos) != 0) return fail(e, RIV_ERR_IO, "writer.seek failed");
+    std::vector<uint8_t> h = header_bytes(e->cfg, e->frame_count);
+    if (e->wr.write(e->wr.user, h.data(), h.size()) != 0) return fail(e, RIV_ERR_IO, "writer.write failed");
+    if (e->wr.seek(e->wr.user, end) != 0) return fail(e, RIV_ERR_IO, "writer.seek failed");
+    if (e->wr.flush(e->wr.user) != 0) return fail(e, RIV_ERR_IO, "writer.flush failed");
+    return RIV_OK;
+}
+
+void riv_encoder_free(riv_encoder* e) {
+    if (!e) return;
+    cudaSetDevice(e->cfg.device);
+    for (auto& j : e->jobs)
+        if (j.fut.valid()) j.fut.wait();
+    e->pool.reset();
+    if (e->S) cudaStreamSynchronize(e->S);
+    if (e->C) cudaStreamSynchronize(e->C);
+    for (auto& s : e->slots) {
+        s.rgb.release(); s.side.release(); s.index.release(); s.packed.release(); s.peobs.release(); s.count.release();
+        s.h_side.release(); s.h_count.release(); s.h_packed.release(); s.h_peobs.release(); s.h_status.release();
+        if (s.ev_h2d) cudaEventDestroy(s.ev_h2d);
+        if (s.ev_gpu) cudaEventDestroy(s.ev_gpu);
+        if (s.ev_side) cudaEventDestroy(s.ev_side);
+        if (s.ev_coef) cudaEventDestroy(s.ev_coef);
+        for (int k = 0; k < EV_N; k++)
+            if (s.ev_k[k]) cudaEventDestroy(s.ev_k[k]);
+    }
+    DevBuf* bufs[] = {&e->cur, &e->ref[0], &e->ref[1], &e->pred, &e->mbout, &e->coded[0], &e->coded[1], &e->rec,
+                      &e->varsum, &e->lnv, &e->qs, &e->coeffs, &e->opt_skip, &e->fmask, &e->eobs, &e->status,
+                      &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab};
+    for (DevBuf* b : bufs) b->release();
+    if (e->S) cudaStreamDestroy(e->S);
+    if (e->C) cudaStreamDestroy(e->C);
+    delete e;
+}
+
+const char* riv_last_error(const riv_encoder* e) { return e ? e->err.c_str() : "null encoder"; }
+uint64_t riv_frame_count(const riv_encoder* e) { return e ? e->frame_count : 0; }
+
+riv_status riv_last_recon(riv_encoder* e, uint8_t* y, uint8_t* u, uint8_t* v) {
+    if (!e || !e->has_ref) return RIV_ERR_FRAME;
+    try {
+        CK(cudaSetDevice(e->cfg.device));
+        CK(cudaStreamSynchronize(e->S));
+        const uint8_t* d = e->ref[e->ref_cur].as<uint8_t>();
+        size_t ys = (size_t)e->W * e->H, cs = ys / 4;
+        CK(cudaMemcpy(y, d, ys, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(u, d + ys, cs, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(v, d + ys + cs, cs, cudaMemcpyDeviceToHost));
+    } catch (const CudaError& ce) {
+        return fail(e, RIV_ERR_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
+    }
+    return RIV_OK;
+}
+
+riv_status riv_debug_frame_state(riv_encoder* e, int what, void* out, size_t size) {
+    if (!e || !out) return RIV_ERR_FRAME;
+    const DevBuf* b = nullptr;
+    switch (what) {
+        case 0: b = &e->mbout; break;
+        case 1: b = &e->qs; break;
+        case 2: b = &e->pred; break;
+        case 3: b = &e->cur; break;
+        case 4: b = &e->coeffs; break;
+        case 5: b = &e->opt_skip; break;
+        default: return RIV_ERR_FRAME;
+    }
+    if (size < b->n) return RIV_ERR_FRAME;
+    try {
+        CK(cudaSetDevice(e->cfg.device));
+        CK(cudaStreamSynchronize(e->S));
+        CK(cudaMemcpy(out, b->p, b->n, cudaMemcpyDeviceToHost));
+    } catch (const CudaError& ce) {
+        return fail(e, RIV_ERR_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
+    }
+    return RIV_OK;
+}
+
+riv_status riv_last_kernel_times(riv_encoder* e, float* us8) {
+    if (!e || !e->have_times) return RIV_ERR_FRAME;
+    memcpy(us8, e->last_times, sizeof(e->last_times));
+    return RIV_OK;
+}
+
+// ---- in-memory writer (VecWriter semantics, enc/writer.rs:49-69) ----
+struct riv_memwriter {
+    std::vector<uint8_t> buf;
+    uint64_t pos = 0;
+};
+static int mw_write(void* u, const uint8_t* d, size_t n) {
+    riv_memwriter* w = (riv_memwriter*)u;
+    if (w->pos + n > w->buf.size()) w->buf.resize(w->pos + n, 0);
+    memcpy(w->buf.data() + w->pos, d, n);
+    w->pos += n;
+    return 0;
+}
+static uint64_t mw_position(void* u) { return ((riv_memwriter*)u)->pos; }
+static int mw_seek(void* u, uint64_t p) {
+    riv_memwriter* w = (riv_memwriter*)u;
+    if (p > w->buf.size()) w->buf.resize(p, 0);
+    w->pos = p;
+    return 0;
+}
+static int mw_flush(void*) { return 0; }
+riv_memwriter* riv_memwriter_new(void) { return new riv_memwriter(); }
+void riv_memwriter_vtable(riv_memwriter* w, riv_writer_vtable* o) {
+    o->write = mw_write;
+    o->position = mw_position;
+    o->seek = mw_seek;
+    o->flush = mw_flush;
+    o->user = w;
+}
+size_t riv_memwriter_size(const riv_memwriter* w) { return w->buf.size(); }
+const uint8_t* riv_memwriter_data(const riv_memwriter* w) { return w->buf.data(); }
+void riv_memwriter_free(riv_memwriter* w) { delete w; }
+
+// ---- stage entry points ----
+riv_status riv_stage_rgb_to_yuv(const uint8_t* rgb, uint32_t dw, uint32_t dh, uint32_t sw, uint32_t sh, uint8_t* out) {
+    if (!rgb || !out || sw < dw || sh < dh || sw % 2 || sh % 2) return RIV_ERR_FRAME;
+    void *d_rgb = nullptr, *d_yuv = nullptr;
+    size_t nin = (size_t)dw * dh * 3, nout = (size_t)sw * sh * 3 / 2;
+    riv_status st = RIV_OK;
+    if (cudaMalloc(&d_rgb, nin) || cudaMalloc(&d_yuv, nout) || cudaMemcpy(d_rgb, rgb, nin, cudaMemcpyHostToDevice) ||
+        launch_rgb_to_yuv((const uint8_t*)d_rgb, (int)dw, (int)dh, (uint8_t*)d_yuv, (int)sw, (int)sh, 0) ||
+        cudaMemcpy(out, d_yuv, nout, cudaMemcpyDeviceToHost))
+        st = RIV_ERR_CUDA;
+    cudaFree(d_rgb);
+    cudaFree(d_yuv);
+    return st;
+}
+
+riv_status riv_stage_deblock(uint8_t* yuv, uint32_t w, uint32_t h, int level, int intra, const uint8_t* mask) {
+    if (!yuv || w % 16 || h % 16) return RIV_ERR_FRAME;
+    if (level <= 0) return RIV_OK;
+    int E, I, Hv;
+    deblock_thresholds(level, intra != 0, E, I, Hv);
+    size_t n = (size_t)w * h * 3 / 2, nm = (size_t)(w / 16) * (h / 16);
+    void *d = nullptr, *dm = nullptr;
+    riv_status st = RIV_OK;
+    if (cudaMalloc(&d, n) || cudaMemcpy(d, yuv, n, cudaMemcpyHostToDevice)) st = RIV_ERR_CUDA;
+    if (!st && mask && (cudaMalloc(&dm, nm) || cudaMemcpy(dm, mask, nm, cudaMemcpyHostToDevice))) st = RIV_ERR_CUDA;
+    if (!st && (launch_deblock((uint8_t*)d, (int)w, (int)h, E, I, Hv, (const uint8_t*)dm, 0) ||
+                cudaMemcpy(yuv, d, n, cudaMemcpyDeviceToHost)))
+        st = RIV_ERR_CUDA;
+    cudaFree(d);
+    cudaFree(dm);
+    return st;
+}
+
+riv_status riv_stage_libm(int which, const float* in, float* out, size_t n) {
+    LibmFix& F = libm_fix();
+    if (!F.ok) return RIV_ERR_ENCODING_FAILED;
+    const std::vector<uint32_t>& fx = which == 0 ? F.logf : F.exp2f;
+    void *di = nullptr, *dout = nullptr, *df = nullptr;
+    riv_status st = RIV_OK;
+    if (cudaMalloc(&di, n * 4) || cudaMalloc(&dout, n * 4) || cudaMalloc(&df, fx.size() * 4 + 4) ||
+        cudaMemcpy(di, in, n * 4, cudaMemcpyHostToDevice) ||
+        cudaMemcpy(df, fx.data(), fx.size() * 4, cudaMemcpyHostToDevice) ||
+        launch_libm_eval(which, (const float*)di, (float*)dout, n, (const uint32_t*)df, (int)(fx.size() / 2), 0) ||
+        cudaMemcpy(out, dout, n * 4, cudaMemcpyDeviceToHost))
+        st = RIV_ERR_CUDA;
+    cudaFree(di);
+    cudaFree(dout);
+    cudaFree(df);
+    return st;
+}
+
+riv_status riv_libm_fixup_counts(uint32_t* nlog, uint32_t* nexp) {
+    LibmFix& F = libm_fix();
+    if (!F.ok) return RIV_ERR_ENCODING_FAILED;
+    *nlog = (uint32_t)(F.logf.size() / 2);
+    *nexp = (uint32_t)(F.exp2f.size() / 2);
+    return RIV_OK;
+}
+
+void riv_dct_tables(int32_t* t16, int32_t* t8) { dct_tables(t16, t8); }
+
+}  // extern "C"

@@ -1,0 +1,86 @@
+// riv_internal.h -- shared definitions between the sm_100a kernels and the host encoder.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace riv {
+
+// Per-macroblock output of the search/mode kernel (k_search) -- 20 bytes.
+struct MbOut {
+    int8_t raw[4];     // canonical search MV: dx, dy, sx, sy (enc/motion/scalar.rs:619-635)
+    int8_t coded[4];   // coded_prefix (reconstructed) MV (enc/encoder.rs:667-718)
+    int8_t rdelta[2];  // NEW raw delta = clamp(actual - base) (enc/encoder.rs:654-656)
+    uint8_t mode;      // MvMode::as_u8 (res/mv_predictor.rs:22-32)
+    uint8_t base;      // NEW base index 0..4
+    uint8_t flags;     // fractional bits for NEW (0x01 x+1/2, 0x04 y+1/2), skip bit patched later
+    uint8_t rdo_skip;  // RDO skip candidate (enc/rdo.rs:140-178)
+    uint8_t pad[2];
+    int32_t best_sad;  // half-pel refinement SAD of the chosen MV
+};
+static_assert(sizeof(MbOut) == 20, "MbOut layout");
+
+// Per-macroblock record published by the search wavefront for the next MB row:
+// [63:48] frame tag, [47:40] raw dx, [39:32] raw dy, [31:24] coded dx, [23:16] coded dy,
+// [15:8] coded sx, [7:0] coded sy.
+typedef unsigned long long MbRec;
+
+struct SearchParams {
+    const uint8_t* ref_y;
+    const uint8_t* cur_y;
+    int W, H, BW, BH, sr;
+    const int8_t* prev_coded;  // 4 bytes/MB from the previous P-frame, or nullptr
+    long long zthr, pthr;
+    double lam2;      // lambda * 2.0 (the search's bit-cost scale)
+    long long c15;    // (lambda * 2.0 * 1.5) as i64
+    long long c05;    // (lambda * 2.0 * 0.5) as i64
+    int lambda_zero;  // lambda == 0.0
+    const double* mvbits;  // 256 entries: b(0)=1, b(d)=2*log2(d)+2 (glibc log2, host-computed)
+    // RDO (enc/rdo.rs)
+    double rdo_lambda, rdo_skip_bits, rdo_keep_bits, rdo_icpt, rdo_slope, rdo_ret, rdo_guard;
+    int rdo_allow;
+    MbRec* rec;
+    unsigned tag;
+    MbOut* out;
+    unsigned* status;
+    long long spin_limit;
+};
+
+struct ResidualParams {
+    const uint8_t* cur;   // planar YUV (Y then U then V)
+    const uint8_t* pred;  // planar YUV
+    uint8_t* recon;       // planar YUV (pre-deblock)
+    int16_t* coeffs;      // 384 per MB
+    uint8_t* opt_skip;    // 1 byte per MB
+    uint8_t* fmask;       // deblock mask, 1 byte per MB
+    uint8_t* eobs;        // 3 per MB (last non-zero index per plane block)
+    const MbOut* mb;      // nullptr for intra
+    const float* qs;      // per-MB quant step (inter)
+    float dead_zone;
+    int W, H, BW, intra;
+    const uint16_t* intra_ytab;  // 256 (intra)
+    const uint16_t* intra_ctab;  // 64 (intra)
+};
+
+enum StatusBits : unsigned {
+    ST_WAIT_TIMEOUT = 1u,
+    ST_HEX_CAP = 2u,
+};
+
+// Launchers (riv_kernels.cu).  All are asynchronous on `stream`.
+int launch_rgb_to_yuv(const uint8_t* rgb, int dw, int dh, uint8_t* yuv, int W, int H, void* stream);
+int launch_search(const SearchParams& p, int grid, void* stream);
+int search_max_grid(int sr, int* grid_out);
+size_t search_smem_bytes(int sr);
+int launch_predict(const uint8_t* ref, const MbOut* mb, uint8_t* pred, uint2* varsum, int W, int H, void* stream);
+int launch_aq(const uint2* varsum, int n, float base, const uint32_t* logfix, int nlog, const uint32_t* expfix,
+              int nexp, float* lnv_scratch, float* qs, void* stream);
+int launch_residual(const ResidualParams& p, int nmb, void* stream);
+int launch_deblock(uint8_t* yuv, int W, int H, int E, int I, int Hev, const uint8_t* mask, void* stream);
+int launch_compact(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coeffs, const uint8_t* eobs, int nmb,
+                   int intra, uint32_t* side, int32_t* index, int16_t* packed, uint8_t* packed_eobs, uint32_t* count,
+                   void* stream);
+// libm device helpers exposed for the exhaustive check
+int launch_libm_eval(int which, const float* in, float* out, size_t n, const uint32_t* fix, int nfix, void* stream);
+
+}  // namespace riv

@@ -1,0 +1,1079 @@
+// riv_kernels.cu -- sm_100a kernels of the riv2 P-frame encoder hot path.
+//
+// Reference semantics (paths relative to the reference project root):
+//   enc/ = reitero_video/reitero_encode/src/       com/ = reitero_video/reitero_video_common/src/
+//   res/ = reitero_video/reitero_residual/src/     dct/ = reitero_video/reitero_dct/src/
+// Floating point reproduces the reference op for op with explicit round-to-nearest
+// intrinsics (__fadd_rn, __dmul_rn, ...): no FMA contraction the reference lacks.
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cstdint>
+
+#include "riv_internal.h"
+
+namespace riv {
+
+// ---------------------------------------------------------------------------------
+// Shared tables
+// ---------------------------------------------------------------------------------
+// T16[i][j] = round(2^18 * c_j * cos((2i+1) j pi / 32)), T8 likewise with /16: the
+// reference's fixed-point DCT bases (dct/dct16.rs:7-145, dct/dct8.rs:6-25), uploaded by
+// the host (which derives them from the formula) into constant memory.
+__constant__ int32_t c_T16[256];
+__constant__ int32_t c_T8[64];
+
+// ---------------------------------------------------------------------------------
+// K1: RGB24 (display size) -> planar YUV 4:2:0 (storage size), pad fused.
+// pad_rgb24 (enc/encoder.rs:1049-1096) == reading the display frame at clamped
+// coordinates.  BT.709 limited range, 13-bit fixed point (same definition as the oracle).
+// ---------------------------------------------------------------------------------
+__global__ void k_rgb_to_yuv(const uint8_t* __restrict__ rgb, int dw, int dh, uint8_t* __restrict__ Yp,
+                             uint8_t* __restrict__ Up, uint8_t* __restrict__ Vp, int W, int H) {
+    int cx = blockIdx.x * blockDim.x + threadIdx.x;
+    int cy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (cx >= W / 2 || cy >= H / 2) return;
+    int sr = 0, sg = 0, sb = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        int x = 2 * cx + (k & 1), y = 2 * cy + (k >> 1);
+        int sx = min(x, dw - 1), sy = min(y, dh - 1);
+        const uint8_t* p = rgb + ((size_t)sy * dw + sx) * 3;
+        int r = p[0], g = p[1], b = p[2];
+        int v = (1496 * r + 5032 * g + 508 * b + (16 << 13) + (1 << 12)) >> 13;
+        Yp[(size_t)y * W + x] = (uint8_t)min(max(v, 16), 235);
+        sr += r; sg += g; sb += b;
+    }
+    int r = (sr + 2) >> 2, g = (sg + 2) >> 2, b = (sb + 2) >> 2;
+    int cb = (-824 * r - 2774 * g + 3598 * b + (128 << 13) + (1 << 12)) >> 13;
+    int cr = (3598 * r - 3268 * g - 330 * b + (128 << 13) + (1 << 12)) >> 13;
+    size_t ci = (size_t)cy * (W / 2) + cx;
+    Up[ci] = (uint8_t)min(max(cb, 16), 240);
+    Vp[ci] = (uint8_t)min(max(cr, 16), 240);
+}
+
+int launch_rgb_to_yuv(const uint8_t* rgb, int dw, int dh, uint8_t* yuv, int W, int H, void* stream) {
+    dim3 blk(64, 4), grd((W / 2 + 63) / 64, (H / 2 + 3) / 4);
+    uint8_t* Y = yuv;
+    uint8_t* U = yuv + (size_t)W * H;
+    uint8_t* V = U + (size_t)(W / 2) * (H / 2);
+    k_rgb_to_yuv<<<grd, blk, 0, (cudaStream_t)stream>>>(rgb, dw, dh, Y, U, V, W, H);
+    return (int)cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------
+// K4: motion search + RDO skip + MV mode decision, one warp per macroblock row.
+//
+// The reference processes macroblocks in raster order; each block's seeds, MV-cost
+// predictors and coded-MV predictors depend on its left, top, top-right and top-left
+// neighbours (enc/motion/scalar.rs:56-156, res/mv_predictor.rs:59-272).  Here CTA r
+// owns MB rows r, r+grid, ...; it walks its row left to right keeping the left
+// neighbour in registers and waits (bounded spin, acquire) for the top-right record
+// published by the CTA of row r-1.  Critical path = (BW + 2*(BH-1)) MB steps with only
+// BH-1 cross-CTA hand-offs.
+//
+// Within an MB every round of candidates (seeds, one hex ring, the diamond, the nine
+// half-pel points) is evaluated in parallel: each lane owns 8 pixels (half a row) and
+// forms partial SADs for every candidate, reduced with redux.sync.  The reference
+// evaluates candidates sequentially with early-exit limits; an early exit only ever
+// returns a partial SAD already above the limit (so the candidate cannot win), hence
+// full SADs followed by the same in-order strict-'<' scan give identical decisions.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned warp_sum(unsigned v) { return __reduce_add_sync(0xffffffffu, v); }
+
+struct CostCtx {
+    int nx, ny, rx, ry, mx, my;
+};
+
+// estimate_mv_cost (enc/motion/scalar.rs:453-544)
+__device__ __forceinline__ long long mv_cost(int dx, int dy, const CostCtx& c, const SearchParams& p,
+                                             const double* bits) {
+    if (p.lambda_zero) return 0;
+    long long best = LLONG_MAX;
+    if ((dx == c.nx && dy == c.ny) || (dx == c.rx && dy == c.ry) || (dx == c.mx && dy == c.my)) best = p.c15;
+    if (dx == 0 && dy == 0) best = min(best, p.c05);
+    {
+        double b = __dadd_rn(__dadd_rn(6.0, bits[abs(dx - c.nx)]), bits[abs(dy - c.ny)]);
+        best = min(best, __double2ll_rz(__dmul_rn(p.lam2, b)));
+    }
+    {
+        double b = __dadd_rn(__dadd_rn(6.0, bits[abs(dx - c.rx)]), bits[abs(dy - c.ry)]);
+        best = min(best, __double2ll_rz(__dmul_rn(p.lam2, b)));
+    }
+    return best;
+}
+
+// Integer SAD partial over this lane's 8 pixels, reproducing the per-4x4 sub-block
+// clamped reference origin of the reference's edge path (enc/motion/satd_scalar.rs:26-97);
+// for interior candidates the clamps are no-ops and this equals the plain 16x16 SAD.
+__device__ __forceinline__ unsigned sad_int_part(const uint8_t* win, int WS, int wx0, int wy0, int x0, int y0,
+                                                 int W, int H, int dx, int dy, int yy, int g0, const uint8_t* cur8) {
+    int ry = min(max(y0 + (yy & ~3) + dy, 0), H - 4) + (yy & 3);
+    const uint8_t* row = win + (ry - wy0) * WS;
+    int rx0 = min(max(x0 + 4 * g0 + dx, 0), W - 4) - wx0;
+    int rx1 = min(max(x0 + 4 * g0 + 4 + dx, 0), W - 4) - wx0;
+    unsigned s = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) s += (unsigned)abs((int)cur8[k] - (int)row[rx0 + k]);
+#pragma unroll
+    for (int k = 0; k < 4; k++) s += (unsigned)abs((int)cur8[4 + k] - (int)row[rx1 + k]);
+    return s;
+}
+
+struct MvT {
+    int dx, dy, sx, sy;
+};
+__device__ __forceinline__ bool mv_eq(const MvT& a, const MvT& b) {
+    return a.dx == b.dx && a.dy == b.dy && a.sx == b.sx && a.sy == b.sy;
+}
+__device__ __forceinline__ int mv_class(int mag) {  // res/mv_rans.rs:80-86
+    if (mag == 0) return 0;
+    return min(32 - __clz(mag), 10);
+}
+__device__ __forceinline__ int comp_bits(int d) {  // enc/encoder.rs:142-154
+    int c = mv_class(abs(d));
+    return c == 0 ? 4 : 4 + c;
+}
+__device__ __forceinline__ int sat8(int v) { return min(max(v, -128), 127); }
+
+__device__ __forceinline__ int median3(int a, int b, int c) {  // enc/motion/scalar.rs:24-43
+    if (a > b) return b > c ? b : (a > c ? c : a);
+    return a > c ? a : (b > c ? c : b);
+}
+
+__global__ void __launch_bounds__(32) k_search(SearchParams p) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    double* bits = (double*)smem;  // 256 doubles
+    uint8_t* win = smem + 256 * sizeof(double);
+    const int lane = threadIdx.x;
+    const int sr = p.sr;
+    const int WS = 18 + 2 * sr;
+    for (int i = lane; i < 256; i += 32) bits[i] = p.mvbits[i];
+    const int yy = lane >> 1;       // this lane's row inside the MB
+    const int xoff = (lane & 1) * 8;  // and its 8-pixel half
+    const int g0 = (lane & 1) * 2;    // first 4x4 sub-block column of the half
+    const unsigned long long tagbits = (unsigned long long)(p.tag & 0xffffu) << 48;
+    bool failed = false;
+
+    for (int r = blockIdx.x; r < p.BH; r += gridDim.x) {
+        const int y0 = r * 16;
+        const int wy0 = y0 - sr - 1;
+        // Left neighbour (this row, previous MB): raw (dx,dy) and coded tuple.
+        MvT L_raw{0, 0, 0, 0}, L_cod{0, 0, 0, 0};
+        // Records of the row above, sliding: TL, T, TR.
+        unsigned long long recT = 0, recTL = 0;
+        for (int bx = 0; bx < p.BW; bx++) {
+            const int x0 = bx * 16;
+            const int wx0 = x0 - sr - 1;
+            const int idx = r * p.BW + bx;
+            // ---- stage the reference window (replicated borders) and the current block
+            __syncwarp();
+            for (int i = lane; i < WS * WS; i += 32) {
+                int wr = i / WS, wc = i - wr * WS;
+                int gy = min(max(wy0 + wr, 0), p.H - 1), gx = min(max(wx0 + wc, 0), p.W - 1);
+                win[i] = p.ref_y[(size_t)gy * p.W + gx];
+            }
+            uint8_t cur8[8];
+            {
+                const uint2 c = *(const uint2*)(p.cur_y + (size_t)(y0 + yy) * p.W + x0 + xoff);
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    cur8[k] = (uint8_t)(c.x >> (8 * k));
+                    cur8[4 + k] = (uint8_t)(c.y >> (8 * k));
+                }
+            }
+            // ---- wait for the row above (top-right, or top at the last column)
+            unsigned long long recTR = 0;
+            bool has_tr = false;
+            if (r > 0) {
+                int wi = (r - 1) * p.BW + min(bx + 1, p.BW - 1);
+                unsigned long long v = 0;
+                if (lane == 0) {
+                    long long spins = 0;
+                    v = ld_acquire_u64(p.rec + wi);
+                    while ((v & 0xffff000000000000ull) != tagbits) {
+                        if (++spins > p.spin_limit || failed) { failed = true; break; }
+                        __nanosleep(20);
+                        v = ld_acquire_u64(p.rec + wi);
+                    }
+                    if (bx == 0) recT = ld_acquire_u64(p.rec + (r - 1) * p.BW);
+                }
+                failed = __shfl_sync(0xffffffffu, (int)failed, 0) != 0;
+                v = __shfl_sync(0xffffffffu, v, 0);
+                recT = __shfl_sync(0xffffffffu, recT, 0);
+                if (bx + 1 < p.BW) { recTR = v; has_tr = true; }
+            }
+            __syncwarp();
+            if (failed) {
+                if (lane == 0) atomicOr(p.status, ST_WAIT_TIMEOUT);
+                return;
+            }
+            const bool has_t = r > 0, has_l = bx > 0, has_tl = r > 0 && bx > 0;
+            auto rec_raw = [](unsigned long long v, int& dx, int& dy) {
+                dx = (int)(int8_t)(v >> 40); dy = (int)(int8_t)(v >> 32);
+            };
+            auto rec_cod = [](unsigned long long v) {
+                return MvT{(int)(int8_t)(v >> 24), (int)(int8_t)(v >> 16), (int)(int8_t)(v >> 8), (int)(int8_t)v};
+            };
+            int Tx = 0, Ty = 0, TRx = 0, TRy = 0, TLx = 0, TLy = 0;
+            if (has_t) rec_raw(recT, Tx, Ty);
+            if (has_tr) rec_raw(recTR, TRx, TRy);
+            if (has_tl) rec_raw(recTL, TLx, TLy);
+            const bool has_tm = p.prev_coded != nullptr;
+            int Tmx = 0, Tmy = 0;
+            MvT Tm_cod{0, 0, 0, 0};
+            if (has_tm) {
+                const int8_t* pc = p.prev_coded + 4 * idx;
+                Tm_cod = MvT{pc[0], pc[1], pc[2], pc[3]};
+                Tmx = Tm_cod.dx; Tmy = Tm_cod.dy;
+            }
+            // ---- seeds, nearest/near/median (enc/motion/scalar.rs:56-156)
+            int px[5], py[5], np = 0;
+            if (has_l) { px[np] = L_raw.dx; py[np] = L_raw.dy; np++; }
+            if (has_t) { px[np] = Tx; py[np] = Ty; np++; }
+            if (has_tr) { px[np] = TRx; py[np] = TRy; np++; }
+            if (has_tl) { px[np] = TLx; py[np] = TLy; np++; }
+            if (has_tm) { px[np] = Tmx; py[np] = Tmy; np++; }
+            int ux[5], uy[5], nu = 0;
+            for (int i = 0; i < np; i++) {
+                bool dup = false;
+                for (int j = 0; j < nu; j++) dup |= (ux[j] == px[i] && uy[j] == py[i]);
+                if (!dup) { ux[nu] = px[i]; uy[nu] = py[i]; nu++; }
+            }
+            CostCtx cc;
+            cc.nx = nu > 0 ? ux[0] : 0; cc.ny = nu > 0 ? uy[0] : 0;
+            cc.rx = nu > 1 ? ux[1] : 0; cc.ry = nu > 1 ? uy[1] : 0;
+            {
+                int lx = has_l ? L_raw.dx : 0, ly = has_l ? L_raw.dy : 0;
+                int tx = has_t ? Tx : 0, ty = has_t ? Ty : 0;
+                int qx = 0, qy = 0;
+                if (has_tr) { qx = TRx; qy = TRy; }
+                else if (has_tl) { qx = TLx; qy = TLy; }
+                cc.mx = median3(lx, tx, qx);
+                cc.my = median3(ly, ty, qy);
+            }
+            // seed candidate list: (0,0) first, then predictors in order, deduped, within sr
+            int cxs[6], cys[6], nc = 0;
+            cxs[nc] = 0; cys[nc] = 0; nc++;
+            for (int i = 0; i < np; i++) {
+                if (abs(px[i]) > sr || abs(py[i]) > sr) continue;
+                bool dup = false;
+                for (int j = 0; j < nc; j++) dup |= (cxs[j] == px[i] && cys[j] == py[i]);
+                if (!dup) { cxs[nc] = px[i]; cys[nc] = py[i]; nc++; }
+            }
+            __syncwarp();  // window visible to all lanes
+            // ---- zero SAD and the seed round (all seeds + zero in one parallel round)
+            unsigned part[6];
+#pragma unroll
+            for (int i = 0; i < 6; i++)
+                part[i] = i < nc ? sad_int_part(win, WS, wx0, wy0, x0, y0, p.W, p.H, cxs[i], cys[i], yy, g0, cur8) : 0u;
+            long long sads[6];
+#pragma unroll
+            for (int i = 0; i < 6; i++) sads[i] = (long long)warp_sum(part[i]);
+            long long zero_sad = sads[0];
+            int sdx = 0, sdy = 0;
+            long long scost = zero_sad + mv_cost(0, 0, cc, p, bits);
+            bool skip_int = p.zthr > 0 && zero_sad <= p.zthr;
+            if (!skip_int) {
+                for (int i = 1; i < nc; i++) {
+                    long long t = sads[i] + mv_cost(cxs[i], cys[i], cc, p, bits);
+                    if (t < scost) { scost = t; sdx = cxs[i]; sdy = cys[i]; }
+                }
+                long long cur_sad = scost - mv_cost(sdx, sdy, cc, p, bits);
+                if (p.pthr > 0 && cur_sad <= p.pthr) skip_int = true;
+            }
+            if (!skip_int) {
+                // large hexagon (enc/motion/scalar.rs:694-729)
+                const int HX[6] = {2, 1, -1, -2, -1, 1}, HY[6] = {0, 2, 2, 0, -2, -2};
+                int iter = 0;
+                for (;;) {
+                    unsigned hp[6];
+#pragma unroll
+                    for (int k = 0; k < 6; k++) {
+                        int dx = sdx + HX[k], dy = sdy + HY[k];
+                        hp[k] = (abs(dx) <= sr && abs(dy) <= sr)
+                                    ? sad_int_part(win, WS, wx0, wy0, x0, y0, p.W, p.H, dx, dy, yy, g0, cur8) : 0u;
+                    }
+                    bool improved = false;
+                    int cx = sdx, cy = sdy;
+#pragma unroll
+                    for (int k = 0; k < 6; k++) {
+                        long long s = (long long)warp_sum(hp[k]);
+                        int dx = cx + HX[k], dy = cy + HY[k];
+                        if (abs(dx) > sr || abs(dy) > sr) continue;
+                        long long t = s + mv_cost(dx, dy, cc, p, bits);
+                        if (t < scost) { scost = t; sdx = dx; sdy = dy; improved = true; }
+                    }
+                    if (!improved) break;
+                    if (++iter > 4096) {  // cost strictly decreases, so this is never reached
+                        if (lane == 0) atomicOr(p.status, ST_HEX_CAP);
+                        break;
+                    }
+                }
+                // small diamond (enc/motion/scalar.rs:731-756)
+                const int DX[4] = {1, -1, 0, 0}, DY[4] = {0, 0, 1, -1};
+                unsigned dp[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    int dx = sdx + DX[k], dy = sdy + DY[k];
+                    dp[k] = (abs(dx) <= sr && abs(dy) <= sr)
+                                ? sad_int_part(win, WS, wx0, wy0, x0, y0, p.W, p.H, dx, dy, yy, g0, cur8) : 0u;
+                }
+                int cx = sdx, cy = sdy;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    long long s = (long long)warp_sum(dp[k]);
+                    int dx = cx + DX[k], dy = cy + DY[k];
+                    if (abs(dx) > sr || abs(dy) > sr) continue;
+                    long long t = s + mv_cost(dx, dy, cc, p, bits);
+                    if (t < scost) { scost = t; sdx = dx; sdy = dy; }
+                }
+            }
+            // ---- half-pel refinement (enc/motion/scalar.rs:759-839): the nine floor-averaged
+            // candidates around (2*sdx, 2*sdy) from the 3x3 integer neighbourhood of each pixel.
+            unsigned hpart[9];
+#pragma unroll
+            for (int k = 0; k < 9; k++) hpart[k] = 0;
+            {
+                const int Yc = y0 + yy + sdy - wy0;  // window row of the centre sample
+                const uint8_t* r0 = win + (Yc - 1) * WS;
+                const uint8_t* r1 = r0 + WS;
+                const uint8_t* r2 = r1 + WS;
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    const int Xc = x0 + xoff + k + sdx - wx0;
+                    int n00 = r0[Xc - 1], n01 = r0[Xc], n02 = r0[Xc + 1];
+                    int n10 = r1[Xc - 1], n11 = r1[Xc], n12 = r1[Xc + 1];
+                    int n20 = r2[Xc - 1], n21 = r2[Xc], n22 = r2[Xc + 1];
+                    int c = cur8[k];
+                    int v[9];
+                    v[0] = (n00 + n01 + n10 + n11) >> 2;  // (sx,sy) = (-1,-1)
+                    v[1] = (n01 + n11) >> 1;              // ( 0,-1)
+                    v[2] = (n01 + n02 + n11 + n12) >> 2;  // (+1,-1)
+                    v[3] = (n10 + n11) >> 1;              // (-1, 0)
+                    v[4] = n11;                           // ( 0, 0)
+                    v[5] = (n11 + n12) >> 1;              // (+1, 0)
+                    v[6] = (n10 + n11 + n20 + n21) >> 2;  // (-1,+1)
+                    v[7] = (n11 + n21) >> 1;              // ( 0,+1)
+                    v[8] = (n11 + n12 + n21 + n22) >> 2;  // (+1,+1)
+#pragma unroll
+                    for (int q = 0; q < 9; q++) hpart[q] += (unsigned)abs(c - v[q]);
+                }
+            }
+            long long hs[9];
+#pragma unroll
+            for (int q = 0; q < 9; q++) hs[q] = (long long)warp_sum(hpart[q]);
+            long long best_total = hs[4], best_sad = hs[4];
+            int bsx = 0, bsy = 0;
+            for (int q = 0; q < 9; q++) {
+                if (q == 4) continue;
+                int sx = q % 3 - 1, sy = q / 3 - 1;
+                if ((sdx == -128 && sx == -1) || (sdy == -128 && sy == -1)) continue;
+                long long pen = p.c15;  // every neighbour is fractional in at least one axis
+                if (best_total - pen < 0) continue;
+                if (hs[q] + pen < best_total) { best_total = hs[q] + pen; best_sad = hs[q]; bsx = sx; bsy = sy; }
+            }
+            int dxh = min(max(2 * sdx + bsx, -255), 255), dyh = min(max(2 * sdy + bsy, -255), 255);
+            // MotionVector::new(dx_hp/2, dy_hp/2, dx_hp%2, dy_hp%2).as_canonicalized()
+            MvT raw{sat8(dxh / 2), sat8(dyh / 2), dxh % 2, dyh % 2};
+            if (raw.dx == -128 && raw.sx == -1) raw.sx = 0;
+            if (raw.dy == -128 && raw.sy == -1) raw.sy = 0;
+            if (raw.sx == -1) { raw.sx = 1; raw.dx = max(-128, raw.dx - 1); }
+            if (raw.sy == -1) { raw.sy = 1; raw.dy = max(-128, raw.dy - 1); }
+
+            // ---- RDO skip decision (enc/rdo.rs:140-178)
+            bool int_al = raw.sx == 0 && raw.sy == 0;
+            double satd = (double)max(best_sad, 0LL);
+            double skip_cost = __dadd_rn(satd, __dmul_rn(p.rdo_lambda, p.rdo_skip_bits));
+            double est = __dadd_rn(p.rdo_icpt, __dmul_rn(p.rdo_slope, satd));
+            if (est < 0.0) est = 0.0;
+            double coded_cost = __dadd_rn(__dmul_rn(satd, p.rdo_ret), __dmul_rn(p.rdo_lambda, __dadd_rn(p.rdo_keep_bits, est)));
+            bool rdo_skip = p.rdo_allow && int_al && !(satd > p.rdo_guard) && (skip_cost <= coded_cost);
+
+            // ---- MV mode decision on the coded (reconstructed) neighbours
+            // (enc/encoder.rs:459-733, res/mv_predictor.rs:59-272)
+            MvT cT = rec_cod(recT), cTR = rec_cod(recTR), cTL = rec_cod(recTL);
+            MvT cand[5];
+            int ncand = 0;
+            auto addc = [&](const MvT& m) {
+                bool dup = false;
+                for (int j = 0; j < ncand; j++) dup |= mv_eq(cand[j], m);
+                if (!dup) cand[ncand++] = m;
+            };
+            if (has_l) addc(L_cod);
+            if (has_t) addc(cT);
+            if (has_tr) addc(cTR);
+            if (has_tl) addc(cTL);
+            if (has_tm) addc(Tm_cod);
+            const MvT zero{0, 0, 0, 0};
+            MvT nearest = ncand > 0 ? cand[0] : zero, nearm = ncand > 1 ? cand[1] : zero;
+            MvT temporal = has_tm ? Tm_cod : zero;
+            const int mx = raw.dx * 2 + raw.sx, my = raw.dy * 2 + raw.sy;
+            auto hpeq = [&](const MvT& t) { return mx == t.dx * 2 + t.sx && my == t.dy * 2 + t.sy; };
+            int mode;
+            if (raw.dx == 0 && raw.dy == 0 && raw.sx == 0 && raw.sy == 0) mode = 0;  // Zero
+            else if (hpeq(nearest)) mode = 1;
+            else if (hpeq(nearm)) mode = 2;
+            else if (has_tr && hpeq(cTR)) mode = 3;
+            else if (has_tl && hpeq(cTL)) mode = 4;
+            else if (hpeq(temporal)) mode = 6;
+            else mode = 5;  // New
+            int chosen = 0, rdx = 0, rdy = 0;
+            MvT coded = raw;
+            if (mode == 5) {
+                const MvT bases[5] = {nearest, nearm, cTR, cTL, temporal};
+                const bool hasb[5] = {true, true, has_tr, has_tl, true};
+                const int selbits[5] = {1, 2, 3, 4, 4};
+                unsigned best = 0xffffffffu;
+                int bbx = nearest.dx, bby = nearest.dy;
+                for (int k = 0; k < 5; k++) {
+                    if (!hasb[k]) continue;
+                    int ddx = sat8(raw.dx - bases[k].dx), ddy = sat8(raw.dy - bases[k].dy);
+                    unsigned cst = (unsigned)(selbits[k] + comp_bits(ddx) + comp_bits(ddy));
+                    if (cst < best) { best = cst; chosen = k; bbx = bases[k].dx; bby = bases[k].dy; }
+                }
+                rdx = sat8(raw.dx - bbx);
+                rdy = sat8(raw.dy - bby);
+                coded.dx = sat8(bbx + rdx);
+                coded.dy = sat8(bby + rdy);
+            } else if (mode == 1) coded = nearest;
+            else if (mode == 2) coded = nearm;
+            else if (mode == 3) coded = cTR;
+            else if (mode == 4) coded = cTL;
+            else if (mode == 6) coded = temporal;
+            uint8_t flags = 0;
+            if (mode == 5) flags = (raw.sx == 1 ? 0x01 : 0) | (raw.sy == 1 ? 0x04 : 0);
+            if (rdo_skip) flags |= 0x40;
+
+            // ---- publish
+            if (lane == 0) {
+                MbOut o;
+                o.raw[0] = (int8_t)raw.dx; o.raw[1] = (int8_t)raw.dy; o.raw[2] = (int8_t)raw.sx; o.raw[3] = (int8_t)raw.sy;
+                o.coded[0] = (int8_t)coded.dx; o.coded[1] = (int8_t)coded.dy;
+                o.coded[2] = (int8_t)coded.sx; o.coded[3] = (int8_t)coded.sy;
+                o.rdelta[0] = (int8_t)rdx; o.rdelta[1] = (int8_t)rdy;
+                o.mode = (uint8_t)mode; o.base = (uint8_t)chosen; o.flags = flags; o.rdo_skip = rdo_skip ? 1 : 0;
+                o.pad[0] = o.pad[1] = 0;
+                o.best_sad = (int32_t)best_sad;
+                p.out[idx] = o;
+                unsigned long long rv = tagbits | ((unsigned long long)(uint8_t)raw.dx << 40) |
+                                        ((unsigned long long)(uint8_t)raw.dy << 32) |
+                                        ((unsigned long long)(uint8_t)coded.dx << 24) |
+                                        ((unsigned long long)(uint8_t)coded.dy << 16) |
+                                        ((unsigned long long)(uint8_t)coded.sx << 8) | (unsigned long long)(uint8_t)coded.sy;
+                st_release_u64(p.rec + idx, rv);
+            }
+            L_raw = MvT{raw.dx, raw.dy, 0, 0};
+            L_cod = coded;
+            recTL = recT;
+            recT = recTR;
+        }
+    }
+}
+
+size_t search_smem_bytes(int sr) {
+    size_t ws = 18 + 2 * (size_t)sr;
+    return 256 * sizeof(double) + ws * ws;
+}
+
+int search_max_grid(int sr, int* grid_out) {
+    size_t sm = search_smem_bytes(sr);
+    cudaError_t e = cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return (int)e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search, 32, sm);
+    if (e != cudaSuccess) return (int)e;
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    *grid_out = per_sm * nsm;
+    return 0;
+}
+
+int launch_search(const SearchParams& p, int grid, void* stream) {
+    size_t sm = search_smem_bytes(p.sr);
+    SearchParams q = p;
+    void* args[] = {&q};
+    // Cooperative launch: every CTA of the grid is co-resident, so the row-to-row waits
+    // can always make progress.
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_search, dim3(grid), dim3(32), args, sm,
+                                                (cudaStream_t)stream);
+    return (int)e;
+}
+
+// ---------------------------------------------------------------------------------
+// K6a: motion-compensated prediction (build_predicted, com/fast_motion.rs:103-352) and
+// the per-MB (sum, sum of squares) of predicted luma for AQ (res/residual.rs:134-153).
+// One CTA of 256 threads per MB.  Luma: per-sample clamped rounded bilinear sampling;
+// chroma: copy at the truncated (x0+dx)/2 origin for in-bounds integer MVs, else
+// rounded bilinear at chroma half-pel (2c + (mv_hp >> 1)).
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ int sample_round(const uint8_t* __restrict__ pl, int w, int h, int xh, int yh) {
+    xh = min(max(xh, 0), (w - 1) * 2);
+    yh = min(max(yh, 0), (h - 1) * 2);
+    int x0 = xh >> 1, y0 = yh >> 1;
+    int xo = xh & 1, yo = yh & 1;
+    int x1 = min(x0 + 1, w - 1), y1 = min(y0 + 1, h - 1);
+    int a = pl[(size_t)y0 * w + x0];
+    if (!xo && !yo) return a;
+    int b = pl[(size_t)y0 * w + x1], d = pl[(size_t)y1 * w + x0], e = pl[(size_t)y1 * w + x1];
+    if (xo && !yo) return (a + b + 1) >> 1;
+    if (!xo && yo) return (a + d + 1) >> 1;
+    return (a + b + d + e + 2) >> 2;
+}
+
+__global__ void __launch_bounds__(256) k_predict(const uint8_t* __restrict__ ref, const MbOut* __restrict__ mbo,
+                                                 uint8_t* __restrict__ pred, uint2* __restrict__ varsum, int W, int H) {
+    const int BW = W / 16;
+    const int mb = blockIdx.x;
+    const int bx = mb % BW, by = mb / BW;
+    const int x0 = bx * 16, y0 = by * 16;
+    const int t = threadIdx.x;
+    const int CW = W / 2, CH = H / 2;
+    const uint8_t* RY = ref;
+    const uint8_t* RU = ref + (size_t)W * H;
+    const uint8_t* RV = RU + (size_t)CW * CH;
+    uint8_t* PY = pred;
+    uint8_t* PU = pred + (size_t)W * H;
+    uint8_t* PV = PU + (size_t)CW * CH;
+    const MbOut m = mbo[mb];
+    const int mdx = m.raw[0] * 2 + m.raw[2], mdy = m.raw[1] * 2 + m.raw[3];
+    const bool integer = ((mdx & 1) == 0) && ((mdy & 1) == 0);
+    const int sx0 = x0 + (mdx >> 1), sy0 = y0 + (mdy >> 1);
+    const bool copy = integer && sx0 >= 0 && sy0 >= 0 && sx0 + 15 < W && sy0 + 15 < H;
+    const int yy = t >> 4, xx = t & 15;
+    int v;
+    if (copy) v = RY[(size_t)(sy0 + yy) * W + sx0 + xx];
+    else v = sample_round(RY, W, H, 2 * (x0 + xx) + mdx, 2 * (y0 + yy) + mdy);
+    PY[(size_t)(y0 + yy) * W + x0 + xx] = (uint8_t)v;
+    if (t < 128) {
+        const uint8_t* R = t < 64 ? RU : RV;
+        uint8_t* P = t < 64 ? PU : PV;
+        int i = t & 63, cy = i >> 3, cx = i & 7;
+        int cxg = x0 / 2 + cx, cyg = y0 / 2 + cy;
+        int c;
+        if (copy) c = R[(size_t)(sy0 / 2 + cy) * CW + sx0 / 2 + cx];
+        else c = sample_round(R, CW, CH, 2 * cxg + (mdx >> 1), 2 * cyg + (mdy >> 1));
+        P[(size_t)cyg * CW + cxg] = (uint8_t)c;
+    }
+    unsigned s = (unsigned)v, s2 = (unsigned)(v * v);
+    s = __reduce_add_sync(0xffffffffu, s);
+    s2 = __reduce_add_sync(0xffffffffu, s2);
+    __shared__ unsigned ws[8], ws2[8];
+    if ((t & 31) == 0) { ws[t >> 5] = s; ws2[t >> 5] = s2; }
+    __syncthreads();
+    if (t == 0) {
+        unsigned a = 0, b = 0;
+        for (int i = 0; i < 8; i++) { a += ws[i]; b += ws2[i]; }
+        varsum[mb] = make_uint2(a, b);
+    }
+}
+
+int launch_predict(const uint8_t* ref, const MbOut* mb, uint8_t* pred, uint2* varsum, int W, int H, void* stream) {
+    int nmb = (W / 16) * (H / 16);
+    k_predict<<<nmb, 256, 0, (cudaStream_t)stream>>>(ref, mb, pred, varsum, W, H);
+    return (int)cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------
+// glibc-exact logf / exp2f.  The reference calls f32::ln / f32::exp2, i.e. glibc logf /
+// exp2f, which are not correctly rounded.  Device: correctly rounded via the double
+// function rounded to float, then a sorted fix-up table (input bits -> glibc output
+// bits) built at build time by running glibc over the whole reachable input domain.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ float apply_fix(float x, float y, const uint32_t* fix, int n) {
+    uint32_t key = __float_as_uint(x);
+    int lo = 0, hi = n;  // pairs (in, out) at fix[2i], fix[2i+1]
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        uint32_t k = __ldg(fix + 2 * mid);
+        if (k < key) lo = mid + 1; else hi = mid;
+    }
+    if (lo < n && __ldg(fix + 2 * lo) == key) return __uint_as_float(__ldg(fix + 2 * lo + 1));
+    return y;
+}
+__device__ __forceinline__ float glibc_logf(float x, const uint32_t* fix, int n) {
+    return apply_fix(x, __double2float_rn(log((double)x)), fix, n);
+}
+__device__ __forceinline__ float glibc_exp2f(float x, const uint32_t* fix, int n) {
+    return apply_fix(x, __double2float_rn(exp2((double)x)), fix, n);
+}
+
+__global__ void k_libm_eval(int which, const float* in, float* out, size_t n, const uint32_t* fix, int nfix) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (; i < n; i += stride) out[i] = which == 0 ? glibc_logf(in[i], fix, nfix) : glibc_exp2f(in[i], fix, nfix);
+}
+int launch_libm_eval(int which, const float* in, float* out, size_t n, const uint32_t* fix, int nfix, void* stream) {
+    k_libm_eval<<<1184, 256, 0, (cudaStream_t)stream>>>(which, in, out, n, fix, nfix);
+    return (int)cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------
+// K_aq: compute_aq_quant_steps (res/residual.rs:116-167).  One CTA: variances and ln in
+// parallel, the f32 sum strictly sequential (Iterator::sum folds left to right), then
+// the per-MB steps in parallel.
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_aq(const uint2* __restrict__ varsum, int n, float base,
+                                             const uint32_t* logfix, int nlog, const uint32_t* expfix, int nexp,
+                                             float* lnv, float* qs) {
+    __shared__ float s_avg;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        uint2 vs = varsum[i];
+        unsigned long long N = 256ull * vs.y - (unsigned long long)vs.x * vs.x;
+        float var = __fdiv_rn(__ull2float_rn(N), 65536.0f);
+        var = var < 4.0f ? 4.0f : var;
+        lnv[i] = glibc_logf(var, logfix, nlog);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float s = 0.0f;
+        int i = 0;
+        for (; i + 4 <= n; i += 4) {
+            float a = lnv[i], b = lnv[i + 1], c = lnv[i + 2], d = lnv[i + 3];
+            s = __fadd_rn(s, a); s = __fadd_rn(s, b); s = __fadd_rn(s, c); s = __fadd_rn(s, d);
+        }
+        for (; i < n; i++) s = __fadd_rn(s, lnv[i]);
+        s_avg = __fdiv_rn(s, (float)n);
+    }
+    __syncthreads();
+    float avg = s_avg;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        float off = __fmul_rn(0.8f, __fsub_rn(lnv[i], avg));
+        qs[i] = __fmul_rn(base, glibc_exp2f(__fdiv_rn(off, 6.0f), expfix, nexp));
+    }
+}
+int launch_aq(const uint2* varsum, int n, float base, const uint32_t* logfix, int nlog, const uint32_t* expfix,
+              int nexp, float* lnv_scratch, float* qs, void* stream) {
+    k_aq<<<1, 1024, 0, (cudaStream_t)stream>>>(varsum, n, base, logfix, nlog, expfix, nexp, lnv_scratch, qs);
+    return (int)cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------
+// K6b: residual -> FDCT (i64 accumulate) -> quant -> zero test -> dequant -> IDCT
+// (wrapping i32) -> recon, one CTA (256 threads) per MB.  Inter: AQ step + dead zone
+// (dct/dct16.rs:274-412, dct/dct8.rs:80-135, dct/fast_dct8.rs:69-174,
+// res/residual.rs:520-752).  Intra: pixel-128, JPEG-derived matrices, no dead zone
+// (res/residual.rs:267-388, dct16.rs:420-560, dct8.rs:142-196).
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ int16_t f32_to_i16_sat(float f) {
+    if (f != f) return 0;
+    if (f <= -32768.0f) return -32768;
+    if (f >= 32767.0f) return 32767;
+    return (int16_t)__float2int_rz(f);
+}
+__device__ __forceinline__ int32_t f32_to_i32_sat(float f) {
+    if (f != f) return 0;
+    if (f <= -2147483648.0f) return INT_MIN;
+    if (f >= 2147483647.0f) return INT_MAX;
+    return __float2int_rz(f);
+}
+__device__ __forceinline__ int32_t wmul(int32_t a, int32_t b) { return (int32_t)((uint32_t)a * (uint32_t)b); }
+__device__ __forceinline__ int32_t wadd(int32_t a, int32_t b) { return (int32_t)((uint32_t)a + (uint32_t)b); }
+__device__ __forceinline__ int32_t wsub(int32_t a, int32_t b) { return (int32_t)((uint32_t)a - (uint32_t)b); }
+
+// AAN 8-point kernel with the reference's constants (dct/fast_dct8.rs:254-330).
+__device__ __forceinline__ void aan_1d(const int32_t s[8], int32_t out[8], int32_t bias, int shift) {
+    int32_t p1 = wmul(wadd(s[2], s[6]), 2218);
+    int32_t t2 = wadd(p1, wmul(s[6], -7572));
+    int32_t t3 = wadd(p1, wmul(s[2], 3136));
+    int32_t t0 = (int32_t)((uint32_t)wadd(s[0], s[4]) << 12);
+    int32_t t1 = (int32_t)((uint32_t)wsub(s[0], s[4]) << 12);
+    int32_t x0 = wadd(wadd(t0, t3), bias), x3 = wadd(wsub(t0, t3), bias);
+    int32_t x1 = wadd(wadd(t1, t2), bias), x2 = wadd(wsub(t1, t2), bias);
+    int32_t a0 = s[7], a1 = s[5], a2 = s[3], a3 = s[1];
+    int32_t q3 = wadd(a0, a2), q4 = wadd(a1, a3), q1 = wadd(a0, a3), q2 = wadd(a1, a2);
+    int32_t q5 = wmul(wadd(q3, q4), 4817);
+    a0 = wmul(a0, 1223); a1 = wmul(a1, 8411); a2 = wmul(a2, 12595); a3 = wmul(a3, 6150);
+    q1 = wadd(q5, wmul(q1, -3685));
+    q2 = wadd(q5, wmul(q2, -10496));
+    q3 = wmul(q3, -8035);
+    q4 = wmul(q4, -1598);
+    int32_t u3 = wadd(a3, wadd(q1, q4)), u2 = wadd(a2, wadd(q2, q3));
+    int32_t u1 = wadd(a1, wadd(q2, q4)), u0 = wadd(a0, wadd(q1, q3));
+    out[0] = wadd(x0, u3) >> shift; out[7] = wsub(x0, u3) >> shift;
+    out[1] = wadd(x1, u2) >> shift; out[6] = wsub(x1, u2) >> shift;
+    out[2] = wadd(x2, u1) >> shift; out[5] = wsub(x2, u1) >> shift;
+    out[3] = wadd(x3, u0) >> shift; out[4] = wsub(x3, u0) >> shift;
+}
+
+__global__ void __launch_bounds__(256) k_residual(ResidualParams p) {
+    __shared__ int32_t sT16[256], sT8[64];
+    __shared__ int32_t res[256], rowt[256];
+    __shared__ int32_t resc[128], rowc[128];
+    __shared__ int16_t q[384];
+    __shared__ int32_t aant[2][64];
+    const int t = threadIdx.x;
+    const int mb = blockIdx.x;
+    const int BW = p.BW, W = p.W, H = p.H, CW = W / 2, CH = H / 2;
+    const int bx = mb % BW, by = mb / BW;
+    const int x0 = bx * 16, y0 = by * 16;
+    const uint8_t *cY = p.cur, *cU = p.cur + (size_t)W * H, *cV = cU + (size_t)CW * CH;
+    const uint8_t *pY = p.pred, *pU = p.pred + (size_t)W * H, *pV = pU + (size_t)CW * CH;
+    uint8_t *rY = p.recon, *rU = p.recon + (size_t)W * H, *rV = rU + (size_t)CW * CH;
+    const int yy = t >> 4, xx = t & 15;
+    const size_t yi = (size_t)(y0 + yy) * W + x0 + xx;
+    // chroma mapping for t < 128: plane pl, index i (row ci>>3, col ci&7)
+    const int pl = t >> 6, ci = t & 63, cyy = ci >> 3, cxx = ci & 7;
+    const size_t cidx = (size_t)(y0 / 2 + cyy) * CW + x0 / 2 + cxx;
+
+    bool rdo_skip = !p.intra && p.mb[mb].rdo_skip;
+    if (rdo_skip) {  // never transformed: residual 0, recon = prediction
+        rY[yi] = pY[yi];
+        if (t < 128) {
+            if (pl == 0) rU[cidx] = pU[cidx]; else rV[cidx] = pV[cidx];
+        }
+        for (int i = t; i < 384; i += 256) p.coeffs[(size_t)mb * 384 + i] = 0;
+        if (t == 0) {
+            p.opt_skip[mb] = 1;
+            const int8_t* c = p.mb[mb].coded;
+            p.fmask[mb] = (c[0] | c[1] | c[2] | c[3]) != 0;
+            p.eobs[3 * mb] = p.eobs[3 * mb + 1] = p.eobs[3 * mb + 2] = 0;
+        }
+        return;
+    }
+    sT16[t] = c_T16[t];
+    if (t < 64) sT8[t] = c_T8[t];
+    if (p.intra) {
+        res[t] = (int)cY[yi] - 128;
+        if (t < 128) resc[t] = (int)(pl == 0 ? cU[cidx] : cV[cidx]) - 128;
+    } else {
+        res[t] = (int)cY[yi] - (int)pY[yi];
+        if (t < 128) resc[t] = pl == 0 ? (int)cU[cidx] - (int)pU[cidx] : (int)cV[cidx] - (int)pV[cidx];
+    }
+    __syncthreads();
+    // row pass: rowt[y][j] = sum_i res[y][i] * T[i][j]
+    {
+        long long acc = 0;
+#pragma unroll
+        for (int i = 0; i < 16; i++) acc += (long long)res[yy * 16 + i] * (long long)sT16[i * 16 + xx];
+        long long v = (acc + (1LL << 17)) >> 18;
+        rowt[t] = (int32_t)min(max(v, (long long)INT_MIN), (long long)INT_MAX);
+    }
+    if (t < 128) {
+        long long acc = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) acc += (long long)resc[pl * 64 + cyy * 8 + i] * (long long)sT8[i * 8 + cxx];
+        long long v = (acc + (1LL << 17)) >> 18;
+        rowc[t] = (int32_t)min(max(v, (long long)INT_MIN), (long long)INT_MAX);
+    }
+    __syncthreads();
+    // column pass: coef[v][u] = sum_i rowt[i][u] * T[i][v]   (v = yy, u = xx)
+    int32_t coef;
+    {
+        long long acc = 0;
+#pragma unroll
+        for (int i = 0; i < 16; i++) acc += (long long)rowt[i * 16 + xx] * (long long)sT16[i * 16 + yy];
+        long long v = (acc + (1LL << 17)) >> 18;
+        coef = (int32_t)min(max(v, (long long)INT_MIN), (long long)INT_MAX);
+    }
+    int32_t coefc = 0;
+    if (t < 128) {
+        long long acc = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) acc += (long long)rowc[pl * 64 + i * 8 + cxx] * (long long)sT8[i * 8 + cyy];
+        long long v = (acc + (1LL << 17)) >> 18;
+        coefc = (int32_t)min(max(v, (long long)INT_MIN), (long long)INT_MAX);
+    }
+    // quantisation
+    float qsv = 0.0f;
+    if (p.intra) {
+        float qy = (float)max((int)p.intra_ytab[t], 1);
+        q[t] = f32_to_i16_sat(roundf(__fdiv_rn(__int2float_rn(coef), qy)));
+        if (t < 128) {
+            float qc = (float)max((int)p.intra_ctab[ci], 1);
+            q[256 + t] = f32_to_i16_sat(roundf(__fdiv_rn(__int2float_rn(coefc), qc)));
+        }
+    } else {
+        qsv = p.qs[mb];
+        float r = __fdiv_rn(__int2float_rn(coef), qsv);
+        q[t] = fabsf(r) < p.dead_zone ? (int16_t)0 : f32_to_i16_sat(roundf(r));
+        if (t < 128) {
+            float rc = __fdiv_rn(__int2float_rn(coefc), qsv);
+            q[256 + t] = fabsf(rc) < p.dead_zone ? (int16_t)0 : f32_to_i16_sat(roundf(rc));
+        }
+    }
+    __syncthreads();
+    int nz = (q[t] != 0) || (t < 128 && q[256 + t] != 0);
+    nz = __syncthreads_or(nz);
+    if (!p.intra && !nz) {  // became all-zero after quantisation: optimized skip
+        rY[yi] = pY[yi];
+        if (t < 128) {
+            if (pl == 0) rU[cidx] = pU[cidx]; else rV[cidx] = pV[cidx];
+        }
+        for (int i = t; i < 384; i += 256) p.coeffs[(size_t)mb * 384 + i] = 0;
+        if (t == 0) {
+            p.opt_skip[mb] = 1;
+            const int8_t* c = p.mb[mb].coded;
+            p.fmask[mb] = (c[0] | c[1] | c[2] | c[3]) != 0;
+            p.eobs[3 * mb] = p.eobs[3 * mb + 1] = p.eobs[3 * mb + 2] = 0;
+        }
+        return;
+    }
+    for (int i = t; i < 384; i += 256) p.coeffs[(size_t)mb * 384 + i] = q[i];
+    // last non-zero index per plane block (0 when all zero), for the host entropy coder
+    {
+        int lz = q[t] != 0 ? t : 0;
+        lz = __reduce_max_sync(0xffffffffu, lz);
+        __shared__ int wl[8];
+        if ((t & 31) == 0) wl[t >> 5] = lz;
+        int lc = 0;
+        if (t < 128) lc = q[256 + t] != 0 ? ci : 0;
+        lc = __reduce_max_sync(0xffffffffu, lc);
+        __shared__ int wc[4];
+        if ((t & 31) == 0 && t < 128) wc[t >> 5] = lc;
+        __syncthreads();
+        if (t == 0) {
+            int a = 0;
+            for (int i = 0; i < 8; i++) a = max(a, wl[i]);
+            p.eobs[3 * mb] = (uint8_t)a;
+            p.eobs[3 * mb + 1] = (uint8_t)max(wc[0], wc[1]);
+            p.eobs[3 * mb + 2] = (uint8_t)max(wc[2], wc[3]);
+            p.opt_skip[mb] = 0;
+            p.fmask[mb] = 1;
+        }
+    }
+    // dequantisation + 16x16 inverse (row pass over u, then column pass over v)
+    if (p.intra) res[t] = (int32_t)q[t] * max((int)p.intra_ytab[t], 1);
+    else {
+        int32_t qfp = f32_to_i32_sat(roundf(__fmul_rn(qsv, 16384.0f)));
+        res[t] = wadd(wmul((int32_t)q[t], qfp), 8192) >> 14;
+    }
+    __syncthreads();
+    {  // rows[v][x] = (sum_i deq[v][i] * T[x][i] + 2^17) >> 18, wrapping
+        uint32_t acc = 0;
+#pragma unroll
+        for (int i = 0; i < 16; i++) acc += (uint32_t)res[yy * 16 + i] * (uint32_t)sT16[xx * 16 + i];
+        rowt[t] = (int32_t)(acc + (1u << 17)) >> 18;
+    }
+    __syncthreads();
+    {  // out[y][x] = (sum_v rows[v][x] * T[y][v] + 2^17) >> 18
+        uint32_t acc = 0;
+#pragma unroll
+        for (int i = 0; i < 16; i++) acc += (uint32_t)rowt[i * 16 + xx] * (uint32_t)sT16[yy * 16 + i];
+        int32_t r = (int32_t)(acc + (1u << 17)) >> 18;
+        r = min(max(r, -32768), 32767);
+        int base = p.intra ? 128 : (int)pY[yi];
+        rY[yi] = (uint8_t)min(max(base + r, 0), 255);
+    }
+    // chroma 8x8 AAN inverse: pass 1 over u for each (plane, v); pass 2 over v for each (plane, x)
+    if (t < 16) {
+        int cp = t >> 3, v = t & 7;
+        int32_t s[8], o[8];
+        int32_t qa = 0;
+        if (!p.intra) {
+            float qr = roundf(qsv);
+            qr = qr < 1.0f ? 1.0f : qr;
+            qa = qr >= 65535.0f ? 65535 : (int32_t)qr;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            int32_t qq = p.intra ? max((int)p.intra_ctab[v * 8 + u], 1) : qa;
+            s[u] = (int32_t)q[256 + cp * 64 + v * 8 + u] * qq;
+        }
+        aan_1d(s, o, 512, 10);
+#pragma unroll
+        for (int x = 0; x < 8; x++) aant[cp][x * 8 + v] = o[x];
+    }
+    __syncthreads();
+    if (t < 16) {
+        int cp = t >> 3, x = t & 7;
+        int32_t s[8], o[8];
+#pragma unroll
+        for (int v = 0; v < 8; v++) s[v] = aant[cp][x * 8 + v];
+        aan_1d(s, o, 65536, 17);
+        const uint8_t* P = cp == 0 ? pU : pV;
+        uint8_t* R = cp == 0 ? rU : rV;
+#pragma unroll
+        for (int y = 0; y < 8; y++) {
+            int r = min(max(o[y], -32768), 32767);
+            size_t i = (size_t)(y0 / 2 + y) * CW + x0 / 2 + x;
+            int base = p.intra ? 128 : (int)P[i];
+            R[i] = (uint8_t)min(max(base + r, 0), 255);
+        }
+    }
+}
+
+int launch_residual(const ResidualParams& p, int nmb, void* stream) {
+    k_residual<<<nmb, 256, 0, (cudaStream_t)stream>>>(p);
+    return (int)cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------
+// K7: in-loop deblock (com/deblock.rs:60-202).  Vertical edges, then horizontal edges,
+// each pass in place: lines of one pass touch disjoint pixels (an edge line reads
+// x-4..x+3 and writes x-3..x+2, edges are >= 8 px apart), so a thread per edge line
+// reproduces the reference's sequential loops exactly.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ int c128(int x) { return min(max(x, -128), 127); }
+__device__ __forceinline__ void filter_line(int* px, int E, int I, int Hv) {
+    int p3 = px[0], p2 = px[1], p1 = px[2], p0 = px[3], q0 = px[4], q1 = px[5], q2 = px[6], q3 = px[7];
+    bool mask = 2 * abs(p0 - q0) + abs(q1 - p1) / 2 <= E && abs(p3 - p2) <= I && abs(p2 - p1) <= I &&
+                abs(p1 - p0) <= I && abs(q1 - q0) <= I && abs(q2 - q1) <= I && abs(q3 - q2) <= I;
+    if (!mask) return;
+    int ps2 = p2 - 128, ps1 = p1 - 128, ps0 = p0 - 128, qs0 = q0 - 128, qs1 = q1 - 128, qs2 = q2 - 128;
+    bool hev = abs(p1 - p0) > Hv || abs(q1 - q0) > Hv;
+    int w = c128(c128(ps1 - qs1) + 3 * (qs0 - ps0));
+    if (hev) {
+        int f1 = c128(w + 4) >> 3, f2 = c128(w + 3) >> 3;
+        px[4] = min(max(c128(qs0 - f1) + 128, 0), 255);
+        px[3] = min(max(c128(ps0 + f2) + 128, 0), 255);
+    } else {
+        int a = c128((27 * w + 63) >> 7);
+        int nq0 = c128(qs0 - a), np0 = c128(ps0 + a);
+        a = c128((18 * w + 63) >> 7);
+        int nq1 = c128(qs1 - a), np1 = c128(ps1 + a);
+        a = c128((9 * w + 63) >> 7);
+        int nq2 = c128(qs2 - a), np2 = c128(ps2 + a);
+        px[1] = min(max(np2 + 128, 0), 255);
+        px[2] = min(max(np1 + 128, 0), 255);
+        px[3] = min(max(np0 + 128, 0), 255);
+        px[4] = min(max(nq0 + 128, 0), 255);
+        px[5] = min(max(nq1 + 128, 0), 255);
+        px[6] = min(max(nq2 + 128, 0), 255);
+    }
+}
+// Vertical edges of one plane: thread per (row y, edge e >= 1).
+__global__ void k_deblock_v(uint8_t* pl, int w, int h, int grid, int BW, int E, int I, int Hv, const uint8_t* mask) {
+    int y = blockIdx.y * blockDim.y + threadIdx.y;
+    int e = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (y >= h || e >= w / grid) return;
+    int by = y / grid;
+    if (mask && !(mask[by * BW + e - 1] | mask[by * BW + e])) return;
+    uint8_t* s = pl + (size_t)y * w + e * grid - 4;
+    int px[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) px[k] = s[k];
+    filter_line(px, E, I, Hv);
+#pragma unroll
+    for (int k = 1; k < 7; k++) s[k] = (uint8_t)px[k];
+}
+// Horizontal edges of one plane: thread per (column x, edge e >= 1).
+__global__ void k_deblock_h(uint8_t* pl, int w, int h, int grid, int BW, int E, int I, int Hv, const uint8_t* mask) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int e = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (x >= w || e >= h / grid) return;
+    int bxm = x / grid;
+    if (mask && !(mask[(e - 1) * BW + bxm] | mask[e * BW + bxm])) return;
+    uint8_t* s = pl + (size_t)(e * grid - 4) * w + x;
+    int px[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) px[k] = s[(size_t)k * w];
+    filter_line(px, E, I, Hv);
+#pragma unroll
+    for (int k = 1; k < 7; k++) s[(size_t)k * w] = (uint8_t)px[k];
+}
+
+int launch_deblock(uint8_t* yuv, int W, int H, int E, int I, int Hv, const uint8_t* mask, void* stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    const int BW = W / 16;
+    uint8_t* planes[3] = {yuv, yuv + (size_t)W * H, yuv + (size_t)W * H + (size_t)(W / 2) * (H / 2)};
+    for (int k = 0; k < 3; k++) {
+        int w = k == 0 ? W : W / 2, h = k == 0 ? H : H / 2, g = k == 0 ? 16 : 8;
+        int ne = w / g - 1;
+        if (ne > 0) {
+            dim3 b(32, 8), gr((ne + 31) / 32, (h + 7) / 8);
+            k_deblock_v<<<gr, b, 0, st>>>(planes[k], w, h, g, BW, E, I, Hv, mask);
+        }
+    }
+    for (int k = 0; k < 3; k++) {
+        int w = k == 0 ? W : W / 2, h = k == 0 ? H : H / 2, g = k == 0 ? 16 : 8;
+        int ne = h / g - 1;
+        if (ne > 0) {
+            dim3 b(128, 1), gr((w + 127) / 128, ne);
+            k_deblock_h<<<gr, b, 0, st>>>(planes[k], w, h, g, BW, E, I, Hv, mask);
+        }
+    }
+    return (int)cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------
+// K8: per-MB side info (4 bytes) and compaction of coded MBs' coefficients for the host
+// entropy coder.  side = mode | base<<3 | subx<<6 | suby<<7, rdx, rdy, optskip|fmask<<1.
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_scan(const uint8_t* opt_skip, int nmb, int intra, int32_t* index,
+                                               uint32_t* count) {
+    __shared__ int wsum[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int base = 0; base < nmb; base += 1024) {
+        int i = base + threadIdx.x;
+        int f = (i < nmb && (intra || !opt_skip[i])) ? 1 : 0;
+        int x = f;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            int s = wsum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += y;
+            }
+            wsum[lane] = s;
+        }
+        __syncthreads();
+        int excl = carry + (wid > 0 ? wsum[wid - 1] : 0) + x - f;
+        if (i < nmb) index[i] = f ? excl : -1;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += wsum[31];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *count = (uint32_t)carry;
+}
+__global__ void k_pack(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coeffs, const uint8_t* eobs,
+                       const int32_t* index, int nmb, int intra, uint32_t* side, int16_t* packed, uint8_t* peobs) {
+    int m = blockIdx.x;
+    int k = index[m];
+    if (threadIdx.x == 0) {
+        uint32_t s = 0;
+        if (!intra) {
+            const MbOut o = mb[m];
+            s = (uint32_t)o.mode | ((uint32_t)o.base << 3) | ((uint32_t)(o.raw[2] & 1) << 6) |
+                ((uint32_t)(o.raw[3] & 1) << 7) | ((uint32_t)(uint8_t)o.rdelta[0] << 8) |
+                ((uint32_t)(uint8_t)o.rdelta[1] << 16) | ((uint32_t)(opt_skip[m] & 1) << 24);
+        }
+        side[m] = s;
+        if (k >= 0) {
+            peobs[3 * k] = eobs[3 * m];
+            peobs[3 * k + 1] = eobs[3 * m + 1];
+            peobs[3 * k + 2] = eobs[3 * m + 2];
+        }
+    }
+    if (k < 0) return;
+    const uint4* src = (const uint4*)(coeffs + (size_t)m * 384);
+    uint4* dst = (uint4*)(packed + (size_t)k * 384);
+    for (int i = threadIdx.x; i < 48; i += blockDim.x) dst[i] = src[i];
+}
+
+int launch_compact(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coeffs, const uint8_t* eobs, int nmb,
+                   int intra, uint32_t* side, int32_t* index, int16_t* packed, uint8_t* packed_eobs, uint32_t* count,
+                   void* stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    k_scan<<<1, 1024, 0, st>>>(opt_skip, nmb, intra, index, count);
+    k_pack<<<nmb, 64, 0, st>>>(opt_skip, mb, coeffs, eobs, index, nmb, intra, side, packed, packed_eobs);
+    return (int)cudaGetLastError();
+}
+
+}  // namespace riv
+
+// Table upload helper (host side of the constant tables).
+extern "C" int riv_upload_dct_tables(const int32_t* t16, const int32_t* t8) {
+    cudaError_t e = cudaMemcpyToSymbol(riv::c_T16, t16, 256 * sizeof(int32_t));
+    if (e != cudaSuccess) return (int)e;
+    return (int)cudaMemcpyToSymbol(riv::c_T8, t8, 64 * sizeof(int32_t));
+}

@@ -1,0 +1,523 @@
+"""Python mirror of reitero_encode's public API over the C ABI (include/riv_gpu.h).
+
+Same names, argument meaning and error behaviour as the reference crate
+(reitero_video/reitero_encode/src/{config,encoder,writer,error}.rs):
+
+    cfg = EncoderConfig.new(1920, 1080, 50).with_intra_quality(85).with_inter_quality(80)
+    enc = Encoder.new(cfg, VecWriter())
+    enc.encode_frame(Frame(rgb_bytes, 1920, 1080, timestamp_ms))
+    enc.finish()
+    data = enc.writer.into_inner()
+
+The encoder runs on the GPU; there is no CPU fallback -- constructing an Encoder without
+the CUDA library or without a device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from typing import Optional
+
+import numpy as np
+
+from ._native import load_cuda
+
+# ---------------------------------------------------------------------------------------
+# Errors (enc/error.rs:4-20)
+# ---------------------------------------------------------------------------------------
+
+
+class EncodeError(Exception):
+    status = 3
+
+
+class IoError(EncodeError):
+    status = 1
+
+
+class InvalidConfig(EncodeError):
+    status = 2
+
+
+class EncodingFailed(EncodeError):
+    status = 3
+
+
+class UnsupportedCodec(EncodeError):
+    status = 4
+
+
+class FrameError(EncodeError):
+    status = 5
+
+
+class CudaError(EncodeError):
+    status = 6
+
+
+class DeviceTimeout(EncodeError):
+    status = 7
+
+
+_ERRORS = {1: IoError, 2: InvalidConfig, 3: EncodingFailed, 4: UnsupportedCodec, 5: FrameError, 6: CudaError,
+           7: DeviceTimeout}
+
+# ---------------------------------------------------------------------------------------
+# C structures
+# ---------------------------------------------------------------------------------------
+
+
+class RivConfig(C.Structure):
+    _fields_ = [
+        ("display_width", C.c_uint32), ("display_height", C.c_uint32),
+        ("storage_width", C.c_uint32), ("storage_height", C.c_uint32),
+        ("fps", C.c_uint32), ("keyframe_mode", C.c_uint32), ("keyframe_interval", C.c_uint64),
+        ("intra_quality", C.c_uint8), ("inter_quality", C.c_uint8), ("search_range", C.c_uint8),
+        ("mv_deflate_level", C.c_uint8), ("skip_threshold", C.c_uint8), ("_pad", C.c_uint8 * 3),
+        ("me_zero_mv_threshold", C.c_int64), ("me_predictor_threshold", C.c_int64),
+        ("rdo_lambda_mult", C.c_double), ("inter_dead_zone", C.c_float),
+        ("device", C.c_int32), ("pipeline_depth", C.c_uint32), ("entropy_threads", C.c_uint32),
+        ("_pad2", C.c_uint32 * 2),
+    ]
+
+
+WRITE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_uint8), C.c_size_t)
+POS_FN = C.CFUNCTYPE(C.c_uint64, C.c_void_p)
+SEEK_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint64)
+FLUSH_FN = C.CFUNCTYPE(C.c_int, C.c_void_p)
+
+
+class RivWriterVtable(C.Structure):
+    _fields_ = [("write", WRITE_FN), ("position", POS_FN), ("seek", SEEK_FN), ("flush", FLUSH_FN),
+                ("user", C.c_void_p)]
+
+
+class RivFrameStats(C.Structure):
+    _fields_ = [
+        ("frame_index", C.c_uint64), ("timestamp_ms", C.c_uint64), ("frame_type", C.c_uint32),
+        ("total_bytes", C.c_uint32), ("mv_bytes", C.c_uint32), ("residual_bytes", C.c_uint32),
+        ("storage_width", C.c_uint32), ("storage_height", C.c_uint32), ("blocks_total", C.c_uint32),
+        ("blocks_skipped", C.c_uint32), ("rdo_blocks_selected_skip", C.c_uint32),
+        ("mv_mode_counts", C.c_uint32 * 7), ("mv_new_base_counts", C.c_uint32 * 5), ("mv_new_blocks", C.c_uint32),
+        ("mv_bias_dx", C.c_int32), ("mv_bias_dy", C.c_int32), ("rdo_lambda", C.c_double),
+    ]
+
+
+# Every symbol include/riv_gpu.h declares (checked by the CPU test suite).
+EXPORTED_SYMBOLS = (
+    "riv_config_default", "riv_encoder_new", "riv_encode_frame", "riv_encode_frame_device", "riv_encode_frame_yuv",
+    "riv_finish", "riv_encoder_free", "riv_last_error", "riv_frame_count", "riv_last_recon", "riv_last_kernel_times",
+    "riv_memwriter_new", "riv_memwriter_vtable", "riv_memwriter_size", "riv_memwriter_data", "riv_memwriter_free",
+    "riv_stage_rgb_to_yuv", "riv_stage_deblock", "riv_stage_libm", "riv_libm_fixup_counts", "riv_dct_tables",
+    "riv_debug_frame_state",
+)
+
+
+def lib() -> C.CDLL:
+    L = load_cuda()
+    if getattr(L, "_riv_typed", False):
+        return L
+    P, U8P = C.c_void_p, C.POINTER(C.c_uint8)
+    L.riv_config_default.argtypes = [C.POINTER(RivConfig), C.c_uint32, C.c_uint32, C.c_uint32]
+    L.riv_encoder_new.argtypes = [C.POINTER(RivConfig), C.POINTER(RivWriterVtable), C.POINTER(P)]
+    L.riv_encode_frame.argtypes = [P, U8P, C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(RivFrameStats)]
+    L.riv_encode_frame_device.argtypes = [P, P, C.c_uint64, C.POINTER(RivFrameStats)]
+    L.riv_encode_frame_yuv.argtypes = [P, U8P, U8P, U8P, C.c_uint64, C.POINTER(RivFrameStats)]
+    L.riv_finish.argtypes = [P]
+    L.riv_encoder_free.argtypes = [P]
+    L.riv_last_error.restype = C.c_char_p
+    L.riv_last_error.argtypes = [P]
+    L.riv_frame_count.restype = C.c_uint64
+    L.riv_frame_count.argtypes = [P]
+    L.riv_last_recon.argtypes = [P, U8P, U8P, U8P]
+    L.riv_last_kernel_times.argtypes = [P, C.POINTER(C.c_float)]
+    L.riv_memwriter_new.restype = P
+    L.riv_memwriter_vtable.argtypes = [P, C.POINTER(RivWriterVtable)]
+    L.riv_memwriter_size.restype = C.c_size_t
+    L.riv_memwriter_size.argtypes = [P]
+    L.riv_memwriter_data.restype = P
+    L.riv_memwriter_data.argtypes = [P]
+    L.riv_memwriter_free.argtypes = [P]
+    L.riv_stage_rgb_to_yuv.argtypes = [U8P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, U8P]
+    L.riv_stage_deblock.argtypes = [U8P, C.c_uint32, C.c_uint32, C.c_int, C.c_int, U8P]
+    L.riv_stage_libm.argtypes = [C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_size_t]
+    L.riv_libm_fixup_counts.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+    L.riv_dct_tables.argtypes = [C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    L.riv_debug_frame_state.argtypes = [P, C.c_int, P, C.c_size_t]
+    L._riv_typed = True
+    return L
+
+
+def _u8(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_uint8))
+
+
+# ---------------------------------------------------------------------------------------
+# Config (enc/config.rs)
+# ---------------------------------------------------------------------------------------
+
+
+@dataclasses.dataclass(frozen=True)
+class KeyframeInterval:
+    """KeyframeInterval::{AllIntra, Automatic, Fixed(n)} (enc/config.rs:5-19)."""
+
+    mode: int
+    interval: int = 0
+
+    @staticmethod
+    def all_intra() -> "KeyframeInterval":
+        return KeyframeInterval(0)
+
+    @staticmethod
+    def automatic() -> "KeyframeInterval":
+        return KeyframeInterval(1)
+
+    @staticmethod
+    def fixed(n: int) -> "KeyframeInterval":
+        return KeyframeInterval(2, n)
+
+
+@dataclasses.dataclass
+class EncoderConfig:
+    display_width: int
+    display_height: int
+    storage_width: int
+    storage_height: int
+    fps: int
+    keyframe_interval: KeyframeInterval = dataclasses.field(default_factory=lambda: KeyframeInterval.fixed(30))
+    intra_quality: int = 90
+    inter_quality: int = 35
+    search_range: int = 12
+    mv_deflate_level: int = 6
+    skip_threshold: int = 3
+    me_zero_mv_threshold: int = 0
+    me_predictor_threshold: int = 0
+    rdo_lambda_mult: float = 0.49
+    inter_dead_zone: float = 0.75
+    # device / runtime tuning (never changes the bitstream)
+    device: int = 0
+    pipeline_depth: int = 0
+    entropy_threads: int = 0
+
+    @staticmethod
+    def new(width: int, height: int, fps: int) -> "EncoderConfig":
+        """EncoderConfig::new: storage dims rounded up to multiples of 16 (enc/config.rs:56-77)."""
+        return EncoderConfig(width, height, (width + 15) // 16 * 16, (height + 15) // 16 * 16, fps)
+
+    def _with(self, **kw) -> "EncoderConfig":
+        return dataclasses.replace(self, **kw)
+
+    def with_rdo_lambda_mult(self, v: float): return self._with(rdo_lambda_mult=v)
+    def with_inter_dead_zone(self, v: float): return self._with(inter_dead_zone=v)
+    def with_intra_quality(self, v: int): return self._with(intra_quality=v)
+    def with_inter_quality(self, v: int): return self._with(inter_quality=v)
+    def with_keyframe_interval(self, v: KeyframeInterval): return self._with(keyframe_interval=v)
+    def with_search_range(self, v: int): return self._with(search_range=v)
+    def with_mv_deflate_level(self, v: int): return self._with(mv_deflate_level=v)
+    def with_skip_threshold(self, v: int): return self._with(skip_threshold=v)
+    def with_me_zero_mv_threshold(self, v: int): return self._with(me_zero_mv_threshold=v)
+    def with_me_predictor_threshold(self, v: int): return self._with(me_predictor_threshold=v)
+    def with_pipeline_depth(self, v: int): return self._with(pipeline_depth=v)
+    def with_device(self, v: int): return self._with(device=v)
+
+    def validate(self) -> None:
+        """EncoderConfig::validate (enc/config.rs:129-164)."""
+        if self.display_width == 0 or self.display_height == 0:
+            raise InvalidConfig("Width and height must be greater than 0")
+        if self.storage_width < self.display_width or self.storage_height < self.display_height:
+            raise InvalidConfig("Storage dimensions must be >= display dimensions")
+        if self.fps == 0:
+            raise InvalidConfig("FPS must be greater than 0")
+        if self.search_range > 127:
+            raise InvalidConfig("search_range must be <= 127 for current MV encoding")
+        if self.mv_deflate_level > 10:
+            raise InvalidConfig("mv_deflate_level must be in 0..=10")
+        if self.keyframe_interval.mode == 2 and self.keyframe_interval.interval == 0:
+            raise InvalidConfig("Keyframe interval must be greater than 0")
+
+    def to_c(self) -> RivConfig:
+        c = RivConfig()
+        for f in ("display_width", "display_height", "storage_width", "storage_height", "fps", "intra_quality",
+                  "inter_quality", "search_range", "mv_deflate_level", "skip_threshold", "me_zero_mv_threshold",
+                  "me_predictor_threshold", "rdo_lambda_mult", "inter_dead_zone", "device", "pipeline_depth",
+                  "entropy_threads"):
+            setattr(c, f, getattr(self, f))
+        c.keyframe_mode = self.keyframe_interval.mode
+        c.keyframe_interval = self.keyframe_interval.interval
+        return c
+
+
+@dataclasses.dataclass
+class Frame:
+    """Raw RGB24 input frame (enc/encoder.rs:18-34): width*height*3 bytes, row-major."""
+
+    data: object
+    width: int
+    height: int
+    timestamp: int
+
+
+# ---------------------------------------------------------------------------------------
+# Writers (enc/writer.rs)
+# ---------------------------------------------------------------------------------------
+
+
+class VideoWriter:
+    """Trait VideoWriter: write / position / seek / flush (enc/writer.rs:5-18)."""
+
+    def write(self, data: bytes) -> None: raise NotImplementedError
+    def position(self) -> int: raise NotImplementedError
+    def seek(self, pos: int) -> None: raise NotImplementedError
+    def flush(self) -> None: raise NotImplementedError
+
+
+class VecWriter(VideoWriter):
+    """In-memory writer (enc/writer.rs:20-69), backed by the C library's buffer."""
+
+    def __init__(self):
+        self._h = lib().riv_memwriter_new()
+
+    def vtable(self) -> RivWriterVtable:
+        vt = RivWriterVtable()
+        lib().riv_memwriter_vtable(self._h, C.byref(vt))
+        return vt
+
+    def into_inner(self) -> bytes:
+        n = lib().riv_memwriter_size(self._h)
+        return C.string_at(lib().riv_memwriter_data(self._h), n)
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().riv_memwriter_free(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+class _PyWriterBridge:
+    """Adapts a Python VideoWriter to the C vtable."""
+
+    def __init__(self, w: VideoWriter):
+        self.w = w
+        self.error: Optional[BaseException] = None
+
+        def _write(_u, ptr, n):
+            try:
+                self.w.write(C.string_at(ptr, n))
+                return 0
+            except BaseException as e:  # noqa: BLE001 - reported as Io
+                self.error = e
+                return 1
+
+        def _pos(_u):
+            return int(self.w.position())
+
+        def _seek(_u, p):
+            try:
+                self.w.seek(int(p))
+                return 0
+            except BaseException as e:  # noqa: BLE001
+                self.error = e
+                return 1
+
+        def _flush(_u):
+            try:
+                self.w.flush()
+                return 0
+            except BaseException as e:  # noqa: BLE001
+                self.error = e
+                return 1
+
+        self._cbs = (WRITE_FN(_write), POS_FN(_pos), SEEK_FN(_seek), FLUSH_FN(_flush))
+
+    def vtable(self) -> RivWriterVtable:
+        vt = RivWriterVtable()
+        vt.write, vt.position, vt.seek, vt.flush = self._cbs
+        vt.user = None
+        return vt
+
+
+# ---------------------------------------------------------------------------------------
+# Encoder (enc/encoder.rs)
+# ---------------------------------------------------------------------------------------
+
+
+@dataclasses.dataclass
+class EncodeFrameStats:
+    frame_index: int
+    timestamp_ms: int
+    frame_type: int
+    total_bytes: int
+    mv_bytes: int
+    residual_bytes: int
+    storage_width: int
+    storage_height: int
+    blocks_total: int
+    blocks_skipped: int
+    mv_mode_counts: tuple
+    mv_new_base_counts: tuple
+    mv_new_blocks: int
+    mv_bias_dx: int
+    mv_bias_dy: int
+    rdo_lambda: float
+
+    @staticmethod
+    def from_c(s: RivFrameStats) -> "EncodeFrameStats":
+        return EncodeFrameStats(s.frame_index, s.timestamp_ms, s.frame_type, s.total_bytes, s.mv_bytes,
+                                s.residual_bytes, s.storage_width, s.storage_height, s.blocks_total, s.blocks_skipped,
+                                tuple(s.mv_mode_counts), tuple(s.mv_new_base_counts), s.mv_new_blocks, s.mv_bias_dx,
+                                s.mv_bias_dy, s.rdo_lambda)
+
+
+class Encoder:
+    """Stateful GPU encoder: ``Encoder.new(config, writer)``, ``encode_frame``, ``finish``."""
+
+    def __init__(self, config: EncoderConfig, writer: VideoWriter, _h, _bridge):
+        self.config = config
+        self.writer = writer
+        self._h = _h
+        self._bridge = _bridge
+
+    @staticmethod
+    def new(config: EncoderConfig, writer: VideoWriter) -> "Encoder":
+        config.validate()
+        L = lib()
+        bridge = None
+        if isinstance(writer, VecWriter):
+            vt = writer.vtable()
+        else:
+            bridge = _PyWriterBridge(writer)
+            vt = bridge.vtable()
+        h = C.c_void_p()
+        cfg = config.to_c()
+        st = L.riv_encoder_new(C.byref(cfg), C.byref(vt), C.byref(h))
+        if st != 0:
+            raise _ERRORS.get(st, EncodeError)(f"riv_encoder_new failed (status {st})")
+        return Encoder(config, writer, h, bridge)
+
+    def _check(self, st: int) -> None:
+        if st != 0:
+            msg = lib().riv_last_error(self._h).decode(errors="replace")
+            if self._bridge is not None and self._bridge.error is not None:
+                msg += f" ({self._bridge.error!r})"
+            raise _ERRORS.get(st, EncodeError)(msg)
+
+    def encode_frame(self, frame: Frame) -> None:
+        self._encode(frame, None)
+
+    def encode_frame_with_stats(self, frame: Frame) -> EncodeFrameStats:
+        s = RivFrameStats()
+        self._encode(frame, s)
+        return EncodeFrameStats.from_c(s)
+
+    def _encode(self, frame: Frame, stats: Optional[RivFrameStats]) -> None:
+        data = frame.data
+        if isinstance(data, (bytes, bytearray, memoryview)):
+            arr = np.frombuffer(data, np.uint8)
+        else:
+            arr = np.ascontiguousarray(data, dtype=np.uint8).reshape(-1)
+        if frame.width != self.config.display_width or frame.height != self.config.display_height:
+            raise FrameError(f"Frame dimensions ({frame.width}, {frame.height}) do not match config "
+                             f"({self.config.display_width}, {self.config.display_height})")
+        if arr.size != frame.width * frame.height * 3:
+            raise FrameError(f"Display RGB24 size mismatch: expected {frame.width * frame.height * 3}, got {arr.size}")
+        st = lib().riv_encode_frame(self._h, _u8(arr), frame.width, frame.height, frame.timestamp,
+                                    C.byref(stats) if stats is not None else None)
+        self._check(st)
+
+    def encode_frame_device(self, ptr: int, timestamp: int) -> None:
+        """Encode a display-size RGB24 frame already resident in device memory."""
+        self._check(lib().riv_encode_frame_device(self._h, C.c_void_p(ptr), timestamp, None))
+
+    def encode_frame_yuv(self, y: np.ndarray, u: np.ndarray, v: np.ndarray, timestamp: int) -> None:
+        y, u, v = (np.ascontiguousarray(p, dtype=np.uint8) for p in (y, u, v))
+        self._check(lib().riv_encode_frame_yuv(self._h, _u8(y), _u8(u), _u8(v), timestamp, None))
+
+    def finish(self) -> None:
+        self._check(lib().riv_finish(self._h))
+
+    def frame_count(self) -> int:
+        return int(lib().riv_frame_count(self._h))
+
+    def last_recon(self):
+        sw, sh = self.config.storage_width, self.config.storage_height
+        y = np.empty((sh, sw), np.uint8)
+        u = np.empty((sh // 2, sw // 2), np.uint8)
+        v = np.empty((sh // 2, sw // 2), np.uint8)
+        self._check(lib().riv_last_recon(self._h, _u8(y), _u8(u), _u8(v)))
+        return y, u, v
+
+    def last_kernel_times_us(self) -> np.ndarray:
+        t = np.zeros(8, np.float32)
+        self._check(lib().riv_last_kernel_times(self._h, t.ctypes.data_as(C.POINTER(C.c_float))))
+        return t
+
+    def debug_state(self, what: int) -> np.ndarray:
+        """Device state of the most recent frame (see riv_debug_frame_state)."""
+        sw, sh = self.config.storage_width, self.config.storage_height
+        nmb = (sw // 16) * (sh // 16)
+        spec = {0: (nmb * 20, np.uint8), 1: (nmb, np.float32), 2: (sw * sh * 3 // 2, np.uint8),
+                3: (sw * sh * 3 // 2, np.uint8), 4: (nmb * 384, np.int16), 5: (nmb, np.uint8)}[what]
+        out = np.empty(spec[0], spec[1])
+        self._check(lib().riv_debug_frame_state(self._h, what, C.c_void_p(out.ctypes.data), out.nbytes))
+        return out
+
+    def close(self) -> None:
+        if self._h:
+            lib().riv_encoder_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------------------
+# Stage entry points (one kernel each) used by the parity tests
+# ---------------------------------------------------------------------------------------
+
+
+def stage_rgb_to_yuv(rgb: np.ndarray, dw: int, dh: int, sw: int, sh: int) -> np.ndarray:
+    rgb = np.ascontiguousarray(rgb, dtype=np.uint8)
+    out = np.empty(sw * sh * 3 // 2, np.uint8)
+    st = lib().riv_stage_rgb_to_yuv(_u8(rgb), dw, dh, sw, sh, _u8(out))
+    if st:
+        raise _ERRORS.get(st, EncodeError)("riv_stage_rgb_to_yuv failed")
+    return out
+
+
+def stage_deblock(yuv: np.ndarray, w: int, h: int, level: int, intra: bool, mask=None) -> np.ndarray:
+    out = np.ascontiguousarray(yuv, dtype=np.uint8).copy()
+    m = None if mask is None else _u8(np.ascontiguousarray(mask, dtype=np.uint8))
+    st = lib().riv_stage_deblock(_u8(out), w, h, level, int(intra), m)
+    if st:
+        raise _ERRORS.get(st, EncodeError)("riv_stage_deblock failed")
+    return out
+
+
+def stage_libm(which: int, x: np.ndarray) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty_like(x)
+    st = lib().riv_stage_libm(which, x.ctypes.data_as(C.POINTER(C.c_float)),
+                              out.ctypes.data_as(C.POINTER(C.c_float)), x.size)
+    if st:
+        raise _ERRORS.get(st, EncodeError)("riv_stage_libm failed")
+    return out
+
+
+def libm_fixup_counts():
+    a, b = C.c_uint32(), C.c_uint32()
+    st = lib().riv_libm_fixup_counts(C.byref(a), C.byref(b))
+    if st:
+        raise EncodeError("libm fix-up table missing")
+    return a.value, b.value
+
+
+def dct_tables():
+    t16 = np.zeros(256, np.int32)
+    t8 = np.zeros(64, np.int32)
+    lib().riv_dct_tables(t16.ctypes.data_as(C.POINTER(C.c_int32)), t8.ctypes.data_as(C.POINTER(C.c_int32)))
+    return t16.reshape(16, 16), t8.reshape(8, 8)
