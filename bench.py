@@ -1,0 +1,333 @@
+#!/usr/bin/env python3
+"""Benchmark: 1080p P-frame encode throughput of the B200 riv2 encoder.
+
+Workload: a seeded synthetic 1920x1080 RGB24 clip (16 rectangles, sides 64-384 px,
+velocities +-16 px/frame at 0.5 px steps, pan +-4, noise sigma 2), quality 85/80, one
+key frame at frame 0, encoder defaults otherwise (search range 12, skip threshold 3,
+lambda multiplier 0.49, dead zone 0.75).  A step is one P-frame.
+
+* ``value``: frames/s of the whole encode (GPU hot path + host rANS coding + record
+  writes, pipelined) with the RGB frames already resident in HBM.
+* ``e2e``: the same through ``riv_encode_frame`` with pinned host RGB buffers; the
+  host->device copy of each frame and the device->host copy of its side info and
+  coefficients are inside the timed region.
+* ``roofline``: the dominant kernel (the search/mode wavefront), achieved bytes/s over
+  its algorithmic bytes against the measured HBM copy bandwidth.
+* ``cpu_baseline``: the CPU oracle (single-threaded restatement of the reference encoder,
+  library-default raster-serial search) on a bounded sample of the same clip.
+
+``--impl reference`` times that CPU implementation alone (the reference itself is Rust
+and cannot be built in this image).  Multi-GPU: one process per GPU, each encoding its
+own clip (replicas, no collective), value = total frames / max time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W_DISP, H_DISP, FPS = 1920, 1080, 50
+MBS_PER_FRAME = (1920 // 16) * (1088 // 16)
+METRIC = json.load(open(os.path.join(ROOT, "BASELINE.json")))["metric"]
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--quality", default="85/80")
+    ap.add_argument("--pipeline-depth", type=int, default=8)
+    ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--cpu-sample-frames", type=int, default=12)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------
+# distributed plumbing (replicas)
+# ---------------------------------------------------------------------------------------
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def init_dist(ws, backend):
+    if ws <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def max_over_ranks(x: float, dist, device=None) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, device=None):
+    if dist is not None:
+        import torch
+        t = torch.zeros(1, device=device)
+        dist.all_reduce(t)
+
+
+# ---------------------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu_index: int):
+        self.samples = []
+        self.idx = gpu_index
+        self.proc = None
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                sm.append(float(s[0]))
+                mx = float(s[1])
+                for k, n in enumerate(names):
+                    if s[4 + k].lower().startswith("active"):
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------------------
+
+def make_frames(n: int, seed: int, clip: int) -> np.ndarray:
+    from riv2_b200.synth import SynthClip
+    return SynthClip("1080p", seed=seed, clip=clip).frames(n)
+
+
+def config(iq: int, pq: int, depth: int, device: int):
+    from riv2_b200 import encoder as E
+    return (E.EncoderConfig.new(W_DISP, H_DISP, FPS).with_intra_quality(iq).with_inter_quality(pq)
+            .with_keyframe_interval(E.KeyframeInterval.fixed(1 << 40)).with_pipeline_depth(depth).with_device(device))
+
+
+def run_ours(args, frames_host, dev_index, dist):
+    import torch
+
+    from riv2_b200 import encoder as E
+    iq, pq = (int(x) for x in args.quality.split("/"))
+    K, Wm = args.steps, args.warmup
+    n = K + Wm + 1
+    torch.cuda.set_device(dev_index)
+    dev = torch.device("cuda", dev_index)
+    frames_dev = torch.from_numpy(frames_host).to(dev)  # (n, H, W, 3), resident in HBM
+    pinned = torch.from_numpy(frames_host).pin_memory()
+    stride = W_DISP * H_DISP * 3
+
+    def session(device_inputs: bool):
+        w = E.VecWriter()
+        enc = E.Encoder.new(config(iq, pq, args.pipeline_depth, dev_index), w)
+        base = frames_dev.data_ptr() if device_inputs else pinned.data_ptr()
+
+        def put(t, drain=False):
+            if device_inputs:
+                enc.encode_frame_device(base + t * stride, t * 20, drain=drain)
+            else:
+                arr = np.ctypeslib.as_array((np.ctypeslib.ctypes.c_uint8 * stride).from_address(base + t * stride))
+                f = E.Frame(arr, W_DISP, H_DISP, t * 20)
+                enc.encode_frame_with_stats(f) if drain else enc.encode_frame(f)
+
+        for t in range(Wm):
+            put(t)
+        put(Wm, drain=True)  # the timed region starts with an empty pipeline
+        c0 = enc.counters()
+        torch.cuda.synchronize()
+        barrier(dist, dev)
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        clocks = ClockSampler(dev_index)
+        clocks.start()
+        ev0.record()
+        for t in range(Wm + 1, n):
+            put(t)
+        enc.finish()  # drains the pipeline: every timed frame's record is written
+        ev1.record()
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        barrier(dist, dev)
+        ms = ev0.elapsed_time(ev1)
+        c1 = enc.counters()
+        data = w.into_inner()
+        enc.close()
+        return ms, c0, c1, clk, data
+
+    ms_v, c0v, c1v, clk_v, data_v = session(True)
+    ms_e, c0e, c1e, clk_e, data_e = session(False)
+    del frames_dev
+    return {"ms_value": ms_v, "ms_e2e": ms_e, "c0": c0v, "c1": c1v, "c0e": c0e, "c1e": c1e, "clocks": clk_v,
+            "clocks_e2e": clk_e, "stream_bytes": len(data_v), "streams_equal": data_v == data_e}
+
+
+def cpu_baseline(frames_host, nframes, iq, pq):
+    """The oracle (single-threaded restatement of the reference encoder) on a sample."""
+    from oracle import oracle as O
+    cfg = O.default_config(W_DISP, H_DISP, FPS)
+    cfg.intra_quality, cfg.inter_quality = iq, pq
+    cfg.keyframe_mode, cfg.keyframe_interval = 2, 1 << 40
+    enc = O.OracleEncoder(cfg)
+    enc.encode_rgb(frames_host[0], 0)
+    t0 = time.perf_counter()
+    for t in range(1, nframes + 1):
+        enc.encode_rgb(frames_host[t], t * 20)
+    dt = time.perf_counter() - t0
+    return nframes / dt, dt
+
+
+def roofline_entry(stage_us_per_frame: float):
+    """Search/mode wavefront: algorithmic bytes per frame = read reference Y + current Y
+    (2 x 1920x1088) + write the per-MB record and output (8 + 20 bytes per MB)."""
+    peaks = {}
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        peaks = json.load(open(p))
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    alg = 2 * 1920 * 1088 + MBS_PER_FRAME * (8 + 20)
+    achieved = alg / (stage_us_per_frame * 1e-6) / 1e9
+    return {"bound": "hbm", "kernel": "k_search (motion search + RDO + mode wavefront)", "achieved": achieved,
+            "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+            "algorithmic_bytes_per_launch": alg, "launch_us": stage_us_per_frame,
+            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_env()
+    iq, pq = (int(x) for x in args.quality.split("/"))
+    K, Wm = args.steps, args.warmup
+    if args.impl == "reference":
+        # rank 0 alone times the CPU implementation; other ranks exit without work.
+        if rank != 0:
+            return
+        n = args.cpu_sample_frames
+        frames = make_frames(n + 1, args.seed, 0)
+        steps_vals = []
+        total = 0.0
+        for _ in range(max(1, min(K, 3))):
+            fps, dt = cpu_baseline(frames, n, iq, pq)
+            steps_vals.append(fps)
+            total += dt
+        fps = statistics.median(steps_vals)
+        line = {"impl": "reference", "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": ws, "steps": K,
+                "warmup": Wm, "ms_per_step": 1000.0 / fps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u8/i16/i32 (f32 AQ, f64 RDO)", "data": "synthetic",
+                "config": {"workload": "1080p synthetic clip, q %d/%d, P-frames" % (iq, pq), "global_batch": 1,
+                           "parallelism": "single host thread (raster-serial search, library-default features)"},
+                "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": 1, "kind": "port",
+                                 "sample": f"{n} P-frames of the 1080p clip after its key frame, x{len(steps_vals)}"},
+                "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    dist = init_dist(ws, "nccl")
+    import torch
+    dev_index = local if torch.cuda.device_count() > 1 else 0
+    frames = make_frames(K + Wm + 1, args.seed, rank)
+    r = run_ours(args, frames, dev_index, dist)
+    ms_v = max_over_ranks(r["ms_value"], dist, torch.device("cuda", dev_index))
+    ms_e = max_over_ranks(r["ms_e2e"], dist, torch.device("cuda", dev_index))
+    c0, c1 = r["c0"], r["c1"]
+    pf = c1["pframes"] - c0["pframes"]
+    stage = [(b - a) / max(pf, 1) for a, b in zip(c0["stage_us_sum"], c1["stage_us_sum"])]
+    launches = c1["launches"] - c0["launches"]
+    h2d = (r["c1e"]["h2d_bytes"] - r["c0e"]["h2d_bytes"]) / K
+    d2h = (r["c1e"]["d2h_bytes"] - r["c0e"]["d2h_bytes"]) / K
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    value = ws * K / (ms_v / 1000.0)
+    e2e = ws * K / (ms_e / 1000.0)
+    cpu = None
+    if ws == 1 and not args.no_cpu_baseline:
+        fps, dt = cpu_baseline(frames, args.cpu_sample_frames, iq, pq)
+        cpu = {"value": fps, "unit": "frames/s", "cores": 1, "kind": "port",
+               "sample": f"{args.cpu_sample_frames} P-frames of the same 1080p clip after its key frame ({dt:.1f} s)"}
+    names = ["rgb_to_yuv", "search", "predict", "aq", "residual", "deblock", "compact", "total"]
+    line = {
+        "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": ws, "steps": K, "warmup": Wm,
+        "ms_per_step": ms_v / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8/i16/i32 (f32 AQ, f64 RDO)", "data": "synthetic",
+        "config": {"workload": "1080p synthetic clip (1920x1080, 16 moving textured rects, pan, noise), plain GPU "
+                               "P-frame encode, q %d/%d, search range 12, one key frame" % (iq, pq),
+                   "global_batch": ws, "seq_len": K, "parallelism": f"replicas x{ws} (one clip per GPU)",
+                   "form": "plain (learned-proposal form not built)",
+                   "pipeline_depth": args.pipeline_depth,
+                   "l2": "inputs larger than L2: %d distinct RGB frames (%.0f MB) resident in HBM"
+                         % (K + Wm + 1, (K + Wm + 1) * W_DISP * H_DISP * 3 / 1e6),
+                   "macroblocks_per_s": value * MBS_PER_FRAME},
+        "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "gpu_stage_us_per_pframe": dict(zip(names, [round(x, 2) for x in stage])),
+        "gpu_pipeline_fps": 1e6 / stage[7] if stage[7] > 0 else None,
+        "roofline": roofline_entry(stage[1]),
+        "cpu_baseline": cpu,
+        "clocks": r["clocks"],
+        "stream_bytes": r["stream_bytes"], "streams_equal_value_vs_e2e": r["streams_equal"],
+    }
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -110,6 +110,11 @@ riv_status riv_last_recon(riv_encoder* enc, uint8_t* y, uint8_t* u, uint8_t* v);
  * [0] rgb->yuv [1] search [2] predict [3] aq [4] residual [5] deblock [6] compact [7] total */
 riv_status riv_last_kernel_times(riv_encoder* enc, float* us8);
 
+/* Cumulative counters since riv_encoder_new: us8 = per-stage GPU time summed over all
+ * P-frames (same stage order as riv_last_kernel_times), io2 = {host->device bytes,
+ * device->host bytes}, n2 = {P-frames, kernel launches}. */
+riv_status riv_counters(riv_encoder* enc, double* us8, uint64_t* io2, uint64_t* n2);
+
 /* In-memory writer (VecWriter, enc/writer.rs:20-69). */
 typedef struct riv_memwriter riv_memwriter;
 riv_memwriter* riv_memwriter_new(void);

@@ -308,6 +308,8 @@ struct riv_encoder {
     float last_times[8] = {0};
     bool have_times = false;
     riv_frame_stats last_stats{};
+    double sum_times[8] = {0};
+    uint64_t h2d_bytes = 0, d2h_bytes = 0, pframes = 0, launches = 0;
 };
 
 namespace {
@@ -432,6 +434,12 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
     const int W = e->W, H = e->H, N = e->NMB;
     cudaStream_t S = e->S;
     CK(cudaEventRecord(s.ev_k[EV_START], S));
+    // kernels per frame: rgb->yuv, (search, predict, aq), residual, deblock (2 per plane), scan + pack
+    const int nplanes_db = 3 * 2;
+    e->launches += (src == 2 ? 0 : 1) + (j.type == 2 ? 3 : 0) + 1 +
+                   ((j.type == 2 ? e->inter_level : e->intra_level) > 0 ? nplanes_db : 0) + 2;
+    if (src == 0) e->h2d_bytes += (uint64_t)c.display_width * c.display_height * 3;
+    if (src == 2) e->h2d_bytes += e->yuv_bytes;
     if (src == 0) {
         CK(cudaMemcpyAsync(s.rgb.p, a, (size_t)c.display_width * c.display_height * 3, cudaMemcpyHostToDevice, e->C));
         CK(cudaEventRecord(s.ev_h2d, e->C));
@@ -551,6 +559,7 @@ static riv_status retire(riv_encoder* e, Job& j) {
                     (st & ST_WAIT_TIMEOUT) ? "device-side wavefront wait timed out" : "device search iteration cap hit");
     }
     j.count = *s.h_count.as<uint32_t>();
+    e->d2h_bytes += (uint64_t)e->NMB * 4 + 8 + (uint64_t)j.count * (768 + 3);
     if (j.count) {
         CK(cudaMemcpyAsync(s.h_packed.p, s.packed.p, (size_t)j.count * 768, cudaMemcpyDeviceToHost, e->C));
         CK(cudaMemcpyAsync(s.h_peobs.p, s.peobs.p, (size_t)j.count * 3, cudaMemcpyDeviceToHost, e->C));
@@ -561,6 +570,10 @@ static riv_status retire(riv_encoder* e, Job& j) {
     for (int k = 0; k < 7; k++) cudaEventElapsedTime(&t[k], s.ev_k[k], s.ev_k[k + 1]);
     cudaEventElapsedTime(&t[7], s.ev_k[EV_START], s.ev_k[EV_COMPACT]);
     for (int k = 0; k < 8; k++) j.times[k] = t[k] * 1000.0f;
+    if (j.type == 2) {
+        for (int k = 0; k < 8; k++) e->sum_times[k] += j.times[k];
+        e->pframes++;
+    }
     const int N = e->NMB;
     riv_frame_stats& S = j.stats;
     memset(&S, 0, sizeof(S));
@@ -909,6 +922,14 @@ riv_status riv_debug_frame_state(riv_encoder* e, int what, void* out, size_t siz
     } catch (const CudaError& ce) {
         return fail(e, RIV_ERR_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
     }
+    return RIV_OK;
+}
+
+riv_status riv_counters(riv_encoder* e, double* us8, uint64_t* io2, uint64_t* n2) {
+    if (!e) return RIV_ERR_FRAME;
+    if (us8) memcpy(us8, e->sum_times, sizeof(e->sum_times));
+    if (io2) { io2[0] = e->h2d_bytes; io2[1] = e->d2h_bytes; }
+    if (n2) { n2[0] = e->pframes; n2[1] = e->launches; }
     return RIV_OK;
 }
 

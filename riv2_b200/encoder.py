@@ -109,7 +109,7 @@ EXPORTED_SYMBOLS = (
     "riv_finish", "riv_encoder_free", "riv_last_error", "riv_frame_count", "riv_last_recon", "riv_last_kernel_times",
     "riv_memwriter_new", "riv_memwriter_vtable", "riv_memwriter_size", "riv_memwriter_data", "riv_memwriter_free",
     "riv_stage_rgb_to_yuv", "riv_stage_deblock", "riv_stage_libm", "riv_libm_fixup_counts", "riv_dct_tables",
-    "riv_debug_frame_state",
+    "riv_debug_frame_state", "riv_counters",
 )
 
 
@@ -144,6 +144,7 @@ def lib() -> C.CDLL:
     L.riv_libm_fixup_counts.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     L.riv_dct_tables.argtypes = [C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     L.riv_debug_frame_state.argtypes = [P, C.c_int, P, C.c_size_t]
+    L.riv_counters.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L._riv_typed = True
     return L
 
@@ -426,9 +427,13 @@ class Encoder:
                                     C.byref(stats) if stats is not None else None)
         self._check(st)
 
-    def encode_frame_device(self, ptr: int, timestamp: int) -> None:
-        """Encode a display-size RGB24 frame already resident in device memory."""
-        self._check(lib().riv_encode_frame_device(self._h, C.c_void_p(ptr), timestamp, None))
+    def encode_frame_device(self, ptr: int, timestamp: int, drain: bool = False) -> Optional[EncodeFrameStats]:
+        """Encode a display-size RGB24 frame already resident in device memory.  With
+        ``drain`` the call returns only after this frame's record was written."""
+        s = RivFrameStats() if drain else None
+        self._check(lib().riv_encode_frame_device(self._h, C.c_void_p(ptr), timestamp,
+                                                  C.byref(s) if s is not None else None))
+        return EncodeFrameStats.from_c(s) if s is not None else None
 
     def encode_frame_yuv(self, y: np.ndarray, u: np.ndarray, v: np.ndarray, timestamp: int) -> None:
         y, u, v = (np.ascontiguousarray(p, dtype=np.uint8) for p in (y, u, v))
@@ -452,6 +457,14 @@ class Encoder:
         t = np.zeros(8, np.float32)
         self._check(lib().riv_last_kernel_times(self._h, t.ctypes.data_as(C.POINTER(C.c_float))))
         return t
+
+    def counters(self) -> dict:
+        """Cumulative GPU stage times (us, P-frames), I/O bytes and kernel launches."""
+        us = (C.c_double * 8)()
+        io = (C.c_uint64 * 2)()
+        n = (C.c_uint64 * 2)()
+        self._check(lib().riv_counters(self._h, us, io, n))
+        return {"stage_us_sum": list(us), "h2d_bytes": io[0], "d2h_bytes": io[1], "pframes": n[0], "launches": n[1]}
 
     def debug_state(self, what: int) -> np.ndarray:
         """Device state of the most recent frame (see riv_debug_frame_state)."""
