@@ -359,7 +359,7 @@ static void setup_device(riv_encoder* e) {
     e->coded[1].alloc((size_t)N * 4);
     e->rec.alloc((size_t)N * sizeof(MbRec));
     e->varsum.alloc((size_t)N * sizeof(uint2));
-    e->lnv.alloc((size_t)N * sizeof(float));
+    e->lnv.alloc((size_t)(N + 4) * sizeof(float));
     e->qs.alloc((size_t)N * sizeof(float));
     e->coeffs.alloc((size_t)N * 384 * sizeof(int16_t));
     e->opt_skip.alloc(N);
@@ -389,7 +389,7 @@ static void setup_device(riv_encoder* e) {
     CK(cudaMemcpy(e->ytab.p, yt, sizeof(yt), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(e->ctab.p, ct, sizeof(ct), cudaMemcpyHostToDevice));
     int g = 0;
-    CK(search_max_grid(c.search_range, &g));
+    CK(search_max_grid(c.search_range, (int)c.storage_width, &g));
     if (g <= 0) throw std::runtime_error("search kernel cannot be made resident");
     e->search_grid = std::min(g, e->BH);
     // frame constants
@@ -434,9 +434,9 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
     const int W = e->W, H = e->H, N = e->NMB;
     cudaStream_t S = e->S;
     CK(cudaEventRecord(s.ev_k[EV_START], S));
-    // kernels per frame: rgb->yuv, (search, predict, aq), residual, deblock (2 per plane), scan + pack
+    // kernels per frame: rgb->yuv, (search, predict, 3 x aq), residual, deblock (2 per plane), scan + pack
     const int nplanes_db = 3 * 2;
-    e->launches += (src == 2 ? 0 : 1) + (j.type == 2 ? 3 : 0) + 1 +
+    e->launches += (src == 2 ? 0 : 1) + (j.type == 2 ? 5 : 0) + 1 +
                    ((j.type == 2 ? e->inter_level : e->intra_level) > 0 ? nplanes_db : 0) + 2;
     if (src == 0) e->h2d_bytes += (uint64_t)c.display_width * c.display_height * 3;
     if (src == 2) e->h2d_bytes += e->yuv_bytes;

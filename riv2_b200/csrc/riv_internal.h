@@ -70,7 +70,7 @@ enum StatusBits : unsigned {
 // Launchers (riv_kernels.cu).  All are asynchronous on `stream`.
 int launch_rgb_to_yuv(const uint8_t* rgb, int dw, int dh, uint8_t* yuv, int W, int H, void* stream);
 int launch_search(const SearchParams& p, int grid, void* stream);
-int search_max_grid(int sr, int* grid_out);
+int search_max_grid(int sr, int W, int* grid_out);
 size_t search_smem_bytes(int sr);
 int launch_predict(const uint8_t* ref, const MbOut* mb, uint8_t* pred, uint2* varsum, int W, int H, void* stream);
 int launch_aq(const uint2* varsum, int n, float base, const uint32_t* logfix, int nlog, const uint32_t* expfix,

@@ -111,21 +111,48 @@ __device__ __forceinline__ long long mv_cost(int dx, int dy, const CostCtx& c, c
     return best;
 }
 
+// Unaligned 32-bit read from shared memory: two aligned words and a funnel shift.  The
+// reference window/band allocation carries 16 bytes of slack so the second word is
+// always inside it.
+__device__ __forceinline__ uint32_t lds_u32(const uint8_t* p) {
+    uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+    uint32_t lo, hi;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(lo) : "r"(a & ~3u));
+    asm volatile("ld.shared.u32 %0, [%1+4];" : "=r"(hi) : "r"(a & ~3u));
+    return __funnelshift_r(lo, hi, (a & 3u) * 8u);
+}
+__device__ __forceinline__ uint32_t lds_aligned(uint32_t saddr) {
+    uint32_t v;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(saddr));
+    return v;
+}
+// floor((a+b)/2) per byte
+__device__ __forceinline__ uint32_t favg(uint32_t a, uint32_t b) { return (a & b) + (((a ^ b) >> 1) & 0x7F7F7F7Fu); }
+// floor((a+b+c+d)/4) per byte, via 16-bit lanes
+__device__ __forceinline__ uint32_t favg4(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+    const uint32_t M = 0x00FF00FFu;
+    uint32_t lo = (a & M) + (b & M) + (c & M) + (d & M);
+    uint32_t hi = ((a >> 8) & M) + ((b >> 8) & M) + ((c >> 8) & M) + ((d >> 8) & M);
+    return ((lo >> 2) & M) | (((hi >> 2) & M) << 8);
+}
+
+// Reference samples of one MB: byte at frame (fx, fy) = org[(fy - wy0) * stride + fx - x0].
+// Replicated borders: positions outside the frame hold the nearest frame sample.
+struct RefView {
+    const uint8_t* org;
+    int stride, wy0;
+};
+
 // Integer SAD partial over this lane's 8 pixels, reproducing the per-4x4 sub-block
 // clamped reference origin of the reference's edge path (enc/motion/satd_scalar.rs:26-97);
 // for interior candidates the clamps are no-ops and this equals the plain 16x16 SAD.
-__device__ __forceinline__ unsigned sad_int_part(const uint8_t* win, int WS, int wx0, int wy0, int x0, int y0,
-                                                 int W, int H, int dx, int dy, int yy, int g0, const uint8_t* cur8) {
+__device__ __forceinline__ unsigned sad_int_part(const RefView& v, int x0, int y0, int W, int H, int dx, int dy,
+                                                 int yy, int xoff, uint32_t c0, uint32_t c1) {
     int ry = min(max(y0 + (yy & ~3) + dy, 0), H - 4) + (yy & 3);
-    const uint8_t* row = win + (ry - wy0) * WS;
-    int rx0 = min(max(x0 + 4 * g0 + dx, 0), W - 4) - wx0;
-    int rx1 = min(max(x0 + 4 * g0 + 4 + dx, 0), W - 4) - wx0;
-    unsigned s = 0;
-#pragma unroll
-    for (int k = 0; k < 4; k++) s += (unsigned)abs((int)cur8[k] - (int)row[rx0 + k]);
-#pragma unroll
-    for (int k = 0; k < 4; k++) s += (unsigned)abs((int)cur8[4 + k] - (int)row[rx1 + k]);
-    return s;
+    const uint8_t* row = v.org + (ry - v.wy0) * v.stride;
+    int rx0 = min(max(x0 + xoff + dx, 0), W - 4) - x0;
+    int rx1 = min(max(x0 + xoff + 4 + dx, 0), W - 4) - x0;
+    return __vsadu4(c0, lds_u32(row + rx0)) + __vsadu4(c1, lds_u32(row + rx1));
 }
 
 struct MvT {
@@ -149,47 +176,113 @@ __device__ __forceinline__ int median3(int a, int b, int c) {  // enc/motion/sca
     return a > c ? a : (b > c ? c : b);
 }
 
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+    uint32_t d = (uint32_t)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Band layout (BAND mode): the reference rows y0-sr-1 .. y0+16+sr of the whole MB row,
+// columns -MARGIN .. W+MARGIN-1, MARGIN = round_up(sr+1, 16), filled 16-column chunk by
+// chunk with cp.async one MB ahead of use.
+__device__ __forceinline__ void fill_chunk(uint8_t* band, int BWB, int WS, int c, int MARGIN, int wy0,
+                                          const uint8_t* __restrict__ ref, int W, int H, int lane) {
+    const int fx0 = 16 * c - MARGIN;
+    for (int i = lane; i < WS; i += 32) {
+        int gy = min(max(wy0 + i, 0), H - 1);
+        uint8_t* dst = band + (size_t)i * BWB + 16 * c;
+        if (fx0 >= 0 && fx0 < W) {
+            cp_async16(dst, ref + (size_t)gy * W + fx0);
+        } else {
+            uint32_t v = ref[(size_t)gy * W + (fx0 < 0 ? 0 : W - 1)] * 0x01010101u;
+            *(uint4*)dst = make_uint4(v, v, v, v);
+        }
+    }
+}
+
+template <bool BAND>
 __global__ void __launch_bounds__(32) k_search(SearchParams p) {
     extern __shared__ __align__(16) uint8_t smem[];
-    double* bits = (double*)smem;  // 256 doubles
-    uint8_t* win = smem + 256 * sizeof(double);
+    double* bits = (double*)smem;                 // 256 doubles
+    uint8_t* curbuf = smem + 256 * sizeof(double);  // 2 x 256 bytes
+    uint8_t* refmem = curbuf + 512;               // band or window (+16 bytes slack)
     const int lane = threadIdx.x;
     const int sr = p.sr;
     const int WS = 18 + 2 * sr;
+    const int MARGIN = (sr + 1 + 15) & ~15;
+    const int BWB = p.W + 2 * MARGIN;
     for (int i = lane; i < 256; i += 32) bits[i] = p.mvbits[i];
-    const int yy = lane >> 1;       // this lane's row inside the MB
+    const int yy = lane >> 1;         // this lane's row inside the MB
     const int xoff = (lane & 1) * 8;  // and its 8-pixel half
-    const int g0 = (lane & 1) * 2;    // first 4x4 sub-block column of the half
     const unsigned long long tagbits = (unsigned long long)(p.tag & 0xffffu) << 48;
     bool failed = false;
 
     for (int r = blockIdx.x; r < p.BH; r += gridDim.x) {
         const int y0 = r * 16;
         const int wy0 = y0 - sr - 1;
-        // Left neighbour (this row, previous MB): raw (dx,dy) and coded tuple.
+        __syncwarp();
+        // ---- prologue: reference columns of MB 0 and its current block
+        int c_done = -1;
+        auto c_hi = [&](int bx) { return (16 * bx + 16 + sr + MARGIN) >> 4; };
+        if (BAND) {
+            for (int c = 0; c <= c_hi(0); c++) fill_chunk(refmem, BWB, WS, c, MARGIN, wy0, p.ref_y, p.W, p.H, lane);
+            c_done = c_hi(0);
+        }
+        if (lane < 16) cp_async16(curbuf + lane * 16, p.cur_y + (size_t)(y0 + lane) * p.W);
+        cp_async_commit();
+
         MvT L_raw{0, 0, 0, 0}, L_cod{0, 0, 0, 0};
-        // Records of the row above, sliding: TL, T, TR.
         unsigned long long recT = 0, recTL = 0;
         for (int bx = 0; bx < p.BW; bx++) {
             const int x0 = bx * 16;
-            const int wx0 = x0 - sr - 1;
             const int idx = r * p.BW + bx;
-            // ---- stage the reference window (replicated borders) and the current block
-            __syncwarp();
-            for (int i = lane; i < WS * WS; i += 32) {
-                int wr = i / WS, wc = i - wr * WS;
-                int gy = min(max(wy0 + wr, 0), p.H - 1), gx = min(max(wx0 + wc, 0), p.W - 1);
-                win[i] = p.ref_y[(size_t)gy * p.W + gx];
-            }
-            uint8_t cur8[8];
-            {
-                const uint2 c = *(const uint2*)(p.cur_y + (size_t)(y0 + yy) * p.W + x0 + xoff);
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    cur8[k] = (uint8_t)(c.x >> (8 * k));
-                    cur8[4 + k] = (uint8_t)(c.y >> (8 * k));
+            // ---- prefetch MB bx+1 (columns and current block), then wait for MB bx's data
+            if (bx + 1 < p.BW) {
+                if (BAND) {
+                    int hi = c_hi(bx + 1);
+                    for (int c = c_done + 1; c <= hi; c++)
+                        fill_chunk(refmem, BWB, WS, c, MARGIN, wy0, p.ref_y, p.W, p.H, lane);
+                    c_done = hi;
                 }
+                if (lane < 16)
+                    cp_async16(curbuf + ((bx + 1) & 1) * 256 + lane * 16, p.cur_y + (size_t)(y0 + lane) * p.W + x0 + 16);
             }
+            cp_async_commit();
+            cp_async_wait1();
+            RefView view;
+            if (BAND) {
+                view.org = refmem + x0 + MARGIN;
+                view.stride = BWB;
+            } else {
+                // per-MB window (large search ranges / very wide frames): rows wy0.., cols x0-sr-1..
+                const int wx0 = x0 - sr - 1;
+                __syncwarp();
+                for (int i0 = 0; i0 < WS * WS; i0 += 32 * 8) {
+                    uint8_t v[8];
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        int i = i0 + u * 32 + lane;
+                        int wr = i / WS, wc = i - wr * WS;
+                        int gy = min(max(wy0 + wr, 0), p.H - 1), gx = min(max(wx0 + wc, 0), p.W - 1);
+                        v[u] = i < WS * WS ? p.ref_y[(size_t)gy * p.W + gx] : 0;
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        int i = i0 + u * 32 + lane;
+                        if (i < WS * WS) refmem[i] = v[u];
+                    }
+                }
+                view.org = refmem + (sr + 1);
+                view.stride = WS;
+            }
+            view.wy0 = wy0;
+            __syncwarp();
+            const uint8_t* cb = curbuf + (bx & 1) * 256;
+            const uint32_t c0 = *(const uint32_t*)(cb + yy * 16 + xoff);
+            const uint32_t c1 = *(const uint32_t*)(cb + yy * 16 + xoff + 4);
+
             // ---- wait for the row above (top-right, or top at the last column)
             unsigned long long recTR = 0;
             bool has_tr = false;
@@ -211,9 +304,9 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                 recT = __shfl_sync(0xffffffffu, recT, 0);
                 if (bx + 1 < p.BW) { recTR = v; has_tr = true; }
             }
-            __syncwarp();
             if (failed) {
                 if (lane == 0) atomicOr(p.status, ST_WAIT_TIMEOUT);
+                cp_async_wait0();
                 return;
             }
             const bool has_t = r > 0, has_l = bx > 0, has_tl = r > 0 && bx > 0;
@@ -231,8 +324,8 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
             int Tmx = 0, Tmy = 0;
             MvT Tm_cod{0, 0, 0, 0};
             if (has_tm) {
-                const int8_t* pc = p.prev_coded + 4 * idx;
-                Tm_cod = MvT{pc[0], pc[1], pc[2], pc[3]};
+                const char4 pc = *(const char4*)(p.prev_coded + 4 * idx);
+                Tm_cod = MvT{pc.x, pc.y, pc.z, pc.w};
                 Tmx = Tm_cod.dx; Tmy = Tm_cod.dy;
             }
             // ---- seeds, nearest/near/median (enc/motion/scalar.rs:56-156)
@@ -242,15 +335,14 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
             if (has_tr) { px[np] = TRx; py[np] = TRy; np++; }
             if (has_tl) { px[np] = TLx; py[np] = TLy; np++; }
             if (has_tm) { px[np] = Tmx; py[np] = Tmy; np++; }
-            int ux[5], uy[5], nu = 0;
-            for (int i = 0; i < np; i++) {
-                bool dup = false;
-                for (int j = 0; j < nu; j++) dup |= (ux[j] == px[i] && uy[j] == py[i]);
-                if (!dup) { ux[nu] = px[i]; uy[nu] = py[i]; nu++; }
+            int ux0 = 0, uy0 = 0, ux1 = 0, uy1 = 0, nu = 0;
+            for (int i = 0; i < np && nu < 2; i++) {
+                if (nu == 1 && px[i] == ux0 && py[i] == uy0) continue;
+                if (nu == 0) { ux0 = px[i]; uy0 = py[i]; } else { ux1 = px[i]; uy1 = py[i]; }
+                nu++;
             }
             CostCtx cc;
-            cc.nx = nu > 0 ? ux[0] : 0; cc.ny = nu > 0 ? uy[0] : 0;
-            cc.rx = nu > 1 ? ux[1] : 0; cc.ry = nu > 1 ? uy[1] : 0;
+            cc.nx = ux0; cc.ny = uy0; cc.rx = ux1; cc.ry = uy1;
             {
                 int lx = has_l ? L_raw.dx : 0, ly = has_l ? L_raw.dy : 0;
                 int tx = has_t ? Tx : 0, ty = has_t ? Ty : 0;
@@ -261,33 +353,44 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                 cc.my = median3(ly, ty, qy);
             }
             // seed candidate list: (0,0) first, then predictors in order, deduped, within sr
-            int cxs[6], cys[6], nc = 0;
-            cxs[nc] = 0; cys[nc] = 0; nc++;
+            int cxs[6], cys[6], nc = 1;
+            cxs[0] = 0; cys[0] = 0;
             for (int i = 0; i < np; i++) {
                 if (abs(px[i]) > sr || abs(py[i]) > sr) continue;
                 bool dup = false;
                 for (int j = 0; j < nc; j++) dup |= (cxs[j] == px[i] && cys[j] == py[i]);
                 if (!dup) { cxs[nc] = px[i]; cys[nc] = py[i]; nc++; }
             }
-            __syncwarp();  // window visible to all lanes
-            // ---- zero SAD and the seed round (all seeds + zero in one parallel round)
+            // ---- zero SAD and the seed round; lane k evaluates the MV cost of candidate k
+            long long my_cost = 0;
+            {
+                int k = min(lane, 5);
+                int kx = 0, ky = 0;
+#pragma unroll
+                for (int i = 0; i < 6; i++)
+                    if (i == k) { kx = cxs[i]; ky = cys[i]; }
+                if (lane < nc) my_cost = mv_cost(kx, ky, cc, p, bits);
+            }
             unsigned part[6];
 #pragma unroll
             for (int i = 0; i < 6; i++)
-                part[i] = i < nc ? sad_int_part(win, WS, wx0, wy0, x0, y0, p.W, p.H, cxs[i], cys[i], yy, g0, cur8) : 0u;
+                part[i] = i < nc ? sad_int_part(view, x0, y0, p.W, p.H, cxs[i], cys[i], yy, xoff, c0, c1) : 0u;
             long long sads[6];
 #pragma unroll
             for (int i = 0; i < 6; i++) sads[i] = (long long)warp_sum(part[i]);
             long long zero_sad = sads[0];
             int sdx = 0, sdy = 0;
-            long long scost = zero_sad + mv_cost(0, 0, cc, p, bits);
+            long long scost = zero_sad + __shfl_sync(0xffffffffu, my_cost, 0);
             bool skip_int = p.zthr > 0 && zero_sad <= p.zthr;
             if (!skip_int) {
-                for (int i = 1; i < nc; i++) {
-                    long long t = sads[i] + mv_cost(cxs[i], cys[i], cc, p, bits);
-                    if (t < scost) { scost = t; sdx = cxs[i]; sdy = cys[i]; }
+                long long sc_cost = __shfl_sync(0xffffffffu, my_cost, 0);
+                for (int i = 1; i < 6; i++) {
+                    long long ci = __shfl_sync(0xffffffffu, my_cost, i);
+                    if (i >= nc) continue;
+                    long long t = sads[i] + ci;
+                    if (t < scost) { scost = t; sdx = cxs[i]; sdy = cys[i]; sc_cost = ci; }
                 }
-                long long cur_sad = scost - mv_cost(sdx, sdy, cc, p, bits);
+                long long cur_sad = scost - sc_cost;
                 if (p.pthr > 0 && cur_sad <= p.pthr) skip_int = true;
             }
             if (!skip_int) {
@@ -295,21 +398,27 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                 const int HX[6] = {2, 1, -1, -2, -1, 1}, HY[6] = {0, 2, 2, 0, -2, -2};
                 int iter = 0;
                 for (;;) {
+                    int cx = sdx, cy = sdy;
+                    long long lc = 0;
+                    if (lane < 6) {
+                        int dx = cx + HX[lane], dy = cy + HY[lane];
+                        if (abs(dx) <= sr && abs(dy) <= sr) lc = mv_cost(dx, dy, cc, p, bits);
+                    }
                     unsigned hp[6];
 #pragma unroll
                     for (int k = 0; k < 6; k++) {
-                        int dx = sdx + HX[k], dy = sdy + HY[k];
+                        int dx = cx + HX[k], dy = cy + HY[k];
                         hp[k] = (abs(dx) <= sr && abs(dy) <= sr)
-                                    ? sad_int_part(win, WS, wx0, wy0, x0, y0, p.W, p.H, dx, dy, yy, g0, cur8) : 0u;
+                                    ? sad_int_part(view, x0, y0, p.W, p.H, dx, dy, yy, xoff, c0, c1) : 0u;
                     }
                     bool improved = false;
-                    int cx = sdx, cy = sdy;
 #pragma unroll
                     for (int k = 0; k < 6; k++) {
                         long long s = (long long)warp_sum(hp[k]);
+                        long long ck = __shfl_sync(0xffffffffu, lc, k);
                         int dx = cx + HX[k], dy = cy + HY[k];
                         if (abs(dx) > sr || abs(dy) > sr) continue;
-                        long long t = s + mv_cost(dx, dy, cc, p, bits);
+                        long long t = s + ck;
                         if (t < scost) { scost = t; sdx = dx; sdy = dy; improved = true; }
                     }
                     if (!improved) break;
@@ -320,52 +429,70 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                 }
                 // small diamond (enc/motion/scalar.rs:731-756)
                 const int DX[4] = {1, -1, 0, 0}, DY[4] = {0, 0, 1, -1};
+                int cx = sdx, cy = sdy;
+                long long lc = 0;
+                if (lane < 4) {
+                    int dx = cx + DX[lane], dy = cy + DY[lane];
+                    if (abs(dx) <= sr && abs(dy) <= sr) lc = mv_cost(dx, dy, cc, p, bits);
+                }
                 unsigned dp[4];
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
-                    int dx = sdx + DX[k], dy = sdy + DY[k];
+                    int dx = cx + DX[k], dy = cy + DY[k];
                     dp[k] = (abs(dx) <= sr && abs(dy) <= sr)
-                                ? sad_int_part(win, WS, wx0, wy0, x0, y0, p.W, p.H, dx, dy, yy, g0, cur8) : 0u;
+                                ? sad_int_part(view, x0, y0, p.W, p.H, dx, dy, yy, xoff, c0, c1) : 0u;
                 }
-                int cx = sdx, cy = sdy;
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
                     long long s = (long long)warp_sum(dp[k]);
+                    long long ck = __shfl_sync(0xffffffffu, lc, k);
                     int dx = cx + DX[k], dy = cy + DY[k];
                     if (abs(dx) > sr || abs(dy) > sr) continue;
-                    long long t = s + mv_cost(dx, dy, cc, p, bits);
+                    long long t = s + ck;
                     if (t < scost) { scost = t; sdx = dx; sdy = dy; }
                 }
             }
-            // ---- half-pel refinement (enc/motion/scalar.rs:759-839): the nine floor-averaged
-            // candidates around (2*sdx, 2*sdy) from the 3x3 integer neighbourhood of each pixel.
+            // ---- half-pel refinement (enc/motion/scalar.rs:759-839): nine floor-averaged
+            // candidates around (2*sdx, 2*sdy), from a 3x3 integer neighbourhood per pixel,
+            // on packed bytes.  Candidate q = (sy+1)*3 + (sx+1).
             unsigned hpart[9];
-#pragma unroll
-            for (int k = 0; k < 9; k++) hpart[k] = 0;
             {
-                const int Yc = y0 + yy + sdy - wy0;  // window row of the centre sample
-                const uint8_t* r0 = win + (Yc - 1) * WS;
-                const uint8_t* r1 = r0 + WS;
-                const uint8_t* r2 = r1 + WS;
+                const int Yr = y0 + yy + sdy - wy0;  // band/window row of the centre samples
+                const int Xr = xoff + sdx - 1;       // column (relative to x0) of the left neighbour
+                uint32_t A[3][2], B[3][2], Cq[3][2];
 #pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    const int Xc = x0 + xoff + k + sdx - wx0;
-                    int n00 = r0[Xc - 1], n01 = r0[Xc], n02 = r0[Xc + 1];
-                    int n10 = r1[Xc - 1], n11 = r1[Xc], n12 = r1[Xc + 1];
-                    int n20 = r2[Xc - 1], n21 = r2[Xc], n22 = r2[Xc + 1];
-                    int c = cur8[k];
-                    int v[9];
-                    v[0] = (n00 + n01 + n10 + n11) >> 2;  // (sx,sy) = (-1,-1)
-                    v[1] = (n01 + n11) >> 1;              // ( 0,-1)
-                    v[2] = (n01 + n02 + n11 + n12) >> 2;  // (+1,-1)
-                    v[3] = (n10 + n11) >> 1;              // (-1, 0)
-                    v[4] = n11;                           // ( 0, 0)
-                    v[5] = (n11 + n12) >> 1;              // (+1, 0)
-                    v[6] = (n10 + n11 + n20 + n21) >> 2;  // (-1,+1)
-                    v[7] = (n11 + n21) >> 1;              // ( 0,+1)
-                    v[8] = (n11 + n12 + n21 + n22) >> 2;  // (+1,+1)
+                for (int j = 0; j < 3; j++) {
+                    const uint8_t* base = view.org + (Yr - 1 + j) * view.stride + Xr;
+                    uint32_t sa = (uint32_t)__cvta_generic_to_shared(base);
+                    uint32_t al = sa & ~3u, o = sa & 3u;
+                    uint32_t w0 = lds_aligned(al), w1 = lds_aligned(al + 4), w2 = lds_aligned(al + 8),
+                             w3 = lds_aligned(al + 12);
+                    // byte offsets o, o+1, o+2 into w0..w3
+                    uint32_t sh = o * 8;
+                    A[j][0] = __funnelshift_r(w0, w1, sh);
+                    A[j][1] = __funnelshift_r(w1, w2, sh);
+                    uint32_t ob = o + 1, shb = (ob & 3) * 8;
+                    B[j][0] = ob < 4 ? __funnelshift_r(w0, w1, shb) : __funnelshift_r(w1, w2, shb);
+                    B[j][1] = ob < 4 ? __funnelshift_r(w1, w2, shb) : __funnelshift_r(w2, w3, shb);
+                    uint32_t oc = o + 2, shc = (oc & 3) * 8;
+                    Cq[j][0] = oc < 4 ? __funnelshift_r(w0, w1, shc) : __funnelshift_r(w1, w2, shc);
+                    Cq[j][1] = oc < 4 ? __funnelshift_r(w1, w2, shc) : __funnelshift_r(w2, w3, shc);
+                }
 #pragma unroll
-                    for (int q = 0; q < 9; q++) hpart[q] += (unsigned)abs(c - v[q]);
+                for (int h = 0; h < 2; h++) {
+                    const uint32_t cw = h ? c1 : c0;
+                    uint32_t v[9];
+                    v[0] = favg4(A[0][h], B[0][h], A[1][h], B[1][h]);
+                    v[1] = favg(B[0][h], B[1][h]);
+                    v[2] = favg4(B[0][h], Cq[0][h], B[1][h], Cq[1][h]);
+                    v[3] = favg(A[1][h], B[1][h]);
+                    v[4] = B[1][h];
+                    v[5] = favg(B[1][h], Cq[1][h]);
+                    v[6] = favg4(A[1][h], B[1][h], A[2][h], B[2][h]);
+                    v[7] = favg(B[1][h], B[2][h]);
+                    v[8] = favg4(B[1][h], Cq[1][h], B[2][h], Cq[2][h]);
+#pragma unroll
+                    for (int q = 0; q < 9; q++) hpart[q] = (h ? hpart[q] : 0u) + __vsadu4(cw, v[q]);
                 }
             }
             long long hs[9];
@@ -373,6 +500,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
             for (int q = 0; q < 9; q++) hs[q] = (long long)warp_sum(hpart[q]);
             long long best_total = hs[4], best_sad = hs[4];
             int bsx = 0, bsy = 0;
+#pragma unroll
             for (int q = 0; q < 9; q++) {
                 if (q == 4) continue;
                 int sx = q % 3 - 1, sy = q / 3 - 1;
@@ -455,6 +583,12 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
 
             // ---- publish
             if (lane == 0) {
+                unsigned long long rv = tagbits | ((unsigned long long)(uint8_t)raw.dx << 40) |
+                                        ((unsigned long long)(uint8_t)raw.dy << 32) |
+                                        ((unsigned long long)(uint8_t)coded.dx << 24) |
+                                        ((unsigned long long)(uint8_t)coded.dy << 16) |
+                                        ((unsigned long long)(uint8_t)coded.sx << 8) | (unsigned long long)(uint8_t)coded.sy;
+                st_release_u64(p.rec + idx, rv);
                 MbOut o;
                 o.raw[0] = (int8_t)raw.dx; o.raw[1] = (int8_t)raw.dy; o.raw[2] = (int8_t)raw.sx; o.raw[3] = (int8_t)raw.sy;
                 o.coded[0] = (int8_t)coded.dx; o.coded[1] = (int8_t)coded.dy;
@@ -464,32 +598,37 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                 o.pad[0] = o.pad[1] = 0;
                 o.best_sad = (int32_t)best_sad;
                 p.out[idx] = o;
-                unsigned long long rv = tagbits | ((unsigned long long)(uint8_t)raw.dx << 40) |
-                                        ((unsigned long long)(uint8_t)raw.dy << 32) |
-                                        ((unsigned long long)(uint8_t)coded.dx << 24) |
-                                        ((unsigned long long)(uint8_t)coded.dy << 16) |
-                                        ((unsigned long long)(uint8_t)coded.sx << 8) | (unsigned long long)(uint8_t)coded.sy;
-                st_release_u64(p.rec + idx, rv);
             }
             L_raw = MvT{raw.dx, raw.dy, 0, 0};
             L_cod = coded;
             recTL = recT;
             recT = recTR;
         }
+        cp_async_wait0();
     }
 }
 
-size_t search_smem_bytes(int sr) {
+// Shared memory of the search kernel; BAND when the whole MB-row band fits.
+static size_t search_smem(int sr, int W, bool band) {
     size_t ws = 18 + 2 * (size_t)sr;
-    return 256 * sizeof(double) + ws * ws;
+    size_t margin = ((size_t)sr + 1 + 15) & ~(size_t)15;
+    size_t ref = band ? ws * ((size_t)W + 2 * margin) : ws * ws;
+    return 256 * sizeof(double) + 512 + ref + 16;
 }
+static const size_t SEARCH_SMEM_MAX = 200 * 1024;
+static bool search_use_band(int sr, int W) { return search_smem(sr, W, true) <= SEARCH_SMEM_MAX; }
 
-int search_max_grid(int sr, int* grid_out) {
-    size_t sm = search_smem_bytes(sr);
-    cudaError_t e = cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+size_t search_smem_bytes(int sr) { return search_smem(sr, 0, false); }
+
+int search_max_grid(int sr, int W, int* grid_out) {
+    bool band = search_use_band(sr, W);
+    size_t sm = search_smem(sr, W, band);
+    const void* fn = band ? (const void*)k_search<true> : (const void*)k_search<false>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return (int)e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search, 32, sm);
+    e = band ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search<true>, 32, sm)
+             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search<false>, 32, sm);
     if (e != cudaSuccess) return (int)e;
     int dev = 0, nsm = 0;
     cudaGetDevice(&dev);
@@ -499,13 +638,14 @@ int search_max_grid(int sr, int* grid_out) {
 }
 
 int launch_search(const SearchParams& p, int grid, void* stream) {
-    size_t sm = search_smem_bytes(p.sr);
+    bool band = search_use_band(p.sr, p.W);
+    size_t sm = search_smem(p.sr, p.W, band);
     SearchParams q = p;
     void* args[] = {&q};
     // Cooperative launch: every CTA of the grid is co-resident, so the row-to-row waits
     // can always make progress.
-    cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_search, dim3(grid), dim3(32), args, sm,
-                                                (cudaStream_t)stream);
+    const void* fn = band ? (const void*)k_search<true> : (const void*)k_search<false>;
+    cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(32), args, sm, (cudaStream_t)stream);
     return (int)e;
 }
 
@@ -622,38 +762,58 @@ int launch_libm_eval(int which, const float* in, float* out, size_t n, const uin
 // parallel, the f32 sum strictly sequential (Iterator::sum folds left to right), then
 // the per-MB steps in parallel.
 // ---------------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_aq(const uint2* __restrict__ varsum, int n, float base,
-                                             const uint32_t* logfix, int nlog, const uint32_t* expfix, int nexp,
-                                             float* lnv, float* qs) {
-    __shared__ float s_avg;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        uint2 vs = varsum[i];
-        unsigned long long N = 256ull * vs.y - (unsigned long long)vs.x * vs.x;
-        float var = __fdiv_rn(__ull2float_rn(N), 65536.0f);
-        var = var < 4.0f ? 4.0f : var;
-        lnv[i] = glibc_logf(var, logfix, nlog);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float s = 0.0f;
-        int i = 0;
-        for (; i + 4 <= n; i += 4) {
-            float a = lnv[i], b = lnv[i + 1], c = lnv[i + 2], d = lnv[i + 3];
-            s = __fadd_rn(s, a); s = __fadd_rn(s, b); s = __fadd_rn(s, c); s = __fadd_rn(s, d);
+// Variance and ln(variance) of every MB in parallel.
+__global__ void k_aq_log(const uint2* __restrict__ varsum, int n, const uint32_t* logfix, int nlog, float* lnv) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint2 vs = varsum[i];
+    unsigned long long N = 256ull * vs.y - (unsigned long long)vs.x * vs.x;
+    float var = __fdiv_rn(__ull2float_rn(N), 65536.0f);
+    var = var < 4.0f ? 4.0f : var;
+    lnv[i] = glibc_logf(var, logfix, nlog);
+}
+// The strictly sequential f32 sum (Iterator::sum folds left to right): staged through
+// shared memory by the whole CTA, folded by one thread.
+__global__ void __launch_bounds__(1024) k_aq_sum(const float* __restrict__ lnv, int n, float* avg_out) {
+    extern __shared__ float sl[];
+    __shared__ float part;
+    if (threadIdx.x == 0) part = 0.0f;
+    const int CH = 8192;
+    for (int base = 0; base < n; base += CH) {
+        int m = min(CH, n - base);
+        __syncthreads();
+        for (int i = threadIdx.x; i < m; i += blockDim.x) sl[i] = lnv[base + i];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float s = part;
+            int i = 0;
+            for (; i + 8 <= m; i += 8) {
+                float4 a = *(const float4*)(sl + i), b = *(const float4*)(sl + i + 4);
+                s = __fadd_rn(s, a.x); s = __fadd_rn(s, a.y); s = __fadd_rn(s, a.z); s = __fadd_rn(s, a.w);
+                s = __fadd_rn(s, b.x); s = __fadd_rn(s, b.y); s = __fadd_rn(s, b.z); s = __fadd_rn(s, b.w);
+            }
+            for (; i < m; i++) s = __fadd_rn(s, sl[i]);
+            part = s;
         }
-        for (; i < n; i++) s = __fadd_rn(s, lnv[i]);
-        s_avg = __fdiv_rn(s, (float)n);
     }
     __syncthreads();
-    float avg = s_avg;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        float off = __fmul_rn(0.8f, __fsub_rn(lnv[i], avg));
-        qs[i] = __fmul_rn(base, glibc_exp2f(__fdiv_rn(off, 6.0f), expfix, nexp));
-    }
+    if (threadIdx.x == 0) *avg_out = __fdiv_rn(part, (float)n);
+}
+__global__ void k_aq_steps(const float* __restrict__ lnv, int n, const float* avg_in, float base,
+                           const uint32_t* expfix, int nexp, float* qs) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float off = __fmul_rn(0.8f, __fsub_rn(lnv[i], *avg_in));
+    qs[i] = __fmul_rn(base, glibc_exp2f(__fdiv_rn(off, 6.0f), expfix, nexp));
 }
 int launch_aq(const uint2* varsum, int n, float base, const uint32_t* logfix, int nlog, const uint32_t* expfix,
               int nexp, float* lnv_scratch, float* qs, void* stream) {
-    k_aq<<<1, 1024, 0, (cudaStream_t)stream>>>(varsum, n, base, logfix, nlog, expfix, nexp, lnv_scratch, qs);
+    cudaStream_t st = (cudaStream_t)stream;
+    // lnv_scratch holds n floats followed by one float for the mean
+    float* avg = lnv_scratch + n;
+    k_aq_log<<<(n + 127) / 128, 128, 0, st>>>(varsum, n, logfix, nlog, lnv_scratch);
+    k_aq_sum<<<1, 1024, 8192 * sizeof(float), st>>>(lnv_scratch, n, avg);
+    k_aq_steps<<<(n + 127) / 128, 128, 0, st>>>(lnv_scratch, n, avg, base, expfix, nexp, qs);
     return (int)cudaGetLastError();
 }
 
