@@ -114,6 +114,10 @@ riv_status riv_last_kernel_times(riv_encoder* enc, float* us8);
  * P-frames (same stage order as riv_last_kernel_times), io2 = {host->device bytes,
  * device->host bytes}, n2 = {P-frames, kernel launches}. */
 riv_status riv_counters(riv_encoder* enc, double* us8, uint64_t* io2, uint64_t* n2);
+/* Cumulative host-side milliseconds: [0] GPU submission, [1] retiring finished frames,
+ * [2] motion-vector coding, [3] DCT-coefficient coding (summed over worker threads),
+ * [4] record writes, [5] waiting for a frame's entropy coding to finish. */
+riv_status riv_host_times(riv_encoder* enc, double* ms6);
 
 /* In-memory writer (VecWriter, enc/writer.rs:20-69). */
 typedef struct riv_memwriter riv_memwriter;

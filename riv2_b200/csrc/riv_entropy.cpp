@@ -159,14 +159,18 @@ void encode_residual_frame(const int16_t* packed, const uint8_t* eobs, int nbloc
     if (nblocks == 0) return;  // the reference never instantiates the coder
     RansWriter w(&out);
     DctContexts* c = new DctContexts();
+    const int16_t* p = packed;
     for (int b = 0; b < nblocks; b++) {
-        const int16_t* p = packed + (size_t)b * 384;
         const uint8_t* e = eobs + 3 * b;
         // With DC prediction the coded range ends at the last non-zero AC coefficient
-        // (res/rans.rs:250-262); the GPU's last-non-zero index already equals it.
+        // (res/rans.rs:250-262); the GPU's last-non-zero index already equals it.  The
+        // compact layout holds each plane block only up to that index.
         encode_plane(w, *c, p, e[0], true, 0, intra);
-        encode_plane(w, *c, p + 256, e[1], false, 1, intra);
-        encode_plane(w, *c, p + 320, e[2], false, 2, intra);
+        p += e[0] + 1;
+        encode_plane(w, *c, p, e[1], false, 1, intra);
+        p += e[1] + 1;
+        encode_plane(w, *c, p, e[2], false, 2, intra);
+        p += e[2] + 1;
     }
     w.finish();
     delete c;

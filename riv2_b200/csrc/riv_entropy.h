@@ -33,8 +33,8 @@ private:
     int sp_;
 };
 
-// One MB's coefficients in the GPU's compact layout: Y[256], U[64], V[64] plus the last
-// non-zero index of each plane block.
+// Coded MBs in the GPU's compact layout: per MB, the Y, U and V blocks each truncated
+// after its last non-zero coefficient (eobs = those three indices per MB).
 void encode_residual_frame(const int16_t* packed, const uint8_t* eobs, int nblocks, bool intra,
                            std::vector<uint8_t>& out);
 

@@ -257,12 +257,31 @@ struct HostBuf {
     T* as() const { return (T*)p; }
 };
 
+// Pinned host memory mapped into the device address space: kernels write the frame's
+// side info and compacted coefficients straight into it.
+struct MappedBuf {
+    void* h = nullptr;
+    void* d = nullptr;
+    void alloc(size_t bytes) {
+        CK(cudaHostAlloc(&h, bytes ? bytes : 1, cudaHostAllocMapped | cudaHostAllocPortable));
+        CK(cudaHostGetDevicePointer(&d, h, 0));
+    }
+    void release() {
+        if (h) cudaFreeHost(h);
+        h = d = nullptr;
+    }
+    template <class T>
+    T* host() const { return (T*)h; }
+    template <class T>
+    T* dev() const { return (T*)d; }
+};
+
 enum { EV_START, EV_YUV, EV_SEARCH, EV_PRED, EV_AQ, EV_RES, EV_DEBLOCK, EV_COMPACT, EV_N };
 
 struct Slot {
-    DevBuf rgb, side, index, packed, peobs, count;
-    HostBuf h_side, h_count, h_packed, h_peobs, h_status;
-    cudaEvent_t ev_h2d = nullptr, ev_gpu = nullptr, ev_side = nullptr, ev_coef = nullptr;
+    DevBuf rgb;
+    MappedBuf side, hdr, packed, peobs;  // hdr: coded MBs, coefficients, device status
+    cudaEvent_t ev_h2d = nullptr, ev_gpu = nullptr;
     cudaEvent_t ev_k[EV_N] = {};
 };
 
@@ -271,7 +290,7 @@ struct Job {
     int type = 0, slot = 0;
     int state = 0;  // 0 submitted, 1 entropy running
     uint32_t count = 0;
-    std::future<void> fut;
+    std::future<void> fut, fut_mv;
     std::vector<uint8_t> res_bytes, mv_bytes;
     int8_t bias[2] = {0, 0};
     riv_frame_stats stats{};
@@ -291,6 +310,7 @@ struct riv_encoder {
     cudaStream_t S = nullptr, C = nullptr;
     // device state
     DevBuf cur, ref[2], pred, mbout, coded[2], rec, varsum, lnv, qs, coeffs, opt_skip, fmask, eobs, status;
+    DevBuf cindex, coffset;
     DevBuf mvbits, logfix, expfix, ytab, ctab;
     int ref_cur = 0, coded_cur = 0;
     bool has_ref = false, has_prev_mvs = false;
@@ -305,6 +325,9 @@ struct riv_encoder {
     std::deque<Job> jobs;
     MvCoder mvc;
     std::unique_ptr<ThreadPool> pool;
+    std::unique_ptr<ThreadPool> mv_exec;  // one thread: MV coding strictly in frame order
+    double host_ms[6] = {0};  // submit, retire, mv coding, dct coding (summed), write, blocked
+    std::mutex stat_mu;
     float last_times[8] = {0};
     bool have_times = false;
     riv_frame_stats last_stats{};
@@ -406,24 +429,19 @@ static void setup_device(riv_encoder* e) {
     for (auto& s : e->slots) {
         s.rgb.alloc(rgb_bytes);
         s.side.alloc((size_t)N * 4);
-        s.index.alloc((size_t)N * 4);
+        s.hdr.alloc(16);
         s.packed.alloc((size_t)N * 384 * 2);
         s.peobs.alloc((size_t)N * 3);
-        s.count.alloc(4);
-        s.h_side.alloc((size_t)N * 4);
-        s.h_count.alloc(4);
-        s.h_packed.alloc((size_t)N * 384 * 2);
-        s.h_peobs.alloc((size_t)N * 3);
-        s.h_status.alloc(4);
         CK(cudaEventCreateWithFlags(&s.ev_h2d, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&s.ev_gpu, cudaEventDisableTiming));
-        CK(cudaEventCreateWithFlags(&s.ev_side, cudaEventDisableTiming));
-        CK(cudaEventCreateWithFlags(&s.ev_coef, cudaEventDisableTiming));
         for (int k = 0; k < EV_N; k++) CK(cudaEventCreate(&s.ev_k[k]));
     }
+    e->cindex.alloc((size_t)N * 4);
+    e->coffset.alloc((size_t)N * 4);
     unsigned nt = c.entropy_threads;
     if (nt == 0) nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency() > 1 ? std::thread::hardware_concurrency() - 1 : 1u));
     e->pool.reset(new ThreadPool(nt));
+    e->mv_exec.reset(new ThreadPool(1));
     CK(cudaStreamSynchronize(e->S));
 }
 
@@ -481,8 +499,8 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         if (e->intra_level > 0) CK(launch_deblock(recon, W, H, e->intra_E, e->intra_I, e->intra_H, nullptr, S));
         CK(cudaEventRecord(s.ev_k[EV_DEBLOCK], S));
         CK(launch_compact(e->opt_skip.as<uint8_t>(), e->mbout.as<MbOut>(), e->coeffs.as<int16_t>(), e->eobs.as<uint8_t>(), N, 1,
-                          s.side.as<uint32_t>(), s.index.as<int32_t>(), s.packed.as<int16_t>(), s.peobs.as<uint8_t>(),
-                          s.count.as<uint32_t>(), S));
+                          e->cindex.as<int32_t>(), e->coffset.as<int32_t>(), s.side.dev<uint32_t>(),
+                          s.packed.dev<int16_t>(), s.peobs.dev<uint8_t>(), s.hdr.dev<uint32_t>(), S));
         e->has_prev_mvs = false;
     } else {
         SearchParams sp{};
@@ -532,40 +550,37 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         if (e->inter_level > 0) CK(launch_deblock(recon, W, H, e->inter_E, e->inter_I, e->inter_H, e->fmask.as<uint8_t>(), S));
         CK(cudaEventRecord(s.ev_k[EV_DEBLOCK], S));
         CK(launch_compact(e->opt_skip.as<uint8_t>(), e->mbout.as<MbOut>(), e->coeffs.as<int16_t>(), e->eobs.as<uint8_t>(), N, 0,
-                          s.side.as<uint32_t>(), s.index.as<int32_t>(), s.packed.as<int16_t>(), s.peobs.as<uint8_t>(),
-                          s.count.as<uint32_t>(), S));
+                          e->cindex.as<int32_t>(), e->coffset.as<int32_t>(), s.side.dev<uint32_t>(),
+                          s.packed.dev<int16_t>(), s.peobs.dev<uint8_t>(), s.hdr.dev<uint32_t>(), S));
         e->coded_cur = cn;
         e->has_prev_mvs = true;
     }
     CK(cudaEventRecord(s.ev_k[EV_COMPACT], S));
+    CK(cudaMemcpyAsync(s.hdr.host<uint32_t>() + 2, e->status.p, 4, cudaMemcpyDeviceToHost, S));
     CK(cudaEventRecord(s.ev_gpu, S));
     e->ref_cur = nxt;
     e->has_ref = true;
-    CK(cudaStreamWaitEvent(e->C, s.ev_gpu, 0));
-    CK(cudaMemcpyAsync(s.h_side.p, s.side.p, (size_t)N * 4, cudaMemcpyDeviceToHost, e->C));
-    CK(cudaMemcpyAsync(s.h_count.p, s.count.p, 4, cudaMemcpyDeviceToHost, e->C));
-    CK(cudaMemcpyAsync(s.h_status.p, e->status.p, 4, cudaMemcpyDeviceToHost, e->C));
-    CK(cudaEventRecord(s.ev_side, e->C));
 }
 
-// Host part of a frame after its side info is back: coefficient copy, MV coding
-// (ordered), then the DCT coder on the pool.
+// Host part of a frame once its GPU work is done: its side info and coefficients are
+// already in mapped host memory.  MV coding goes to the ordered single-thread executor
+// (its contexts carry across frames), DCT-coefficient coding to the pool.
+static double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 static riv_status retire(riv_encoder* e, Job& j) {
     Slot& s = e->slots[j.slot];
-    CK(cudaEventSynchronize(s.ev_side));
-    unsigned st = *s.h_status.as<unsigned>();
+    double t0 = now_ms();
+    CK(cudaEventSynchronize(s.ev_gpu));
+    const uint32_t* hdr = s.hdr.host<uint32_t>();
+    unsigned st = hdr[2];
     if (st) {
         return fail(e, (st & ST_WAIT_TIMEOUT) ? RIV_ERR_DEVICE_TIMEOUT : RIV_ERR_ENCODING_FAILED,
                     (st & ST_WAIT_TIMEOUT) ? "device-side wavefront wait timed out" : "device search iteration cap hit");
     }
-    j.count = *s.h_count.as<uint32_t>();
-    e->d2h_bytes += (uint64_t)e->NMB * 4 + 8 + (uint64_t)j.count * (768 + 3);
-    if (j.count) {
-        CK(cudaMemcpyAsync(s.h_packed.p, s.packed.p, (size_t)j.count * 768, cudaMemcpyDeviceToHost, e->C));
-        CK(cudaMemcpyAsync(s.h_peobs.p, s.peobs.p, (size_t)j.count * 3, cudaMemcpyDeviceToHost, e->C));
-        CK(cudaEventRecord(s.ev_coef, e->C));
-        CK(cudaEventSynchronize(s.ev_coef));
-    }
+    j.count = hdr[0];
+    const uint32_t ncoef = hdr[1];
+    e->d2h_bytes += (uint64_t)e->NMB * 4 + 12 + (uint64_t)j.count * 3 + (uint64_t)ncoef * 2;
     float t[8] = {0};
     for (int k = 0; k < 7; k++) cudaEventElapsedTime(&t[k], s.ev_k[k], s.ev_k[k + 1]);
     cudaEventElapsedTime(&t[7], s.ev_k[EV_START], s.ev_k[EV_COMPACT]);
@@ -583,56 +598,74 @@ static riv_status retire(riv_encoder* e, Job& j) {
     S.storage_width = (uint32_t)e->W;
     S.storage_height = (uint32_t)e->H;
     S.blocks_total = (uint32_t)N;
-    if (j.type == 2) {
-        const uint32_t* side = s.h_side.as<uint32_t>();
-        std::vector<std::pair<int8_t, int8_t>> nd;
-        nd.reserve(N);
-        for (int i = 0; i < N; i++)
-            if ((side[i] & 7) == M_NEW) nd.emplace_back((int8_t)(side[i] >> 8), (int8_t)(side[i] >> 16));
-        compute_delta_bias(nd, j.bias[0], j.bias[1]);
-        // MvCodedBlock assembly (enc/encoder.rs:774-818)
-        std::vector<MvCodedBlock> blocks(N);
-        for (int i = 0; i < N; i++) {
-            uint32_t v = side[i];
-            MvCodedBlock& b = blocks[i];
-            b.mode = (uint8_t)(v & 7);
-            b.new_base = (uint8_t)((v >> 3) & 7);
-            b.skip = (v >> 24) & 1;
-            b.dx = b.dy = 0;
-            b.spx = b.spy = SP_ZERO;
-            if (b.mode == M_NEW) {
-                b.dx = (int8_t)std::min(std::max((int)(int8_t)(v >> 8) - j.bias[0], -128), 127);
-                b.dy = (int8_t)std::min(std::max((int)(int8_t)(v >> 16) - j.bias[1], -128), 127);
-                b.spx = ((v >> 6) & 1) ? SP_PLUS : SP_ZERO;
-                b.spy = ((v >> 7) & 1) ? SP_PLUS : SP_ZERO;
-                S.mv_new_blocks++;
-                S.mv_new_base_counts[std::min<int>(b.new_base, 4)]++;
-            }
-            S.mv_mode_counts[b.mode]++;
-            if (b.skip) S.blocks_skipped++;
-        }
-        e->mvc.encode_frame(blocks, e->BW, j.mv_bytes);
-        S.mv_bias_dx = j.bias[0];
-        S.mv_bias_dy = j.bias[1];
-        S.rdo_lambda = e->L.lambda;
-    } else {
-        e->mvc.reset();  // key frame: MV entropy contexts restart (enc/encoder.rs:335-337)
-    }
-    const int16_t* packed = s.h_packed.as<int16_t>();
-    const uint8_t* peobs = s.h_peobs.as<uint8_t>();
     Job* jp = &j;
+    riv_encoder* ep = e;
+    const uint32_t* side = s.side.host<uint32_t>();
+    if (j.type == 2) {
+        j.fut_mv = e->mv_exec->submit([ep, jp, side, N] {
+            double m0 = now_ms();
+            riv_frame_stats& S = jp->stats;
+            std::vector<std::pair<int8_t, int8_t>> nd;
+            nd.reserve(N);
+            for (int i = 0; i < N; i++)
+                if ((side[i] & 7) == M_NEW) nd.emplace_back((int8_t)(side[i] >> 8), (int8_t)(side[i] >> 16));
+            compute_delta_bias(nd, jp->bias[0], jp->bias[1]);
+            // MvCodedBlock assembly (enc/encoder.rs:774-818)
+            std::vector<MvCodedBlock> blocks(N);
+            for (int i = 0; i < N; i++) {
+                uint32_t v = side[i];
+                MvCodedBlock& b = blocks[i];
+                b.mode = (uint8_t)(v & 7);
+                b.new_base = (uint8_t)((v >> 3) & 7);
+                b.skip = (v >> 24) & 1;
+                b.dx = b.dy = 0;
+                b.spx = b.spy = SP_ZERO;
+                if (b.mode == M_NEW) {
+                    b.dx = (int8_t)std::min(std::max((int)(int8_t)(v >> 8) - jp->bias[0], -128), 127);
+                    b.dy = (int8_t)std::min(std::max((int)(int8_t)(v >> 16) - jp->bias[1], -128), 127);
+                    b.spx = ((v >> 6) & 1) ? SP_PLUS : SP_ZERO;
+                    b.spy = ((v >> 7) & 1) ? SP_PLUS : SP_ZERO;
+                    S.mv_new_blocks++;
+                    S.mv_new_base_counts[std::min<int>(b.new_base, 4)]++;
+                }
+                S.mv_mode_counts[b.mode]++;
+                if (b.skip) S.blocks_skipped++;
+            }
+            ep->mvc.encode_frame(blocks, ep->BW, jp->mv_bytes);
+            S.mv_bias_dx = jp->bias[0];
+            S.mv_bias_dy = jp->bias[1];
+            S.rdo_lambda = ep->L.lambda;
+            double dt = now_ms() - m0;
+            std::lock_guard<std::mutex> g(ep->stat_mu);
+            ep->host_ms[2] += dt;
+        });
+    } else {
+        // key frame: MV entropy contexts restart (enc/encoder.rs:335-337), in frame order
+        j.fut_mv = e->mv_exec->submit([ep] { ep->mvc.reset(); });
+    }
+    const int16_t* packed = s.packed.host<int16_t>();
+    const uint8_t* peobs = s.peobs.host<uint8_t>();
     uint32_t count = j.count;
     bool intra = j.type == 1;
-    j.fut = e->pool->submit([jp, packed, peobs, count, intra] {
+    j.fut = e->pool->submit([jp, ep, packed, peobs, count, intra] {
+        double d0 = now_ms();
         encode_residual_frame(packed, peobs, (int)count, intra, jp->res_bytes);
+        double dt = now_ms() - d0;
+        std::lock_guard<std::mutex> g(ep->stat_mu);
+        ep->host_ms[3] += dt;
     });
     j.state = 1;
+    e->host_ms[1] += now_ms() - t0;
     return RIV_OK;
 }
 
 // PackedFrame::to_bytes (com/format.rs:171-207) and the writer call.
 static riv_status write_job(riv_encoder* e, Job& j) {
+    double b0 = now_ms();
+    j.fut_mv.get();
     j.fut.get();
+    double w0 = now_ms();
+    e->host_ms[5] += w0 - b0;
     const riv_config& c = e->cfg;
     std::vector<uint8_t> rec;
     rec.reserve(32 + j.mv_bytes.size() + j.res_bytes.size());
@@ -657,6 +690,7 @@ static riv_status write_job(riv_encoder* e, Job& j) {
     j.stats.mv_bytes = (uint32_t)j.mv_bytes.size();
     j.stats.residual_bytes = (uint32_t)j.res_bytes.size();
     if (e->wr.write(e->wr.user, rec.data(), rec.size()) != 0) return fail(e, RIV_ERR_IO, "writer.write failed");
+    e->host_ms[4] += now_ms() - w0;
     e->frame_count++;
     memcpy(e->last_times, j.times, sizeof(j.times));
     e->have_times = true;
@@ -672,7 +706,7 @@ static riv_status pump(riv_encoder* e, bool block_front) {
     for (auto& j : e->jobs) {
         if (j.state != 0) continue;
         if (!block) {
-            cudaError_t q = cudaEventQuery(e->slots[j.slot].ev_side);
+            cudaError_t q = cudaEventQuery(e->slots[j.slot].ev_gpu);
             if (q == cudaErrorNotReady) break;
             if (q != cudaSuccess) throw CudaError{q, "cudaEventQuery"};
         }
@@ -684,7 +718,9 @@ static riv_status pump(riv_encoder* e, bool block_front) {
     while (!e->jobs.empty()) {
         Job& f = e->jobs.front();
         if (f.state != 1) break;
-        if (!block && f.fut.wait_for(std::chrono::seconds(0)) != std::future_status::ready) break;
+        if (!block && (f.fut.wait_for(std::chrono::seconds(0)) != std::future_status::ready ||
+                       f.fut_mv.wait_for(std::chrono::seconds(0)) != std::future_status::ready))
+            break;
         riv_status st = write_job(e, f);
         if (st) return st;
         e->jobs.pop_front();
@@ -725,8 +761,10 @@ static riv_status encode_common(riv_encoder* e, int src, const void* a, const vo
         j.ts = ts;
         j.type = intra ? 1 : 2;
         j.slot = (int)(n % cap);
+        double s0 = now_ms();
         submit_gpu(e, j, src, a, b, c3);
         e->submitted++;
+        e->host_ms[0] += now_ms() - s0;
         if (src == 0 || src == 2) CK(cudaEventSynchronize(e->slots[j.slot].ev_h2d));  // caller buffer reusable
         if (e->cfg.pipeline_depth == 0 || stats) {
             riv_status st = drain_all(e);
@@ -859,24 +897,24 @@ riv_status riv_finish(riv_encoder* e) {  // enc/encoder.rs:950-961
 void riv_encoder_free(riv_encoder* e) {
     if (!e) return;
     cudaSetDevice(e->cfg.device);
-    for (auto& j : e->jobs)
+    for (auto& j : e->jobs) {
         if (j.fut.valid()) j.fut.wait();
+        if (j.fut_mv.valid()) j.fut_mv.wait();
+    }
     e->pool.reset();
+    e->mv_exec.reset();
     if (e->S) cudaStreamSynchronize(e->S);
     if (e->C) cudaStreamSynchronize(e->C);
     for (auto& s : e->slots) {
-        s.rgb.release(); s.side.release(); s.index.release(); s.packed.release(); s.peobs.release(); s.count.release();
-        s.h_side.release(); s.h_count.release(); s.h_packed.release(); s.h_peobs.release(); s.h_status.release();
+        s.rgb.release(); s.side.release(); s.hdr.release(); s.packed.release(); s.peobs.release();
         if (s.ev_h2d) cudaEventDestroy(s.ev_h2d);
         if (s.ev_gpu) cudaEventDestroy(s.ev_gpu);
-        if (s.ev_side) cudaEventDestroy(s.ev_side);
-        if (s.ev_coef) cudaEventDestroy(s.ev_coef);
         for (int k = 0; k < EV_N; k++)
             if (s.ev_k[k]) cudaEventDestroy(s.ev_k[k]);
     }
     DevBuf* bufs[] = {&e->cur, &e->ref[0], &e->ref[1], &e->pred, &e->mbout, &e->coded[0], &e->coded[1], &e->rec,
                       &e->varsum, &e->lnv, &e->qs, &e->coeffs, &e->opt_skip, &e->fmask, &e->eobs, &e->status,
-                      &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab};
+                      &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset};
     for (DevBuf* b : bufs) b->release();
     if (e->S) cudaStreamDestroy(e->S);
     if (e->C) cudaStreamDestroy(e->C);
@@ -922,6 +960,13 @@ riv_status riv_debug_frame_state(riv_encoder* e, int what, void* out, size_t siz
     } catch (const CudaError& ce) {
         return fail(e, RIV_ERR_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
     }
+    return RIV_OK;
+}
+
+riv_status riv_host_times(riv_encoder* e, double* ms6) {
+    if (!e || !ms6) return RIV_ERR_FRAME;
+    std::lock_guard<std::mutex> g(e->stat_mu);
+    memcpy(ms6, e->host_ms, sizeof(e->host_ms));
     return RIV_OK;
 }
 

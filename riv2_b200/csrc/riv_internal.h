@@ -78,8 +78,8 @@ int launch_aq(const uint2* varsum, int n, float base, const uint32_t* logfix, in
 int launch_residual(const ResidualParams& p, int nmb, void* stream);
 int launch_deblock(uint8_t* yuv, int W, int H, int E, int I, int Hev, const uint8_t* mask, void* stream);
 int launch_compact(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coeffs, const uint8_t* eobs, int nmb,
-                   int intra, uint32_t* side, int32_t* index, int16_t* packed, uint8_t* packed_eobs, uint32_t* count,
-                   void* stream);
+                   int intra, int32_t* index, int32_t* offset, uint32_t* side, int16_t* packed,
+                   uint8_t* packed_eobs, uint32_t* hdr, void* stream);
 // libm device helpers exposed for the exhaustive check
 int launch_libm_eval(int which, const float* in, float* out, size_t n, const uint32_t* fix, int nfix, void* stream);
 

@@ -79,13 +79,16 @@ int launch_rgb_to_yuv(const uint8_t* rgb, int dw, int dh, uint8_t* yuv, int W, i
 // returns a partial SAD already above the limit (so the candidate cannot win), hence
 // full SADs followed by the same in-order strict-'<' scan give identical decisions.
 // ---------------------------------------------------------------------------------
-__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+// Each MB record is one 64-bit word (tag + payload), single-copy atomic, and consumers
+// read nothing else the producer wrote during the kernel, so relaxed gpu-scope accesses
+// suffice (no fences on the wavefront's critical path).
+__device__ __forceinline__ unsigned long long ld_rec(const unsigned long long* p) {
     unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+__device__ __forceinline__ void st_rec(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 __device__ __forceinline__ unsigned warp_sum(unsigned v) { return __reduce_add_sync(0xffffffffu, v); }
 
@@ -234,7 +237,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
         cp_async_commit();
 
         MvT L_raw{0, 0, 0, 0}, L_cod{0, 0, 0, 0};
-        unsigned long long recT = 0, recTL = 0;
+        unsigned long long recT = 0, recTL = 0, pref = 0;
         for (int bx = 0; bx < p.BW; bx++) {
             const int x0 = bx * 16;
             const int idx = r * p.BW + bx;
@@ -283,7 +286,9 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
             const uint32_t c0 = *(const uint32_t*)(cb + yy * 16 + xoff);
             const uint32_t c1 = *(const uint32_t*)(cb + yy * 16 + xoff + 4);
 
-            // ---- wait for the row above (top-right, or top at the last column)
+            // ---- wait for the row above (top-right, or top at the last column).  The record
+            // of the next MB's top-right was requested one MB earlier (pref); it is polled
+            // again only if it had not been published yet.
             unsigned long long recTR = 0;
             bool has_tr = false;
             if (r > 0) {
@@ -291,13 +296,15 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                 unsigned long long v = 0;
                 if (lane == 0) {
                     long long spins = 0;
-                    v = ld_acquire_u64(p.rec + wi);
+                    v = pref;
+                    if ((v & 0xffff000000000000ull) != tagbits) v = ld_rec(p.rec + wi);
                     while ((v & 0xffff000000000000ull) != tagbits) {
                         if (++spins > p.spin_limit || failed) { failed = true; break; }
                         __nanosleep(20);
-                        v = ld_acquire_u64(p.rec + wi);
+                        v = ld_rec(p.rec + wi);
                     }
-                    if (bx == 0) recT = ld_acquire_u64(p.rec + (r - 1) * p.BW);
+                    if (bx == 0) recT = ld_rec(p.rec + (r - 1) * p.BW);
+                    pref = bx + 1 < p.BW ? ld_rec(p.rec + (r - 1) * p.BW + min(bx + 2, p.BW - 1)) : 0ull;
                 }
                 failed = __shfl_sync(0xffffffffu, (int)failed, 0) != 0;
                 v = __shfl_sync(0xffffffffu, v, 0);
@@ -328,67 +335,68 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                 Tm_cod = MvT{pc.x, pc.y, pc.z, pc.w};
                 Tmx = Tm_cod.dx; Tmy = Tm_cod.dy;
             }
-            // ---- seeds, nearest/near/median (enc/motion/scalar.rs:56-156)
-            int px[5], py[5], np = 0;
-            if (has_l) { px[np] = L_raw.dx; py[np] = L_raw.dy; np++; }
-            if (has_t) { px[np] = Tx; py[np] = Ty; np++; }
-            if (has_tr) { px[np] = TRx; py[np] = TRy; np++; }
-            if (has_tl) { px[np] = TLx; py[np] = TLy; np++; }
-            if (has_tm) { px[np] = Tmx; py[np] = Tmy; np++; }
-            int ux0 = 0, uy0 = 0, ux1 = 0, uy1 = 0, nu = 0;
-            for (int i = 0; i < np && nu < 2; i++) {
-                if (nu == 1 && px[i] == ux0 && py[i] == uy0) continue;
-                if (nu == 0) { ux0 = px[i]; uy0 = py[i]; } else { ux1 = px[i]; uy1 = py[i]; }
-                nu++;
-            }
+            // ---- seeds, nearest/near/median (enc/motion/scalar.rs:56-156).  Predictor slots in
+            // the reference's order: left, top, top-right, top-left, temporal.
+            const int PX[5] = {L_raw.dx, Tx, TRx, TLx, Tmx}, PY[5] = {L_raw.dy, Ty, TRy, TLy, Tmy};
+            const bool PV[5] = {has_l, has_t, has_tr, has_tl, has_tm};
             CostCtx cc;
-            cc.nx = ux0; cc.ny = uy0; cc.rx = ux1; cc.ry = uy1;
+            cc.nx = cc.ny = cc.rx = cc.ry = 0;
             {
+                int nu = 0;
+#pragma unroll
+                for (int i = 0; i < 5; i++) {
+                    bool take = PV[i] && (nu == 0 || (nu == 1 && !(PX[i] == cc.nx && PY[i] == cc.ny)));
+                    if (take && nu == 0) { cc.nx = PX[i]; cc.ny = PY[i]; }
+                    else if (take && nu == 1) { cc.rx = PX[i]; cc.ry = PY[i]; }
+                    nu += take ? 1 : 0;
+                }
                 int lx = has_l ? L_raw.dx : 0, ly = has_l ? L_raw.dy : 0;
                 int tx = has_t ? Tx : 0, ty = has_t ? Ty : 0;
-                int qx = 0, qy = 0;
-                if (has_tr) { qx = TRx; qy = TRy; }
-                else if (has_tl) { qx = TLx; qy = TLy; }
+                int qx = has_tr ? TRx : (has_tl ? TLx : 0), qy = has_tr ? TRy : (has_tl ? TLy : 0);
                 cc.mx = median3(lx, tx, qx);
                 cc.my = median3(ly, ty, qy);
             }
-            // seed candidate list: (0,0) first, then predictors in order, deduped, within sr
-            int cxs[6], cys[6], nc = 1;
-            cxs[0] = 0; cys[0] = 0;
-            for (int i = 0; i < np; i++) {
-                if (abs(px[i]) > sr || abs(py[i]) > sr) continue;
-                bool dup = false;
-                for (int j = 0; j < nc; j++) dup |= (cxs[j] == px[i] && cys[j] == py[i]);
-                if (!dup) { cxs[nc] = px[i]; cys[nc] = py[i]; nc++; }
+            // seed slots: 0 = (0,0), 1..5 = predictors kept if within range and not already
+            // pushed (push_candidate, enc/motion/scalar.rs:46-53)
+            bool SV[6];
+            SV[0] = true;
+#pragma unroll
+            for (int i = 0; i < 5; i++) {
+                bool ok = PV[i] && abs(PX[i]) <= sr && abs(PY[i]) <= sr && !(PX[i] == 0 && PY[i] == 0);
+#pragma unroll
+                for (int j = 0; j < i; j++) ok = ok && !(SV[j + 1] && PX[j] == PX[i] && PY[j] == PY[i]);
+                SV[i + 1] = ok;
             }
-            // ---- zero SAD and the seed round; lane k evaluates the MV cost of candidate k
+            // ---- zero SAD and the seed round; lane k evaluates the MV cost of slot k
             long long my_cost = 0;
             {
-                int k = min(lane, 5);
                 int kx = 0, ky = 0;
+                bool kv = lane == 0;
 #pragma unroll
-                for (int i = 0; i < 6; i++)
-                    if (i == k) { kx = cxs[i]; ky = cys[i]; }
-                if (lane < nc) my_cost = mv_cost(kx, ky, cc, p, bits);
+                for (int i = 0; i < 5; i++)
+                    if (lane == i + 1) { kx = PX[i]; ky = PY[i]; kv = SV[i + 1]; }
+                if (kv) my_cost = mv_cost(kx, ky, cc, p, bits);
             }
             unsigned part[6];
+            part[0] = sad_int_part(view, x0, y0, p.W, p.H, 0, 0, yy, xoff, c0, c1);
 #pragma unroll
-            for (int i = 0; i < 6; i++)
-                part[i] = i < nc ? sad_int_part(view, x0, y0, p.W, p.H, cxs[i], cys[i], yy, xoff, c0, c1) : 0u;
+            for (int i = 0; i < 5; i++)
+                part[i + 1] = SV[i + 1] ? sad_int_part(view, x0, y0, p.W, p.H, PX[i], PY[i], yy, xoff, c0, c1) : 0u;
             long long sads[6];
 #pragma unroll
             for (int i = 0; i < 6; i++) sads[i] = (long long)warp_sum(part[i]);
             long long zero_sad = sads[0];
             int sdx = 0, sdy = 0;
-            long long scost = zero_sad + __shfl_sync(0xffffffffu, my_cost, 0);
+            long long sc_cost = __shfl_sync(0xffffffffu, my_cost, 0);
+            long long scost = zero_sad + sc_cost;
             bool skip_int = p.zthr > 0 && zero_sad <= p.zthr;
             if (!skip_int) {
-                long long sc_cost = __shfl_sync(0xffffffffu, my_cost, 0);
-                for (int i = 1; i < 6; i++) {
-                    long long ci = __shfl_sync(0xffffffffu, my_cost, i);
-                    if (i >= nc) continue;
-                    long long t = sads[i] + ci;
-                    if (t < scost) { scost = t; sdx = cxs[i]; sdy = cys[i]; sc_cost = ci; }
+#pragma unroll
+                for (int i = 0; i < 5; i++) {
+                    long long ci = __shfl_sync(0xffffffffu, my_cost, i + 1);
+                    if (!SV[i + 1]) continue;
+                    long long t = sads[i + 1] + ci;
+                    if (t < scost) { scost = t; sdx = PX[i]; sdy = PY[i]; sc_cost = ci; }
                 }
                 long long cur_sad = scost - sc_cost;
                 if (p.pthr > 0 && cur_sad <= p.pthr) skip_int = true;
@@ -396,12 +404,15 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
             if (!skip_int) {
                 // large hexagon (enc/motion/scalar.rs:694-729)
                 const int HX[6] = {2, 1, -1, -2, -1, 1}, HY[6] = {0, 2, 2, 0, -2, -2};
+                // HX/HY of lane k (k < 6) without a lane-indexed array
+                const int hxl = (int)(int8_t)(0x01FFFEFF0102ull >> (8 * min(lane, 5)));
+                const int hyl = (int)(int8_t)(0xFEFE00020200ull >> (8 * min(lane, 5)));
                 int iter = 0;
                 for (;;) {
                     int cx = sdx, cy = sdy;
                     long long lc = 0;
                     if (lane < 6) {
-                        int dx = cx + HX[lane], dy = cy + HY[lane];
+                        int dx = cx + hxl, dy = cy + hyl;
                         if (abs(dx) <= sr && abs(dy) <= sr) lc = mv_cost(dx, dy, cc, p, bits);
                     }
                     unsigned hp[6];
@@ -429,10 +440,12 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                 }
                 // small diamond (enc/motion/scalar.rs:731-756)
                 const int DX[4] = {1, -1, 0, 0}, DY[4] = {0, 0, 1, -1};
+                const int dxl = (int)(int8_t)(0x0000FF01u >> (8 * min(lane, 3)));
+                const int dyl = (int)(int8_t)(0xFF010000u >> (8 * min(lane, 3)));
                 int cx = sdx, cy = sdy;
                 long long lc = 0;
                 if (lane < 4) {
-                    int dx = cx + DX[lane], dy = cy + DY[lane];
+                    int dx = cx + dxl, dy = cy + dyl;
                     if (abs(dx) <= sr && abs(dy) <= sr) lc = mv_cost(dx, dy, cc, p, bits);
                 }
                 unsigned dp[4];
@@ -529,20 +542,19 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
             // ---- MV mode decision on the coded (reconstructed) neighbours
             // (enc/encoder.rs:459-733, res/mv_predictor.rs:59-272)
             MvT cT = rec_cod(recT), cTR = rec_cod(recTR), cTL = rec_cod(recTL);
-            MvT cand[5];
-            int ncand = 0;
-            auto addc = [&](const MvT& m) {
-                bool dup = false;
-                for (int j = 0; j < ncand; j++) dup |= mv_eq(cand[j], m);
-                if (!dup) cand[ncand++] = m;
-            };
-            if (has_l) addc(L_cod);
-            if (has_t) addc(cT);
-            if (has_tr) addc(cTR);
-            if (has_tl) addc(cTL);
-            if (has_tm) addc(Tm_cod);
             const MvT zero{0, 0, 0, 0};
-            MvT nearest = ncand > 0 ? cand[0] : zero, nearm = ncand > 1 ? cand[1] : zero;
+            MvT nearest = zero, nearm = zero;
+            {
+                const MvT CS[5] = {L_cod, cT, cTR, cTL, Tm_cod};
+                int nu = 0;
+#pragma unroll
+                for (int i = 0; i < 5; i++) {
+                    bool take = PV[i] && (nu == 0 || (nu == 1 && !mv_eq(CS[i], nearest)));
+                    if (take && nu == 0) nearest = CS[i];
+                    else if (take && nu == 1) nearm = CS[i];
+                    nu += take ? 1 : 0;
+                }
+            }
             MvT temporal = has_tm ? Tm_cod : zero;
             const int mx = raw.dx * 2 + raw.sx, my = raw.dy * 2 + raw.sy;
             auto hpeq = [&](const MvT& t) { return mx == t.dx * 2 + t.sx && my == t.dy * 2 + t.sy; };
@@ -562,6 +574,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                 const int selbits[5] = {1, 2, 3, 4, 4};
                 unsigned best = 0xffffffffu;
                 int bbx = nearest.dx, bby = nearest.dy;
+#pragma unroll
                 for (int k = 0; k < 5; k++) {
                     if (!hasb[k]) continue;
                     int ddx = sat8(raw.dx - bases[k].dx), ddy = sat8(raw.dy - bases[k].dy);
@@ -588,7 +601,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                                         ((unsigned long long)(uint8_t)coded.dx << 24) |
                                         ((unsigned long long)(uint8_t)coded.dy << 16) |
                                         ((unsigned long long)(uint8_t)coded.sx << 8) | (unsigned long long)(uint8_t)coded.sy;
-                st_release_u64(p.rec + idx, rv);
+                st_rec(p.rec + idx, rv);
                 MbOut o;
                 o.raw[0] = (int8_t)raw.dx; o.raw[1] = (int8_t)raw.dy; o.raw[2] = (int8_t)raw.sx; o.raw[3] = (int8_t)raw.sy;
                 o.coded[0] = (int8_t)coded.dx; o.coded[1] = (int8_t)coded.dy;
@@ -1156,49 +1169,57 @@ int launch_deblock(uint8_t* yuv, int W, int H, int E, int I, int Hv, const uint8
 }
 
 // ---------------------------------------------------------------------------------
-// K8: per-MB side info (4 bytes) and compaction of coded MBs' coefficients for the host
-// entropy coder.  side = mode | base<<3 | subx<<6 | suby<<7, rdx, rdy, optskip|fmask<<1.
+// K8: per-MB side info and compaction of the coded MBs' coefficients for the host entropy
+// coder, written straight into mapped pinned host memory (no separate device->host copy).
+// side = mode | base<<3 | subx<<6 | suby<<7 | rdx<<8 | rdy<<16 | optskip<<24.
+// Each coded MB contributes its three plane blocks truncated after the last non-zero
+// coefficient (the entropy coder never reads beyond it): Y[0..eY], U[0..eU], V[0..eV].
+// hdr[0] = coded MB count, hdr[1] = total coefficients written.
 // ---------------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_scan(const uint8_t* opt_skip, int nmb, int intra, int32_t* index,
-                                               uint32_t* count) {
-    __shared__ int wsum[32];
-    __shared__ int carry;
-    if (threadIdx.x == 0) carry = 0;
+__global__ void __launch_bounds__(1024) k_scan(const uint8_t* opt_skip, const uint8_t* eobs, int nmb, int intra,
+                                               int32_t* index, int32_t* offset, uint32_t* hdr) {
+    __shared__ int wsum[32], wsz[32];
+    __shared__ int carry, carry_sz;
+    if (threadIdx.x == 0) { carry = 0; carry_sz = 0; }
     __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int base = 0; base < nmb; base += 1024) {
         int i = base + threadIdx.x;
         int f = (i < nmb && (intra || !opt_skip[i])) ? 1 : 0;
-        int x = f;
+        int z = f ? (int)eobs[3 * i] + (int)eobs[3 * i + 1] + (int)eobs[3 * i + 2] + 3 : 0;
+        int x = f, y = z;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
+            int a = __shfl_up_sync(0xffffffffu, x, o), b = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) { x += a; y += b; }
         }
-        if (lane == 31) wsum[wid] = x;
+        if (lane == 31) { wsum[wid] = x; wsz[wid] = y; }
         __syncthreads();
         if (wid == 0) {
-            int s = wsum[lane];
+            int s1 = wsum[lane], s2 = wsz[lane];
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                int y = __shfl_up_sync(0xffffffffu, s, o);
-                if (lane >= o) s += y;
+                int a = __shfl_up_sync(0xffffffffu, s1, o), b = __shfl_up_sync(0xffffffffu, s2, o);
+                if (lane >= o) { s1 += a; s2 += b; }
             }
-            wsum[lane] = s;
+            wsum[lane] = s1;
+            wsz[lane] = s2;
         }
         __syncthreads();
-        int excl = carry + (wid > 0 ? wsum[wid - 1] : 0) + x - f;
-        if (i < nmb) index[i] = f ? excl : -1;
+        int ex = carry + (wid > 0 ? wsum[wid - 1] : 0) + x - f;
+        int ez = carry_sz + (wid > 0 ? wsz[wid - 1] : 0) + y - z;
+        if (i < nmb) { index[i] = f ? ex : -1; offset[i] = ez; }
         __syncthreads();
-        if (threadIdx.x == 0) carry += wsum[31];
+        if (threadIdx.x == 0) { carry += wsum[31]; carry_sz += wsz[31]; }
         __syncthreads();
     }
-    if (threadIdx.x == 0) *count = (uint32_t)carry;
+    if (threadIdx.x == 0) { hdr[0] = (uint32_t)carry; hdr[1] = (uint32_t)carry_sz; }
 }
-__global__ void k_pack(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coeffs, const uint8_t* eobs,
-                       const int32_t* index, int nmb, int intra, uint32_t* side, int16_t* packed, uint8_t* peobs) {
-    int m = blockIdx.x;
-    int k = index[m];
+__global__ void __launch_bounds__(128) k_pack(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coeffs,
+                                              const uint8_t* eobs, const int32_t* index, const int32_t* offset,
+                                              int intra, uint32_t* side, int16_t* packed, uint8_t* peobs) {
+    const int m = blockIdx.x;
+    const int k = index[m];
     if (threadIdx.x == 0) {
         uint32_t s = 0;
         if (!intra) {
@@ -1215,17 +1236,21 @@ __global__ void k_pack(const uint8_t* opt_skip, const MbOut* mb, const int16_t* 
         }
     }
     if (k < 0) return;
-    const uint4* src = (const uint4*)(coeffs + (size_t)m * 384);
-    uint4* dst = (uint4*)(packed + (size_t)k * 384);
-    for (int i = threadIdx.x; i < 48; i += blockDim.x) dst[i] = src[i];
+    const int n0 = eobs[3 * m] + 1, n1 = eobs[3 * m + 1] + 1, n2 = eobs[3 * m + 2] + 1;
+    const int16_t* src = coeffs + (size_t)m * 384;
+    int16_t* dst = packed + offset[m];
+    for (int i = threadIdx.x; i < n0 + n1 + n2; i += blockDim.x) {
+        int si = i < n0 ? i : (i < n0 + n1 ? 256 + (i - n0) : 320 + (i - n0 - n1));
+        dst[i] = src[si];
+    }
 }
 
 int launch_compact(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coeffs, const uint8_t* eobs, int nmb,
-                   int intra, uint32_t* side, int32_t* index, int16_t* packed, uint8_t* packed_eobs, uint32_t* count,
-                   void* stream) {
+                   int intra, int32_t* index, int32_t* offset, uint32_t* side, int16_t* packed,
+                   uint8_t* packed_eobs, uint32_t* hdr, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
-    k_scan<<<1, 1024, 0, st>>>(opt_skip, nmb, intra, index, count);
-    k_pack<<<nmb, 64, 0, st>>>(opt_skip, mb, coeffs, eobs, index, nmb, intra, side, packed, packed_eobs);
+    k_scan<<<1, 1024, 0, st>>>(opt_skip, eobs, nmb, intra, index, offset, hdr);
+    k_pack<<<nmb, 128, 0, st>>>(opt_skip, mb, coeffs, eobs, index, offset, intra, side, packed, packed_eobs);
     return (int)cudaGetLastError();
 }
 

@@ -109,7 +109,7 @@ EXPORTED_SYMBOLS = (
     "riv_finish", "riv_encoder_free", "riv_last_error", "riv_frame_count", "riv_last_recon", "riv_last_kernel_times",
     "riv_memwriter_new", "riv_memwriter_vtable", "riv_memwriter_size", "riv_memwriter_data", "riv_memwriter_free",
     "riv_stage_rgb_to_yuv", "riv_stage_deblock", "riv_stage_libm", "riv_libm_fixup_counts", "riv_dct_tables",
-    "riv_debug_frame_state", "riv_counters",
+    "riv_debug_frame_state", "riv_counters", "riv_host_times",
 )
 
 
@@ -145,6 +145,7 @@ def lib() -> C.CDLL:
     L.riv_dct_tables.argtypes = [C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     L.riv_debug_frame_state.argtypes = [P, C.c_int, P, C.c_size_t]
     L.riv_counters.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    L.riv_host_times.argtypes = [P, C.POINTER(C.c_double)]
     L._riv_typed = True
     return L
 
@@ -464,7 +465,10 @@ class Encoder:
         io = (C.c_uint64 * 2)()
         n = (C.c_uint64 * 2)()
         self._check(lib().riv_counters(self._h, us, io, n))
-        return {"stage_us_sum": list(us), "h2d_bytes": io[0], "d2h_bytes": io[1], "pframes": n[0], "launches": n[1]}
+        hm = (C.c_double * 6)()
+        self._check(lib().riv_host_times(self._h, hm))
+        return {"stage_us_sum": list(us), "h2d_bytes": io[0], "d2h_bytes": io[1], "pframes": n[0], "launches": n[1],
+                "host_ms": list(hm)}
 
     def debug_state(self, what: int) -> np.ndarray:
         """Device state of the most recent frame (see riv_debug_frame_state)."""
