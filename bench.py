@@ -319,6 +319,8 @@ def main():
         "gpu_launches": int(launches),
         "gpu_stage_us_per_pframe": dict(zip(names, [round(x, 2) for x in stage])),
         "gpu_pipeline_fps": 1e6 / stage[7] if stage[7] > 0 else None,
+        "host_ms_per_frame": dict(zip(["submit", "retire", "mv_coding", "dct_coding_sum", "write", "blocked"],
+                                      [round((b - a) / K, 3) for a, b in zip(c0["host_ms"], c1["host_ms"])])),
         "roofline": roofline_entry(stage[1]),
         "cpu_baseline": cpu,
         "clocks": r["clocks"],

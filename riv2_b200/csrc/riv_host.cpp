@@ -310,7 +310,7 @@ struct riv_encoder {
     cudaStream_t S = nullptr, C = nullptr;
     // device state
     DevBuf cur, ref[2], pred, mbout, coded[2], rec, varsum, lnv, qs, coeffs, opt_skip, fmask, eobs, status;
-    DevBuf cindex, coffset;
+    DevBuf cindex, coffset, sadtab, dside, dpacked, dpeobs, dhdr;
     DevBuf mvbits, logfix, expfix, ytab, ctab;
     int ref_cur = 0, coded_cur = 0;
     bool has_ref = false, has_prev_mvs = false;
@@ -428,16 +428,22 @@ static void setup_device(riv_encoder* e) {
     size_t rgb_bytes = (size_t)c.display_width * c.display_height * 3;
     for (auto& s : e->slots) {
         s.rgb.alloc(rgb_bytes);
-        s.side.alloc((size_t)N * 4);
+        s.side.alloc((size_t)N * 4 + 16);
         s.hdr.alloc(16);
-        s.packed.alloc((size_t)N * 384 * 2);
-        s.peobs.alloc((size_t)N * 3);
+        s.packed.alloc((size_t)N * 384 * 2 + 16);
+        s.peobs.alloc((size_t)N * 3 + 16);
         CK(cudaEventCreateWithFlags(&s.ev_h2d, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&s.ev_gpu, cudaEventDisableTiming));
         for (int k = 0; k < EV_N; k++) CK(cudaEventCreate(&s.ev_k[k]));
     }
     e->cindex.alloc((size_t)N * 4);
     e->coffset.alloc((size_t)N * 4);
+    e->dside.alloc((size_t)N * 4 + 16);
+    e->dpacked.alloc((size_t)N * 384 * 2 + 16);
+    e->dpeobs.alloc((size_t)N * 3 + 16);
+    e->dhdr.alloc(16);
+    if (search_use_table(c.search_range))
+        e->sadtab.alloc((size_t)N * sad_table_stride(c.search_range) * sizeof(uint16_t));
     unsigned nt = c.entropy_threads;
     if (nt == 0) nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency() > 1 ? std::thread::hardware_concurrency() - 1 : 1u));
     e->pool.reset(new ThreadPool(nt));
@@ -454,8 +460,8 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
     CK(cudaEventRecord(s.ev_k[EV_START], S));
     // kernels per frame: rgb->yuv, (search, predict, 3 x aq), residual, deblock (2 per plane), scan + pack
     const int nplanes_db = 3 * 2;
-    e->launches += (src == 2 ? 0 : 1) + (j.type == 2 ? 5 : 0) + 1 +
-                   ((j.type == 2 ? e->inter_level : e->intra_level) > 0 ? nplanes_db : 0) + 2;
+    e->launches += (src == 2 ? 0 : 1) + (j.type == 2 ? 5 + (search_use_table(c.search_range) ? 1 : 0) : 0) + 1 +
+                   ((j.type == 2 ? e->inter_level : e->intra_level) > 0 ? nplanes_db : 0) + 3;
     if (src == 0) e->h2d_bytes += (uint64_t)c.display_width * c.display_height * 3;
     if (src == 2) e->h2d_bytes += e->yuv_bytes;
     if (src == 0) {
@@ -499,7 +505,8 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         if (e->intra_level > 0) CK(launch_deblock(recon, W, H, e->intra_E, e->intra_I, e->intra_H, nullptr, S));
         CK(cudaEventRecord(s.ev_k[EV_DEBLOCK], S));
         CK(launch_compact(e->opt_skip.as<uint8_t>(), e->mbout.as<MbOut>(), e->coeffs.as<int16_t>(), e->eobs.as<uint8_t>(), N, 1,
-                          e->cindex.as<int32_t>(), e->coffset.as<int32_t>(), s.side.dev<uint32_t>(),
+                          e->cindex.as<int32_t>(), e->coffset.as<int32_t>(), e->dside.as<uint32_t>(),
+                          e->dpacked.as<int16_t>(), e->dpeobs.as<uint8_t>(), e->dhdr.as<uint32_t>(), s.side.dev<uint32_t>(),
                           s.packed.dev<int16_t>(), s.peobs.dev<uint8_t>(), s.hdr.dev<uint32_t>(), S));
         e->has_prev_mvs = false;
     } else {
@@ -531,6 +538,13 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         sp.out = e->mbout.as<MbOut>();
         sp.status = e->status.as<unsigned>();
         sp.spin_limit = 1ll << 22;  // ~ a few seconds, far above any legitimate wait
+        sp.tab = nullptr;
+        sp.tstride = 0;
+        if (search_use_table(c.search_range)) {
+            sp.tstride = sad_table_stride(c.search_range);
+            sp.tab = e->sadtab.as<uint16_t>();
+            CK(launch_sad_table(sp.ref_y, sp.cur_y, W, H, c.search_range, e->sadtab.as<uint16_t>(), sp.tstride, S));
+        }
         CK(launch_search(sp, e->search_grid, S));
         CK(cudaEventRecord(s.ev_k[EV_SEARCH], S));
         // coded MVs of this frame become next frame's temporal predictors
@@ -550,7 +564,8 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         if (e->inter_level > 0) CK(launch_deblock(recon, W, H, e->inter_E, e->inter_I, e->inter_H, e->fmask.as<uint8_t>(), S));
         CK(cudaEventRecord(s.ev_k[EV_DEBLOCK], S));
         CK(launch_compact(e->opt_skip.as<uint8_t>(), e->mbout.as<MbOut>(), e->coeffs.as<int16_t>(), e->eobs.as<uint8_t>(), N, 0,
-                          e->cindex.as<int32_t>(), e->coffset.as<int32_t>(), s.side.dev<uint32_t>(),
+                          e->cindex.as<int32_t>(), e->coffset.as<int32_t>(), e->dside.as<uint32_t>(),
+                          e->dpacked.as<int16_t>(), e->dpeobs.as<uint8_t>(), e->dhdr.as<uint32_t>(), s.side.dev<uint32_t>(),
                           s.packed.dev<int16_t>(), s.peobs.dev<uint8_t>(), s.hdr.dev<uint32_t>(), S));
         e->coded_cur = cn;
         e->has_prev_mvs = true;
@@ -914,7 +929,8 @@ void riv_encoder_free(riv_encoder* e) {
     }
     DevBuf* bufs[] = {&e->cur, &e->ref[0], &e->ref[1], &e->pred, &e->mbout, &e->coded[0], &e->coded[1], &e->rec,
                       &e->varsum, &e->lnv, &e->qs, &e->coeffs, &e->opt_skip, &e->fmask, &e->eobs, &e->status,
-                      &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset};
+                      &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset, &e->sadtab,
+                      &e->dside, &e->dpacked, &e->dpeobs, &e->dhdr};
     for (DevBuf* b : bufs) b->release();
     if (e->S) cudaStreamDestroy(e->S);
     if (e->C) cudaStreamDestroy(e->C);

@@ -39,6 +39,8 @@ struct SearchParams {
     // RDO (enc/rdo.rs)
     double rdo_lambda, rdo_skip_bits, rdo_keep_bits, rdo_icpt, rdo_slope, rdo_ret, rdo_guard;
     int rdo_allow;
+    const uint16_t* tab;  // exhaustive integer-SAD table (when search_use_table), tstride entries per MB
+    int tstride;
     MbRec* rec;
     unsigned tag;
     MbOut* out;
@@ -70,6 +72,10 @@ enum StatusBits : unsigned {
 // Launchers (riv_kernels.cu).  All are asynchronous on `stream`.
 int launch_rgb_to_yuv(const uint8_t* rgb, int dw, int dh, uint8_t* yuv, int W, int H, void* stream);
 int launch_search(const SearchParams& p, int grid, void* stream);
+bool search_use_table(int sr);
+int sad_table_stride(int sr);
+int launch_sad_table(const uint8_t* ref, const uint8_t* cur, int W, int H, int sr, uint16_t* tab, int tstride,
+                     void* stream);
 int search_max_grid(int sr, int W, int* grid_out);
 size_t search_smem_bytes(int sr);
 int launch_predict(const uint8_t* ref, const MbOut* mb, uint8_t* pred, uint2* varsum, int W, int H, void* stream);
@@ -78,8 +84,8 @@ int launch_aq(const uint2* varsum, int n, float base, const uint32_t* logfix, in
 int launch_residual(const ResidualParams& p, int nmb, void* stream);
 int launch_deblock(uint8_t* yuv, int W, int H, int E, int I, int Hev, const uint8_t* mask, void* stream);
 int launch_compact(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coeffs, const uint8_t* eobs, int nmb,
-                   int intra, int32_t* index, int32_t* offset, uint32_t* side, int16_t* packed,
-                   uint8_t* packed_eobs, uint32_t* hdr, void* stream);
+                   int intra, int32_t* index, int32_t* offset, uint32_t* dside, int16_t* dpacked, uint8_t* dpeobs,
+                   uint32_t* dhdr, uint32_t* hside, int16_t* hpacked, uint8_t* hpeobs, uint32_t* hhdr, void* stream);
 // libm device helpers exposed for the exhaustive check
 int launch_libm_eval(int which, const float* in, float* out, size_t n, const uint32_t* fix, int nfix, void* stream);
 

@@ -205,12 +205,104 @@ __device__ __forceinline__ void fill_chunk(uint8_t* band, int BWB, int WS, int c
     }
 }
 
-template <bool BAND>
+
+// ---------------------------------------------------------------------------------
+// K3: exhaustive integer-SAD table of every MB over the whole search range, computed by
+// the full GPU before the wavefront so its integer rounds become shared-memory lookups.
+// tab[mb][(dy+sr)*(2sr+1) + dx+sr] = SAD(dx,dy) with the reference's semantics
+// (per-4x4 sub-block clamped reference origin at frame edges,
+// enc/motion/satd_scalar.rs:26-97; the plain 16x16 SAD elsewhere).  Values <= 65280.
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_sad_table(const uint8_t* __restrict__ ref, const uint8_t* __restrict__ cur,
+                                                   int W, int H, int BW, int sr, uint16_t* __restrict__ tab,
+                                                   int tstride) {
+    extern __shared__ __align__(16) uint8_t sm[];
+    const int WT = 16 + 2 * sr;                 // window side
+    const int WTS = (WT + 3 + 15) & ~15;        // row stride (+ slack for unaligned word reads)
+    uint8_t* win = sm;
+    uint32_t* cw = (uint32_t*)(sm + WT * WTS + 16);  // 64 words of the current block
+    const int mb = blockIdx.x;
+    const int bx = mb % BW, by = mb / BW;
+    const int x0 = bx * 16, y0 = by * 16;
+    const int wx0 = x0 - sr, wy0 = y0 - sr;
+    for (int i = threadIdx.x; i < WT * WT; i += blockDim.x) {
+        int r = i / WT, c = i - r * WT;
+        int gy = min(max(wy0 + r, 0), H - 1), gx = min(max(wx0 + c, 0), W - 1);
+        win[r * WTS + c] = ref[(size_t)gy * W + gx];
+    }
+    if (threadIdx.x < 64) {
+        int r = threadIdx.x >> 2, g = threadIdx.x & 3;
+        cw[threadIdx.x] = *(const uint32_t*)(cur + (size_t)(y0 + r) * W + x0 + 4 * g);
+    }
+    __syncthreads();
+    const int side = 2 * sr + 1, P = side * side;
+    const bool interior = x0 - sr >= 0 && y0 - sr >= 0 && x0 + 15 + sr <= W - 1 && y0 + 15 + sr <= H - 1;
+    uint16_t* out = tab + (size_t)mb * tstride;
+    for (int pidx = threadIdx.x; pidx < P; pidx += blockDim.x) {
+        const int dy = pidx / side - sr, dx = pidx % side - sr;
+        unsigned s = 0;
+        if (interior) {
+#pragma unroll 4
+            for (int r = 0; r < 16; r++) {
+                const uint8_t* row = win + (r + dy + sr) * WTS + dx + sr;
+#pragma unroll
+                for (int g = 0; g < 4; g++) s += __vsadu4(cw[r * 4 + g], lds_u32(row + 4 * g));
+            }
+        } else {
+            for (int r = 0; r < 16; r++) {
+                int ry = min(max(y0 + (r & ~3) + dy, 0), H - 4) + (r & 3) - wy0;
+                const uint8_t* row = win + ry * WTS;
+#pragma unroll
+                for (int g = 0; g < 4; g++) {
+                    int rx = min(max(x0 + 4 * g + dx, 0), W - 4) - wx0;
+                    s += __vsadu4(cw[r * 4 + g], lds_u32(row + rx));
+                }
+            }
+        }
+        out[pidx] = (uint16_t)s;
+    }
+}
+size_t sad_table_smem(int sr) {
+    int WT = 16 + 2 * sr, WTS = (WT + 3 + 15) & ~15;
+    return (size_t)WT * WTS + 16 + 256;
+}
+int launch_sad_table(const uint8_t* ref, const uint8_t* cur, int W, int H, int sr, uint16_t* tab, int tstride,
+                     void* stream) {
+    int BW = W / 16, n = BW * (H / 16);
+    size_t sm = sad_table_smem(sr);
+    if (sm > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_sad_table, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return (int)e;
+    }
+    k_sad_table<<<n, 128, sm, (cudaStream_t)stream>>>(ref, cur, W, H, BW, sr, tab, tstride);
+    return (int)cudaGetLastError();
+}
+
+// Warp argmin over lanes 0..7 of (total, lane) with the lowest lane winning ties; lanes
+// with valid == false do not compete.  Returns the winning lane (or -1).
+__device__ __forceinline__ int argmin8(long long total, bool valid, long long& best_total) {
+    long long t = valid ? total : LLONG_MAX;
+    int k = valid ? (int)(threadIdx.x & 31) : 64;
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) {
+        long long t2 = __shfl_xor_sync(0xffffffffu, t, o);
+        int k2 = __shfl_xor_sync(0xffffffffu, k, o);
+        if (t2 < t || (t2 == t && k2 < k)) { t = t2; k = k2; }
+    }
+    t = __shfl_sync(0xffffffffu, t, 0);
+    k = __shfl_sync(0xffffffffu, k, 0);
+    best_total = t;
+    return k < 64 ? k : -1;
+}
+
+template <bool BAND, bool TABLE>
 __global__ void __launch_bounds__(32) k_search(SearchParams p) {
     extern __shared__ __align__(16) uint8_t smem[];
     double* bits = (double*)smem;                 // 256 doubles
     uint8_t* curbuf = smem + 256 * sizeof(double);  // 2 x 256 bytes
-    uint8_t* refmem = curbuf + 512;               // band or window (+16 bytes slack)
+    uint16_t* tabbuf = (uint16_t*)(curbuf + 512);   // TABLE: 2 x tstride entries
+    uint8_t* refmem = curbuf + 512 + (TABLE ? 4 * p.tstride : 0);  // band or window (+16 bytes slack)
+    const int side = 2 * p.sr + 1;
     const int lane = threadIdx.x;
     const int sr = p.sr;
     const int WS = 18 + 2 * sr;
@@ -234,6 +326,9 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
             c_done = c_hi(0);
         }
         if (lane < 16) cp_async16(curbuf + lane * 16, p.cur_y + (size_t)(y0 + lane) * p.W);
+        if (TABLE)
+            for (int i = lane; i < p.tstride / 8; i += 32)
+                cp_async16(tabbuf + i * 8, p.tab + (size_t)(r * p.BW) * p.tstride + i * 8);
         cp_async_commit();
 
         MvT L_raw{0, 0, 0, 0}, L_cod{0, 0, 0, 0};
@@ -251,6 +346,10 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                 }
                 if (lane < 16)
                     cp_async16(curbuf + ((bx + 1) & 1) * 256 + lane * 16, p.cur_y + (size_t)(y0 + lane) * p.W + x0 + 16);
+                if (TABLE)
+                    for (int i = lane; i < p.tstride / 8; i += 32)
+                        cp_async16(tabbuf + ((bx + 1) & 1) * p.tstride + i * 8,
+                                   p.tab + (size_t)(idx + 1) * p.tstride + i * 8);
             }
             cp_async_commit();
             cp_async_wait1();
@@ -367,102 +466,162 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                 for (int j = 0; j < i; j++) ok = ok && !(SV[j + 1] && PX[j] == PX[i] && PY[j] == PY[i]);
                 SV[i + 1] = ok;
             }
-            // ---- zero SAD and the seed round; lane k evaluates the MV cost of slot k
-            long long my_cost = 0;
-            {
+            const uint16_t* tb = tabbuf + (bx & 1) * p.tstride;
+            int sdx = 0, sdy = 0;
+            if (TABLE) {
+                // ---- table-driven integer search: lane k holds candidate k of a round; the
+                // in-order strict-'<' scan of the reference equals an argmin with the lowest
+                // index winning ties.
                 int kx = 0, ky = 0;
                 bool kv = lane == 0;
 #pragma unroll
                 for (int i = 0; i < 5; i++)
                     if (lane == i + 1) { kx = PX[i]; ky = PY[i]; kv = SV[i + 1]; }
-                if (kv) my_cost = mv_cost(kx, ky, cc, p, bits);
-            }
-            unsigned part[6];
-            part[0] = sad_int_part(view, x0, y0, p.W, p.H, 0, 0, yy, xoff, c0, c1);
-#pragma unroll
-            for (int i = 0; i < 5; i++)
-                part[i + 1] = SV[i + 1] ? sad_int_part(view, x0, y0, p.W, p.H, PX[i], PY[i], yy, xoff, c0, c1) : 0u;
-            long long sads[6];
-#pragma unroll
-            for (int i = 0; i < 6; i++) sads[i] = (long long)warp_sum(part[i]);
-            long long zero_sad = sads[0];
-            int sdx = 0, sdy = 0;
-            long long sc_cost = __shfl_sync(0xffffffffu, my_cost, 0);
-            long long scost = zero_sad + sc_cost;
-            bool skip_int = p.zthr > 0 && zero_sad <= p.zthr;
-            if (!skip_int) {
-#pragma unroll
-                for (int i = 0; i < 5; i++) {
-                    long long ci = __shfl_sync(0xffffffffu, my_cost, i + 1);
-                    if (!SV[i + 1]) continue;
-                    long long t = sads[i + 1] + ci;
-                    if (t < scost) { scost = t; sdx = PX[i]; sdy = PY[i]; sc_cost = ci; }
+                long long ksad = kv ? (long long)tb[(ky + sr) * side + kx + sr] : 0;
+                long long kcost = kv ? mv_cost(kx, ky, cc, p, bits) : 0;
+                long long zero_sad = (long long)tb[sr * side + sr];
+                long long scost;
+                int w = argmin8(ksad + kcost, kv && lane < 6, scost);
+                bool skip_int = p.zthr > 0 && zero_sad <= p.zthr;
+                if (skip_int) {
+                    scost = zero_sad + __shfl_sync(0xffffffffu, kcost, 0);
+                } else {
+                    sdx = __shfl_sync(0xffffffffu, kx, w);
+                    sdy = __shfl_sync(0xffffffffu, ky, w);
+                    long long wsad = __shfl_sync(0xffffffffu, ksad, w);
+                    if (p.pthr > 0 && wsad <= p.pthr) skip_int = true;
                 }
-                long long cur_sad = scost - sc_cost;
-                if (p.pthr > 0 && cur_sad <= p.pthr) skip_int = true;
-            }
-            if (!skip_int) {
-                // large hexagon (enc/motion/scalar.rs:694-729)
-                const int HX[6] = {2, 1, -1, -2, -1, 1}, HY[6] = {0, 2, 2, 0, -2, -2};
-                // HX/HY of lane k (k < 6) without a lane-indexed array
-                const int hxl = (int)(int8_t)(0x01FFFEFF0102ull >> (8 * min(lane, 5)));
-                const int hyl = (int)(int8_t)(0xFEFE00020200ull >> (8 * min(lane, 5)));
-                int iter = 0;
-                for (;;) {
+                if (!skip_int) {
+                    const int hxl = (int)(int8_t)(0x01FFFEFF0102ull >> (8 * min(lane, 5)));
+                    const int hyl = (int)(int8_t)(0xFEFE00020200ull >> (8 * min(lane, 5)));
+                    int iter = 0;
+                    for (;;) {  // large hexagon (enc/motion/scalar.rs:694-729)
+                        int dx = sdx + hxl, dy = sdy + hyl;
+                        bool v = lane < 6 && abs(dx) <= sr && abs(dy) <= sr;
+                        long long t = v ? (long long)tb[(dy + sr) * side + dx + sr] + mv_cost(dx, dy, cc, p, bits) : 0;
+                        long long bt;
+                        int wk = argmin8(t, v, bt);
+                        if (wk < 0 || bt >= scost) break;
+                        scost = bt;
+                        sdx = __shfl_sync(0xffffffffu, dx, wk);
+                        sdy = __shfl_sync(0xffffffffu, dy, wk);
+                        if (++iter > 4096) {  // cost strictly decreases, so this is never reached
+                            if (lane == 0) atomicOr(p.status, ST_HEX_CAP);
+                            break;
+                        }
+                    }
+                    {  // small diamond (enc/motion/scalar.rs:731-756)
+                        const int dxl = (int)(int8_t)(0x0000FF01u >> (8 * min(lane, 3)));
+                        const int dyl = (int)(int8_t)(0xFF010000u >> (8 * min(lane, 3)));
+                        int dx = sdx + dxl, dy = sdy + dyl;
+                        bool v = lane < 4 && abs(dx) <= sr && abs(dy) <= sr;
+                        long long t = v ? (long long)tb[(dy + sr) * side + dx + sr] + mv_cost(dx, dy, cc, p, bits) : 0;
+                        long long bt;
+                        int wk = argmin8(t, v, bt);
+                        if (wk >= 0 && bt < scost) {
+                            scost = bt;
+                            sdx = __shfl_sync(0xffffffffu, dx, wk);
+                            sdy = __shfl_sync(0xffffffffu, dy, wk);
+                        }
+                    }
+                }
+            } else {
+                // ---- zero SAD and the seed round; lane k evaluates the MV cost of slot k
+                long long my_cost = 0;
+                {
+                    int kx = 0, ky = 0;
+                    bool kv = lane == 0;
+    #pragma unroll
+                    for (int i = 0; i < 5; i++)
+                        if (lane == i + 1) { kx = PX[i]; ky = PY[i]; kv = SV[i + 1]; }
+                    if (kv) my_cost = mv_cost(kx, ky, cc, p, bits);
+                }
+                unsigned part[6];
+                part[0] = sad_int_part(view, x0, y0, p.W, p.H, 0, 0, yy, xoff, c0, c1);
+    #pragma unroll
+                for (int i = 0; i < 5; i++)
+                    part[i + 1] = SV[i + 1] ? sad_int_part(view, x0, y0, p.W, p.H, PX[i], PY[i], yy, xoff, c0, c1) : 0u;
+                long long sads[6];
+    #pragma unroll
+                for (int i = 0; i < 6; i++) sads[i] = (long long)warp_sum(part[i]);
+                long long zero_sad = sads[0];
+                long long sc_cost = __shfl_sync(0xffffffffu, my_cost, 0);
+                long long scost = zero_sad + sc_cost;
+                bool skip_int = p.zthr > 0 && zero_sad <= p.zthr;
+                if (!skip_int) {
+    #pragma unroll
+                    for (int i = 0; i < 5; i++) {
+                        long long ci = __shfl_sync(0xffffffffu, my_cost, i + 1);
+                        if (!SV[i + 1]) continue;
+                        long long t = sads[i + 1] + ci;
+                        if (t < scost) { scost = t; sdx = PX[i]; sdy = PY[i]; sc_cost = ci; }
+                    }
+                    long long cur_sad = scost - sc_cost;
+                    if (p.pthr > 0 && cur_sad <= p.pthr) skip_int = true;
+                }
+                if (!skip_int) {
+                    // large hexagon (enc/motion/scalar.rs:694-729)
+                    const int HX[6] = {2, 1, -1, -2, -1, 1}, HY[6] = {0, 2, 2, 0, -2, -2};
+                    // HX/HY of lane k (k < 6) without a lane-indexed array
+                    const int hxl = (int)(int8_t)(0x01FFFEFF0102ull >> (8 * min(lane, 5)));
+                    const int hyl = (int)(int8_t)(0xFEFE00020200ull >> (8 * min(lane, 5)));
+                    int iter = 0;
+                    for (;;) {
+                        int cx = sdx, cy = sdy;
+                        long long lc = 0;
+                        if (lane < 6) {
+                            int dx = cx + hxl, dy = cy + hyl;
+                            if (abs(dx) <= sr && abs(dy) <= sr) lc = mv_cost(dx, dy, cc, p, bits);
+                        }
+                        unsigned hp[6];
+    #pragma unroll
+                        for (int k = 0; k < 6; k++) {
+                            int dx = cx + HX[k], dy = cy + HY[k];
+                            hp[k] = (abs(dx) <= sr && abs(dy) <= sr)
+                                        ? sad_int_part(view, x0, y0, p.W, p.H, dx, dy, yy, xoff, c0, c1) : 0u;
+                        }
+                        bool improved = false;
+    #pragma unroll
+                        for (int k = 0; k < 6; k++) {
+                            long long s = (long long)warp_sum(hp[k]);
+                            long long ck = __shfl_sync(0xffffffffu, lc, k);
+                            int dx = cx + HX[k], dy = cy + HY[k];
+                            if (abs(dx) > sr || abs(dy) > sr) continue;
+                            long long t = s + ck;
+                            if (t < scost) { scost = t; sdx = dx; sdy = dy; improved = true; }
+                        }
+                        if (!improved) break;
+                        if (++iter > 4096) {  // cost strictly decreases, so this is never reached
+                            if (lane == 0) atomicOr(p.status, ST_HEX_CAP);
+                            break;
+                        }
+                    }
+                    // small diamond (enc/motion/scalar.rs:731-756)
+                    const int DX[4] = {1, -1, 0, 0}, DY[4] = {0, 0, 1, -1};
+                    const int dxl = (int)(int8_t)(0x0000FF01u >> (8 * min(lane, 3)));
+                    const int dyl = (int)(int8_t)(0xFF010000u >> (8 * min(lane, 3)));
                     int cx = sdx, cy = sdy;
                     long long lc = 0;
-                    if (lane < 6) {
-                        int dx = cx + hxl, dy = cy + hyl;
+                    if (lane < 4) {
+                        int dx = cx + dxl, dy = cy + dyl;
                         if (abs(dx) <= sr && abs(dy) <= sr) lc = mv_cost(dx, dy, cc, p, bits);
                     }
-                    unsigned hp[6];
-#pragma unroll
-                    for (int k = 0; k < 6; k++) {
-                        int dx = cx + HX[k], dy = cy + HY[k];
-                        hp[k] = (abs(dx) <= sr && abs(dy) <= sr)
+                    unsigned dp[4];
+    #pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        int dx = cx + DX[k], dy = cy + DY[k];
+                        dp[k] = (abs(dx) <= sr && abs(dy) <= sr)
                                     ? sad_int_part(view, x0, y0, p.W, p.H, dx, dy, yy, xoff, c0, c1) : 0u;
                     }
-                    bool improved = false;
-#pragma unroll
-                    for (int k = 0; k < 6; k++) {
-                        long long s = (long long)warp_sum(hp[k]);
+    #pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        long long s = (long long)warp_sum(dp[k]);
                         long long ck = __shfl_sync(0xffffffffu, lc, k);
-                        int dx = cx + HX[k], dy = cy + HY[k];
+                        int dx = cx + DX[k], dy = cy + DY[k];
                         if (abs(dx) > sr || abs(dy) > sr) continue;
                         long long t = s + ck;
-                        if (t < scost) { scost = t; sdx = dx; sdy = dy; improved = true; }
+                        if (t < scost) { scost = t; sdx = dx; sdy = dy; }
                     }
-                    if (!improved) break;
-                    if (++iter > 4096) {  // cost strictly decreases, so this is never reached
-                        if (lane == 0) atomicOr(p.status, ST_HEX_CAP);
-                        break;
-                    }
-                }
-                // small diamond (enc/motion/scalar.rs:731-756)
-                const int DX[4] = {1, -1, 0, 0}, DY[4] = {0, 0, 1, -1};
-                const int dxl = (int)(int8_t)(0x0000FF01u >> (8 * min(lane, 3)));
-                const int dyl = (int)(int8_t)(0xFF010000u >> (8 * min(lane, 3)));
-                int cx = sdx, cy = sdy;
-                long long lc = 0;
-                if (lane < 4) {
-                    int dx = cx + dxl, dy = cy + dyl;
-                    if (abs(dx) <= sr && abs(dy) <= sr) lc = mv_cost(dx, dy, cc, p, bits);
-                }
-                unsigned dp[4];
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    int dx = cx + DX[k], dy = cy + DY[k];
-                    dp[k] = (abs(dx) <= sr && abs(dy) <= sr)
-                                ? sad_int_part(view, x0, y0, p.W, p.H, dx, dy, yy, xoff, c0, c1) : 0u;
-                }
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    long long s = (long long)warp_sum(dp[k]);
-                    long long ck = __shfl_sync(0xffffffffu, lc, k);
-                    int dx = cx + DX[k], dy = cy + DY[k];
-                    if (abs(dx) > sr || abs(dy) > sr) continue;
-                    long long t = s + ck;
-                    if (t < scost) { scost = t; sdx = dx; sdy = dy; }
                 }
             }
             // ---- half-pel refinement (enc/motion/scalar.rs:759-839): nine floor-averaged
@@ -621,27 +780,35 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
     }
 }
 
-// Shared memory of the search kernel; BAND when the whole MB-row band fits.
-static size_t search_smem(int sr, int W, bool band) {
+// Shared memory of the search kernel; BAND when the whole MB-row band fits, TABLE when
+// the exhaustive SAD table is used (search ranges up to 15).
+int sad_table_stride(int sr) { return ((2 * sr + 1) * (2 * sr + 1) + 7) & ~7; }
+bool search_use_table(int sr) { return sr <= 15; }
+static size_t search_smem(int sr, int W, bool band, bool table) {
     size_t ws = 18 + 2 * (size_t)sr;
     size_t margin = ((size_t)sr + 1 + 15) & ~(size_t)15;
     size_t ref = band ? ws * ((size_t)W + 2 * margin) : ws * ws;
-    return 256 * sizeof(double) + 512 + ref + 16;
+    return 256 * sizeof(double) + 512 + (table ? 4 * (size_t)sad_table_stride(sr) : 0) + ref + 16;
 }
 static const size_t SEARCH_SMEM_MAX = 200 * 1024;
-static bool search_use_band(int sr, int W) { return search_smem(sr, W, true) <= SEARCH_SMEM_MAX; }
+static bool search_use_band(int sr, int W) {
+    return search_smem(sr, W, true, search_use_table(sr)) <= SEARCH_SMEM_MAX;
+}
+static const void* search_fn(bool band, bool table) {
+    if (band) return table ? (const void*)k_search<true, true> : (const void*)k_search<true, false>;
+    return table ? (const void*)k_search<false, true> : (const void*)k_search<false, false>;
+}
 
-size_t search_smem_bytes(int sr) { return search_smem(sr, 0, false); }
+size_t search_smem_bytes(int sr) { return search_smem(sr, 0, false, search_use_table(sr)); }
 
 int search_max_grid(int sr, int W, int* grid_out) {
-    bool band = search_use_band(sr, W);
-    size_t sm = search_smem(sr, W, band);
-    const void* fn = band ? (const void*)k_search<true> : (const void*)k_search<false>;
+    bool band = search_use_band(sr, W), table = search_use_table(sr);
+    size_t sm = search_smem(sr, W, band, table);
+    const void* fn = search_fn(band, table);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return (int)e;
     int per_sm = 0;
-    e = band ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search<true>, 32, sm)
-             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search<false>, 32, sm);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32, sm);
     if (e != cudaSuccess) return (int)e;
     int dev = 0, nsm = 0;
     cudaGetDevice(&dev);
@@ -651,14 +818,14 @@ int search_max_grid(int sr, int W, int* grid_out) {
 }
 
 int launch_search(const SearchParams& p, int grid, void* stream) {
-    bool band = search_use_band(p.sr, p.W);
-    size_t sm = search_smem(p.sr, p.W, band);
+    bool band = search_use_band(p.sr, p.W), table = search_use_table(p.sr);
+    size_t sm = search_smem(p.sr, p.W, band, table);
     SearchParams q = p;
     void* args[] = {&q};
     // Cooperative launch: every CTA of the grid is co-resident, so the row-to-row waits
     // can always make progress.
-    const void* fn = band ? (const void*)k_search<true> : (const void*)k_search<false>;
-    cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(32), args, sm, (cudaStream_t)stream);
+    cudaError_t e = cudaLaunchCooperativeKernel(search_fn(band, table), dim3(grid), dim3(32), args, sm,
+                                                (cudaStream_t)stream);
     return (int)e;
 }
 
@@ -1245,12 +1412,30 @@ __global__ void __launch_bounds__(128) k_pack(const uint8_t* opt_skip, const MbO
     }
 }
 
+// Copies the packed side info, EOBs and coefficients (sizes read from the device header)
+// into mapped host memory with full 16-byte stores.
+__global__ void k_copy_out(const uint32_t* __restrict__ dside, const uint8_t* __restrict__ dpeobs,
+                           const int16_t* __restrict__ dpacked, const uint32_t* __restrict__ dhdr, int nmb,
+                           uint32_t* hside, uint8_t* hpeobs, int16_t* hpacked, uint32_t* hhdr) {
+    const uint32_t count = dhdr[0], total = dhdr[1];
+    const size_t n_side = ((size_t)nmb * 4 + 15) / 16, n_eob = ((size_t)count * 3 + 15) / 16,
+                 n_coef = ((size_t)total * 2 + 15) / 16;
+    const size_t n = n_side + n_eob + n_coef;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        if (i < n_side) ((uint4*)hside)[i] = ((const uint4*)dside)[i];
+        else if (i < n_side + n_eob) ((uint4*)hpeobs)[i - n_side] = ((const uint4*)dpeobs)[i - n_side];
+        else ((uint4*)hpacked)[i - n_side - n_eob] = ((const uint4*)dpacked)[i - n_side - n_eob];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) { hhdr[0] = count; hhdr[1] = total; }
+}
+
 int launch_compact(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coeffs, const uint8_t* eobs, int nmb,
-                   int intra, int32_t* index, int32_t* offset, uint32_t* side, int16_t* packed,
-                   uint8_t* packed_eobs, uint32_t* hdr, void* stream) {
+                   int intra, int32_t* index, int32_t* offset, uint32_t* dside, int16_t* dpacked, uint8_t* dpeobs,
+                   uint32_t* dhdr, uint32_t* hside, int16_t* hpacked, uint8_t* hpeobs, uint32_t* hhdr, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
-    k_scan<<<1, 1024, 0, st>>>(opt_skip, eobs, nmb, intra, index, offset, hdr);
-    k_pack<<<nmb, 128, 0, st>>>(opt_skip, mb, coeffs, eobs, index, offset, intra, side, packed, packed_eobs);
+    k_scan<<<1, 1024, 0, st>>>(opt_skip, eobs, nmb, intra, index, offset, dhdr);
+    k_pack<<<nmb, 128, 0, st>>>(opt_skip, mb, coeffs, eobs, index, offset, intra, dside, dpacked, dpeobs);
+    k_copy_out<<<296, 256, 0, st>>>(dside, dpeobs, dpacked, dhdr, nmb, hside, hpeobs, hpacked, hhdr);
     return (int)cudaGetLastError();
 }
 
