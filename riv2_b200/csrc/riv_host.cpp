@@ -276,12 +276,15 @@ struct MappedBuf {
     T* dev() const { return (T*)d; }
 };
 
-enum { EV_START, EV_YUV, EV_SEARCH, EV_PRED, EV_AQ, EV_RES, EV_DEBLOCK, EV_COMPACT, EV_N };
+enum { EV_START, EV_YUV, EV_TABLE, EV_SEARCH, EV_PRED, EV_AQ, EV_RES, EV_DEBLOCK, EV_COMPACT, EV_N };
+static const int NSTAGE = EV_N - 1;  // + total
 
 struct Slot {
-    DevBuf rgb;
-    MappedBuf side, hdr, packed, peobs;  // hdr: coded MBs, coefficients, device status
-    cudaEvent_t ev_h2d = nullptr, ev_gpu = nullptr;
+    DevBuf rgb, dside, dpacked, dpeobs;        // compacted frame output on the device
+    HostBuf side, packed, peobs;               // pinned copies (DMA on the copy stream)
+    MappedBuf hdr;                             // coded MBs, coefficients, device status
+    size_t prefetched = 0;                     // coefficient bytes included in the first copy
+    cudaEvent_t ev_h2d = nullptr, ev_gpu = nullptr, ev_d2h = nullptr;
     cudaEvent_t ev_k[EV_N] = {};
 };
 
@@ -294,7 +297,7 @@ struct Job {
     std::vector<uint8_t> res_bytes, mv_bytes;
     int8_t bias[2] = {0, 0};
     riv_frame_stats stats{};
-    float times[8] = {0};
+    float times[NSTAGE + 1] = {0};
 };
 
 }  // namespace
@@ -310,7 +313,7 @@ struct riv_encoder {
     cudaStream_t S = nullptr, C = nullptr;
     // device state
     DevBuf cur, ref[2], pred, mbout, coded[2], rec, varsum, lnv, qs, coeffs, opt_skip, fmask, eobs, status;
-    DevBuf cindex, coffset, sadtab, dside, dpacked, dpeobs, dhdr;
+    DevBuf cindex, coffset, sadtab;
     DevBuf mvbits, logfix, expfix, ytab, ctab;
     int ref_cur = 0, coded_cur = 0;
     bool has_ref = false, has_prev_mvs = false;
@@ -328,10 +331,12 @@ struct riv_encoder {
     std::unique_ptr<ThreadPool> mv_exec;  // one thread: MV coding strictly in frame order
     double host_ms[6] = {0};  // submit, retire, mv coding, dct coding (summed), write, blocked
     std::mutex stat_mu;
-    float last_times[8] = {0};
+    float last_times[NSTAGE + 1] = {0};
     bool have_times = false;
     riv_frame_stats last_stats{};
-    double sum_times[8] = {0};
+    double sum_times[NSTAGE + 1] = {0};
+    size_t coef_guess = 0;  // bytes of coefficients copied eagerly per frame
+    DevBuf prof;            // optional per-MB phase stamps of the search kernel
     uint64_t h2d_bytes = 0, d2h_bytes = 0, pframes = 0, launches = 0;
 };
 
@@ -428,20 +433,25 @@ static void setup_device(riv_encoder* e) {
     size_t rgb_bytes = (size_t)c.display_width * c.display_height * 3;
     for (auto& s : e->slots) {
         s.rgb.alloc(rgb_bytes);
-        s.side.alloc((size_t)N * 4 + 16);
+        s.dside.alloc((size_t)N * 4);
+        s.dpacked.alloc((size_t)N * 384 * 2);
+        s.dpeobs.alloc((size_t)N * 3);
+        s.side.alloc((size_t)N * 4);
+        s.packed.alloc((size_t)N * 384 * 2);
+        s.peobs.alloc((size_t)N * 3);
         s.hdr.alloc(16);
-        s.packed.alloc((size_t)N * 384 * 2 + 16);
-        s.peobs.alloc((size_t)N * 3 + 16);
         CK(cudaEventCreateWithFlags(&s.ev_h2d, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&s.ev_gpu, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&s.ev_d2h, cudaEventDisableTiming));
         for (int k = 0; k < EV_N; k++) CK(cudaEventCreate(&s.ev_k[k]));
+    }
+    e->coef_guess = (size_t)N * 384;  // half the dense size until the first frames are seen
+    if (getenv("RIV_PROFILE_SEARCH")) {
+        e->prof.alloc((size_t)N * 8 * sizeof(long long));
+        e->prof.zero(e->S);
     }
     e->cindex.alloc((size_t)N * 4);
     e->coffset.alloc((size_t)N * 4);
-    e->dside.alloc((size_t)N * 4 + 16);
-    e->dpacked.alloc((size_t)N * 384 * 2 + 16);
-    e->dpeobs.alloc((size_t)N * 3 + 16);
-    e->dhdr.alloc(16);
     if (search_use_table(c.search_range))
         e->sadtab.alloc((size_t)N * sad_table_stride(c.search_range) * sizeof(uint16_t));
     unsigned nt = c.entropy_threads;
@@ -497,6 +507,7 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         rp.intra = 1;
         rp.intra_ytab = e->ytab.as<uint16_t>();
         rp.intra_ctab = e->ctab.as<uint16_t>();
+        CK(cudaEventRecord(s.ev_k[EV_TABLE], S));
         CK(cudaEventRecord(s.ev_k[EV_SEARCH], S));
         CK(cudaEventRecord(s.ev_k[EV_PRED], S));
         CK(cudaEventRecord(s.ev_k[EV_AQ], S));
@@ -505,9 +516,8 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         if (e->intra_level > 0) CK(launch_deblock(recon, W, H, e->intra_E, e->intra_I, e->intra_H, nullptr, S));
         CK(cudaEventRecord(s.ev_k[EV_DEBLOCK], S));
         CK(launch_compact(e->opt_skip.as<uint8_t>(), e->mbout.as<MbOut>(), e->coeffs.as<int16_t>(), e->eobs.as<uint8_t>(), N, 1,
-                          e->cindex.as<int32_t>(), e->coffset.as<int32_t>(), e->dside.as<uint32_t>(),
-                          e->dpacked.as<int16_t>(), e->dpeobs.as<uint8_t>(), e->dhdr.as<uint32_t>(), s.side.dev<uint32_t>(),
-                          s.packed.dev<int16_t>(), s.peobs.dev<uint8_t>(), s.hdr.dev<uint32_t>(), S));
+                          e->cindex.as<int32_t>(), e->coffset.as<int32_t>(), s.dside.as<uint32_t>(),
+                          s.dpacked.as<int16_t>(), s.dpeobs.as<uint8_t>(), s.hdr.dev<uint32_t>(), S));
         e->has_prev_mvs = false;
     } else {
         SearchParams sp{};
@@ -545,6 +555,8 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
             sp.tab = e->sadtab.as<uint16_t>();
             CK(launch_sad_table(sp.ref_y, sp.cur_y, W, H, c.search_range, e->sadtab.as<uint16_t>(), sp.tstride, S));
         }
+        CK(cudaEventRecord(s.ev_k[EV_TABLE], S));
+        sp.prof = e->prof.as<long long>();
         CK(launch_search(sp, e->search_grid, S));
         CK(cudaEventRecord(s.ev_k[EV_SEARCH], S));
         // coded MVs of this frame become next frame's temporal predictors
@@ -564,9 +576,8 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         if (e->inter_level > 0) CK(launch_deblock(recon, W, H, e->inter_E, e->inter_I, e->inter_H, e->fmask.as<uint8_t>(), S));
         CK(cudaEventRecord(s.ev_k[EV_DEBLOCK], S));
         CK(launch_compact(e->opt_skip.as<uint8_t>(), e->mbout.as<MbOut>(), e->coeffs.as<int16_t>(), e->eobs.as<uint8_t>(), N, 0,
-                          e->cindex.as<int32_t>(), e->coffset.as<int32_t>(), e->dside.as<uint32_t>(),
-                          e->dpacked.as<int16_t>(), e->dpeobs.as<uint8_t>(), e->dhdr.as<uint32_t>(), s.side.dev<uint32_t>(),
-                          s.packed.dev<int16_t>(), s.peobs.dev<uint8_t>(), s.hdr.dev<uint32_t>(), S));
+                          e->cindex.as<int32_t>(), e->coffset.as<int32_t>(), s.dside.as<uint32_t>(),
+                          s.dpacked.as<int16_t>(), s.dpeobs.as<uint8_t>(), s.hdr.dev<uint32_t>(), S));
         e->coded_cur = cn;
         e->has_prev_mvs = true;
     }
@@ -575,6 +586,14 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
     CK(cudaEventRecord(s.ev_gpu, S));
     e->ref_cur = nxt;
     e->has_ref = true;
+    // DMA the side info, EOBs and (a bounded prefix of) the coefficients on the copy
+    // stream; the exact size is only known once the frame is done.
+    CK(cudaStreamWaitEvent(e->C, s.ev_gpu, 0));
+    CK(cudaMemcpyAsync(s.side.p, s.dside.p, (size_t)N * 4, cudaMemcpyDeviceToHost, e->C));
+    CK(cudaMemcpyAsync(s.peobs.p, s.dpeobs.p, (size_t)N * 3, cudaMemcpyDeviceToHost, e->C));
+    s.prefetched = std::min(e->coef_guess, (size_t)N * 384 * 2);
+    CK(cudaMemcpyAsync(s.packed.p, s.dpacked.p, s.prefetched, cudaMemcpyDeviceToHost, e->C));
+    CK(cudaEventRecord(s.ev_d2h, e->C));
 }
 
 // Host part of a frame once its GPU work is done: its side info and coefficients are
@@ -586,7 +605,7 @@ static double now_ms() {
 static riv_status retire(riv_encoder* e, Job& j) {
     Slot& s = e->slots[j.slot];
     double t0 = now_ms();
-    CK(cudaEventSynchronize(s.ev_gpu));
+    CK(cudaEventSynchronize(s.ev_d2h));
     const uint32_t* hdr = s.hdr.host<uint32_t>();
     unsigned st = hdr[2];
     if (st) {
@@ -594,14 +613,21 @@ static riv_status retire(riv_encoder* e, Job& j) {
                     (st & ST_WAIT_TIMEOUT) ? "device-side wavefront wait timed out" : "device search iteration cap hit");
     }
     j.count = hdr[0];
-    const uint32_t ncoef = hdr[1];
-    e->d2h_bytes += (uint64_t)e->NMB * 4 + 12 + (uint64_t)j.count * 3 + (uint64_t)ncoef * 2;
-    float t[8] = {0};
-    for (int k = 0; k < 7; k++) cudaEventElapsedTime(&t[k], s.ev_k[k], s.ev_k[k + 1]);
-    cudaEventElapsedTime(&t[7], s.ev_k[EV_START], s.ev_k[EV_COMPACT]);
-    for (int k = 0; k < 8; k++) j.times[k] = t[k] * 1000.0f;
+    const size_t coef_bytes = (size_t)hdr[1] * 2;
+    if (coef_bytes > s.prefetched) {  // the eager copy fell short: fetch the rest now
+        CK(cudaMemcpyAsync((char*)s.packed.p + s.prefetched, (const char*)s.dpacked.p + s.prefetched,
+                           coef_bytes - s.prefetched, cudaMemcpyDeviceToHost, e->C));
+        CK(cudaStreamSynchronize(e->C));
+    }
+    // next frames: copy 25% + 64 KiB more than this frame needed
+    e->coef_guess = coef_bytes + coef_bytes / 4 + 65536;
+    e->d2h_bytes += (uint64_t)e->NMB * 7 + 12 + std::max(coef_bytes, s.prefetched);
+    float t[NSTAGE + 1] = {0};
+    for (int k = 0; k < NSTAGE; k++) cudaEventElapsedTime(&t[k], s.ev_k[k], s.ev_k[k + 1]);
+    cudaEventElapsedTime(&t[NSTAGE], s.ev_k[EV_START], s.ev_k[EV_COMPACT]);
+    for (int k = 0; k <= NSTAGE; k++) j.times[k] = t[k] * 1000.0f;
     if (j.type == 2) {
-        for (int k = 0; k < 8; k++) e->sum_times[k] += j.times[k];
+        for (int k = 0; k <= NSTAGE; k++) e->sum_times[k] += j.times[k];
         e->pframes++;
     }
     const int N = e->NMB;
@@ -615,7 +641,7 @@ static riv_status retire(riv_encoder* e, Job& j) {
     S.blocks_total = (uint32_t)N;
     Job* jp = &j;
     riv_encoder* ep = e;
-    const uint32_t* side = s.side.host<uint32_t>();
+    const uint32_t* side = s.side.as<uint32_t>();
     if (j.type == 2) {
         j.fut_mv = e->mv_exec->submit([ep, jp, side, N] {
             double m0 = now_ms();
@@ -658,8 +684,8 @@ static riv_status retire(riv_encoder* e, Job& j) {
         // key frame: MV entropy contexts restart (enc/encoder.rs:335-337), in frame order
         j.fut_mv = e->mv_exec->submit([ep] { ep->mvc.reset(); });
     }
-    const int16_t* packed = s.packed.host<int16_t>();
-    const uint8_t* peobs = s.peobs.host<uint8_t>();
+    const int16_t* packed = s.packed.as<int16_t>();
+    const uint8_t* peobs = s.peobs.as<uint8_t>();
     uint32_t count = j.count;
     bool intra = j.type == 1;
     j.fut = e->pool->submit([jp, ep, packed, peobs, count, intra] {
@@ -921,16 +947,17 @@ void riv_encoder_free(riv_encoder* e) {
     if (e->S) cudaStreamSynchronize(e->S);
     if (e->C) cudaStreamSynchronize(e->C);
     for (auto& s : e->slots) {
-        s.rgb.release(); s.side.release(); s.hdr.release(); s.packed.release(); s.peobs.release();
+        s.rgb.release(); s.dside.release(); s.dpacked.release(); s.dpeobs.release();
+        s.side.release(); s.packed.release(); s.peobs.release(); s.hdr.release();
         if (s.ev_h2d) cudaEventDestroy(s.ev_h2d);
         if (s.ev_gpu) cudaEventDestroy(s.ev_gpu);
+        if (s.ev_d2h) cudaEventDestroy(s.ev_d2h);
         for (int k = 0; k < EV_N; k++)
             if (s.ev_k[k]) cudaEventDestroy(s.ev_k[k]);
     }
     DevBuf* bufs[] = {&e->cur, &e->ref[0], &e->ref[1], &e->pred, &e->mbout, &e->coded[0], &e->coded[1], &e->rec,
                       &e->varsum, &e->lnv, &e->qs, &e->coeffs, &e->opt_skip, &e->fmask, &e->eobs, &e->status,
-                      &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset, &e->sadtab,
-                      &e->dside, &e->dpacked, &e->dpeobs, &e->dhdr};
+                      &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset, &e->sadtab, &e->prof};
     for (DevBuf* b : bufs) b->release();
     if (e->S) cudaStreamDestroy(e->S);
     if (e->C) cudaStreamDestroy(e->C);
@@ -966,6 +993,7 @@ riv_status riv_debug_frame_state(riv_encoder* e, int what, void* out, size_t siz
         case 3: b = &e->cur; break;
         case 4: b = &e->coeffs; break;
         case 5: b = &e->opt_skip; break;
+        case 6: b = &e->prof; break;
         default: return RIV_ERR_FRAME;
     }
     if (size < b->n) return RIV_ERR_FRAME;

@@ -46,6 +46,7 @@ struct SearchParams {
     MbOut* out;
     unsigned* status;
     long long spin_limit;
+    long long* prof;  // optional: 8 clock64 stamps per MB (phase boundaries), nullptr = off
 };
 
 struct ResidualParams {
@@ -83,9 +84,11 @@ int launch_aq(const uint2* varsum, int n, float base, const uint32_t* logfix, in
               int nexp, float* lnv_scratch, float* qs, void* stream);
 int launch_residual(const ResidualParams& p, int nmb, void* stream);
 int launch_deblock(uint8_t* yuv, int W, int H, int E, int I, int Hev, const uint8_t* mask, void* stream);
+// k_scan writes {coded MBs, coefficients} to hhdr (mapped host memory); k_pack fills the
+// device-side side info / EOB / coefficient buffers, copied back by DMA afterwards.
 int launch_compact(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coeffs, const uint8_t* eobs, int nmb,
                    int intra, int32_t* index, int32_t* offset, uint32_t* dside, int16_t* dpacked, uint8_t* dpeobs,
-                   uint32_t* dhdr, uint32_t* hside, int16_t* hpacked, uint8_t* hpeobs, uint32_t* hhdr, void* stream);
+                   uint32_t* hhdr, void* stream);
 // libm device helpers exposed for the exhaustive check
 int launch_libm_eval(int which, const float* in, float* out, size_t n, const uint32_t* fix, int nfix, void* stream);
 

@@ -295,6 +295,11 @@ __device__ __forceinline__ int argmin8(long long total, bool valid, long long& b
     return k < 64 ? k : -1;
 }
 
+#define RIV_STAMP(k)                                                        \
+    do {                                                                    \
+        if (p.prof != nullptr && lane == 0) p.prof[(size_t)idx * 8 + (k)] = clock64(); \
+    } while (0)
+
 template <bool BAND, bool TABLE>
 __global__ void __launch_bounds__(32) k_search(SearchParams p) {
     extern __shared__ __align__(16) uint8_t smem[];
@@ -336,6 +341,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
         for (int bx = 0; bx < p.BW; bx++) {
             const int x0 = bx * 16;
             const int idx = r * p.BW + bx;
+            RIV_STAMP(0);
             // ---- prefetch MB bx+1 (columns and current block), then wait for MB bx's data
             if (bx + 1 < p.BW) {
                 if (BAND) {
@@ -385,6 +391,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
             const uint32_t c0 = *(const uint32_t*)(cb + yy * 16 + xoff);
             const uint32_t c1 = *(const uint32_t*)(cb + yy * 16 + xoff + 4);
 
+            RIV_STAMP(1);
             // ---- wait for the row above (top-right, or top at the last column).  The record
             // of the next MB's top-right was requested one MB earlier (pref); it is polled
             // again only if it had not been published yet.
@@ -415,6 +422,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                 cp_async_wait0();
                 return;
             }
+            RIV_STAMP(2);
             const bool has_t = r > 0, has_l = bx > 0, has_tl = r > 0 && bx > 0;
             auto rec_raw = [](unsigned long long v, int& dx, int& dy) {
                 dx = (int)(int8_t)(v >> 40); dy = (int)(int8_t)(v >> 32);
@@ -624,6 +632,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                     }
                 }
             }
+            RIV_STAMP(3);
             // ---- half-pel refinement (enc/motion/scalar.rs:759-839): nine floor-averaged
             // candidates around (2*sdx, 2*sdy), from a 3x3 integer neighbourhood per pixel,
             // on packed bytes.  Candidate q = (sy+1)*3 + (sx+1).
@@ -689,6 +698,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
             if (raw.sx == -1) { raw.sx = 1; raw.dx = max(-128, raw.dx - 1); }
             if (raw.sy == -1) { raw.sy = 1; raw.dy = max(-128, raw.dy - 1); }
 
+            RIV_STAMP(4);
             // ---- RDO skip decision (enc/rdo.rs:140-178)
             bool int_al = raw.sx == 0 && raw.sy == 0;
             double satd = (double)max(best_sad, 0LL);
@@ -753,6 +763,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
             if (mode == 5) flags = (raw.sx == 1 ? 0x01 : 0) | (raw.sy == 1 ? 0x04 : 0);
             if (rdo_skip) flags |= 0x40;
 
+            RIV_STAMP(5);
             // ---- publish
             if (lane == 0) {
                 unsigned long long rv = tagbits | ((unsigned long long)(uint8_t)raw.dx << 40) |
@@ -771,6 +782,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                 o.best_sad = (int32_t)best_sad;
                 p.out[idx] = o;
             }
+            RIV_STAMP(6);
             L_raw = MvT{raw.dx, raw.dy, 0, 0};
             L_cod = coded;
             recTL = recT;
@@ -1412,30 +1424,12 @@ __global__ void __launch_bounds__(128) k_pack(const uint8_t* opt_skip, const MbO
     }
 }
 
-// Copies the packed side info, EOBs and coefficients (sizes read from the device header)
-// into mapped host memory with full 16-byte stores.
-__global__ void k_copy_out(const uint32_t* __restrict__ dside, const uint8_t* __restrict__ dpeobs,
-                           const int16_t* __restrict__ dpacked, const uint32_t* __restrict__ dhdr, int nmb,
-                           uint32_t* hside, uint8_t* hpeobs, int16_t* hpacked, uint32_t* hhdr) {
-    const uint32_t count = dhdr[0], total = dhdr[1];
-    const size_t n_side = ((size_t)nmb * 4 + 15) / 16, n_eob = ((size_t)count * 3 + 15) / 16,
-                 n_coef = ((size_t)total * 2 + 15) / 16;
-    const size_t n = n_side + n_eob + n_coef;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        if (i < n_side) ((uint4*)hside)[i] = ((const uint4*)dside)[i];
-        else if (i < n_side + n_eob) ((uint4*)hpeobs)[i - n_side] = ((const uint4*)dpeobs)[i - n_side];
-        else ((uint4*)hpacked)[i - n_side - n_eob] = ((const uint4*)dpacked)[i - n_side - n_eob];
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) { hhdr[0] = count; hhdr[1] = total; }
-}
-
 int launch_compact(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coeffs, const uint8_t* eobs, int nmb,
                    int intra, int32_t* index, int32_t* offset, uint32_t* dside, int16_t* dpacked, uint8_t* dpeobs,
-                   uint32_t* dhdr, uint32_t* hside, int16_t* hpacked, uint8_t* hpeobs, uint32_t* hhdr, void* stream) {
+                   uint32_t* hhdr, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
-    k_scan<<<1, 1024, 0, st>>>(opt_skip, eobs, nmb, intra, index, offset, dhdr);
+    k_scan<<<1, 1024, 0, st>>>(opt_skip, eobs, nmb, intra, index, offset, hhdr);
     k_pack<<<nmb, 128, 0, st>>>(opt_skip, mb, coeffs, eobs, index, offset, intra, dside, dpacked, dpeobs);
-    k_copy_out<<<296, 256, 0, st>>>(dside, dpeobs, dpacked, dhdr, nmb, hside, hpeobs, hpacked, hhdr);
     return (int)cudaGetLastError();
 }
 

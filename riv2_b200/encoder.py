@@ -455,13 +455,13 @@ class Encoder:
         return y, u, v
 
     def last_kernel_times_us(self) -> np.ndarray:
-        t = np.zeros(8, np.float32)
+        t = np.zeros(9, np.float32)
         self._check(lib().riv_last_kernel_times(self._h, t.ctypes.data_as(C.POINTER(C.c_float))))
         return t
 
     def counters(self) -> dict:
         """Cumulative GPU stage times (us, P-frames), I/O bytes and kernel launches."""
-        us = (C.c_double * 8)()
+        us = (C.c_double * 9)()
         io = (C.c_uint64 * 2)()
         n = (C.c_uint64 * 2)()
         self._check(lib().riv_counters(self._h, us, io, n))
@@ -475,7 +475,8 @@ class Encoder:
         sw, sh = self.config.storage_width, self.config.storage_height
         nmb = (sw // 16) * (sh // 16)
         spec = {0: (nmb * 20, np.uint8), 1: (nmb, np.float32), 2: (sw * sh * 3 // 2, np.uint8),
-                3: (sw * sh * 3 // 2, np.uint8), 4: (nmb * 384, np.int16), 5: (nmb, np.uint8)}[what]
+                3: (sw * sh * 3 // 2, np.uint8), 4: (nmb * 384, np.int16), 5: (nmb, np.uint8),
+                6: (nmb * 8, np.int64)}[what]
         out = np.empty(spec[0], spec[1])
         self._check(lib().riv_debug_frame_state(self._h, what, C.c_void_p(out.ctypes.data), out.nbytes))
         return out
