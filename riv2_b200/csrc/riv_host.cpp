@@ -310,7 +310,7 @@ struct riv_encoder {
     uint64_t header_pos = 0, frame_count = 0, submitted = 0;
     int W = 0, H = 0, BW = 0, BH = 0, NMB = 0;
     size_t yuv_bytes = 0;
-    cudaStream_t S = nullptr, C = nullptr;
+    cudaStream_t S = nullptr, C = nullptr, Hs = nullptr;  // compute, device->host, host->device
     // device state
     DevBuf cur, ref[2], pred, mbout, coded[2], rec, varsum, lnv, qs, coeffs, opt_skip, fmask, eobs, status;
     DevBuf cindex, coffset, sadtab;
@@ -374,6 +374,7 @@ static void setup_device(riv_encoder* e) {
     e->yuv_bytes = (size_t)e->W * e->H * 3 / 2;
     CK(cudaStreamCreateWithFlags(&e->S, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&e->C, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&e->Hs, cudaStreamNonBlocking));
     int32_t t16[256], t8[64];
     dct_tables(t16, t8);
     CK(riv_upload_dct_tables(t16, t8));
@@ -432,7 +433,7 @@ static void setup_device(riv_encoder* e) {
     e->slots.resize(nslots);
     size_t rgb_bytes = (size_t)c.display_width * c.display_height * 3;
     for (auto& s : e->slots) {
-        s.rgb.alloc(rgb_bytes);
+        s.rgb.alloc(std::max(rgb_bytes, e->yuv_bytes));
         s.dside.alloc((size_t)N * 4);
         s.dpacked.alloc((size_t)N * 384 * 2);
         s.dpeobs.alloc((size_t)N * 3);
@@ -475,20 +476,22 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
     if (src == 0) e->h2d_bytes += (uint64_t)c.display_width * c.display_height * 3;
     if (src == 2) e->h2d_bytes += e->yuv_bytes;
     if (src == 0) {
-        CK(cudaMemcpyAsync(s.rgb.p, a, (size_t)c.display_width * c.display_height * 3, cudaMemcpyHostToDevice, e->C));
-        CK(cudaEventRecord(s.ev_h2d, e->C));
+        CK(cudaMemcpyAsync(s.rgb.p, a, (size_t)c.display_width * c.display_height * 3, cudaMemcpyHostToDevice, e->Hs));
+        CK(cudaEventRecord(s.ev_h2d, e->Hs));
         CK(cudaStreamWaitEvent(S, s.ev_h2d, 0));
         CK(launch_rgb_to_yuv((const uint8_t*)s.rgb.p, (int)c.display_width, (int)c.display_height, e->cur.as<uint8_t>(), W, H, S));
     } else if (src == 1) {
         CK(launch_rgb_to_yuv((const uint8_t*)a, (int)c.display_width, (int)c.display_height, e->cur.as<uint8_t>(), W, H, S));
     } else {
-        uint8_t* d = e->cur.as<uint8_t>();
+        // staged through the slot buffer: the previous frame's kernels may still read `cur`
+        uint8_t* d = s.rgb.as<uint8_t>();
         size_t ys = (size_t)W * H, cs = ys / 4;
-        CK(cudaMemcpyAsync(d, a, ys, cudaMemcpyHostToDevice, e->C));
-        CK(cudaMemcpyAsync(d + ys, b, cs, cudaMemcpyHostToDevice, e->C));
-        CK(cudaMemcpyAsync(d + ys + cs, c3, cs, cudaMemcpyHostToDevice, e->C));
-        CK(cudaEventRecord(s.ev_h2d, e->C));
+        CK(cudaMemcpyAsync(d, a, ys, cudaMemcpyHostToDevice, e->Hs));
+        CK(cudaMemcpyAsync(d + ys, b, cs, cudaMemcpyHostToDevice, e->Hs));
+        CK(cudaMemcpyAsync(d + ys + cs, c3, cs, cudaMemcpyHostToDevice, e->Hs));
+        CK(cudaEventRecord(s.ev_h2d, e->Hs));
         CK(cudaStreamWaitEvent(S, s.ev_h2d, 0));
+        CK(cudaMemcpyAsync(e->cur.p, d, e->yuv_bytes, cudaMemcpyDeviceToDevice, S));
     }
     CK(cudaEventRecord(s.ev_k[EV_YUV], S));
     const int nxt = e->ref_cur ^ 1;
@@ -946,6 +949,7 @@ void riv_encoder_free(riv_encoder* e) {
     e->mv_exec.reset();
     if (e->S) cudaStreamSynchronize(e->S);
     if (e->C) cudaStreamSynchronize(e->C);
+    if (e->Hs) cudaStreamSynchronize(e->Hs);
     for (auto& s : e->slots) {
         s.rgb.release(); s.dside.release(); s.dpacked.release(); s.dpeobs.release();
         s.side.release(); s.packed.release(); s.peobs.release(); s.hdr.release();
@@ -961,6 +965,7 @@ void riv_encoder_free(riv_encoder* e) {
     for (DevBuf* b : bufs) b->release();
     if (e->S) cudaStreamDestroy(e->S);
     if (e->C) cudaStreamDestroy(e->C);
+    if (e->Hs) cudaStreamDestroy(e->Hs);
     delete e;
 }
 
