@@ -314,7 +314,8 @@ struct riv_encoder {
     // device state
     DevBuf cur, ref[2], pred, mbout, coded[2], rec, varsum, lnv, qs, coeffs, opt_skip, fmask, eobs, status;
     DevBuf cindex, coffset, sadtab;
-    DevBuf mvbits, logfix, expfix, ytab, ctab;
+    DevBuf mvbits, logfix, expfix, ytab, ctab, newcost;
+    bool table_ok = false;  // exhaustive SAD table + packed argmin usable (costs < 2^59)
     int ref_cur = 0, coded_cur = 0;
     bool has_ref = false, has_prev_mvs = false;
     unsigned tag = 0;
@@ -403,6 +404,22 @@ static void setup_device(riv_encoder* e) {
     for (int d = 1; d < 256; d++) bits[d] = 2.0 * log2((double)d) + 2.0;
     e->mvbits.alloc(sizeof(bits));
     CK(cudaMemcpy(e->mvbits.p, bits, sizeof(bits), cudaMemcpyHostToDevice));
+    {
+        // NEW-mode cost table: (lambda * 2.0 * (6.0 + bx + by)) as i64 (enc/motion/scalar.rs:503-541)
+        Lambda Lq = lambda_for(c.inter_quality, c.rdo_lambda_mult);
+        std::vector<long long> nt(256 * 256);
+        long long mx = 0;
+        for (int a = 0; a < 256; a++)
+            for (int b = 0; b < 256; b++) {
+                long long v = f64_as_i64(Lq.lambda * 2.0 * (6.0 + bits[a] + bits[b]));
+                nt[a * 256 + b] = v;
+                mx = std::max<long long>(mx, v);
+            }
+        mx = std::max<long long>(mx, f64_as_i64(Lq.lambda * 2.0 * 1.5));
+        e->table_ok = search_use_table(c.search_range) && mx < (1ll << 58) && Lq.lambda >= 0.0;
+        e->newcost.alloc(nt.size() * sizeof(long long));
+        CK(cudaMemcpy(e->newcost.p, nt.data(), nt.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    }
     LibmFix& F = libm_fix();
     if (!F.ok) throw std::runtime_error("glibc fix-up table: " + F.err);
     e->nlog = (int)(F.logf.size() / 2);
@@ -418,7 +435,7 @@ static void setup_device(riv_encoder* e) {
     CK(cudaMemcpy(e->ytab.p, yt, sizeof(yt), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(e->ctab.p, ct, sizeof(ct), cudaMemcpyHostToDevice));
     int g = 0;
-    CK(search_max_grid(c.search_range, (int)c.storage_width, &g));
+    CK(search_max_grid(c.search_range, (int)c.storage_width, e->table_ok, &g));
     if (g <= 0) throw std::runtime_error("search kernel cannot be made resident");
     e->search_grid = std::min(g, e->BH);
     // frame constants
@@ -453,7 +470,7 @@ static void setup_device(riv_encoder* e) {
     }
     e->cindex.alloc((size_t)N * 4);
     e->coffset.alloc((size_t)N * 4);
-    if (search_use_table(c.search_range))
+    if (e->table_ok)
         e->sadtab.alloc((size_t)N * sad_table_stride(c.search_range) * sizeof(uint16_t));
     unsigned nt = c.entropy_threads;
     if (nt == 0) nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency() > 1 ? std::thread::hardware_concurrency() - 1 : 1u));
@@ -471,7 +488,7 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
     CK(cudaEventRecord(s.ev_k[EV_START], S));
     // kernels per frame: rgb->yuv, (search, predict, 3 x aq), residual, deblock (2 per plane), scan + pack
     const int nplanes_db = 3 * 2;
-    e->launches += (src == 2 ? 0 : 1) + (j.type == 2 ? 5 + (search_use_table(c.search_range) ? 1 : 0) : 0) + 1 +
+    e->launches += (src == 2 ? 0 : 1) + (j.type == 2 ? 5 + (e->table_ok ? 1 : 0) : 0) + 1 +
                    ((j.type == 2 ? e->inter_level : e->intra_level) > 0 ? nplanes_db : 0) + 3;
     if (src == 0) e->h2d_bytes += (uint64_t)c.display_width * c.display_height * 3;
     if (src == 2) e->h2d_bytes += e->yuv_bytes;
@@ -536,6 +553,7 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         sp.c05 = f64_as_i64(lam * 2.0 * 0.5);
         sp.lambda_zero = lam == 0.0;
         sp.mvbits = e->mvbits.as<double>();
+        sp.newcost = e->newcost.as<long long>();
         sp.rdo_lambda = lam;
         sp.rdo_skip_bits = e->L.skip_bits;
         sp.rdo_keep_bits = e->L.keep_bits;
@@ -553,7 +571,7 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         sp.spin_limit = 1ll << 22;  // ~ a few seconds, far above any legitimate wait
         sp.tab = nullptr;
         sp.tstride = 0;
-        if (search_use_table(c.search_range)) {
+        if (e->table_ok) {
             sp.tstride = sad_table_stride(c.search_range);
             sp.tab = e->sadtab.as<uint16_t>();
             CK(launch_sad_table(sp.ref_y, sp.cur_y, W, H, c.search_range, e->sadtab.as<uint16_t>(), sp.tstride, S));
@@ -961,7 +979,7 @@ void riv_encoder_free(riv_encoder* e) {
     }
     DevBuf* bufs[] = {&e->cur, &e->ref[0], &e->ref[1], &e->pred, &e->mbout, &e->coded[0], &e->coded[1], &e->rec,
                       &e->varsum, &e->lnv, &e->qs, &e->coeffs, &e->opt_skip, &e->fmask, &e->eobs, &e->status,
-                      &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset, &e->sadtab, &e->prof};
+                      &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset, &e->sadtab, &e->prof, &e->newcost};
     for (DevBuf* b : bufs) b->release();
     if (e->S) cudaStreamDestroy(e->S);
     if (e->C) cudaStreamDestroy(e->C);

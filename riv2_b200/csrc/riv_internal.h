@@ -36,6 +36,9 @@ struct SearchParams {
     long long c05;    // (lambda * 2.0 * 0.5) as i64
     int lambda_zero;  // lambda == 0.0
     const double* mvbits;  // 256 entries: b(0)=1, b(d)=2*log2(d)+2 (glibc log2, host-computed)
+    // NEW-mode bit cost (lambda*2*(6 + b(ax) + b(ay))) as i64, for ax, ay in [0,255], host-computed
+    // in f64 exactly like the reference; nullptr = evaluate in f64 on the device.
+    const long long* newcost;
     // RDO (enc/rdo.rs)
     double rdo_lambda, rdo_skip_bits, rdo_keep_bits, rdo_icpt, rdo_slope, rdo_ret, rdo_guard;
     int rdo_allow;
@@ -77,7 +80,7 @@ bool search_use_table(int sr);
 int sad_table_stride(int sr);
 int launch_sad_table(const uint8_t* ref, const uint8_t* cur, int W, int H, int sr, uint16_t* tab, int tstride,
                      void* stream);
-int search_max_grid(int sr, int W, int* grid_out);
+int search_max_grid(int sr, int W, bool table, int* grid_out);
 size_t search_smem_bytes(int sr);
 int launch_predict(const uint8_t* ref, const MbOut* mb, uint8_t* pred, uint2* varsum, int W, int H, void* stream);
 int launch_aq(const uint2* varsum, int n, float base, const uint32_t* logfix, int nlog, const uint32_t* expfix,

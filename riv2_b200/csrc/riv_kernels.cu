@@ -103,6 +103,11 @@ __device__ __forceinline__ long long mv_cost(int dx, int dy, const CostCtx& c, c
     long long best = LLONG_MAX;
     if ((dx == c.nx && dy == c.ny) || (dx == c.rx && dy == c.ry) || (dx == c.mx && dy == c.my)) best = p.c15;
     if (dx == 0 && dy == 0) best = min(best, p.c05);
+    if (p.newcost) {
+        long long a = __ldg(p.newcost + abs(dx - c.nx) * 256 + abs(dy - c.ny));
+        long long b = __ldg(p.newcost + abs(dx - c.rx) * 256 + abs(dy - c.ry));
+        return min(best, min(a, b));
+    }
     {
         double b = __dadd_rn(__dadd_rn(6.0, bits[abs(dx - c.nx)]), bits[abs(dy - c.ny)]);
         best = min(best, __double2ll_rz(__dmul_rn(p.lam2, b)));
@@ -218,7 +223,7 @@ __global__ void __launch_bounds__(128) k_sad_table(const uint8_t* __restrict__ r
                                                    int tstride) {
     extern __shared__ __align__(16) uint8_t sm[];
     const int WT = 16 + 2 * sr;                 // window side
-    const int WTS = (WT + 3 + 15) & ~15;        // row stride (+ slack for unaligned word reads)
+    const int WTS = (WT + 8 + 15) & ~15;        // row stride (+ slack for the 24-byte row reads)
     uint8_t* win = sm;
     uint32_t* cw = (uint32_t*)(sm + WT * WTS + 16);  // 64 words of the current block
     const int mb = blockIdx.x;
@@ -238,17 +243,39 @@ __global__ void __launch_bounds__(128) k_sad_table(const uint8_t* __restrict__ r
     const int side = 2 * sr + 1, P = side * side;
     const bool interior = x0 - sr >= 0 && y0 - sr >= 0 && x0 + 15 + sr <= W - 1 && y0 + 15 + sr <= H - 1;
     uint16_t* out = tab + (size_t)mb * tstride;
-    for (int pidx = threadIdx.x; pidx < P; pidx += blockDim.x) {
-        const int dy = pidx / side - sr, dx = pidx % side - sr;
-        unsigned s = 0;
-        if (interior) {
-#pragma unroll 4
+    if (interior) {
+        // Thread = 8 horizontally adjacent positions dx = 8q-sr .. 8q-sr+7 of one dy; their
+        // reference rows start at window column 8q (4-byte aligned), so the shifted words
+        // come from aligned loads with compile-time funnel shifts.
+        const int nq = (side + 7) >> 3;
+        for (int item = threadIdx.x; item < side * nq; item += blockDim.x) {
+            const int dyi = item / nq, q = item - dyi * nq;
+            unsigned acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll 2
             for (int r = 0; r < 16; r++) {
-                const uint8_t* row = win + (r + dy + sr) * WTS + dx + sr;
+                const uint2* rowp = (const uint2*)(win + (r + dyi) * WTS + 8 * q);
+                const uint2 a = rowp[0], b = rowp[1], c = rowp[2];
+                const uint32_t w[6] = {a.x, a.y, b.x, b.y, c.x, c.y};
+                const uint4 cv = ((const uint4*)cw)[r];
+                const uint32_t cg[4] = {cv.x, cv.y, cv.z, cv.w};
 #pragma unroll
-                for (int g = 0; g < 4; g++) s += __vsadu4(cw[r * 4 + g], lds_u32(row + 4 * g));
+                for (int g = 0; g < 4; g++) {
+#pragma unroll
+                    for (int j = 0; j < 8; j++) {
+                        const int k = (j >> 2) + g, sh = (j & 3) * 8;
+                        const uint32_t ref = sh ? __funnelshift_r(w[k], w[k + 1], sh) : w[k];
+                        acc[j] += __vsadu4(cg[g], ref);
+                    }
+                }
             }
-        } else {
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+                if (8 * q + j < side) out[dyi * side + 8 * q + j] = (uint16_t)acc[j];
+        }
+    } else {
+        for (int pidx = threadIdx.x; pidx < P; pidx += blockDim.x) {
+            const int dy = pidx / side - sr, dx = pidx % side - sr;
+            unsigned s = 0;
             for (int r = 0; r < 16; r++) {
                 int ry = min(max(y0 + (r & ~3) + dy, 0), H - 4) + (r & 3) - wy0;
                 const uint8_t* row = win + ry * WTS;
@@ -258,12 +285,12 @@ __global__ void __launch_bounds__(128) k_sad_table(const uint8_t* __restrict__ r
                     s += __vsadu4(cw[r * 4 + g], lds_u32(row + rx));
                 }
             }
+            out[pidx] = (uint16_t)s;
         }
-        out[pidx] = (uint16_t)s;
     }
 }
 size_t sad_table_smem(int sr) {
-    int WT = 16 + 2 * sr, WTS = (WT + 3 + 15) & ~15;
+    int WT = 16 + 2 * sr, WTS = (WT + 8 + 15) & ~15;
     return (size_t)WT * WTS + 16 + 256;
 }
 int launch_sad_table(const uint8_t* ref, const uint8_t* cur, int W, int H, int sr, uint16_t* tab, int tstride,
@@ -279,20 +306,19 @@ int launch_sad_table(const uint8_t* ref, const uint8_t* cur, int W, int H, int s
 }
 
 // Warp argmin over lanes 0..7 of (total, lane) with the lowest lane winning ties; lanes
-// with valid == false do not compete.  Returns the winning lane (or -1).
+// with valid == false do not compete.  Totals are below 2^59 (the host enables the table
+// path only then), so (total << 3 | lane) is an exact sort key.  Returns the winning lane
+// (or -1) and the minimum total.
 __device__ __forceinline__ int argmin8(long long total, bool valid, long long& best_total) {
-    long long t = valid ? total : LLONG_MAX;
-    int k = valid ? (int)(threadIdx.x & 31) : 64;
+    unsigned long long key = valid ? ((unsigned long long)total << 3) | (threadIdx.x & 7) : ~0ull;
 #pragma unroll
     for (int o = 1; o < 8; o <<= 1) {
-        long long t2 = __shfl_xor_sync(0xffffffffu, t, o);
-        int k2 = __shfl_xor_sync(0xffffffffu, k, o);
-        if (t2 < t || (t2 == t && k2 < k)) { t = t2; k = k2; }
+        unsigned long long k2 = __shfl_xor_sync(0xffffffffu, key, o);
+        key = k2 < key ? k2 : key;
     }
-    t = __shfl_sync(0xffffffffu, t, 0);
-    k = __shfl_sync(0xffffffffu, k, 0);
-    best_total = t;
-    return k < 64 ? k : -1;
+    key = __shfl_sync(0xffffffffu, key, 0);
+    best_total = (long long)(key >> 3);
+    return key == ~0ull ? -1 : (int)(key & 7);
 }
 
 #define RIV_STAMP(k)                                                        \
@@ -813,8 +839,8 @@ static const void* search_fn(bool band, bool table) {
 
 size_t search_smem_bytes(int sr) { return search_smem(sr, 0, false, search_use_table(sr)); }
 
-int search_max_grid(int sr, int W, int* grid_out) {
-    bool band = search_use_band(sr, W), table = search_use_table(sr);
+int search_max_grid(int sr, int W, bool table, int* grid_out) {
+    bool band = search_use_band(sr, W);
     size_t sm = search_smem(sr, W, band, table);
     const void* fn = search_fn(band, table);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -830,7 +856,7 @@ int search_max_grid(int sr, int W, int* grid_out) {
 }
 
 int launch_search(const SearchParams& p, int grid, void* stream) {
-    bool band = search_use_band(p.sr, p.W), table = search_use_table(p.sr);
+    bool band = search_use_band(p.sr, p.W), table = p.tab != nullptr;
     size_t sm = search_smem(p.sr, p.W, band, table);
     SearchParams q = p;
     void* args[] = {&q};
