@@ -314,7 +314,8 @@ struct riv_encoder {
     // device state
     DevBuf cur, ref[2], pred, mbout, coded[2], rec, varsum, lnv, qs, coeffs, opt_skip, fmask, eobs, status;
     DevBuf cindex, coffset, sadtab;
-    DevBuf mvbits, logfix, expfix, ytab, ctab, newcost;
+    DevBuf mvbits, logfix, expfix, ytab, ctab, newcost, newcost32;
+    bool small_costs = false;
     bool table_ok = false;  // exhaustive SAD table + packed argmin usable (costs < 2^59)
     int ref_cur = 0, coded_cur = 0;
     bool has_ref = false, has_prev_mvs = false;
@@ -419,6 +420,12 @@ static void setup_device(riv_encoder* e) {
         e->table_ok = search_use_table(c.search_range) && mx < (1ll << 58) && Lq.lambda >= 0.0;
         e->newcost.alloc(nt.size() * sizeof(long long));
         CK(cudaMemcpy(e->newcost.p, nt.data(), nt.size() * sizeof(long long), cudaMemcpyHostToDevice));
+        e->small_costs = mx < (1ll << 27) && Lq.lambda >= 0.0;
+        std::vector<int> n32(64 * 64);
+        for (int a = 0; a < 64; a++)
+            for (int b = 0; b < 64; b++) n32[a * 64 + b] = (int)std::min<long long>(nt[a * 256 + b], INT32_MAX);
+        e->newcost32.alloc(n32.size() * sizeof(int));
+        CK(cudaMemcpy(e->newcost32.p, n32.data(), n32.size() * sizeof(int), cudaMemcpyHostToDevice));
     }
     LibmFix& F = libm_fix();
     if (!F.ok) throw std::runtime_error("glibc fix-up table: " + F.err);
@@ -554,6 +561,8 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         sp.lambda_zero = lam == 0.0;
         sp.mvbits = e->mvbits.as<double>();
         sp.newcost = e->newcost.as<long long>();
+        sp.newcost32 = e->newcost32.as<int>();
+        sp.small = e->small_costs ? 1 : 0;
         sp.rdo_lambda = lam;
         sp.rdo_skip_bits = e->L.skip_bits;
         sp.rdo_keep_bits = e->L.keep_bits;
@@ -979,7 +988,7 @@ void riv_encoder_free(riv_encoder* e) {
     }
     DevBuf* bufs[] = {&e->cur, &e->ref[0], &e->ref[1], &e->pred, &e->mbout, &e->coded[0], &e->coded[1], &e->rec,
                       &e->varsum, &e->lnv, &e->qs, &e->coeffs, &e->opt_skip, &e->fmask, &e->eobs, &e->status,
-                      &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset, &e->sadtab, &e->prof, &e->newcost};
+                      &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset, &e->sadtab, &e->prof, &e->newcost, &e->newcost32};
     for (DevBuf* b : bufs) b->release();
     if (e->S) cudaStreamDestroy(e->S);
     if (e->C) cudaStreamDestroy(e->C);

@@ -39,6 +39,10 @@ struct SearchParams {
     // NEW-mode bit cost (lambda*2*(6 + b(ax) + b(ay))) as i64, for ax, ay in [0,255], host-computed
     // in f64 exactly like the reference; nullptr = evaluate in f64 on the device.
     const long long* newcost;
+    // Same costs for |ax|,|ay| < 64 as a 64x64 int32 table (staged in shared memory), valid
+    // when every cost is below 2^27 (small == 1); then warp argmins use 32-bit keys.
+    const int* newcost32;
+    int small;
     // RDO (enc/rdo.rs)
     double rdo_lambda, rdo_skip_bits, rdo_keep_bits, rdo_icpt, rdo_slope, rdo_ret, rdo_guard;
     int rdo_allow;

@@ -98,22 +98,25 @@ struct CostCtx {
 
 // estimate_mv_cost (enc/motion/scalar.rs:453-544)
 __device__ __forceinline__ long long mv_cost(int dx, int dy, const CostCtx& c, const SearchParams& p,
-                                             const double* bits) {
+                                             const double* bits, const int* nc32) {
     if (p.lambda_zero) return 0;
     long long best = LLONG_MAX;
     if ((dx == c.nx && dy == c.ny) || (dx == c.rx && dy == c.ry) || (dx == c.mx && dy == c.my)) best = p.c15;
     if (dx == 0 && dy == 0) best = min(best, p.c05);
+    const int ax = abs(dx - c.nx), ay = abs(dy - c.ny), bx = abs(dx - c.rx), by = abs(dy - c.ry);
+    if (nc32 != nullptr && ((ax | ay | bx | by) < 64))
+        return min(best, (long long)min(nc32[ax * 64 + ay], nc32[bx * 64 + by]));
     if (p.newcost) {
-        long long a = __ldg(p.newcost + abs(dx - c.nx) * 256 + abs(dy - c.ny));
-        long long b = __ldg(p.newcost + abs(dx - c.rx) * 256 + abs(dy - c.ry));
+        long long a = __ldg(p.newcost + ax * 256 + ay);
+        long long b = __ldg(p.newcost + bx * 256 + by);
         return min(best, min(a, b));
     }
     {
-        double b = __dadd_rn(__dadd_rn(6.0, bits[abs(dx - c.nx)]), bits[abs(dy - c.ny)]);
+        double b = __dadd_rn(__dadd_rn(6.0, bits[ax]), bits[ay]);
         best = min(best, __double2ll_rz(__dmul_rn(p.lam2, b)));
     }
     {
-        double b = __dadd_rn(__dadd_rn(6.0, bits[abs(dx - c.rx)]), bits[abs(dy - c.ry)]);
+        double b = __dadd_rn(__dadd_rn(6.0, bits[bx]), bits[by]);
         best = min(best, __double2ll_rz(__dmul_rn(p.lam2, b)));
     }
     return best;
@@ -309,7 +312,13 @@ int launch_sad_table(const uint8_t* ref, const uint8_t* cur, int W, int H, int s
 // with valid == false do not compete.  Totals are below 2^59 (the host enables the table
 // path only then), so (total << 3 | lane) is an exact sort key.  Returns the winning lane
 // (or -1) and the minimum total.
-__device__ __forceinline__ int argmin8(long long total, bool valid, long long& best_total) {
+__device__ __forceinline__ int argmin8(long long total, bool valid, long long& best_total, bool small) {
+    if (small) {  // totals < 2^28: one redux.sync on a 32-bit key
+        uint32_t k32 = valid ? ((uint32_t)total << 3) | (threadIdx.x & 7) : 0xffffffffu;
+        k32 = __reduce_min_sync(0xffffffffu, k32);
+        best_total = (long long)(k32 >> 3);
+        return k32 == 0xffffffffu ? -1 : (int)(k32 & 7);
+    }
     unsigned long long key = valid ? ((unsigned long long)total << 3) | (threadIdx.x & 7) : ~0ull;
 #pragma unroll
     for (int o = 1; o < 8; o <<= 1) {
@@ -330,7 +339,8 @@ template <bool BAND, bool TABLE>
 __global__ void __launch_bounds__(32) k_search(SearchParams p) {
     extern __shared__ __align__(16) uint8_t smem[];
     double* bits = (double*)smem;                 // 256 doubles
-    uint8_t* curbuf = smem + 256 * sizeof(double);  // 2 x 256 bytes
+    int* nc32s = (int*)(smem + 256 * sizeof(double));  // 64 x 64 NEW costs (small mode)
+    uint8_t* curbuf = smem + 256 * sizeof(double) + 64 * 64 * 4;  // 2 x 256 bytes
     uint16_t* tabbuf = (uint16_t*)(curbuf + 512);   // TABLE: 2 x tstride entries
     uint8_t* refmem = curbuf + 512 + (TABLE ? 4 * p.tstride : 0);  // band or window (+16 bytes slack)
     const int side = 2 * p.sr + 1;
@@ -340,6 +350,10 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
     const int MARGIN = (sr + 1 + 15) & ~15;
     const int BWB = p.W + 2 * MARGIN;
     for (int i = lane; i < 256; i += 32) bits[i] = p.mvbits[i];
+    const bool small = p.small != 0;
+    const int* nc32 = small ? nc32s : nullptr;
+    if (small)
+        for (int i = lane; i < 64 * 64; i += 32) nc32s[i] = p.newcost32[i];
     const int yy = lane >> 1;         // this lane's row inside the MB
     const int xoff = (lane & 1) * 8;  // and its 8-pixel half
     const unsigned long long tagbits = (unsigned long long)(p.tag & 0xffffu) << 48;
@@ -512,10 +526,10 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                 for (int i = 0; i < 5; i++)
                     if (lane == i + 1) { kx = PX[i]; ky = PY[i]; kv = SV[i + 1]; }
                 long long ksad = kv ? (long long)tb[(ky + sr) * side + kx + sr] : 0;
-                long long kcost = kv ? mv_cost(kx, ky, cc, p, bits) : 0;
+                long long kcost = kv ? mv_cost(kx, ky, cc, p, bits, nc32) : 0;
                 long long zero_sad = (long long)tb[sr * side + sr];
                 long long scost;
-                int w = argmin8(ksad + kcost, kv && lane < 6, scost);
+                int w = argmin8(ksad + kcost, kv && lane < 6, scost, small);
                 bool skip_int = p.zthr > 0 && zero_sad <= p.zthr;
                 if (skip_int) {
                     scost = zero_sad + __shfl_sync(0xffffffffu, kcost, 0);
@@ -532,9 +546,9 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                     for (;;) {  // large hexagon (enc/motion/scalar.rs:694-729)
                         int dx = sdx + hxl, dy = sdy + hyl;
                         bool v = lane < 6 && abs(dx) <= sr && abs(dy) <= sr;
-                        long long t = v ? (long long)tb[(dy + sr) * side + dx + sr] + mv_cost(dx, dy, cc, p, bits) : 0;
+                        long long t = v ? (long long)tb[(dy + sr) * side + dx + sr] + mv_cost(dx, dy, cc, p, bits, nc32) : 0;
                         long long bt;
-                        int wk = argmin8(t, v, bt);
+                        int wk = argmin8(t, v, bt, small);
                         if (wk < 0 || bt >= scost) break;
                         scost = bt;
                         sdx = __shfl_sync(0xffffffffu, dx, wk);
@@ -549,9 +563,9 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                         const int dyl = (int)(int8_t)(0xFF010000u >> (8 * min(lane, 3)));
                         int dx = sdx + dxl, dy = sdy + dyl;
                         bool v = lane < 4 && abs(dx) <= sr && abs(dy) <= sr;
-                        long long t = v ? (long long)tb[(dy + sr) * side + dx + sr] + mv_cost(dx, dy, cc, p, bits) : 0;
+                        long long t = v ? (long long)tb[(dy + sr) * side + dx + sr] + mv_cost(dx, dy, cc, p, bits, nc32) : 0;
                         long long bt;
-                        int wk = argmin8(t, v, bt);
+                        int wk = argmin8(t, v, bt, small);
                         if (wk >= 0 && bt < scost) {
                             scost = bt;
                             sdx = __shfl_sync(0xffffffffu, dx, wk);
@@ -568,7 +582,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
     #pragma unroll
                     for (int i = 0; i < 5; i++)
                         if (lane == i + 1) { kx = PX[i]; ky = PY[i]; kv = SV[i + 1]; }
-                    if (kv) my_cost = mv_cost(kx, ky, cc, p, bits);
+                    if (kv) my_cost = mv_cost(kx, ky, cc, p, bits, nc32);
                 }
                 unsigned part[6];
                 part[0] = sad_int_part(view, x0, y0, p.W, p.H, 0, 0, yy, xoff, c0, c1);
@@ -605,7 +619,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                         long long lc = 0;
                         if (lane < 6) {
                             int dx = cx + hxl, dy = cy + hyl;
-                            if (abs(dx) <= sr && abs(dy) <= sr) lc = mv_cost(dx, dy, cc, p, bits);
+                            if (abs(dx) <= sr && abs(dy) <= sr) lc = mv_cost(dx, dy, cc, p, bits, nc32);
                         }
                         unsigned hp[6];
     #pragma unroll
@@ -638,7 +652,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                     long long lc = 0;
                     if (lane < 4) {
                         int dx = cx + dxl, dy = cy + dyl;
-                        if (abs(dx) <= sr && abs(dy) <= sr) lc = mv_cost(dx, dy, cc, p, bits);
+                        if (abs(dx) <= sr && abs(dy) <= sr) lc = mv_cost(dx, dy, cc, p, bits, nc32);
                     }
                     unsigned dp[4];
     #pragma unroll
@@ -826,7 +840,7 @@ static size_t search_smem(int sr, int W, bool band, bool table) {
     size_t ws = 18 + 2 * (size_t)sr;
     size_t margin = ((size_t)sr + 1 + 15) & ~(size_t)15;
     size_t ref = band ? ws * ((size_t)W + 2 * margin) : ws * ws;
-    return 256 * sizeof(double) + 512 + (table ? 4 * (size_t)sad_table_stride(sr) : 0) + ref + 16;
+    return 256 * sizeof(double) + 64 * 64 * 4 + 512 + (table ? 4 * (size_t)sad_table_stride(sr) : 0) + ref + 16;
 }
 static const size_t SEARCH_SMEM_MAX = 200 * 1024;
 static bool search_use_band(int sr, int W) {
