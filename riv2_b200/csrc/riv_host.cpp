@@ -421,6 +421,7 @@ static void setup_device(riv_encoder* e) {
         e->newcost.alloc(nt.size() * sizeof(long long));
         CK(cudaMemcpy(e->newcost.p, nt.data(), nt.size() * sizeof(long long), cudaMemcpyHostToDevice));
         e->small_costs = mx < (1ll << 27) && Lq.lambda >= 0.0;
+        if (const char* v = getenv("RIV_SEARCH_SMALL")) e->small_costs = e->small_costs && atoi(v) != 0;
         std::vector<int> n32(64 * 64);
         for (int a = 0; a < 64; a++)
             for (int b = 0; b < 64; b++) n32[a * 64 + b] = (int)std::min<long long>(nt[a * 256 + b], INT32_MAX);
@@ -442,7 +443,7 @@ static void setup_device(riv_encoder* e) {
     CK(cudaMemcpy(e->ytab.p, yt, sizeof(yt), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(e->ctab.p, ct, sizeof(ct), cudaMemcpyHostToDevice));
     int g = 0;
-    CK(search_max_grid(c.search_range, (int)c.storage_width, e->table_ok, &g));
+    CK(search_max_grid(c.search_range, (int)c.storage_width, e->table_ok, e->small_costs, &g));
     if (g <= 0) throw std::runtime_error("search kernel cannot be made resident");
     e->search_grid = std::min(g, e->BH);
     // frame constants

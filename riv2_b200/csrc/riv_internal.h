@@ -84,7 +84,7 @@ bool search_use_table(int sr);
 int sad_table_stride(int sr);
 int launch_sad_table(const uint8_t* ref, const uint8_t* cur, int W, int H, int sr, uint16_t* tab, int tstride,
                      void* stream);
-int search_max_grid(int sr, int W, bool table, int* grid_out);
+int search_max_grid(int sr, int W, bool table, bool small, int* grid_out);
 size_t search_smem_bytes(int sr);
 int launch_predict(const uint8_t* ref, const MbOut* mb, uint8_t* pred, uint2* varsum, int W, int H, void* stream);
 int launch_aq(const uint2* varsum, int n, float base, const uint32_t* logfix, int nlog, const uint32_t* expfix,

@@ -97,6 +97,9 @@ struct CostCtx {
 };
 
 // estimate_mv_cost (enc/motion/scalar.rs:453-544)
+// SMALL: all costs < 2^27, |diff| < 64 entries from the shared 64x64 int32 table, the rest
+// from the exact i64 table in global memory.  Otherwise the i64 table (or f64 if absent).
+template <bool SMALL>
 __device__ __forceinline__ long long mv_cost(int dx, int dy, const CostCtx& c, const SearchParams& p,
                                              const double* bits, const int* nc32) {
     if (p.lambda_zero) return 0;
@@ -104,22 +107,11 @@ __device__ __forceinline__ long long mv_cost(int dx, int dy, const CostCtx& c, c
     if ((dx == c.nx && dy == c.ny) || (dx == c.rx && dy == c.ry) || (dx == c.mx && dy == c.my)) best = p.c15;
     if (dx == 0 && dy == 0) best = min(best, p.c05);
     const int ax = abs(dx - c.nx), ay = abs(dy - c.ny), bx = abs(dx - c.rx), by = abs(dy - c.ry);
-    if (nc32 != nullptr && ((ax | ay | bx | by) < 64))
-        return min(best, (long long)min(nc32[ax * 64 + ay], nc32[bx * 64 + by]));
-    if (p.newcost) {
-        long long a = __ldg(p.newcost + ax * 256 + ay);
-        long long b = __ldg(p.newcost + bx * 256 + by);
-        return min(best, min(a, b));
-    }
-    {
-        double b = __dadd_rn(__dadd_rn(6.0, bits[ax]), bits[ay]);
-        best = min(best, __double2ll_rz(__dmul_rn(p.lam2, b)));
-    }
-    {
-        double b = __dadd_rn(__dadd_rn(6.0, bits[bx]), bits[by]);
-        best = min(best, __double2ll_rz(__dmul_rn(p.lam2, b)));
-    }
-    return best;
+    if (SMALL && ((ax | ay | bx | by) < 64)) return min(best, (long long)min(nc32[ax * 64 + ay], nc32[bx * 64 + by]));
+    if (p.newcost) return min(best, min(__ldg(p.newcost + ax * 256 + ay), __ldg(p.newcost + bx * 256 + by)));
+    double ba = __dadd_rn(__dadd_rn(6.0, bits[ax]), bits[ay]);
+    double bb = __dadd_rn(__dadd_rn(6.0, bits[bx]), bits[by]);
+    return min(best, min(__double2ll_rz(__dmul_rn(p.lam2, ba)), __double2ll_rz(__dmul_rn(p.lam2, bb))));
 }
 
 // Unaligned 32-bit read from shared memory: two aligned words and a funnel shift.  The
@@ -312,8 +304,9 @@ int launch_sad_table(const uint8_t* ref, const uint8_t* cur, int W, int H, int s
 // with valid == false do not compete.  Totals are below 2^59 (the host enables the table
 // path only then), so (total << 3 | lane) is an exact sort key.  Returns the winning lane
 // (or -1) and the minimum total.
-__device__ __forceinline__ int argmin8(long long total, bool valid, long long& best_total, bool small) {
-    if (small) {  // totals < 2^28: one redux.sync on a 32-bit key
+template <bool SMALL>
+__device__ __forceinline__ int argmin8(long long total, bool valid, long long& best_total) {
+    if (SMALL) {  // totals < 2^28: one redux.sync on a 32-bit key
         uint32_t k32 = valid ? ((uint32_t)total << 3) | (threadIdx.x & 7) : 0xffffffffu;
         k32 = __reduce_min_sync(0xffffffffu, k32);
         best_total = (long long)(k32 >> 3);
@@ -335,7 +328,7 @@ __device__ __forceinline__ int argmin8(long long total, bool valid, long long& b
         if (p.prof != nullptr && lane == 0) p.prof[(size_t)idx * 8 + (k)] = clock64(); \
     } while (0)
 
-template <bool BAND, bool TABLE>
+template <bool BAND, bool TABLE, bool SMALL>
 __global__ void __launch_bounds__(32) k_search(SearchParams p) {
     extern __shared__ __align__(16) uint8_t smem[];
     double* bits = (double*)smem;                 // 256 doubles
@@ -350,9 +343,8 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
     const int MARGIN = (sr + 1 + 15) & ~15;
     const int BWB = p.W + 2 * MARGIN;
     for (int i = lane; i < 256; i += 32) bits[i] = p.mvbits[i];
-    const bool small = p.small != 0;
-    const int* nc32 = small ? nc32s : nullptr;
-    if (small)
+    const int* nc32 = nc32s;
+    if (SMALL)
         for (int i = lane; i < 64 * 64; i += 32) nc32s[i] = p.newcost32[i];
     const int yy = lane >> 1;         // this lane's row inside the MB
     const int xoff = (lane & 1) * 8;  // and its 8-pixel half
@@ -519,58 +511,51 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
             if (TABLE) {
                 // ---- table-driven integer search: lane k holds candidate k of a round; the
                 // in-order strict-'<' scan of the reference equals an argmin with the lowest
-                // index winning ties.
+                // index winning ties.  One loop for the three round kinds (seeds, hexagon,
+                // diamond) keeps a single MV-cost evaluation site.
                 int kx = 0, ky = 0;
                 bool kv = lane == 0;
 #pragma unroll
                 for (int i = 0; i < 5; i++)
                     if (lane == i + 1) { kx = PX[i]; ky = PY[i]; kv = SV[i + 1]; }
-                long long ksad = kv ? (long long)tb[(ky + sr) * side + kx + sr] : 0;
-                long long kcost = kv ? mv_cost(kx, ky, cc, p, bits, nc32) : 0;
-                long long zero_sad = (long long)tb[sr * side + sr];
-                long long scost;
-                int w = argmin8(ksad + kcost, kv && lane < 6, scost, small);
-                bool skip_int = p.zthr > 0 && zero_sad <= p.zthr;
-                if (skip_int) {
-                    scost = zero_sad + __shfl_sync(0xffffffffu, kcost, 0);
-                } else {
-                    sdx = __shfl_sync(0xffffffffu, kx, w);
-                    sdy = __shfl_sync(0xffffffffu, ky, w);
-                    long long wsad = __shfl_sync(0xffffffffu, ksad, w);
-                    if (p.pthr > 0 && wsad <= p.pthr) skip_int = true;
-                }
-                if (!skip_int) {
-                    const int hxl = (int)(int8_t)(0x01FFFEFF0102ull >> (8 * min(lane, 5)));
-                    const int hyl = (int)(int8_t)(0xFEFE00020200ull >> (8 * min(lane, 5)));
-                    int iter = 0;
-                    for (;;) {  // large hexagon (enc/motion/scalar.rs:694-729)
-                        int dx = sdx + hxl, dy = sdy + hyl;
-                        bool v = lane < 6 && abs(dx) <= sr && abs(dy) <= sr;
-                        long long t = v ? (long long)tb[(dy + sr) * side + dx + sr] + mv_cost(dx, dy, cc, p, bits, nc32) : 0;
-                        long long bt;
-                        int wk = argmin8(t, v, bt, small);
-                        if (wk < 0 || bt >= scost) break;
+                const int hxl = (int)(int8_t)(0x01FFFEFF0102ull >> (8 * min(lane, 5)));
+                const int hyl = (int)(int8_t)(0xFEFE00020200ull >> (8 * min(lane, 5)));
+                const int dxl = (int)(int8_t)(0x0000FF01u >> (8 * min(lane, 3)));
+                const int dyl = (int)(int8_t)(0xFF010000u >> (8 * min(lane, 3)));
+                long long scost = 0;
+                int phase = 0, iter = 0;
+                for (;;) {
+                    int cx, cy;
+                    bool v;
+                    if (phase == 0) { cx = kx; cy = ky; v = kv && lane < 6; }
+                    else if (phase == 1) { cx = sdx + hxl; cy = sdy + hyl; v = lane < 6 && abs(cx) <= sr && abs(cy) <= sr; }
+                    else { cx = sdx + dxl; cy = sdy + dyl; v = lane < 4 && abs(cx) <= sr && abs(cy) <= sr; }
+                    long long t = v ? (long long)tb[(cy + sr) * side + cx + sr] + mv_cost<SMALL>(cx, cy, cc, p, bits, nc32) : 0;
+                    long long bt;
+                    const int wk = argmin8<SMALL>(t, v, bt);
+                    if (phase == 0) {
+                        const long long zero_sad = (long long)tb[sr * side + sr];
+                        if (p.zthr > 0 && zero_sad <= p.zthr) break;  // stay at (0,0)
                         scost = bt;
-                        sdx = __shfl_sync(0xffffffffu, dx, wk);
-                        sdy = __shfl_sync(0xffffffffu, dy, wk);
+                        sdx = __shfl_sync(0xffffffffu, cx, wk);
+                        sdy = __shfl_sync(0xffffffffu, cy, wk);
+                        if (p.pthr > 0 && (long long)tb[(sdy + sr) * side + sdx + sr] <= p.pthr) break;
+                        phase = 1;
+                    } else if (phase == 1) {  // large hexagon (enc/motion/scalar.rs:694-729)
+                        if (wk < 0 || bt >= scost) { phase = 2; continue; }
+                        scost = bt;
+                        sdx = __shfl_sync(0xffffffffu, cx, wk);
+                        sdy = __shfl_sync(0xffffffffu, cy, wk);
                         if (++iter > 4096) {  // cost strictly decreases, so this is never reached
                             if (lane == 0) atomicOr(p.status, ST_HEX_CAP);
-                            break;
+                            phase = 2;
                         }
-                    }
-                    {  // small diamond (enc/motion/scalar.rs:731-756)
-                        const int dxl = (int)(int8_t)(0x0000FF01u >> (8 * min(lane, 3)));
-                        const int dyl = (int)(int8_t)(0xFF010000u >> (8 * min(lane, 3)));
-                        int dx = sdx + dxl, dy = sdy + dyl;
-                        bool v = lane < 4 && abs(dx) <= sr && abs(dy) <= sr;
-                        long long t = v ? (long long)tb[(dy + sr) * side + dx + sr] + mv_cost(dx, dy, cc, p, bits, nc32) : 0;
-                        long long bt;
-                        int wk = argmin8(t, v, bt, small);
+                    } else {  // small diamond (enc/motion/scalar.rs:731-756)
                         if (wk >= 0 && bt < scost) {
-                            scost = bt;
-                            sdx = __shfl_sync(0xffffffffu, dx, wk);
-                            sdy = __shfl_sync(0xffffffffu, dy, wk);
+                            sdx = __shfl_sync(0xffffffffu, cx, wk);
+                            sdy = __shfl_sync(0xffffffffu, cy, wk);
                         }
+                        break;
                     }
                 }
             } else {
@@ -582,7 +567,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
     #pragma unroll
                     for (int i = 0; i < 5; i++)
                         if (lane == i + 1) { kx = PX[i]; ky = PY[i]; kv = SV[i + 1]; }
-                    if (kv) my_cost = mv_cost(kx, ky, cc, p, bits, nc32);
+                    if (kv) my_cost = mv_cost<SMALL>(kx, ky, cc, p, bits, nc32);
                 }
                 unsigned part[6];
                 part[0] = sad_int_part(view, x0, y0, p.W, p.H, 0, 0, yy, xoff, c0, c1);
@@ -619,7 +604,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                         long long lc = 0;
                         if (lane < 6) {
                             int dx = cx + hxl, dy = cy + hyl;
-                            if (abs(dx) <= sr && abs(dy) <= sr) lc = mv_cost(dx, dy, cc, p, bits, nc32);
+                            if (abs(dx) <= sr && abs(dy) <= sr) lc = mv_cost<SMALL>(dx, dy, cc, p, bits, nc32);
                         }
                         unsigned hp[6];
     #pragma unroll
@@ -652,7 +637,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                     long long lc = 0;
                     if (lane < 4) {
                         int dx = cx + dxl, dy = cy + dyl;
-                        if (abs(dx) <= sr && abs(dy) <= sr) lc = mv_cost(dx, dy, cc, p, bits, nc32);
+                        if (abs(dx) <= sr && abs(dy) <= sr) lc = mv_cost<SMALL>(dx, dy, cc, p, bits, nc32);
                     }
                     unsigned dp[4];
     #pragma unroll
@@ -846,17 +831,18 @@ static const size_t SEARCH_SMEM_MAX = 200 * 1024;
 static bool search_use_band(int sr, int W) {
     return search_smem(sr, W, true, search_use_table(sr)) <= SEARCH_SMEM_MAX;
 }
-static const void* search_fn(bool band, bool table) {
-    if (band) return table ? (const void*)k_search<true, true> : (const void*)k_search<true, false>;
-    return table ? (const void*)k_search<false, true> : (const void*)k_search<false, false>;
+static const void* search_fn(bool band, bool table, bool small) {
+    if (table && small) return band ? (const void*)k_search<true, true, true> : (const void*)k_search<false, true, true>;
+    if (table) return band ? (const void*)k_search<true, true, false> : (const void*)k_search<false, true, false>;
+    return band ? (const void*)k_search<true, false, false> : (const void*)k_search<false, false, false>;
 }
 
 size_t search_smem_bytes(int sr) { return search_smem(sr, 0, false, search_use_table(sr)); }
 
-int search_max_grid(int sr, int W, bool table, int* grid_out) {
+int search_max_grid(int sr, int W, bool table, bool small, int* grid_out) {
     bool band = search_use_band(sr, W);
     size_t sm = search_smem(sr, W, band, table);
-    const void* fn = search_fn(band, table);
+    const void* fn = search_fn(band, table, table && small);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return (int)e;
     int per_sm = 0;
@@ -876,7 +862,7 @@ int launch_search(const SearchParams& p, int grid, void* stream) {
     void* args[] = {&q};
     // Cooperative launch: every CTA of the grid is co-resident, so the row-to-row waits
     // can always make progress.
-    cudaError_t e = cudaLaunchCooperativeKernel(search_fn(band, table), dim3(grid), dim3(32), args, sm,
+    cudaError_t e = cudaLaunchCooperativeKernel(search_fn(band, table, table && p.small), dim3(grid), dim3(32), args, sm,
                                                 (cudaStream_t)stream);
     return (int)e;
 }
