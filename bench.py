@@ -26,7 +26,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -98,52 +97,61 @@ def barrier(dist, device=None):
 # ---------------------------------------------------------------------------------------
 
 class ClockSampler:
-    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
-             "clocks_event_reasons.sw_power_cap"
+    """Samples the SM clock and the clock-event reasons of the benchmarked GPU every
+    ``period`` seconds while the timed region runs (NVML reads only; nothing is set).
+    The GPU is found by its PCI bus id, so the sample is of the device CUDA uses even
+    when CUDA_VISIBLE_DEVICES renumbers devices."""
 
-    def __init__(self, gpu_index: int):
-        self.samples = []
-        self.idx = gpu_index
-        self.proc = None
-        self.t = None
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
+
+    def __init__(self, cuda_index: int, period: float = 0.02):
+        self.idx, self.period = cuda_index, period
+        self.samples, self.max_mhz = [], None
+        self.stop_ev, self.t, self.nvml, self.h = threading.Event(), None, None, None
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            pr = torch.cuda.get_device_properties(self.idx)
+            bus = "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            try:
+                self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            except Exception:
+                self.h = pynvml.nvmlDeviceGetHandleByIndex(self.idx)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
         except Exception:
-            self.proc = None
+            self.nvml = None
+            return
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.samples.append([x.strip() for x in line.split(",")])
+    def _run(self):
+        while not self.stop_ev.is_set():
+            try:
+                mhz = self.nvml.nvmlDeviceGetClockInfo(self.h, self.nvml.NVML_CLOCK_SM)
+                rs = self.nvml.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.samples.append((float(mhz), int(rs)))
+            except Exception:
+                pass
+            self.stop_ev.wait(self.period)
 
     def stop(self):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
+        self.stop_ev.set()
         if self.t:
             self.t.join(timeout=2)
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for s in self.samples:
+        if self.nvml is not None:
             try:
-                sm.append(float(s[0]))
-                mx = float(s[1])
-                for k, n in enumerate(names):
-                    if s[4 + k].lower().startswith("active"):
-                        reasons.add(n)
-            except (ValueError, IndexError):
+                self.nvml.nvmlShutdown()
+            except Exception:
                 pass
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        sm = [m for m, _ in self.samples]
+        reasons = sorted({n for _, r in self.samples for n, bit in self.REASONS if r & bit})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(sm), "source": "nvml %d ms" % int(self.period * 1000)}
 
 
 # ---------------------------------------------------------------------------------------
@@ -233,9 +241,17 @@ def cpu_baseline(frames_host, nframes, iq, pq):
     return nframes / dt, dt
 
 
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_search launch at this workload
+# (ncu --set full, caches flushed before the pass): 14,647,296 + 6,656 bytes.  The excess
+# over the algorithmic bytes is the exhaustive SAD table read back from memory.
+SEARCH_TRAFFIC_BYTES = 14_647_296 + 6_656
+
+
 def roofline_entry(stage_us_per_frame: float):
     """Search/mode wavefront: algorithmic bytes per frame = read reference Y + current Y
-    (2 x 1920x1088) + write the per-MB record and output (8 + 20 bytes per MB)."""
+    (2 x 1920x1088) + write the per-MB record and output (8 + 20 bytes per MB).  The
+    kernel is bound by the latency of its serial MB chain (120 + 2 x 67 = 254 wavefront
+    steps at 1080p), not by HBM; the step time is reported beside the HBM fraction."""
     peaks = {}
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -243,10 +259,12 @@ def roofline_entry(stage_us_per_frame: float):
     peak = float(peaks.get("hbm_gbs", 6650.0))
     alg = 2 * 1920 * 1088 + MBS_PER_FRAME * (8 + 20)
     achieved = alg / (stage_us_per_frame * 1e-6) / 1e9
+    steps = (1920 // 16) + 2 * (1088 // 16 - 1)
     return {"bound": "hbm", "kernel": "k_search (motion search + RDO + mode wavefront)", "achieved": achieved,
-            "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+            "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": SEARCH_TRAFFIC_BYTES,
             "algorithmic_bytes_per_launch": alg, "launch_us": stage_us_per_frame,
-            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+            "critical_path": {"wavefront_steps": steps, "us_per_step": stage_us_per_frame / steps}}
 
 
 def main():
@@ -323,7 +341,7 @@ def main():
                                       [round((b - a) / K, 3) for a, b in zip(c0["host_ms"], c1["host_ms"])])),
         "roofline": roofline_entry(stage[2]),
         "cpu_baseline": cpu,
-        "clocks": r["clocks"],
+        "clocks": r["clocks"], "clocks_e2e": r["clocks_e2e"],
         "stream_bytes": r["stream_bytes"], "streams_equal_value_vs_e2e": r["streams_equal"],
     }
     print(json.dumps(line))
