@@ -134,6 +134,24 @@ riv_status riv_stage_rgb_to_yuv(const uint8_t* rgb, uint32_t dw, uint32_t dh, ui
                                 uint8_t* yuv_out);
 /* deblock_yuv420 (com/deblock.rs:189-202); mask: one byte per MB or NULL. */
 riv_status riv_stage_deblock(uint8_t* yuv, uint32_t w, uint32_t h, int level, int intra, const uint8_t* mask);
+/* No reference counterpart.  riv_stage_deblock without any device allocation: the planes
+ * and the optional mask are staged in one fixed device scratch area (a file-scope
+ * __device__ array of RIV_DEBLOCK_NOALLOC_MAX_BYTES bytes, 256-byte aligned) instead of
+ * memory allocated and freed on every call.  Same arguments and result as
+ * riv_stage_deblock, on the current CUDA device.
+ * Limit: w*h*3/2 bytes, plus (w/16)*(h/16) when mask != NULL, at most
+ * RIV_DEBLOCK_NOALLOC_MAX_BYTES (4 MiB: storage sizes up to 1920x1088); larger requests
+ * return RIV_ERR_FRAME and write the reason to errbuf (nullable, errbuf_len bytes).
+ * Set-up: the first call on a device looks up the scratch address
+ * (cudaGetSymbolAddress, device current); make that first call before any stream
+ * capture on that device.
+ * Zero state: nothing in the scratch has to start at zero; each call writes every byte
+ * it reads.
+ * Calls that overlap on one device (from several host threads) share the scratch and
+ * race: serialise them. */
+#define RIV_DEBLOCK_NOALLOC_MAX_BYTES (4u << 20)
+riv_status riv_stage_deblock_noalloc(uint8_t* yuv, uint32_t w, uint32_t h, int level, int intra,
+                                     const uint8_t* mask, char* errbuf, size_t errbuf_len);
 /* glibc-exact logf (which=0) / exp2f (which=1) on the device over n inputs. */
 riv_status riv_stage_libm(int which, const float* in, float* out, size_t n);
 /* Test hook: device state left by the most recent frame (synchronises the device; meant

@@ -1126,6 +1126,55 @@ riv_status riv_stage_deblock(uint8_t* yuv, uint32_t w, uint32_t h, int level, in
     return st;
 }
 
+// riv_stage_deblock without device allocation: staging in the fixed device scratch.  The
+// scratch address is looked up once per device, with that device current.
+static_assert(DEBLOCK_NOALLOC_MAX_BYTES == RIV_DEBLOCK_NOALLOC_MAX_BYTES, "scratch size must match the header");
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_scratch[64];
+
+static riv_status noalloc_fail(char* errbuf, size_t len, riv_status st, const char* msg) {
+    if (errbuf && len) snprintf(errbuf, len, "%s", msg);
+    return st;
+}
+
+riv_status riv_stage_deblock_noalloc(uint8_t* yuv, uint32_t w, uint32_t h, int level, int intra,
+                                     const uint8_t* mask, char* errbuf, size_t errbuf_len) {
+    if (errbuf && errbuf_len) errbuf[0] = 0;
+    if (!yuv || w == 0 || h == 0 || w % 16 || h % 16)
+        return noalloc_fail(errbuf, errbuf_len, RIV_ERR_FRAME, "planes must be non-null with width and height multiples of 16");
+    const size_t n = (size_t)w * h * 3 / 2, nm = (size_t)(w / 16) * (h / 16);
+    const size_t need = n + (mask ? nm : 0);
+    if (need > RIV_DEBLOCK_NOALLOC_MAX_BYTES) {
+        char msg[160];
+        snprintf(msg, sizeof msg, "%ux%u needs %zu bytes of scratch, more than the fixed %u (RIV_DEBLOCK_NOALLOC_MAX_BYTES)",
+                 w, h, need, (unsigned)RIV_DEBLOCK_NOALLOC_MAX_BYTES);
+        return noalloc_fail(errbuf, errbuf_len, RIV_ERR_FRAME, msg);
+    }
+    if (level <= 0) return RIV_OK;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+        return noalloc_fail(errbuf, errbuf_len, RIV_ERR_CUDA, "no usable current CUDA device");
+    uint8_t* scr = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_scratch[dev]) {
+            void* p = nullptr;
+            if (deblock_scratch_address(&p) != 0 || !p)
+                return noalloc_fail(errbuf, errbuf_len, RIV_ERR_CUDA, "cudaGetSymbolAddress of the deblock scratch failed");
+            g_noalloc_scratch[dev] = p;
+        }
+        scr = (uint8_t*)g_noalloc_scratch[dev];
+    }
+    int E, I, Hv;
+    deblock_thresholds(level, intra != 0, E, I, Hv);
+    if (cudaMemcpy(scr, yuv, n, cudaMemcpyHostToDevice) != cudaSuccess ||
+        (mask && cudaMemcpy(scr + n, mask, nm, cudaMemcpyHostToDevice) != cudaSuccess) ||
+        launch_deblock(scr, (int)w, (int)h, E, I, Hv, mask ? scr + n : nullptr, 0) != 0 ||
+        cudaMemcpy(yuv, scr, n, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return noalloc_fail(errbuf, errbuf_len, RIV_ERR_CUDA, "CUDA copy or launch failed");
+    return RIV_OK;
+}
+
 riv_status riv_stage_libm(int which, const float* in, float* out, size_t n) {
     LibmFix& F = libm_fix();
     if (!F.ok) return RIV_ERR_ENCODING_FAILED;

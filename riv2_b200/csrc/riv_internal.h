@@ -91,6 +91,10 @@ int launch_aq(const uint2* varsum, int n, float base, const uint32_t* logfix, in
               int nexp, float* lnv_scratch, float* qs, void* stream);
 int launch_residual(const ResidualParams& p, int nmb, void* stream);
 int launch_deblock(uint8_t* yuv, int W, int H, int E, int I, int Hev, const uint8_t* mask, void* stream);
+// Scratch of the no-allocation deblock entry point (a file-scope __device__ array of
+// DEBLOCK_NOALLOC_MAX_BYTES bytes); the address is valid on the current device.
+constexpr size_t DEBLOCK_NOALLOC_MAX_BYTES = (size_t)4 << 20;
+int deblock_scratch_address(void** out);
 // k_scan writes {coded MBs, coefficients} to hhdr (mapped host memory); k_pack fills the
 // device-side side info / EOB / coefficient buffers, copied back by DMA afterwards.
 int launch_compact(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coeffs, const uint8_t* eobs, int nmb,

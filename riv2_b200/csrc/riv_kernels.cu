@@ -1373,6 +1373,14 @@ int launch_deblock(uint8_t* yuv, int W, int H, int E, int I, int Hv, const uint8
     return (int)cudaGetLastError();
 }
 
+// Fixed device scratch of the no-allocation deblock entry point: the YUV planes and the
+// optional per-MB mask of one call are staged here instead of in memory allocated per
+// call.  Nothing in it has to start at zero (each call writes every byte it reads), and
+// calls that overlap on one device share it.
+static __device__ __align__(256) uint8_t g_deblock_scratch[DEBLOCK_NOALLOC_MAX_BYTES];
+
+int deblock_scratch_address(void** out) { return (int)cudaGetSymbolAddress(out, g_deblock_scratch); }
+
 // ---------------------------------------------------------------------------------
 // K8: per-MB side info and compaction of the coded MBs' coefficients for the host entropy
 // coder, written straight into mapped pinned host memory (no separate device->host copy).

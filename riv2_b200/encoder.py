@@ -109,7 +109,7 @@ EXPORTED_SYMBOLS = (
     "riv_finish", "riv_encoder_free", "riv_last_error", "riv_frame_count", "riv_last_recon", "riv_last_kernel_times",
     "riv_memwriter_new", "riv_memwriter_vtable", "riv_memwriter_size", "riv_memwriter_data", "riv_memwriter_free",
     "riv_stage_rgb_to_yuv", "riv_stage_deblock", "riv_stage_libm", "riv_libm_fixup_counts", "riv_dct_tables",
-    "riv_debug_frame_state", "riv_counters", "riv_host_times",
+    "riv_debug_frame_state", "riv_counters", "riv_host_times", "riv_stage_deblock_noalloc",
 )
 
 
@@ -140,6 +140,8 @@ def lib() -> C.CDLL:
     L.riv_memwriter_free.argtypes = [P]
     L.riv_stage_rgb_to_yuv.argtypes = [U8P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, U8P]
     L.riv_stage_deblock.argtypes = [U8P, C.c_uint32, C.c_uint32, C.c_int, C.c_int, U8P]
+    L.riv_stage_deblock_noalloc.argtypes = [U8P, C.c_uint32, C.c_uint32, C.c_int, C.c_int, U8P, C.c_char_p,
+                                            C.c_size_t]
     L.riv_stage_libm.argtypes = [C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_size_t]
     L.riv_libm_fixup_counts.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     L.riv_dct_tables.argtypes = [C.POINTER(C.c_int32), C.POINTER(C.c_int32)]

@@ -1,0 +1,79 @@
+"""The no-allocation deblock entry point (riv_stage_deblock_noalloc) against the existing
+riv_stage_deblock: identical planes over two calls in a row (the fixed device scratch
+carries nothing from one call to the next), and the size limit rejected with a message."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+MAX_BYTES = 4 << 20
+
+
+def _lib():
+    from riv2_b200 import encoder as E
+    return E.lib()
+
+
+def _u8(a):
+    return a.ctypes.data_as(C.POINTER(C.c_uint8))
+
+
+def _noalloc(yuv, w, h, level, intra, mask):
+    out = yuv.copy()
+    err = C.create_string_buffer(256)
+    m = None if mask is None else _u8(mask)
+    st = _lib().riv_stage_deblock_noalloc(_u8(out), w, h, level, int(intra), m, err, len(err))
+    return st, out, err.value.decode()
+
+
+def _existing(yuv, w, h, level, intra, mask):
+    out = yuv.copy()
+    m = None if mask is None else _u8(mask)
+    st = _lib().riv_stage_deblock(_u8(out), w, h, level, int(intra), m)
+    return st, out
+
+
+def _planes(w, h, seed):
+    rng = np.random.default_rng(seed)
+    n = w * h * 3 // 2
+    # blocky content with small steps at the MB edges, so the filter changes many samples
+    base = rng.integers(60, 200, size=n, dtype=np.int32)
+    noise = rng.integers(-3, 4, size=n, dtype=np.int32)
+    y = np.repeat(np.repeat(rng.integers(90, 110, size=(h // 16, w // 16)), 16, 0), 16, 1).reshape(-1)
+    base[: w * h] = y + noise[: w * h]
+    return np.clip(base, 0, 255).astype(np.uint8)
+
+
+def test_noalloc_rejects_oversize_and_bad_dims():
+    # no device call happens before these checks
+    w, h = 3840, 2160
+    st, _, msg = _noalloc(np.zeros(w * h * 3 // 2, np.uint8), w, h, 20, False, None)
+    assert st == 5 and "RIV_DEBLOCK_NOALLOC_MAX_BYTES" in msg and str(MAX_BYTES) in msg
+    st, _, msg = _noalloc(np.zeros(100 * 70 * 3 // 2, np.uint8), 100, 70, 20, False, None)
+    assert st == 5 and "multiples of 16" in msg
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("w,h,with_mask", [(352, 288, True), (1920, 1088, False), (1920, 1088, True)])
+def test_noalloc_matches_existing_entry_point_twice(w, h, with_mask):
+    rng = np.random.default_rng(w + h)
+    for call in range(2):  # two calls in a row, different content each time
+        yuv = _planes(w, h, seed=call * 7 + w)
+        mask = (rng.integers(0, 2, size=(w // 16) * (h // 16)).astype(np.uint8) if with_mask else None)
+        level, intra = (30 + 9 * call), bool(call)
+        st0, ref = _existing(yuv, w, h, level, intra, mask)
+        st1, out, msg = _noalloc(yuv, w, h, level, intra, mask)
+        assert st0 == 0 and st1 == 0, msg
+        assert not np.array_equal(ref, yuv), "the filter should change this content"
+        assert np.array_equal(out, ref), f"call {call}: {(out != ref).sum()} samples differ"
+
+
+@pytest.mark.gpu
+def test_noalloc_at_the_size_limit_edge():
+    # largest storage size the scratch takes with a mask: 1920x1088 (3,141,600 bytes)
+    w, h = 1920, 1088
+    assert w * h * 3 // 2 + (w // 16) * (h // 16) <= MAX_BYTES
+    yuv = _planes(w, h, seed=3)
+    st0, ref = _existing(yuv, w, h, 0, False, None)
+    st1, out, _ = _noalloc(yuv, w, h, 0, False, None)  # level 0: nothing to do
+    assert st0 == st1 == 0 and np.array_equal(out, yuv) and np.array_equal(ref, yuv)
