@@ -157,7 +157,7 @@ riv_status riv_stage_libm(int which, const float* in, float* out, size_t n);
 /* Test hook: device state left by the most recent frame (synchronises the device; meant
  * for pipeline_depth == 0).  what: 0 per-MB search/mode output (20 B/MB), 1 AQ steps
  * (f32/MB), 2 prediction (YUV), 3 converted input (YUV), 4 quantised coefficients
- * (384 x i16 per MB), 5 optimized skip (u8/MB), 6 search-kernel phase stamps (8 x i64 per
+ * (384 x i16 per MB), 5 optimized skip (u8/MB), 6 search-kernel phase stamps (16 x i64 per
  * MB; only when the encoder was created with RIV_PROFILE_SEARCH set in the environment).
  * Returns RIV_ERR_FRAME if `size` is short. */
 riv_status riv_debug_frame_state(riv_encoder* enc, int what, void* out, size_t size);

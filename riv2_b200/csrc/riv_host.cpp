@@ -388,7 +388,7 @@ static void setup_device(riv_encoder* e) {
     e->mbout.alloc((size_t)N * sizeof(MbOut));
     e->coded[0].alloc((size_t)N * 4);
     e->coded[1].alloc((size_t)N * 4);
-    e->rec.alloc((size_t)N * sizeof(MbRec));
+    e->rec.alloc((size_t)2 * N * sizeof(MbRec));  // raw-MV records, then coded-MV records
     e->varsum.alloc((size_t)N * sizeof(uint2));
     e->lnv.alloc((size_t)(N + 4) * sizeof(float));
     e->qs.alloc((size_t)N * sizeof(float));
@@ -473,7 +473,7 @@ static void setup_device(riv_encoder* e) {
     }
     e->coef_guess = (size_t)N * 384;  // half the dense size until the first frames are seen
     if (getenv("RIV_PROFILE_SEARCH")) {
-        e->prof.alloc((size_t)N * 8 * sizeof(long long));
+        e->prof.alloc((size_t)N * 16 * sizeof(long long));
         e->prof.zero(e->S);
     }
     e->cindex.alloc((size_t)N * 4);

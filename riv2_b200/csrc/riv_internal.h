@@ -48,12 +48,12 @@ struct SearchParams {
     int rdo_allow;
     const uint16_t* tab;  // exhaustive integer-SAD table (when search_use_table), tstride entries per MB
     int tstride;
-    MbRec* rec;
+    MbRec* rec;       // 2 x BW*BH wavefront records: raw MVs (search), then coded MVs (mode)
     unsigned tag;
     MbOut* out;
     unsigned* status;
     long long spin_limit;
-    long long* prof;  // optional: 8 clock64 stamps per MB (phase boundaries), nullptr = off
+    long long* prof;  // optional: 16 words per MB (phase clock stamps, hexagon rounds), nullptr = off
 };
 
 struct ResidualParams {

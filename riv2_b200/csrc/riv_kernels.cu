@@ -323,33 +323,382 @@ __device__ __forceinline__ int argmin8(long long total, bool valid, long long& b
     return key == ~0ull ? -1 : (int)(key & 7);
 }
 
+#define RIV_PUT(k, v)                                                      \
+    do {                                                                    \
+        if (p.prof != nullptr && lane == 0) p.prof[(size_t)idx * 16 + (k)] = (v); \
+    } while (0)
 #define RIV_STAMP(k)                                                        \
     do {                                                                    \
-        if (p.prof != nullptr && lane == 0) p.prof[(size_t)idx * 8 + (k)] = clock64(); \
+        if (p.prof != nullptr && lane == 0) p.prof[(size_t)idx * 16 + (k)] = clock64(); \
     } while (0)
 
+// ---- search warp -> mode warp handoff through a shared-memory ring (one CTA per MB row)
+// Slot word: [63:49] (n + 1) mod 2^15 for the n-th MB of the CTA, [48] failure, [47:32] best
+// SAD (at most 255 * 256), [31:0] raw MV (dx, dy, sx, sy as bytes).  Tag and payload share
+// one 64-bit word, so a single volatile store publishes both.
+constexpr int HAND_RING = 64;
+constexpr unsigned long long HAND_FAIL = 1ull << 48;
+
+__device__ __forceinline__ bool hand_put(unsigned long long* hand, volatile int* done, int n,
+                                         unsigned long long payload, long long limit) {
+    long long spins = 0;
+    while (n - *done >= HAND_RING) {  // the slot's previous MB has not been taken yet
+        if (++spins > limit) return false;
+        __nanosleep(32);
+    }
+    volatile unsigned long long* h = hand + (n & (HAND_RING - 1));
+    *h = ((unsigned long long)((n + 1) & 0x7fff) << 49) | payload;
+    return true;
+}
+
+__device__ __forceinline__ bool hand_get(const unsigned long long* hand, int n, unsigned long long& w,
+                                         long long limit) {
+    const volatile unsigned long long* h = hand + (n & (HAND_RING - 1));
+    const unsigned long long want = (unsigned long long)((n + 1) & 0x7fff) << 49;
+    unsigned long long v = *h;
+    long long spins = 0;
+    while ((v & ~((1ull << 49) - 1)) != want) {
+        if (++spins > limit) return false;
+        if (spins > 64) __nanosleep(16);
+        v = *h;
+    }
+    w = v;
+    return true;
+}
+
+// Bounded wait for a wavefront record of this frame (tag in bits 63:48).
+__device__ __forceinline__ bool rec_wait(const unsigned long long* rp, unsigned long long tagbits,
+                                         unsigned long long& v, long long limit) {
+    v = ld_rec(rp);
+    long long spins = 0;
+    while ((v & 0xffff000000000000ull) != tagbits) {
+        if (++spins > limit) return false;
+        __nanosleep(20);
+        v = ld_rec(rp);
+    }
+    return true;
+}
+
+// The second warp of each row CTA: RDO skip (enc/rdo.rs:140-178) and the MV mode decision on
+// the coded (reconstructed) neighbours (enc/encoder.rs:459-733, res/mv_predictor.rs:59-272)
+// for the MBs the search warp hands over, in raster order.  It publishes the coded-MV records
+// the next row's mode warp reads (second half of p.rec) and the per-MB output.  None of this
+// feeds the search, so it runs beside the search chain instead of on it.
+__device__ __forceinline__ void mode_warp(const SearchParams& p, const unsigned long long* hand, volatile int* hand_done,
+                                       unsigned long long tagbits) {
+    const int lane = threadIdx.x & 31;
+    MbRec* rc = p.rec + (size_t)p.BW * p.BH;
+    auto rec_cod = [](unsigned long long v) {
+        return MvT{(int)(int8_t)(v >> 24), (int)(int8_t)(v >> 16), (int)(int8_t)(v >> 8), (int)(int8_t)v};
+    };
+    const bool has_tm = p.prev_coded != nullptr;
+    int n = 0;
+    for (int r = blockIdx.x; r < p.BH; r += gridDim.x) {
+        MvT L_cod{0, 0, 0, 0};
+        unsigned long long vT = 0, vTL = 0;
+        for (int bx = 0; bx < p.BW; bx++) {
+            const int idx = r * p.BW + bx;
+            unsigned long long hw = 0, vTR = 0;
+            int st = 0;  // 0 ok, 1 wait expired, 2 the search warp gave up
+            if (lane == 0) {
+                if (!hand_get(hand, n, hw, p.spin_limit)) st = 1;
+                else if (hw & HAND_FAIL) st = 2;
+                if (st == 0 && r > 0) {
+                    if (bx == 0 && !rec_wait(rc + (size_t)(r - 1) * p.BW, tagbits, vT, p.spin_limit)) st = 1;
+                    if (st == 0 && bx + 1 < p.BW &&
+                        !rec_wait(rc + (size_t)(r - 1) * p.BW + bx + 1, tagbits, vTR, p.spin_limit))
+                        st = 1;
+                }
+                if (st == 0) *hand_done = n + 1;
+            }
+            st = __shfl_sync(0xffffffffu, st, 0);
+            if (st != 0) {
+                if (lane == 0 && st == 1) atomicOr(p.status, ST_WAIT_TIMEOUT);
+                return;
+            }
+            n++;
+            hw = __shfl_sync(0xffffffffu, hw, 0);
+            vT = __shfl_sync(0xffffffffu, vT, 0);
+            vTR = __shfl_sync(0xffffffffu, vTR, 0);
+            const MvT raw{(int)(int8_t)hw, (int)(int8_t)(hw >> 8), (int)(int8_t)(hw >> 16), (int)(int8_t)(hw >> 24)};
+            const long long best_sad = (long long)((hw >> 32) & 0xffff);
+            const bool has_t = r > 0, has_l = bx > 0, has_tl = r > 0 && bx > 0, has_tr = r > 0 && bx + 1 < p.BW;
+            MvT Tm_cod{0, 0, 0, 0};
+            if (has_tm) {
+                const char4 pc = *(const char4*)(p.prev_coded + 4 * idx);
+                Tm_cod = MvT{pc.x, pc.y, pc.z, pc.w};
+            }
+
+            // ---- RDO skip decision (enc/rdo.rs:140-178)
+            bool int_al = raw.sx == 0 && raw.sy == 0;
+            double satd = (double)best_sad;
+            double skip_cost = __dadd_rn(satd, __dmul_rn(p.rdo_lambda, p.rdo_skip_bits));
+            double est = __dadd_rn(p.rdo_icpt, __dmul_rn(p.rdo_slope, satd));
+            if (est < 0.0) est = 0.0;
+            double coded_cost = __dadd_rn(__dmul_rn(satd, p.rdo_ret), __dmul_rn(p.rdo_lambda, __dadd_rn(p.rdo_keep_bits, est)));
+            bool rdo_skip = p.rdo_allow && int_al && !(satd > p.rdo_guard) && (skip_cost <= coded_cost);
+
+            // ---- mode decision on the coded neighbours
+            MvT cT = has_t ? rec_cod(vT) : MvT{0, 0, 0, 0}, cTR = has_tr ? rec_cod(vTR) : MvT{0, 0, 0, 0},
+                cTL = has_tl ? rec_cod(vTL) : MvT{0, 0, 0, 0};
+            const MvT zero{0, 0, 0, 0};
+            MvT nearest = zero, nearm = zero;
+            {
+                const MvT CS[5] = {L_cod, cT, cTR, cTL, Tm_cod};
+                const bool PV[5] = {has_l, has_t, has_tr, has_tl, has_tm};
+                int nu = 0;
+#pragma unroll
+                for (int i = 0; i < 5; i++) {
+                    bool take = PV[i] && (nu == 0 || (nu == 1 && !mv_eq(CS[i], nearest)));
+                    if (take && nu == 0) nearest = CS[i];
+                    else if (take && nu == 1) nearm = CS[i];
+                    nu += take ? 1 : 0;
+                }
+            }
+            MvT temporal = has_tm ? Tm_cod : zero;
+            const int mx = raw.dx * 2 + raw.sx, my = raw.dy * 2 + raw.sy;
+            auto hpeq = [&](const MvT& t) { return mx == t.dx * 2 + t.sx && my == t.dy * 2 + t.sy; };
+            int mode;
+            if (raw.dx == 0 && raw.dy == 0 && raw.sx == 0 && raw.sy == 0) mode = 0;  // Zero
+            else if (hpeq(nearest)) mode = 1;
+            else if (hpeq(nearm)) mode = 2;
+            else if (has_tr && hpeq(cTR)) mode = 3;
+            else if (has_tl && hpeq(cTL)) mode = 4;
+            else if (hpeq(temporal)) mode = 6;
+            else mode = 5;  // New
+            int chosen = 0, rdx = 0, rdy = 0;
+            MvT coded = raw;
+            if (mode == 5) {
+                const MvT bases[5] = {nearest, nearm, cTR, cTL, temporal};
+                const bool hasb[5] = {true, true, has_tr, has_tl, true};
+                const int selbits[5] = {1, 2, 3, 4, 4};
+                unsigned best = 0xffffffffu;
+                int bbx = nearest.dx, bby = nearest.dy;
+#pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    if (!hasb[k]) continue;
+                    int ddx = sat8(raw.dx - bases[k].dx), ddy = sat8(raw.dy - bases[k].dy);
+                    unsigned cst = (unsigned)(selbits[k] + comp_bits(ddx) + comp_bits(ddy));
+                    if (cst < best) { best = cst; chosen = k; bbx = bases[k].dx; bby = bases[k].dy; }
+                }
+                rdx = sat8(raw.dx - bbx);
+                rdy = sat8(raw.dy - bby);
+                coded.dx = sat8(bbx + rdx);
+                coded.dy = sat8(bby + rdy);
+            } else if (mode == 1) coded = nearest;
+            else if (mode == 2) coded = nearm;
+            else if (mode == 3) coded = cTR;
+            else if (mode == 4) coded = cTL;
+            else if (mode == 6) coded = temporal;
+            uint8_t flags = 0;
+            if (mode == 5) flags = (raw.sx == 1 ? 0x01 : 0) | (raw.sy == 1 ? 0x04 : 0);
+            if (rdo_skip) flags |= 0x40;
+
+            RIV_STAMP(5);
+            // ---- publish
+            if (lane == 0) {
+                unsigned long long rv = tagbits | ((unsigned long long)(uint8_t)coded.dx << 24) |
+                                        ((unsigned long long)(uint8_t)coded.dy << 16) |
+                                        ((unsigned long long)(uint8_t)coded.sx << 8) | (unsigned long long)(uint8_t)coded.sy;
+                st_rec(rc + idx, rv);
+                MbOut o;
+                o.raw[0] = (int8_t)raw.dx; o.raw[1] = (int8_t)raw.dy; o.raw[2] = (int8_t)raw.sx; o.raw[3] = (int8_t)raw.sy;
+                o.coded[0] = (int8_t)coded.dx; o.coded[1] = (int8_t)coded.dy;
+                o.coded[2] = (int8_t)coded.sx; o.coded[3] = (int8_t)coded.sy;
+                o.rdelta[0] = (int8_t)rdx; o.rdelta[1] = (int8_t)rdy;
+                o.mode = (uint8_t)mode; o.base = (uint8_t)chosen; o.flags = flags; o.rdo_skip = rdo_skip ? 1 : 0;
+                o.pad[0] = o.pad[1] = 0;
+                o.best_sad = (int32_t)best_sad;
+                p.out[idx] = o;
+            }
+            RIV_STAMP(6);
+            L_cod = coded;
+            vTL = vT;
+            vT = vTR;
+        }
+    }
+}
+
+// ---- mbarrier and bulk-copy helpers (sm_90+ PTX; no multicast)
+__device__ __forceinline__ uint32_t sa32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sa32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+    unsigned long long st;
+    asm volatile("mbarrier.arrive.shared::cta.b64 %0, [%1];" : "=l"(st) : "r"(sa32(bar)) : "memory");
+    (void)st;
+}
+__device__ __forceinline__ void mbar_arrive_tx(unsigned long long* bar, unsigned tx) {
+    unsigned long long st;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;" : "=l"(st) : "r"(sa32(bar)), "r"(tx) : "memory");
+    (void)st;
+}
+__device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(sa32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait of the whole warp for a completed phase; false when the wait gave up.
+__device__ __forceinline__ bool mbar_wait_warp(unsigned long long* bar, unsigned parity, long long limit) {
+    long long spins = 0;
+    while (!__all_sync(0xffffffffu, mbar_test(bar, parity))) {
+        if (++spins > limit) return false;
+    }
+    return true;
+}
+// Global -> shared bulk copy completing on an mbarrier (16-byte aligned, size a multiple of 16).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(sa32(dst)),
+                 "l"(src), "r"(bytes), "r"(sa32(bar))
+                 : "memory");
+}
+
+// Staging ring of the band+table search (LD_RING MBs ahead): per slot the MB's SAD-table row
+// (2*tstride bytes), its 16x16 current block and the previous frame's coded MV (4 bytes).
+constexpr int LD_RING = 4;
+__host__ __device__ inline int ld_slot_bytes(int tstride) { return 2 * tstride + 256 + 16; }
+
+// The third warp of each row CTA (band + table instantiations): fills the MB-row reference
+// band once per row (one bulk copy per band row plus the replicated edge margins) and, up to
+// LD_RING MBs ahead of the search warp, each MB's table row, current block and temporal MV,
+// so that no copy is issued on the search chain.  ctl[0] = MBs the search warp has released,
+// ctl[1] = rows it has finished, ctl[2] = abort.
+__device__ __forceinline__ void loader_warp(const SearchParams& p, unsigned long long* fullb, unsigned long long* bandb,
+                                            volatile int* ctl, uint8_t* slots, uint8_t* band) {
+    const int lane = threadIdx.x & 31;
+    const int sr = p.sr, WS = 18 + 2 * sr, MARGIN = (sr + 1 + 15) & ~15, BWB = p.W + 2 * MARGIN;
+    const int SLOT = ld_slot_bytes(p.tstride);
+    const unsigned tab_bytes = 2u * (unsigned)p.tstride;
+    int n = 0, rows = 0;
+    bool abort = false;
+    auto wait_ctl = [&](int which, int target) {  // lane 0 polls; the answer is warp-uniform
+        int ok = 1;
+        if (lane == 0) {
+            long long spins = 0;
+            while (ctl[which] < target) {
+                if (ctl[2] != 0 || ++spins > p.spin_limit) { ok = 0; break; }
+                __nanosleep(64);
+            }
+        }
+        return __shfl_sync(0xffffffffu, ok, 0) != 0;
+    };
+    for (int r = blockIdx.x; r < p.BH && !abort; r += gridDim.x) {
+        const int wy0 = r * 16 - sr - 1;
+        if (rows > 0 && !wait_ctl(1, rows)) { abort = true; break; }
+        // ---- the band: rows wy0 .. wy0+WS-1 (edge-clamped), columns -MARGIN .. W+MARGIN-1
+        for (int i = lane; i < WS; i += 32) {
+            const int gy = min(max(wy0 + i, 0), p.H - 1);
+            const uint8_t* src = p.ref_y + (size_t)gy * p.W;
+            uint8_t* dst = band + (size_t)i * BWB;
+            bulk_g2s(dst + MARGIN, src, (unsigned)p.W, bandb);
+            const uint4 l = make_uint4(src[0] * 0x01010101u, 0, 0, 0), rr = make_uint4(src[p.W - 1] * 0x01010101u, 0, 0, 0);
+            const uint4 lv = make_uint4(l.x, l.x, l.x, l.x), rv = make_uint4(rr.x, rr.x, rr.x, rr.x);
+            for (int c = 0; c < MARGIN; c += 16) {
+                *(uint4*)(dst + c) = lv;
+                *(uint4*)(dst + MARGIN + p.W + c) = rv;
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive_tx(bandb, (unsigned)(WS * p.W));
+        else mbar_arrive(bandb);
+        // ---- per-MB staging
+        for (int bx = 0; bx < p.BW; bx++) {
+            const int idx = r * p.BW + bx;
+            const int s = n & (LD_RING - 1);
+            if (n >= LD_RING && !wait_ctl(0, n - LD_RING + 1)) { abort = true; break; }
+            uint8_t* slot = slots + (size_t)s * SLOT;
+            if (lane < 16)
+                bulk_g2s(slot + tab_bytes + lane * 16, p.cur_y + (size_t)(r * 16 + lane) * p.W + bx * 16, 16u, fullb + s);
+            if (lane == 0) {
+                bulk_g2s(slot, p.tab + (size_t)idx * p.tstride, tab_bytes, fullb + s);
+                const int tm = p.prev_coded ? *(const int*)(p.prev_coded + 4 * (size_t)idx) : 0;
+                *(int*)(slot + tab_bytes + 256) = tm;
+                mbar_arrive_tx(fullb + s, tab_bytes + 256u);
+            }
+            __syncwarp();
+            n++;
+        }
+        rows++;
+    }
+    // never leave with copies in flight: the last use of every slot and the last band fill
+    if (lane == 0) {
+        for (int k = max(0, n - LD_RING); k < n; k++) {
+            long long spins = 0;
+            while (!mbar_test(fullb + (k & (LD_RING - 1)), (unsigned)((k / LD_RING) & 1)) && ++spins <= p.spin_limit) {}
+        }
+        if (rows > 0) {
+            long long spins = 0;
+            while (!mbar_test(bandb, (unsigned)((rows - 1) & 1)) && ++spins <= p.spin_limit) {}
+        }
+        if (abort && ctl[2] == 0) atomicOr(p.status, ST_WAIT_TIMEOUT);
+    }
+}
+
 template <bool BAND, bool TABLE, bool SMALL>
-__global__ void __launch_bounds__(32) k_search(SearchParams p) {
+__global__ void __launch_bounds__(96, 1) k_search(SearchParams p) {
+    // FAST (band + table): three warps -- search chain, mode decision, loader.  Otherwise the
+    // search warp stages its own data with cp.async and the third warp is not launched.
+    constexpr bool FAST = BAND && TABLE;
     extern __shared__ __align__(16) uint8_t smem[];
     double* bits = (double*)smem;                 // 256 doubles
     int* nc32s = (int*)(smem + 256 * sizeof(double));  // 64 x 64 NEW costs (small mode)
-    uint8_t* curbuf = smem + 256 * sizeof(double) + 64 * 64 * 4;  // 2 x 256 bytes
+    unsigned long long* hand = (unsigned long long*)(smem + 256 * sizeof(double) + 64 * 64 * 4);  // HAND_RING
+    volatile int* hand_done = (volatile int*)(hand + HAND_RING);  // MBs the mode warp has taken
+    uint8_t* after_hand = (uint8_t*)(hand + HAND_RING) + 16;
+    // FAST layout: LD_RING full barriers, the band barrier, loader control words, the slots
+    unsigned long long* fullb = (unsigned long long*)after_hand;
+    unsigned long long* bandb = fullb + LD_RING;
+    volatile int* ld_ctl = (volatile int*)(bandb + 1);
+    uint8_t* slots = after_hand + 64;
+    // other layouts: double-buffered current block and table row
+    uint8_t* curbuf = after_hand;  // 2 x 256 bytes
     uint16_t* tabbuf = (uint16_t*)(curbuf + 512);   // TABLE: 2 x tstride entries
-    uint8_t* refmem = curbuf + 512 + (TABLE ? 4 * p.tstride : 0);  // band or window (+16 bytes slack)
+    uint8_t* refmem = FAST ? slots + LD_RING * ld_slot_bytes(p.tstride)
+                           : curbuf + 512 + (TABLE ? 4 * p.tstride : 0);  // band or window (+16 bytes slack)
     const int side = 2 * p.sr + 1;
-    const int lane = threadIdx.x;
+    const int lane = threadIdx.x & 31;
     const int sr = p.sr;
     const int WS = 18 + 2 * sr;
     const int MARGIN = (sr + 1 + 15) & ~15;
     const int BWB = p.W + 2 * MARGIN;
-    for (int i = lane; i < 256; i += 32) bits[i] = p.mvbits[i];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) bits[i] = p.mvbits[i];
     const int* nc32 = nc32s;
     if (SMALL)
-        for (int i = lane; i < 64 * 64; i += 32) nc32s[i] = p.newcost32[i];
+        for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x) nc32s[i] = p.newcost32[i];
+    for (int i = threadIdx.x; i < HAND_RING; i += blockDim.x) hand[i] = 0ull;
+    if (threadIdx.x == 0) {
+        *hand_done = 0;
+        if (FAST) {
+            for (int i = 0; i < LD_RING; i++) mbar_init(fullb + i, 1);
+            mbar_init(bandb, 32);
+            ld_ctl[0] = ld_ctl[1] = ld_ctl[2] = 0;
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+    }
+    __syncthreads();
+    const unsigned long long tagbits = (unsigned long long)(p.tag & 0xffffu) << 48;
+    if (threadIdx.x >= 64) {
+        if (FAST) loader_warp(p, fullb, bandb, ld_ctl, slots, refmem);
+        return;
+    }
+    if (threadIdx.x >= 32) {
+        mode_warp(p, hand, hand_done, tagbits);
+        return;
+    }
+    int ln = 0;      // MBs taken from the loader (FAST)
+    int lrows = 0;   // rows finished (FAST)
+    auto abort_loader = [&]() {
+        if (FAST && lane == 0) ld_ctl[2] = 1;
+    };
     const int yy = lane >> 1;         // this lane's row inside the MB
     const int xoff = (lane & 1) * 8;  // and its 8-pixel half
-    const unsigned long long tagbits = (unsigned long long)(p.tag & 0xffffu) << 48;
     bool failed = false;
+    int hn = 0;  // MBs handed to the mode warp so far
 
     for (int r = blockIdx.x; r < p.BH; r += gridDim.x) {
         const int y0 = r * 16;
@@ -358,39 +707,64 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
         // ---- prologue: reference columns of MB 0 and its current block
         int c_done = -1;
         auto c_hi = [&](int bx) { return (16 * bx + 16 + sr + MARGIN) >> 4; };
-        if (BAND) {
+        if (FAST) {
+            if (!mbar_wait_warp(bandb, (unsigned)(lrows & 1), p.spin_limit)) {
+                if (lane == 0) {
+                    atomicOr(p.status, ST_WAIT_TIMEOUT);
+                    hand_put(hand, hand_done, hn, HAND_FAIL, p.spin_limit);
+                }
+                abort_loader();
+                return;
+            }
+        } else if (BAND) {
             for (int c = 0; c <= c_hi(0); c++) fill_chunk(refmem, BWB, WS, c, MARGIN, wy0, p.ref_y, p.W, p.H, lane);
             c_done = c_hi(0);
         }
-        if (lane < 16) cp_async16(curbuf + lane * 16, p.cur_y + (size_t)(y0 + lane) * p.W);
-        if (TABLE)
-            for (int i = lane; i < p.tstride / 8; i += 32)
-                cp_async16(tabbuf + i * 8, p.tab + (size_t)(r * p.BW) * p.tstride + i * 8);
-        cp_async_commit();
+        if (!FAST) {
+            if (lane < 16) cp_async16(curbuf + lane * 16, p.cur_y + (size_t)(y0 + lane) * p.W);
+            if (TABLE)
+                for (int i = lane; i < p.tstride / 8; i += 32)
+                    cp_async16(tabbuf + i * 8, p.tab + (size_t)(r * p.BW) * p.tstride + i * 8);
+            cp_async_commit();
+        }
 
-        MvT L_raw{0, 0, 0, 0}, L_cod{0, 0, 0, 0};
+        MvT L_raw{0, 0, 0, 0};
         unsigned long long recT = 0, recTL = 0, pref = 0;
         for (int bx = 0; bx < p.BW; bx++) {
             const int x0 = bx * 16;
             const int idx = r * p.BW + bx;
             RIV_STAMP(0);
-            // ---- prefetch MB bx+1 (columns and current block), then wait for MB bx's data
-            if (bx + 1 < p.BW) {
+            // ---- FAST: wait for the loader's slot; otherwise prefetch MB bx+1 (columns, current
+            // block, table row) and wait for MB bx's data
+            const uint8_t* lslot = slots + (size_t)(ln & (LD_RING - 1)) * ld_slot_bytes(p.tstride);
+            if (FAST) {
+                if (!mbar_wait_warp(fullb + (ln & (LD_RING - 1)), (unsigned)((ln / LD_RING) & 1), p.spin_limit)) {
+                    if (lane == 0) {
+                        atomicOr(p.status, ST_WAIT_TIMEOUT);
+                        hand_put(hand, hand_done, hn, HAND_FAIL, p.spin_limit);
+                    }
+                    abort_loader();
+                    return;
+                }
+            } else if (bx + 1 < p.BW) {
                 if (BAND) {
                     int hi = c_hi(bx + 1);
                     for (int c = c_done + 1; c <= hi; c++)
                         fill_chunk(refmem, BWB, WS, c, MARGIN, wy0, p.ref_y, p.W, p.H, lane);
                     c_done = hi;
                 }
+                RIV_STAMP(10);
                 if (lane < 16)
                     cp_async16(curbuf + ((bx + 1) & 1) * 256 + lane * 16, p.cur_y + (size_t)(y0 + lane) * p.W + x0 + 16);
                 if (TABLE)
                     for (int i = lane; i < p.tstride / 8; i += 32)
                         cp_async16(tabbuf + ((bx + 1) & 1) * p.tstride + i * 8,
                                    p.tab + (size_t)(idx + 1) * p.tstride + i * 8);
+                RIV_STAMP(11);
             }
-            cp_async_commit();
-            cp_async_wait1();
+            if (!FAST) cp_async_commit();
+            RIV_STAMP(7);
+            if (!FAST) cp_async_wait1();
             RefView view;
             if (BAND) {
                 view.org = refmem + x0 + MARGIN;
@@ -419,7 +793,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
             }
             view.wy0 = wy0;
             __syncwarp();
-            const uint8_t* cb = curbuf + (bx & 1) * 256;
+            const uint8_t* cb = FAST ? lslot + 2 * p.tstride : curbuf + (bx & 1) * 256;
             const uint32_t c0 = *(const uint32_t*)(cb + yy * 16 + xoff);
             const uint32_t c1 = *(const uint32_t*)(cb + yy * 16 + xoff + 4);
 
@@ -441,7 +815,14 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                         __nanosleep(20);
                         v = ld_rec(p.rec + wi);
                     }
-                    if (bx == 0) recT = ld_rec(p.rec + (r - 1) * p.BW);
+                    if (bx == 0 && !failed) {  // the top record, checked like every other
+                        recT = ld_rec(p.rec + (r - 1) * p.BW);
+                        while ((recT & 0xffff000000000000ull) != tagbits) {
+                            if (++spins > p.spin_limit) { failed = true; break; }
+                            __nanosleep(20);
+                            recT = ld_rec(p.rec + (r - 1) * p.BW);
+                        }
+                    }
                     pref = bx + 1 < p.BW ? ld_rec(p.rec + (r - 1) * p.BW + min(bx + 2, p.BW - 1)) : 0ull;
                 }
                 failed = __shfl_sync(0xffffffffu, (int)failed, 0) != 0;
@@ -450,17 +831,18 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                 if (bx + 1 < p.BW) { recTR = v; has_tr = true; }
             }
             if (failed) {
-                if (lane == 0) atomicOr(p.status, ST_WAIT_TIMEOUT);
-                cp_async_wait0();
+                if (lane == 0) {
+                    atomicOr(p.status, ST_WAIT_TIMEOUT);
+                    hand_put(hand, hand_done, hn, HAND_FAIL, p.spin_limit);
+                }
+                abort_loader();
+                if (!FAST) cp_async_wait0();
                 return;
             }
             RIV_STAMP(2);
             const bool has_t = r > 0, has_l = bx > 0, has_tl = r > 0 && bx > 0;
             auto rec_raw = [](unsigned long long v, int& dx, int& dy) {
                 dx = (int)(int8_t)(v >> 40); dy = (int)(int8_t)(v >> 32);
-            };
-            auto rec_cod = [](unsigned long long v) {
-                return MvT{(int)(int8_t)(v >> 24), (int)(int8_t)(v >> 16), (int)(int8_t)(v >> 8), (int)(int8_t)v};
             };
             int Tx = 0, Ty = 0, TRx = 0, TRy = 0, TLx = 0, TLy = 0;
             if (has_t) rec_raw(recT, Tx, Ty);
@@ -470,7 +852,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
             int Tmx = 0, Tmy = 0;
             MvT Tm_cod{0, 0, 0, 0};
             if (has_tm) {
-                const char4 pc = *(const char4*)(p.prev_coded + 4 * idx);
+                const char4 pc = FAST ? *(const char4*)(lslot + 2 * p.tstride + 256) : *(const char4*)(p.prev_coded + 4 * idx);
                 Tm_cod = MvT{pc.x, pc.y, pc.z, pc.w};
                 Tmx = Tm_cod.dx; Tmy = Tm_cod.dy;
             }
@@ -506,7 +888,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                 for (int j = 0; j < i; j++) ok = ok && !(SV[j + 1] && PX[j] == PX[i] && PY[j] == PY[i]);
                 SV[i + 1] = ok;
             }
-            const uint16_t* tb = tabbuf + (bx & 1) * p.tstride;
+            const uint16_t* tb = FAST ? (const uint16_t*)lslot : tabbuf + (bx & 1) * p.tstride;
             int sdx = 0, sdy = 0;
             if (TABLE) {
                 // ---- table-driven integer search: lane k holds candidate k of a round; the
@@ -524,6 +906,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                 const int dyl = (int)(int8_t)(0xFF010000u >> (8 * min(lane, 3)));
                 long long scost = 0;
                 int phase = 0, iter = 0;
+                RIV_STAMP(12);
                 for (;;) {
                     int cx, cy;
                     bool v;
@@ -533,6 +916,8 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                     long long t = v ? (long long)tb[(cy + sr) * side + cx + sr] + mv_cost<SMALL>(cx, cy, cc, p, bits, nc32) : 0;
                     long long bt;
                     const int wk = argmin8<SMALL>(t, v, bt);
+                    if (phase == 0) RIV_STAMP(13);
+                    if (phase == 2) RIV_STAMP(15);
                     if (phase == 0) {
                         const long long zero_sad = (long long)tb[sr * side + sr];
                         if (p.zthr > 0 && zero_sad <= p.zthr) break;  // stay at (0,0)
@@ -541,8 +926,9 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                         sdy = __shfl_sync(0xffffffffu, cy, wk);
                         if (p.pthr > 0 && (long long)tb[(sdy + sr) * side + sdx + sr] <= p.pthr) break;
                         phase = 1;
+                        RIV_STAMP(9);
                     } else if (phase == 1) {  // large hexagon (enc/motion/scalar.rs:694-729)
-                        if (wk < 0 || bt >= scost) { phase = 2; continue; }
+                        if (wk < 0 || bt >= scost) { phase = 2; RIV_STAMP(14); continue; }
                         scost = bt;
                         sdx = __shfl_sync(0xffffffffu, cx, wk);
                         sdy = __shfl_sync(0xffffffffu, cy, wk);
@@ -551,6 +937,7 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                             phase = 2;
                         }
                     } else {  // small diamond (enc/motion/scalar.rs:731-756)
+                        RIV_PUT(8, iter);
                         if (wk >= 0 && bt < scost) {
                             sdx = __shfl_sync(0xffffffffu, cx, wk);
                             sdy = __shfl_sync(0xffffffffu, cy, wk);
@@ -657,6 +1044,11 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
                     }
                 }
             }
+            if (FAST) {  // the table row, current block and temporal MV are in registers now
+                __syncwarp();
+                if (lane == 0) ld_ctl[0] = ln + 1;
+                ln++;
+            }
             RIV_STAMP(3);
             // ---- half-pel refinement (enc/motion/scalar.rs:759-839): nine floor-averaged
             // candidates around (2*sdx, 2*sdy), from a 3x3 integer neighbourhood per pixel,
@@ -724,96 +1116,36 @@ __global__ void __launch_bounds__(32) k_search(SearchParams p) {
             if (raw.sy == -1) { raw.sy = 1; raw.dy = max(-128, raw.dy - 1); }
 
             RIV_STAMP(4);
-            // ---- RDO skip decision (enc/rdo.rs:140-178)
-            bool int_al = raw.sx == 0 && raw.sy == 0;
-            double satd = (double)max(best_sad, 0LL);
-            double skip_cost = __dadd_rn(satd, __dmul_rn(p.rdo_lambda, p.rdo_skip_bits));
-            double est = __dadd_rn(p.rdo_icpt, __dmul_rn(p.rdo_slope, satd));
-            if (est < 0.0) est = 0.0;
-            double coded_cost = __dadd_rn(__dmul_rn(satd, p.rdo_ret), __dmul_rn(p.rdo_lambda, __dadd_rn(p.rdo_keep_bits, est)));
-            bool rdo_skip = p.rdo_allow && int_al && !(satd > p.rdo_guard) && (skip_cost <= coded_cost);
-
-            // ---- MV mode decision on the coded (reconstructed) neighbours
-            // (enc/encoder.rs:459-733, res/mv_predictor.rs:59-272)
-            MvT cT = rec_cod(recT), cTR = rec_cod(recTR), cTL = rec_cod(recTL);
-            const MvT zero{0, 0, 0, 0};
-            MvT nearest = zero, nearm = zero;
-            {
-                const MvT CS[5] = {L_cod, cT, cTR, cTL, Tm_cod};
-                int nu = 0;
-#pragma unroll
-                for (int i = 0; i < 5; i++) {
-                    bool take = PV[i] && (nu == 0 || (nu == 1 && !mv_eq(CS[i], nearest)));
-                    if (take && nu == 0) nearest = CS[i];
-                    else if (take && nu == 1) nearm = CS[i];
-                    nu += take ? 1 : 0;
-                }
-            }
-            MvT temporal = has_tm ? Tm_cod : zero;
-            const int mx = raw.dx * 2 + raw.sx, my = raw.dy * 2 + raw.sy;
-            auto hpeq = [&](const MvT& t) { return mx == t.dx * 2 + t.sx && my == t.dy * 2 + t.sy; };
-            int mode;
-            if (raw.dx == 0 && raw.dy == 0 && raw.sx == 0 && raw.sy == 0) mode = 0;  // Zero
-            else if (hpeq(nearest)) mode = 1;
-            else if (hpeq(nearm)) mode = 2;
-            else if (has_tr && hpeq(cTR)) mode = 3;
-            else if (has_tl && hpeq(cTL)) mode = 4;
-            else if (hpeq(temporal)) mode = 6;
-            else mode = 5;  // New
-            int chosen = 0, rdx = 0, rdy = 0;
-            MvT coded = raw;
-            if (mode == 5) {
-                const MvT bases[5] = {nearest, nearm, cTR, cTL, temporal};
-                const bool hasb[5] = {true, true, has_tr, has_tl, true};
-                const int selbits[5] = {1, 2, 3, 4, 4};
-                unsigned best = 0xffffffffu;
-                int bbx = nearest.dx, bby = nearest.dy;
-#pragma unroll
-                for (int k = 0; k < 5; k++) {
-                    if (!hasb[k]) continue;
-                    int ddx = sat8(raw.dx - bases[k].dx), ddy = sat8(raw.dy - bases[k].dy);
-                    unsigned cst = (unsigned)(selbits[k] + comp_bits(ddx) + comp_bits(ddy));
-                    if (cst < best) { best = cst; chosen = k; bbx = bases[k].dx; bby = bases[k].dy; }
-                }
-                rdx = sat8(raw.dx - bbx);
-                rdy = sat8(raw.dy - bby);
-                coded.dx = sat8(bbx + rdx);
-                coded.dy = sat8(bby + rdy);
-            } else if (mode == 1) coded = nearest;
-            else if (mode == 2) coded = nearm;
-            else if (mode == 3) coded = cTR;
-            else if (mode == 4) coded = cTL;
-            else if (mode == 6) coded = temporal;
-            uint8_t flags = 0;
-            if (mode == 5) flags = (raw.sx == 1 ? 0x01 : 0) | (raw.sy == 1 ? 0x04 : 0);
-            if (rdo_skip) flags |= 0x40;
-
-            RIV_STAMP(5);
-            // ---- publish
+            // ---- publish the raw MV for the next row's search; hand the MB (raw MV, best SAD)
+            // to the mode warp, which runs the RDO skip and the mode decision off this chain
             if (lane == 0) {
-                unsigned long long rv = tagbits | ((unsigned long long)(uint8_t)raw.dx << 40) |
-                                        ((unsigned long long)(uint8_t)raw.dy << 32) |
-                                        ((unsigned long long)(uint8_t)coded.dx << 24) |
-                                        ((unsigned long long)(uint8_t)coded.dy << 16) |
-                                        ((unsigned long long)(uint8_t)coded.sx << 8) | (unsigned long long)(uint8_t)coded.sy;
-                st_rec(p.rec + idx, rv);
-                MbOut o;
-                o.raw[0] = (int8_t)raw.dx; o.raw[1] = (int8_t)raw.dy; o.raw[2] = (int8_t)raw.sx; o.raw[3] = (int8_t)raw.sy;
-                o.coded[0] = (int8_t)coded.dx; o.coded[1] = (int8_t)coded.dy;
-                o.coded[2] = (int8_t)coded.sx; o.coded[3] = (int8_t)coded.sy;
-                o.rdelta[0] = (int8_t)rdx; o.rdelta[1] = (int8_t)rdy;
-                o.mode = (uint8_t)mode; o.base = (uint8_t)chosen; o.flags = flags; o.rdo_skip = rdo_skip ? 1 : 0;
-                o.pad[0] = o.pad[1] = 0;
-                o.best_sad = (int32_t)best_sad;
-                p.out[idx] = o;
+                st_rec(p.rec + idx, tagbits | ((unsigned long long)(uint8_t)raw.dx << 40) |
+                                        ((unsigned long long)(uint8_t)raw.dy << 32));
+                const unsigned long long pay = ((unsigned long long)(uint16_t)best_sad << 32) |
+                                               (unsigned long long)((uint32_t)(uint8_t)raw.dx | ((uint32_t)(uint8_t)raw.dy << 8) |
+                                                                    ((uint32_t)(uint8_t)raw.sx << 16) |
+                                                                    ((uint32_t)(uint8_t)raw.sy << 24));
+                if (!hand_put(hand, hand_done, hn, pay, p.spin_limit)) failed = true;
             }
-            RIV_STAMP(6);
+            hn++;
+            failed = __shfl_sync(0xffffffffu, (int)failed, 0) != 0;
+            if (failed) {
+                if (lane == 0) atomicOr(p.status, ST_WAIT_TIMEOUT);
+                abort_loader();
+                if (!FAST) cp_async_wait0();
+                return;
+            }
             L_raw = MvT{raw.dx, raw.dy, 0, 0};
-            L_cod = coded;
             recTL = recT;
             recT = recTR;
         }
-        cp_async_wait0();
+        if (FAST) {  // the band of this row is no longer read
+            __syncwarp();
+            if (lane == 0) ld_ctl[1] = lrows + 1;
+            lrows++;
+        } else {
+            cp_async_wait0();
+        }
     }
 }
 
@@ -825,8 +1157,11 @@ static size_t search_smem(int sr, int W, bool band, bool table) {
     size_t ws = 18 + 2 * (size_t)sr;
     size_t margin = ((size_t)sr + 1 + 15) & ~(size_t)15;
     size_t ref = band ? ws * ((size_t)W + 2 * margin) : ws * ws;
-    return 256 * sizeof(double) + 64 * 64 * 4 + 512 + (table ? 4 * (size_t)sad_table_stride(sr) : 0) + ref + 16;
+    size_t head = 256 * sizeof(double) + 64 * 64 * 4 + HAND_RING * 8 + 16;
+    if (band && table) return head + 64 + LD_RING * (size_t)ld_slot_bytes(sad_table_stride(sr)) + ref + 16;
+    return head + 512 + (table ? 4 * (size_t)sad_table_stride(sr) : 0) + ref + 16;
 }
+static int search_threads(bool band, bool table) { return band && table ? 96 : 64; }
 static const size_t SEARCH_SMEM_MAX = 200 * 1024;
 static bool search_use_band(int sr, int W) {
     return search_smem(sr, W, true, search_use_table(sr)) <= SEARCH_SMEM_MAX;
@@ -846,7 +1181,7 @@ int search_max_grid(int sr, int W, bool table, bool small, int* grid_out) {
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return (int)e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32, sm);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, search_threads(band, table), sm);
     if (e != cudaSuccess) return (int)e;
     int dev = 0, nsm = 0;
     cudaGetDevice(&dev);
@@ -862,7 +1197,8 @@ int launch_search(const SearchParams& p, int grid, void* stream) {
     void* args[] = {&q};
     // Cooperative launch: every CTA of the grid is co-resident, so the row-to-row waits
     // can always make progress.
-    cudaError_t e = cudaLaunchCooperativeKernel(search_fn(band, table, table && p.small), dim3(grid), dim3(32), args, sm,
+    cudaError_t e = cudaLaunchCooperativeKernel(search_fn(band, table, table && p.small), dim3(grid),
+                                                dim3(search_threads(band, table)), args, sm,
                                                 (cudaStream_t)stream);
     return (int)e;
 }

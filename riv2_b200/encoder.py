@@ -478,7 +478,7 @@ class Encoder:
         nmb = (sw // 16) * (sh // 16)
         spec = {0: (nmb * 20, np.uint8), 1: (nmb, np.float32), 2: (sw * sh * 3 // 2, np.uint8),
                 3: (sw * sh * 3 // 2, np.uint8), 4: (nmb * 384, np.int16), 5: (nmb, np.uint8),
-                6: (nmb * 8, np.int64)}[what]
+                6: (nmb * 16, np.int64)}[what]
         out = np.empty(spec[0], spec[1])
         self._check(lib().riv_debug_frame_state(self._h, what, C.c_void_p(out.ctypes.data), out.nbytes))
         return out
