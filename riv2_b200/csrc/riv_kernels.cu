@@ -525,14 +525,10 @@ __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned coun
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sa32(bar)), "r"(count) : "memory");
 }
 __device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
-    unsigned long long st;
-    asm volatile("mbarrier.arrive.shared::cta.b64 %0, [%1];" : "=l"(st) : "r"(sa32(bar)) : "memory");
-    (void)st;
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(sa32(bar)) : "memory");
 }
 __device__ __forceinline__ void mbar_arrive_tx(unsigned long long* bar, unsigned tx) {
-    unsigned long long st;
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;" : "=l"(st) : "r"(sa32(bar)), "r"(tx) : "memory");
-    (void)st;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sa32(bar)), "r"(tx) : "memory");
 }
 __device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned parity) {
     unsigned ok;
@@ -856,191 +852,304 @@ __global__ void __launch_bounds__(96, 1) k_search(SearchParams p) {
                 Tm_cod = MvT{pc.x, pc.y, pc.z, pc.w};
                 Tmx = Tm_cod.dx; Tmy = Tm_cod.dy;
             }
-            // ---- seeds, nearest/near/median (enc/motion/scalar.rs:56-156).  Predictor slots in
-            // the reference's order: left, top, top-right, top-left, temporal.
-            const int PX[5] = {L_raw.dx, Tx, TRx, TLx, Tmx}, PY[5] = {L_raw.dy, Ty, TRy, TLy, Tmy};
-            const bool PV[5] = {has_l, has_t, has_tr, has_tl, has_tm};
-            CostCtx cc;
-            cc.nx = cc.ny = cc.rx = cc.ry = 0;
-            {
-                int nu = 0;
+            int sdx = 0, sdy = 0;
+            if constexpr (TABLE && SMALL) {
+                // ---- seeds and nearest/near/median (enc/motion/scalar.rs:56-156) in a flat form:
+                // predictor slots 0..4 = left, top, top-right, top-left, temporal; lane 0 holds
+                // the (0,0) seed, lane 1+i predictor i when push_candidate keeps it.
+                const uint16_t* tb = FAST ? (const uint16_t*)lslot : tabbuf + (bx & 1) * p.tstride;
+                const int QX[5] = {L_raw.dx, Tx, TRx, TLx, Tmx}, QY[5] = {L_raw.dy, Ty, TRy, TLy, Tmy};
+                const unsigned pvm = (has_l ? 1u : 0u) | (has_t ? 2u : 0u) | (has_tr ? 4u : 0u) | (has_tl ? 8u : 0u) |
+                                     (has_tm ? 16u : 0u);
+                unsigned long long X5 = 0, Y5 = 0;
+                unsigned okm = 0;
 #pragma unroll
                 for (int i = 0; i < 5; i++) {
-                    bool take = PV[i] && (nu == 0 || (nu == 1 && !(PX[i] == cc.nx && PY[i] == cc.ny)));
-                    if (take && nu == 0) { cc.nx = PX[i]; cc.ny = PY[i]; }
-                    else if (take && nu == 1) { cc.rx = PX[i]; cc.ry = PY[i]; }
-                    nu += take ? 1 : 0;
+                    X5 |= (unsigned long long)(uint8_t)QX[i] << (8 * i);
+                    Y5 |= (unsigned long long)(uint8_t)QY[i] << (8 * i);
+                    const bool ok = ((pvm >> i) & 1u) && abs(QX[i]) <= sr && abs(QY[i]) <= sr && (QX[i] | QY[i]) != 0;
+                    okm |= ok ? (1u << i) : 0u;
                 }
-                int lx = has_l ? L_raw.dx : 0, ly = has_l ? L_raw.dy : 0;
-                int tx = has_t ? Tx : 0, ty = has_t ? Ty : 0;
-                int qx = has_tr ? TRx : (has_tl ? TLx : 0), qy = has_tr ? TRy : (has_tl ? TLy : 0);
-                cc.mx = median3(lx, tx, qx);
-                cc.my = median3(ly, ty, qy);
-            }
-            // seed slots: 0 = (0,0), 1..5 = predictors kept if within range and not already
-            // pushed (push_candidate, enc/motion/scalar.rs:46-53)
-            bool SV[6];
-            SV[0] = true;
+                auto qx = [&](int i) { return (int)(int8_t)(X5 >> (8 * i)); };
+                auto qy = [&](int i) { return (int)(int8_t)(Y5 >> (8 * i)); };
+                int nix = 0, niy = 0, rix = 0, riy = 0;
+                if (pvm) {  // nearest = first available; near = first later one that differs
+                    const int ni = __ffs(pvm) - 1;
+                    nix = qx(ni);
+                    niy = qy(ni);
+                    unsigned dm = 0;
 #pragma unroll
-            for (int i = 0; i < 5; i++) {
-                bool ok = PV[i] && abs(PX[i]) <= sr && abs(PY[i]) <= sr && !(PX[i] == 0 && PY[i] == 0);
-#pragma unroll
-                for (int j = 0; j < i; j++) ok = ok && !(SV[j + 1] && PX[j] == PX[i] && PY[j] == PY[i]);
-                SV[i + 1] = ok;
-            }
-            const uint16_t* tb = FAST ? (const uint16_t*)lslot : tabbuf + (bx & 1) * p.tstride;
-            int sdx = 0, sdy = 0;
-            if (TABLE) {
-                // ---- table-driven integer search: lane k holds candidate k of a round; the
-                // in-order strict-'<' scan of the reference equals an argmin with the lowest
-                // index winning ties.  One loop for the three round kinds (seeds, hexagon,
-                // diamond) keeps a single MV-cost evaluation site.
+                    for (int i = 0; i < 5; i++) dm |= (QX[i] != nix || QY[i] != niy) ? (1u << i) : 0u;
+                    const unsigned rm = pvm & dm & ~((2u << ni) - 1u);
+                    if (rm) {
+                        const int ri = __ffs(rm) - 1;
+                        rix = qx(ri);
+                        riy = qy(ri);
+                    }
+                }
+                const int mdx = median3(L_raw.dx, Tx, has_tr ? TRx : TLx), mdy = median3(L_raw.dy, Ty, has_tr ? TRy : TLy);
                 int kx = 0, ky = 0;
                 bool kv = lane == 0;
+                if (lane >= 1 && lane <= 5) {
+                    const int ci = lane - 1;
+                    kx = qx(ci);
+                    ky = qy(ci);
+                    unsigned eq = 0;
 #pragma unroll
-                for (int i = 0; i < 5; i++)
-                    if (lane == i + 1) { kx = PX[i]; ky = PY[i]; kv = SV[i + 1]; }
-                const int hxl = (int)(int8_t)(0x01FFFEFF0102ull >> (8 * min(lane, 5)));
-                const int hyl = (int)(int8_t)(0xFEFE00020200ull >> (8 * min(lane, 5)));
-                const int dxl = (int)(int8_t)(0x0000FF01u >> (8 * min(lane, 3)));
-                const int dyl = (int)(int8_t)(0xFF010000u >> (8 * min(lane, 3)));
-                long long scost = 0;
-                int phase = 0, iter = 0;
+                    for (int j = 0; j < 5; j++) eq |= (QX[j] == kx && QY[j] == ky) ? (1u << j) : 0u;
+                    kv = ((okm >> ci) & 1u) && (eq & okm & ((1u << ci) - 1u)) == 0;
+                }
+                const int c15i = (int)p.c15, c05i = (int)p.c05;
+                // estimate_mv_cost (enc/motion/scalar.rs:453-544), every term below 2^27 here
+                auto cost = [&](int cx, int cy) -> int {
+                    if (p.lambda_zero) return 0;
+                    int best = INT_MAX;
+                    if ((cx == nix && cy == niy) || (cx == rix && cy == riy) || (cx == mdx && cy == mdy)) best = c15i;
+                    if ((cx | cy) == 0) best = min(best, c05i);
+                    const int ax = abs(cx - nix), ay = abs(cy - niy), bx2 = abs(cx - rix), by2 = abs(cy - riy);
+                    int nc;
+                    if (((ax | ay | bx2 | by2) & ~63) == 0) nc = min(nc32[ax * 64 + ay], nc32[bx2 * 64 + by2]);
+                    else nc = (int)min(__ldg(p.newcost + ax * 256 + ay), __ldg(p.newcost + bx2 * 256 + by2));
+                    return min(best, nc);
+                };
                 RIV_STAMP(12);
-                for (;;) {
-                    int cx, cy;
-                    bool v;
-                    if (phase == 0) { cx = kx; cy = ky; v = kv && lane < 6; }
-                    else if (phase == 1) { cx = sdx + hxl; cy = sdy + hyl; v = lane < 6 && abs(cx) <= sr && abs(cy) <= sr; }
-                    else { cx = sdx + dxl; cy = sdy + dyl; v = lane < 4 && abs(cx) <= sr && abs(cy) <= sr; }
-                    long long t = v ? (long long)tb[(cy + sr) * side + cx + sr] + mv_cost<SMALL>(cx, cy, cc, p, bits, nc32) : 0;
-                    long long bt;
-                    const int wk = argmin8<SMALL>(t, v, bt);
-                    if (phase == 0) RIV_STAMP(13);
-                    if (phase == 2) RIV_STAMP(15);
-                    if (phase == 0) {
-                        const long long zero_sad = (long long)tb[sr * side + sr];
-                        if (p.zthr > 0 && zero_sad <= p.zthr) break;  // stay at (0,0)
-                        scost = bt;
-                        sdx = __shfl_sync(0xffffffffu, cx, wk);
-                        sdy = __shfl_sync(0xffffffffu, cy, wk);
-                        if (p.pthr > 0 && (long long)tb[(sdy + sr) * side + sdx + sr] <= p.pthr) break;
-                        phase = 1;
-                        RIV_STAMP(9);
-                    } else if (phase == 1) {  // large hexagon (enc/motion/scalar.rs:694-729)
-                        if (wk < 0 || bt >= scost) { phase = 2; RIV_STAMP(14); continue; }
-                        scost = bt;
-                        sdx = __shfl_sync(0xffffffffu, cx, wk);
-                        sdy = __shfl_sync(0xffffffffu, cy, wk);
-                        if (++iter > 4096) {  // cost strictly decreases, so this is never reached
-                            if (lane == 0) atomicOr(p.status, ST_HEX_CAP);
-                            phase = 2;
+                // seed round: the in-order strict-'<' scan = argmin with the lowest slot winning ties
+                const int t0 = kv ? (int)tb[(ky + sr) * side + kx + sr] + cost(kx, ky) : 0;
+                const uint32_t k0 = __reduce_min_sync(0xffffffffu, kv ? ((uint32_t)t0 << 3) | (uint32_t)lane : 0xffffffffu);
+                RIV_STAMP(13);
+                const int zero_sad = (int)tb[sr * side + sr];
+                if (!(p.zthr > 0 && zero_sad <= p.zthr)) {  // else stay at (0,0)
+                    int scost = (int)(k0 >> 3);
+                    const int w0 = (int)(k0 & 7u);
+                    sdx = w0 == 0 ? 0 : qx(w0 - 1);
+                    sdy = w0 == 0 ? 0 : qy(w0 - 1);
+                    RIV_STAMP(9);
+                    if (!(p.pthr > 0 && (int)tb[(sdy + sr) * side + sdx + sr] <= p.pthr)) {
+                        // hexagon (lanes 0-5, enc/motion/scalar.rs:694-729) and the small diamond
+                        // around the same centre (lanes 6-9, :731-756) in one round: the diamond
+                        // result is used when the hexagon does not improve.
+                        const int ol = lane < 6 ? lane : lane - 6;
+                        const int ox = lane < 6 ? (int)(int8_t)(0x01FFFEFF0102ull >> (8 * ol))
+                                                : (lane < 10 ? (int)(int8_t)(0x0000FF01u >> (8 * ol)) : 0);
+                        const int oy = lane < 6 ? (int)(int8_t)(0xFEFE00020200ull >> (8 * ol))
+                                                : (lane < 10 ? (int)(int8_t)(0xFF010000u >> (8 * ol)) : 0);
+                        int iter = 0;
+                        for (;;) {
+                            const int cx = sdx + ox, cy = sdy + oy;
+                            const bool v = lane < 10 && abs(cx) <= sr && abs(cy) <= sr;
+                            const int t = v ? (int)tb[(cy + sr) * side + cx + sr] + cost(cx, cy) : 0;
+                            const uint32_t kh = __reduce_min_sync(
+                                0xffffffffu, v && lane < 6 ? ((uint32_t)t << 3) | (uint32_t)lane : 0xffffffffu);
+                            const uint32_t kd = __reduce_min_sync(
+                                0xffffffffu, v && lane >= 6 ? ((uint32_t)t << 3) | (uint32_t)(lane - 6) : 0xffffffffu);
+                            if (kh != 0xffffffffu && (int)(kh >> 3) < scost) {
+                                const int w = (int)(kh & 7u);
+                                scost = (int)(kh >> 3);
+                                sdx += (int)(int8_t)(0x01FFFEFF0102ull >> (8 * w));
+                                sdy += (int)(int8_t)(0xFEFE00020200ull >> (8 * w));
+                                if (++iter > 4096) {  // cost strictly decreases, so this is never reached
+                                    if (lane == 0) atomicOr(p.status, ST_HEX_CAP);
+                                    break;
+                                }
+                                continue;
+                            }
+                            RIV_STAMP(14);
+                            RIV_PUT(8, iter);
+                            if (kd != 0xffffffffu && (int)(kd >> 3) < scost) {
+                                const int w = (int)(kd & 7u);
+                                sdx += (int)(int8_t)(0x0000FF01u >> (8 * w));
+                                sdy += (int)(int8_t)(0xFF010000u >> (8 * w));
+                            }
+                            break;
                         }
-                    } else {  // small diamond (enc/motion/scalar.rs:731-756)
-                        RIV_PUT(8, iter);
-                        if (wk >= 0 && bt < scost) {
-                            sdx = __shfl_sync(0xffffffffu, cx, wk);
-                            sdy = __shfl_sync(0xffffffffu, cy, wk);
-                        }
-                        break;
                     }
                 }
             } else {
-                // ---- zero SAD and the seed round; lane k evaluates the MV cost of slot k
-                long long my_cost = 0;
+                // ---- seeds, nearest/near/median (enc/motion/scalar.rs:56-156).  Predictor slots in
+                // the reference's order: left, top, top-right, top-left, temporal.
+                const int PX[5] = {L_raw.dx, Tx, TRx, TLx, Tmx}, PY[5] = {L_raw.dy, Ty, TRy, TLy, Tmy};
+                const bool PV[5] = {has_l, has_t, has_tr, has_tl, has_tm};
+                CostCtx cc;
+                cc.nx = cc.ny = cc.rx = cc.ry = 0;
                 {
+                    int nu = 0;
+    #pragma unroll
+                    for (int i = 0; i < 5; i++) {
+                        bool take = PV[i] && (nu == 0 || (nu == 1 && !(PX[i] == cc.nx && PY[i] == cc.ny)));
+                        if (take && nu == 0) { cc.nx = PX[i]; cc.ny = PY[i]; }
+                        else if (take && nu == 1) { cc.rx = PX[i]; cc.ry = PY[i]; }
+                        nu += take ? 1 : 0;
+                    }
+                    int lx = has_l ? L_raw.dx : 0, ly = has_l ? L_raw.dy : 0;
+                    int tx = has_t ? Tx : 0, ty = has_t ? Ty : 0;
+                    int qx = has_tr ? TRx : (has_tl ? TLx : 0), qy = has_tr ? TRy : (has_tl ? TLy : 0);
+                    cc.mx = median3(lx, tx, qx);
+                    cc.my = median3(ly, ty, qy);
+                }
+                // seed slots: 0 = (0,0), 1..5 = predictors kept if within range and not already
+                // pushed (push_candidate, enc/motion/scalar.rs:46-53)
+                bool SV[6];
+                SV[0] = true;
+    #pragma unroll
+                for (int i = 0; i < 5; i++) {
+                    bool ok = PV[i] && abs(PX[i]) <= sr && abs(PY[i]) <= sr && !(PX[i] == 0 && PY[i] == 0);
+    #pragma unroll
+                    for (int j = 0; j < i; j++) ok = ok && !(SV[j + 1] && PX[j] == PX[i] && PY[j] == PY[i]);
+                    SV[i + 1] = ok;
+                }
+                const uint16_t* tb = FAST ? (const uint16_t*)lslot : tabbuf + (bx & 1) * p.tstride;
+                if (TABLE) {
+                    // ---- table-driven integer search: lane k holds candidate k of a round; the
+                    // in-order strict-'<' scan of the reference equals an argmin with the lowest
+                    // index winning ties.  One loop for the three round kinds (seeds, hexagon,
+                    // diamond) keeps a single MV-cost evaluation site.
                     int kx = 0, ky = 0;
                     bool kv = lane == 0;
     #pragma unroll
                     for (int i = 0; i < 5; i++)
                         if (lane == i + 1) { kx = PX[i]; ky = PY[i]; kv = SV[i + 1]; }
-                    if (kv) my_cost = mv_cost<SMALL>(kx, ky, cc, p, bits, nc32);
-                }
-                unsigned part[6];
-                part[0] = sad_int_part(view, x0, y0, p.W, p.H, 0, 0, yy, xoff, c0, c1);
-    #pragma unroll
-                for (int i = 0; i < 5; i++)
-                    part[i + 1] = SV[i + 1] ? sad_int_part(view, x0, y0, p.W, p.H, PX[i], PY[i], yy, xoff, c0, c1) : 0u;
-                long long sads[6];
-    #pragma unroll
-                for (int i = 0; i < 6; i++) sads[i] = (long long)warp_sum(part[i]);
-                long long zero_sad = sads[0];
-                long long sc_cost = __shfl_sync(0xffffffffu, my_cost, 0);
-                long long scost = zero_sad + sc_cost;
-                bool skip_int = p.zthr > 0 && zero_sad <= p.zthr;
-                if (!skip_int) {
-    #pragma unroll
-                    for (int i = 0; i < 5; i++) {
-                        long long ci = __shfl_sync(0xffffffffu, my_cost, i + 1);
-                        if (!SV[i + 1]) continue;
-                        long long t = sads[i + 1] + ci;
-                        if (t < scost) { scost = t; sdx = PX[i]; sdy = PY[i]; sc_cost = ci; }
-                    }
-                    long long cur_sad = scost - sc_cost;
-                    if (p.pthr > 0 && cur_sad <= p.pthr) skip_int = true;
-                }
-                if (!skip_int) {
-                    // large hexagon (enc/motion/scalar.rs:694-729)
-                    const int HX[6] = {2, 1, -1, -2, -1, 1}, HY[6] = {0, 2, 2, 0, -2, -2};
-                    // HX/HY of lane k (k < 6) without a lane-indexed array
                     const int hxl = (int)(int8_t)(0x01FFFEFF0102ull >> (8 * min(lane, 5)));
                     const int hyl = (int)(int8_t)(0xFEFE00020200ull >> (8 * min(lane, 5)));
-                    int iter = 0;
+                    const int dxl = (int)(int8_t)(0x0000FF01u >> (8 * min(lane, 3)));
+                    const int dyl = (int)(int8_t)(0xFF010000u >> (8 * min(lane, 3)));
+                    long long scost = 0;
+                    int phase = 0, iter = 0;
+                    RIV_STAMP(12);
                     for (;;) {
-                        int cx = sdx, cy = sdy;
-                        long long lc = 0;
-                        if (lane < 6) {
-                            int dx = cx + hxl, dy = cy + hyl;
-                            if (abs(dx) <= sr && abs(dy) <= sr) lc = mv_cost<SMALL>(dx, dy, cc, p, bits, nc32);
-                        }
-                        unsigned hp[6];
-    #pragma unroll
-                        for (int k = 0; k < 6; k++) {
-                            int dx = cx + HX[k], dy = cy + HY[k];
-                            hp[k] = (abs(dx) <= sr && abs(dy) <= sr)
-                                        ? sad_int_part(view, x0, y0, p.W, p.H, dx, dy, yy, xoff, c0, c1) : 0u;
-                        }
-                        bool improved = false;
-    #pragma unroll
-                        for (int k = 0; k < 6; k++) {
-                            long long s = (long long)warp_sum(hp[k]);
-                            long long ck = __shfl_sync(0xffffffffu, lc, k);
-                            int dx = cx + HX[k], dy = cy + HY[k];
-                            if (abs(dx) > sr || abs(dy) > sr) continue;
-                            long long t = s + ck;
-                            if (t < scost) { scost = t; sdx = dx; sdy = dy; improved = true; }
-                        }
-                        if (!improved) break;
-                        if (++iter > 4096) {  // cost strictly decreases, so this is never reached
-                            if (lane == 0) atomicOr(p.status, ST_HEX_CAP);
+                        int cx, cy;
+                        bool v;
+                        if (phase == 0) { cx = kx; cy = ky; v = kv && lane < 6; }
+                        else if (phase == 1) { cx = sdx + hxl; cy = sdy + hyl; v = lane < 6 && abs(cx) <= sr && abs(cy) <= sr; }
+                        else { cx = sdx + dxl; cy = sdy + dyl; v = lane < 4 && abs(cx) <= sr && abs(cy) <= sr; }
+                        long long t = v ? (long long)tb[(cy + sr) * side + cx + sr] + mv_cost<SMALL>(cx, cy, cc, p, bits, nc32) : 0;
+                        long long bt;
+                        const int wk = argmin8<SMALL>(t, v, bt);
+                        if (phase == 0) RIV_STAMP(13);
+                        if (phase == 2) RIV_STAMP(15);
+                        if (phase == 0) {
+                            const long long zero_sad = (long long)tb[sr * side + sr];
+                            if (p.zthr > 0 && zero_sad <= p.zthr) break;  // stay at (0,0)
+                            scost = bt;
+                            sdx = __shfl_sync(0xffffffffu, cx, wk);
+                            sdy = __shfl_sync(0xffffffffu, cy, wk);
+                            if (p.pthr > 0 && (long long)tb[(sdy + sr) * side + sdx + sr] <= p.pthr) break;
+                            phase = 1;
+                            RIV_STAMP(9);
+                        } else if (phase == 1) {  // large hexagon (enc/motion/scalar.rs:694-729)
+                            if (wk < 0 || bt >= scost) { phase = 2; RIV_STAMP(14); continue; }
+                            scost = bt;
+                            sdx = __shfl_sync(0xffffffffu, cx, wk);
+                            sdy = __shfl_sync(0xffffffffu, cy, wk);
+                            if (++iter > 4096) {  // cost strictly decreases, so this is never reached
+                                if (lane == 0) atomicOr(p.status, ST_HEX_CAP);
+                                phase = 2;
+                            }
+                        } else {  // small diamond (enc/motion/scalar.rs:731-756)
+                            RIV_PUT(8, iter);
+                            if (wk >= 0 && bt < scost) {
+                                sdx = __shfl_sync(0xffffffffu, cx, wk);
+                                sdy = __shfl_sync(0xffffffffu, cy, wk);
+                            }
                             break;
                         }
                     }
-                    // small diamond (enc/motion/scalar.rs:731-756)
-                    const int DX[4] = {1, -1, 0, 0}, DY[4] = {0, 0, 1, -1};
-                    const int dxl = (int)(int8_t)(0x0000FF01u >> (8 * min(lane, 3)));
-                    const int dyl = (int)(int8_t)(0xFF010000u >> (8 * min(lane, 3)));
-                    int cx = sdx, cy = sdy;
-                    long long lc = 0;
-                    if (lane < 4) {
-                        int dx = cx + dxl, dy = cy + dyl;
-                        if (abs(dx) <= sr && abs(dy) <= sr) lc = mv_cost<SMALL>(dx, dy, cc, p, bits, nc32);
+                } else {
+                    // ---- zero SAD and the seed round; lane k evaluates the MV cost of slot k
+                    long long my_cost = 0;
+                    {
+                        int kx = 0, ky = 0;
+                        bool kv = lane == 0;
+        #pragma unroll
+                        for (int i = 0; i < 5; i++)
+                            if (lane == i + 1) { kx = PX[i]; ky = PY[i]; kv = SV[i + 1]; }
+                        if (kv) my_cost = mv_cost<SMALL>(kx, ky, cc, p, bits, nc32);
                     }
-                    unsigned dp[4];
-    #pragma unroll
-                    for (int k = 0; k < 4; k++) {
-                        int dx = cx + DX[k], dy = cy + DY[k];
-                        dp[k] = (abs(dx) <= sr && abs(dy) <= sr)
-                                    ? sad_int_part(view, x0, y0, p.W, p.H, dx, dy, yy, xoff, c0, c1) : 0u;
+                    unsigned part[6];
+                    part[0] = sad_int_part(view, x0, y0, p.W, p.H, 0, 0, yy, xoff, c0, c1);
+        #pragma unroll
+                    for (int i = 0; i < 5; i++)
+                        part[i + 1] = SV[i + 1] ? sad_int_part(view, x0, y0, p.W, p.H, PX[i], PY[i], yy, xoff, c0, c1) : 0u;
+                    long long sads[6];
+        #pragma unroll
+                    for (int i = 0; i < 6; i++) sads[i] = (long long)warp_sum(part[i]);
+                    long long zero_sad = sads[0];
+                    long long sc_cost = __shfl_sync(0xffffffffu, my_cost, 0);
+                    long long scost = zero_sad + sc_cost;
+                    bool skip_int = p.zthr > 0 && zero_sad <= p.zthr;
+                    if (!skip_int) {
+        #pragma unroll
+                        for (int i = 0; i < 5; i++) {
+                            long long ci = __shfl_sync(0xffffffffu, my_cost, i + 1);
+                            if (!SV[i + 1]) continue;
+                            long long t = sads[i + 1] + ci;
+                            if (t < scost) { scost = t; sdx = PX[i]; sdy = PY[i]; sc_cost = ci; }
+                        }
+                        long long cur_sad = scost - sc_cost;
+                        if (p.pthr > 0 && cur_sad <= p.pthr) skip_int = true;
                     }
-    #pragma unroll
-                    for (int k = 0; k < 4; k++) {
-                        long long s = (long long)warp_sum(dp[k]);
-                        long long ck = __shfl_sync(0xffffffffu, lc, k);
-                        int dx = cx + DX[k], dy = cy + DY[k];
-                        if (abs(dx) > sr || abs(dy) > sr) continue;
-                        long long t = s + ck;
-                        if (t < scost) { scost = t; sdx = dx; sdy = dy; }
+                    if (!skip_int) {
+                        // large hexagon (enc/motion/scalar.rs:694-729)
+                        const int HX[6] = {2, 1, -1, -2, -1, 1}, HY[6] = {0, 2, 2, 0, -2, -2};
+                        // HX/HY of lane k (k < 6) without a lane-indexed array
+                        const int hxl = (int)(int8_t)(0x01FFFEFF0102ull >> (8 * min(lane, 5)));
+                        const int hyl = (int)(int8_t)(0xFEFE00020200ull >> (8 * min(lane, 5)));
+                        int iter = 0;
+                        for (;;) {
+                            int cx = sdx, cy = sdy;
+                            long long lc = 0;
+                            if (lane < 6) {
+                                int dx = cx + hxl, dy = cy + hyl;
+                                if (abs(dx) <= sr && abs(dy) <= sr) lc = mv_cost<SMALL>(dx, dy, cc, p, bits, nc32);
+                            }
+                            unsigned hp[6];
+        #pragma unroll
+                            for (int k = 0; k < 6; k++) {
+                                int dx = cx + HX[k], dy = cy + HY[k];
+                                hp[k] = (abs(dx) <= sr && abs(dy) <= sr)
+                                            ? sad_int_part(view, x0, y0, p.W, p.H, dx, dy, yy, xoff, c0, c1) : 0u;
+                            }
+                            bool improved = false;
+        #pragma unroll
+                            for (int k = 0; k < 6; k++) {
+                                long long s = (long long)warp_sum(hp[k]);
+                                long long ck = __shfl_sync(0xffffffffu, lc, k);
+                                int dx = cx + HX[k], dy = cy + HY[k];
+                                if (abs(dx) > sr || abs(dy) > sr) continue;
+                                long long t = s + ck;
+                                if (t < scost) { scost = t; sdx = dx; sdy = dy; improved = true; }
+                            }
+                            if (!improved) break;
+                            if (++iter > 4096) {  // cost strictly decreases, so this is never reached
+                                if (lane == 0) atomicOr(p.status, ST_HEX_CAP);
+                                break;
+                            }
+                        }
+                        // small diamond (enc/motion/scalar.rs:731-756)
+                        const int DX[4] = {1, -1, 0, 0}, DY[4] = {0, 0, 1, -1};
+                        const int dxl = (int)(int8_t)(0x0000FF01u >> (8 * min(lane, 3)));
+                        const int dyl = (int)(int8_t)(0xFF010000u >> (8 * min(lane, 3)));
+                        int cx = sdx, cy = sdy;
+                        long long lc = 0;
+                        if (lane < 4) {
+                            int dx = cx + dxl, dy = cy + dyl;
+                            if (abs(dx) <= sr && abs(dy) <= sr) lc = mv_cost<SMALL>(dx, dy, cc, p, bits, nc32);
+                        }
+                        unsigned dp[4];
+        #pragma unroll
+                        for (int k = 0; k < 4; k++) {
+                            int dx = cx + DX[k], dy = cy + DY[k];
+                            dp[k] = (abs(dx) <= sr && abs(dy) <= sr)
+                                        ? sad_int_part(view, x0, y0, p.W, p.H, dx, dy, yy, xoff, c0, c1) : 0u;
+                        }
+        #pragma unroll
+                        for (int k = 0; k < 4; k++) {
+                            long long s = (long long)warp_sum(dp[k]);
+                            long long ck = __shfl_sync(0xffffffffu, lc, k);
+                            int dx = cx + DX[k], dy = cy + DY[k];
+                            if (abs(dx) > sr || abs(dy) > sr) continue;
+                            long long t = s + ck;
+                            if (t < scost) { scost = t; sdx = dx; sdy = dy; }
+                        }
                     }
                 }
             }
@@ -1093,19 +1202,47 @@ __global__ void __launch_bounds__(96, 1) k_search(SearchParams p) {
                     for (int q = 0; q < 9; q++) hpart[q] = (h ? hpart[q] : 0u) + __vsadu4(cw, v[q]);
                 }
             }
-            long long hs[9];
-#pragma unroll
-            for (int q = 0; q < 9; q++) hs[q] = (long long)warp_sum(hpart[q]);
-            long long best_total = hs[4], best_sad = hs[4];
+            long long best_sad;
             int bsx = 0, bsy = 0;
+            if constexpr (SMALL) {
+                // Per-lane partials are at most 8 * 255, so the warp totals (<= 65280) of two
+                // candidates share one 32-bit reduction.  Then lane q < 9 holds candidate q and one
+                // argmin replaces the in-order scan: the centre is the incumbent (order 0), the
+                // neighbours follow in scan order (0,1,2,3,5,6,7,8), ties keep the earlier one.
+                const unsigned w01 = __reduce_add_sync(0xffffffffu, hpart[0] | (hpart[1] << 16));
+                const unsigned w23 = __reduce_add_sync(0xffffffffu, hpart[2] | (hpart[3] << 16));
+                const unsigned w45 = __reduce_add_sync(0xffffffffu, hpart[4] | (hpart[5] << 16));
+                const unsigned w67 = __reduce_add_sync(0xffffffffu, hpart[6] | (hpart[7] << 16));
+                const unsigned w8 = __reduce_add_sync(0xffffffffu, hpart[8]);
+                const int q = lane < 9 ? lane : 4;
+                const unsigned wq = q < 2 ? w01 : q < 4 ? w23 : q < 6 ? w45 : q < 8 ? w67 : w8;
+                const int hsq = (int)((wq >> ((q & 1) * 16)) & 0xffffu);
+                const int sxq = q % 3 - 1, syq = q / 3 - 1;
+                const bool vq = lane < 9 && !((sdx == -128 && sxq == -1) || (sdy == -128 && syq == -1));
+                const int c15i = (int)p.c15;  // every neighbour is fractional in at least one axis
+                const int ord = q == 4 ? 0 : (q < 4 ? q + 1 : q);
+                const int tot = hsq + (q == 4 ? 0 : c15i);
+                const uint32_t key = __reduce_min_sync(0xffffffffu, vq ? ((uint32_t)tot << 4) | (uint32_t)ord : 0xffffffffu);
+                const int ow = (int)(key & 15u);
+                const int qw = ow == 0 ? 4 : (ow <= 4 ? ow - 1 : ow);
+                bsx = qw % 3 - 1;
+                bsy = qw / 3 - 1;
+                best_sad = (long long)((int)(key >> 4) - (qw == 4 ? 0 : c15i));
+            } else {
+                long long hs[9];
 #pragma unroll
-            for (int q = 0; q < 9; q++) {
-                if (q == 4) continue;
-                int sx = q % 3 - 1, sy = q / 3 - 1;
-                if ((sdx == -128 && sx == -1) || (sdy == -128 && sy == -1)) continue;
-                long long pen = p.c15;  // every neighbour is fractional in at least one axis
-                if (best_total - pen < 0) continue;
-                if (hs[q] + pen < best_total) { best_total = hs[q] + pen; best_sad = hs[q]; bsx = sx; bsy = sy; }
+                for (int q = 0; q < 9; q++) hs[q] = (long long)warp_sum(hpart[q]);
+                long long best_total = hs[4];
+                best_sad = hs[4];
+#pragma unroll
+                for (int q = 0; q < 9; q++) {
+                    if (q == 4) continue;
+                    int sx = q % 3 - 1, sy = q / 3 - 1;
+                    if ((sdx == -128 && sx == -1) || (sdy == -128 && sy == -1)) continue;
+                    long long pen = p.c15;  // every neighbour is fractional in at least one axis
+                    if (best_total - pen < 0) continue;
+                    if (hs[q] + pen < best_total) { best_total = hs[q] + pen; best_sad = hs[q]; bsx = sx; bsy = sy; }
+                }
             }
             int dxh = min(max(2 * sdx + bsx, -255), 255), dyh = min(max(2 * sdy + bsy, -255), 255);
             // MotionVector::new(dx_hp/2, dy_hp/2, dx_hp%2, dy_hp%2).as_canonicalized()
