@@ -320,7 +320,7 @@ struct riv_encoder {
     int ref_cur = 0, coded_cur = 0;
     bool has_ref = false, has_prev_mvs = false;
     unsigned tag = 0;
-    int search_grid = 0;
+    SearchPlan splan{};
     Lambda L{};
     int inter_E = 0, inter_I = 0, inter_H = 0, inter_level = 0;
     int intra_E = 0, intra_I = 0, intra_H = 0, intra_level = 0;
@@ -339,6 +339,7 @@ struct riv_encoder {
     double sum_times[NSTAGE + 1] = {0};
     size_t coef_guess = 0;  // bytes of coefficients copied eagerly per frame
     DevBuf prof;            // optional per-MB phase stamps of the search kernel
+    DevBuf tflag;           // fused table: per-MB "table row written" flags (frame tag)
     uint64_t h2d_bytes = 0, d2h_bytes = 0, pframes = 0, launches = 0;
 };
 
@@ -442,10 +443,12 @@ static void setup_device(riv_encoder* e) {
     e->ctab.alloc(sizeof(ct));
     CK(cudaMemcpy(e->ytab.p, yt, sizeof(yt), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(e->ctab.p, ct, sizeof(ct), cudaMemcpyHostToDevice));
-    int g = 0;
-    CK(search_max_grid(c.search_range, (int)c.storage_width, e->table_ok, e->small_costs, &g));
-    if (g <= 0) throw std::runtime_error("search kernel cannot be made resident");
-    e->search_grid = std::min(g, e->BH);
+    CK(search_plan(c.search_range, (int)c.storage_width, e->BH, e->table_ok, e->small_costs, &e->splan));
+    if (e->splan.grid <= 0) throw std::runtime_error("search kernel cannot be made resident");
+    if (e->splan.fused) {
+        e->tflag.alloc((size_t)N * sizeof(unsigned));
+        e->tflag.zero(e->S);
+    }
     // frame constants
     e->L = lambda_for(c.inter_quality, c.rdo_lambda_mult);
     e->inter_base = quant_step(c.inter_quality);
@@ -496,7 +499,7 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
     CK(cudaEventRecord(s.ev_k[EV_START], S));
     // kernels per frame: rgb->yuv, (search, predict, 3 x aq), residual, deblock (2 per plane), scan + pack
     const int nplanes_db = 3 * 2;
-    e->launches += (src == 2 ? 0 : 1) + (j.type == 2 ? 5 + (e->table_ok ? 1 : 0) : 0) + 1 +
+    e->launches += (src == 2 ? 0 : 1) + (j.type == 2 ? 5 + (e->table_ok && !e->splan.fused ? 1 : 0) : 0) + 1 +
                    ((j.type == 2 ? e->inter_level : e->intra_level) > 0 ? nplanes_db : 0) + 3;
     if (src == 0) e->h2d_bytes += (uint64_t)c.display_width * c.display_height * 3;
     if (src == 2) e->h2d_bytes += e->yuv_bytes;
@@ -581,14 +584,16 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         sp.spin_limit = 1ll << 22;  // ~ a few seconds, far above any legitimate wait
         sp.tab = nullptr;
         sp.tstride = 0;
+        sp.tflag = nullptr;
         if (e->table_ok) {
             sp.tstride = sad_table_stride(c.search_range);
             sp.tab = e->sadtab.as<uint16_t>();
-            CK(launch_sad_table(sp.ref_y, sp.cur_y, W, H, c.search_range, e->sadtab.as<uint16_t>(), sp.tstride, S));
+            if (e->splan.fused) sp.tflag = e->tflag.as<unsigned>();  // computed inside the search launch
+            else CK(launch_sad_table(sp.ref_y, sp.cur_y, W, H, c.search_range, e->sadtab.as<uint16_t>(), sp.tstride, S));
         }
         CK(cudaEventRecord(s.ev_k[EV_TABLE], S));
         sp.prof = e->prof.as<long long>();
-        CK(launch_search(sp, e->search_grid, S));
+        CK(launch_search(sp, e->splan, S));
         CK(cudaEventRecord(s.ev_k[EV_SEARCH], S));
         // coded MVs of this frame become next frame's temporal predictors
         const int cn = e->coded_cur ^ 1;
@@ -989,7 +994,7 @@ void riv_encoder_free(riv_encoder* e) {
     }
     DevBuf* bufs[] = {&e->cur, &e->ref[0], &e->ref[1], &e->pred, &e->mbout, &e->coded[0], &e->coded[1], &e->rec,
                       &e->varsum, &e->lnv, &e->qs, &e->coeffs, &e->opt_skip, &e->fmask, &e->eobs, &e->status,
-                      &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset, &e->sadtab, &e->prof, &e->newcost, &e->newcost32};
+                      &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset, &e->sadtab, &e->prof, &e->tflag, &e->newcost, &e->newcost32};
     for (DevBuf* b : bufs) b->release();
     if (e->S) cudaStreamDestroy(e->S);
     if (e->C) cudaStreamDestroy(e->C);

@@ -54,6 +54,8 @@ struct SearchParams {
     unsigned* status;
     long long spin_limit;
     long long* prof;  // optional: 16 words per MB (phase clock stamps, hexagon rounds), nullptr = off
+    int nrow_ctas;    // CTAs that own MB rows (row stride); the rest of the grid are table workers
+    unsigned* tflag;  // fused table: per-MB flag = tag once its table row is written; nullptr = precomputed
 };
 
 struct ResidualParams {
@@ -79,12 +81,19 @@ enum StatusBits : unsigned {
 
 // Launchers (riv_kernels.cu).  All are asynchronous on `stream`.
 int launch_rgb_to_yuv(const uint8_t* rgb, int dw, int dh, uint8_t* yuv, int W, int H, void* stream);
-int launch_search(const SearchParams& p, int grid, void* stream);
+// Launch plan of the search wavefront (chosen once per encoder).  fused: the SAD table is
+// computed inside the same cooperative launch by `grid - nrow` worker CTAs.
+struct SearchPlan {
+    bool fused;
+    int grid, nrow, threads;
+    size_t smem;
+};
+int search_plan(int sr, int W, int BH, bool table, bool small, SearchPlan* out);
+int launch_search(const SearchParams& p, const SearchPlan& plan, void* stream);
 bool search_use_table(int sr);
 int sad_table_stride(int sr);
 int launch_sad_table(const uint8_t* ref, const uint8_t* cur, int W, int H, int sr, uint16_t* tab, int tstride,
                      void* stream);
-int search_max_grid(int sr, int W, bool table, bool small, int* grid_out);
 size_t search_smem_bytes(int sr);
 int launch_predict(const uint8_t* ref, const MbOut* mb, uint8_t* pred, uint2* varsum, int W, int H, void* stream);
 int launch_aq(const uint2* varsum, int n, float base, const uint32_t* logfix, int nlog, const uint32_t* expfix,

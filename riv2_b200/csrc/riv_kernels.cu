@@ -213,28 +213,34 @@ __device__ __forceinline__ void fill_chunk(uint8_t* band, int BWB, int WS, int c
 // (per-4x4 sub-block clamped reference origin at frame edges,
 // enc/motion/satd_scalar.rs:26-97; the plain 16x16 SAD elsewhere).  Values <= 65280.
 // ---------------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_sad_table(const uint8_t* __restrict__ ref, const uint8_t* __restrict__ cur,
-                                                   int W, int H, int BW, int sr, uint16_t* __restrict__ tab,
-                                                   int tstride) {
-    extern __shared__ __align__(16) uint8_t sm[];
+// One MB's table row by the whole CTA (at least 64 threads); `sm` holds the window and the
+// current block.
+// tid/nthr: this thread's index and the thread count of the group computing the MB; bar_id 0
+// = the whole CTA (__syncthreads), else a named barrier of the group's nthr threads.
+__device__ __forceinline__ void group_sync(int bar_id, int nthr) {
+    if (bar_id == 0) __syncthreads();
+    else asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthr) : "memory");
+}
+__device__ __forceinline__ void sad_table_mb(const uint8_t* __restrict__ ref, const uint8_t* __restrict__ cur, int W,
+                                             int H, int BW, int sr, uint16_t* __restrict__ tab, int tstride, int mb,
+                                             uint8_t* sm, int tid, int nthr, int bar_id) {
     const int WT = 16 + 2 * sr;                 // window side
     const int WTS = (WT + 8 + 15) & ~15;        // row stride (+ slack for the 24-byte row reads)
     uint8_t* win = sm;
     uint32_t* cw = (uint32_t*)(sm + WT * WTS + 16);  // 64 words of the current block
-    const int mb = blockIdx.x;
     const int bx = mb % BW, by = mb / BW;
     const int x0 = bx * 16, y0 = by * 16;
     const int wx0 = x0 - sr, wy0 = y0 - sr;
-    for (int i = threadIdx.x; i < WT * WT; i += blockDim.x) {
+    for (int i = tid; i < WT * WT; i += nthr) {
         int r = i / WT, c = i - r * WT;
         int gy = min(max(wy0 + r, 0), H - 1), gx = min(max(wx0 + c, 0), W - 1);
         win[r * WTS + c] = ref[(size_t)gy * W + gx];
     }
-    if (threadIdx.x < 64) {
-        int r = threadIdx.x >> 2, g = threadIdx.x & 3;
-        cw[threadIdx.x] = *(const uint32_t*)(cur + (size_t)(y0 + r) * W + x0 + 4 * g);
+    if (tid < 64) {
+        int r = tid >> 2, g = tid & 3;
+        cw[tid] = *(const uint32_t*)(cur + (size_t)(y0 + r) * W + x0 + 4 * g);
     }
-    __syncthreads();
+    group_sync(bar_id, nthr);
     const int side = 2 * sr + 1, P = side * side;
     const bool interior = x0 - sr >= 0 && y0 - sr >= 0 && x0 + 15 + sr <= W - 1 && y0 + 15 + sr <= H - 1;
     uint16_t* out = tab + (size_t)mb * tstride;
@@ -243,7 +249,7 @@ __global__ void __launch_bounds__(128) k_sad_table(const uint8_t* __restrict__ r
         // reference rows start at window column 8q (4-byte aligned), so the shifted words
         // come from aligned loads with compile-time funnel shifts.
         const int nq = (side + 7) >> 3;
-        for (int item = threadIdx.x; item < side * nq; item += blockDim.x) {
+        for (int item = tid; item < side * nq; item += nthr) {
             const int dyi = item / nq, q = item - dyi * nq;
             unsigned acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll 2
@@ -268,7 +274,7 @@ __global__ void __launch_bounds__(128) k_sad_table(const uint8_t* __restrict__ r
                 if (8 * q + j < side) out[dyi * side + 8 * q + j] = (uint16_t)acc[j];
         }
     } else {
-        for (int pidx = threadIdx.x; pidx < P; pidx += blockDim.x) {
+        for (int pidx = tid; pidx < P; pidx += nthr) {
             const int dy = pidx / side - sr, dx = pidx % side - sr;
             unsigned s = 0;
             for (int r = 0; r < 16; r++) {
@@ -283,6 +289,13 @@ __global__ void __launch_bounds__(128) k_sad_table(const uint8_t* __restrict__ r
             out[pidx] = (uint16_t)s;
         }
     }
+}
+
+__global__ void __launch_bounds__(128) k_sad_table(const uint8_t* __restrict__ ref, const uint8_t* __restrict__ cur,
+                                                   int W, int H, int BW, int sr, uint16_t* __restrict__ tab,
+                                                   int tstride) {
+    extern __shared__ __align__(16) uint8_t sm[];
+    sad_table_mb(ref, cur, W, H, BW, sr, tab, tstride, blockIdx.x, sm, threadIdx.x, blockDim.x, 0);
 }
 size_t sad_table_smem(int sr) {
     int WT = 16 + 2 * sr, WTS = (WT + 8 + 15) & ~15;
@@ -393,7 +406,7 @@ __device__ __forceinline__ void mode_warp(const SearchParams& p, const unsigned 
     };
     const bool has_tm = p.prev_coded != nullptr;
     int n = 0;
-    for (int r = blockIdx.x; r < p.BH; r += gridDim.x) {
+    for (int r = blockIdx.x; r < p.BH; r += p.nrow_ctas) {
         MvT L_cod{0, 0, 0, 0};
         unsigned long long vT = 0, vTL = 0;
         for (int bx = 0; bx < p.BW; bx++) {
@@ -519,6 +532,41 @@ __device__ __forceinline__ void mode_warp(const SearchParams& p, const unsigned 
     }
 }
 
+__device__ __forceinline__ size_t sad_table_smem_dev(int sr) {
+    const int WT = 16 + 2 * sr, WTS = (WT + 8 + 15) & ~15;
+    return ((size_t)WT * WTS + 16 + 256 + 15) & ~(size_t)15;
+}
+// ---- table workers of the fused search launch: the CTAs beyond the row CTAs compute the
+// SAD-table rows in raster order while the wavefront runs, and publish each MB's row with a
+// flag holding the frame tag (release after the CTA's writes; the loader acquires it).
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+constexpr int TW_GROUP = 128;  // threads per table-worker group (one MB at a time)
+__device__ __forceinline__ void table_worker(const SearchParams& p, uint8_t* sm) {
+    const int groups = blockDim.x / TW_GROUP, g = threadIdx.x / TW_GROUP, tid = threadIdx.x % TW_GROUP;
+    if (g >= groups) return;
+    const int nw = (gridDim.x - p.nrow_ctas) * groups, w = (blockIdx.x - p.nrow_ctas) * groups + g;
+    uint8_t* gsm = sm + (size_t)g * sad_table_smem_dev(p.sr);
+    const int n = p.BW * p.BH;
+    for (int mb = w; mb < n; mb += nw) {
+        sad_table_mb(p.ref_y, p.cur_y, p.W, p.H, p.BW, p.sr, const_cast<uint16_t*>(p.tab), p.tstride, mb, gsm, tid,
+                     TW_GROUP, 1 + g);
+        group_sync(1 + g, TW_GROUP);
+        if (tid == 0) {
+            __threadfence();
+            st_release_u32(p.tflag + mb, p.tag);
+        }
+        group_sync(1 + g, TW_GROUP);
+    }
+}
+
 // ---- mbarrier and bulk-copy helpers (sm_90+ PTX; no multicast)
 __device__ __forceinline__ uint32_t sa32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
@@ -583,7 +631,7 @@ __device__ __forceinline__ void loader_warp(const SearchParams& p, unsigned long
         }
         return __shfl_sync(0xffffffffu, ok, 0) != 0;
     };
-    for (int r = blockIdx.x; r < p.BH && !abort; r += gridDim.x) {
+    for (int r = blockIdx.x; r < p.BH && !abort; r += p.nrow_ctas) {
         const int wy0 = r * 16 - sr - 1;
         if (rows > 0 && !wait_ctl(1, rows)) { abort = true; break; }
         // ---- the band: rows wy0 .. wy0+WS-1 (edge-clamped), columns -MARGIN .. W+MARGIN-1
@@ -608,6 +656,18 @@ __device__ __forceinline__ void loader_warp(const SearchParams& p, unsigned long
             const int s = n & (LD_RING - 1);
             if (n >= LD_RING && !wait_ctl(0, n - LD_RING + 1)) { abort = true; break; }
             uint8_t* slot = slots + (size_t)s * SLOT;
+            if (p.tflag != nullptr) {  // fused launch: wait until a table worker published this MB's row
+                int ok = 1;
+                if (lane == 0) {
+                    long long spins = 0;
+                    while (ld_acquire_u32(p.tflag + idx) != p.tag) {
+                        if (ctl[2] != 0 || ++spins > p.spin_limit) { ok = 0; break; }
+                        __nanosleep(32);
+                    }
+                    asm volatile("fence.proxy.async.global;" ::: "memory");  // generic writes -> bulk-copy reads
+                }
+                if (!__shfl_sync(0xffffffffu, ok, 0)) { abort = true; break; }
+            }
             if (lane < 16)
                 bulk_g2s(slot + tab_bytes + lane * 16, p.cur_y + (size_t)(r * 16 + lane) * p.W + bx * 16, 16u, fullb + s);
             if (lane == 0) {
@@ -636,11 +696,15 @@ __device__ __forceinline__ void loader_warp(const SearchParams& p, unsigned long
 }
 
 template <bool BAND, bool TABLE, bool SMALL>
-__global__ void __launch_bounds__(96, 1) k_search(SearchParams p) {
+__global__ void __launch_bounds__(512, 1) k_search(SearchParams p) {
     // FAST (band + table): three warps -- search chain, mode decision, loader.  Otherwise the
     // search warp stages its own data with cp.async and the third warp is not launched.
     constexpr bool FAST = BAND && TABLE;
     extern __shared__ __align__(16) uint8_t smem[];
+    if (FAST && p.tflag != nullptr && (int)blockIdx.x >= p.nrow_ctas) {
+        table_worker(p, smem);
+        return;
+    }
     double* bits = (double*)smem;                 // 256 doubles
     int* nc32s = (int*)(smem + 256 * sizeof(double));  // 64 x 64 NEW costs (small mode)
     unsigned long long* hand = (unsigned long long*)(smem + 256 * sizeof(double) + 64 * 64 * 4);  // HAND_RING
@@ -679,7 +743,7 @@ __global__ void __launch_bounds__(96, 1) k_search(SearchParams p) {
     __syncthreads();
     const unsigned long long tagbits = (unsigned long long)(p.tag & 0xffffu) << 48;
     if (threadIdx.x >= 64) {
-        if (FAST) loader_warp(p, fullb, bandb, ld_ctl, slots, refmem);
+        if (FAST && threadIdx.x < 96) loader_warp(p, fullb, bandb, ld_ctl, slots, refmem);
         return;
     }
     if (threadIdx.x >= 32) {
@@ -696,7 +760,7 @@ __global__ void __launch_bounds__(96, 1) k_search(SearchParams p) {
     bool failed = false;
     int hn = 0;  // MBs handed to the mode warp so far
 
-    for (int r = blockIdx.x; r < p.BH; r += gridDim.x) {
+    for (int r = blockIdx.x; r < p.BH; r += p.nrow_ctas) {
         const int y0 = r * 16;
         const int wy0 = y0 - sr - 1;
         __syncwarp();
@@ -1311,32 +1375,63 @@ static const void* search_fn(bool band, bool table, bool small) {
 
 size_t search_smem_bytes(int sr) { return search_smem(sr, 0, false, search_use_table(sr)); }
 
-int search_max_grid(int sr, int W, bool table, bool small, int* grid_out) {
-    bool band = search_use_band(sr, W);
-    size_t sm = search_smem(sr, W, band, table);
+int search_plan(int sr, int W, int BH, bool table, bool small, SearchPlan* out) {
+    const bool band = search_use_band(sr, W);
     const void* fn = search_fn(band, table, table && small);
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return (int)e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, search_threads(band, table), sm);
-    if (e != cudaSuccess) return (int)e;
+    const int threads = search_threads(band, table);
     int dev = 0, nsm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    *grid_out = per_sm * nsm;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return (int)e;
+    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return (int)e;
+    auto resident = [&](size_t sm, int nthreads, int* per_sm) {
+        cudaError_t r = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (r == cudaSuccess) r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, fn, nthreads, sm);
+        return r;
+    };
+    const size_t sm = search_smem(sr, W, band, table);
+    SearchPlan pl{};
+    pl.threads = threads;
+    if (band && table) {
+        // fused: one CTA per SM (the shared-memory request rules out a second), rows first,
+        // table workers on the SMs the rows leave free -- used when enough of them remain
+        const size_t smf = sm > (size_t)116 * 1024 ? sm : (size_t)116 * 1024;
+        int per_sm = 0;
+        e = resident(smf, 4 * 128, &per_sm);
+        if (e != cudaSuccess) return (int)e;
+        const int total = per_sm * nsm;
+        const int nrow = BH < total ? BH : total;
+        const size_t gsm = ((size_t)sad_table_smem(sr) + 15) & ~(size_t)15;
+        if (per_sm == 1 && total - nrow >= 32 && 4 * gsm <= smf) {
+            pl.fused = true;
+            pl.threads = 4 * 128;  // row CTAs use three warps; table workers four groups of 128
+            pl.smem = smf;
+            pl.nrow = nrow;
+            pl.grid = total;
+            *out = pl;
+            return 0;
+        }
+    }
+    int per_sm = 0;
+    e = resident(sm, threads, &per_sm);
+    if (e != cudaSuccess) return (int)e;
+    pl.fused = false;
+    pl.smem = sm;
+    pl.grid = pl.nrow = BH < per_sm * nsm ? BH : per_sm * nsm;
+    *out = pl;
     return 0;
 }
 
-int launch_search(const SearchParams& p, int grid, void* stream) {
-    bool band = search_use_band(p.sr, p.W), table = p.tab != nullptr;
-    size_t sm = search_smem(p.sr, p.W, band, table);
+int launch_search(const SearchParams& p, const SearchPlan& plan, void* stream) {
+    const bool band = search_use_band(p.sr, p.W), table = p.tab != nullptr;
     SearchParams q = p;
+    q.nrow_ctas = plan.nrow;
+    if (!plan.fused) q.tflag = nullptr;
     void* args[] = {&q};
     // Cooperative launch: every CTA of the grid is co-resident, so the row-to-row waits
-    // can always make progress.
-    cudaError_t e = cudaLaunchCooperativeKernel(search_fn(band, table, table && p.small), dim3(grid),
-                                                dim3(search_threads(band, table)), args, sm,
-                                                (cudaStream_t)stream);
+    // and the waits for table rows can always make progress.
+    cudaError_t e = cudaLaunchCooperativeKernel(search_fn(band, table, table && p.small), dim3(plan.grid),
+                                                dim3(plan.threads), args, plan.smem, (cudaStream_t)stream);
     return (int)e;
 }
 
