@@ -134,11 +134,16 @@ riv_status riv_stage_rgb_to_yuv(const uint8_t* rgb, uint32_t dw, uint32_t dh, ui
                                 uint8_t* yuv_out);
 /* deblock_yuv420 (com/deblock.rs:189-202); mask: one byte per MB or NULL. */
 riv_status riv_stage_deblock(uint8_t* yuv, uint32_t w, uint32_t h, int level, int intra, const uint8_t* mask);
-/* No reference counterpart.  riv_stage_deblock without any device allocation: the planes
- * and the optional mask are staged in one fixed device scratch area (a file-scope
- * __device__ array of RIV_DEBLOCK_NOALLOC_MAX_BYTES bytes, 256-byte aligned) instead of
- * memory allocated and freed on every call.  Same arguments and result as
- * riv_stage_deblock, on the current CUDA device.
+/* No reference counterpart.  riv_stage_deblock without any device allocation, for callers
+ * that cannot call cudaMalloc/cudaFree around each stage: applications whose device
+ * memory is handed in full to their own pool allocator (a framework's caching allocator),
+ * where a raw cudaMalloc fails or fragments the pool, and latency-critical threads, where
+ * cudaFree would synchronise the whole device and stall the work already in flight.  The
+ * planes and the optional mask are staged in one fixed device scratch area (a file-scope
+ * __device__ array of RIV_DEBLOCK_NOALLOC_MAX_BYTES bytes, 256-byte aligned, held by every
+ * GPU that loads the library until the process exits) instead of memory allocated and
+ * freed on every call.  Same arguments and result as riv_stage_deblock, on the current
+ * CUDA device.
  * Limit: w*h*3/2 bytes, plus (w/16)*(h/16) when mask != NULL, at most
  * RIV_DEBLOCK_NOALLOC_MAX_BYTES (4 MiB: storage sizes up to 1920x1088); larger requests
  * return RIV_ERR_FRAME and write the reason to errbuf (nullable, errbuf_len bytes).

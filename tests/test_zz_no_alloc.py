@@ -1,6 +1,10 @@
 """The no-allocation deblock entry point (riv_stage_deblock_noalloc) against the existing
-riv_stage_deblock: identical planes over two calls in a row (the fixed device scratch
-carries nothing from one call to the next), and the size limit rejected with a message."""
+riv_stage_deblock.  It serves callers that cannot allocate device memory per call (their
+memory belongs to their own pool allocator, or cudaFree's device-wide synchronisation would
+stall a latency-critical thread).  Checked: identical planes over two calls in a row (the
+fixed device scratch carries nothing from one call to the next), and the size limit
+rejected with a message.  Collected last, so a run that stops at its first failure has
+already run every other test."""
 import ctypes as C
 
 import numpy as np
