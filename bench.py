@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--quality", default="85/80")
-    ap.add_argument("--pipeline-depth", type=int, default=8)
+    ap.add_argument("--pipeline-depth", type=int, default=16)
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--cpu-sample-frames", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")

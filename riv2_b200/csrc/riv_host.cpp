@@ -276,8 +276,9 @@ struct MappedBuf {
     T* dev() const { return (T*)d; }
 };
 
-enum { EV_START, EV_YUV, EV_TABLE, EV_SEARCH, EV_PRED, EV_AQ, EV_RES, EV_DEBLOCK, EV_COMPACT, EV_N };
-static const int NSTAGE = EV_N - 1;  // + total
+// Per-frame timing events: Y = input stream, S = main chain, K = compaction stream.
+enum { EV_START, EV_YUV, EV_S0, EV_TABLE, EV_SEARCH, EV_PRED, EV_AQ, EV_RES, EV_DEBLOCK, EV_K0, EV_COMPACT, EV_N };
+static const int NSTAGE = 8;  // rgb->yuv, table, search, predict, aq, residual, deblock, compact (+ total)
 
 struct Slot {
     DevBuf rgb, dside, dpacked, dpeobs;        // compacted frame output on the device
@@ -310,9 +311,17 @@ struct riv_encoder {
     uint64_t header_pos = 0, frame_count = 0, submitted = 0;
     int W = 0, H = 0, BW = 0, BH = 0, NMB = 0;
     size_t yuv_bytes = 0;
-    cudaStream_t S = nullptr, C = nullptr, Hs = nullptr;  // compute, device->host, host->device
+    cudaStream_t S = nullptr, C = nullptr, Hs = nullptr;  // main chain, device->host, host->device
+    cudaStream_t Y = nullptr, K = nullptr;                // input conversion, compaction
+    // cross-stream reuse guards: cur[k] free (its residual is done), mbout[k] and the
+    // coefficient buffers free (their compaction is done)
+    cudaEvent_t ev_cur_free[2] = {}, ev_mbout_free[2] = {}, ev_coef_free = nullptr;
+    // the last search launch: input conversion waits for it, so that it never holds SMs the
+    // next cooperative search launch needs
+    cudaEvent_t ev_search_done = nullptr;
+    int fpar = 0, last_par = 0;  // double-buffer index of the next / last submitted frame
     // device state
-    DevBuf cur, ref[2], pred, mbout, coded[2], rec, varsum, lnv, qs, coeffs, opt_skip, fmask, eobs, status;
+    DevBuf curb[2], ref[2], recon_pre, pred, mboutb[2], coded[2], rec, varsum, lnv, qs, coeffs, opt_skip, fmask, eobs, status;
     DevBuf cindex, coffset, sadtab;
     DevBuf mvbits, logfix, expfix, ytab, ctab, newcost, newcost32;
     bool small_costs = false;
@@ -378,15 +387,26 @@ static void setup_device(riv_encoder* e) {
     CK(cudaStreamCreateWithFlags(&e->S, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&e->C, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&e->Hs, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&e->Y, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&e->K, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; k++) {
+        CK(cudaEventCreateWithFlags(&e->ev_cur_free[k], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&e->ev_mbout_free[k], cudaEventDisableTiming));
+    }
+    CK(cudaEventCreateWithFlags(&e->ev_coef_free, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&e->ev_search_done, cudaEventDisableTiming));
     int32_t t16[256], t8[64];
     dct_tables(t16, t8);
     CK(riv_upload_dct_tables(t16, t8));
     const int N = e->NMB;
-    e->cur.alloc(e->yuv_bytes);
+    e->curb[0].alloc(e->yuv_bytes);
+    e->curb[1].alloc(e->yuv_bytes);
     e->ref[0].alloc(e->yuv_bytes);
     e->ref[1].alloc(e->yuv_bytes);
+    e->recon_pre.alloc(e->yuv_bytes);  // reconstruction before the (out-of-place) deblock
     e->pred.alloc(e->yuv_bytes);
-    e->mbout.alloc((size_t)N * sizeof(MbOut));
+    e->mboutb[0].alloc((size_t)N * sizeof(MbOut));
+    e->mboutb[1].alloc((size_t)N * sizeof(MbOut));
     e->coded[0].alloc((size_t)N * 4);
     e->coded[1].alloc((size_t)N * 4);
     e->rec.alloc((size_t)2 * N * sizeof(MbRec));  // raw-MV records, then coded-MV records
@@ -495,39 +515,50 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
     const riv_config& c = e->cfg;
     Slot& s = e->slots[j.slot];
     const int W = e->W, H = e->H, N = e->NMB;
-    cudaStream_t S = e->S;
-    CK(cudaEventRecord(s.ev_k[EV_START], S));
-    // kernels per frame: rgb->yuv, (search, predict, 3 x aq), residual, deblock (2 per plane), scan + pack
-    const int nplanes_db = 3 * 2;
+    cudaStream_t S = e->S, Y = e->Y, K = e->K;
+    const int ck = e->fpar;  // this frame's input planes and per-MB output buffers
+    uint8_t* cur = e->curb[ck].as<uint8_t>();
+    MbOut* mbo = e->mboutb[ck].as<MbOut>();
+    // kernels per frame: rgb->yuv, (search, predict, 3 x aq), residual, deblock, scan + pack
+    const int nplanes_db = 1;  // one launch for the three planes
     e->launches += (src == 2 ? 0 : 1) + (j.type == 2 ? 5 + (e->table_ok && !e->splan.fused ? 1 : 0) : 0) + 1 +
-                   ((j.type == 2 ? e->inter_level : e->intra_level) > 0 ? nplanes_db : 0) + 3;
+                   ((j.type == 2 ? e->inter_level : e->intra_level) > 0 ? nplanes_db : 0) + 2;
     if (src == 0) e->h2d_bytes += (uint64_t)c.display_width * c.display_height * 3;
     if (src == 2) e->h2d_bytes += e->yuv_bytes;
+    // ---- input conversion on Y, overlapping the previous frame's main chain; cur[ck] is
+    // free once the residual of the frame two back has read it
+    CK(cudaStreamWaitEvent(Y, e->ev_cur_free[ck], 0));
+    CK(cudaStreamWaitEvent(Y, e->ev_search_done, 0));
     if (src == 0) {
         CK(cudaMemcpyAsync(s.rgb.p, a, (size_t)c.display_width * c.display_height * 3, cudaMemcpyHostToDevice, e->Hs));
         CK(cudaEventRecord(s.ev_h2d, e->Hs));
-        CK(cudaStreamWaitEvent(S, s.ev_h2d, 0));
-        CK(launch_rgb_to_yuv((const uint8_t*)s.rgb.p, (int)c.display_width, (int)c.display_height, e->cur.as<uint8_t>(), W, H, S));
+        CK(cudaStreamWaitEvent(Y, s.ev_h2d, 0));
+        CK(cudaEventRecord(s.ev_k[EV_START], Y));
+        CK(launch_rgb_to_yuv((const uint8_t*)s.rgb.p, (int)c.display_width, (int)c.display_height, cur, W, H, Y));
     } else if (src == 1) {
-        CK(launch_rgb_to_yuv((const uint8_t*)a, (int)c.display_width, (int)c.display_height, e->cur.as<uint8_t>(), W, H, S));
+        CK(cudaEventRecord(s.ev_k[EV_START], Y));
+        CK(launch_rgb_to_yuv((const uint8_t*)a, (int)c.display_width, (int)c.display_height, cur, W, H, Y));
     } else {
-        // staged through the slot buffer: the previous frame's kernels may still read `cur`
         uint8_t* d = s.rgb.as<uint8_t>();
         size_t ys = (size_t)W * H, cs = ys / 4;
         CK(cudaMemcpyAsync(d, a, ys, cudaMemcpyHostToDevice, e->Hs));
         CK(cudaMemcpyAsync(d + ys, b, cs, cudaMemcpyHostToDevice, e->Hs));
         CK(cudaMemcpyAsync(d + ys + cs, c3, cs, cudaMemcpyHostToDevice, e->Hs));
         CK(cudaEventRecord(s.ev_h2d, e->Hs));
-        CK(cudaStreamWaitEvent(S, s.ev_h2d, 0));
-        CK(cudaMemcpyAsync(e->cur.p, d, e->yuv_bytes, cudaMemcpyDeviceToDevice, S));
+        CK(cudaStreamWaitEvent(Y, s.ev_h2d, 0));
+        CK(cudaEventRecord(s.ev_k[EV_START], Y));
+        CK(cudaMemcpyAsync(cur, d, e->yuv_bytes, cudaMemcpyDeviceToDevice, Y));
     }
-    CK(cudaEventRecord(s.ev_k[EV_YUV], S));
+    CK(cudaEventRecord(s.ev_k[EV_YUV], Y));
+    // ---- main chain on S
+    CK(cudaStreamWaitEvent(S, s.ev_k[EV_YUV], 0));
+    CK(cudaEventRecord(s.ev_k[EV_S0], S));
     const int nxt = e->ref_cur ^ 1;
     uint8_t* recon = e->ref[nxt].as<uint8_t>();
     ResidualParams rp{};
-    rp.cur = e->cur.as<uint8_t>();
+    rp.cur = cur;
     rp.pred = e->pred.as<uint8_t>();
-    rp.recon = recon;
+    rp.recon = recon;  // or recon_pre when a deblock follows (set per frame type below)
     rp.coeffs = e->coeffs.as<int16_t>();
     rp.opt_skip = e->opt_skip.as<uint8_t>();
     rp.fmask = e->fmask.as<uint8_t>();
@@ -542,18 +573,19 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         CK(cudaEventRecord(s.ev_k[EV_SEARCH], S));
         CK(cudaEventRecord(s.ev_k[EV_PRED], S));
         CK(cudaEventRecord(s.ev_k[EV_AQ], S));
+        CK(cudaStreamWaitEvent(S, e->ev_coef_free, 0));  // the previous frame's compaction read them
+        if (e->intra_level > 0) rp.recon = e->recon_pre.as<uint8_t>();
         CK(launch_residual(rp, N, S));
         CK(cudaEventRecord(s.ev_k[EV_RES], S));
-        if (e->intra_level > 0) CK(launch_deblock(recon, W, H, e->intra_E, e->intra_I, e->intra_H, nullptr, S));
+        CK(cudaEventRecord(e->ev_cur_free[ck], S));
+        if (e->intra_level > 0)
+            CK(launch_deblock_tiled(e->recon_pre.as<uint8_t>(), recon, W, H, e->intra_E, e->intra_I, e->intra_H, nullptr, S));
         CK(cudaEventRecord(s.ev_k[EV_DEBLOCK], S));
-        CK(launch_compact(e->opt_skip.as<uint8_t>(), e->mbout.as<MbOut>(), e->coeffs.as<int16_t>(), e->eobs.as<uint8_t>(), N, 1,
-                          e->cindex.as<int32_t>(), e->coffset.as<int32_t>(), s.dside.as<uint32_t>(),
-                          s.dpacked.as<int16_t>(), s.dpeobs.as<uint8_t>(), s.hdr.dev<uint32_t>(), S));
         e->has_prev_mvs = false;
     } else {
         SearchParams sp{};
         sp.ref_y = e->ref[e->ref_cur].as<uint8_t>();
-        sp.cur_y = e->cur.as<uint8_t>();
+        sp.cur_y = cur;
         sp.W = W; sp.H = H; sp.BW = e->BW; sp.BH = e->BH; sp.sr = c.search_range;
         sp.prev_coded = e->has_prev_mvs ? e->coded[e->coded_cur].as<int8_t>() : nullptr;
         sp.zthr = c.me_zero_mv_threshold;
@@ -579,7 +611,7 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         e->tag = (e->tag + 1) & 0xffffu;
         if (e->tag == 0) e->tag = 1;
         sp.tag = e->tag;
-        sp.out = e->mbout.as<MbOut>();
+        sp.out = mbo;
         sp.status = e->status.as<unsigned>();
         sp.spin_limit = 1ll << 22;  // ~ a few seconds, far above any legitimate wait
         sp.tab = nullptr;
@@ -593,35 +625,50 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         }
         CK(cudaEventRecord(s.ev_k[EV_TABLE], S));
         sp.prof = e->prof.as<long long>();
-        CK(launch_search(sp, e->splan, S));
-        CK(cudaEventRecord(s.ev_k[EV_SEARCH], S));
         // coded MVs of this frame become next frame's temporal predictors
         const int cn = e->coded_cur ^ 1;
-        CK(cudaMemcpy2DAsync(e->coded[cn].p, 4, (const char*)e->mbout.p + offsetof(MbOut, coded), sizeof(MbOut), 4, N,
-                             cudaMemcpyDeviceToDevice, S));
-        CK(launch_predict(e->ref[e->ref_cur].as<uint8_t>(), e->mbout.as<MbOut>(), e->pred.as<uint8_t>(), e->varsum.as<uint2>(), W, H, S));
+        sp.coded_out = e->coded[cn].as<int8_t>();
+        CK(cudaStreamWaitEvent(S, e->ev_mbout_free[ck], 0));  // compaction of the frame two back
+        CK(launch_search(sp, e->splan, S));
+        CK(cudaEventRecord(s.ev_k[EV_SEARCH], S));
+        CK(cudaEventRecord(e->ev_search_done, S));
+        CK(launch_predict(e->ref[e->ref_cur].as<uint8_t>(), mbo, e->pred.as<uint8_t>(), e->varsum.as<uint2>(), W, H, S));
         CK(cudaEventRecord(s.ev_k[EV_PRED], S));
         CK(launch_aq(e->varsum.as<uint2>(), N, e->inter_base, e->logfix.as<uint32_t>(), e->nlog, e->expfix.as<uint32_t>(),
                      e->nexp, e->lnv.as<float>(), e->qs.as<float>(), S));
         CK(cudaEventRecord(s.ev_k[EV_AQ], S));
         rp.intra = 0;
-        rp.mb = e->mbout.as<MbOut>();
+        rp.mb = mbo;
         rp.qs = e->qs.as<float>();
+        CK(cudaStreamWaitEvent(S, e->ev_coef_free, 0));  // the previous frame's compaction read them
+        if (e->inter_level > 0) rp.recon = e->recon_pre.as<uint8_t>();
         CK(launch_residual(rp, N, S));
         CK(cudaEventRecord(s.ev_k[EV_RES], S));
-        if (e->inter_level > 0) CK(launch_deblock(recon, W, H, e->inter_E, e->inter_I, e->inter_H, e->fmask.as<uint8_t>(), S));
+        CK(cudaEventRecord(e->ev_cur_free[ck], S));
+        if (e->inter_level > 0)
+            CK(launch_deblock_tiled(e->recon_pre.as<uint8_t>(), recon, W, H, e->inter_E, e->inter_I, e->inter_H,
+                                    e->fmask.as<uint8_t>(), S));
         CK(cudaEventRecord(s.ev_k[EV_DEBLOCK], S));
-        CK(launch_compact(e->opt_skip.as<uint8_t>(), e->mbout.as<MbOut>(), e->coeffs.as<int16_t>(), e->eobs.as<uint8_t>(), N, 0,
-                          e->cindex.as<int32_t>(), e->coffset.as<int32_t>(), s.dside.as<uint32_t>(),
-                          s.dpacked.as<int16_t>(), s.dpeobs.as<uint8_t>(), s.hdr.dev<uint32_t>(), S));
         e->coded_cur = cn;
         e->has_prev_mvs = true;
     }
-    CK(cudaEventRecord(s.ev_k[EV_COMPACT], S));
-    CK(cudaMemcpyAsync(s.hdr.host<uint32_t>() + 2, e->status.p, 4, cudaMemcpyDeviceToHost, S));
-    CK(cudaEventRecord(s.ev_gpu, S));
+    // ---- compaction on K once the frame's main chain is done: run alone it takes a few
+    // microseconds, while beside the deblock it delays the next (cooperative, whole-GPU)
+    // search launch by longer
+    CK(cudaStreamWaitEvent(K, s.ev_k[EV_DEBLOCK], 0));
+    CK(cudaEventRecord(s.ev_k[EV_K0], K));
+    CK(launch_compact(e->opt_skip.as<uint8_t>(), mbo, e->coeffs.as<int16_t>(), e->eobs.as<uint8_t>(), N, j.type == 1 ? 1 : 0,
+                      e->cindex.as<int32_t>(), e->coffset.as<int32_t>(), s.dside.as<uint32_t>(), s.dpacked.as<int16_t>(),
+                      s.dpeobs.as<uint8_t>(), s.hdr.dev<uint32_t>(), K));
+    CK(cudaEventRecord(e->ev_coef_free, K));
+    CK(cudaEventRecord(e->ev_mbout_free[ck], K));
+    CK(cudaEventRecord(s.ev_k[EV_COMPACT], K));
+    CK(cudaMemcpyAsync(s.hdr.host<uint32_t>() + 2, e->status.p, 4, cudaMemcpyDeviceToHost, K));
+    CK(cudaEventRecord(s.ev_gpu, K));
     e->ref_cur = nxt;
     e->has_ref = true;
+    e->last_par = ck;
+    e->fpar ^= 1;
     // DMA the side info, EOBs and (a bounded prefix of) the coefficients on the copy
     // stream; the exact size is only known once the frame is done.
     CK(cudaStreamWaitEvent(e->C, s.ev_gpu, 0));
@@ -659,8 +706,11 @@ static riv_status retire(riv_encoder* e, Job& j) {
     e->coef_guess = coef_bytes + coef_bytes / 4 + 65536;
     e->d2h_bytes += (uint64_t)e->NMB * 7 + 12 + std::max(coef_bytes, s.prefetched);
     float t[NSTAGE + 1] = {0};
-    for (int k = 0; k < NSTAGE; k++) cudaEventElapsedTime(&t[k], s.ev_k[k], s.ev_k[k + 1]);
-    cudaEventElapsedTime(&t[NSTAGE], s.ev_k[EV_START], s.ev_k[EV_COMPACT]);
+    CK(cudaEventSynchronize(s.ev_k[EV_DEBLOCK]));  // the D2H did not wait for the deblock
+    const int spans[NSTAGE + 1][2] = {{EV_START, EV_YUV},   {EV_S0, EV_TABLE},  {EV_TABLE, EV_SEARCH},
+                                      {EV_SEARCH, EV_PRED}, {EV_PRED, EV_AQ},   {EV_AQ, EV_RES},
+                                      {EV_RES, EV_DEBLOCK}, {EV_K0, EV_COMPACT}, {EV_S0, EV_DEBLOCK}};
+    for (int k = 0; k <= NSTAGE; k++) cudaEventElapsedTime(&t[k], s.ev_k[spans[k][0]], s.ev_k[spans[k][1]]);
     for (int k = 0; k <= NSTAGE; k++) j.times[k] = t[k] * 1000.0f;
     if (j.type == 2) {
         for (int k = 0; k <= NSTAGE; k++) e->sum_times[k] += j.times[k];
@@ -983,6 +1033,8 @@ void riv_encoder_free(riv_encoder* e) {
     if (e->S) cudaStreamSynchronize(e->S);
     if (e->C) cudaStreamSynchronize(e->C);
     if (e->Hs) cudaStreamSynchronize(e->Hs);
+    if (e->Y) cudaStreamSynchronize(e->Y);
+    if (e->K) cudaStreamSynchronize(e->K);
     for (auto& s : e->slots) {
         s.rgb.release(); s.dside.release(); s.dpacked.release(); s.dpeobs.release();
         s.side.release(); s.packed.release(); s.peobs.release(); s.hdr.release();
@@ -992,13 +1044,22 @@ void riv_encoder_free(riv_encoder* e) {
         for (int k = 0; k < EV_N; k++)
             if (s.ev_k[k]) cudaEventDestroy(s.ev_k[k]);
     }
-    DevBuf* bufs[] = {&e->cur, &e->ref[0], &e->ref[1], &e->pred, &e->mbout, &e->coded[0], &e->coded[1], &e->rec,
+    DevBuf* bufs[] = {&e->curb[0], &e->curb[1], &e->ref[0], &e->ref[1], &e->recon_pre, &e->pred, &e->mboutb[0], &e->mboutb[1],
+                      &e->coded[0], &e->coded[1], &e->rec,
                       &e->varsum, &e->lnv, &e->qs, &e->coeffs, &e->opt_skip, &e->fmask, &e->eobs, &e->status,
                       &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset, &e->sadtab, &e->prof, &e->tflag, &e->newcost, &e->newcost32};
     for (DevBuf* b : bufs) b->release();
     if (e->S) cudaStreamDestroy(e->S);
     if (e->C) cudaStreamDestroy(e->C);
     if (e->Hs) cudaStreamDestroy(e->Hs);
+    if (e->Y) cudaStreamDestroy(e->Y);
+    if (e->K) cudaStreamDestroy(e->K);
+    for (int k = 0; k < 2; k++) {
+        if (e->ev_cur_free[k]) cudaEventDestroy(e->ev_cur_free[k]);
+        if (e->ev_mbout_free[k]) cudaEventDestroy(e->ev_mbout_free[k]);
+    }
+    if (e->ev_coef_free) cudaEventDestroy(e->ev_coef_free);
+    if (e->ev_search_done) cudaEventDestroy(e->ev_search_done);
     delete e;
 }
 
@@ -1025,10 +1086,10 @@ riv_status riv_debug_frame_state(riv_encoder* e, int what, void* out, size_t siz
     if (!e || !out) return RIV_ERR_FRAME;
     const DevBuf* b = nullptr;
     switch (what) {
-        case 0: b = &e->mbout; break;
+        case 0: b = &e->mboutb[e->last_par]; break;
         case 1: b = &e->qs; break;
         case 2: b = &e->pred; break;
-        case 3: b = &e->cur; break;
+        case 3: b = &e->curb[e->last_par]; break;
         case 4: b = &e->coeffs; break;
         case 5: b = &e->opt_skip; break;
         case 6: b = &e->prof; break;
@@ -1037,7 +1098,9 @@ riv_status riv_debug_frame_state(riv_encoder* e, int what, void* out, size_t siz
     if (size < b->n) return RIV_ERR_FRAME;
     try {
         CK(cudaSetDevice(e->cfg.device));
+        CK(cudaStreamSynchronize(e->Y));
         CK(cudaStreamSynchronize(e->S));
+        CK(cudaStreamSynchronize(e->K));
         CK(cudaMemcpy(out, b->p, b->n, cudaMemcpyDeviceToHost));
     } catch (const CudaError& ce) {
         return fail(e, RIV_ERR_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
@@ -1119,14 +1182,15 @@ riv_status riv_stage_deblock(uint8_t* yuv, uint32_t w, uint32_t h, int level, in
     int E, I, Hv;
     deblock_thresholds(level, intra != 0, E, I, Hv);
     size_t n = (size_t)w * h * 3 / 2, nm = (size_t)(w / 16) * (h / 16);
-    void *d = nullptr, *dm = nullptr;
+    void *d = nullptr, *d2 = nullptr, *dm = nullptr;
     riv_status st = RIV_OK;
-    if (cudaMalloc(&d, n) || cudaMemcpy(d, yuv, n, cudaMemcpyHostToDevice)) st = RIV_ERR_CUDA;
+    if (cudaMalloc(&d, n) || cudaMalloc(&d2, n) || cudaMemcpy(d, yuv, n, cudaMemcpyHostToDevice)) st = RIV_ERR_CUDA;
     if (!st && mask && (cudaMalloc(&dm, nm) || cudaMemcpy(dm, mask, nm, cudaMemcpyHostToDevice))) st = RIV_ERR_CUDA;
-    if (!st && (launch_deblock((uint8_t*)d, (int)w, (int)h, E, I, Hv, (const uint8_t*)dm, 0) ||
-                cudaMemcpy(yuv, d, n, cudaMemcpyDeviceToHost)))
+    if (!st && (launch_deblock_tiled((const uint8_t*)d, (uint8_t*)d2, (int)w, (int)h, E, I, Hv, (const uint8_t*)dm, 0) ||
+                cudaMemcpy(yuv, d2, n, cudaMemcpyDeviceToHost)))
         st = RIV_ERR_CUDA;
     cudaFree(d);
+    cudaFree(d2);
     cudaFree(dm);
     return st;
 }

@@ -51,6 +51,7 @@ struct SearchParams {
     MbRec* rec;       // 2 x BW*BH wavefront records: raw MVs (search), then coded MVs (mode)
     unsigned tag;
     MbOut* out;
+    int8_t* coded_out;  // coded MV (dx, dy, sx, sy) per MB: the next frame's temporal predictors
     unsigned* status;
     long long spin_limit;
     long long* prof;  // optional: 16 words per MB (phase clock stamps, hexagon rounds), nullptr = off
@@ -100,6 +101,9 @@ int launch_aq(const uint2* varsum, int n, float base, const uint32_t* logfix, in
               int nexp, float* lnv_scratch, float* qs, void* stream);
 int launch_residual(const ResidualParams& p, int nmb, void* stream);
 int launch_deblock(uint8_t* yuv, int W, int H, int E, int I, int Hev, const uint8_t* mask, void* stream);
+// Out-of-place deblock of all three planes in one launch (src != dst, no overlap).
+int launch_deblock_tiled(const uint8_t* src, uint8_t* dst, int W, int H, int E, int I, int Hev, const uint8_t* mask,
+                         void* stream);
 // Scratch of the no-allocation deblock entry point (a file-scope __device__ array of
 // DEBLOCK_NOALLOC_MAX_BYTES bytes); the address is valid on the current device.
 constexpr size_t DEBLOCK_NOALLOC_MAX_BYTES = (size_t)4 << 20;

@@ -523,6 +523,8 @@ __device__ __forceinline__ void mode_warp(const SearchParams& p, const unsigned 
                 o.pad[0] = o.pad[1] = 0;
                 o.best_sad = (int32_t)best_sad;
                 p.out[idx] = o;
+                *(char4*)(p.coded_out + 4 * (size_t)idx) =
+                    make_char4((signed char)coded.dx, (signed char)coded.dy, (signed char)coded.sx, (signed char)coded.sy);
             }
             RIV_STAMP(6);
             L_cod = coded;
@@ -1696,38 +1698,39 @@ __global__ void __launch_bounds__(256) k_residual(ResidualParams p) {
         if (t < 128) resc[t] = pl == 0 ? (int)cU[cidx] - (int)pU[cidx] : (int)cV[cidx] - (int)pV[cidx];
     }
     __syncthreads();
+    // The reference accumulates both FDCT passes in i64 and clamps to i32.  With residuals in
+    // [-255, 255] and these bases, every partial sum stays below 2^31 (16x16: row pass
+    // <= 255 * 1048576 = 2.7e8, rows <= 1020, column pass <= 1020 * 1048576 + 2^17 = 1.07e9;
+    // 8x8: 1.9e8, 721, 5.3e8), so exact int32 accumulation gives the same values and the
+    // clamp never applies.
     // row pass: rowt[y][j] = sum_i res[y][i] * T[i][j]
     {
-        long long acc = 0;
+        int32_t acc = 0;
 #pragma unroll
-        for (int i = 0; i < 16; i++) acc += (long long)res[yy * 16 + i] * (long long)sT16[i * 16 + xx];
-        long long v = (acc + (1LL << 17)) >> 18;
-        rowt[t] = (int32_t)min(max(v, (long long)INT_MIN), (long long)INT_MAX);
+        for (int i = 0; i < 16; i++) acc += res[yy * 16 + i] * sT16[i * 16 + xx];
+        rowt[t] = (acc + (1 << 17)) >> 18;
     }
     if (t < 128) {
-        long long acc = 0;
+        int32_t acc = 0;
 #pragma unroll
-        for (int i = 0; i < 8; i++) acc += (long long)resc[pl * 64 + cyy * 8 + i] * (long long)sT8[i * 8 + cxx];
-        long long v = (acc + (1LL << 17)) >> 18;
-        rowc[t] = (int32_t)min(max(v, (long long)INT_MIN), (long long)INT_MAX);
+        for (int i = 0; i < 8; i++) acc += resc[pl * 64 + cyy * 8 + i] * sT8[i * 8 + cxx];
+        rowc[t] = (acc + (1 << 17)) >> 18;
     }
     __syncthreads();
     // column pass: coef[v][u] = sum_i rowt[i][u] * T[i][v]   (v = yy, u = xx)
     int32_t coef;
     {
-        long long acc = 0;
+        int32_t acc = 0;
 #pragma unroll
-        for (int i = 0; i < 16; i++) acc += (long long)rowt[i * 16 + xx] * (long long)sT16[i * 16 + yy];
-        long long v = (acc + (1LL << 17)) >> 18;
-        coef = (int32_t)min(max(v, (long long)INT_MIN), (long long)INT_MAX);
+        for (int i = 0; i < 16; i++) acc += rowt[i * 16 + xx] * sT16[i * 16 + yy];
+        coef = (acc + (1 << 17)) >> 18;
     }
     int32_t coefc = 0;
     if (t < 128) {
-        long long acc = 0;
+        int32_t acc = 0;
 #pragma unroll
-        for (int i = 0; i < 8; i++) acc += (long long)rowc[pl * 64 + i * 8 + cxx] * (long long)sT8[i * 8 + cyy];
-        long long v = (acc + (1LL << 17)) >> 18;
-        coefc = (int32_t)min(max(v, (long long)INT_MIN), (long long)INT_MAX);
+        for (int i = 0; i < 8; i++) acc += rowc[pl * 64 + i * 8 + cxx] * sT8[i * 8 + cyy];
+        coefc = (acc + (1 << 17)) >> 18;
     }
     // quantisation
     float qsv = 0.0f;
@@ -1887,6 +1890,86 @@ __device__ __forceinline__ void filter_line(int* px, int E, int I, int Hv) {
         px[6] = min(max(nq2 + 128, 0), 255);
     }
 }
+// Out of place, all planes in one launch (src and dst must not overlap: neighbouring tiles
+// read each other's pixels as halo).  A CTA owns one band of an edge grid (16 luma / 8
+// chroma rows) and DB_TW luma (DB_TW/2 chroma) columns.  It loads the tile with a 4-pixel
+// halo, filters every vertical edge of the halo rows in shared memory (rows are independent
+// in that pass), then the horizontal edges at the band's top and bottom (their lines are 4+
+// pixels apart, so they touch disjoint pixels), and stores only its own pixels.  That equals
+// the reference's whole-plane vertical pass followed by the whole-plane horizontal pass.
+constexpr int DB_TW = 128;
+__global__ void __launch_bounds__(128) k_deblock_tiled(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, int W,
+                                                       int H, int BW, int E, int I, int Hv, const uint8_t* mask,
+                                                       int ntiles_y) {
+    __shared__ uint8_t tile[(16 + 8) * (DB_TW + 8)];
+    int t = blockIdx.x;
+    int plane = t < ntiles_y ? 0 : (t - ntiles_y) % 2 + 1;
+    if (plane > 0) t = (t - ntiles_y) / 2;
+    const int w = plane ? W / 2 : W, h = plane ? H / 2 : H, g = plane ? 8 : 16, tw = plane ? DB_TW / 2 : DB_TW;
+    const size_t poff = plane == 0 ? 0 : (size_t)W * H + (plane == 2 ? (size_t)(W / 2) * (H / 2) : 0);
+    const uint8_t* pl = src + poff;
+    uint8_t* po = dst + poff;
+    const int tpb = (w + tw - 1) / tw;
+    const int band = t / tpb, X0 = (t % tpb) * tw, X1 = min(X0 + tw, w);
+    const int Y0 = band * g, Y1 = Y0 + g;
+    const int ry0 = max(Y0 - 4, 0), ry1 = min(Y1 + 4, h), cx0 = max(X0 - 4, 0), cx1 = min(X1 + 4, w);
+    const int TS = DB_TW + 8, oy = Y0 - 4, ox = X0 - 4;  // tile row stride and origin
+    const int nrow = ry1 - ry0, ncol = cx1 - cx0;
+    for (int i = threadIdx.x; i < nrow * ncol; i += blockDim.x) {
+        const int r = i / ncol, c = i - r * ncol;
+        tile[(ry0 + r - oy) * TS + cx0 + c - ox] = pl[(size_t)(ry0 + r) * w + cx0 + c];
+    }
+    __syncthreads();
+    // vertical edges x = k*g (1 <= k < w/g) with X0 <= x <= X1, on every loaded row
+    const int k0 = max(1, (X0 + g - 1) / g), k1 = min(w / g - 1, X1 / g);
+    const int nk = k1 - k0 + 1;
+    if (nk > 0) {
+        for (int i = threadIdx.x; i < nrow * nk; i += blockDim.x) {
+            const int r = i / nk, k = k0 + (i - r * nk), y = ry0 + r;
+            const int by = y / g;
+            if (mask && !(mask[by * BW + k - 1] | mask[by * BW + k])) continue;
+            uint8_t* sp = tile + (y - oy) * TS + k * g - 4 - ox;
+            int px[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) px[q] = sp[q];
+            filter_line(px, E, I, Hv);
+#pragma unroll
+            for (int q = 1; q < 7; q++) sp[q] = (uint8_t)px[q];
+        }
+    }
+    __syncthreads();
+    // horizontal edges at the band's top (Y0) and bottom (Y1), columns X0 .. X1-1
+    for (int i = threadIdx.x; i < 2 * (X1 - X0); i += blockDim.x) {
+        const int e = (i < X1 - X0 ? Y0 : Y1) / g, x = X0 + (i < X1 - X0 ? i : i - (X1 - X0));
+        if (e < 1 || e >= h / g) continue;
+        const int bxm = x / g;
+        if (mask && !(mask[(e - 1) * BW + bxm] | mask[e * BW + bxm])) continue;
+        uint8_t* sp = tile + (e * g - 4 - oy) * TS + x - ox;
+        int px[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) px[q] = sp[q * TS];
+        filter_line(px, E, I, Hv);
+#pragma unroll
+        for (int q = 1; q < 7; q++) sp[q * TS] = (uint8_t)px[q];
+    }
+    __syncthreads();
+    const int ow = X1 - X0;
+    for (int i = threadIdx.x; i < g * ow; i += blockDim.x) {
+        const int r = i / ow, c = i - r * ow;
+        po[(size_t)(Y0 + r) * w + X0 + c] = tile[(Y0 + r - oy) * TS + X0 + c - ox];
+    }
+}
+
+int launch_deblock_tiled(const uint8_t* src, uint8_t* dst, int W, int H, int E, int I, int Hv, const uint8_t* mask,
+                         void* stream) {
+    const int BW = W / 16;
+    const int ty = (H / 16) * ((W + DB_TW - 1) / DB_TW);
+    const int tc = ((H / 2) / 8) * ((W / 2 + DB_TW / 2 - 1) / (DB_TW / 2));
+    k_deblock_tiled<<<ty + 2 * tc, 128, 0, (cudaStream_t)stream>>>(src, dst, W, H, BW, E, I, Hv, mask, ty);
+    return (int)cudaGetLastError();
+}
+
+// In place, two passes over each plane (vertical edges, then horizontal edges).
 // Vertical edges of one plane: thread per (row y, edge e >= 1).
 __global__ void k_deblock_v(uint8_t* pl, int w, int h, int grid, int BW, int E, int I, int Hv, const uint8_t* mask) {
     int y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -1957,51 +2040,69 @@ int deblock_scratch_address(void** out) { return (int)cudaGetSymbolAddress(out, 
 // coefficient (the entropy coder never reads beyond it): Y[0..eY], U[0..eU], V[0..eV].
 // hdr[0] = coded MB count, hdr[1] = total coefficients written.
 // ---------------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_scan(const uint8_t* opt_skip, const uint8_t* eobs, int nmb, int intra,
-                                               int32_t* index, int32_t* offset, uint32_t* hdr) {
-    __shared__ int wsum[32], wsz[32];
-    __shared__ int carry, carry_sz;
-    if (threadIdx.x == 0) { carry = 0; carry_sz = 0; }
-    __syncthreads();
+// Scan: each of SC_THREADS threads owns SC_IPT consecutive MBs of a SC_THREADS * SC_IPT
+// chunk (all their loads are issued together), then one block-wide scan of the thread totals
+// per chunk.  Small enough (256 threads, few registers) to run beside the search kernel.
+constexpr int SC_THREADS = 256, SC_IPT = 32;
+__global__ void __launch_bounds__(SC_THREADS) k_scan(const uint8_t* opt_skip, const uint8_t* eobs, int nmb, int intra,
+                                                     int32_t* index, int32_t* offset, uint32_t* hdr) {
+    __shared__ int wsum[SC_THREADS / 32], wsz[SC_THREADS / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int base = 0; base < nmb; base += 1024) {
-        int i = base + threadIdx.x;
-        int f = (i < nmb && (intra || !opt_skip[i])) ? 1 : 0;
-        int z = f ? (int)eobs[3 * i] + (int)eobs[3 * i + 1] + (int)eobs[3 * i + 2] + 3 : 0;
-        int x = f, y = z;
+    int carry = 0, carry_sz = 0;  // identical in every thread
+    for (int base = 0; base < nmb; base += SC_THREADS * SC_IPT) {
+        const int i0 = base + threadIdx.x * SC_IPT;
+        // v = coded << 16 | coefficient count (<= 3 * 256): 32 of them sum without carry
+        uint32_t v[SC_IPT];
+#pragma unroll
+        for (int k = 0; k < SC_IPT; k++) {
+            const int i = i0 + k;
+            const bool f = i < nmb && (intra || !opt_skip[i]);
+            v[k] = f ? (1u << 16) | (uint32_t)(eobs[3 * i] + eobs[3 * i + 1] + eobs[3 * i + 2] + 3) : 0u;
+        }
+        uint32_t tot = 0;
+#pragma unroll
+        for (int k = 0; k < SC_IPT; k++) tot += v[k];
+        const int x = (int)(tot >> 16), y = (int)(tot & 0xffffu);
+        int xs = x, ys = y;  // inclusive warp scan of the thread totals
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            int a = __shfl_up_sync(0xffffffffu, x, o), b = __shfl_up_sync(0xffffffffu, y, o);
-            if (lane >= o) { x += a; y += b; }
+            const int a2 = __shfl_up_sync(0xffffffffu, xs, o), b2 = __shfl_up_sync(0xffffffffu, ys, o);
+            if (lane >= o) { xs += a2; ys += b2; }
         }
-        if (lane == 31) { wsum[wid] = x; wsz[wid] = y; }
+        if (lane == 31) { wsum[wid] = xs; wsz[wid] = ys; }
         __syncthreads();
-        if (wid == 0) {
-            int s1 = wsum[lane], s2 = wsz[lane];
+        int wx = 0, wy = 0, tx = 0, ty = 0;  // exclusive prefix of this warp, chunk totals
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                int a = __shfl_up_sync(0xffffffffu, s1, o), b = __shfl_up_sync(0xffffffffu, s2, o);
-                if (lane >= o) { s1 += a; s2 += b; }
-            }
-            wsum[lane] = s1;
-            wsz[lane] = s2;
+        for (int q = 0; q < SC_THREADS / 32; q++) {
+            if (q < wid) { wx += wsum[q]; wy += wsz[q]; }
+            tx += wsum[q];
+            ty += wsz[q];
         }
-        __syncthreads();
-        int ex = carry + (wid > 0 ? wsum[wid - 1] : 0) + x - f;
-        int ez = carry_sz + (wid > 0 ? wsz[wid - 1] : 0) + y - z;
-        if (i < nmb) { index[i] = f ? ex : -1; offset[i] = ez; }
-        __syncthreads();
-        if (threadIdx.x == 0) { carry += wsum[31]; carry_sz += wsz[31]; }
-        __syncthreads();
+        int ex = carry + wx + xs - x;
+        int ez = carry_sz + wy + ys - y;
+#pragma unroll
+        for (int k = 0; k < SC_IPT; k++) {
+            const int i = i0 + k;
+            const int f = (int)(v[k] >> 16), z = (int)(v[k] & 0xffffu);
+            if (i < nmb) { index[i] = f ? ex : -1; offset[i] = ez; }
+            ex += f;
+            ez += z;
+        }
+        carry += tx;
+        carry_sz += ty;
+        __syncthreads();  // wsum / wsz are rewritten by the next chunk
     }
     if (threadIdx.x == 0) { hdr[0] = (uint32_t)carry; hdr[1] = (uint32_t)carry_sz; }
 }
-__global__ void __launch_bounds__(128) k_pack(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coeffs,
+// Pack: one warp per MB.
+__global__ void __launch_bounds__(256) k_pack(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coeffs,
                                               const uint8_t* eobs, const int32_t* index, const int32_t* offset,
-                                              int intra, uint32_t* side, int16_t* packed, uint8_t* peobs) {
-    const int m = blockIdx.x;
+                                              int intra, int nmb, uint32_t* side, int16_t* packed, uint8_t* peobs) {
+    const int m = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (m >= nmb) return;
     const int k = index[m];
-    if (threadIdx.x == 0) {
+    const int e0 = eobs[3 * m], e1 = eobs[3 * m + 1], e2 = eobs[3 * m + 2];
+    if (lane == 0) {
         uint32_t s = 0;
         if (!intra) {
             const MbOut o = mb[m];
@@ -2011,17 +2112,17 @@ __global__ void __launch_bounds__(128) k_pack(const uint8_t* opt_skip, const MbO
         }
         side[m] = s;
         if (k >= 0) {
-            peobs[3 * k] = eobs[3 * m];
-            peobs[3 * k + 1] = eobs[3 * m + 1];
-            peobs[3 * k + 2] = eobs[3 * m + 2];
+            peobs[3 * k] = (uint8_t)e0;
+            peobs[3 * k + 1] = (uint8_t)e1;
+            peobs[3 * k + 2] = (uint8_t)e2;
         }
     }
     if (k < 0) return;
-    const int n0 = eobs[3 * m] + 1, n1 = eobs[3 * m + 1] + 1, n2 = eobs[3 * m + 2] + 1;
+    const int n0 = e0 + 1, n1 = e1 + 1, n2 = e2 + 1;
     const int16_t* src = coeffs + (size_t)m * 384;
     int16_t* dst = packed + offset[m];
-    for (int i = threadIdx.x; i < n0 + n1 + n2; i += blockDim.x) {
-        int si = i < n0 ? i : (i < n0 + n1 ? 256 + (i - n0) : 320 + (i - n0 - n1));
+    for (int i = lane; i < n0 + n1 + n2; i += 32) {
+        const int si = i < n0 ? i : (i < n0 + n1 ? 256 + (i - n0) : 320 + (i - n0 - n1));
         dst[i] = src[si];
     }
 }
@@ -2030,8 +2131,8 @@ int launch_compact(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coef
                    int intra, int32_t* index, int32_t* offset, uint32_t* dside, int16_t* dpacked, uint8_t* dpeobs,
                    uint32_t* hhdr, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
-    k_scan<<<1, 1024, 0, st>>>(opt_skip, eobs, nmb, intra, index, offset, hhdr);
-    k_pack<<<nmb, 128, 0, st>>>(opt_skip, mb, coeffs, eobs, index, offset, intra, dside, dpacked, dpeobs);
+    k_scan<<<1, SC_THREADS, 0, st>>>(opt_skip, eobs, nmb, intra, index, offset, hhdr);
+    k_pack<<<(nmb + 7) / 8, 256, 0, st>>>(opt_skip, mb, coeffs, eobs, index, offset, intra, nmb, dside, dpacked, dpeobs);
     return (int)cudaGetLastError();
 }
 

@@ -306,3 +306,18 @@ def test_entropy_coders_match_oracle_on_host():
     from riv2_b200.encoder import libm_fixup_counts
     nlog, nexp = libm_fixup_counts()
     assert 1000 < nlog < 200000 and 1000 < nexp < 500000
+
+
+def test_fdct_int32_accumulation_is_exact_for_reference_bases():
+    """The device forward DCTs accumulate in int32 where the reference uses i64 and clamps to
+    i32; that is exact only while every partial sum of both passes stays below 2^31 for
+    residuals in [-255, 255].  Checked from the reference's own bases."""
+    import numpy as np
+    d = json.load(open(os.path.join(ROOT, "tests", "golden", "reference_constants.json")))
+    for name, n in (("fdct16", 16), ("fdct8", 8)):
+        T = np.array(d[name], dtype=np.int64).reshape(n, n)
+        col = np.abs(T).sum(axis=0).max()          # largest sum over i of |T[i][j]|
+        row_pass = 255 * col + (1 << 17)
+        rows = row_pass >> 18
+        col_pass = rows * col + (1 << 17)
+        assert row_pass < 2 ** 31 and col_pass < 2 ** 31, (name, row_pass, col_pass)
