@@ -242,9 +242,9 @@ def cpu_baseline(frames_host, nframes, iq, pq):
 
 
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_search launch at this workload
-# (ncu --set full, caches flushed before the pass): 14,647,296 + 6,656 bytes.  The excess
-# over the algorithmic bytes is the exhaustive SAD table read back from memory.
-SEARCH_TRAFFIC_BYTES = 14_647_296 + 6_656
+# (ncu --set full, caches flushed before the pass): 4,689,408 + 12,288 bytes.  The SAD table
+# is produced and consumed inside the same launch and stays in L2.
+SEARCH_TRAFFIC_BYTES = 4_689_408 + 12_288
 
 
 def roofline_entry(stage_us_per_frame: float):
