@@ -1653,170 +1653,236 @@ __device__ __forceinline__ void aan_1d(const int32_t s[8], int32_t out[8], int32
     out[3] = wadd(x3, u0) >> shift; out[4] = wsub(x3, u0) >> shift;
 }
 
-__global__ void __launch_bounds__(256) k_residual(ResidualParams p) {
-    __shared__ int32_t sT16[256], sT8[64];
-    __shared__ int32_t res[256], rowt[256];
-    __shared__ int32_t resc[128], rowc[128];
-    __shared__ int16_t q[384];
-    __shared__ int32_t aant[2][64];
-    const int t = threadIdx.x;
-    const int mb = blockIdx.x;
+// Four MBs per CTA, 64 threads (two warps) per MB.  Thread u of an MB owns luma row u >> 2,
+// columns 4 * (u & 3) .. +3 in every 16x16 pass, and two adjacent chroma samples (plane
+// u >> 5).  Each pass reads one basis row and one data row per term as 128-bit shared loads,
+// four multiply-accumulates per pair of loads.  Per-MB named barriers (ids 1..4, 64 threads).
+constexpr int RS_MB = 4;
+__device__ __forceinline__ void mb_sync(int g) { asm volatile("bar.sync %0, 64;" ::"r"(g + 1) : "memory"); }
+
+__global__ void __launch_bounds__(256) k_residual(ResidualParams p, int nmb) {
+    __shared__ __align__(16) int32_t sT16[256], sT16t[256], sT8[64];
+    __shared__ __align__(16) int32_t res[RS_MB][256], rowt[RS_MB][256];
+    __shared__ __align__(16) int32_t resc[RS_MB][128], rowc[RS_MB][128];
+    __shared__ __align__(16) int16_t q[RS_MB][384];
+    __shared__ int32_t aant[RS_MB][2][64];
+    __shared__ int flags[RS_MB][4];  // nonzero, luma eob of warp 0 / warp 1
+    const int tid = threadIdx.x;
+    for (int i = tid; i < 256; i += 256) {
+        sT16[i] = c_T16[i];
+        sT16t[(i & 15) * 16 + (i >> 4)] = c_T16[i];  // sT16t[i][x] = T[x][i]
+    }
+    if (tid < 64) sT8[tid] = c_T8[tid];
+    __syncthreads();
+    const int g = tid >> 6, u = tid & 63;
+    const int mb = blockIdx.x * RS_MB + g;
+    if (mb >= nmb) return;
     const int BW = p.BW, W = p.W, H = p.H, CW = W / 2, CH = H / 2;
     const int bx = mb % BW, by = mb / BW;
     const int x0 = bx * 16, y0 = by * 16;
     const uint8_t *cY = p.cur, *cU = p.cur + (size_t)W * H, *cV = cU + (size_t)CW * CH;
     const uint8_t *pY = p.pred, *pU = p.pred + (size_t)W * H, *pV = pU + (size_t)CW * CH;
     uint8_t *rY = p.recon, *rU = p.recon + (size_t)W * H, *rV = rU + (size_t)CW * CH;
-    const int yy = t >> 4, xx = t & 15;
-    const size_t yi = (size_t)(y0 + yy) * W + x0 + xx;
-    // chroma mapping for t < 128: plane pl, index i (row ci>>3, col ci&7)
-    const int pl = t >> 6, ci = t & 63, cyy = ci >> 3, cxx = ci & 7;
+    const int yy = u >> 2, xb = (u & 3) * 4;
+    const size_t yi = (size_t)(y0 + yy) * W + x0 + xb;
+    const int pl = u >> 5, ci = (u & 31) * 2, cyy = ci >> 3, cxx = ci & 7;
     const size_t cidx = (size_t)(y0 / 2 + cyy) * CW + x0 / 2 + cxx;
+    const uint8_t* cC = pl == 0 ? cU : cV;
+    const uint8_t* pC = pl == 0 ? pU : pV;
+    uint8_t* rC = pl == 0 ? rU : rV;
+    int32_t* R = res[g];
+    int32_t* RT = rowt[g];
+    int32_t* RC = resc[g];
+    int32_t* RCT = rowc[g];
+    int16_t* Q = q[g];
 
-    bool rdo_skip = !p.intra && p.mb[mb].rdo_skip;
-    if (rdo_skip) {  // never transformed: residual 0, recon = prediction
-        rY[yi] = pY[yi];
-        if (t < 128) {
-            if (pl == 0) rU[cidx] = pU[cidx]; else rV[cidx] = pV[cidx];
-        }
-        for (int i = t; i < 384; i += 256) p.coeffs[(size_t)mb * 384 + i] = 0;
-        if (t == 0) {
+    auto copy_pred = [&]() {  // recon = prediction, coefficients zero
+        *(uint32_t*)(rY + yi) = *(const uint32_t*)(pY + yi);
+        *(uint16_t*)(rC + cidx) = *(const uint16_t*)(pC + cidx);
+        int16_t* co = p.coeffs + (size_t)mb * 384;
+        *(uint2*)(co + yy * 16 + xb) = make_uint2(0u, 0u);
+        *(uint32_t*)(co + 256 + pl * 64 + ci) = 0u;
+        if (u == 0) {
             p.opt_skip[mb] = 1;
             const int8_t* c = p.mb[mb].coded;
             p.fmask[mb] = (c[0] | c[1] | c[2] | c[3]) != 0;
             p.eobs[3 * mb] = p.eobs[3 * mb + 1] = p.eobs[3 * mb + 2] = 0;
         }
+    };
+    if (!p.intra && p.mb[mb].rdo_skip) {  // never transformed: residual 0, recon = prediction
+        copy_pred();
         return;
     }
-    sT16[t] = c_T16[t];
-    if (t < 64) sT8[t] = c_T8[t];
-    if (p.intra) {
-        res[t] = (int)cY[yi] - 128;
-        if (t < 128) resc[t] = (int)(pl == 0 ? cU[cidx] : cV[cidx]) - 128;
-    } else {
-        res[t] = (int)cY[yi] - (int)pY[yi];
-        if (t < 128) resc[t] = pl == 0 ? (int)cU[cidx] - (int)pU[cidx] : (int)cV[cidx] - (int)pV[cidx];
+    {
+        const uint32_t cv = *(const uint32_t*)(cY + yi);
+        const uint32_t pv = p.intra ? 0x80808080u : *(const uint32_t*)(pY + yi);
+#pragma unroll
+        for (int k = 0; k < 4; k++) R[yy * 16 + xb + k] = (int)((cv >> (8 * k)) & 255u) - (int)((pv >> (8 * k)) & 255u);
+        const uint32_t cc = *(const uint16_t*)(cC + cidx);
+        const uint32_t pc = p.intra ? 0x8080u : *(const uint16_t*)(pC + cidx);
+        RC[pl * 64 + ci] = (int)(cc & 255u) - (int)(pc & 255u);
+        RC[pl * 64 + ci + 1] = (int)(cc >> 8) - (int)(pc >> 8);
     }
-    __syncthreads();
+    mb_sync(g);
     // The reference accumulates both FDCT passes in i64 and clamps to i32.  With residuals in
     // [-255, 255] and these bases, every partial sum stays below 2^31 (16x16: row pass
     // <= 255 * 1048576 = 2.7e8, rows <= 1020, column pass <= 1020 * 1048576 + 2^17 = 1.07e9;
     // 8x8: 1.9e8, 721, 5.3e8), so exact int32 accumulation gives the same values and the
     // clamp never applies.
-    // row pass: rowt[y][j] = sum_i res[y][i] * T[i][j]
-    {
-        int32_t acc = 0;
+    {  // row pass: rowt[y][j] = sum_i res[y][i] * T[i][j]
+        int32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
 #pragma unroll
-        for (int i = 0; i < 16; i++) acc += res[yy * 16 + i] * sT16[i * 16 + xx];
-        rowt[t] = (acc + (1 << 17)) >> 18;
+        for (int i = 0; i < 16; i++) {
+            const int r = R[yy * 16 + i];
+            const int4 t = *(const int4*)(sT16 + i * 16 + xb);
+            a0 += r * t.x; a1 += r * t.y; a2 += r * t.z; a3 += r * t.w;
+        }
+        *(int4*)(RT + yy * 16 + xb) = make_int4((a0 + (1 << 17)) >> 18, (a1 + (1 << 17)) >> 18,
+                                                (a2 + (1 << 17)) >> 18, (a3 + (1 << 17)) >> 18);
+        int32_t c0 = 0, c1 = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int r = RC[pl * 64 + cyy * 8 + i];
+            const int2 t = *(const int2*)(sT8 + i * 8 + cxx);
+            c0 += r * t.x; c1 += r * t.y;
+        }
+        *(int2*)(RCT + pl * 64 + ci) = make_int2((c0 + (1 << 17)) >> 18, (c1 + (1 << 17)) >> 18);
     }
-    if (t < 128) {
-        int32_t acc = 0;
+    mb_sync(g);
+    int32_t coef[4], coefc[2];
+    {  // column pass: coef[v][x] = sum_i rowt[i][x] * T[i][v]   (v = yy)
+        int32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
 #pragma unroll
-        for (int i = 0; i < 8; i++) acc += resc[pl * 64 + cyy * 8 + i] * sT8[i * 8 + cxx];
-        rowc[t] = (acc + (1 << 17)) >> 18;
-    }
-    __syncthreads();
-    // column pass: coef[v][u] = sum_i rowt[i][u] * T[i][v]   (v = yy, u = xx)
-    int32_t coef;
-    {
-        int32_t acc = 0;
+        for (int i = 0; i < 16; i++) {
+            const int4 r = *(const int4*)(RT + i * 16 + xb);
+            const int t = sT16[i * 16 + yy];
+            a0 += r.x * t; a1 += r.y * t; a2 += r.z * t; a3 += r.w * t;
+        }
+        coef[0] = (a0 + (1 << 17)) >> 18; coef[1] = (a1 + (1 << 17)) >> 18;
+        coef[2] = (a2 + (1 << 17)) >> 18; coef[3] = (a3 + (1 << 17)) >> 18;
+        int32_t c0 = 0, c1 = 0;
 #pragma unroll
-        for (int i = 0; i < 16; i++) acc += rowt[i * 16 + xx] * sT16[i * 16 + yy];
-        coef = (acc + (1 << 17)) >> 18;
-    }
-    int32_t coefc = 0;
-    if (t < 128) {
-        int32_t acc = 0;
-#pragma unroll
-        for (int i = 0; i < 8; i++) acc += rowc[pl * 64 + i * 8 + cxx] * sT8[i * 8 + cyy];
-        coefc = (acc + (1 << 17)) >> 18;
+        for (int i = 0; i < 8; i++) {
+            const int2 r = *(const int2*)(RCT + pl * 64 + i * 8 + cxx);
+            const int t = sT8[i * 8 + cyy];
+            c0 += r.x * t; c1 += r.y * t;
+        }
+        coefc[0] = (c0 + (1 << 17)) >> 18; coefc[1] = (c1 + (1 << 17)) >> 18;
     }
     // quantisation
     float qsv = 0.0f;
+    int16_t ql[4], qc[2];
     if (p.intra) {
-        float qy = (float)max((int)p.intra_ytab[t], 1);
-        q[t] = f32_to_i16_sat(roundf(__fdiv_rn(__int2float_rn(coef), qy)));
-        if (t < 128) {
-            float qc = (float)max((int)p.intra_ctab[ci], 1);
-            q[256 + t] = f32_to_i16_sat(roundf(__fdiv_rn(__int2float_rn(coefc), qc)));
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const float qy = (float)max((int)p.intra_ytab[yy * 16 + xb + k], 1);
+            ql[k] = f32_to_i16_sat(roundf(__fdiv_rn(__int2float_rn(coef[k]), qy)));
+        }
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const float qq = (float)max((int)p.intra_ctab[ci + k], 1);
+            qc[k] = f32_to_i16_sat(roundf(__fdiv_rn(__int2float_rn(coefc[k]), qq)));
         }
     } else {
         qsv = p.qs[mb];
-        float r = __fdiv_rn(__int2float_rn(coef), qsv);
-        q[t] = fabsf(r) < p.dead_zone ? (int16_t)0 : f32_to_i16_sat(roundf(r));
-        if (t < 128) {
-            float rc = __fdiv_rn(__int2float_rn(coefc), qsv);
-            q[256 + t] = fabsf(rc) < p.dead_zone ? (int16_t)0 : f32_to_i16_sat(roundf(rc));
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const float r = __fdiv_rn(__int2float_rn(coef[k]), qsv);
+            ql[k] = fabsf(r) < p.dead_zone ? (int16_t)0 : f32_to_i16_sat(roundf(r));
+        }
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const float r = __fdiv_rn(__int2float_rn(coefc[k]), qsv);
+            qc[k] = fabsf(r) < p.dead_zone ? (int16_t)0 : f32_to_i16_sat(roundf(r));
         }
     }
-    __syncthreads();
-    int nz = (q[t] != 0) || (t < 128 && q[256 + t] != 0);
-    nz = __syncthreads_or(nz);
+    // last non-zero index per plane block (0 when all zero) and "any non-zero"
+    int lz = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) lz = ql[k] != 0 ? yy * 16 + xb + k : lz;
+    int lc = 0;
+#pragma unroll
+    for (int k = 0; k < 2; k++) lc = qc[k] != 0 ? ci + k : lc;
+    const bool any = (ql[0] | ql[1] | ql[2] | ql[3] | qc[0] | qc[1]) != 0;
+    lz = __reduce_max_sync(0xffffffffu, lz);
+    lc = __reduce_max_sync(0xffffffffu, lc);
+    const unsigned anyw = __any_sync(0xffffffffu, any);
+    if ((u & 31) == 0) {
+        flags[g][u >> 5] = lz;
+        flags[g][2 + (u >> 5)] = (int)anyw | (lc << 1);
+    }
+    mb_sync(g);
+    const bool nz = ((flags[g][2] | flags[g][3]) & 1) != 0;
     if (!p.intra && !nz) {  // became all-zero after quantisation: optimized skip
-        rY[yi] = pY[yi];
-        if (t < 128) {
-            if (pl == 0) rU[cidx] = pU[cidx]; else rV[cidx] = pV[cidx];
-        }
-        for (int i = t; i < 384; i += 256) p.coeffs[(size_t)mb * 384 + i] = 0;
-        if (t == 0) {
-            p.opt_skip[mb] = 1;
-            const int8_t* c = p.mb[mb].coded;
-            p.fmask[mb] = (c[0] | c[1] | c[2] | c[3]) != 0;
-            p.eobs[3 * mb] = p.eobs[3 * mb + 1] = p.eobs[3 * mb + 2] = 0;
-        }
+        copy_pred();
         return;
     }
-    for (int i = t; i < 384; i += 256) p.coeffs[(size_t)mb * 384 + i] = q[i];
-    // last non-zero index per plane block (0 when all zero), for the host entropy coder
     {
-        int lz = q[t] != 0 ? t : 0;
-        lz = __reduce_max_sync(0xffffffffu, lz);
-        __shared__ int wl[8];
-        if ((t & 31) == 0) wl[t >> 5] = lz;
-        int lc = 0;
-        if (t < 128) lc = q[256 + t] != 0 ? ci : 0;
-        lc = __reduce_max_sync(0xffffffffu, lc);
-        __shared__ int wc[4];
-        if ((t & 31) == 0 && t < 128) wc[t >> 5] = lc;
-        __syncthreads();
-        if (t == 0) {
-            int a = 0;
-            for (int i = 0; i < 8; i++) a = max(a, wl[i]);
-            p.eobs[3 * mb] = (uint8_t)a;
-            p.eobs[3 * mb + 1] = (uint8_t)max(wc[0], wc[1]);
-            p.eobs[3 * mb + 2] = (uint8_t)max(wc[2], wc[3]);
+        int16_t* co = p.coeffs + (size_t)mb * 384;
+        const uint32_t w0 = (uint32_t)(uint16_t)ql[0] | ((uint32_t)(uint16_t)ql[1] << 16);
+        const uint32_t w1 = (uint32_t)(uint16_t)ql[2] | ((uint32_t)(uint16_t)ql[3] << 16);
+        *(uint2*)(co + yy * 16 + xb) = make_uint2(w0, w1);
+        *(uint32_t*)(co + 256 + pl * 64 + ci) = (uint32_t)(uint16_t)qc[0] | ((uint32_t)(uint16_t)qc[1] << 16);
+        Q[256 + pl * 64 + ci] = qc[0];
+        Q[256 + pl * 64 + ci + 1] = qc[1];
+        if (u == 0) {
+            p.eobs[3 * mb] = (uint8_t)max(flags[g][0], flags[g][1]);
+            p.eobs[3 * mb + 1] = (uint8_t)(flags[g][2] >> 1);
+            p.eobs[3 * mb + 2] = (uint8_t)(flags[g][3] >> 1);
             p.opt_skip[mb] = 0;
             p.fmask[mb] = 1;
         }
     }
     // dequantisation + 16x16 inverse (row pass over u, then column pass over v)
-    if (p.intra) res[t] = (int32_t)q[t] * max((int)p.intra_ytab[t], 1);
-    else {
-        int32_t qfp = f32_to_i32_sat(roundf(__fmul_rn(qsv, 16384.0f)));
-        res[t] = wadd(wmul((int32_t)q[t], qfp), 8192) >> 14;
-    }
-    __syncthreads();
-    {  // rows[v][x] = (sum_i deq[v][i] * T[x][i] + 2^17) >> 18, wrapping
-        uint32_t acc = 0;
+    {
+        int32_t d[4];
+        if (p.intra) {
 #pragma unroll
-        for (int i = 0; i < 16; i++) acc += (uint32_t)res[yy * 16 + i] * (uint32_t)sT16[xx * 16 + i];
-        rowt[t] = (int32_t)(acc + (1u << 17)) >> 18;
-    }
-    __syncthreads();
-    {  // out[y][x] = (sum_v rows[v][x] * T[y][v] + 2^17) >> 18
-        uint32_t acc = 0;
+            for (int k = 0; k < 4; k++) d[k] = (int32_t)ql[k] * max((int)p.intra_ytab[yy * 16 + xb + k], 1);
+        } else {
+            const int32_t qfp = f32_to_i32_sat(roundf(__fmul_rn(qsv, 16384.0f)));
 #pragma unroll
-        for (int i = 0; i < 16; i++) acc += (uint32_t)rowt[i * 16 + xx] * (uint32_t)sT16[yy * 16 + i];
-        int32_t r = (int32_t)(acc + (1u << 17)) >> 18;
-        r = min(max(r, -32768), 32767);
-        int base = p.intra ? 128 : (int)pY[yi];
-        rY[yi] = (uint8_t)min(max(base + r, 0), 255);
+            for (int k = 0; k < 4; k++) d[k] = wadd(wmul((int32_t)ql[k], qfp), 8192) >> 14;
+        }
+        *(int4*)(R + yy * 16 + xb) = make_int4(d[0], d[1], d[2], d[3]);
+    }
+    mb_sync(g);
+    {  // rows[v][x] = (sum_i deq[v][i] * T[x][i] + 2^17) >> 18, wrapping   (v = yy)
+        uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const uint32_t r = (uint32_t)R[yy * 16 + i];
+            const int4 t = *(const int4*)(sT16t + i * 16 + xb);
+            a0 += r * (uint32_t)t.x; a1 += r * (uint32_t)t.y; a2 += r * (uint32_t)t.z; a3 += r * (uint32_t)t.w;
+        }
+        *(int4*)(RT + yy * 16 + xb) = make_int4((int32_t)(a0 + (1u << 17)) >> 18, (int32_t)(a1 + (1u << 17)) >> 18,
+                                                (int32_t)(a2 + (1u << 17)) >> 18, (int32_t)(a3 + (1u << 17)) >> 18);
+    }
+    mb_sync(g);
+    {  // out[y][x] = (sum_v rows[v][x] * T[y][v] + 2^17) >> 18   (y = yy)
+        uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll
+        for (int v = 0; v < 16; v++) {
+            const int4 r = *(const int4*)(RT + v * 16 + xb);
+            const uint32_t t = (uint32_t)sT16[yy * 16 + v];
+            a0 += (uint32_t)r.x * t; a1 += (uint32_t)r.y * t; a2 += (uint32_t)r.z * t; a3 += (uint32_t)r.w * t;
+        }
+        const uint32_t acc[4] = {a0, a1, a2, a3};
+        const uint32_t bv = p.intra ? 0x80808080u : *(const uint32_t*)(pY + yi);
+        uint32_t o = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            int32_t r = (int32_t)(acc[k] + (1u << 17)) >> 18;
+            r = min(max(r, -32768), 32767);
+            const int base = (int)((bv >> (8 * k)) & 255u);
+            o |= (uint32_t)min(max(base + r, 0), 255) << (8 * k);
+        }
+        *(uint32_t*)(rY + yi) = o;
     }
     // chroma 8x8 AAN inverse: pass 1 over u for each (plane, v); pass 2 over v for each (plane, x)
-    if (t < 16) {
-        int cp = t >> 3, v = t & 7;
-        int32_t s[8], o[8];
+    if (u < 16) {
+        const int cp = u >> 3, v = u & 7;
+        int32_t sv[8], o[8];
         int32_t qa = 0;
         if (!p.intra) {
             float qr = roundf(qsv);
@@ -1824,35 +1890,35 @@ __global__ void __launch_bounds__(256) k_residual(ResidualParams p) {
             qa = qr >= 65535.0f ? 65535 : (int32_t)qr;
         }
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
-            int32_t qq = p.intra ? max((int)p.intra_ctab[v * 8 + u], 1) : qa;
-            s[u] = (int32_t)q[256 + cp * 64 + v * 8 + u] * qq;
+        for (int k = 0; k < 8; k++) {
+            const int32_t qq = p.intra ? max((int)p.intra_ctab[v * 8 + k], 1) : qa;
+            sv[k] = (int32_t)Q[256 + cp * 64 + v * 8 + k] * qq;
         }
-        aan_1d(s, o, 512, 10);
+        aan_1d(sv, o, 512, 10);
 #pragma unroll
-        for (int x = 0; x < 8; x++) aant[cp][x * 8 + v] = o[x];
+        for (int x = 0; x < 8; x++) aant[g][cp][x * 8 + v] = o[x];
     }
-    __syncthreads();
-    if (t < 16) {
-        int cp = t >> 3, x = t & 7;
-        int32_t s[8], o[8];
+    mb_sync(g);
+    if (u < 16) {
+        const int cp = u >> 3, x = u & 7;
+        int32_t sv[8], o[8];
 #pragma unroll
-        for (int v = 0; v < 8; v++) s[v] = aant[cp][x * 8 + v];
-        aan_1d(s, o, 65536, 17);
+        for (int v = 0; v < 8; v++) sv[v] = aant[g][cp][x * 8 + v];
+        aan_1d(sv, o, 65536, 17);
         const uint8_t* P = cp == 0 ? pU : pV;
-        uint8_t* R = cp == 0 ? rU : rV;
+        uint8_t* Rr = cp == 0 ? rU : rV;
 #pragma unroll
         for (int y = 0; y < 8; y++) {
-            int r = min(max(o[y], -32768), 32767);
-            size_t i = (size_t)(y0 / 2 + y) * CW + x0 / 2 + x;
-            int base = p.intra ? 128 : (int)P[i];
-            R[i] = (uint8_t)min(max(base + r, 0), 255);
+            const int r = min(max(o[y], -32768), 32767);
+            const size_t i = (size_t)(y0 / 2 + y) * CW + x0 / 2 + x;
+            const int base = p.intra ? 128 : (int)P[i];
+            Rr[i] = (uint8_t)min(max(base + r, 0), 255);
         }
     }
 }
 
 int launch_residual(const ResidualParams& p, int nmb, void* stream) {
-    k_residual<<<nmb, 256, 0, (cudaStream_t)stream>>>(p);
+    k_residual<<<(nmb + RS_MB - 1) / RS_MB, 64 * RS_MB, 0, (cudaStream_t)stream>>>(p, nmb);
     return (int)cudaGetLastError();
 }
 
