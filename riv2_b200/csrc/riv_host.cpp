@@ -195,7 +195,10 @@ static std::vector<uint8_t> header_bytes(const riv_config& c, uint64_t frame_cou
 
 // glibc logf/exp2f fix-up tables, generated next to the library at build time.
 struct LibmFix {
-    std::vector<uint32_t> logf, exp2f;  // (in, out) pairs
+    std::vector<uint32_t> logf, exp2f;  // (in, out) pairs, sorted by input bits
+    // device layout: the pairs, then FIX_INDEX + 1 bucket starts (first pair whose input bits
+    // have top 16 bits >= the bucket number)
+    std::vector<uint32_t> logf_dev, exp2f_dev;
     bool ok = false;
     std::string err;
 };
@@ -226,6 +229,26 @@ static LibmFix& libm_fix() {
                     fread(F.exp2f.data(), 4, F.exp2f.size(), f) == F.exp2f.size();
         fclose(f);
         if (!good) { F.err = "short " + path; return; }
+        auto with_index = [](const std::vector<uint32_t>& pairs) {
+            std::vector<uint32_t> d(pairs);
+            const size_t n = pairs.size() / 2;
+            size_t k = 0;
+            for (uint32_t h = 0; h <= 65536u; h++) {
+                while (k < n && (pairs[2 * k] >> 16) < h) k++;
+                d.push_back((uint32_t)k);
+            }
+            return d;
+        };
+        F.logf_dev = with_index(F.logf);
+        F.exp2f_dev = with_index(F.exp2f);
+        // the batched device logf search takes 9 fixed steps: every bucket must hold < 512 pairs
+        for (uint32_t h = 0; h < 65536u; h++) {
+            const size_t n0 = F.logf.size() / 2;
+            if (F.logf_dev[n0 * 2 + h + 1] - F.logf_dev[n0 * 2 + h] >= 512u) {
+                F.err = "logf fix-up bucket too large in " + path;
+                return;
+            }
+        }
         F.ok = true;
     });
     return F;
@@ -349,6 +372,7 @@ struct riv_encoder {
     size_t coef_guess = 0;  // bytes of coefficients copied eagerly per frame
     DevBuf prof;            // optional per-MB phase stamps of the search kernel
     DevBuf tflag;           // fused table: per-MB "table row written" flags (frame tag)
+    DevBuf rowdone;         // AQ inside the search: per-row "ln variances written" flags (frame tag)
     uint64_t h2d_bytes = 0, d2h_bytes = 0, pframes = 0, launches = 0;
 };
 
@@ -453,10 +477,10 @@ static void setup_device(riv_encoder* e) {
     if (!F.ok) throw std::runtime_error("glibc fix-up table: " + F.err);
     e->nlog = (int)(F.logf.size() / 2);
     e->nexp = (int)(F.exp2f.size() / 2);
-    e->logfix.alloc(F.logf.size() * 4);
-    e->expfix.alloc(F.exp2f.size() * 4);
-    CK(cudaMemcpy(e->logfix.p, F.logf.data(), F.logf.size() * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(e->expfix.p, F.exp2f.data(), F.exp2f.size() * 4, cudaMemcpyHostToDevice));
+    e->logfix.alloc(F.logf_dev.size() * 4);
+    e->expfix.alloc(F.exp2f_dev.size() * 4);
+    CK(cudaMemcpy(e->logfix.p, F.logf_dev.data(), F.logf_dev.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(e->expfix.p, F.exp2f_dev.data(), F.exp2f_dev.size() * 4, cudaMemcpyHostToDevice));
     uint16_t yt[256], ct[64];
     intra_tables(quant_step(c.intra_quality), yt, ct);
     e->ytab.alloc(sizeof(yt));
@@ -468,6 +492,10 @@ static void setup_device(riv_encoder* e) {
     if (e->splan.fused) {
         e->tflag.alloc((size_t)N * sizeof(unsigned));
         e->tflag.zero(e->S);
+    }
+    if (e->splan.fast) {
+        e->rowdone.alloc((size_t)e->BH * sizeof(unsigned));
+        e->rowdone.zero(e->S);
     }
     // frame constants
     e->L = lambda_for(c.inter_quality, c.rdo_lambda_mult);
@@ -521,7 +549,9 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
     MbOut* mbo = e->mboutb[ck].as<MbOut>();
     // kernels per frame: rgb->yuv, (search, predict, 3 x aq), residual, deblock, scan + pack
     const int nplanes_db = 1;  // one launch for the three planes
-    e->launches += (src == 2 ? 0 : 1) + (j.type == 2 ? 5 + (e->table_ok && !e->splan.fused ? 1 : 0) : 0) + 1 +
+    // P-frame: search (+ table unless fused) (+ predict and 3 AQ unless inside the search)
+    const int p_launches = 1 + (e->table_ok && !e->splan.fused ? 1 : 0) + (e->splan.fast && e->table_ok ? 0 : 4);
+    e->launches += (src == 2 ? 0 : 1) + (j.type == 2 ? p_launches : 0) + 1 +
                    ((j.type == 2 ? e->inter_level : e->intra_level) > 0 ? nplanes_db : 0) + 2;
     if (src == 0) e->h2d_bytes += (uint64_t)c.display_width * c.display_height * 3;
     if (src == 2) e->h2d_bytes += e->yuv_bytes;
@@ -628,15 +658,34 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         // coded MVs of this frame become next frame's temporal predictors
         const int cn = e->coded_cur ^ 1;
         sp.coded_out = e->coded[cn].as<int8_t>();
+        const bool aq_in_search = e->splan.fast && e->table_ok;
+        if (aq_in_search) {  // prediction, variances and ln inside the search launch
+            sp.pred = e->pred.as<uint8_t>();
+            sp.varsum = e->varsum.as<uint2>();
+            sp.lnv = e->lnv.as<float>();
+            sp.row_done = e->rowdone.as<unsigned>();
+            sp.logfix = e->logfix.as<uint32_t>();
+            sp.nlog = e->nlog;
+        }
         CK(cudaStreamWaitEvent(S, e->ev_mbout_free[ck], 0));  // compaction of the frame two back
         CK(launch_search(sp, e->splan, S));
         CK(cudaEventRecord(s.ev_k[EV_SEARCH], S));
         CK(cudaEventRecord(e->ev_search_done, S));
-        CK(launch_predict(e->ref[e->ref_cur].as<uint8_t>(), mbo, e->pred.as<uint8_t>(), e->varsum.as<uint2>(), W, H, S));
+        if (!aq_in_search)
+            CK(launch_predict(e->ref[e->ref_cur].as<uint8_t>(), mbo, e->pred.as<uint8_t>(), e->varsum.as<uint2>(), W, H, S));
         CK(cudaEventRecord(s.ev_k[EV_PRED], S));
-        CK(launch_aq(e->varsum.as<uint2>(), N, e->inter_base, e->logfix.as<uint32_t>(), e->nlog, e->expfix.as<uint32_t>(),
-                     e->nexp, e->lnv.as<float>(), e->qs.as<float>(), S));
+        if (!aq_in_search)
+            CK(launch_aq(e->varsum.as<uint2>(), N, e->inter_base, e->logfix.as<uint32_t>(), e->nlog, e->expfix.as<uint32_t>(),
+                         e->nexp, e->lnv.as<float>(), e->qs.as<float>(), S));
         CK(cudaEventRecord(s.ev_k[EV_AQ], S));
+        if (aq_in_search) {  // the residual derives the steps from the ln variances and their mean
+            rp.lnv = e->lnv.as<float>();
+            rp.aq_base = e->inter_base;
+            rp.expfix = e->expfix.as<uint32_t>();
+            rp.nexp = e->nexp;
+            rp.qs_out = e->qs.as<float>();
+            rp.ref = e->ref[e->ref_cur].as<uint8_t>();  // chroma prediction in the residual kernel
+        }
         rp.intra = 0;
         rp.mb = mbo;
         rp.qs = e->qs.as<float>();
@@ -1047,7 +1096,7 @@ void riv_encoder_free(riv_encoder* e) {
     DevBuf* bufs[] = {&e->curb[0], &e->curb[1], &e->ref[0], &e->ref[1], &e->recon_pre, &e->pred, &e->mboutb[0], &e->mboutb[1],
                       &e->coded[0], &e->coded[1], &e->rec,
                       &e->varsum, &e->lnv, &e->qs, &e->coeffs, &e->opt_skip, &e->fmask, &e->eobs, &e->status,
-                      &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset, &e->sadtab, &e->prof, &e->tflag, &e->newcost, &e->newcost32};
+                      &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset, &e->sadtab, &e->prof, &e->tflag, &e->rowdone, &e->newcost, &e->newcost32};
     for (DevBuf* b : bufs) b->release();
     if (e->S) cudaStreamDestroy(e->S);
     if (e->C) cudaStreamDestroy(e->C);
@@ -1247,13 +1296,14 @@ riv_status riv_stage_deblock_noalloc(uint8_t* yuv, uint32_t w, uint32_t h, int l
 riv_status riv_stage_libm(int which, const float* in, float* out, size_t n) {
     LibmFix& F = libm_fix();
     if (!F.ok) return RIV_ERR_ENCODING_FAILED;
-    const std::vector<uint32_t>& fx = which == 0 ? F.logf : F.exp2f;
+    const std::vector<uint32_t>& fx = which == 0 ? F.logf_dev : F.exp2f_dev;
+    const int npairs = (int)((which == 0 ? F.logf : F.exp2f).size() / 2);
     void *di = nullptr, *dout = nullptr, *df = nullptr;
     riv_status st = RIV_OK;
     if (cudaMalloc(&di, n * 4) || cudaMalloc(&dout, n * 4) || cudaMalloc(&df, fx.size() * 4 + 4) ||
         cudaMemcpy(di, in, n * 4, cudaMemcpyHostToDevice) ||
         cudaMemcpy(df, fx.data(), fx.size() * 4, cudaMemcpyHostToDevice) ||
-        launch_libm_eval(which, (const float*)di, (float*)dout, n, (const uint32_t*)df, (int)(fx.size() / 2), 0) ||
+        launch_libm_eval(which, (const float*)di, (float*)dout, n, (const uint32_t*)df, npairs, 0) ||
         cudaMemcpy(out, dout, n * 4, cudaMemcpyDeviceToHost))
         st = RIV_ERR_CUDA;
     cudaFree(di);

@@ -57,6 +57,14 @@ struct SearchParams {
     long long* prof;  // optional: 16 words per MB (phase clock stamps, hexagon rounds), nullptr = off
     int nrow_ctas;    // CTAs that own MB rows (row stride); the rest of the grid are table workers
     unsigned* tflag;  // fused table: per-MB flag = tag once its table row is written; nullptr = precomputed
+    // Prediction and AQ inside the search launch (band + table instantiations): nullptr lnv =
+    // done by the separate predict / AQ kernels.
+    uint8_t* pred;             // planar YUV prediction out
+    uint2* varsum;             // per MB (sum, sum of squares) of the predicted luma
+    float* lnv;                // BW*BH ln variances, then the mean
+    unsigned* row_done;        // per MB row: tag once its ln variances are written
+    const uint32_t* logfix;    // glibc logf fix-up pairs + bucket index
+    int nlog;
 };
 
 struct ResidualParams {
@@ -73,6 +81,13 @@ struct ResidualParams {
     int W, H, BW, intra;
     const uint16_t* intra_ytab;  // 256 (intra)
     const uint16_t* intra_ctab;  // 64 (intra)
+    // AQ step computed here from the ln variances and their mean (lnv != nullptr), else read qs
+    const float* lnv;            // n ln variances, then the mean
+    float aq_base;
+    const uint32_t* expfix;
+    int nexp;
+    float* qs_out;               // the steps, written for inspection
+    const uint8_t* ref;          // chroma prediction computed here from this reference (nullptr: read pred)
 };
 
 enum StatusBits : unsigned {
@@ -85,6 +100,7 @@ int launch_rgb_to_yuv(const uint8_t* rgb, int dw, int dh, uint8_t* yuv, int W, i
 // Launch plan of the search wavefront (chosen once per encoder).  fused: the SAD table is
 // computed inside the same cooperative launch by `grid - nrow` worker CTAs.
 struct SearchPlan {
+    bool fast;   // band + table instantiation: loader and AQ warps (prediction and AQ in the launch)
     bool fused;
     int grid, nrow, threads;
     size_t smem;

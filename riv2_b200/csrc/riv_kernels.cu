@@ -345,6 +345,74 @@ __device__ __forceinline__ int argmin8(long long total, bool valid, long long& b
         if (p.prof != nullptr && lane == 0) p.prof[(size_t)idx * 16 + (k)] = clock64(); \
     } while (0)
 
+// Rounded bilinear sample at half-pel position (xh, yh) with the coordinates clamped to the
+// plane (com/motion.rs:28-117).
+__device__ __forceinline__ int sample_round(const uint8_t* __restrict__ pl, int w, int h, int xh, int yh) {
+    xh = min(max(xh, 0), (w - 1) * 2);
+    yh = min(max(yh, 0), (h - 1) * 2);
+    int x0 = xh >> 1, y0 = yh >> 1;
+    int xo = xh & 1, yo = yh & 1;
+    int x1 = min(x0 + 1, w - 1), y1 = min(y0 + 1, h - 1);
+    int a = pl[(size_t)y0 * w + x0];
+    if (!xo && !yo) return a;
+    int b = pl[(size_t)y0 * w + x1], d = pl[(size_t)y1 * w + x0], e = pl[(size_t)y1 * w + x1];
+    if (xo && !yo) return (a + b + 1) >> 1;
+    if (!xo && yo) return (a + d + 1) >> 1;
+    return (a + b + d + e + 2) >> 2;
+}
+
+// fix: n (input bits, glibc result bits) pairs sorted by input bits, followed by 65537 bucket
+// starts indexed by the top 16 input bits; the search runs inside one bucket.
+__device__ __forceinline__ float apply_fix(float x, float y, const uint32_t* fix, int n) {
+    uint32_t key = __float_as_uint(x);
+    const uint32_t* idx = fix + 2 * (size_t)n;
+    int lo = (int)__ldg(idx + (key >> 16)), hi = (int)__ldg(idx + (key >> 16) + 1);
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        uint32_t k = __ldg(fix + 2 * mid);
+        if (k < key) lo = mid + 1; else hi = mid;
+    }
+    if (lo < n && __ldg(fix + 2 * lo) == key) return __uint_as_float(__ldg(fix + 2 * lo + 1));
+    return y;
+}
+__device__ __forceinline__ float glibc_logf(float x, const uint32_t* fix, int n) {
+    return apply_fix(x, __double2float_rn(log((double)x)), fix, n);
+}
+__device__ __forceinline__ float glibc_exp2f(float x, const uint32_t* fix, int n) {
+    return apply_fix(x, __double2float_rn(exp2((double)x)), fix, n);
+}
+// glibc logf of FB values at once: FB independent bucket searches advance together (a fixed
+// FIX_STEPS steps covers the longest bucket, 478 entries), so their dependent loads overlap.
+constexpr int FIX_STEPS = 9;
+template <int FB>
+__device__ __forceinline__ void glibc_logf_batch(const float (&x)[FB], float (&y)[FB], const uint32_t* fix, int n) {
+    const uint32_t* idx = fix + 2 * (size_t)n;
+    uint32_t key[FB];
+    int lo[FB], hi[FB];
+#pragma unroll
+    for (int j = 0; j < FB; j++) {
+        key[j] = __float_as_uint(x[j]);
+        y[j] = __double2float_rn(log((double)x[j]));
+        lo[j] = (int)__ldg(idx + (key[j] >> 16));
+        hi[j] = (int)__ldg(idx + (key[j] >> 16) + 1);
+    }
+#pragma unroll 1
+    for (int step = 0; step < FIX_STEPS; step++) {
+#pragma unroll
+        for (int j = 0; j < FB; j++) {
+            const int mid = (lo[j] + hi[j]) >> 1;
+            const uint32_t k = lo[j] < hi[j] ? __ldg(fix + 2 * mid) : 0u;
+            if (lo[j] < hi[j]) {
+                if (k < key[j]) lo[j] = mid + 1;
+                else hi[j] = mid;
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < FB; j++)
+        if (lo[j] < n && __ldg(fix + 2 * lo[j]) == key[j]) y[j] = __uint_as_float(__ldg(fix + 2 * lo[j] + 1));
+}
+
 // ---- search warp -> mode warp handoff through a shared-memory ring (one CTA per MB row)
 // Slot word: [63:49] (n + 1) mod 2^15 for the n-th MB of the CTA, [48] failure, [47:32] best
 // SAD (at most 255 * 256), [31:0] raw MV (dx, dy, sx, sy as bytes).  Tag and payload share
@@ -352,10 +420,12 @@ __device__ __forceinline__ int argmin8(long long total, bool valid, long long& b
 constexpr int HAND_RING = 64;
 constexpr unsigned long long HAND_FAIL = 1ull << 48;
 
+// done[0]: MBs the mode warp has taken, done[1]: MBs the AQ warp has taken (a large value
+// when there is none); a slot is reused once both have taken its previous MB.
 __device__ __forceinline__ bool hand_put(unsigned long long* hand, volatile int* done, int n,
                                          unsigned long long payload, long long limit) {
     long long spins = 0;
-    while (n - *done >= HAND_RING) {  // the slot's previous MB has not been taken yet
+    while (n - min(done[0], done[1]) >= HAND_RING) {  // the slot's previous MB has not been taken yet
         if (++spins > limit) return false;
         __nanosleep(32);
     }
@@ -635,7 +705,7 @@ __device__ __forceinline__ void loader_warp(const SearchParams& p, unsigned long
     };
     for (int r = blockIdx.x; r < p.BH && !abort; r += p.nrow_ctas) {
         const int wy0 = r * 16 - sr - 1;
-        if (rows > 0 && !wait_ctl(1, rows)) { abort = true; break; }
+        if (rows > 0 && !(wait_ctl(1, rows) && (p.lnv == nullptr || wait_ctl(3, rows)))) { abort = true; break; }
         // ---- the band: rows wy0 .. wy0+WS-1 (edge-clamped), columns -MARGIN .. W+MARGIN-1
         for (int i = lane; i < WS; i += 32) {
             const int gy = min(max(wy0 + i, 0), p.H - 1);
@@ -697,6 +767,151 @@ __device__ __forceinline__ void loader_warp(const SearchParams& p, unsigned long
     }
 }
 
+// The fourth warp of each row CTA (band + table instantiations, P-frames): for every MB the
+// search warp hands over, in raster order, the luma motion-compensated prediction
+// (build_predicted, com/fast_motion.rs:103-352) from the row's reference band, where the
+// replicated edges give the same samples as the reference's clamped coordinates, and the
+// predicted-luma sums (sum, sum of squares) for the MB's variance (compute_aq_quant_steps,
+// res/residual.rs:116-153).  Chroma prediction is left to the residual kernel.  After each row it publishes row_done[r] = tag.  ctl[3] = rows it has finished (the loader refills
+// the band only after both the search warp and this warp are done with it).
+__device__ __forceinline__ void aq_warp(const SearchParams& p, const unsigned long long* hand, volatile int* hand_done,
+                                        volatile int* ctl, const uint8_t* band, unsigned long long* bandb) {
+    const int lane = threadIdx.x & 31;
+    const int sr = p.sr, MARGIN = (sr + 1 + 15) & ~15, BWB = p.W + 2 * MARGIN;
+    const int W = p.W, H = p.H, CW = W / 2, CH = H / 2;
+    uint8_t* PY = p.pred;
+    const int yy = lane >> 1, xoff = (lane & 1) * 8;  // luma: row, 8-pixel half
+    int n = 0, rows = 0;
+    for (int r = blockIdx.x; r < p.BH; r += p.nrow_ctas) {
+        const int y0 = r * 16, wy0 = y0 - sr - 1;
+        // observe the band fill of this row (the loader refills only after this warp is done)
+        if (!mbar_wait_warp(bandb, (unsigned)(rows & 1), p.spin_limit)) {
+            if (lane == 0) atomicOr(p.status, ST_WAIT_TIMEOUT);
+            return;
+        }
+        for (int bx = 0; bx < p.BW; bx++) {
+            const int idx = r * p.BW + bx, x0 = bx * 16;
+            unsigned long long hw = 0;
+            int st = 0;
+            if (lane == 0) {
+                if (!hand_get(hand, n, hw, p.spin_limit)) st = 1;
+                else if (hw & HAND_FAIL) st = 2;
+                else hand_done[1] = n + 1;
+            }
+            st = __shfl_sync(0xffffffffu, st, 0);
+            if (st != 0) {
+                if (lane == 0 && st == 1) atomicOr(p.status, ST_WAIT_TIMEOUT);
+                return;
+            }
+            n++;
+            hw = __shfl_sync(0xffffffffu, hw, 0);
+            const int mdx = 2 * (int)(int8_t)hw + (int)(int8_t)(hw >> 16);
+            const int mdy = 2 * (int)(int8_t)(hw >> 8) + (int)(int8_t)(hw >> 24);
+            const int xo = mdx & 1, yo = mdy & 1;
+            // luma: 8 samples of row yy from two 12-byte windows (this row and the next) of the
+            // band, with packed rounded averages; the sums come from dp4a
+            unsigned s = 0, s2 = 0;
+            {
+                const int byp = (2 * (y0 + yy) + mdy) >> 1;
+                const int c0 = x0 + xoff + (mdx >> 1);  // first integer column (floor)
+                const uint8_t* rp = band + (size_t)(byp - wy0) * BWB + MARGIN + c0;
+                uint32_t A[2][3];  // bytes c0 .. c0+11 of rows byp, byp+1
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(rp + j * BWB);
+                    const uint32_t al = sa & ~3u, sh = (sa & 3u) * 8;
+                    const uint32_t q0 = lds_aligned(al), q1 = lds_aligned(al + 4), q2 = lds_aligned(al + 8),
+                                   q3 = lds_aligned(al + 12);
+                    A[j][0] = __funnelshift_r(q0, q1, sh);
+                    A[j][1] = __funnelshift_r(q1, q2, sh);
+                    A[j][2] = __funnelshift_r(q2, q3, sh);
+                }
+                uint32_t P[2];
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const uint32_t a = A[0][h], b = __funnelshift_r(A[0][h], A[0][h + 1], 8);
+                    const uint32_t d = A[1][h], e = __funnelshift_r(A[1][h], A[1][h + 1], 8);
+                    if (!xo && !yo) P[h] = a;
+                    else if (xo && !yo) P[h] = (a | b) - (((a ^ b) >> 1) & 0x7F7F7F7Fu);  // (a + b + 1) >> 1
+                    else if (!xo && yo) P[h] = (a | d) - (((a ^ d) >> 1) & 0x7F7F7F7Fu);
+                    else {  // (a + b + d + e + 2) >> 2 in 16-bit lanes (sums <= 1022)
+                        const uint32_t m = 0x00FF00FFu;
+                        const uint32_t lo = ((a & m) + (b & m) + (d & m) + (e & m) + 0x00020002u) >> 2;
+                        const uint32_t hi = (((a >> 8) & m) + ((b >> 8) & m) + ((d >> 8) & m) + ((e >> 8) & m) + 0x00020002u) >> 2;
+                        P[h] = (lo & m) | ((hi & m) << 8);
+                    }
+                    s = __dp4a(P[h], 0x01010101u, s);
+                    s2 = __dp4a(P[h], P[h], s2);
+                }
+                *(uint2*)(PY + (size_t)(y0 + yy) * W + x0 + xoff) = make_uint2(P[0], P[1]);
+            }
+            s = __reduce_add_sync(0xffffffffu, s);
+            s2 = __reduce_add_sync(0xffffffffu, s2);
+            if (lane == 0) p.varsum[idx] = make_uint2(s, s2);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            __threadfence();
+            st_release_u32(p.row_done + r, p.tag);
+            ctl[3] = rows + 1;
+        }
+        rows++;
+    }
+}
+
+// The per-MB ln variances and their Iterator::sum, strictly left to right in raster order,
+// while the rows are still being searched: one warp waits for each row's row_done flag,
+// computes the row's glibc-exact ln variances in parallel, stages them in shared memory and
+// its lane 0 folds them.  Then avg = sum / n (res/residual.rs:116-167).
+__device__ __forceinline__ void aq_fold(const SearchParams& p, volatile int* ctl, float* stage) {
+    const int lane = threadIdx.x & 31;
+    float part = 0.0f;
+    for (int r = 0; r < p.BH; r++) {
+        long long spins = 0;
+        bool ok = true;
+        while (!__all_sync(0xffffffffu, ld_acquire_u32(p.row_done + r) == p.tag)) {
+            if (ctl[2] != 0 || ++spins > p.spin_limit) { ok = false; break; }
+            __nanosleep(64);
+        }
+        if (!ok) {
+            if (lane == 0) atomicOr(p.status, ST_WAIT_TIMEOUT);
+            return;
+        }
+        for (int c0 = 0; c0 < p.BW; c0 += 256) {
+            const int m = min(256, p.BW - c0);
+            for (int b0 = 0; b0 < m; b0 += 4 * 32) {  // ln variance of each MB (res/residual.rs:134-153)
+                float v4[4], l4[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int i = b0 + j * 32 + lane;
+                    float var = 4.0f;
+                    if (i < m) {
+                        const uint2 vs = p.varsum[(size_t)r * p.BW + c0 + i];
+                        const unsigned long long N = 256ull * vs.y - (unsigned long long)vs.x * vs.x;
+                        var = __fdiv_rn(__ull2float_rn(N), 65536.0f);
+                        var = var < 4.0f ? 4.0f : var;
+                    }
+                    v4[j] = var;
+                }
+                glibc_logf_batch<4>(v4, l4, p.logfix, p.nlog);
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int i = b0 + j * 32 + lane;
+                    if (i < m) {
+                        p.lnv[(size_t)r * p.BW + c0 + i] = l4[j];
+                        stage[i] = l4[j];
+                    }
+                }
+            }
+            __syncwarp();
+            if (lane == 0)
+                for (int i = 0; i < m; i++) part = __fadd_rn(part, stage[i]);
+            __syncwarp();
+        }
+    }
+    if (lane == 0) p.lnv[(size_t)p.BW * p.BH] = __fdiv_rn(part, (float)(p.BW * p.BH));
+}
+
 template <bool BAND, bool TABLE, bool SMALL>
 __global__ void __launch_bounds__(512, 1) k_search(SearchParams p) {
     // FAST (band + table): three warps -- search chain, mode decision, loader.  Otherwise the
@@ -716,7 +931,8 @@ __global__ void __launch_bounds__(512, 1) k_search(SearchParams p) {
     unsigned long long* fullb = (unsigned long long*)after_hand;
     unsigned long long* bandb = fullb + LD_RING;
     volatile int* ld_ctl = (volatile int*)(bandb + 1);
-    uint8_t* slots = after_hand + 64;
+    float* fold_stage = (float*)(after_hand + 64);  // 256 floats (CTA 0's ln-variance fold)
+    uint8_t* slots = after_hand + 64 + 1024;
     // other layouts: double-buffered current block and table row
     uint8_t* curbuf = after_hand;  // 2 x 256 bytes
     uint16_t* tabbuf = (uint16_t*)(curbuf + 512);   // TABLE: 2 x tstride entries
@@ -734,18 +950,24 @@ __global__ void __launch_bounds__(512, 1) k_search(SearchParams p) {
         for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x) nc32s[i] = p.newcost32[i];
     for (int i = threadIdx.x; i < HAND_RING; i += blockDim.x) hand[i] = 0ull;
     if (threadIdx.x == 0) {
-        *hand_done = 0;
+        hand_done[0] = 0;
+        hand_done[1] = FAST && p.lnv != nullptr ? 0 : 0x3fffffff;  // no AQ warp: never waited for
         if (FAST) {
             for (int i = 0; i < LD_RING; i++) mbar_init(fullb + i, 1);
             mbar_init(bandb, 32);
-            ld_ctl[0] = ld_ctl[1] = ld_ctl[2] = 0;
+            ld_ctl[0] = ld_ctl[1] = ld_ctl[2] = ld_ctl[3] = 0;
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
     }
     __syncthreads();
     const unsigned long long tagbits = (unsigned long long)(p.tag & 0xffffu) << 48;
     if (threadIdx.x >= 64) {
-        if (FAST && threadIdx.x < 96) loader_warp(p, fullb, bandb, ld_ctl, slots, refmem);
+        if (FAST && threadIdx.x < 96) {
+            loader_warp(p, fullb, bandb, ld_ctl, slots, refmem);
+            if (p.lnv != nullptr && blockIdx.x == 0) aq_fold(p, ld_ctl, fold_stage);
+        } else if (FAST && threadIdx.x < 128 && p.lnv != nullptr) {
+            aq_warp(p, hand, hand_done, ld_ctl, refmem, bandb);
+        }
         return;
     }
     if (threadIdx.x >= 32) {
@@ -1361,10 +1583,10 @@ static size_t search_smem(int sr, int W, bool band, bool table) {
     size_t margin = ((size_t)sr + 1 + 15) & ~(size_t)15;
     size_t ref = band ? ws * ((size_t)W + 2 * margin) : ws * ws;
     size_t head = 256 * sizeof(double) + 64 * 64 * 4 + HAND_RING * 8 + 16;
-    if (band && table) return head + 64 + LD_RING * (size_t)ld_slot_bytes(sad_table_stride(sr)) + ref + 16;
+    if (band && table) return head + 64 + 1024 + LD_RING * (size_t)ld_slot_bytes(sad_table_stride(sr)) + ref + 16;
     return head + 512 + (table ? 4 * (size_t)sad_table_stride(sr) : 0) + ref + 16;
 }
-static int search_threads(bool band, bool table) { return band && table ? 96 : 64; }
+static int search_threads(bool band, bool table) { return band && table ? 128 : 64; }
 static const size_t SEARCH_SMEM_MAX = 200 * 1024;
 static bool search_use_band(int sr, int W) {
     return search_smem(sr, W, true, search_use_table(sr)) <= SEARCH_SMEM_MAX;
@@ -1394,6 +1616,7 @@ int search_plan(int sr, int W, int BH, bool table, bool small, SearchPlan* out) 
     const size_t sm = search_smem(sr, W, band, table);
     SearchPlan pl{};
     pl.threads = threads;
+    pl.fast = band && table;
     if (band && table) {
         // fused: one CTA per SM (the shared-memory request rules out a second), rows first,
         // table workers on the SMs the rows leave free -- used when enough of them remain
@@ -1444,20 +1667,6 @@ int launch_search(const SearchParams& p, const SearchPlan& plan, void* stream) {
 // chroma: copy at the truncated (x0+dx)/2 origin for in-bounds integer MVs, else
 // rounded bilinear at chroma half-pel (2c + (mv_hp >> 1)).
 // ---------------------------------------------------------------------------------
-__device__ __forceinline__ int sample_round(const uint8_t* __restrict__ pl, int w, int h, int xh, int yh) {
-    xh = min(max(xh, 0), (w - 1) * 2);
-    yh = min(max(yh, 0), (h - 1) * 2);
-    int x0 = xh >> 1, y0 = yh >> 1;
-    int xo = xh & 1, yo = yh & 1;
-    int x1 = min(x0 + 1, w - 1), y1 = min(y0 + 1, h - 1);
-    int a = pl[(size_t)y0 * w + x0];
-    if (!xo && !yo) return a;
-    int b = pl[(size_t)y0 * w + x1], d = pl[(size_t)y1 * w + x0], e = pl[(size_t)y1 * w + x1];
-    if (xo && !yo) return (a + b + 1) >> 1;
-    if (!xo && yo) return (a + d + 1) >> 1;
-    return (a + b + d + e + 2) >> 2;
-}
-
 __global__ void __launch_bounds__(256) k_predict(const uint8_t* __restrict__ ref, const MbOut* __restrict__ mbo,
                                                  uint8_t* __restrict__ pred, uint2* __restrict__ varsum, int W, int H) {
     const int BW = W / 16;
@@ -1517,24 +1726,6 @@ int launch_predict(const uint8_t* ref, const MbOut* mb, uint8_t* pred, uint2* va
 // function rounded to float, then a sorted fix-up table (input bits -> glibc output
 // bits) built at build time by running glibc over the whole reachable input domain.
 // ---------------------------------------------------------------------------------
-__device__ __forceinline__ float apply_fix(float x, float y, const uint32_t* fix, int n) {
-    uint32_t key = __float_as_uint(x);
-    int lo = 0, hi = n;  // pairs (in, out) at fix[2i], fix[2i+1]
-    while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        uint32_t k = __ldg(fix + 2 * mid);
-        if (k < key) lo = mid + 1; else hi = mid;
-    }
-    if (lo < n && __ldg(fix + 2 * lo) == key) return __uint_as_float(__ldg(fix + 2 * lo + 1));
-    return y;
-}
-__device__ __forceinline__ float glibc_logf(float x, const uint32_t* fix, int n) {
-    return apply_fix(x, __double2float_rn(log((double)x)), fix, n);
-}
-__device__ __forceinline__ float glibc_exp2f(float x, const uint32_t* fix, int n) {
-    return apply_fix(x, __double2float_rn(exp2((double)x)), fix, n);
-}
-
 __global__ void k_libm_eval(int which, const float* in, float* out, size_t n, const uint32_t* fix, int nfix) {
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     size_t stride = (size_t)gridDim.x * blockDim.x;
@@ -1667,6 +1858,8 @@ __global__ void __launch_bounds__(256) k_residual(ResidualParams p, int nmb) {
     __shared__ __align__(16) int16_t q[RS_MB][384];
     __shared__ int32_t aant[RS_MB][2][64];
     __shared__ int flags[RS_MB][4];  // nonzero, luma eob of warp 0 / warp 1
+    __shared__ float qsh[RS_MB];
+    __shared__ uint8_t predc[RS_MB][128];  // chroma prediction (U then V, 8x8 each)
     const int tid = threadIdx.x;
     for (int i = tid; i < 256; i += 256) {
         sT16[i] = c_T16[i];
@@ -1696,9 +1889,33 @@ __global__ void __launch_bounds__(256) k_residual(ResidualParams p, int nmb) {
     int32_t* RCT = rowc[g];
     int16_t* Q = q[g];
 
+    // chroma prediction of this thread's two samples: computed here from the reference planes
+    // (build_predicted's chroma rule, com/fast_motion.rs:264-345) or read from pred
+    uint32_t pcw;
+    if (!p.intra && p.ref != nullptr) {
+        const MbOut m = p.mb[mb];
+        const int mdx = m.raw[0] * 2 + m.raw[2], mdy = m.raw[1] * 2 + m.raw[3];
+        const bool integer = ((mdx & 1) == 0) && ((mdy & 1) == 0);
+        const int sx0 = x0 + (mdx >> 1), sy0 = y0 + (mdy >> 1);
+        const bool copy = integer && sx0 >= 0 && sy0 >= 0 && sx0 + 15 < W && sy0 + 15 < H;
+        const uint8_t* Rp = p.ref + (size_t)W * H + (pl == 0 ? 0 : (size_t)CW * CH);
+        const int cyg = y0 / 2 + cyy;
+        int c2[2];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const int cxg = x0 / 2 + cxx + k;
+            c2[k] = copy ? Rp[(size_t)(sy0 / 2 + cyy) * CW + sx0 / 2 + cxx + k]
+                         : sample_round(Rp, CW, CH, 2 * cxg + (mdx >> 1), 2 * cyg + (mdy >> 1));
+        }
+        pcw = (uint32_t)c2[0] | ((uint32_t)c2[1] << 8);
+    } else {
+        pcw = p.intra ? 0x8080u : *(const uint16_t*)(pC + cidx);
+    }
+    predc[g][pl * 64 + ci] = (uint8_t)pcw;
+    predc[g][pl * 64 + ci + 1] = (uint8_t)(pcw >> 8);
     auto copy_pred = [&]() {  // recon = prediction, coefficients zero
         *(uint32_t*)(rY + yi) = *(const uint32_t*)(pY + yi);
-        *(uint16_t*)(rC + cidx) = *(const uint16_t*)(pC + cidx);
+        *(uint16_t*)(rC + cidx) = (uint16_t)pcw;
         int16_t* co = p.coeffs + (size_t)mb * 384;
         *(uint2*)(co + yy * 16 + xb) = make_uint2(0u, 0u);
         *(uint32_t*)(co + 256 + pl * 64 + ci) = 0u;
@@ -1709,6 +1926,15 @@ __global__ void __launch_bounds__(256) k_residual(ResidualParams p, int nmb) {
             p.eobs[3 * mb] = p.eobs[3 * mb + 1] = p.eobs[3 * mb + 2] = 0;
         }
     };
+    if (!p.intra && p.lnv != nullptr) {  // AQ step (compute_aq_quant_steps, res/residual.rs:154-167)
+        if (u == 0) {
+            const float off = __fmul_rn(0.8f, __fsub_rn(p.lnv[mb], p.lnv[nmb]));
+            const float q = __fmul_rn(p.aq_base, glibc_exp2f(__fdiv_rn(off, 6.0f), p.expfix, p.nexp));
+            qsh[g] = q;
+            p.qs_out[mb] = q;
+        }
+        mb_sync(g);
+    }
     if (!p.intra && p.mb[mb].rdo_skip) {  // never transformed: residual 0, recon = prediction
         copy_pred();
         return;
@@ -1719,7 +1945,7 @@ __global__ void __launch_bounds__(256) k_residual(ResidualParams p, int nmb) {
 #pragma unroll
         for (int k = 0; k < 4; k++) R[yy * 16 + xb + k] = (int)((cv >> (8 * k)) & 255u) - (int)((pv >> (8 * k)) & 255u);
         const uint32_t cc = *(const uint16_t*)(cC + cidx);
-        const uint32_t pc = p.intra ? 0x8080u : *(const uint16_t*)(pC + cidx);
+        const uint32_t pc = pcw;
         RC[pl * 64 + ci] = (int)(cc & 255u) - (int)(pc & 255u);
         RC[pl * 64 + ci + 1] = (int)(cc >> 8) - (int)(pc >> 8);
     }
@@ -1784,7 +2010,7 @@ __global__ void __launch_bounds__(256) k_residual(ResidualParams p, int nmb) {
             qc[k] = f32_to_i16_sat(roundf(__fdiv_rn(__int2float_rn(coefc[k]), qq)));
         }
     } else {
-        qsv = p.qs[mb];
+        qsv = p.lnv != nullptr ? qsh[g] : p.qs[mb];
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             const float r = __fdiv_rn(__int2float_rn(coef[k]), qsv);
@@ -1905,13 +2131,12 @@ __global__ void __launch_bounds__(256) k_residual(ResidualParams p, int nmb) {
 #pragma unroll
         for (int v = 0; v < 8; v++) sv[v] = aant[g][cp][x * 8 + v];
         aan_1d(sv, o, 65536, 17);
-        const uint8_t* P = cp == 0 ? pU : pV;
         uint8_t* Rr = cp == 0 ? rU : rV;
 #pragma unroll
         for (int y = 0; y < 8; y++) {
             const int r = min(max(o[y], -32768), 32767);
             const size_t i = (size_t)(y0 / 2 + y) * CW + x0 / 2 + x;
-            const int base = p.intra ? 128 : (int)P[i];
+            const int base = p.intra ? 128 : (int)predc[g][cp * 64 + y * 8 + x];
             Rr[i] = (uint8_t)min(max(base + r, 0), 255);
         }
     }
