@@ -171,6 +171,35 @@ riv_status riv_libm_fixup_counts(uint32_t* nlog, uint32_t* nexp);
 /* The DCT bases the device uses (T16[i][j], T8[i][j]: sample i, frequency j). */
 void riv_dct_tables(int32_t* t16, int32_t* t8);
 
+/* ---- Decoder (reitero_decode) up to the YUV reconstruction ---- */
+/* DecodeError (dec/error.rs:4-20): Io, InvalidHeader, DecodingFailed, InvalidFrame,
+ * EndOfStream, plus device failures. */
+typedef enum {
+    RIV_DEC_OK = 0,
+    RIV_DEC_IO = 1,               /* truncated stream */
+    RIV_DEC_INVALID_HEADER = 2,
+    RIV_DEC_DECODING_FAILED = 3,
+    RIV_DEC_INVALID_FRAME = 4,
+    RIV_DEC_END_OF_STREAM = 5,
+    RIV_DEC_CUDA = 6
+} riv_dec_status;
+typedef struct riv_decoder riv_decoder;
+/* Decoder::new (dec/decoder.rs:112-171) over an in-memory .riv stream (copied): parses and
+ * validates the 36-byte header; reconstruction runs on CUDA device `device`. */
+riv_dec_status riv_decoder_new(const uint8_t* data, size_t len, int device, riv_decoder** out);
+/* Decoder::header (dec/decoder.rs:470-473): dims5 = display w, h, storage w, h, fps. */
+riv_dec_status riv_decoder_info(const riv_decoder* dec, uint32_t* dims5, uint64_t* frame_count);
+/* Decoder::decode_frame (dec/decoder.rs:174-460) up to the storage-size YUV 4:2:0
+ * reconstruction (the reference's final RGB conversion and crop are not on this path).
+ * y/u/v (each nullable) receive the planes; the call returns once the frame is decoded.
+ * RIV_DEC_END_OF_STREAM after the last frame. */
+riv_dec_status riv_decode_frame_yuv(riv_decoder* dec, uint8_t* y, uint8_t* u, uint8_t* v, uint32_t* frame_type,
+                                    uint64_t* timestamp_ms);
+/* Decoder::current_frame (dec/decoder.rs:475-478). */
+uint64_t riv_decoder_current_frame(const riv_decoder* dec);
+const char* riv_decoder_last_error(const riv_decoder* dec);
+void riv_decoder_free(riv_decoder* dec);
+
 #ifdef __cplusplus
 }
 #endif

@@ -110,6 +110,60 @@ void RansWriter::drain() {
     sp_ = BATCH;
 }
 
+// RansDecoder (com/rans.rs:299-354): two interleaved states, each symbol first takes the
+// older state; a drain boundary every BATCH symbols reloads both states.
+RansReader::RansReader(const uint8_t* data, size_t len) : d_(data), len_(len) {
+    entropy_init();
+    r0_ = word();
+    r0_ |= (uint32_t)word() << 16;
+    r1_ = word();
+    r1_ |= (uint32_t)word() << 16;
+}
+uint16_t RansReader::word() {
+    if (pos_ + 2 > len_) {
+        error = true;
+        pos_ = len_;
+        return 0;
+    }
+    uint16_t v = (uint16_t)(d_[pos_] | (d_[pos_ + 1] << 8));
+    pos_ += 2;
+    return v;
+}
+void RansReader::next_symbol() {
+    if (count_ == BATCH) {
+        count_ = 0;
+        r0_ = word();
+        r0_ |= (uint32_t)word() << 16;
+        r1_ = word();
+        r1_ |= (uint32_t)word() << 16;
+    }
+    count_++;
+}
+void RansReader::advance(uint32_t& r, uint32_t start, uint32_t freq) {
+    r = freq * (r >> 8) + (r & 255) - start;
+    if (r < 65536) r = (r << 16) | word();
+}
+bool RansReader::get(BinProb& ctx) {
+    next_symbol();
+    uint32_t r = r0_;
+    r0_ = r1_;
+    const uint32_t p = prob_zero(ctx);
+    const bool bit = (r & 255) >= p;
+    observe(ctx, bit);
+    advance(r, bit ? p : 0, bit ? 256u - p : p);
+    r1_ = r;
+    return bit;
+}
+bool RansReader::get_bypass() {
+    next_symbol();
+    uint32_t r = r0_;
+    r0_ = r1_;
+    const uint32_t start = r & 0x80;
+    advance(r, start, 128);
+    r1_ = r;
+    return start != 0;
+}
+
 // ---------------------------------------------------------------------------------
 // DCT coefficient coder (res/rans.rs:34-330)
 // ---------------------------------------------------------------------------------
@@ -174,6 +228,50 @@ void encode_residual_frame(const int16_t* packed, const uint8_t* eobs, int nbloc
     }
     w.finish();
     delete c;
+}
+
+static inline unsigned get_class_value(RansReader& r, BinProb* ctx, int nctx) {
+    int maxc = nctx - 1, cls = 0;
+    while (cls < maxc && r.get(ctx[cls])) cls++;
+    if (cls <= 1) return (unsigned)cls;
+    unsigned off = 0;
+    for (int k = 0; k < cls - 1; k++) off = (off << 1) | (unsigned)r.get_bypass();
+    return (1u << (cls - 1)) + off;
+}
+
+static bool decode_plane(RansReader& r, DctContexts& c, int16_t* blk, int n, bool luma, int pi, bool dcp) {
+    const unsigned end = luma ? get_class_value(r, c.eob_y, 9) : get_class_value(r, c.eob_c, 7);
+    if ((int)end >= n) return false;
+    BinProb* sig = luma ? c.sig_y : c.sig_c;
+    for (unsigned i = 0; i <= end; i++) {
+        if (!r.get(sig[i])) continue;
+        const bool neg = r.get_bypass();
+        BinProb* mc = luma ? c.mag_y[luma_band((int)i)] : c.mag_c[chroma_band((int)i)];
+        const int16_t a = (int16_t)(get_class_value(r, mc, 13) + 1);
+        blk[i] = neg ? (int16_t)-a : a;
+    }
+    if (dcp) {
+        blk[0] = (int16_t)(blk[0] + c.prev_dc[pi]);
+        c.prev_dc[pi] = blk[0];
+    }
+    return true;
+}
+
+bool decode_residual_frame(const uint8_t* data, size_t len, const uint8_t* coded, int nmb, bool intra,
+                           int16_t* coeffs) {
+    memset(coeffs, 0, (size_t)nmb * 384 * sizeof(int16_t));
+    if (len == 0) return true;  // no coded MB: the encoder wrote nothing
+    RansReader r(data, len);
+    DctContexts* c = new DctContexts();
+    bool ok = true;
+    for (int b = 0; b < nmb && ok; b++) {
+        if (!coded[b]) continue;
+        int16_t* p = coeffs + (size_t)b * 384;
+        ok = decode_plane(r, *c, p, 256, true, 0, intra) && decode_plane(r, *c, p + 256, 64, false, 1, intra) &&
+             decode_plane(r, *c, p + 320, 64, false, 2, intra);
+    }
+    delete c;
+    return ok && !r.error;
 }
 
 // ---------------------------------------------------------------------------------
@@ -295,6 +393,101 @@ void MvCoder::encode_frame(const std::vector<MvCodedBlock>& blocks, int bw, std:
     }
     w.finish();
     update(blocks);
+}
+
+static int dec_class(RansReader& r, BinProb* ctx) {
+    int lo = 0, hi = 10, d = 0;
+    while (lo < hi) {
+        const int mid = (lo + hi) / 2;
+        if (r.get(ctx[d])) lo = mid + 1;
+        else hi = mid;
+        d++;
+    }
+    return lo;
+}
+static int8_t dec_comp(RansReader& r, BinProb* cls, BinProb& sign, BinProb* mag) {
+    const int c = dec_class(r, cls);
+    if (c == 0) return 0;
+    const bool neg = r.get(sign);
+    const unsigned bits = c <= 1 ? 0 : c - 1;
+    unsigned off = 0;
+    for (unsigned b = 0; b < bits; b++)
+        if (r.get(mag[b])) off |= 1u << b;
+    const int v = (int)((1u << (c - 1)) + off);
+    return (int8_t)std::min(std::max(neg ? -v : v, -128), 127);
+}
+
+bool MvCoder::decode_frame(const uint8_t* data, size_t len, int bw, int bh, std::vector<MvCodedBlock>& out) {
+    RansReader r(data, len);
+    const int n = bw * bh;
+    out.assign(n, MvCodedBlock{});
+    std::vector<uint8_t> modes(n), hits(n);
+    for (int i = 0; i < n; i++) {
+        const int bx = i % bw, by = i / bw;
+        MvCodedBlock& b = out[i];
+        b.skip = r.get(skip_);
+        int score = 0;
+        auto sc = [](int m) { return m == M_ZERO ? 2 : (m == M_NEW ? 0 : 1); };
+        if (bx > 0) score += sc(modes[i - 1]);
+        if (by > 0) score += sc(modes[i - bw]);
+        const int ctx = std::min(score, 3);
+        int mode;
+        if (r.get(m_new_[ctx])) mode = M_NEW;
+        else if (!r.get(m_nz_[ctx])) mode = M_ZERO;
+        else if (r.get(m_near_[ctx])) mode = M_NEAR;
+        else if (r.get(m_tmp_[ctx])) mode = M_TEMPORAL;
+        else if (r.get(m_tr_[ctx])) mode = M_TOPRIGHT;
+        else if (r.get(m_tl_[ctx])) mode = M_TOPLEFT;
+        else mode = M_NEAREST;
+        b.mode = (uint8_t)mode;
+        b.new_base = 0;
+        b.dx = b.dy = 0;
+        b.spx = b.spy = SP_ZERO;
+        hits[i] = 0;
+        if (mode == M_NEW) {
+            if (r.get(b_nearest_[ctx])) b.new_base = 0;
+            else if (r.get(b_near_[ctx])) b.new_base = 1;
+            else if (r.get(b_tr_[ctx])) b.new_base = 2;
+            else b.new_base = r.get(b_tl_[ctx]) ? 3 : 4;
+            bool via = false;
+            if (!cands_.empty()) {
+                const int lh = bx > 0 ? hits[i - 1] : 0, th = by > 0 ? hits[i - bw] : 0;
+                const bool hit = r.get(hit_[lh + th]);
+                if (hit) {
+                    int lo = 0, hi = 16, d = 0;
+                    while (hi - lo > 1) {
+                        const int mid = (lo + hi) / 2;
+                        if (r.get(cidx_[d])) lo = mid;
+                        else hi = mid;
+                        d++;
+                    }
+                    if (lo < (int)cands_.size()) {  // unpack cand_key
+                        const uint32_t k = cands_[lo];
+                        b.dx = (int8_t)(uint8_t)((k >> 24) ^ 0x80);
+                        b.dy = (int8_t)(uint8_t)(((k >> 16) & 0xff) ^ 0x80);
+                        b.spx = (uint8_t)((k >> 8) & 0xff);
+                        b.spy = (uint8_t)(k & 0xff);
+                        via = true;
+                    }
+                } else {
+                    b.dx = dec_comp(r, cls_x_, sign_x_, mag_x_);
+                    b.dy = dec_comp(r, cls_y_, sign_y_, mag_y_);
+                }
+                hits[i] = hit ? 1 : 0;
+            } else {
+                b.dx = dec_comp(r, cls_x_, sign_x_, mag_x_);
+                b.dy = dec_comp(r, cls_y_, sign_y_, mag_y_);
+            }
+            if (!via) {
+                b.spx = r.get(sub_x_) ? SP_PLUS : SP_ZERO;
+                b.spy = r.get(sub_y_) ? SP_PLUS : SP_ZERO;
+            }
+        }
+        modes[i] = (uint8_t)mode;
+    }
+    if (r.error) return false;
+    update(out);
+    return true;
 }
 
 void MvCoder::update(const std::vector<MvCodedBlock>& blocks) {  // encoder.rs:370-412

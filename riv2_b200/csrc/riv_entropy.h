@@ -33,6 +33,31 @@ private:
     int sp_;
 };
 
+// Binary rANS reader (com/rans.rs:299-354): the inverse of RansWriter.  Reads past the end
+// of the data set `error` and yield zeros.
+class RansReader {
+public:
+    RansReader(const uint8_t* data, size_t len);
+    bool get(BinProb& ctx);
+    bool get_bypass();
+    bool error = false;
+
+private:
+    uint16_t word();
+    void next_symbol();
+    void advance(uint32_t& r, uint32_t start, uint32_t freq);
+    const uint8_t* d_;
+    size_t len_, pos_ = 0;
+    uint32_t r0_ = 0, r1_ = 0;
+    int count_ = 0;
+};
+
+// Inverse of encode_residual_frame for a dense layout: coeffs holds 384 int16 per MB (Y, U,
+// V), zero-filled; MBs with coded[mb] == 0 are not in the stream (res/rans.rs:392-459).
+// Returns false on malformed data.
+bool decode_residual_frame(const uint8_t* data, size_t len, const uint8_t* coded, int nmb, bool intra,
+                           int16_t* coeffs);
+
 // Coded MBs in the GPU's compact layout: per MB, the Y, U and V blocks each truncated
 // after its last non-zero coefficient (eobs = those three indices per MB).
 void encode_residual_frame(const int16_t* packed, const uint8_t* eobs, int nblocks, bool intra,
@@ -52,6 +77,9 @@ class MvCoder {  // res/mv_rans/encoder.rs:60-412
 public:
     void reset();
     void encode_frame(const std::vector<MvCodedBlock>& blocks, int bw, std::vector<uint8_t>& out);
+    // res/mv_rans/decoder.rs:149-283; the same context and candidate-history state as the
+    // encoder, so a decoder instance follows the encoder's across frames.  false on bad data.
+    bool decode_frame(const uint8_t* data, size_t len, int bw, int bh, std::vector<MvCodedBlock>& out);
 
 private:
     void update(const std::vector<MvCodedBlock>& blocks);

@@ -1323,3 +1323,298 @@ riv_status riv_libm_fixup_counts(uint32_t* nlog, uint32_t* nexp) {
 void riv_dct_tables(int32_t* t16, int32_t* t8) { dct_tables(t16, t8); }
 
 }  // extern "C"
+
+// =====================================================================================
+// Decoder (dec/decoder.rs:112-460) up to the YUV reconstruction: host entropy decoding and
+// MV reconstruction, GPU prediction, AQ, inverse transforms and deblock.
+// =====================================================================================
+namespace {
+struct DecMv {
+    int8_t dx = 0, dy = 0, sx = 0, sy = 0;
+    bool operator==(const DecMv& o) const { return dx == o.dx && dy == o.dy && sx == o.sx && sy == o.sy; }
+};
+static int8_t sat8i(int v) { return (int8_t)std::min(std::max(v, -128), 127); }
+static uint64_t get_le(const uint8_t* b, int n) {
+    uint64_t v = 0;
+    for (int i = n - 1; i >= 0; i--) v = (v << 8) | b[i];
+    return v;
+}
+}  // namespace
+
+struct riv_decoder {
+    std::vector<uint8_t> data;
+    size_t pos = 36;
+    uint32_t dw = 0, dh = 0, sw = 0, sh = 0, fps = 0;
+    uint64_t frame_count = 0, current = 0;
+    int W = 0, H = 0, BW = 0, BH = 0, N = 0;
+    int device = 0;
+    std::string err;
+    bool poisoned = false, has_ref = false, has_prev_mvs = false;
+    int ref_cur = 0;
+    cudaStream_t S = nullptr;
+    DevBuf ref[2], recon_pre, pred, coeffs, mbout, skip, fmask, varsum, lnv, qs, logfix, expfix, ytab, ctab;
+    HostBuf hcoeffs, hmbout, hskip, hfmask;
+    int nlog = 0, nexp = 0;
+    riv::MvCoder mvc;
+    std::vector<DecMv> prev_mvs, mvs;
+    std::vector<riv::MvCodedBlock> blocks;
+    std::vector<uint8_t> coded;
+};
+
+static riv_dec_status dec_fail(riv_decoder* d, riv_dec_status s, const std::string& m) {
+    d->err = m;
+    if (s == RIV_DEC_CUDA) d->poisoned = true;
+    return s;
+}
+
+extern "C" {
+
+riv_dec_status riv_decoder_new(const uint8_t* data, size_t len, int device, riv_decoder** out) {
+    if (!out) return RIV_DEC_INVALID_HEADER;
+    *out = nullptr;
+    if (!data || len < 36 || memcmp(data, "RIV\0", 4) != 0 || get_le(data + 4, 4) != 5) return RIV_DEC_INVALID_HEADER;
+    riv_decoder* d = new riv_decoder();
+    d->data.assign(data, data + len);
+    d->dw = (uint32_t)get_le(data + 8, 4);
+    d->dh = (uint32_t)get_le(data + 12, 4);
+    d->sw = (uint32_t)get_le(data + 16, 4);
+    d->sh = (uint32_t)get_le(data + 20, 4);
+    d->fps = (uint32_t)get_le(data + 24, 4);
+    d->frame_count = get_le(data + 28, 8);
+    if (d->sw == 0 || d->sh == 0 || d->sw % 16 || d->sh % 16 || d->dw > d->sw || d->dh > d->sh || d->sw > 16384 ||
+        d->sh > 16384) {
+        delete d;
+        return RIV_DEC_INVALID_HEADER;
+    }
+    d->W = (int)d->sw;
+    d->H = (int)d->sh;
+    d->BW = d->W / 16;
+    d->BH = d->H / 16;
+    d->N = d->BW * d->BH;
+    d->device = device;
+    LibmFix& F = libm_fix();
+    if (!F.ok) {
+        d->err = F.err;
+        riv_decoder_free(d);
+        return RIV_DEC_DECODING_FAILED;
+    }
+    try {
+        CK(cudaSetDevice(device));
+        CK(cudaStreamCreateWithFlags(&d->S, cudaStreamNonBlocking));
+        const size_t yuv = (size_t)d->W * d->H * 3 / 2, N = (size_t)d->N;
+        d->ref[0].alloc(yuv);
+        d->ref[1].alloc(yuv);
+        d->recon_pre.alloc(yuv);
+        d->pred.alloc(yuv);
+        d->coeffs.alloc(N * 384 * 2);
+        d->mbout.alloc(N * sizeof(MbOut));
+        d->skip.alloc(N);
+        d->fmask.alloc(N);
+        d->varsum.alloc(N * sizeof(uint2));
+        d->lnv.alloc((N + 4) * sizeof(float));
+        d->qs.alloc(N * sizeof(float));
+        d->ytab.alloc(256 * 2);
+        d->ctab.alloc(64 * 2);
+        d->hcoeffs.alloc(N * 384 * 2);
+        d->hmbout.alloc(N * sizeof(MbOut));
+        d->hskip.alloc(N);
+        d->hfmask.alloc(N);
+        d->nlog = (int)(F.logf.size() / 2);
+        d->nexp = (int)(F.exp2f.size() / 2);
+        d->logfix.alloc(F.logf_dev.size() * 4);
+        d->expfix.alloc(F.exp2f_dev.size() * 4);
+        CK(cudaMemcpy(d->logfix.p, F.logf_dev.data(), F.logf_dev.size() * 4, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d->expfix.p, F.exp2f_dev.data(), F.exp2f_dev.size() * 4, cudaMemcpyHostToDevice));
+        int32_t t16[256], t8[64];
+        dct_tables(t16, t8);
+        CK(riv_upload_dct_tables(t16, t8));
+    } catch (const CudaError& ce) {
+        d->err = std::string(ce.where) + ": " + cudaGetErrorString(ce.e);
+        riv_decoder_free(d);
+        return RIV_DEC_CUDA;
+    }
+    riv::entropy_init();
+    *out = d;
+    return RIV_DEC_OK;
+}
+
+riv_dec_status riv_decoder_info(const riv_decoder* d, uint32_t* dims5, uint64_t* frame_count) {
+    if (!d) return RIV_DEC_INVALID_HEADER;
+    if (dims5) {
+        dims5[0] = d->dw; dims5[1] = d->dh; dims5[2] = d->sw; dims5[3] = d->sh; dims5[4] = d->fps;
+    }
+    if (frame_count) *frame_count = d->frame_count;
+    return RIV_DEC_OK;
+}
+
+uint64_t riv_decoder_current_frame(const riv_decoder* d) { return d ? d->current : 0; }
+const char* riv_decoder_last_error(const riv_decoder* d) { return d ? d->err.c_str() : "null decoder"; }
+
+riv_dec_status riv_decode_frame_yuv(riv_decoder* d, uint8_t* y, uint8_t* u, uint8_t* v, uint32_t* frame_type,
+                                    uint64_t* timestamp_ms) {
+    if (!d) return RIV_DEC_INVALID_HEADER;
+    if (d->poisoned) return dec_fail(d, RIV_DEC_CUDA, "decoder unusable after a device failure");
+    if (d->current >= d->frame_count) return dec_fail(d, RIV_DEC_END_OF_STREAM, "end of stream");
+    const uint8_t* b = d->data.data() + d->pos;
+    const size_t left = d->data.size() - d->pos;
+    if (left < 9) return dec_fail(d, RIV_DEC_IO, "truncated record");
+    const uint64_t ts = get_le(b, 8);
+    const int type = b[8];
+    const int W = d->W, H = d->H, N = d->N;
+    const size_t ysz = (size_t)W * H, csz = ysz / 4;
+    const int nxt = d->ref_cur ^ 1;
+    uint8_t* recon = d->ref[nxt].as<uint8_t>();
+    try {
+        CK(cudaSetDevice(d->device));
+        cudaStream_t S = d->S;
+        if (type == 1) {  // intra (residual.rs:815-887)
+            if (left < 14) return dec_fail(d, RIV_DEC_IO, "truncated intra record");
+            const uint8_t q = b[9];
+            const size_t sz = get_le(b + 10, 4);
+            if (left < 14 + sz) return dec_fail(d, RIV_DEC_IO, "truncated intra payload");
+            d->coded.assign(N, 1);
+            // the previous frame's copies out of the pinned staging are complete (the last
+            // call synchronised)
+            if (!riv::decode_residual_frame(b + 14, sz, d->coded.data(), N, true, d->hcoeffs.as<int16_t>()))
+                return dec_fail(d, RIV_DEC_INVALID_FRAME, "malformed intra coefficient data");
+            uint16_t yt[256], ct[64];
+            intra_tables(quant_step(q), yt, ct);
+            CK(cudaMemcpyAsync(d->ytab.p, yt, sizeof yt, cudaMemcpyHostToDevice, S));
+            CK(cudaMemcpyAsync(d->ctab.p, ct, sizeof ct, cudaMemcpyHostToDevice, S));
+            CK(cudaMemcpyAsync(d->coeffs.p, d->hcoeffs.p, (size_t)N * 768, cudaMemcpyHostToDevice, S));
+            const int level = deblock_level(quant_step(q));
+            uint8_t* target = level > 0 ? d->recon_pre.as<uint8_t>() : recon;
+            CK(launch_reconstruct(d->coeffs.as<int16_t>(), nullptr, nullptr, nullptr, 1, d->ytab.as<uint16_t>(),
+                                  d->ctab.as<uint16_t>(), target, W, H, S));
+            if (level > 0) {
+                int E, I, Hv;
+                deblock_thresholds(level, true, E, I, Hv);
+                CK(launch_deblock_tiled(target, recon, W, H, E, I, Hv, nullptr, S));
+            }
+            d->pos += 14 + sz;
+            d->has_prev_mvs = false;
+            d->prev_mvs.clear();
+            d->mvc.reset();
+        } else if (type == 2) {  // inter (residual.rs:889-1079, decoder.rs:255-430)
+            if (left < 17 || !d->has_ref) return dec_fail(d, RIV_DEC_INVALID_FRAME, "inter frame without a reference");
+            const uint8_t q = b[9];
+            const int biasx = (int8_t)b[10], biasy = (int8_t)b[11];
+            const size_t mvs = get_le(b + 13, 4);
+            if (left < 17 + mvs + 4) return dec_fail(d, RIV_DEC_IO, "truncated motion data");
+            const uint8_t* mvd = b + 17;
+            const size_t rs = get_le(b + 17 + mvs, 4);
+            if (left < 21 + mvs + rs) return dec_fail(d, RIV_DEC_IO, "truncated residual data");
+            const uint8_t* rd = b + 21 + mvs;
+            if (!d->mvc.decode_frame(mvd, mvs, d->BW, d->BH, d->blocks))
+                return dec_fail(d, RIV_DEC_INVALID_FRAME, "malformed motion data");
+            // MV reconstruction in raster order from the decoded neighbours (mv_predictor.rs)
+            const int BW = d->BW;
+            d->mvs.assign(N, DecMv{});
+            d->coded.assign(N, 0);
+            MbOut* mo = d->hmbout.as<MbOut>();
+            uint8_t* hs = d->hskip.as<uint8_t>();
+            uint8_t* hf = d->hfmask.as<uint8_t>();
+            const bool tm = d->has_prev_mvs;
+            for (int i = 0; i < N; i++) {
+                const riv::MvCodedBlock& cb = d->blocks[i];
+                const int bx = i % BW, by = i / BW;
+                const bool hl = bx > 0, ht = by > 0, htr = by > 0 && bx + 1 < BW, htl = by > 0 && bx > 0;
+                const DecMv L = hl ? d->mvs[i - 1] : DecMv{}, T = ht ? d->mvs[i - BW] : DecMv{};
+                const DecMv TR = htr ? d->mvs[i - BW + 1] : DecMv{}, TL = htl ? d->mvs[i - BW - 1] : DecMv{};
+                const DecMv TM = tm ? d->prev_mvs[i] : DecMv{};
+                DecMv cand[5];
+                int nc = 0;
+                auto add = [&](bool has, const DecMv& m) {
+                    if (!has) return;
+                    for (int k = 0; k < nc; k++)
+                        if (cand[k] == m) return;
+                    cand[nc++] = m;
+                };
+                add(hl, L); add(ht, T); add(htr, TR); add(htl, TL); add(tm, TM);
+                const DecMv nearest = nc > 0 ? cand[0] : DecMv{}, nearm = nc > 1 ? cand[1] : DecMv{};
+                const DecMv temporal = tm ? TM : DecMv{};
+                DecMv base{};
+                switch (cb.mode) {
+                    case riv::M_ZERO: break;
+                    case riv::M_NEAREST: base = nearest; break;
+                    case riv::M_NEAR: base = nearm; break;
+                    case riv::M_TOPRIGHT: base = htr ? TR : nearest; break;
+                    case riv::M_TOPLEFT: base = htl ? TL : nearest; break;
+                    case riv::M_TEMPORAL: base = temporal; break;
+                    default:
+                        base = cb.new_base == 0 ? nearest : cb.new_base == 1 ? nearm
+                               : cb.new_base == 2 ? (htr ? TR : nearest)
+                               : cb.new_base == 3 ? (htl ? TL : nearest) : cb.new_base == 4 ? temporal : nearest;
+                }
+                DecMv m;
+                if (cb.mode == riv::M_NEW) {
+                    m.dx = sat8i(base.dx + sat8i(cb.dx + biasx));
+                    m.dy = sat8i(base.dy + sat8i(cb.dy + biasy));
+                    m.sx = cb.spx == riv::SP_PLUS ? 1 : (cb.spx == riv::SP_MINUS ? -1 : 0);
+                    m.sy = cb.spy == riv::SP_PLUS ? 1 : (cb.spy == riv::SP_MINUS ? -1 : 0);
+                } else {
+                    m = base;
+                }
+                d->mvs[i] = m;
+                MbOut o{};
+                o.raw[0] = m.dx; o.raw[1] = m.dy; o.raw[2] = m.sx; o.raw[3] = m.sy;
+                mo[i] = o;
+                hs[i] = cb.skip ? 1 : 0;
+                hf[i] = (!cb.skip || m.dx || m.dy || m.sx || m.sy) ? 1 : 0;
+                d->coded[i] = cb.skip ? 0 : 1;
+            }
+            if (!riv::decode_residual_frame(rd, rs, d->coded.data(), N, false, d->hcoeffs.as<int16_t>()))
+                return dec_fail(d, RIV_DEC_INVALID_FRAME, "malformed residual data");
+            CK(cudaMemcpyAsync(d->mbout.p, mo, (size_t)N * sizeof(MbOut), cudaMemcpyHostToDevice, S));
+            CK(cudaMemcpyAsync(d->skip.p, hs, N, cudaMemcpyHostToDevice, S));
+            CK(cudaMemcpyAsync(d->fmask.p, hf, N, cudaMemcpyHostToDevice, S));
+            CK(cudaMemcpyAsync(d->coeffs.p, d->hcoeffs.p, (size_t)N * 768, cudaMemcpyHostToDevice, S));
+            const uint8_t* ref = d->ref[d->ref_cur].as<uint8_t>();
+            CK(launch_predict(ref, d->mbout.as<MbOut>(), d->pred.as<uint8_t>(), d->varsum.as<uint2>(), W, H, S));
+            CK(launch_aq(d->varsum.as<uint2>(), N, quant_step(q), d->logfix.as<uint32_t>(), d->nlog,
+                         d->expfix.as<uint32_t>(), d->nexp, d->lnv.as<float>(), d->qs.as<float>(), S));
+            const int level = deblock_level(quant_step(q));
+            uint8_t* target = level > 0 ? d->recon_pre.as<uint8_t>() : recon;
+            CK(launch_reconstruct(d->coeffs.as<int16_t>(), d->pred.as<uint8_t>(), d->skip.as<uint8_t>(),
+                                  d->qs.as<float>(), 0, nullptr, nullptr, target, W, H, S));
+            if (level > 0) {
+                int E, I, Hv;
+                deblock_thresholds(level, false, E, I, Hv);
+                CK(launch_deblock_tiled(target, recon, W, H, E, I, Hv, d->fmask.as<uint8_t>(), S));
+            }
+            d->pos += 21 + mvs + rs;
+            d->prev_mvs.swap(d->mvs);
+            d->has_prev_mvs = true;
+        } else {
+            return dec_fail(d, RIV_DEC_INVALID_FRAME, "unknown frame type");
+        }
+        if (y) CK(cudaMemcpyAsync(y, recon, ysz, cudaMemcpyDeviceToHost, S));
+        if (u) CK(cudaMemcpyAsync(u, recon + ysz, csz, cudaMemcpyDeviceToHost, S));
+        if (v) CK(cudaMemcpyAsync(v, recon + ysz + csz, csz, cudaMemcpyDeviceToHost, S));
+        // the pinned staging buffers are rewritten by the next call: finish this frame
+        CK(cudaStreamSynchronize(S));
+    } catch (const CudaError& ce) {
+        return dec_fail(d, RIV_DEC_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
+    }
+    d->ref_cur = nxt;
+    d->has_ref = true;
+    if (frame_type) *frame_type = (uint32_t)type;
+    if (timestamp_ms) *timestamp_ms = ts;
+    d->current++;
+    return RIV_DEC_OK;
+}
+
+void riv_decoder_free(riv_decoder* d) {
+    if (!d) return;
+    cudaSetDevice(d->device);
+    if (d->S) cudaStreamSynchronize(d->S);
+    DevBuf* bufs[] = {&d->ref[0], &d->ref[1], &d->recon_pre, &d->pred, &d->coeffs, &d->mbout, &d->skip, &d->fmask,
+                      &d->varsum, &d->lnv, &d->qs, &d->logfix, &d->expfix, &d->ytab, &d->ctab};
+    for (DevBuf* x : bufs) x->release();
+    HostBuf* hb[] = {&d->hcoeffs, &d->hmbout, &d->hskip, &d->hfmask};
+    for (HostBuf* x : hb) x->release();
+    if (d->S) cudaStreamDestroy(d->S);
+    delete d;
+}
+
+}  // extern "C"

@@ -116,6 +116,10 @@ int launch_predict(const uint8_t* ref, const MbOut* mb, uint8_t* pred, uint2* va
 int launch_aq(const uint2* varsum, int n, float base, const uint32_t* logfix, int nlog, const uint32_t* expfix,
               int nexp, float* lnv_scratch, float* qs, void* stream);
 int launch_residual(const ResidualParams& p, int nmb, void* stream);
+// Decoder: dequantise + inverse-transform dense coefficients onto the prediction (inter) or
+// 128 (intra); skip[mb] != 0 copies the prediction (inter).
+int launch_reconstruct(const int16_t* coeffs, const uint8_t* pred, const uint8_t* skip, const float* qs, int intra,
+                       const uint16_t* ytab, const uint16_t* ctab, uint8_t* recon, int W, int H, void* stream);
 int launch_deblock(uint8_t* yuv, int W, int H, int E, int I, int Hev, const uint8_t* mask, void* stream);
 // Out-of-place deblock of all three planes in one launch (src != dst, no overlap).
 int launch_deblock_tiled(const uint8_t* src, uint8_t* dst, int W, int H, int E, int I, int Hev, const uint8_t* mask,

@@ -1848,8 +1848,101 @@ __device__ __forceinline__ void aan_1d(const int32_t s[8], int32_t out[8], int32
 // columns 4 * (u & 3) .. +3 in every 16x16 pass, and two adjacent chroma samples (plane
 // u >> 5).  Each pass reads one basis row and one data row per term as 128-bit shared loads,
 // four multiply-accumulates per pair of loads.  Per-MB named barriers (ids 1..4, 64 threads).
-constexpr int RS_MB = 4;
 __device__ __forceinline__ void mb_sync(int g) { asm volatile("bar.sync %0, 64;" ::"r"(g + 1) : "memory"); }
+// Dequantisation and inverse transforms of one MB and its reconstruction onto the prediction
+// (dct/dct16.rs:345-412, dct/fast_dct8.rs:69-174, res/residual.rs:740-752), shared by the
+// encoder's residual kernel and the decoder.  64 threads per MB (group g, thread u: luma row
+// yy, columns xb..xb+3; own quantised luma ql); Qc = the MB's 128 chroma coefficients and
+// predc its chroma prediction in shared memory; R, RT, aant = per-MB shared scratch.
+__device__ __forceinline__ void inverse_mb(int g, int u, int yy, int xb, const int16_t (&ql)[4], float qsv, bool intra,
+                                           const uint16_t* ytab, const uint16_t* ctab, uint32_t lbase, uint8_t* ry,
+                                           uint8_t* rU, uint8_t* rV, int CW, int x0, int y0, const int32_t* sT16,
+                                           const int32_t* sT16t, int32_t* R, int32_t* RT, int32_t* aant,
+                                           const int16_t* Qc, const uint8_t* predc) {
+    // dequantisation + 16x16 inverse (row pass over u, then column pass over v)
+    {
+        int32_t d[4];
+        if (intra) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) d[k] = (int32_t)ql[k] * max((int)ytab[yy * 16 + xb + k], 1);
+        } else {
+            const int32_t qfp = f32_to_i32_sat(roundf(__fmul_rn(qsv, 16384.0f)));
+#pragma unroll
+            for (int k = 0; k < 4; k++) d[k] = wadd(wmul((int32_t)ql[k], qfp), 8192) >> 14;
+        }
+        *(int4*)(R + yy * 16 + xb) = make_int4(d[0], d[1], d[2], d[3]);
+    }
+    mb_sync(g);
+    {  // rows[v][x] = (sum_i deq[v][i] * T[x][i] + 2^17) >> 18, wrapping   (v = yy)
+        uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const uint32_t r = (uint32_t)R[yy * 16 + i];
+            const int4 t = *(const int4*)(sT16t + i * 16 + xb);
+            a0 += r * (uint32_t)t.x; a1 += r * (uint32_t)t.y; a2 += r * (uint32_t)t.z; a3 += r * (uint32_t)t.w;
+        }
+        *(int4*)(RT + yy * 16 + xb) = make_int4((int32_t)(a0 + (1u << 17)) >> 18, (int32_t)(a1 + (1u << 17)) >> 18,
+                                                (int32_t)(a2 + (1u << 17)) >> 18, (int32_t)(a3 + (1u << 17)) >> 18);
+    }
+    mb_sync(g);
+    {  // out[y][x] = (sum_v rows[v][x] * T[y][v] + 2^17) >> 18   (y = yy)
+        uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll
+        for (int v = 0; v < 16; v++) {
+            const int4 r = *(const int4*)(RT + v * 16 + xb);
+            const uint32_t t = (uint32_t)sT16[yy * 16 + v];
+            a0 += (uint32_t)r.x * t; a1 += (uint32_t)r.y * t; a2 += (uint32_t)r.z * t; a3 += (uint32_t)r.w * t;
+        }
+        const uint32_t acc[4] = {a0, a1, a2, a3};
+        const uint32_t bv = lbase;
+        uint32_t o = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            int32_t r = (int32_t)(acc[k] + (1u << 17)) >> 18;
+            r = min(max(r, -32768), 32767);
+            const int base = (int)((bv >> (8 * k)) & 255u);
+            o |= (uint32_t)min(max(base + r, 0), 255) << (8 * k);
+        }
+        *(uint32_t*)ry = o;
+    }
+    // chroma 8x8 AAN inverse: pass 1 over u for each (plane, v); pass 2 over v for each (plane, x)
+    if (u < 16) {
+        const int cp = u >> 3, v = u & 7;
+        int32_t sv[8], o[8];
+        int32_t qa = 0;
+        if (!intra) {
+            float qr = roundf(qsv);
+            qr = qr < 1.0f ? 1.0f : qr;
+            qa = qr >= 65535.0f ? 65535 : (int32_t)qr;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const int32_t qq = intra ? max((int)ctab[v * 8 + k], 1) : qa;
+            sv[k] = (int32_t)Qc[cp * 64 + v * 8 + k] * qq;
+        }
+        aan_1d(sv, o, 512, 10);
+#pragma unroll
+        for (int x = 0; x < 8; x++) aant[cp * 64 + x * 8 + v] = o[x];
+    }
+    mb_sync(g);
+    if (u < 16) {
+        const int cp = u >> 3, x = u & 7;
+        int32_t sv[8], o[8];
+#pragma unroll
+        for (int v = 0; v < 8; v++) sv[v] = aant[cp * 64 + x * 8 + v];
+        aan_1d(sv, o, 65536, 17);
+        uint8_t* Rr = cp == 0 ? rU : rV;
+#pragma unroll
+        for (int y = 0; y < 8; y++) {
+            const int r = min(max(o[y], -32768), 32767);
+            const size_t i = (size_t)(y0 / 2 + y) * CW + x0 / 2 + x;
+            const int base = intra ? 128 : (int)predc[cp * 64 + y * 8 + x];
+            Rr[i] = (uint8_t)min(max(base + r, 0), 255);
+        }
+    }
+}
+
+constexpr int RS_MB = 4;
 
 __global__ void __launch_bounds__(256) k_residual(ResidualParams p, int nmb) {
     __shared__ __align__(16) int32_t sT16[256], sT16t[256], sT8[64];
@@ -2059,87 +2152,65 @@ __global__ void __launch_bounds__(256) k_residual(ResidualParams p, int nmb) {
             p.fmask[mb] = 1;
         }
     }
-    // dequantisation + 16x16 inverse (row pass over u, then column pass over v)
-    {
-        int32_t d[4];
-        if (p.intra) {
-#pragma unroll
-            for (int k = 0; k < 4; k++) d[k] = (int32_t)ql[k] * max((int)p.intra_ytab[yy * 16 + xb + k], 1);
-        } else {
-            const int32_t qfp = f32_to_i32_sat(roundf(__fmul_rn(qsv, 16384.0f)));
-#pragma unroll
-            for (int k = 0; k < 4; k++) d[k] = wadd(wmul((int32_t)ql[k], qfp), 8192) >> 14;
-        }
-        *(int4*)(R + yy * 16 + xb) = make_int4(d[0], d[1], d[2], d[3]);
+    const uint32_t lbase = p.intra ? 0x80808080u : *(const uint32_t*)(pY + yi);
+    inverse_mb(g, u, yy, xb, ql, qsv, p.intra != 0, p.intra_ytab, p.intra_ctab, lbase, rY + yi, rU, rV, CW, x0, y0,
+               sT16, sT16t, R, RT, aant[g][0], Q + 256, predc[g]);
+}
+
+// Decoder reconstruction (res/residual.rs:815-887 intra, :889-1079 inter): the decoded
+// coefficients (384 per MB, dense) dequantised, inverse-transformed and added to the
+// prediction (inter) or to 128 (intra); skipped inter MBs copy the prediction.  Same thread
+// layout and arithmetic as the encoder's reconstruction (inverse_mb).
+__global__ void __launch_bounds__(256) k_reconstruct(const int16_t* __restrict__ coeffs, const uint8_t* __restrict__ pred,
+                                                     const uint8_t* __restrict__ skip, const float* __restrict__ qs,
+                                                     int intra, const uint16_t* ytab, const uint16_t* ctab,
+                                                     uint8_t* __restrict__ recon, int W, int H, int BW, int nmb) {
+    __shared__ __align__(16) int32_t sT16[256], sT16t[256];
+    __shared__ __align__(16) int32_t res[RS_MB][256], rowt[RS_MB][256];
+    __shared__ __align__(16) int16_t qc[RS_MB][128];
+    __shared__ int32_t aant[RS_MB][2][64];
+    __shared__ uint8_t predc[RS_MB][128];
+    const int tid = threadIdx.x;
+    sT16[tid] = c_T16[tid];
+    sT16t[(tid & 15) * 16 + (tid >> 4)] = c_T16[tid];
+    __syncthreads();
+    const int g = tid >> 6, u = tid & 63;
+    const int mb = blockIdx.x * RS_MB + g;
+    if (mb >= nmb) return;
+    const int CW = W / 2, CH = H / 2;
+    const int bx = mb % BW, by = mb / BW, x0 = bx * 16, y0 = by * 16;
+    const int yy = u >> 2, xb = (u & 3) * 4;
+    const size_t yi = (size_t)(y0 + yy) * W + x0 + xb;
+    const int pl = u >> 5, ci = (u & 31) * 2, cyy = ci >> 3, cxx = ci & 7;
+    const size_t cidx = (size_t)(y0 / 2 + cyy) * CW + x0 / 2 + cxx;
+    const size_t coff = (size_t)W * H + (pl == 0 ? 0 : (size_t)CW * CH);
+    uint8_t *rY = recon, *rU = recon + (size_t)W * H, *rV = rU + (size_t)CW * CH;
+    if (!intra && skip[mb]) {
+        *(uint32_t*)(rY + yi) = *(const uint32_t*)(pred + yi);
+        *(uint16_t*)(recon + coff + cidx) = *(const uint16_t*)(pred + coff + cidx);
+        return;
     }
-    mb_sync(g);
-    {  // rows[v][x] = (sum_i deq[v][i] * T[x][i] + 2^17) >> 18, wrapping   (v = yy)
-        uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-#pragma unroll
-        for (int i = 0; i < 16; i++) {
-            const uint32_t r = (uint32_t)R[yy * 16 + i];
-            const int4 t = *(const int4*)(sT16t + i * 16 + xb);
-            a0 += r * (uint32_t)t.x; a1 += r * (uint32_t)t.y; a2 += r * (uint32_t)t.z; a3 += r * (uint32_t)t.w;
-        }
-        *(int4*)(RT + yy * 16 + xb) = make_int4((int32_t)(a0 + (1u << 17)) >> 18, (int32_t)(a1 + (1u << 17)) >> 18,
-                                                (int32_t)(a2 + (1u << 17)) >> 18, (int32_t)(a3 + (1u << 17)) >> 18);
-    }
-    mb_sync(g);
-    {  // out[y][x] = (sum_v rows[v][x] * T[y][v] + 2^17) >> 18   (y = yy)
-        uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-#pragma unroll
-        for (int v = 0; v < 16; v++) {
-            const int4 r = *(const int4*)(RT + v * 16 + xb);
-            const uint32_t t = (uint32_t)sT16[yy * 16 + v];
-            a0 += (uint32_t)r.x * t; a1 += (uint32_t)r.y * t; a2 += (uint32_t)r.z * t; a3 += (uint32_t)r.w * t;
-        }
-        const uint32_t acc[4] = {a0, a1, a2, a3};
-        const uint32_t bv = p.intra ? 0x80808080u : *(const uint32_t*)(pY + yi);
-        uint32_t o = 0;
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            int32_t r = (int32_t)(acc[k] + (1u << 17)) >> 18;
-            r = min(max(r, -32768), 32767);
-            const int base = (int)((bv >> (8 * k)) & 255u);
-            o |= (uint32_t)min(max(base + r, 0), 255) << (8 * k);
-        }
-        *(uint32_t*)(rY + yi) = o;
-    }
-    // chroma 8x8 AAN inverse: pass 1 over u for each (plane, v); pass 2 over v for each (plane, x)
-    if (u < 16) {
-        const int cp = u >> 3, v = u & 7;
-        int32_t sv[8], o[8];
-        int32_t qa = 0;
-        if (!p.intra) {
-            float qr = roundf(qsv);
-            qr = qr < 1.0f ? 1.0f : qr;
-            qa = qr >= 65535.0f ? 65535 : (int32_t)qr;
-        }
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            const int32_t qq = p.intra ? max((int)p.intra_ctab[v * 8 + k], 1) : qa;
-            sv[k] = (int32_t)Q[256 + cp * 64 + v * 8 + k] * qq;
-        }
-        aan_1d(sv, o, 512, 10);
-#pragma unroll
-        for (int x = 0; x < 8; x++) aant[g][cp][x * 8 + v] = o[x];
-    }
-    mb_sync(g);
-    if (u < 16) {
-        const int cp = u >> 3, x = u & 7;
-        int32_t sv[8], o[8];
-#pragma unroll
-        for (int v = 0; v < 8; v++) sv[v] = aant[g][cp][x * 8 + v];
-        aan_1d(sv, o, 65536, 17);
-        uint8_t* Rr = cp == 0 ? rU : rV;
-#pragma unroll
-        for (int y = 0; y < 8; y++) {
-            const int r = min(max(o[y], -32768), 32767);
-            const size_t i = (size_t)(y0 / 2 + y) * CW + x0 / 2 + x;
-            const int base = p.intra ? 128 : (int)predc[g][cp * 64 + y * 8 + x];
-            Rr[i] = (uint8_t)min(max(base + r, 0), 255);
-        }
-    }
+    const int16_t* co = coeffs + (size_t)mb * 384;
+    const uint2 lw = *(const uint2*)(co + yy * 16 + xb);
+    const int16_t ql[4] = {(int16_t)(lw.x & 0xffff), (int16_t)(lw.x >> 16), (int16_t)(lw.y & 0xffff), (int16_t)(lw.y >> 16)};
+    const uint32_t cw = *(const uint32_t*)(co + 256 + pl * 64 + ci);
+    qc[g][pl * 64 + ci] = (int16_t)(cw & 0xffff);
+    qc[g][pl * 64 + ci + 1] = (int16_t)(cw >> 16);
+    const uint32_t pcw = intra ? 0x8080u : *(const uint16_t*)(pred + coff + cidx);
+    predc[g][pl * 64 + ci] = (uint8_t)pcw;
+    predc[g][pl * 64 + ci + 1] = (uint8_t)(pcw >> 8);
+    const uint32_t lbase = intra ? 0x80808080u : *(const uint32_t*)(pred + yi);
+    const float qsv = intra ? 0.0f : qs[mb];
+    inverse_mb(g, u, yy, xb, ql, qsv, intra != 0, ytab, ctab, lbase, rY + yi, rU, rV, CW, x0, y0, sT16, sT16t, res[g],
+               rowt[g], aant[g][0], qc[g], predc[g]);
+}
+
+int launch_reconstruct(const int16_t* coeffs, const uint8_t* pred, const uint8_t* skip, const float* qs, int intra,
+                       const uint16_t* ytab, const uint16_t* ctab, uint8_t* recon, int W, int H, void* stream) {
+    const int BW = W / 16, n = BW * (H / 16);
+    k_reconstruct<<<(n + RS_MB - 1) / RS_MB, 64 * RS_MB, 0, (cudaStream_t)stream>>>(coeffs, pred, skip, qs, intra, ytab,
+                                                                                   ctab, recon, W, H, BW, n);
+    return (int)cudaGetLastError();
 }
 
 int launch_residual(const ResidualParams& p, int nmb, void* stream) {
