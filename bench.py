@@ -220,10 +220,34 @@ def run_ours(args, frames_host, dev_index, dist):
         return ms, c0, c1, clk, data
 
     ms_v, c0v, c1v, clk_v, data_v = session(True)
+    dec = decode_rate(data_v, dev_index)
     ms_e, c0e, c1e, clk_e, data_e = session(False)
     del frames_dev
     return {"ms_value": ms_v, "ms_e2e": ms_e, "c0": c0v, "c1": c1v, "c0e": c0e, "c1e": c1e, "clocks": clk_v,
-            "clocks_e2e": clk_e, "stream_bytes": len(data_v), "streams_equal": data_v == data_e}
+            "clocks_e2e": clk_e, "stream_bytes": len(data_v), "streams_equal": data_v == data_e, "decode": dec}
+
+
+def decode_rate(stream: bytes, dev_index: int):
+    """GPU decoder (riv_decode_frame_yuv) over the stream just encoded: host entropy decoding
+    and MV reconstruction, GPU reconstruction, no copy-out; whole-call wall time with CUDA
+    events around it."""
+    import torch
+
+    from riv2_b200.decoder import Decoder
+    dec = Decoder.new(stream, dev_index)
+    n = dec.header().frame_count
+    dec.decode_frame(copy_out=False)  # the key frame, untimed
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(n - 1):
+        dec.decode_frame(copy_out=False)
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    dec.close()
+    return {"value": (n - 1) / (ms / 1000.0), "unit": "frames/s", "frames": n - 1,
+            "what": "P-frames of the bench stream through the GPU decoder (YUV reconstruction, no copy-out)"}
 
 
 def cpu_baseline(frames_host, nframes, iq, pq):
@@ -343,6 +367,7 @@ def main():
         "cpu_baseline": cpu,
         "clocks": r["clocks"], "clocks_e2e": r["clocks_e2e"],
         "stream_bytes": r["stream_bytes"], "streams_equal_value_vs_e2e": r["streams_equal"],
+        "decode": r["decode"],
     }
     print(json.dumps(line))
     if dist is not None:
