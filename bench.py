@@ -329,8 +329,10 @@ def main():
     ms_e = max_over_ranks(r["ms_e2e"], dist, torch.device("cuda", dev_index))
     c0, c1 = r["c0"], r["c1"]
     pf = c1["pframes"] - c0["pframes"]
-    stage = [(b - a) / max(pf, 1) for a, b in zip(c0["stage_us_sum"], c1["stage_us_sum"])]
+    ptimed = c1["timed_pframes"] - c0["timed_pframes"]  # stage timing events ride on sampled frames
+    stage = [(b - a) / max(ptimed, 1) for a, b in zip(c0["stage_us_sum"], c1["stage_us_sum"])]
     launches = c1["launches"] - c0["launches"]
+    deferred = (c1["deferred_pframes"] - c0["deferred_pframes"]) / max(pf, 1)
     h2d = (r["c1e"]["h2d_bytes"] - r["c0e"]["h2d_bytes"]) / K
     d2h = (r["c1e"]["d2h_bytes"] - r["c0e"]["d2h_bytes"]) / K
     if rank != 0:
@@ -360,6 +362,7 @@ def main():
         "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
         "gpu_stage_us_per_pframe": dict(zip(names, [round(x, 2) for x in stage])),
+        "pframes_reconstructed_in_next_launch": round(deferred, 3),
         "gpu_pipeline_fps": 1e6 / stage[8] if stage[8] > 0 else None,
         "host_ms_per_frame": dict(zip(["submit", "retire", "mv_coding", "dct_coding_sum", "write", "blocked"],
                                       [round((b - a) / K, 3) for a, b in zip(c0["host_ms"], c1["host_ms"])])),

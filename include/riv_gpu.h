@@ -106,15 +106,20 @@ uint64_t riv_frame_count(const riv_encoder* enc);
 /* Reconstruction (deblocked reference) of the last frame whose GPU work finished;
  * storage-size planes.  Synchronises the device. */
 riv_status riv_last_recon(riv_encoder* enc, uint8_t* y, uint8_t* u, uint8_t* v);
-/* Per-frame GPU timing of the last completed frame, microseconds: [0] rgb->yuv
+/* Per-frame GPU timing of the last completed frame that carried stage timing events (every
+ * frame at pipeline_depth 0 or with per-frame stats, else one in 8), microseconds: [0] rgb->yuv
  * [1] integer-SAD table [2] search/mode wavefront [3] predict [4] aq [5] residual
  * [6] deblock [7] compact [8] total */
 riv_status riv_last_kernel_times(riv_encoder* enc, float* us9);
 
 /* Cumulative counters since riv_encoder_new: us9 = per-stage GPU time summed over all
  * P-frames (same stage order as riv_last_kernel_times), io2 = {host->device bytes,
- * device->host bytes}, n2 = {P-frames, kernel launches}. */
-riv_status riv_counters(riv_encoder* enc, double* us9, uint64_t* io2, uint64_t* n2);
+ * device->host bytes}, n4 = {P-frames, kernel launches, P-frames whose residual and deblock
+ * ran inside the next P-frame's search launch, P-frames with stage timings}.  With
+ * pipeline_depth > 0 only one frame in 8 carries stage timing events (timing-enabled
+ * events between back-to-back search launches idle the GPU for microseconds each), so us9
+ * sums over the timed P-frames: divide by n4[3]. */
+riv_status riv_counters(riv_encoder* enc, double* us9, uint64_t* io2, uint64_t* n4);
 /* Cumulative host-side milliseconds: [0] GPU submission, [1] retiring finished frames,
  * [2] motion-vector coding, [3] DCT-coefficient coding (summed over worker threads),
  * [4] record writes, [5] waiting for a frame's entropy coding to finish. */
@@ -162,8 +167,10 @@ riv_status riv_stage_libm(int which, const float* in, float* out, size_t n);
 /* Test hook: device state left by the most recent frame (synchronises the device; meant
  * for pipeline_depth == 0).  what: 0 per-MB search/mode output (20 B/MB), 1 AQ steps
  * (f32/MB), 2 prediction (YUV), 3 converted input (YUV), 4 quantised coefficients
- * (384 x i16 per MB), 5 optimized skip (u8/MB), 6 search-kernel phase stamps (16 x i64 per
- * MB; only when the encoder was created with RIV_PROFILE_SEARCH set in the environment).
+ * (384 x i16 per MB), 5 optimized skip (u8/MB), 6 search-kernel phase stamps (32 x i64 per
+ * MB: words 0-15 SM clock cycles, 16-27 global-timer nanoseconds of the search start, the
+ * deferred residual / deblock / SAD-table tasks and the loaders' reference waits; only when
+ * the encoder was created with RIV_PROFILE_SEARCH set in the environment).
  * Returns RIV_ERR_FRAME if `size` is short. */
 riv_status riv_debug_frame_state(riv_encoder* enc, int what, void* out, size_t size);
 /* Number of glibc fix-up entries loaded for logf / exp2f. */

@@ -50,7 +50,8 @@ static inline void observe(BinProb& b, bool bit) {  // com/rans.rs:73-84
 
 static const int BATCH = 16386;  // com/rans.rs:201
 
-RansWriter::RansWriter(std::vector<uint8_t>* sink) : sink_(sink), stack_(BATCH), words_(BATCH + 8), sp_(BATCH) {}
+RansWriter::RansWriter(std::vector<uint8_t>* sink, const BatchSubmit* submit)
+    : sink_(sink), stack_(BATCH), sp_(BATCH), submit_(submit) {}
 
 inline void RansWriter::put(bool bit, BinProb& ctx) {
     uint8_t p = prob_zero(ctx);
@@ -62,7 +63,7 @@ inline void RansWriter::put_bypass(bool bit) {
     if (sp_ == 0) drain();
     stack_[--sp_] = (uint16_t)(128 | (bit ? 0x100 : 0));
 }
-void RansWriter::finish() { drain(); }
+
 
 static inline void enc_sym(uint32_t& r, uint16_t* words, int& wp, uint16_t e) {
     uint32_t p = e & 0xff;
@@ -80,34 +81,66 @@ static inline void enc_sym(uint32_t& r, uint16_t* words, int& wp, uint16_t e) {
 
 // RansEncoder::drain (com/rans.rs:231-269): walk the stack from the newest symbol
 // back to the oldest with two interleaved states; words are pushed to the front, so
-// they are written here from the end of `words_` backwards.
-void RansWriter::drain() {
+// they are written here from the end of the word buffer backwards, then appended to
+// `out` as little-endian bytes.
+static void code_batch(const uint16_t* stack, int sp, std::vector<uint8_t>& out) {
+    thread_local std::vector<uint16_t> words(BATCH + 8);
     uint32_t r0 = 65536, r1 = 65536;
-    uint16_t* w = words_.data();
-    int wp = (int)words_.size();
-    int i = sp_;
+    uint16_t* w = words.data();
+    int wp = (int)words.size();
+    int i = sp;
     if (i & 1) {
-        enc_sym(r0, w, wp, stack_[i]);
+        enc_sym(r0, w, wp, stack[i]);
         i++;
         std::swap(r0, r1);
     }
     for (; i < BATCH; i += 2) {
-        enc_sym(r0, w, wp, stack_[i]);
-        enc_sym(r1, w, wp, stack_[i + 1]);
+        enc_sym(r0, w, wp, stack[i]);
+        enc_sym(r1, w, wp, stack[i + 1]);
     }
     w[--wp] = (uint16_t)(r0 >> 16);
     w[--wp] = (uint16_t)(r0 & 0xffff);
     w[--wp] = (uint16_t)(r1 >> 16);
     w[--wp] = (uint16_t)(r1 & 0xffff);
-    size_t n = words_.size() - wp, base = sink_->size();
-    sink_->resize(base + 2 * n);
-    uint8_t* o = sink_->data() + base;
+    size_t n = words.size() - wp, base = out.size();
+    out.resize(base + 2 * n);
+    uint8_t* o = out.data() + base;
     for (size_t k = 0; k < n; k++) {
         uint16_t v = w[wp + k];
         o[2 * k] = (uint8_t)v;
         o[2 * k + 1] = (uint8_t)(v >> 8);
     }
+}
+
+void RansWriter::drain() {
+    if (submit_ == nullptr) {
+        code_batch(stack_.data(), sp_, *sink_);
+    } else {  // hand the full stack off and continue on a fresh one
+        batches_.emplace_back();
+        Batch& b = batches_.back();
+        b.stack.swap(stack_);
+        stack_.resize(BATCH);
+        b.sp = sp_;
+        b.done = (*submit_)([&b] { code_batch(b.stack.data(), b.sp, b.bytes); });
+    }
     sp_ = BATCH;
+}
+
+RansWriter::~RansWriter() {
+    for (Batch& b : batches_)
+        if (b.done.valid()) b.done.wait();
+}
+
+void RansWriter::finish() {
+    std::vector<uint8_t> last;
+    code_batch(stack_.data(), sp_, last);  // the partial batch, here while the others finish
+    sp_ = BATCH;
+    for (Batch& b : batches_) {
+        b.done.get();
+        sink_->insert(sink_->end(), b.bytes.begin(), b.bytes.end());
+    }
+    batches_.clear();
+    sink_->insert(sink_->end(), last.begin(), last.end());
 }
 
 // RansDecoder (com/rans.rs:299-354): two interleaved states, each symbol first takes the
@@ -208,10 +241,10 @@ static void encode_plane(RansWriter& w, DctContexts& c, const int16_t* pl, int l
 }
 
 void encode_residual_frame(const int16_t* packed, const uint8_t* eobs, int nblocks, bool intra,
-                           std::vector<uint8_t>& out) {
+                           std::vector<uint8_t>& out, const BatchSubmit* submit) {
     out.clear();
     if (nblocks == 0) return;  // the reference never instantiates the coder
-    RansWriter w(&out);
+    RansWriter w(&out, submit);
     DctContexts* c = new DctContexts();
     const int16_t* p = packed;
     for (int b = 0; b < nblocks; b++) {

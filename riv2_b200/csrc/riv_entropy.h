@@ -4,6 +4,9 @@
 // per-MB side info and compacted coefficients produced by the GPU.
 #pragma once
 #include <cstdint>
+#include <deque>
+#include <functional>
+#include <future>
 #include <tuple>
 #include <unordered_map>
 #include <vector>
@@ -16,11 +19,20 @@ struct BinProb {
     uint16_t packed = 0x0101;
 };
 
+// Runs a job on another thread and returns its completion.
+using BatchSubmit = std::function<std::future<void>(std::function<void()>)>;
+
 // Binary rANS writer with the reference's buffering (BATCH = 16386 symbols per drain,
-// two interleaved states, 8-bit scale, RANS_L = 2^16, u16 emission).
+// two interleaved states, 8-bit scale, RANS_L = 2^16, u16 emission).  Every drain starts
+// from fresh states, so a full batch's (probability, bit) stack is coded independently of
+// the rest: with `submit` the writer hands each full batch to it and keeps modelling, and
+// finish() codes the last batch itself, then appends the batches' words in order.
 class RansWriter {
 public:
-    explicit RansWriter(std::vector<uint8_t>* sink);
+    explicit RansWriter(std::vector<uint8_t>* sink, const BatchSubmit* submit = nullptr);
+    ~RansWriter();  // waits for batches still being coded (finish() not reached)
+    RansWriter(const RansWriter&) = delete;
+    RansWriter& operator=(const RansWriter&) = delete;
     inline void put(bool bit, BinProb& ctx);
     inline void put_bypass(bool bit);
     void finish();
@@ -29,8 +41,15 @@ private:
     void drain();
     std::vector<uint8_t>* sink_;
     std::vector<uint16_t> stack_;  // entry = p | bit << 8; stack_[BATCH-1] is the oldest
-    std::vector<uint16_t> words_;
     int sp_;
+    const BatchSubmit* submit_;
+    struct Batch {
+        std::vector<uint16_t> stack;
+        int sp = 0;
+        std::vector<uint8_t> bytes;
+        std::future<void> done;
+    };
+    std::deque<Batch> batches_;  // handed off, in stream order
 };
 
 // Binary rANS reader (com/rans.rs:299-354): the inverse of RansWriter.  Reads past the end
@@ -60,8 +79,9 @@ bool decode_residual_frame(const uint8_t* data, size_t len, const uint8_t* coded
 
 // Coded MBs in the GPU's compact layout: per MB, the Y, U and V blocks each truncated
 // after its last non-zero coefficient (eobs = those three indices per MB).
+// `submit` (optional) codes the full rANS batches on other threads.
 void encode_residual_frame(const int16_t* packed, const uint8_t* eobs, int nblocks, bool intra,
-                           std::vector<uint8_t>& out);
+                           std::vector<uint8_t>& out, const BatchSubmit* submit = nullptr);
 
 enum MvMode { M_ZERO = 0, M_NEAREST = 1, M_NEAR = 2, M_TOPRIGHT = 3, M_TOPLEFT = 4, M_NEW = 5, M_TEMPORAL = 6 };
 enum Subpel { SP_ZERO = 0, SP_PLUS = 1, SP_MINUS = 2 };

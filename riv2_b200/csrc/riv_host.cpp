@@ -300,6 +300,8 @@ struct MappedBuf {
 };
 
 // Per-frame timing events: Y = input stream, S = main chain, K = compaction stream.
+constexpr int NPAR = 3;  // rotation depth of the per-frame device buffers
+constexpr uint64_t TIMING_SAMPLE = 8;  // pipelined frames carry stage timing events one in this many
 enum { EV_START, EV_YUV, EV_S0, EV_TABLE, EV_SEARCH, EV_PRED, EV_AQ, EV_RES, EV_DEBLOCK, EV_K0, EV_COMPACT, EV_N };
 static const int NSTAGE = 8;  // rgb->yuv, table, search, predict, aq, residual, deblock, compact (+ total)
 
@@ -309,13 +311,18 @@ struct Slot {
     MappedBuf hdr;                             // coded MBs, coefficients, device status
     size_t prefetched = 0;                     // coefficient bytes included in the first copy
     cudaEvent_t ev_h2d = nullptr, ev_gpu = nullptr, ev_d2h = nullptr;
-    cudaEvent_t ev_k[EV_N] = {};
+    cudaEvent_t ev_k[EV_N] = {};  // stage timing (recorded on timed frames only)
+    cudaEvent_t ev_yuv = nullptr, ev_recon = nullptr;  // dependencies: input converted / reconstruction done
 };
 
 struct Job {
     uint64_t index = 0, ts = 0;
     int type = 0, slot = 0;
     int state = 0;  // 0 submitted, 1 entropy running
+    bool tail_done = true;  // compaction and copies enqueued (false while the frame is pending)
+    bool deferred = false;  // reconstructed inside the next P-frame's search launch
+    bool timed = false;     // stage timing events recorded for this frame
+    int ck = 0;             // double-buffer parity of the frame's buffers
     uint32_t count = 0;
     std::future<void> fut, fut_mv;
     std::vector<uint8_t> res_bytes, mv_bytes;
@@ -338,14 +345,27 @@ struct riv_encoder {
     cudaStream_t Y = nullptr, K = nullptr;                // input conversion, compaction
     // cross-stream reuse guards: cur[k] free (its residual is done), mbout[k] and the
     // coefficient buffers free (their compaction is done)
-    cudaEvent_t ev_cur_free[2] = {}, ev_mbout_free[2] = {}, ev_coef_free = nullptr;
+    cudaEvent_t ev_cur_free[NPAR] = {}, ev_mbout_free[NPAR] = {}, ev_coef_free[NPAR] = {};
     // the last search launch: input conversion waits for it, so that it never holds SMs the
     // next cooperative search launch needs
     cudaEvent_t ev_search_done = nullptr;
-    int fpar = 0, last_par = 0;  // double-buffer index of the next / last submitted frame
+    int fpar = 0, last_par = 0;  // rotation index of the next / last submitted frame
+    // A P-frame whose residual, deblock and compaction are handed to the next P-frame's
+    // search launch (pipelined encoding with the fused launch); flushed on demand.
+    struct Pending {
+        bool active = false;
+        uint64_t index = 0;
+        int ck = 0, level = 0;
+        ResidualParams rp{};
+        uint8_t* recon = nullptr;
+    } pend;
+    bool defer_ok = false;
+    int wq_words = 0, wq_par = 0;  // queue words of one launch; the array the next launch uses
     // device state
-    DevBuf curb[2], ref[2], recon_pre, pred, mboutb[2], coded[2], rec, varsum, lnv, qs, coeffs, opt_skip, fmask, eobs, status;
+    DevBuf curb[NPAR], ref[2], recon_pre, predb[NPAR], mboutb[NPAR], coded[2], rec, varsum, lnvb[NPAR], qs, coeffsb[NPAR], optskipb[NPAR],
+        fmaskb[NPAR], eobsb[NPAR], status, wq;
     DevBuf cindex, coffset, sadtab;
+    DevBuf lcindex, lcoffset;  // the search launch's own compaction scan (never shared with stream K's)
     DevBuf mvbits, logfix, expfix, ytab, ctab, newcost, newcost32;
     bool small_costs = false;
     bool table_ok = false;  // exhaustive SAD table + packed argmin usable (costs < 2^59)
@@ -363,6 +383,8 @@ struct riv_encoder {
     MvCoder mvc;
     std::unique_ptr<ThreadPool> pool;
     std::unique_ptr<ThreadPool> mv_exec;  // one thread: MV coding strictly in frame order
+    std::unique_ptr<ThreadPool> rans_pool;  // rANS coding of full coefficient batches (never waits)
+    BatchSubmit rans_submit;
     double host_ms[6] = {0};  // submit, retire, mv coding, dct coding (summed), write, blocked
     std::mutex stat_mu;
     float last_times[NSTAGE + 1] = {0};
@@ -373,7 +395,7 @@ struct riv_encoder {
     DevBuf prof;            // optional per-MB phase stamps of the search kernel
     DevBuf tflag;           // fused table: per-MB "table row written" flags (frame tag)
     DevBuf rowdone;         // AQ inside the search: per-row "ln variances written" flags (frame tag)
-    uint64_t h2d_bytes = 0, d2h_bytes = 0, pframes = 0, launches = 0;
+    uint64_t h2d_bytes = 0, d2h_bytes = 0, pframes = 0, launches = 0, pdeferred = 0, ptimed = 0;
 };
 
 namespace {
@@ -413,34 +435,37 @@ static void setup_device(riv_encoder* e) {
     CK(cudaStreamCreateWithFlags(&e->Hs, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&e->Y, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&e->K, cudaStreamNonBlocking));
-    for (int k = 0; k < 2; k++) {
+    for (int k = 0; k < NPAR; k++) {
         CK(cudaEventCreateWithFlags(&e->ev_cur_free[k], cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&e->ev_mbout_free[k], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&e->ev_coef_free[k], cudaEventDisableTiming));
     }
-    CK(cudaEventCreateWithFlags(&e->ev_coef_free, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&e->ev_search_done, cudaEventDisableTiming));
     int32_t t16[256], t8[64];
     dct_tables(t16, t8);
     CK(riv_upload_dct_tables(t16, t8));
     const int N = e->NMB;
-    e->curb[0].alloc(e->yuv_bytes);
-    e->curb[1].alloc(e->yuv_bytes);
     e->ref[0].alloc(e->yuv_bytes);
     e->ref[1].alloc(e->yuv_bytes);
     e->recon_pre.alloc(e->yuv_bytes);  // reconstruction before the (out-of-place) deblock
-    e->pred.alloc(e->yuv_bytes);
-    e->mboutb[0].alloc((size_t)N * sizeof(MbOut));
-    e->mboutb[1].alloc((size_t)N * sizeof(MbOut));
     e->coded[0].alloc((size_t)N * 4);
     e->coded[1].alloc((size_t)N * 4);
     e->rec.alloc((size_t)2 * N * sizeof(MbRec));  // raw-MV records, then coded-MV records
     e->varsum.alloc((size_t)N * sizeof(uint2));
-    e->lnv.alloc((size_t)(N + 4) * sizeof(float));
     e->qs.alloc((size_t)N * sizeof(float));
-    e->coeffs.alloc((size_t)N * 384 * sizeof(int16_t));
-    e->opt_skip.alloc(N);
-    e->fmask.alloc(N);
-    e->eobs.alloc((size_t)N * 3);
+    for (int k = 0; k < NPAR; k++) {  // per frame: the next frame's launch may still reconstruct this one
+        e->curb[k].alloc(e->yuv_bytes);
+        e->predb[k].alloc(e->yuv_bytes);
+        e->mboutb[k].alloc((size_t)N * sizeof(MbOut));
+        e->lnvb[k].alloc((size_t)(N + 4) * sizeof(float));
+        e->coeffsb[k].alloc((size_t)N * 384 * sizeof(int16_t));
+        e->optskipb[k].alloc(N);
+        e->fmaskb[k].alloc(N);
+        e->eobsb[k].alloc((size_t)N * 3);
+    }
+    e->wq_words = 2 + 2 * e->BH;
+    e->wq.alloc((size_t)2 * e->wq_words * sizeof(unsigned));  // two queue arrays, alternating per launch
+    e->wq.zero(e->S);
     e->status.alloc(sizeof(unsigned));
     e->rec.zero(e->S);
     e->status.zero(e->S);
@@ -489,6 +514,8 @@ static void setup_device(riv_encoder* e) {
     CK(cudaMemcpy(e->ctab.p, ct, sizeof(ct), cudaMemcpyHostToDevice));
     CK(search_plan(c.search_range, (int)c.storage_width, e->BH, e->table_ok, e->small_costs, &e->splan));
     if (e->splan.grid <= 0) throw std::runtime_error("search kernel cannot be made resident");
+    // P-frame reconstruction folded into the next P-frame's search launch (its worker CTAs)
+    e->defer_ok = e->splan.fused && e->splan.fast && e->table_ok && c.pipeline_depth > 1;
     if (e->splan.fused) {
         e->tflag.alloc((size_t)N * sizeof(unsigned));
         e->tflag.zero(e->S);
@@ -521,21 +548,104 @@ static void setup_device(riv_encoder* e) {
         CK(cudaEventCreateWithFlags(&s.ev_gpu, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&s.ev_d2h, cudaEventDisableTiming));
         for (int k = 0; k < EV_N; k++) CK(cudaEventCreate(&s.ev_k[k]));
+        CK(cudaEventCreateWithFlags(&s.ev_yuv, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&s.ev_recon, cudaEventDisableTiming));
     }
     e->coef_guess = (size_t)N * 384;  // half the dense size until the first frames are seen
     if (getenv("RIV_PROFILE_SEARCH")) {
-        e->prof.alloc((size_t)N * 16 * sizeof(long long));
+        e->prof.alloc((size_t)N * RIV_PROF_WORDS * sizeof(long long));
         e->prof.zero(e->S);
     }
     e->cindex.alloc((size_t)N * 4);
     e->coffset.alloc((size_t)N * 4);
+    e->lcindex.alloc((size_t)N * 4);
+    e->lcoffset.alloc((size_t)N * 4);
     if (e->table_ok)
         e->sadtab.alloc((size_t)N * sad_table_stride(c.search_range) * sizeof(uint16_t));
     unsigned nt = c.entropy_threads;
     if (nt == 0) nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency() > 1 ? std::thread::hardware_concurrency() - 1 : 1u));
     e->pool.reset(new ThreadPool(nt));
     e->mv_exec.reset(new ThreadPool(1));
+    e->rans_pool.reset(new ThreadPool(std::max(2u, nt / 2)));
+    {
+        ThreadPool* rp = e->rans_pool.get();
+        e->rans_submit = [rp](std::function<void()> f) { return rp->submit(std::move(f)); };
+    }
     CK(cudaStreamSynchronize(e->S));
+}
+
+// Stage marks.  Timing-enabled events between back-to-back cooperative launches cost a few
+// microseconds of idle GPU each, so the stage timing events are recorded on sampled frames
+// only; the two marks other streams depend on also record a non-timing event every frame.
+static void mark(riv_encoder* e, const Job& j, int k, cudaStream_t st) {
+    Slot& s = e->slots[j.slot];
+    if (j.timed) CK(cudaEventRecord(s.ev_k[k], st));
+    if (k == EV_YUV) CK(cudaEventRecord(s.ev_yuv, st));
+    if (k == EV_DEBLOCK) CK(cudaEventRecord(s.ev_recon, st));
+}
+
+static Job* find_job(riv_encoder* e, uint64_t index) {
+    for (auto& j : e->jobs)
+        if (j.index == index) return &j;
+    return nullptr;
+}
+
+// Compaction of a frame whose reconstruction is enqueued (it waits for the frame's
+// EV_DEBLOCK; `compacted`: the search launch that reconstructed it compacted it too), then
+// the status and the device->host copies of its side info and coefficients.
+static void frame_tail(riv_encoder* e, Job& j, bool compacted = false) {
+    Slot& s = e->slots[j.slot];
+    const int N = e->NMB, ck = j.ck;
+    cudaStream_t K = e->K;
+    CK(cudaStreamWaitEvent(K, s.ev_recon, 0));
+    mark(e, j, EV_K0, K);
+    if (!compacted) {
+        e->launches += 2;  // scan + pack
+        CK(launch_compact(e->optskipb[ck].as<uint8_t>(), e->mboutb[ck].as<MbOut>(), e->coeffsb[ck].as<int16_t>(),
+                          e->eobsb[ck].as<uint8_t>(), N, j.type == 1 ? 1 : 0, e->cindex.as<int32_t>(),
+                          e->coffset.as<int32_t>(), s.dside.as<uint32_t>(), s.dpacked.as<int16_t>(),
+                          s.dpeobs.as<uint8_t>(), s.hdr.dev<uint32_t>(), K));
+    }
+    CK(cudaEventRecord(e->ev_coef_free[ck], K));
+    CK(cudaEventRecord(e->ev_mbout_free[ck], K));
+    mark(e, j, EV_COMPACT, K);
+    CK(cudaMemcpyAsync(s.hdr.host<uint32_t>() + 2, e->status.p, 4, cudaMemcpyDeviceToHost, K));
+    CK(cudaEventRecord(s.ev_gpu, K));
+    // DMA the side info, EOBs and (a bounded prefix of) the coefficients on the copy
+    // stream; the exact size is only known once the frame is done.
+    CK(cudaStreamWaitEvent(e->C, s.ev_gpu, 0));
+    CK(cudaMemcpyAsync(s.side.p, s.dside.p, (size_t)N * 4, cudaMemcpyDeviceToHost, e->C));
+    CK(cudaMemcpyAsync(s.peobs.p, s.dpeobs.p, (size_t)N * 3, cudaMemcpyDeviceToHost, e->C));
+    s.prefetched = std::min(e->coef_guess, (size_t)N * 384 * 2);
+    CK(cudaMemcpyAsync(s.packed.p, s.dpacked.p, s.prefetched, cudaMemcpyDeviceToHost, e->C));
+    CK(cudaEventRecord(s.ev_d2h, e->C));
+    j.tail_done = true;
+}
+
+// Residual and deblock of a frame as separate kernels on S, then its tail.
+static void reconstruct_now(riv_encoder* e, Job& j, const ResidualParams& rp, int level, int E, int I, int Hv,
+                            const uint8_t* mask, uint8_t* recon) {
+    Slot& s = e->slots[j.slot];
+    cudaStream_t S = e->S;
+    CK(cudaStreamWaitEvent(S, e->ev_coef_free[j.ck], 0));  // compaction of the frame NPAR back
+    e->launches += 1 + (level > 0 ? 1 : 0);
+    CK(launch_residual(rp, e->NMB, S));
+    mark(e, j, EV_RES, S);
+    CK(cudaEventRecord(e->ev_cur_free[j.ck], S));
+    if (level > 0) CK(launch_deblock_tiled(e->recon_pre.as<uint8_t>(), recon, e->W, e->H, E, I, Hv, mask, S));
+    mark(e, j, EV_DEBLOCK, S);
+    frame_tail(e, j);
+}
+
+// Run the pending frame's reconstruction now (separate kernels), when no later launch will.
+static void flush_pending(riv_encoder* e) {
+    if (!e->pend.active) return;
+    Job* j = find_job(e, e->pend.index);
+    e->pend.active = false;
+    if (!j) return;
+    j->deferred = false;
+    reconstruct_now(e, *j, e->pend.rp, e->pend.level, e->inter_E, e->inter_I, e->inter_H,
+                    e->fmaskb[e->pend.ck].as<uint8_t>(), e->pend.recon);
 }
 
 // Enqueue the GPU work of one frame.  `src` = 0 host RGB, 1 device RGB, 2 host YUV.
@@ -543,30 +653,32 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
     const riv_config& c = e->cfg;
     Slot& s = e->slots[j.slot];
     const int W = e->W, H = e->H, N = e->NMB;
-    cudaStream_t S = e->S, Y = e->Y, K = e->K;
+    cudaStream_t S = e->S, Y = e->Y;
     const int ck = e->fpar;  // this frame's input planes and per-MB output buffers
+    j.ck = ck;
     uint8_t* cur = e->curb[ck].as<uint8_t>();
     MbOut* mbo = e->mboutb[ck].as<MbOut>();
+    const bool defer_this = j.type == 2 && e->defer_ok;
+    if (j.type == 1) flush_pending(e);  // key frames reconstruct immediately
     // kernels per frame: rgb->yuv, (search, predict, 3 x aq), residual, deblock, scan + pack
-    const int nplanes_db = 1;  // one launch for the three planes
-    // P-frame: search (+ table unless fused) (+ predict and 3 AQ unless inside the search)
     const int p_launches = 1 + (e->table_ok && !e->splan.fused ? 1 : 0) + (e->splan.fast && e->table_ok ? 0 : 4);
-    e->launches += (src == 2 ? 0 : 1) + (j.type == 2 ? p_launches : 0) + 1 +
-                   ((j.type == 2 ? e->inter_level : e->intra_level) > 0 ? nplanes_db : 0) + 2;
+    e->launches += (src == 2 ? 0 : 1) + (j.type == 2 ? p_launches : 0);  // + residual / deblock / compaction below
     if (src == 0) e->h2d_bytes += (uint64_t)c.display_width * c.display_height * 3;
     if (src == 2) e->h2d_bytes += e->yuv_bytes;
     // ---- input conversion on Y, overlapping the previous frame's main chain; cur[ck] is
-    // free once the residual of the frame two back has read it
+    // free once the residual of the frame NPAR back has read it
     CK(cudaStreamWaitEvent(Y, e->ev_cur_free[ck], 0));
-    CK(cudaStreamWaitEvent(Y, e->ev_search_done, 0));
+    // without deferral: after the previous search launch, i.e. beside that frame's residual;
+    // with it the conversion runs in the gap between two launches, one frame ahead
+    if (!e->defer_ok) CK(cudaStreamWaitEvent(Y, e->ev_search_done, 0));
     if (src == 0) {
         CK(cudaMemcpyAsync(s.rgb.p, a, (size_t)c.display_width * c.display_height * 3, cudaMemcpyHostToDevice, e->Hs));
         CK(cudaEventRecord(s.ev_h2d, e->Hs));
         CK(cudaStreamWaitEvent(Y, s.ev_h2d, 0));
-        CK(cudaEventRecord(s.ev_k[EV_START], Y));
+        mark(e, j, EV_START, Y);
         CK(launch_rgb_to_yuv((const uint8_t*)s.rgb.p, (int)c.display_width, (int)c.display_height, cur, W, H, Y));
     } else if (src == 1) {
-        CK(cudaEventRecord(s.ev_k[EV_START], Y));
+        mark(e, j, EV_START, Y);
         CK(launch_rgb_to_yuv((const uint8_t*)a, (int)c.display_width, (int)c.display_height, cur, W, H, Y));
     } else {
         uint8_t* d = s.rgb.as<uint8_t>();
@@ -576,41 +688,35 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         CK(cudaMemcpyAsync(d + ys + cs, c3, cs, cudaMemcpyHostToDevice, e->Hs));
         CK(cudaEventRecord(s.ev_h2d, e->Hs));
         CK(cudaStreamWaitEvent(Y, s.ev_h2d, 0));
-        CK(cudaEventRecord(s.ev_k[EV_START], Y));
+        mark(e, j, EV_START, Y);
         CK(cudaMemcpyAsync(cur, d, e->yuv_bytes, cudaMemcpyDeviceToDevice, Y));
     }
-    CK(cudaEventRecord(s.ev_k[EV_YUV], Y));
+    mark(e, j, EV_YUV, Y);
     // ---- main chain on S
-    CK(cudaStreamWaitEvent(S, s.ev_k[EV_YUV], 0));
-    CK(cudaEventRecord(s.ev_k[EV_S0], S));
+    CK(cudaStreamWaitEvent(S, s.ev_yuv, 0));
+    mark(e, j, EV_S0, S);
     const int nxt = e->ref_cur ^ 1;
     uint8_t* recon = e->ref[nxt].as<uint8_t>();
     ResidualParams rp{};
     rp.cur = cur;
-    rp.pred = e->pred.as<uint8_t>();
+    rp.pred = e->predb[ck].as<uint8_t>();
     rp.recon = recon;  // or recon_pre when a deblock follows (set per frame type below)
-    rp.coeffs = e->coeffs.as<int16_t>();
-    rp.opt_skip = e->opt_skip.as<uint8_t>();
-    rp.fmask = e->fmask.as<uint8_t>();
-    rp.eobs = e->eobs.as<uint8_t>();
+    rp.coeffs = e->coeffsb[ck].as<int16_t>();
+    rp.opt_skip = e->optskipb[ck].as<uint8_t>();
+    rp.fmask = e->fmaskb[ck].as<uint8_t>();
+    rp.eobs = e->eobsb[ck].as<uint8_t>();
     rp.dead_zone = c.inter_dead_zone;
     rp.W = W; rp.H = H; rp.BW = e->BW;
     if (j.type == 1) {
         rp.intra = 1;
         rp.intra_ytab = e->ytab.as<uint16_t>();
         rp.intra_ctab = e->ctab.as<uint16_t>();
-        CK(cudaEventRecord(s.ev_k[EV_TABLE], S));
-        CK(cudaEventRecord(s.ev_k[EV_SEARCH], S));
-        CK(cudaEventRecord(s.ev_k[EV_PRED], S));
-        CK(cudaEventRecord(s.ev_k[EV_AQ], S));
-        CK(cudaStreamWaitEvent(S, e->ev_coef_free, 0));  // the previous frame's compaction read them
+        mark(e, j, EV_TABLE, S);
+        mark(e, j, EV_SEARCH, S);
+        mark(e, j, EV_PRED, S);
+        mark(e, j, EV_AQ, S);
         if (e->intra_level > 0) rp.recon = e->recon_pre.as<uint8_t>();
-        CK(launch_residual(rp, N, S));
-        CK(cudaEventRecord(s.ev_k[EV_RES], S));
-        CK(cudaEventRecord(e->ev_cur_free[ck], S));
-        if (e->intra_level > 0)
-            CK(launch_deblock_tiled(e->recon_pre.as<uint8_t>(), recon, W, H, e->intra_E, e->intra_I, e->intra_H, nullptr, S));
-        CK(cudaEventRecord(s.ev_k[EV_DEBLOCK], S));
+        reconstruct_now(e, j, rp, e->intra_level, e->intra_E, e->intra_I, e->intra_H, nullptr, recon);
         e->has_prev_mvs = false;
     } else {
         SearchParams sp{};
@@ -647,39 +753,71 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         sp.tab = nullptr;
         sp.tstride = 0;
         sp.tflag = nullptr;
+        sp.wq = e->wq.as<unsigned>() + (size_t)e->wq_par * e->wq_words;
+        sp.wq_next = e->wq.as<unsigned>() + (size_t)(e->wq_par ^ 1) * e->wq_words;
+        sp.wq_words = e->wq_words;
         if (e->table_ok) {
             sp.tstride = sad_table_stride(c.search_range);
             sp.tab = e->sadtab.as<uint16_t>();
             if (e->splan.fused) sp.tflag = e->tflag.as<unsigned>();  // computed inside the search launch
             else CK(launch_sad_table(sp.ref_y, sp.cur_y, W, H, c.search_range, e->sadtab.as<uint16_t>(), sp.tstride, S));
         }
-        CK(cudaEventRecord(s.ev_k[EV_TABLE], S));
+        mark(e, j, EV_TABLE, S);
         sp.prof = e->prof.as<long long>();
         // coded MVs of this frame become next frame's temporal predictors
         const int cn = e->coded_cur ^ 1;
         sp.coded_out = e->coded[cn].as<int8_t>();
         const bool aq_in_search = e->splan.fast && e->table_ok;
         if (aq_in_search) {  // prediction, variances and ln inside the search launch
-            sp.pred = e->pred.as<uint8_t>();
+            sp.pred = e->predb[ck].as<uint8_t>();
             sp.varsum = e->varsum.as<uint2>();
-            sp.lnv = e->lnv.as<float>();
+            sp.lnv = e->lnvb[ck].as<float>();
             sp.row_done = e->rowdone.as<unsigned>();
             sp.logfix = e->logfix.as<uint32_t>();
             sp.nlog = e->nlog;
         }
-        CK(cudaStreamWaitEvent(S, e->ev_mbout_free[ck], 0));  // compaction of the frame two back
+        // the pending frame's residual and deblock run inside this launch
+        Job* pj = e->pend.active ? find_job(e, e->pend.index) : nullptr;
+        if (pj) {
+            sp.defer = 1;
+            sp.dres = e->pend.rp;
+            sp.db_level = e->pend.level;
+            sp.db_E = e->inter_E; sp.db_I = e->inter_I; sp.db_H = e->inter_H;
+            sp.db_src = e->recon_pre.as<uint8_t>();
+            sp.db_dst = e->pend.recon;
+            sp.db_mask = e->fmaskb[e->pend.ck].as<uint8_t>();
+            Slot& ps = e->slots[pj->slot];  // its compaction at the end of the queue
+            sp.compact = 1;
+            sp.c_index = e->lcindex.as<int32_t>();
+            sp.c_offset = e->lcoffset.as<int32_t>();
+            sp.c_side = ps.dside.as<uint32_t>();
+            sp.c_packed = ps.dpacked.as<int16_t>();
+            sp.c_peobs = ps.dpeobs.as<uint8_t>();
+            sp.c_hdr = ps.hdr.dev<uint32_t>();
+            CK(cudaStreamWaitEvent(S, e->ev_coef_free[e->pend.ck], 0));  // compaction of the frame NPAR back
+        }
+        e->pend.active = false;
+        CK(cudaStreamWaitEvent(S, e->ev_mbout_free[ck], 0));  // compaction of the frame NPAR back
         CK(launch_search(sp, e->splan, S));
-        CK(cudaEventRecord(s.ev_k[EV_SEARCH], S));
+        e->wq_par ^= 1;
+        mark(e, j, EV_SEARCH, S);
         CK(cudaEventRecord(e->ev_search_done, S));
+        if (pj) {  // the pending frame is reconstructed: its compaction and copies follow
+            Slot& ps = e->slots[pj->slot];
+            CK(cudaEventRecord(e->ev_cur_free[pj->ck], S));
+            mark(e, *pj, EV_DEBLOCK, S);
+            frame_tail(e, *pj, true);
+        }
         if (!aq_in_search)
-            CK(launch_predict(e->ref[e->ref_cur].as<uint8_t>(), mbo, e->pred.as<uint8_t>(), e->varsum.as<uint2>(), W, H, S));
-        CK(cudaEventRecord(s.ev_k[EV_PRED], S));
+            CK(launch_predict(e->ref[e->ref_cur].as<uint8_t>(), mbo, e->predb[ck].as<uint8_t>(), e->varsum.as<uint2>(), W,
+                              H, S));
+        mark(e, j, EV_PRED, S);
         if (!aq_in_search)
             CK(launch_aq(e->varsum.as<uint2>(), N, e->inter_base, e->logfix.as<uint32_t>(), e->nlog, e->expfix.as<uint32_t>(),
-                         e->nexp, e->lnv.as<float>(), e->qs.as<float>(), S));
-        CK(cudaEventRecord(s.ev_k[EV_AQ], S));
+                         e->nexp, e->lnvb[ck].as<float>(), e->qs.as<float>(), S));
+        mark(e, j, EV_AQ, S);
         if (aq_in_search) {  // the residual derives the steps from the ln variances and their mean
-            rp.lnv = e->lnv.as<float>();
+            rp.lnv = e->lnvb[ck].as<float>();
             rp.aq_base = e->inter_base;
             rp.expfix = e->expfix.as<uint32_t>();
             rp.nexp = e->nexp;
@@ -689,43 +827,28 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         rp.intra = 0;
         rp.mb = mbo;
         rp.qs = e->qs.as<float>();
-        CK(cudaStreamWaitEvent(S, e->ev_coef_free, 0));  // the previous frame's compaction read them
         if (e->inter_level > 0) rp.recon = e->recon_pre.as<uint8_t>();
-        CK(launch_residual(rp, N, S));
-        CK(cudaEventRecord(s.ev_k[EV_RES], S));
-        CK(cudaEventRecord(e->ev_cur_free[ck], S));
-        if (e->inter_level > 0)
-            CK(launch_deblock_tiled(e->recon_pre.as<uint8_t>(), recon, W, H, e->inter_E, e->inter_I, e->inter_H,
-                                    e->fmask.as<uint8_t>(), S));
-        CK(cudaEventRecord(s.ev_k[EV_DEBLOCK], S));
+        if (defer_this) {  // reconstructed by the next P-frame's launch (or a flush)
+            mark(e, j, EV_RES, S);
+            e->pend.active = true;
+            e->pend.index = j.index;
+            e->pend.ck = ck;
+            e->pend.level = e->inter_level;
+            e->pend.rp = rp;
+            e->pend.recon = recon;
+            j.tail_done = false;
+            j.deferred = true;
+        } else {
+            reconstruct_now(e, j, rp, e->inter_level, e->inter_E, e->inter_I, e->inter_H, e->fmaskb[ck].as<uint8_t>(),
+                            recon);
+        }
         e->coded_cur = cn;
         e->has_prev_mvs = true;
     }
-    // ---- compaction on K once the frame's main chain is done: run alone it takes a few
-    // microseconds, while beside the deblock it delays the next (cooperative, whole-GPU)
-    // search launch by longer
-    CK(cudaStreamWaitEvent(K, s.ev_k[EV_DEBLOCK], 0));
-    CK(cudaEventRecord(s.ev_k[EV_K0], K));
-    CK(launch_compact(e->opt_skip.as<uint8_t>(), mbo, e->coeffs.as<int16_t>(), e->eobs.as<uint8_t>(), N, j.type == 1 ? 1 : 0,
-                      e->cindex.as<int32_t>(), e->coffset.as<int32_t>(), s.dside.as<uint32_t>(), s.dpacked.as<int16_t>(),
-                      s.dpeobs.as<uint8_t>(), s.hdr.dev<uint32_t>(), K));
-    CK(cudaEventRecord(e->ev_coef_free, K));
-    CK(cudaEventRecord(e->ev_mbout_free[ck], K));
-    CK(cudaEventRecord(s.ev_k[EV_COMPACT], K));
-    CK(cudaMemcpyAsync(s.hdr.host<uint32_t>() + 2, e->status.p, 4, cudaMemcpyDeviceToHost, K));
-    CK(cudaEventRecord(s.ev_gpu, K));
     e->ref_cur = nxt;
     e->has_ref = true;
     e->last_par = ck;
-    e->fpar ^= 1;
-    // DMA the side info, EOBs and (a bounded prefix of) the coefficients on the copy
-    // stream; the exact size is only known once the frame is done.
-    CK(cudaStreamWaitEvent(e->C, s.ev_gpu, 0));
-    CK(cudaMemcpyAsync(s.side.p, s.dside.p, (size_t)N * 4, cudaMemcpyDeviceToHost, e->C));
-    CK(cudaMemcpyAsync(s.peobs.p, s.dpeobs.p, (size_t)N * 3, cudaMemcpyDeviceToHost, e->C));
-    s.prefetched = std::min(e->coef_guess, (size_t)N * 384 * 2);
-    CK(cudaMemcpyAsync(s.packed.p, s.dpacked.p, s.prefetched, cudaMemcpyDeviceToHost, e->C));
-    CK(cudaEventRecord(s.ev_d2h, e->C));
+    e->fpar = (ck + 1) % NPAR;
 }
 
 // Host part of a frame once its GPU work is done: its side info and coefficients are
@@ -755,15 +878,25 @@ static riv_status retire(riv_encoder* e, Job& j) {
     e->coef_guess = coef_bytes + coef_bytes / 4 + 65536;
     e->d2h_bytes += (uint64_t)e->NMB * 7 + 12 + std::max(coef_bytes, s.prefetched);
     float t[NSTAGE + 1] = {0};
-    CK(cudaEventSynchronize(s.ev_k[EV_DEBLOCK]));  // the D2H did not wait for the deblock
+    CK(cudaEventSynchronize(s.ev_recon));  // the D2H did not wait for the deblock
     const int spans[NSTAGE + 1][2] = {{EV_START, EV_YUV},   {EV_S0, EV_TABLE},  {EV_TABLE, EV_SEARCH},
                                       {EV_SEARCH, EV_PRED}, {EV_PRED, EV_AQ},   {EV_AQ, EV_RES},
                                       {EV_RES, EV_DEBLOCK}, {EV_K0, EV_COMPACT}, {EV_S0, EV_DEBLOCK}};
-    for (int k = 0; k <= NSTAGE; k++) cudaEventElapsedTime(&t[k], s.ev_k[spans[k][0]], s.ev_k[spans[k][1]]);
+    if (j.timed) {
+        for (int k = 0; k <= NSTAGE; k++) cudaEventElapsedTime(&t[k], s.ev_k[spans[k][0]], s.ev_k[spans[k][1]]);
+        if (j.deferred) {  // residual and deblock ran inside the next launch: the chain ends with the search launch
+            t[5] = t[6] = 0.0f;
+            cudaEventElapsedTime(&t[NSTAGE], s.ev_k[EV_S0], s.ev_k[EV_AQ]);
+        }
+    }
     for (int k = 0; k <= NSTAGE; k++) j.times[k] = t[k] * 1000.0f;
     if (j.type == 2) {
-        for (int k = 0; k <= NSTAGE; k++) e->sum_times[k] += j.times[k];
+        if (j.timed) {
+            for (int k = 0; k <= NSTAGE; k++) e->sum_times[k] += j.times[k];
+            e->ptimed++;
+        }
         e->pframes++;
+        if (j.deferred) e->pdeferred++;
     }
     const int N = e->NMB;
     riv_frame_stats& S = j.stats;
@@ -825,7 +958,7 @@ static riv_status retire(riv_encoder* e, Job& j) {
     bool intra = j.type == 1;
     j.fut = e->pool->submit([jp, ep, packed, peobs, count, intra] {
         double d0 = now_ms();
-        encode_residual_frame(packed, peobs, (int)count, intra, jp->res_bytes);
+        encode_residual_frame(packed, peobs, (int)count, intra, jp->res_bytes, &ep->rans_submit);
         double dt = now_ms() - d0;
         std::lock_guard<std::mutex> g(ep->stat_mu);
         ep->host_ms[3] += dt;
@@ -868,8 +1001,10 @@ static riv_status write_job(riv_encoder* e, Job& j) {
     if (e->wr.write(e->wr.user, rec.data(), rec.size()) != 0) return fail(e, RIV_ERR_IO, "writer.write failed");
     e->host_ms[4] += now_ms() - w0;
     e->frame_count++;
-    memcpy(e->last_times, j.times, sizeof(j.times));
-    e->have_times = true;
+    if (j.timed) {
+        memcpy(e->last_times, j.times, sizeof(j.times));
+        e->have_times = true;
+    }
     e->last_stats = j.stats;
     return RIV_OK;
 }
@@ -881,6 +1016,12 @@ static riv_status pump(riv_encoder* e, bool block_front) {
     bool block = block_front;
     for (auto& j : e->jobs) {
         if (j.state != 0) continue;
+        if (!j.tail_done) {  // still waiting for the next frame's launch
+            // flush only when nothing older can complete instead (a retired front frame
+            // whose entropy coding the loop below waits for keeps the deferral)
+            if (!block || e->jobs.front().state == 1) break;
+            flush_pending(e);
+        }
         if (!block) {
             cudaError_t q = cudaEventQuery(e->slots[j.slot].ev_gpu);
             if (q == cudaErrorNotReady) break;
@@ -906,6 +1047,7 @@ static riv_status pump(riv_encoder* e, bool block_front) {
 }
 
 static riv_status drain_all(riv_encoder* e) {
+    flush_pending(e);  // no later launch is coming: reconstruct now, before the host work queued ahead of it
     while (!e->jobs.empty()) {
         riv_status st = pump(e, true);
         if (st) return st;
@@ -937,6 +1079,7 @@ static riv_status encode_common(riv_encoder* e, int src, const void* a, const vo
         j.ts = ts;
         j.type = intra ? 1 : 2;
         j.slot = (int)(n % cap);
+        j.timed = e->cfg.pipeline_depth == 0 || stats != nullptr || n % TIMING_SAMPLE == 0;
         double s0 = now_ms();
         submit_gpu(e, j, src, a, b, c3);
         e->submitted++;
@@ -1079,6 +1222,7 @@ void riv_encoder_free(riv_encoder* e) {
     }
     e->pool.reset();
     e->mv_exec.reset();
+    e->rans_pool.reset();
     if (e->S) cudaStreamSynchronize(e->S);
     if (e->C) cudaStreamSynchronize(e->C);
     if (e->Hs) cudaStreamSynchronize(e->Hs);
@@ -1092,22 +1236,27 @@ void riv_encoder_free(riv_encoder* e) {
         if (s.ev_d2h) cudaEventDestroy(s.ev_d2h);
         for (int k = 0; k < EV_N; k++)
             if (s.ev_k[k]) cudaEventDestroy(s.ev_k[k]);
+        if (s.ev_yuv) cudaEventDestroy(s.ev_yuv);
+        if (s.ev_recon) cudaEventDestroy(s.ev_recon);
     }
-    DevBuf* bufs[] = {&e->curb[0], &e->curb[1], &e->ref[0], &e->ref[1], &e->recon_pre, &e->pred, &e->mboutb[0], &e->mboutb[1],
-                      &e->coded[0], &e->coded[1], &e->rec,
-                      &e->varsum, &e->lnv, &e->qs, &e->coeffs, &e->opt_skip, &e->fmask, &e->eobs, &e->status,
-                      &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset, &e->sadtab, &e->prof, &e->tflag, &e->rowdone, &e->newcost, &e->newcost32};
+    for (int k = 0; k < NPAR; k++)
+        for (DevBuf* b : {&e->curb[k], &e->predb[k], &e->mboutb[k], &e->lnvb[k], &e->coeffsb[k], &e->optskipb[k], &e->fmaskb[k],
+                          &e->eobsb[k]})
+            b->release();
+    DevBuf* bufs[] = {&e->ref[0], &e->ref[1], &e->recon_pre, &e->wq, &e->coded[0], &e->coded[1], &e->rec,
+                      &e->varsum, &e->qs, &e->status,
+                      &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset, &e->lcindex, &e->lcoffset, &e->sadtab, &e->prof, &e->tflag, &e->rowdone, &e->newcost, &e->newcost32};
     for (DevBuf* b : bufs) b->release();
     if (e->S) cudaStreamDestroy(e->S);
     if (e->C) cudaStreamDestroy(e->C);
     if (e->Hs) cudaStreamDestroy(e->Hs);
     if (e->Y) cudaStreamDestroy(e->Y);
     if (e->K) cudaStreamDestroy(e->K);
-    for (int k = 0; k < 2; k++) {
+    for (int k = 0; k < NPAR; k++) {
         if (e->ev_cur_free[k]) cudaEventDestroy(e->ev_cur_free[k]);
         if (e->ev_mbout_free[k]) cudaEventDestroy(e->ev_mbout_free[k]);
+        if (e->ev_coef_free[k]) cudaEventDestroy(e->ev_coef_free[k]);
     }
-    if (e->ev_coef_free) cudaEventDestroy(e->ev_coef_free);
     if (e->ev_search_done) cudaEventDestroy(e->ev_search_done);
     delete e;
 }
@@ -1119,6 +1268,7 @@ riv_status riv_last_recon(riv_encoder* e, uint8_t* y, uint8_t* u, uint8_t* v) {
     if (!e || !e->has_ref) return RIV_ERR_FRAME;
     try {
         CK(cudaSetDevice(e->cfg.device));
+        flush_pending(e);
         CK(cudaStreamSynchronize(e->S));
         const uint8_t* d = e->ref[e->ref_cur].as<uint8_t>();
         size_t ys = (size_t)e->W * e->H, cs = ys / 4;
@@ -1137,16 +1287,17 @@ riv_status riv_debug_frame_state(riv_encoder* e, int what, void* out, size_t siz
     switch (what) {
         case 0: b = &e->mboutb[e->last_par]; break;
         case 1: b = &e->qs; break;
-        case 2: b = &e->pred; break;
+        case 2: b = &e->predb[e->last_par]; break;
         case 3: b = &e->curb[e->last_par]; break;
-        case 4: b = &e->coeffs; break;
-        case 5: b = &e->opt_skip; break;
+        case 4: b = &e->coeffsb[e->last_par]; break;
+        case 5: b = &e->optskipb[e->last_par]; break;
         case 6: b = &e->prof; break;
         default: return RIV_ERR_FRAME;
     }
     if (size < b->n) return RIV_ERR_FRAME;
     try {
         CK(cudaSetDevice(e->cfg.device));
+        flush_pending(e);
         CK(cudaStreamSynchronize(e->Y));
         CK(cudaStreamSynchronize(e->S));
         CK(cudaStreamSynchronize(e->K));
@@ -1164,11 +1315,11 @@ riv_status riv_host_times(riv_encoder* e, double* ms6) {
     return RIV_OK;
 }
 
-riv_status riv_counters(riv_encoder* e, double* us8, uint64_t* io2, uint64_t* n2) {
+riv_status riv_counters(riv_encoder* e, double* us8, uint64_t* io2, uint64_t* n4) {
     if (!e) return RIV_ERR_FRAME;
     if (us8) memcpy(us8, e->sum_times, sizeof(e->sum_times));
     if (io2) { io2[0] = e->h2d_bytes; io2[1] = e->d2h_bytes; }
-    if (n2) { n2[0] = e->pframes; n2[1] = e->launches; }
+    if (n4) { n4[0] = e->pframes; n4[1] = e->launches; n4[2] = e->pdeferred; n4[3] = e->ptimed; }
     return RIV_OK;
 }
 

@@ -25,6 +25,31 @@ static_assert(sizeof(MbOut) == 20, "MbOut layout");
 // [15:8] coded sx, [7:0] coded sy.
 typedef unsigned long long MbRec;
 
+constexpr int RIV_PROF_WORDS = 32;  // i64 phase stamps per MB in SearchParams::prof
+
+struct ResidualParams {
+    const uint8_t* cur;   // planar YUV (Y then U then V)
+    const uint8_t* pred;  // planar YUV
+    uint8_t* recon;       // planar YUV (pre-deblock)
+    int16_t* coeffs;      // 384 per MB
+    uint8_t* opt_skip;    // 1 byte per MB
+    uint8_t* fmask;       // deblock mask, 1 byte per MB
+    uint8_t* eobs;        // 3 per MB (last non-zero index per plane block)
+    const MbOut* mb;      // nullptr for intra
+    const float* qs;      // per-MB quant step (inter)
+    float dead_zone;
+    int W, H, BW, intra;
+    const uint16_t* intra_ytab;  // 256 (intra)
+    const uint16_t* intra_ctab;  // 64 (intra)
+    // AQ step computed here from the ln variances and their mean (lnv != nullptr), else read qs
+    const float* lnv;            // n ln variances, then the mean
+    float aq_base;
+    const uint32_t* expfix;
+    int nexp;
+    float* qs_out;               // the steps, written for inspection
+    const uint8_t* ref;          // chroma prediction computed here from this reference (nullptr: read pred)
+};
+
 struct SearchParams {
     const uint8_t* ref_y;
     const uint8_t* cur_y;
@@ -54,7 +79,7 @@ struct SearchParams {
     int8_t* coded_out;  // coded MV (dx, dy, sx, sy) per MB: the next frame's temporal predictors
     unsigned* status;
     long long spin_limit;
-    long long* prof;  // optional: 16 words per MB (phase clock stamps, hexagon rounds), nullptr = off
+    long long* prof;  // optional: RIV_PROF_WORDS words per MB (phase stamps, hexagon rounds), nullptr = off
     int nrow_ctas;    // CTAs that own MB rows (row stride); the rest of the grid are table workers
     unsigned* tflag;  // fused table: per-MB flag = tag once its table row is written; nullptr = precomputed
     // Prediction and AQ inside the search launch (band + table instantiations): nullptr lnv =
@@ -65,30 +90,30 @@ struct SearchParams {
     unsigned* row_done;        // per MB row: tag once its ln variances are written
     const uint32_t* logfix;    // glibc logf fix-up pairs + bucket index
     int nlog;
+    // Residual and deblock of the previous P-frame, run by the table workers of this launch
+    // ahead of the table rows that need them (defer != 0), then (compact != 0) its compaction
+    // (scan + pack, as k_scan / k_pack) at the end of the queue.  wq: [0] task counter,
+    // [1 .. BH] residual MBs done per MB row, [BH+1 .. 2BH] deblock tiles done per band,
+    // [2BH+1] scan done.  Launches alternate between two such arrays: each zeroes the other
+    // (wq_next, wq_words words) for the next launch, its own having been zeroed by the last.
+    int defer;
+    ResidualParams dres;
+    int db_level, db_E, db_I, db_H;
+    const uint8_t* db_src;
+    uint8_t* db_dst;
+    const uint8_t* db_mask;
+    unsigned* wq;
+    unsigned* wq_next;
+    int wq_words;
+    int compact;
+    int32_t* c_index;
+    int32_t* c_offset;
+    uint32_t* c_side;
+    int16_t* c_packed;
+    uint8_t* c_peobs;
+    uint32_t* c_hdr;
 };
 
-struct ResidualParams {
-    const uint8_t* cur;   // planar YUV (Y then U then V)
-    const uint8_t* pred;  // planar YUV
-    uint8_t* recon;       // planar YUV (pre-deblock)
-    int16_t* coeffs;      // 384 per MB
-    uint8_t* opt_skip;    // 1 byte per MB
-    uint8_t* fmask;       // deblock mask, 1 byte per MB
-    uint8_t* eobs;        // 3 per MB (last non-zero index per plane block)
-    const MbOut* mb;      // nullptr for intra
-    const float* qs;      // per-MB quant step (inter)
-    float dead_zone;
-    int W, H, BW, intra;
-    const uint16_t* intra_ytab;  // 256 (intra)
-    const uint16_t* intra_ctab;  // 64 (intra)
-    // AQ step computed here from the ln variances and their mean (lnv != nullptr), else read qs
-    const float* lnv;            // n ln variances, then the mean
-    float aq_base;
-    const uint32_t* expfix;
-    int nexp;
-    float* qs_out;               // the steps, written for inspection
-    const uint8_t* ref;          // chroma prediction computed here from this reference (nullptr: read pred)
-};
 
 enum StatusBits : unsigned {
     ST_WAIT_TIMEOUT = 1u,

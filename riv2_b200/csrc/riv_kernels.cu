@@ -28,11 +28,8 @@ __constant__ int32_t c_T8[64];
 // pad_rgb24 (enc/encoder.rs:1049-1096) == reading the display frame at clamped
 // coordinates.  BT.709 limited range, 13-bit fixed point (same definition as the oracle).
 // ---------------------------------------------------------------------------------
-__global__ void k_rgb_to_yuv(const uint8_t* __restrict__ rgb, int dw, int dh, uint8_t* __restrict__ Yp,
-                             uint8_t* __restrict__ Up, uint8_t* __restrict__ Vp, int W, int H) {
-    int cx = blockIdx.x * blockDim.x + threadIdx.x;
-    int cy = blockIdx.y * blockDim.y + threadIdx.y;
-    if (cx >= W / 2 || cy >= H / 2) return;
+__device__ __forceinline__ void rgb_to_yuv_quad(const uint8_t* __restrict__ rgb, int dw, int dh, uint8_t* __restrict__ Yp,
+                                                uint8_t* __restrict__ Up, uint8_t* __restrict__ Vp, int W, int cx, int cy) {
     int sr = 0, sg = 0, sb = 0;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -51,9 +48,29 @@ __global__ void k_rgb_to_yuv(const uint8_t* __restrict__ rgb, int dw, int dh, ui
     Up[ci] = (uint8_t)min(max(cb, 16), 240);
     Vp[ci] = (uint8_t)min(max(cr, 16), 240);
 }
+// Grid-stride over the 2x2 quads (one chroma sample each), consecutive threads on
+// consecutive quads of a row.
+__global__ void k_rgb_to_yuv(const uint8_t* __restrict__ rgb, int dw, int dh, uint8_t* __restrict__ Yp,
+                             uint8_t* __restrict__ Up, uint8_t* __restrict__ Vp, int W, int H) {
+    const int cw = W / 2, nq = cw * (H / 2);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x)
+        rgb_to_yuv_quad(rgb, dw, dh, Yp, Up, Vp, W, q % cw, q / cw);
+}
 
 int launch_rgb_to_yuv(const uint8_t* rgb, int dw, int dh, uint8_t* yuv, int W, int H, void* stream) {
-    dim3 blk(64, 4), grd((W / 2 + 63) / 64, (H / 2 + 3) / 4);
+    // One 128-thread CTA (4K registers) per SM at most: every SM keeps room for a search CTA
+    // (61,440 registers), so a search launch never waits for a conversion to drain.
+    // Its preferred shared-memory carveout is the search kernel's (maximum shared memory), so
+    // an SM that ran a conversion CTA needs no reconfiguration before the next search CTA.
+    static int nsm = 0;
+    if (nsm == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            nsm = 1;
+        cudaFuncSetAttribute(k_rgb_to_yuv, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+    }
+    const int nq = (W / 2) * (H / 2);
+    const int blk = 128, grd = std::max(1, std::min(nsm, (nq + blk - 1) / blk));
     uint8_t* Y = yuv;
     uint8_t* U = yuv + (size_t)W * H;
     uint8_t* V = U + (size_t)(W / 2) * (H / 2);
@@ -336,13 +353,27 @@ __device__ __forceinline__ int argmin8(long long total, bool valid, long long& b
     return key == ~0ull ? -1 : (int)(key & 7);
 }
 
+// Phase stamps, written when p.prof is set: RIV_PROF_WORDS i64 per MB.  Words 0-15 are SM clock
+// cycles (clock64) of the search and mode warps; words 16-27 are %globaltimer nanoseconds,
+// comparable across SMs: 16/17 search warp MB start / slot ready; 18/19 deferred residual of
+// the MB pair starting here; 20/21/22 deblock tile (wait start, work start, end); 23/24/25
+// SAD-table MB (wait start, work start, end); 26/27 the row loader's wait for reference bands.
+__device__ __forceinline__ long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return (long long)t;
+}
 #define RIV_PUT(k, v)                                                      \
     do {                                                                    \
-        if (p.prof != nullptr && lane == 0) p.prof[(size_t)idx * 16 + (k)] = (v); \
+        if (p.prof != nullptr && lane == 0) p.prof[(size_t)idx * RIV_PROF_WORDS + (k)] = (v); \
     } while (0)
 #define RIV_STAMP(k)                                                        \
     do {                                                                    \
-        if (p.prof != nullptr && lane == 0) p.prof[(size_t)idx * 16 + (k)] = clock64(); \
+        if (p.prof != nullptr && lane == 0) p.prof[(size_t)idx * RIV_PROF_WORDS + (k)] = clock64(); \
+    } while (0)
+#define RIV_GSTAMP(mbi, k)                                                  \
+    do {                                                                    \
+        if (p.prof != nullptr) p.prof[(size_t)(mbi) * RIV_PROF_WORDS + (k)] = gtimer(); \
     } while (0)
 
 // Rounded bilinear sample at half-pel position (xh, yh) with the coordinates clamped to the
@@ -411,6 +442,452 @@ __device__ __forceinline__ void glibc_logf_batch(const float (&x)[FB], float (&y
 #pragma unroll
     for (int j = 0; j < FB; j++)
         if (lo[j] < n && __ldg(fix + 2 * lo[j]) == key[j]) y[j] = __uint_as_float(__ldg(fix + 2 * lo[j] + 1));
+}
+
+__device__ __forceinline__ int16_t f32_to_i16_sat(float f) {
+    if (f != f) return 0;
+    if (f <= -32768.0f) return -32768;
+    if (f >= 32767.0f) return 32767;
+    return (int16_t)__float2int_rz(f);
+}
+__device__ __forceinline__ int32_t f32_to_i32_sat(float f) {
+    if (f != f) return 0;
+    if (f <= -2147483648.0f) return INT_MIN;
+    if (f >= 2147483647.0f) return INT_MAX;
+    return __float2int_rz(f);
+}
+__device__ __forceinline__ int32_t wmul(int32_t a, int32_t b) { return (int32_t)((uint32_t)a * (uint32_t)b); }
+__device__ __forceinline__ int32_t wadd(int32_t a, int32_t b) { return (int32_t)((uint32_t)a + (uint32_t)b); }
+__device__ __forceinline__ int32_t wsub(int32_t a, int32_t b) { return (int32_t)((uint32_t)a - (uint32_t)b); }
+
+// AAN 8-point kernel with the reference's constants (dct/fast_dct8.rs:254-330).
+__device__ __forceinline__ void aan_1d(const int32_t s[8], int32_t out[8], int32_t bias, int shift) {
+    int32_t p1 = wmul(wadd(s[2], s[6]), 2218);
+    int32_t t2 = wadd(p1, wmul(s[6], -7572));
+    int32_t t3 = wadd(p1, wmul(s[2], 3136));
+    int32_t t0 = (int32_t)((uint32_t)wadd(s[0], s[4]) << 12);
+    int32_t t1 = (int32_t)((uint32_t)wsub(s[0], s[4]) << 12);
+    int32_t x0 = wadd(wadd(t0, t3), bias), x3 = wadd(wsub(t0, t3), bias);
+    int32_t x1 = wadd(wadd(t1, t2), bias), x2 = wadd(wsub(t1, t2), bias);
+    int32_t a0 = s[7], a1 = s[5], a2 = s[3], a3 = s[1];
+    int32_t q3 = wadd(a0, a2), q4 = wadd(a1, a3), q1 = wadd(a0, a3), q2 = wadd(a1, a2);
+    int32_t q5 = wmul(wadd(q3, q4), 4817);
+    a0 = wmul(a0, 1223); a1 = wmul(a1, 8411); a2 = wmul(a2, 12595); a3 = wmul(a3, 6150);
+    q1 = wadd(q5, wmul(q1, -3685));
+    q2 = wadd(q5, wmul(q2, -10496));
+    q3 = wmul(q3, -8035);
+    q4 = wmul(q4, -1598);
+    int32_t u3 = wadd(a3, wadd(q1, q4)), u2 = wadd(a2, wadd(q2, q3));
+    int32_t u1 = wadd(a1, wadd(q2, q4)), u0 = wadd(a0, wadd(q1, q3));
+    out[0] = wadd(x0, u3) >> shift; out[7] = wsub(x0, u3) >> shift;
+    out[1] = wadd(x1, u2) >> shift; out[6] = wsub(x1, u2) >> shift;
+    out[2] = wadd(x2, u1) >> shift; out[5] = wsub(x2, u1) >> shift;
+    out[3] = wadd(x3, u0) >> shift; out[4] = wsub(x3, u0) >> shift;
+}
+
+// Four MBs per CTA, 64 threads (two warps) per MB.  Thread u of an MB owns luma row u >> 2,
+// columns 4 * (u & 3) .. +3 in every 16x16 pass, and two adjacent chroma samples (plane
+// u >> 5).  Each pass reads one basis row and one data row per term as 128-bit shared loads,
+// four multiply-accumulates per pair of loads.  Per-MB named barriers (ids 1..4, 64 threads).
+__device__ __forceinline__ void mb_sync(int bar) { asm volatile("bar.sync %0, 64;" ::"r"(bar) : "memory"); }
+// Dequantisation and inverse transforms of one MB and its reconstruction onto the prediction
+// (dct/dct16.rs:345-412, dct/fast_dct8.rs:69-174, res/residual.rs:740-752), shared by the
+// encoder's residual kernel and the decoder.  64 threads per MB (named barrier bar, thread u: luma row
+// yy, columns xb..xb+3; own quantised luma ql); Qc = the MB's 128 chroma coefficients and
+// predc its chroma prediction in shared memory; R, RT, aant = per-MB shared scratch.
+__device__ __forceinline__ void inverse_mb(int bar, int u, int yy, int xb, const int16_t (&ql)[4], float qsv, bool intra,
+                                           const uint16_t* ytab, const uint16_t* ctab, uint32_t lbase, uint8_t* ry,
+                                           uint8_t* rU, uint8_t* rV, int CW, int x0, int y0, const int32_t* sT16,
+                                           const int32_t* sT16t, int32_t* R, int32_t* RT, int32_t* aant,
+                                           const int16_t* Qc, const uint8_t* predc) {
+    // dequantisation + 16x16 inverse (row pass over u, then column pass over v)
+    {
+        int32_t d[4];
+        if (intra) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) d[k] = (int32_t)ql[k] * max((int)ytab[yy * 16 + xb + k], 1);
+        } else {
+            const int32_t qfp = f32_to_i32_sat(roundf(__fmul_rn(qsv, 16384.0f)));
+#pragma unroll
+            for (int k = 0; k < 4; k++) d[k] = wadd(wmul((int32_t)ql[k], qfp), 8192) >> 14;
+        }
+        *(int4*)(R + yy * 16 + xb) = make_int4(d[0], d[1], d[2], d[3]);
+    }
+    mb_sync(bar);
+    {  // rows[v][x] = (sum_i deq[v][i] * T[x][i] + 2^17) >> 18, wrapping   (v = yy)
+        uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const uint32_t r = (uint32_t)R[yy * 16 + i];
+            const int4 t = *(const int4*)(sT16t + i * 16 + xb);
+            a0 += r * (uint32_t)t.x; a1 += r * (uint32_t)t.y; a2 += r * (uint32_t)t.z; a3 += r * (uint32_t)t.w;
+        }
+        *(int4*)(RT + yy * 16 + xb) = make_int4((int32_t)(a0 + (1u << 17)) >> 18, (int32_t)(a1 + (1u << 17)) >> 18,
+                                                (int32_t)(a2 + (1u << 17)) >> 18, (int32_t)(a3 + (1u << 17)) >> 18);
+    }
+    mb_sync(bar);
+    {  // out[y][x] = (sum_v rows[v][x] * T[y][v] + 2^17) >> 18   (y = yy)
+        uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll
+        for (int v = 0; v < 16; v++) {
+            const int4 r = *(const int4*)(RT + v * 16 + xb);
+            const uint32_t t = (uint32_t)sT16[yy * 16 + v];
+            a0 += (uint32_t)r.x * t; a1 += (uint32_t)r.y * t; a2 += (uint32_t)r.z * t; a3 += (uint32_t)r.w * t;
+        }
+        const uint32_t acc[4] = {a0, a1, a2, a3};
+        const uint32_t bv = lbase;
+        uint32_t o = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            int32_t r = (int32_t)(acc[k] + (1u << 17)) >> 18;
+            r = min(max(r, -32768), 32767);
+            const int base = (int)((bv >> (8 * k)) & 255u);
+            o |= (uint32_t)min(max(base + r, 0), 255) << (8 * k);
+        }
+        *(uint32_t*)ry = o;
+    }
+    // chroma 8x8 AAN inverse: pass 1 over u for each (plane, v); pass 2 over v for each (plane, x)
+    if (u < 16) {
+        const int cp = u >> 3, v = u & 7;
+        int32_t sv[8], o[8];
+        int32_t qa = 0;
+        if (!intra) {
+            float qr = roundf(qsv);
+            qr = qr < 1.0f ? 1.0f : qr;
+            qa = qr >= 65535.0f ? 65535 : (int32_t)qr;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const int32_t qq = intra ? max((int)ctab[v * 8 + k], 1) : qa;
+            sv[k] = (int32_t)Qc[cp * 64 + v * 8 + k] * qq;
+        }
+        aan_1d(sv, o, 512, 10);
+#pragma unroll
+        for (int x = 0; x < 8; x++) aant[cp * 64 + x * 8 + v] = o[x];
+    }
+    mb_sync(bar);
+    if (u < 16) {
+        const int cp = u >> 3, x = u & 7;
+        int32_t sv[8], o[8];
+#pragma unroll
+        for (int v = 0; v < 8; v++) sv[v] = aant[cp * 64 + x * 8 + v];
+        aan_1d(sv, o, 65536, 17);
+        uint8_t* Rr = cp == 0 ? rU : rV;
+#pragma unroll
+        for (int y = 0; y < 8; y++) {
+            const int r = min(max(o[y], -32768), 32767);
+            const size_t i = (size_t)(y0 / 2 + y) * CW + x0 / 2 + x;
+            const int base = intra ? 128 : (int)predc[cp * 64 + y * 8 + x];
+            Rr[i] = (uint8_t)min(max(base + r, 0), 255);
+        }
+    }
+}
+
+constexpr int RS_MB = 4;
+
+// Per-MB shared scratch of the residual (one 64-thread group).
+struct __align__(16) ResSmem {  // 16-byte rows: element k of an array must stay aligned
+    int32_t res[256], rowt[256], resc[128], rowc[128];
+    int16_t q[384];
+    int32_t aant[2][64];
+    int flags[4];  // luma eob of warp 0 / warp 1, (chroma eob << 1 | any non-zero) of warp 0 / warp 1
+    float qsh;
+    uint8_t predc[128];  // chroma prediction (U then V, 8x8 each)
+};
+
+// Residual, transforms, quantisation and reconstruction of MB mb by 64 threads (u = 0..63)
+// synchronised on named barrier `bar`; sT16 / sT16t / sT8 hold the bases (sT16t transposed).
+__device__ __forceinline__ void residual_mb(const ResidualParams& p, int nmb, int mb, int u, int bar, ResSmem& S,
+                                            const int32_t* sT16, const int32_t* sT16t, const int32_t* sT8) {
+    const int BW = p.BW, W = p.W, H = p.H, CW = W / 2, CH = H / 2;
+    const int bx = mb % BW, by = mb / BW;
+    const int x0 = bx * 16, y0 = by * 16;
+    const uint8_t *cY = p.cur, *cU = p.cur + (size_t)W * H, *cV = cU + (size_t)CW * CH;
+    const uint8_t *pY = p.pred, *pU = p.pred + (size_t)W * H, *pV = pU + (size_t)CW * CH;
+    uint8_t *rY = p.recon, *rU = p.recon + (size_t)W * H, *rV = rU + (size_t)CW * CH;
+    const int yy = u >> 2, xb = (u & 3) * 4;
+    const size_t yi = (size_t)(y0 + yy) * W + x0 + xb;
+    const int pl = u >> 5, ci = (u & 31) * 2, cyy = ci >> 3, cxx = ci & 7;
+    const size_t cidx = (size_t)(y0 / 2 + cyy) * CW + x0 / 2 + cxx;
+    const uint8_t* cC = pl == 0 ? cU : cV;
+    const uint8_t* pC = pl == 0 ? pU : pV;
+    uint8_t* rC = pl == 0 ? rU : rV;
+    int32_t* R = S.res;
+    int32_t* RT = S.rowt;
+    int32_t* RC = S.resc;
+    int32_t* RCT = S.rowc;
+    int16_t* Q = S.q;
+
+    // chroma prediction of this thread's two samples: computed here from the reference planes
+    // (build_predicted's chroma rule, com/fast_motion.rs:264-345) or read from pred
+    uint32_t pcw;
+    if (!p.intra && p.ref != nullptr) {
+        const MbOut m = p.mb[mb];
+        const int mdx = m.raw[0] * 2 + m.raw[2], mdy = m.raw[1] * 2 + m.raw[3];
+        const bool integer = ((mdx & 1) == 0) && ((mdy & 1) == 0);
+        const int sx0 = x0 + (mdx >> 1), sy0 = y0 + (mdy >> 1);
+        const bool copy = integer && sx0 >= 0 && sy0 >= 0 && sx0 + 15 < W && sy0 + 15 < H;
+        const uint8_t* Rp = p.ref + (size_t)W * H + (pl == 0 ? 0 : (size_t)CW * CH);
+        const int cyg = y0 / 2 + cyy;
+        int c2[2];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const int cxg = x0 / 2 + cxx + k;
+            c2[k] = copy ? Rp[(size_t)(sy0 / 2 + cyy) * CW + sx0 / 2 + cxx + k]
+                         : sample_round(Rp, CW, CH, 2 * cxg + (mdx >> 1), 2 * cyg + (mdy >> 1));
+        }
+        pcw = (uint32_t)c2[0] | ((uint32_t)c2[1] << 8);
+    } else {
+        pcw = p.intra ? 0x8080u : *(const uint16_t*)(pC + cidx);
+    }
+    S.predc[pl * 64 + ci] = (uint8_t)pcw;
+    S.predc[pl * 64 + ci + 1] = (uint8_t)(pcw >> 8);
+    auto copy_pred = [&]() {  // recon = prediction, coefficients zero
+        *(uint32_t*)(rY + yi) = *(const uint32_t*)(pY + yi);
+        *(uint16_t*)(rC + cidx) = (uint16_t)pcw;
+        int16_t* co = p.coeffs + (size_t)mb * 384;
+        *(uint2*)(co + yy * 16 + xb) = make_uint2(0u, 0u);
+        *(uint32_t*)(co + 256 + pl * 64 + ci) = 0u;
+        if (u == 0) {
+            p.opt_skip[mb] = 1;
+            const int8_t* c = p.mb[mb].coded;
+            p.fmask[mb] = (c[0] | c[1] | c[2] | c[3]) != 0;
+            p.eobs[3 * mb] = p.eobs[3 * mb + 1] = p.eobs[3 * mb + 2] = 0;
+        }
+    };
+    if (!p.intra && p.lnv != nullptr) {  // AQ step (compute_aq_quant_steps, res/residual.rs:154-167)
+        if (u == 0) {
+            const float off = __fmul_rn(0.8f, __fsub_rn(p.lnv[mb], p.lnv[nmb]));
+            const float q = __fmul_rn(p.aq_base, glibc_exp2f(__fdiv_rn(off, 6.0f), p.expfix, p.nexp));
+            S.qsh = q;
+            p.qs_out[mb] = q;
+        }
+        mb_sync(bar);
+    }
+    if (!p.intra && p.mb[mb].rdo_skip) {  // never transformed: residual 0, recon = prediction
+        copy_pred();
+        return;
+    }
+    {
+        const uint32_t cv = *(const uint32_t*)(cY + yi);
+        const uint32_t pv = p.intra ? 0x80808080u : *(const uint32_t*)(pY + yi);
+#pragma unroll
+        for (int k = 0; k < 4; k++) R[yy * 16 + xb + k] = (int)((cv >> (8 * k)) & 255u) - (int)((pv >> (8 * k)) & 255u);
+        const uint32_t cc = *(const uint16_t*)(cC + cidx);
+        const uint32_t pc = pcw;
+        RC[pl * 64 + ci] = (int)(cc & 255u) - (int)(pc & 255u);
+        RC[pl * 64 + ci + 1] = (int)(cc >> 8) - (int)(pc >> 8);
+    }
+    mb_sync(bar);
+    // The reference accumulates both FDCT passes in i64 and clamps to i32.  With residuals in
+    // [-255, 255] and these bases, every partial sum stays below 2^31 (16x16: row pass
+    // <= 255 * 1048576 = 2.7e8, rows <= 1020, column pass <= 1020 * 1048576 + 2^17 = 1.07e9;
+    // 8x8: 1.9e8, 721, 5.3e8), so exact int32 accumulation gives the same values and the
+    // clamp never applies.
+    {  // row pass: rowt[y][j] = sum_i res[y][i] * T[i][j]
+        int32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const int r = R[yy * 16 + i];
+            const int4 t = *(const int4*)(sT16 + i * 16 + xb);
+            a0 += r * t.x; a1 += r * t.y; a2 += r * t.z; a3 += r * t.w;
+        }
+        *(int4*)(RT + yy * 16 + xb) = make_int4((a0 + (1 << 17)) >> 18, (a1 + (1 << 17)) >> 18,
+                                                (a2 + (1 << 17)) >> 18, (a3 + (1 << 17)) >> 18);
+        int32_t c0 = 0, c1 = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int r = RC[pl * 64 + cyy * 8 + i];
+            const int2 t = *(const int2*)(sT8 + i * 8 + cxx);
+            c0 += r * t.x; c1 += r * t.y;
+        }
+        *(int2*)(RCT + pl * 64 + ci) = make_int2((c0 + (1 << 17)) >> 18, (c1 + (1 << 17)) >> 18);
+    }
+    mb_sync(bar);
+    int32_t coef[4], coefc[2];
+    {  // column pass: coef[v][x] = sum_i rowt[i][x] * T[i][v]   (v = yy)
+        int32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const int4 r = *(const int4*)(RT + i * 16 + xb);
+            const int t = sT16[i * 16 + yy];
+            a0 += r.x * t; a1 += r.y * t; a2 += r.z * t; a3 += r.w * t;
+        }
+        coef[0] = (a0 + (1 << 17)) >> 18; coef[1] = (a1 + (1 << 17)) >> 18;
+        coef[2] = (a2 + (1 << 17)) >> 18; coef[3] = (a3 + (1 << 17)) >> 18;
+        int32_t c0 = 0, c1 = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int2 r = *(const int2*)(RCT + pl * 64 + i * 8 + cxx);
+            const int t = sT8[i * 8 + cyy];
+            c0 += r.x * t; c1 += r.y * t;
+        }
+        coefc[0] = (c0 + (1 << 17)) >> 18; coefc[1] = (c1 + (1 << 17)) >> 18;
+    }
+    // quantisation
+    float qsv = 0.0f;
+    int16_t ql[4], qc[2];
+    if (p.intra) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const float qy = (float)max((int)p.intra_ytab[yy * 16 + xb + k], 1);
+            ql[k] = f32_to_i16_sat(roundf(__fdiv_rn(__int2float_rn(coef[k]), qy)));
+        }
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const float qq = (float)max((int)p.intra_ctab[ci + k], 1);
+            qc[k] = f32_to_i16_sat(roundf(__fdiv_rn(__int2float_rn(coefc[k]), qq)));
+        }
+    } else {
+        qsv = p.lnv != nullptr ? S.qsh : p.qs[mb];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const float r = __fdiv_rn(__int2float_rn(coef[k]), qsv);
+            ql[k] = fabsf(r) < p.dead_zone ? (int16_t)0 : f32_to_i16_sat(roundf(r));
+        }
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const float r = __fdiv_rn(__int2float_rn(coefc[k]), qsv);
+            qc[k] = fabsf(r) < p.dead_zone ? (int16_t)0 : f32_to_i16_sat(roundf(r));
+        }
+    }
+    // last non-zero index per plane block (0 when all zero) and "any non-zero"
+    int lz = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) lz = ql[k] != 0 ? yy * 16 + xb + k : lz;
+    int lc = 0;
+#pragma unroll
+    for (int k = 0; k < 2; k++) lc = qc[k] != 0 ? ci + k : lc;
+    const bool any = (ql[0] | ql[1] | ql[2] | ql[3] | qc[0] | qc[1]) != 0;
+    lz = __reduce_max_sync(0xffffffffu, lz);
+    lc = __reduce_max_sync(0xffffffffu, lc);
+    const unsigned anyw = __any_sync(0xffffffffu, any);
+    if ((u & 31) == 0) {
+        S.flags[u >> 5] = lz;
+        S.flags[2 + (u >> 5)] = (int)anyw | (lc << 1);
+    }
+    mb_sync(bar);
+    const bool nz = ((S.flags[2] | S.flags[3]) & 1) != 0;
+    if (!p.intra && !nz) {  // became all-zero after quantisation: optimized skip
+        copy_pred();
+        return;
+    }
+    {
+        int16_t* co = p.coeffs + (size_t)mb * 384;
+        const uint32_t w0 = (uint32_t)(uint16_t)ql[0] | ((uint32_t)(uint16_t)ql[1] << 16);
+        const uint32_t w1 = (uint32_t)(uint16_t)ql[2] | ((uint32_t)(uint16_t)ql[3] << 16);
+        *(uint2*)(co + yy * 16 + xb) = make_uint2(w0, w1);
+        *(uint32_t*)(co + 256 + pl * 64 + ci) = (uint32_t)(uint16_t)qc[0] | ((uint32_t)(uint16_t)qc[1] << 16);
+        Q[256 + pl * 64 + ci] = qc[0];
+        Q[256 + pl * 64 + ci + 1] = qc[1];
+        if (u == 0) {
+            p.eobs[3 * mb] = (uint8_t)max(S.flags[0], S.flags[1]);
+            p.eobs[3 * mb + 1] = (uint8_t)(S.flags[2] >> 1);
+            p.eobs[3 * mb + 2] = (uint8_t)(S.flags[3] >> 1);
+            p.opt_skip[mb] = 0;
+            p.fmask[mb] = 1;
+        }
+    }
+    const uint32_t lbase = p.intra ? 0x80808080u : *(const uint32_t*)(pY + yi);
+    inverse_mb(bar, u, yy, xb, ql, qsv, p.intra != 0, p.intra_ytab, p.intra_ctab, lbase, rY + yi, rU, rV, CW, x0, y0,
+               sT16, sT16t, R, RT, S.aant[0], Q + 256, S.predc);
+}
+
+__device__ __forceinline__ int c128(int x) { return min(max(x, -128), 127); }
+__device__ __forceinline__ void filter_line(int* px, int E, int I, int Hv) {
+    int p3 = px[0], p2 = px[1], p1 = px[2], p0 = px[3], q0 = px[4], q1 = px[5], q2 = px[6], q3 = px[7];
+    bool mask = 2 * abs(p0 - q0) + abs(q1 - p1) / 2 <= E && abs(p3 - p2) <= I && abs(p2 - p1) <= I &&
+                abs(p1 - p0) <= I && abs(q1 - q0) <= I && abs(q2 - q1) <= I && abs(q3 - q2) <= I;
+    if (!mask) return;
+    int ps2 = p2 - 128, ps1 = p1 - 128, ps0 = p0 - 128, qs0 = q0 - 128, qs1 = q1 - 128, qs2 = q2 - 128;
+    bool hev = abs(p1 - p0) > Hv || abs(q1 - q0) > Hv;
+    int w = c128(c128(ps1 - qs1) + 3 * (qs0 - ps0));
+    if (hev) {
+        int f1 = c128(w + 4) >> 3, f2 = c128(w + 3) >> 3;
+        px[4] = min(max(c128(qs0 - f1) + 128, 0), 255);
+        px[3] = min(max(c128(ps0 + f2) + 128, 0), 255);
+    } else {
+        int a = c128((27 * w + 63) >> 7);
+        int nq0 = c128(qs0 - a), np0 = c128(ps0 + a);
+        a = c128((18 * w + 63) >> 7);
+        int nq1 = c128(qs1 - a), np1 = c128(ps1 + a);
+        a = c128((9 * w + 63) >> 7);
+        int nq2 = c128(qs2 - a), np2 = c128(ps2 + a);
+        px[1] = min(max(np2 + 128, 0), 255);
+        px[2] = min(max(np1 + 128, 0), 255);
+        px[3] = min(max(np0 + 128, 0), 255);
+        px[4] = min(max(nq0 + 128, 0), 255);
+        px[5] = min(max(nq1 + 128, 0), 255);
+        px[6] = min(max(nq2 + 128, 0), 255);
+    }
+}
+// Out of place, all planes in one launch (src and dst must not overlap: neighbouring tiles
+// read each other's pixels as halo).  A CTA owns one band of an edge grid (16 luma / 8
+// chroma rows) and DB_TW luma (DB_TW/2 chroma) columns.  It loads the tile with a 4-pixel
+// halo, filters every vertical edge of the halo rows in shared memory (rows are independent
+// in that pass), then the horizontal edges at the band's top and bottom (their lines are 4+
+// pixels apart, so they touch disjoint pixels), and stores only its own pixels.  That equals
+// the reference's whole-plane vertical pass followed by the whole-plane horizontal pass.
+constexpr int DB_TW = 128;
+constexpr int DB_TILE_BYTES = (16 + 8) * (DB_TW + 8);
+// One tile (plane, t: band-major tile index within the plane) by nthr threads synchronised on
+// group barrier `bar` (0 = the whole CTA); `tile` = DB_TILE_BYTES of shared memory.
+__device__ __forceinline__ void deblock_tile(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, int W, int H,
+                                             int BW, int E, int I, int Hv, const uint8_t* mask, int plane, int t,
+                                             uint8_t* tile, int tid, int nthr, int bar) {
+    const int w = plane ? W / 2 : W, h = plane ? H / 2 : H, g = plane ? 8 : 16, tw = plane ? DB_TW / 2 : DB_TW;
+    const size_t poff = plane == 0 ? 0 : (size_t)W * H + (plane == 2 ? (size_t)(W / 2) * (H / 2) : 0);
+    const uint8_t* pl = src + poff;
+    uint8_t* po = dst + poff;
+    const int tpb = (w + tw - 1) / tw;
+    const int band = t / tpb, X0 = (t % tpb) * tw, X1 = min(X0 + tw, w);
+    const int Y0 = band * g, Y1 = Y0 + g;
+    const int ry0 = max(Y0 - 4, 0), ry1 = min(Y1 + 4, h), cx0 = max(X0 - 4, 0), cx1 = min(X1 + 4, w);
+    const int TS = DB_TW + 8, oy = Y0 - 4, ox = X0 - 4;  // tile row stride and origin
+    const int nrow = ry1 - ry0, ncol = cx1 - cx0;
+    for (int i = tid; i < nrow * ncol; i += nthr) {
+        const int r = i / ncol, c = i - r * ncol;
+        tile[(ry0 + r - oy) * TS + cx0 + c - ox] = pl[(size_t)(ry0 + r) * w + cx0 + c];
+    }
+    group_sync(bar, nthr);
+    // vertical edges x = k*g (1 <= k < w/g) with X0 <= x <= X1, on every loaded row
+    const int k0 = max(1, (X0 + g - 1) / g), k1 = min(w / g - 1, X1 / g);
+    const int nk = k1 - k0 + 1;
+    if (nk > 0) {
+        for (int i = tid; i < nrow * nk; i += nthr) {
+            const int r = i / nk, k = k0 + (i - r * nk), y = ry0 + r;
+            const int by = y / g;
+            if (mask && !(mask[by * BW + k - 1] | mask[by * BW + k])) continue;
+            uint8_t* sp = tile + (y - oy) * TS + k * g - 4 - ox;
+            int px[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) px[q] = sp[q];
+            filter_line(px, E, I, Hv);
+#pragma unroll
+            for (int q = 1; q < 7; q++) sp[q] = (uint8_t)px[q];
+        }
+    }
+    group_sync(bar, nthr);
+    // horizontal edges at the band's top (Y0) and bottom (Y1), columns X0 .. X1-1
+    for (int i = tid; i < 2 * (X1 - X0); i += nthr) {
+        const int e = (i < X1 - X0 ? Y0 : Y1) / g, x = X0 + (i < X1 - X0 ? i : i - (X1 - X0));
+        if (e < 1 || e >= h / g) continue;
+        const int bxm = x / g;
+        if (mask && !(mask[(e - 1) * BW + bxm] | mask[e * BW + bxm])) continue;
+        uint8_t* sp = tile + (e * g - 4 - oy) * TS + x - ox;
+        int px[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) px[q] = sp[q * TS];
+        filter_line(px, E, I, Hv);
+#pragma unroll
+        for (int q = 1; q < 7; q++) sp[q * TS] = (uint8_t)px[q];
+    }
+    group_sync(bar, nthr);
+    const int ow = X1 - X0;
+    for (int i = tid; i < g * ow; i += nthr) {
+        const int r = i / ow, c = i - r * ow;
+        po[(size_t)(Y0 + r) * w + X0 + c] = tile[(Y0 + r - oy) * TS + X0 + c - ox];
+    }
 }
 
 // ---- search warp -> mode warp handoff through a shared-memory ring (one CTA per MB row)
@@ -620,22 +1097,295 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
     return v;
 }
 
-constexpr int TW_GROUP = 128;  // threads per table-worker group (one MB at a time)
-__device__ __forceinline__ void table_worker(const SearchParams& p, uint8_t* sm) {
-    const int groups = blockDim.x / TW_GROUP, g = threadIdx.x / TW_GROUP, tid = threadIdx.x % TW_GROUP;
-    if (g >= groups) return;
-    const int nw = (gridDim.x - p.nrow_ctas) * groups, w = (blockIdx.x - p.nrow_ctas) * groups + g;
-    uint8_t* gsm = sm + (size_t)g * sad_table_smem_dev(p.sr);
-    const int n = p.BW * p.BH;
-    for (int mb = w; mb < n; mb += nw) {
-        sad_table_mb(p.ref_y, p.cur_y, p.W, p.H, p.BW, p.sr, const_cast<uint16_t*>(p.tab), p.tstride, mb, gsm, tid,
-                     TW_GROUP, 1 + g);
-        group_sync(1 + g, TW_GROUP);
-        if (tid == 0) {
-            __threadfence();
-            st_release_u32(p.tflag + mb, p.tag);
+constexpr int TW_GROUP = 128;  // threads per worker group
+constexpr int RES_HALF_BYTES = (sizeof(ResSmem) + 15) & ~15;
+static_assert(sizeof(ResSmem) % 16 == 0 && offsetof(ResSmem, q) % 16 == 0 && offsetof(ResSmem, aant) % 16 == 0, "ResSmem rows");
+__host__ __device__ constexpr int worker_group_bytes() {
+    return 2 * RES_HALF_BYTES > DB_TILE_BYTES + 16 ? 2 * RES_HALF_BYTES : DB_TILE_BYTES + 16;
+}
+constexpr int WK_BASES = 2304;  // sT16, sT16t, sT8 of the deferred residual
+static_assert(WK_BASES + 4 * worker_group_bytes() + 2 * 4 * 4 <= 116 * 1024, "worker CTA shared memory");
+
+// Bounded wait until *c >= target (acquire); every thread of the group polls.
+__device__ __forceinline__ bool wait_at_least(const unsigned* c, unsigned target, long long limit) {
+    long long spins = 0;
+    while (ld_acquire_u32(c) < target) {
+        if (++spins > limit) return false;
+        __nanosleep(64);
+    }
+    return true;
+}
+// The rows / bands MB row r depends on before its reference samples may be read: the
+// previous frame's deblocked bands r-1 .. r+1 (or its residual rows when it has no deblock).
+__device__ __forceinline__ bool wait_ref_rows(const SearchParams& p, int r, int tiles_per_band) {
+    if (!p.defer) return true;
+    for (int b = max(r - 1, 0); b <= min(r + 1, p.BH - 1); b++) {
+        const bool ok = p.db_level > 0 ? wait_at_least(p.wq + 1 + p.BH + b, (unsigned)tiles_per_band, p.spin_limit)
+                                       : wait_at_least(p.wq + 1 + b, (unsigned)p.BW, p.spin_limit);
+        if (!ok) return false;
+    }
+    return true;
+}
+__host__ __device__ inline int deblock_tiles_per_band(int W) {
+    return (W + DB_TW - 1) / DB_TW + 2 * ((W / 2 + DB_TW / 2 - 1) / (DB_TW / 2));
+}
+
+// ---------------------------------------------------------------------------------
+// K8 helpers: per-MB side info and compaction of the coded MBs' coefficients for the host
+// entropy coder.  side = mode | base<<3 | subx<<6 | suby<<7 | rdx<<8 | rdy<<16 | optskip<<24.
+// Each coded MB contributes its three plane blocks truncated after the last non-zero
+// coefficient (the entropy coder never reads beyond it): Y[0..eY], U[0..eU], V[0..eV].
+// hdr[0] = coded MB count, hdr[1] = total coefficients written.
+// ---------------------------------------------------------------------------------
+// Scan by NT threads (named barrier `bar`): each thread owns IPT consecutive MBs of an
+// NT * IPT chunk (all their loads are issued together), then one scan of the thread totals
+// per chunk.  wsum / wsz: NT / 32 ints of shared memory each.
+constexpr int SC_THREADS = 256, SC_IPT = 32;
+template <int NT, int IPT>
+__device__ __forceinline__ void scan_mbs(const uint8_t* opt_skip, const uint8_t* eobs, int nmb, int intra,
+                                         int32_t* index, int32_t* offset, uint32_t* hdr, int tid, int bar, int* wsum,
+                                         int* wsz) {
+    const int lane = tid & 31, wid = tid >> 5;
+    int carry = 0, carry_sz = 0;  // identical in every thread
+    for (int base = 0; base < nmb; base += NT * IPT) {
+        const int i0 = base + tid * IPT;
+        // v = coded << 16 | coefficient count (<= 3 * 256): 32 of them sum without carry
+        uint32_t v[IPT];
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            const int i = i0 + k;
+            const bool f = i < nmb && (intra || !opt_skip[i]);
+            v[k] = f ? (1u << 16) | (uint32_t)(eobs[3 * i] + eobs[3 * i + 1] + eobs[3 * i + 2] + 3) : 0u;
         }
-        group_sync(1 + g, TW_GROUP);
+        uint32_t tot = 0;
+#pragma unroll
+        for (int k = 0; k < IPT; k++) tot += v[k];
+        const int x = (int)(tot >> 16), y = (int)(tot & 0xffffu);
+        int xs = x, ys = y;  // inclusive warp scan of the thread totals
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int a2 = __shfl_up_sync(0xffffffffu, xs, o), b2 = __shfl_up_sync(0xffffffffu, ys, o);
+            if (lane >= o) { xs += a2; ys += b2; }
+        }
+        if (lane == 31) { wsum[wid] = xs; wsz[wid] = ys; }
+        group_sync(bar, NT);
+        int wx = 0, wy = 0, tx = 0, ty = 0;  // exclusive prefix of this warp, chunk totals
+#pragma unroll
+        for (int q = 0; q < NT / 32; q++) {
+            if (q < wid) { wx += wsum[q]; wy += wsz[q]; }
+            tx += wsum[q];
+            ty += wsz[q];
+        }
+        int ex = carry + wx + xs - x;
+        int ez = carry_sz + wy + ys - y;
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            const int i = i0 + k;
+            const int f = (int)(v[k] >> 16), z = (int)(v[k] & 0xffffu);
+            if (i < nmb) { index[i] = f ? ex : -1; offset[i] = ez; }
+            ex += f;
+            ez += z;
+        }
+        carry += tx;
+        carry_sz += ty;
+        group_sync(bar, NT);  // wsum / wsz are rewritten by the next chunk
+    }
+    if (tid == 0) { hdr[0] = (uint32_t)carry; hdr[1] = (uint32_t)carry_sz; }
+}
+// Pack MB m with one warp: side info, EOBs and the truncated coefficient blocks.
+__device__ __forceinline__ void pack_mb(int m, int lane, const uint8_t* opt_skip, const MbOut* mb,
+                                        const int16_t* coeffs, const uint8_t* eobs, const int32_t* index,
+                                        const int32_t* offset, int intra, uint32_t* side, int16_t* packed,
+                                        uint8_t* peobs) {
+    const int k = index[m];
+    const int e0 = eobs[3 * m], e1 = eobs[3 * m + 1], e2 = eobs[3 * m + 2];
+    if (lane == 0) {
+        uint32_t s = 0;
+        if (!intra) {
+            const MbOut o = mb[m];
+            s = (uint32_t)o.mode | ((uint32_t)o.base << 3) | ((uint32_t)(o.raw[2] & 1) << 6) |
+                ((uint32_t)(o.raw[3] & 1) << 7) | ((uint32_t)(uint8_t)o.rdelta[0] << 8) |
+                ((uint32_t)(uint8_t)o.rdelta[1] << 16) | ((uint32_t)(opt_skip[m] & 1) << 24);
+        }
+        side[m] = s;
+        if (k >= 0) {
+            peobs[3 * k] = (uint8_t)e0;
+            peobs[3 * k + 1] = (uint8_t)e1;
+            peobs[3 * k + 2] = (uint8_t)e2;
+        }
+    }
+    if (k < 0) return;
+    const int n0 = e0 + 1, n1 = e1 + 1, n2 = e2 + 1;
+    const int16_t* src = coeffs + (size_t)m * 384;
+    int16_t* dst = packed + offset[m];
+    for (int i = lane; i < n0 + n1 + n2; i += 32) {
+        const int si = i < n0 ? i : (i < n0 + n1 ? 256 + (i - n0) : 320 + (i - n0 - n1));
+        dst[i] = src[si];
+    }
+}
+
+// The worker CTAs of the fused search launch (the CTAs beyond the row CTAs), in groups of 128
+// threads that take tasks from one queue in a fixed order: for step k, the previous frame's
+// residual of MB row k (pairs of MBs), its deblock of band k-DB_LAG (tiles), then the
+// SAD-table MBs of row k-TAB_LAG (k when nothing is deferred).  Each task waits only for
+// tasks earlier in the queue (residual rows b-1 .. b+1 for band b, deblocked bands r-1 .. r+1
+// for table row r), all of which are held by running groups of this cooperative launch, so
+// the waits end; the lags put two steps (more tasks than there are groups) between a task
+// and what it waits for, so a group rarely holds a task whose inputs are still being made.
+// One thread per group polls; the group barrier then orders the others' reads after its
+// acquire.  Completion is published with release operations: per-row / per-band counters in
+// wq, per-MB table flags (the frame tag) that the loaders acquire.  With p.compact the queue
+// ends with the previous frame's compaction: one scan task (after every residual row), then
+// one pack task per MB row (after the scan, published in wq[2BH+1]).
+constexpr int DB_LAG = 3, TAB_LAG = 6;
+constexpr int WK_SCAN_IPT = 8;  // MBs per thread of the in-launch scan (registers are capped)
+__device__ __forceinline__ void frame_worker(const SearchParams& p, uint8_t* sm) {
+    const int groups = blockDim.x / TW_GROUP, g = threadIdx.x / TW_GROUP, tid = threadIdx.x % TW_GROUP;
+    int32_t* sT16 = (int32_t*)sm;
+    int32_t* sT16t = sT16 + 256;
+    int32_t* sT8 = sT16t + 256;
+    if (p.defer) {
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+            sT16[i] = c_T16[i];
+            sT16t[(i & 15) * 16 + (i >> 4)] = c_T16[i];
+        }
+        for (int i = threadIdx.x; i < 64; i += blockDim.x) sT8[i] = c_T8[i];
+    }
+    __syncthreads();
+    if (g >= groups) return;
+    uint8_t* gsm = sm + WK_BASES + (size_t)g * worker_group_bytes();
+    volatile int* gtask = (volatile int*)(sm + WK_BASES + (size_t)groups * worker_group_bytes()) + g;
+    volatile int* gok = gtask + groups;
+    const int nr = p.defer ? (p.BW + 1) / 2 : 0;
+    const int tb = deblock_tiles_per_band(p.W);
+    const int nd = p.defer && p.db_level > 0 ? tb : 0;
+    const int nt = p.tflag != nullptr ? p.BW : 0;
+    const int lag = p.defer ? TAB_LAG : 0;
+    const int steps = p.BH + (p.defer ? TAB_LAG : 0);
+    const int nmb = p.BW * p.BH;
+    const int bar = 1 + g;
+    // Task indices a group takes only grow, so the step cursor (k, first task of step k) only
+    // moves forward.  Thread 0 takes the next index while the group works on the current one;
+    // a group holding index n + 1 still finishes n first, so the smallest unfinished task is
+    // always being worked on and the queue drains.
+    int next = 0;
+    if (tid == 0) next = (int)atomicAdd(p.wq, 1u);
+    int k = 0, base = 0;
+    const int csteps = p.defer && p.compact ? 2 : 0;
+    unsigned* scan_done = p.wq + 1 + 2 * p.BH;
+    for (;;) {
+        if (tid == 0) {
+            *gtask = next;
+            next = (int)atomicAdd(p.wq, 1u);
+        }
+        group_sync(bar, TW_GROUP);  // (the previous task ended with a group barrier too)
+        const int task = *gtask;
+        int R = 0, D = 0, T = 0;
+        for (; k < steps + csteps; k++) {
+            if (k < steps) {
+                R = k < p.BH ? nr : 0;
+                D = k >= DB_LAG && k - DB_LAG < p.BH ? nd : 0;
+                T = k >= lag && k - lag < p.BH ? nt : 0;
+            } else {  // compaction: the scan, then the pack rows (counted as T)
+                R = D = 0;
+                T = k == steps ? 1 : p.BH;
+            }
+            if (task < base + R + D + T) break;
+            base += R + D + T;
+        }
+        if (k >= steps + csteps) return;  // the queue is empty
+        const int t = task - base;
+        int kind = t < R ? 0 : t < R + D ? 1 : 2;
+        int row = kind == 0 ? k : kind == 1 ? k - DB_LAG : k - lag;
+        const int idx = kind == 0 ? t : kind == 1 ? t - R : t - R - D;
+        if (k >= steps) {
+            kind = k == steps ? 3 : 4;
+            row = t;
+        }
+        if (kind == 0) {  // residual of MBs (row, 2 idx) and (row, 2 idx + 1)
+            const int half = tid >> 6, x = 2 * idx + half;
+            if (tid == 0) RIV_GSTAMP(row * p.BW + 2 * idx, 18);
+            if (x < p.BW)
+                residual_mb(p.dres, nmb, row * p.BW + x, tid & 63, 5 + 2 * g + half,
+                            *(ResSmem*)(gsm + half * RES_HALF_BYTES), sT16, sT16t, sT8);
+            group_sync(bar, TW_GROUP);
+            if (tid == 0) {
+                __threadfence();
+                atomicAdd(p.wq + 1 + row, (unsigned)min(2, p.BW - 2 * idx));
+                RIV_GSTAMP(row * p.BW + 2 * idx, 19);
+            }
+        } else if (kind == 1) {  // deblock tile idx of band `row`
+            if (tid == 0) {
+                RIV_GSTAMP(row * p.BW + idx, 20);
+                bool ok = true;
+                for (int r = max(row - 1, 0); r <= min(row + 1, p.BH - 1) && ok; r++)
+                    ok = wait_at_least(p.wq + 1 + r, (unsigned)p.BW, p.spin_limit);
+                *gok = ok ? 1 : 0;
+                if (!ok) atomicOr(p.status, ST_WAIT_TIMEOUT);
+            }
+            group_sync(bar, TW_GROUP);
+            if (!*gok) return;
+            if (tid == 0) RIV_GSTAMP(row * p.BW + idx, 21);
+            const int tpy = (p.W + DB_TW - 1) / DB_TW, tpc = (p.W / 2 + DB_TW / 2 - 1) / (DB_TW / 2);
+            const int plane = idx < tpy ? 0 : 1 + (idx - tpy) / tpc;
+            const int tile = idx < tpy ? row * tpy + idx : row * tpc + (idx - tpy) % tpc;
+            deblock_tile(p.db_src, p.db_dst, p.W, p.H, p.BW, p.db_E, p.db_I, p.db_H, p.db_mask, plane, tile, gsm, tid,
+                         TW_GROUP, bar);
+            group_sync(bar, TW_GROUP);
+            if (tid == 0) {
+                __threadfence();
+                atomicAdd(p.wq + 1 + p.BH + row, 1u);
+                RIV_GSTAMP(row * p.BW + idx, 22);
+            }
+        } else if (kind == 3) {  // scan of the previous frame's coded MBs (all residual rows done)
+            if (tid == 0) {
+                bool ok = true;
+                for (int r = 0; r < p.BH && ok; r++) ok = wait_at_least(p.wq + 1 + r, (unsigned)p.BW, p.spin_limit);
+                *gok = ok ? 1 : 0;
+                if (!ok) atomicOr(p.status, ST_WAIT_TIMEOUT);
+            }
+            group_sync(bar, TW_GROUP);
+            if (!*gok) return;
+            int* ws = (int*)gsm;
+            scan_mbs<TW_GROUP, WK_SCAN_IPT>(p.dres.opt_skip, p.dres.eobs, nmb, 0, p.c_index, p.c_offset, p.c_hdr, tid,
+                                            bar, ws, ws + TW_GROUP / 32);
+            group_sync(bar, TW_GROUP);
+            if (tid == 0) {
+                __threadfence();
+                st_release_u32(scan_done, 1u);
+            }
+        } else if (kind == 4) {  // pack MB row `row` of the previous frame
+            if (tid == 0) {
+                const bool ok = wait_at_least(scan_done, 1u, p.spin_limit);
+                *gok = ok ? 1 : 0;
+                if (!ok) atomicOr(p.status, ST_WAIT_TIMEOUT);
+            }
+            group_sync(bar, TW_GROUP);
+            if (!*gok) return;
+            for (int x = tid >> 5; x < p.BW; x += TW_GROUP / 32)
+                pack_mb(row * p.BW + x, tid & 31, p.dres.opt_skip, p.dres.mb, p.dres.coeffs, p.dres.eobs, p.c_index,
+                        p.c_offset, 0, p.c_side, p.c_packed, p.c_peobs);
+        } else {  // SAD-table row of MB (row, idx)
+            if (tid == 0) {
+                RIV_GSTAMP(row * p.BW + idx, 23);
+                const bool ok = wait_ref_rows(p, row, tb);
+                *gok = ok ? 1 : 0;
+                if (!ok) atomicOr(p.status, ST_WAIT_TIMEOUT);
+            }
+            group_sync(bar, TW_GROUP);
+            if (!*gok) return;
+            const int mb = row * p.BW + idx;
+            if (tid == 0) RIV_GSTAMP(mb, 24);
+            sad_table_mb(p.ref_y, p.cur_y, p.W, p.H, p.BW, p.sr, const_cast<uint16_t*>(p.tab), p.tstride, mb, gsm, tid,
+                         TW_GROUP, bar);
+            group_sync(bar, TW_GROUP);
+            if (tid == 0) {
+                __threadfence();
+                st_release_u32(p.tflag + mb, p.tag);
+                RIV_GSTAMP(mb, 25);
+            }
+        }
+        group_sync(bar, TW_GROUP);
     }
 }
 
@@ -706,6 +1456,17 @@ __device__ __forceinline__ void loader_warp(const SearchParams& p, unsigned long
     for (int r = blockIdx.x; r < p.BH && !abort; r += p.nrow_ctas) {
         const int wy0 = r * 16 - sr - 1;
         if (rows > 0 && !(wait_ctl(1, rows) && (p.lnv == nullptr || wait_ctl(3, rows)))) { abort = true; break; }
+        if (p.defer) {  // the previous frame's bands r-1 .. r+1 must be deblocked (written by workers)
+            int ok = 1;
+            if (lane == 0) {
+                RIV_GSTAMP(r * p.BW, 26);
+                ok = wait_ref_rows(p, r, deblock_tiles_per_band(p.W)) ? 1 : 0;
+                RIV_GSTAMP(r * p.BW, 27);
+            }
+            __syncwarp();  // orders every lane's copies after lane 0's acquire
+            asm volatile("fence.proxy.async.global;" ::: "memory");  // generic writes -> bulk-copy reads
+            if (!__shfl_sync(0xffffffffu, ok, 0)) { abort = true; break; }
+        }
         // ---- the band: rows wy0 .. wy0+WS-1 (edge-clamped), columns -MARGIN .. W+MARGIN-1
         for (int i = lane; i < WS; i += 32) {
             const int gy = min(max(wy0 + i, 0), p.H - 1);
@@ -913,13 +1674,13 @@ __device__ __forceinline__ void aq_fold(const SearchParams& p, volatile int* ctl
 }
 
 template <bool BAND, bool TABLE, bool SMALL>
-__global__ void __launch_bounds__(512, 1) k_search(SearchParams p) {
+__device__ __forceinline__ void search_body(const SearchParams& p) {
     // FAST (band + table): three warps -- search chain, mode decision, loader.  Otherwise the
     // search warp stages its own data with cp.async and the third warp is not launched.
     constexpr bool FAST = BAND && TABLE;
     extern __shared__ __align__(16) uint8_t smem[];
     if (FAST && p.tflag != nullptr && (int)blockIdx.x >= p.nrow_ctas) {
-        table_worker(p, smem);
+        frame_worker(p, smem);
         return;
     }
     double* bits = (double*)smem;                 // 256 doubles
@@ -1018,6 +1779,7 @@ __global__ void __launch_bounds__(512, 1) k_search(SearchParams p) {
             const int x0 = bx * 16;
             const int idx = r * p.BW + bx;
             RIV_STAMP(0);
+            if (lane == 0) RIV_GSTAMP(idx, 16);
             // ---- FAST: wait for the loader's slot; otherwise prefetch MB bx+1 (columns, current
             // block, table row) and wait for MB bx's data
             const uint8_t* lslot = slots + (size_t)(ln & (LD_RING - 1)) * ld_slot_bytes(p.tstride);
@@ -1048,6 +1810,7 @@ __global__ void __launch_bounds__(512, 1) k_search(SearchParams p) {
             }
             if (!FAST) cp_async_commit();
             RIV_STAMP(7);
+            if (lane == 0) RIV_GSTAMP(idx, 17);
             if (!FAST) cp_async_wait1();
             RefView view;
             if (BAND) {
@@ -1574,6 +2337,22 @@ __global__ void __launch_bounds__(512, 1) k_search(SearchParams p) {
     }
 }
 
+// One CTA of 512 threads per SM, at most 120 registers a thread: 61,440 of the SM's 65,536,
+// so a 128-thread CTA of the next frame's input conversion (32 registers) runs beside it.
+// (An 80-register cap slows the worker tasks' residual and table code measurably.)
+// Launch timeline when profiling: words 28 / 29 of ring entry (tag mod 256) get the global
+// time of the first CTA's start and of the last warp's exit.
+template <bool BAND, bool TABLE, bool SMALL>
+__global__ void __maxnreg__(120) k_search(SearchParams p) {
+    const int ring = (int)(p.tag % (unsigned)min(256, p.BW * p.BH));
+    unsigned long long* tl = p.prof != nullptr ? (unsigned long long*)(p.prof + (size_t)ring * RIV_PROF_WORDS + 28) : nullptr;
+    if (tl != nullptr && threadIdx.x == 0) atomicCAS(tl, 0ull, (unsigned long long)gtimer());
+    if (p.wq_next != nullptr && blockIdx.x == gridDim.x - 1)  // the next launch's queue words
+        for (int i = threadIdx.x; i < p.wq_words; i += blockDim.x) p.wq_next[i] = 0u;
+    search_body<BAND, TABLE, SMALL>(p);
+    if (tl != nullptr && (threadIdx.x & 31) == 0) atomicMax(tl + 1, (unsigned long long)gtimer());
+}
+
 // Shared memory of the search kernel; BAND when the whole MB-row band fits, TABLE when
 // the exhaustive SAD table is used (search ranges up to 15).
 int sad_table_stride(int sr) { return ((2 * sr + 1) * (2 * sr + 1) + 7) & ~7; }
@@ -1803,358 +2582,18 @@ int launch_aq(const uint2* varsum, int n, float base, const uint32_t* logfix, in
 // res/residual.rs:520-752).  Intra: pixel-128, JPEG-derived matrices, no dead zone
 // (res/residual.rs:267-388, dct16.rs:420-560, dct8.rs:142-196).
 // ---------------------------------------------------------------------------------
-__device__ __forceinline__ int16_t f32_to_i16_sat(float f) {
-    if (f != f) return 0;
-    if (f <= -32768.0f) return -32768;
-    if (f >= 32767.0f) return 32767;
-    return (int16_t)__float2int_rz(f);
-}
-__device__ __forceinline__ int32_t f32_to_i32_sat(float f) {
-    if (f != f) return 0;
-    if (f <= -2147483648.0f) return INT_MIN;
-    if (f >= 2147483647.0f) return INT_MAX;
-    return __float2int_rz(f);
-}
-__device__ __forceinline__ int32_t wmul(int32_t a, int32_t b) { return (int32_t)((uint32_t)a * (uint32_t)b); }
-__device__ __forceinline__ int32_t wadd(int32_t a, int32_t b) { return (int32_t)((uint32_t)a + (uint32_t)b); }
-__device__ __forceinline__ int32_t wsub(int32_t a, int32_t b) { return (int32_t)((uint32_t)a - (uint32_t)b); }
-
-// AAN 8-point kernel with the reference's constants (dct/fast_dct8.rs:254-330).
-__device__ __forceinline__ void aan_1d(const int32_t s[8], int32_t out[8], int32_t bias, int shift) {
-    int32_t p1 = wmul(wadd(s[2], s[6]), 2218);
-    int32_t t2 = wadd(p1, wmul(s[6], -7572));
-    int32_t t3 = wadd(p1, wmul(s[2], 3136));
-    int32_t t0 = (int32_t)((uint32_t)wadd(s[0], s[4]) << 12);
-    int32_t t1 = (int32_t)((uint32_t)wsub(s[0], s[4]) << 12);
-    int32_t x0 = wadd(wadd(t0, t3), bias), x3 = wadd(wsub(t0, t3), bias);
-    int32_t x1 = wadd(wadd(t1, t2), bias), x2 = wadd(wsub(t1, t2), bias);
-    int32_t a0 = s[7], a1 = s[5], a2 = s[3], a3 = s[1];
-    int32_t q3 = wadd(a0, a2), q4 = wadd(a1, a3), q1 = wadd(a0, a3), q2 = wadd(a1, a2);
-    int32_t q5 = wmul(wadd(q3, q4), 4817);
-    a0 = wmul(a0, 1223); a1 = wmul(a1, 8411); a2 = wmul(a2, 12595); a3 = wmul(a3, 6150);
-    q1 = wadd(q5, wmul(q1, -3685));
-    q2 = wadd(q5, wmul(q2, -10496));
-    q3 = wmul(q3, -8035);
-    q4 = wmul(q4, -1598);
-    int32_t u3 = wadd(a3, wadd(q1, q4)), u2 = wadd(a2, wadd(q2, q3));
-    int32_t u1 = wadd(a1, wadd(q2, q4)), u0 = wadd(a0, wadd(q1, q3));
-    out[0] = wadd(x0, u3) >> shift; out[7] = wsub(x0, u3) >> shift;
-    out[1] = wadd(x1, u2) >> shift; out[6] = wsub(x1, u2) >> shift;
-    out[2] = wadd(x2, u1) >> shift; out[5] = wsub(x2, u1) >> shift;
-    out[3] = wadd(x3, u0) >> shift; out[4] = wsub(x3, u0) >> shift;
-}
-
-// Four MBs per CTA, 64 threads (two warps) per MB.  Thread u of an MB owns luma row u >> 2,
-// columns 4 * (u & 3) .. +3 in every 16x16 pass, and two adjacent chroma samples (plane
-// u >> 5).  Each pass reads one basis row and one data row per term as 128-bit shared loads,
-// four multiply-accumulates per pair of loads.  Per-MB named barriers (ids 1..4, 64 threads).
-__device__ __forceinline__ void mb_sync(int g) { asm volatile("bar.sync %0, 64;" ::"r"(g + 1) : "memory"); }
-// Dequantisation and inverse transforms of one MB and its reconstruction onto the prediction
-// (dct/dct16.rs:345-412, dct/fast_dct8.rs:69-174, res/residual.rs:740-752), shared by the
-// encoder's residual kernel and the decoder.  64 threads per MB (group g, thread u: luma row
-// yy, columns xb..xb+3; own quantised luma ql); Qc = the MB's 128 chroma coefficients and
-// predc its chroma prediction in shared memory; R, RT, aant = per-MB shared scratch.
-__device__ __forceinline__ void inverse_mb(int g, int u, int yy, int xb, const int16_t (&ql)[4], float qsv, bool intra,
-                                           const uint16_t* ytab, const uint16_t* ctab, uint32_t lbase, uint8_t* ry,
-                                           uint8_t* rU, uint8_t* rV, int CW, int x0, int y0, const int32_t* sT16,
-                                           const int32_t* sT16t, int32_t* R, int32_t* RT, int32_t* aant,
-                                           const int16_t* Qc, const uint8_t* predc) {
-    // dequantisation + 16x16 inverse (row pass over u, then column pass over v)
-    {
-        int32_t d[4];
-        if (intra) {
-#pragma unroll
-            for (int k = 0; k < 4; k++) d[k] = (int32_t)ql[k] * max((int)ytab[yy * 16 + xb + k], 1);
-        } else {
-            const int32_t qfp = f32_to_i32_sat(roundf(__fmul_rn(qsv, 16384.0f)));
-#pragma unroll
-            for (int k = 0; k < 4; k++) d[k] = wadd(wmul((int32_t)ql[k], qfp), 8192) >> 14;
-        }
-        *(int4*)(R + yy * 16 + xb) = make_int4(d[0], d[1], d[2], d[3]);
-    }
-    mb_sync(g);
-    {  // rows[v][x] = (sum_i deq[v][i] * T[x][i] + 2^17) >> 18, wrapping   (v = yy)
-        uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-#pragma unroll
-        for (int i = 0; i < 16; i++) {
-            const uint32_t r = (uint32_t)R[yy * 16 + i];
-            const int4 t = *(const int4*)(sT16t + i * 16 + xb);
-            a0 += r * (uint32_t)t.x; a1 += r * (uint32_t)t.y; a2 += r * (uint32_t)t.z; a3 += r * (uint32_t)t.w;
-        }
-        *(int4*)(RT + yy * 16 + xb) = make_int4((int32_t)(a0 + (1u << 17)) >> 18, (int32_t)(a1 + (1u << 17)) >> 18,
-                                                (int32_t)(a2 + (1u << 17)) >> 18, (int32_t)(a3 + (1u << 17)) >> 18);
-    }
-    mb_sync(g);
-    {  // out[y][x] = (sum_v rows[v][x] * T[y][v] + 2^17) >> 18   (y = yy)
-        uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-#pragma unroll
-        for (int v = 0; v < 16; v++) {
-            const int4 r = *(const int4*)(RT + v * 16 + xb);
-            const uint32_t t = (uint32_t)sT16[yy * 16 + v];
-            a0 += (uint32_t)r.x * t; a1 += (uint32_t)r.y * t; a2 += (uint32_t)r.z * t; a3 += (uint32_t)r.w * t;
-        }
-        const uint32_t acc[4] = {a0, a1, a2, a3};
-        const uint32_t bv = lbase;
-        uint32_t o = 0;
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            int32_t r = (int32_t)(acc[k] + (1u << 17)) >> 18;
-            r = min(max(r, -32768), 32767);
-            const int base = (int)((bv >> (8 * k)) & 255u);
-            o |= (uint32_t)min(max(base + r, 0), 255) << (8 * k);
-        }
-        *(uint32_t*)ry = o;
-    }
-    // chroma 8x8 AAN inverse: pass 1 over u for each (plane, v); pass 2 over v for each (plane, x)
-    if (u < 16) {
-        const int cp = u >> 3, v = u & 7;
-        int32_t sv[8], o[8];
-        int32_t qa = 0;
-        if (!intra) {
-            float qr = roundf(qsv);
-            qr = qr < 1.0f ? 1.0f : qr;
-            qa = qr >= 65535.0f ? 65535 : (int32_t)qr;
-        }
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            const int32_t qq = intra ? max((int)ctab[v * 8 + k], 1) : qa;
-            sv[k] = (int32_t)Qc[cp * 64 + v * 8 + k] * qq;
-        }
-        aan_1d(sv, o, 512, 10);
-#pragma unroll
-        for (int x = 0; x < 8; x++) aant[cp * 64 + x * 8 + v] = o[x];
-    }
-    mb_sync(g);
-    if (u < 16) {
-        const int cp = u >> 3, x = u & 7;
-        int32_t sv[8], o[8];
-#pragma unroll
-        for (int v = 0; v < 8; v++) sv[v] = aant[cp * 64 + x * 8 + v];
-        aan_1d(sv, o, 65536, 17);
-        uint8_t* Rr = cp == 0 ? rU : rV;
-#pragma unroll
-        for (int y = 0; y < 8; y++) {
-            const int r = min(max(o[y], -32768), 32767);
-            const size_t i = (size_t)(y0 / 2 + y) * CW + x0 / 2 + x;
-            const int base = intra ? 128 : (int)predc[cp * 64 + y * 8 + x];
-            Rr[i] = (uint8_t)min(max(base + r, 0), 255);
-        }
-    }
-}
-
-constexpr int RS_MB = 4;
-
 __global__ void __launch_bounds__(256) k_residual(ResidualParams p, int nmb) {
     __shared__ __align__(16) int32_t sT16[256], sT16t[256], sT8[64];
-    __shared__ __align__(16) int32_t res[RS_MB][256], rowt[RS_MB][256];
-    __shared__ __align__(16) int32_t resc[RS_MB][128], rowc[RS_MB][128];
-    __shared__ __align__(16) int16_t q[RS_MB][384];
-    __shared__ int32_t aant[RS_MB][2][64];
-    __shared__ int flags[RS_MB][4];  // nonzero, luma eob of warp 0 / warp 1
-    __shared__ float qsh[RS_MB];
-    __shared__ uint8_t predc[RS_MB][128];  // chroma prediction (U then V, 8x8 each)
+    __shared__ __align__(16) ResSmem S[RS_MB];
     const int tid = threadIdx.x;
-    for (int i = tid; i < 256; i += 256) {
-        sT16[i] = c_T16[i];
-        sT16t[(i & 15) * 16 + (i >> 4)] = c_T16[i];  // sT16t[i][x] = T[x][i]
-    }
+    sT16[tid] = c_T16[tid];
+    sT16t[(tid & 15) * 16 + (tid >> 4)] = c_T16[tid];  // sT16t[i][x] = T[x][i]
     if (tid < 64) sT8[tid] = c_T8[tid];
     __syncthreads();
     const int g = tid >> 6, u = tid & 63;
     const int mb = blockIdx.x * RS_MB + g;
     if (mb >= nmb) return;
-    const int BW = p.BW, W = p.W, H = p.H, CW = W / 2, CH = H / 2;
-    const int bx = mb % BW, by = mb / BW;
-    const int x0 = bx * 16, y0 = by * 16;
-    const uint8_t *cY = p.cur, *cU = p.cur + (size_t)W * H, *cV = cU + (size_t)CW * CH;
-    const uint8_t *pY = p.pred, *pU = p.pred + (size_t)W * H, *pV = pU + (size_t)CW * CH;
-    uint8_t *rY = p.recon, *rU = p.recon + (size_t)W * H, *rV = rU + (size_t)CW * CH;
-    const int yy = u >> 2, xb = (u & 3) * 4;
-    const size_t yi = (size_t)(y0 + yy) * W + x0 + xb;
-    const int pl = u >> 5, ci = (u & 31) * 2, cyy = ci >> 3, cxx = ci & 7;
-    const size_t cidx = (size_t)(y0 / 2 + cyy) * CW + x0 / 2 + cxx;
-    const uint8_t* cC = pl == 0 ? cU : cV;
-    const uint8_t* pC = pl == 0 ? pU : pV;
-    uint8_t* rC = pl == 0 ? rU : rV;
-    int32_t* R = res[g];
-    int32_t* RT = rowt[g];
-    int32_t* RC = resc[g];
-    int32_t* RCT = rowc[g];
-    int16_t* Q = q[g];
-
-    // chroma prediction of this thread's two samples: computed here from the reference planes
-    // (build_predicted's chroma rule, com/fast_motion.rs:264-345) or read from pred
-    uint32_t pcw;
-    if (!p.intra && p.ref != nullptr) {
-        const MbOut m = p.mb[mb];
-        const int mdx = m.raw[0] * 2 + m.raw[2], mdy = m.raw[1] * 2 + m.raw[3];
-        const bool integer = ((mdx & 1) == 0) && ((mdy & 1) == 0);
-        const int sx0 = x0 + (mdx >> 1), sy0 = y0 + (mdy >> 1);
-        const bool copy = integer && sx0 >= 0 && sy0 >= 0 && sx0 + 15 < W && sy0 + 15 < H;
-        const uint8_t* Rp = p.ref + (size_t)W * H + (pl == 0 ? 0 : (size_t)CW * CH);
-        const int cyg = y0 / 2 + cyy;
-        int c2[2];
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-            const int cxg = x0 / 2 + cxx + k;
-            c2[k] = copy ? Rp[(size_t)(sy0 / 2 + cyy) * CW + sx0 / 2 + cxx + k]
-                         : sample_round(Rp, CW, CH, 2 * cxg + (mdx >> 1), 2 * cyg + (mdy >> 1));
-        }
-        pcw = (uint32_t)c2[0] | ((uint32_t)c2[1] << 8);
-    } else {
-        pcw = p.intra ? 0x8080u : *(const uint16_t*)(pC + cidx);
-    }
-    predc[g][pl * 64 + ci] = (uint8_t)pcw;
-    predc[g][pl * 64 + ci + 1] = (uint8_t)(pcw >> 8);
-    auto copy_pred = [&]() {  // recon = prediction, coefficients zero
-        *(uint32_t*)(rY + yi) = *(const uint32_t*)(pY + yi);
-        *(uint16_t*)(rC + cidx) = (uint16_t)pcw;
-        int16_t* co = p.coeffs + (size_t)mb * 384;
-        *(uint2*)(co + yy * 16 + xb) = make_uint2(0u, 0u);
-        *(uint32_t*)(co + 256 + pl * 64 + ci) = 0u;
-        if (u == 0) {
-            p.opt_skip[mb] = 1;
-            const int8_t* c = p.mb[mb].coded;
-            p.fmask[mb] = (c[0] | c[1] | c[2] | c[3]) != 0;
-            p.eobs[3 * mb] = p.eobs[3 * mb + 1] = p.eobs[3 * mb + 2] = 0;
-        }
-    };
-    if (!p.intra && p.lnv != nullptr) {  // AQ step (compute_aq_quant_steps, res/residual.rs:154-167)
-        if (u == 0) {
-            const float off = __fmul_rn(0.8f, __fsub_rn(p.lnv[mb], p.lnv[nmb]));
-            const float q = __fmul_rn(p.aq_base, glibc_exp2f(__fdiv_rn(off, 6.0f), p.expfix, p.nexp));
-            qsh[g] = q;
-            p.qs_out[mb] = q;
-        }
-        mb_sync(g);
-    }
-    if (!p.intra && p.mb[mb].rdo_skip) {  // never transformed: residual 0, recon = prediction
-        copy_pred();
-        return;
-    }
-    {
-        const uint32_t cv = *(const uint32_t*)(cY + yi);
-        const uint32_t pv = p.intra ? 0x80808080u : *(const uint32_t*)(pY + yi);
-#pragma unroll
-        for (int k = 0; k < 4; k++) R[yy * 16 + xb + k] = (int)((cv >> (8 * k)) & 255u) - (int)((pv >> (8 * k)) & 255u);
-        const uint32_t cc = *(const uint16_t*)(cC + cidx);
-        const uint32_t pc = pcw;
-        RC[pl * 64 + ci] = (int)(cc & 255u) - (int)(pc & 255u);
-        RC[pl * 64 + ci + 1] = (int)(cc >> 8) - (int)(pc >> 8);
-    }
-    mb_sync(g);
-    // The reference accumulates both FDCT passes in i64 and clamps to i32.  With residuals in
-    // [-255, 255] and these bases, every partial sum stays below 2^31 (16x16: row pass
-    // <= 255 * 1048576 = 2.7e8, rows <= 1020, column pass <= 1020 * 1048576 + 2^17 = 1.07e9;
-    // 8x8: 1.9e8, 721, 5.3e8), so exact int32 accumulation gives the same values and the
-    // clamp never applies.
-    {  // row pass: rowt[y][j] = sum_i res[y][i] * T[i][j]
-        int32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-#pragma unroll
-        for (int i = 0; i < 16; i++) {
-            const int r = R[yy * 16 + i];
-            const int4 t = *(const int4*)(sT16 + i * 16 + xb);
-            a0 += r * t.x; a1 += r * t.y; a2 += r * t.z; a3 += r * t.w;
-        }
-        *(int4*)(RT + yy * 16 + xb) = make_int4((a0 + (1 << 17)) >> 18, (a1 + (1 << 17)) >> 18,
-                                                (a2 + (1 << 17)) >> 18, (a3 + (1 << 17)) >> 18);
-        int32_t c0 = 0, c1 = 0;
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const int r = RC[pl * 64 + cyy * 8 + i];
-            const int2 t = *(const int2*)(sT8 + i * 8 + cxx);
-            c0 += r * t.x; c1 += r * t.y;
-        }
-        *(int2*)(RCT + pl * 64 + ci) = make_int2((c0 + (1 << 17)) >> 18, (c1 + (1 << 17)) >> 18);
-    }
-    mb_sync(g);
-    int32_t coef[4], coefc[2];
-    {  // column pass: coef[v][x] = sum_i rowt[i][x] * T[i][v]   (v = yy)
-        int32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-#pragma unroll
-        for (int i = 0; i < 16; i++) {
-            const int4 r = *(const int4*)(RT + i * 16 + xb);
-            const int t = sT16[i * 16 + yy];
-            a0 += r.x * t; a1 += r.y * t; a2 += r.z * t; a3 += r.w * t;
-        }
-        coef[0] = (a0 + (1 << 17)) >> 18; coef[1] = (a1 + (1 << 17)) >> 18;
-        coef[2] = (a2 + (1 << 17)) >> 18; coef[3] = (a3 + (1 << 17)) >> 18;
-        int32_t c0 = 0, c1 = 0;
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const int2 r = *(const int2*)(RCT + pl * 64 + i * 8 + cxx);
-            const int t = sT8[i * 8 + cyy];
-            c0 += r.x * t; c1 += r.y * t;
-        }
-        coefc[0] = (c0 + (1 << 17)) >> 18; coefc[1] = (c1 + (1 << 17)) >> 18;
-    }
-    // quantisation
-    float qsv = 0.0f;
-    int16_t ql[4], qc[2];
-    if (p.intra) {
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const float qy = (float)max((int)p.intra_ytab[yy * 16 + xb + k], 1);
-            ql[k] = f32_to_i16_sat(roundf(__fdiv_rn(__int2float_rn(coef[k]), qy)));
-        }
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-            const float qq = (float)max((int)p.intra_ctab[ci + k], 1);
-            qc[k] = f32_to_i16_sat(roundf(__fdiv_rn(__int2float_rn(coefc[k]), qq)));
-        }
-    } else {
-        qsv = p.lnv != nullptr ? qsh[g] : p.qs[mb];
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const float r = __fdiv_rn(__int2float_rn(coef[k]), qsv);
-            ql[k] = fabsf(r) < p.dead_zone ? (int16_t)0 : f32_to_i16_sat(roundf(r));
-        }
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-            const float r = __fdiv_rn(__int2float_rn(coefc[k]), qsv);
-            qc[k] = fabsf(r) < p.dead_zone ? (int16_t)0 : f32_to_i16_sat(roundf(r));
-        }
-    }
-    // last non-zero index per plane block (0 when all zero) and "any non-zero"
-    int lz = 0;
-#pragma unroll
-    for (int k = 0; k < 4; k++) lz = ql[k] != 0 ? yy * 16 + xb + k : lz;
-    int lc = 0;
-#pragma unroll
-    for (int k = 0; k < 2; k++) lc = qc[k] != 0 ? ci + k : lc;
-    const bool any = (ql[0] | ql[1] | ql[2] | ql[3] | qc[0] | qc[1]) != 0;
-    lz = __reduce_max_sync(0xffffffffu, lz);
-    lc = __reduce_max_sync(0xffffffffu, lc);
-    const unsigned anyw = __any_sync(0xffffffffu, any);
-    if ((u & 31) == 0) {
-        flags[g][u >> 5] = lz;
-        flags[g][2 + (u >> 5)] = (int)anyw | (lc << 1);
-    }
-    mb_sync(g);
-    const bool nz = ((flags[g][2] | flags[g][3]) & 1) != 0;
-    if (!p.intra && !nz) {  // became all-zero after quantisation: optimized skip
-        copy_pred();
-        return;
-    }
-    {
-        int16_t* co = p.coeffs + (size_t)mb * 384;
-        const uint32_t w0 = (uint32_t)(uint16_t)ql[0] | ((uint32_t)(uint16_t)ql[1] << 16);
-        const uint32_t w1 = (uint32_t)(uint16_t)ql[2] | ((uint32_t)(uint16_t)ql[3] << 16);
-        *(uint2*)(co + yy * 16 + xb) = make_uint2(w0, w1);
-        *(uint32_t*)(co + 256 + pl * 64 + ci) = (uint32_t)(uint16_t)qc[0] | ((uint32_t)(uint16_t)qc[1] << 16);
-        Q[256 + pl * 64 + ci] = qc[0];
-        Q[256 + pl * 64 + ci + 1] = qc[1];
-        if (u == 0) {
-            p.eobs[3 * mb] = (uint8_t)max(flags[g][0], flags[g][1]);
-            p.eobs[3 * mb + 1] = (uint8_t)(flags[g][2] >> 1);
-            p.eobs[3 * mb + 2] = (uint8_t)(flags[g][3] >> 1);
-            p.opt_skip[mb] = 0;
-            p.fmask[mb] = 1;
-        }
-    }
-    const uint32_t lbase = p.intra ? 0x80808080u : *(const uint32_t*)(pY + yi);
-    inverse_mb(g, u, yy, xb, ql, qsv, p.intra != 0, p.intra_ytab, p.intra_ctab, lbase, rY + yi, rU, rV, CW, x0, y0,
-               sT16, sT16t, R, RT, aant[g][0], Q + 256, predc[g]);
+    residual_mb(p, nmb, mb, u, g + 1, S[g], sT16, sT16t, sT8);
 }
 
 // Decoder reconstruction (res/residual.rs:815-887 intra, :889-1079 inter): the decoded
@@ -2201,7 +2640,7 @@ __global__ void __launch_bounds__(256) k_reconstruct(const int16_t* __restrict__
     predc[g][pl * 64 + ci + 1] = (uint8_t)(pcw >> 8);
     const uint32_t lbase = intra ? 0x80808080u : *(const uint32_t*)(pred + yi);
     const float qsv = intra ? 0.0f : qs[mb];
-    inverse_mb(g, u, yy, xb, ql, qsv, intra != 0, ytab, ctab, lbase, rY + yi, rU, rV, CW, x0, y0, sT16, sT16t, res[g],
+    inverse_mb(g + 1, u, yy, xb, ql, qsv, intra != 0, ytab, ctab, lbase, rY + yi, rU, rV, CW, x0, y0, sT16, sT16t, res[g],
                rowt[g], aant[g][0], qc[g], predc[g]);
 }
 
@@ -2224,102 +2663,14 @@ int launch_residual(const ResidualParams& p, int nmb, void* stream) {
 // x-4..x+3 and writes x-3..x+2, edges are >= 8 px apart), so a thread per edge line
 // reproduces the reference's sequential loops exactly.
 // ---------------------------------------------------------------------------------
-__device__ __forceinline__ int c128(int x) { return min(max(x, -128), 127); }
-__device__ __forceinline__ void filter_line(int* px, int E, int I, int Hv) {
-    int p3 = px[0], p2 = px[1], p1 = px[2], p0 = px[3], q0 = px[4], q1 = px[5], q2 = px[6], q3 = px[7];
-    bool mask = 2 * abs(p0 - q0) + abs(q1 - p1) / 2 <= E && abs(p3 - p2) <= I && abs(p2 - p1) <= I &&
-                abs(p1 - p0) <= I && abs(q1 - q0) <= I && abs(q2 - q1) <= I && abs(q3 - q2) <= I;
-    if (!mask) return;
-    int ps2 = p2 - 128, ps1 = p1 - 128, ps0 = p0 - 128, qs0 = q0 - 128, qs1 = q1 - 128, qs2 = q2 - 128;
-    bool hev = abs(p1 - p0) > Hv || abs(q1 - q0) > Hv;
-    int w = c128(c128(ps1 - qs1) + 3 * (qs0 - ps0));
-    if (hev) {
-        int f1 = c128(w + 4) >> 3, f2 = c128(w + 3) >> 3;
-        px[4] = min(max(c128(qs0 - f1) + 128, 0), 255);
-        px[3] = min(max(c128(ps0 + f2) + 128, 0), 255);
-    } else {
-        int a = c128((27 * w + 63) >> 7);
-        int nq0 = c128(qs0 - a), np0 = c128(ps0 + a);
-        a = c128((18 * w + 63) >> 7);
-        int nq1 = c128(qs1 - a), np1 = c128(ps1 + a);
-        a = c128((9 * w + 63) >> 7);
-        int nq2 = c128(qs2 - a), np2 = c128(ps2 + a);
-        px[1] = min(max(np2 + 128, 0), 255);
-        px[2] = min(max(np1 + 128, 0), 255);
-        px[3] = min(max(np0 + 128, 0), 255);
-        px[4] = min(max(nq0 + 128, 0), 255);
-        px[5] = min(max(nq1 + 128, 0), 255);
-        px[6] = min(max(nq2 + 128, 0), 255);
-    }
-}
-// Out of place, all planes in one launch (src and dst must not overlap: neighbouring tiles
-// read each other's pixels as halo).  A CTA owns one band of an edge grid (16 luma / 8
-// chroma rows) and DB_TW luma (DB_TW/2 chroma) columns.  It loads the tile with a 4-pixel
-// halo, filters every vertical edge of the halo rows in shared memory (rows are independent
-// in that pass), then the horizontal edges at the band's top and bottom (their lines are 4+
-// pixels apart, so they touch disjoint pixels), and stores only its own pixels.  That equals
-// the reference's whole-plane vertical pass followed by the whole-plane horizontal pass.
-constexpr int DB_TW = 128;
 __global__ void __launch_bounds__(128) k_deblock_tiled(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, int W,
                                                        int H, int BW, int E, int I, int Hv, const uint8_t* mask,
                                                        int ntiles_y) {
-    __shared__ uint8_t tile[(16 + 8) * (DB_TW + 8)];
+    __shared__ uint8_t tile[DB_TILE_BYTES];
     int t = blockIdx.x;
     int plane = t < ntiles_y ? 0 : (t - ntiles_y) % 2 + 1;
     if (plane > 0) t = (t - ntiles_y) / 2;
-    const int w = plane ? W / 2 : W, h = plane ? H / 2 : H, g = plane ? 8 : 16, tw = plane ? DB_TW / 2 : DB_TW;
-    const size_t poff = plane == 0 ? 0 : (size_t)W * H + (plane == 2 ? (size_t)(W / 2) * (H / 2) : 0);
-    const uint8_t* pl = src + poff;
-    uint8_t* po = dst + poff;
-    const int tpb = (w + tw - 1) / tw;
-    const int band = t / tpb, X0 = (t % tpb) * tw, X1 = min(X0 + tw, w);
-    const int Y0 = band * g, Y1 = Y0 + g;
-    const int ry0 = max(Y0 - 4, 0), ry1 = min(Y1 + 4, h), cx0 = max(X0 - 4, 0), cx1 = min(X1 + 4, w);
-    const int TS = DB_TW + 8, oy = Y0 - 4, ox = X0 - 4;  // tile row stride and origin
-    const int nrow = ry1 - ry0, ncol = cx1 - cx0;
-    for (int i = threadIdx.x; i < nrow * ncol; i += blockDim.x) {
-        const int r = i / ncol, c = i - r * ncol;
-        tile[(ry0 + r - oy) * TS + cx0 + c - ox] = pl[(size_t)(ry0 + r) * w + cx0 + c];
-    }
-    __syncthreads();
-    // vertical edges x = k*g (1 <= k < w/g) with X0 <= x <= X1, on every loaded row
-    const int k0 = max(1, (X0 + g - 1) / g), k1 = min(w / g - 1, X1 / g);
-    const int nk = k1 - k0 + 1;
-    if (nk > 0) {
-        for (int i = threadIdx.x; i < nrow * nk; i += blockDim.x) {
-            const int r = i / nk, k = k0 + (i - r * nk), y = ry0 + r;
-            const int by = y / g;
-            if (mask && !(mask[by * BW + k - 1] | mask[by * BW + k])) continue;
-            uint8_t* sp = tile + (y - oy) * TS + k * g - 4 - ox;
-            int px[8];
-#pragma unroll
-            for (int q = 0; q < 8; q++) px[q] = sp[q];
-            filter_line(px, E, I, Hv);
-#pragma unroll
-            for (int q = 1; q < 7; q++) sp[q] = (uint8_t)px[q];
-        }
-    }
-    __syncthreads();
-    // horizontal edges at the band's top (Y0) and bottom (Y1), columns X0 .. X1-1
-    for (int i = threadIdx.x; i < 2 * (X1 - X0); i += blockDim.x) {
-        const int e = (i < X1 - X0 ? Y0 : Y1) / g, x = X0 + (i < X1 - X0 ? i : i - (X1 - X0));
-        if (e < 1 || e >= h / g) continue;
-        const int bxm = x / g;
-        if (mask && !(mask[(e - 1) * BW + bxm] | mask[e * BW + bxm])) continue;
-        uint8_t* sp = tile + (e * g - 4 - oy) * TS + x - ox;
-        int px[8];
-#pragma unroll
-        for (int q = 0; q < 8; q++) px[q] = sp[q * TS];
-        filter_line(px, E, I, Hv);
-#pragma unroll
-        for (int q = 1; q < 7; q++) sp[q * TS] = (uint8_t)px[q];
-    }
-    __syncthreads();
-    const int ow = X1 - X0;
-    for (int i = threadIdx.x; i < g * ow; i += blockDim.x) {
-        const int r = i / ow, c = i - r * ow;
-        po[(size_t)(Y0 + r) * w + X0 + c] = tile[(Y0 + r - oy) * TS + X0 + c - ox];
-    }
+    deblock_tile(src, dst, W, H, BW, E, I, Hv, mask, plane, t, tile, threadIdx.x, blockDim.x, 0);
 }
 
 int launch_deblock_tiled(const uint8_t* src, uint8_t* dst, int W, int H, int E, int I, int Hv, const uint8_t* mask,
@@ -2395,98 +2746,21 @@ static __device__ __align__(256) uint8_t g_deblock_scratch[DEBLOCK_NOALLOC_MAX_B
 int deblock_scratch_address(void** out) { return (int)cudaGetSymbolAddress(out, g_deblock_scratch); }
 
 // ---------------------------------------------------------------------------------
-// K8: per-MB side info and compaction of the coded MBs' coefficients for the host entropy
-// coder, written straight into mapped pinned host memory (no separate device->host copy).
-// side = mode | base<<3 | subx<<6 | suby<<7 | rdx<<8 | rdy<<16 | optskip<<24.
-// Each coded MB contributes its three plane blocks truncated after the last non-zero
-// coefficient (the entropy coder never reads beyond it): Y[0..eY], U[0..eU], V[0..eV].
-// hdr[0] = coded MB count, hdr[1] = total coefficients written.
+// K8 kernels (compaction of a frame reconstructed outside a search launch; the layout is
+// described at scan_mbs / pack_mb).
 // ---------------------------------------------------------------------------------
-// Scan: each of SC_THREADS threads owns SC_IPT consecutive MBs of a SC_THREADS * SC_IPT
-// chunk (all their loads are issued together), then one block-wide scan of the thread totals
-// per chunk.  Small enough (256 threads, few registers) to run beside the search kernel.
-constexpr int SC_THREADS = 256, SC_IPT = 32;
+// Scan: one CTA of SC_THREADS threads (scan_mbs), small enough to run beside the search kernel.
 __global__ void __launch_bounds__(SC_THREADS) k_scan(const uint8_t* opt_skip, const uint8_t* eobs, int nmb, int intra,
                                                      int32_t* index, int32_t* offset, uint32_t* hdr) {
     __shared__ int wsum[SC_THREADS / 32], wsz[SC_THREADS / 32];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    int carry = 0, carry_sz = 0;  // identical in every thread
-    for (int base = 0; base < nmb; base += SC_THREADS * SC_IPT) {
-        const int i0 = base + threadIdx.x * SC_IPT;
-        // v = coded << 16 | coefficient count (<= 3 * 256): 32 of them sum without carry
-        uint32_t v[SC_IPT];
-#pragma unroll
-        for (int k = 0; k < SC_IPT; k++) {
-            const int i = i0 + k;
-            const bool f = i < nmb && (intra || !opt_skip[i]);
-            v[k] = f ? (1u << 16) | (uint32_t)(eobs[3 * i] + eobs[3 * i + 1] + eobs[3 * i + 2] + 3) : 0u;
-        }
-        uint32_t tot = 0;
-#pragma unroll
-        for (int k = 0; k < SC_IPT; k++) tot += v[k];
-        const int x = (int)(tot >> 16), y = (int)(tot & 0xffffu);
-        int xs = x, ys = y;  // inclusive warp scan of the thread totals
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int a2 = __shfl_up_sync(0xffffffffu, xs, o), b2 = __shfl_up_sync(0xffffffffu, ys, o);
-            if (lane >= o) { xs += a2; ys += b2; }
-        }
-        if (lane == 31) { wsum[wid] = xs; wsz[wid] = ys; }
-        __syncthreads();
-        int wx = 0, wy = 0, tx = 0, ty = 0;  // exclusive prefix of this warp, chunk totals
-#pragma unroll
-        for (int q = 0; q < SC_THREADS / 32; q++) {
-            if (q < wid) { wx += wsum[q]; wy += wsz[q]; }
-            tx += wsum[q];
-            ty += wsz[q];
-        }
-        int ex = carry + wx + xs - x;
-        int ez = carry_sz + wy + ys - y;
-#pragma unroll
-        for (int k = 0; k < SC_IPT; k++) {
-            const int i = i0 + k;
-            const int f = (int)(v[k] >> 16), z = (int)(v[k] & 0xffffu);
-            if (i < nmb) { index[i] = f ? ex : -1; offset[i] = ez; }
-            ex += f;
-            ez += z;
-        }
-        carry += tx;
-        carry_sz += ty;
-        __syncthreads();  // wsum / wsz are rewritten by the next chunk
-    }
-    if (threadIdx.x == 0) { hdr[0] = (uint32_t)carry; hdr[1] = (uint32_t)carry_sz; }
+    scan_mbs<SC_THREADS, SC_IPT>(opt_skip, eobs, nmb, intra, index, offset, hdr, threadIdx.x, 1, wsum, wsz);
 }
 // Pack: one warp per MB.
 __global__ void __launch_bounds__(256) k_pack(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coeffs,
                                               const uint8_t* eobs, const int32_t* index, const int32_t* offset,
                                               int intra, int nmb, uint32_t* side, int16_t* packed, uint8_t* peobs) {
-    const int m = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-    if (m >= nmb) return;
-    const int k = index[m];
-    const int e0 = eobs[3 * m], e1 = eobs[3 * m + 1], e2 = eobs[3 * m + 2];
-    if (lane == 0) {
-        uint32_t s = 0;
-        if (!intra) {
-            const MbOut o = mb[m];
-            s = (uint32_t)o.mode | ((uint32_t)o.base << 3) | ((uint32_t)(o.raw[2] & 1) << 6) |
-                ((uint32_t)(o.raw[3] & 1) << 7) | ((uint32_t)(uint8_t)o.rdelta[0] << 8) |
-                ((uint32_t)(uint8_t)o.rdelta[1] << 16) | ((uint32_t)(opt_skip[m] & 1) << 24);
-        }
-        side[m] = s;
-        if (k >= 0) {
-            peobs[3 * k] = (uint8_t)e0;
-            peobs[3 * k + 1] = (uint8_t)e1;
-            peobs[3 * k + 2] = (uint8_t)e2;
-        }
-    }
-    if (k < 0) return;
-    const int n0 = e0 + 1, n1 = e1 + 1, n2 = e2 + 1;
-    const int16_t* src = coeffs + (size_t)m * 384;
-    int16_t* dst = packed + offset[m];
-    for (int i = lane; i < n0 + n1 + n2; i += 32) {
-        const int si = i < n0 ? i : (i < n0 + n1 ? 256 + (i - n0) : 320 + (i - n0 - n1));
-        dst[i] = src[si];
-    }
+    const int m = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (m < nmb) pack_mb(m, threadIdx.x & 31, opt_skip, mb, coeffs, eobs, index, offset, intra, side, packed, peobs);
 }
 
 int launch_compact(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coeffs, const uint8_t* eobs, int nmb,

@@ -475,11 +475,12 @@ class Encoder:
         """Cumulative GPU stage times (us, P-frames), I/O bytes and kernel launches."""
         us = (C.c_double * 9)()
         io = (C.c_uint64 * 2)()
-        n = (C.c_uint64 * 2)()
+        n = (C.c_uint64 * 4)()
         self._check(lib().riv_counters(self._h, us, io, n))
         hm = (C.c_double * 6)()
         self._check(lib().riv_host_times(self._h, hm))
         return {"stage_us_sum": list(us), "h2d_bytes": io[0], "d2h_bytes": io[1], "pframes": n[0], "launches": n[1],
+                "deferred_pframes": n[2], "timed_pframes": n[3],
                 "host_ms": list(hm)}
 
     def debug_state(self, what: int) -> np.ndarray:
@@ -488,7 +489,7 @@ class Encoder:
         nmb = (sw // 16) * (sh // 16)
         spec = {0: (nmb * 20, np.uint8), 1: (nmb, np.float32), 2: (sw * sh * 3 // 2, np.uint8),
                 3: (sw * sh * 3 // 2, np.uint8), 4: (nmb * 384, np.int16), 5: (nmb, np.uint8),
-                6: (nmb * 16, np.int64)}[what]
+                6: (nmb * 32, np.int64)}[what]
         out = np.empty(spec[0], spec[1])
         self._check(lib().riv_debug_frame_state(self._h, what, C.c_void_p(out.ctypes.data), out.nbytes))
         return out
