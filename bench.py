@@ -265,28 +265,55 @@ def cpu_baseline(frames_host, nframes, iq, pq):
     return nframes / dt, dt
 
 
-# dram__bytes_read.sum + dram__bytes_write.sum of one k_search launch at this workload
-# (ncu --set full, caches flushed before the pass): 4,689,408 + 12,288 bytes.  The SAD table
-# is produced and consumed inside the same launch and stays in L2.
-SEARCH_TRAFFIC_BYTES = 4_689_408 + 12_288
+# dram__bytes_read.sum + dram__bytes_write.sum of one steady-state k_search launch at this
+# workload (ncu --set full, caches flushed before each pass, launches 7 and 8 of the bench
+# command): 9,730,048 + 101,632 bytes.  The SAD table, the prediction, the pre-deblock
+# reconstruction and the coefficients are produced and consumed inside the launch (or by the
+# next one) and stay in L2.
+SEARCH_TRAFFIC_BYTES = 9_730_048 + 101_632
+
+Y_BYTES = 1920 * 1088            # one luma plane (storage size)
+YUV_BYTES = Y_BYTES * 3 // 2     # one 4:2:0 frame
 
 
-def roofline_entry(stage_us_per_frame: float):
-    """Search/mode wavefront: algorithmic bytes per frame = read reference Y + current Y
-    (2 x 1920x1088) + write the per-MB record and output (8 + 20 bytes per MB).  The
-    kernel is bound by the latency of its serial MB chain (120 + 2 x 67 = 254 wavefront
-    steps at 1080p), not by HBM; the step time is reported beside the HBM fraction."""
+def launch_algorithmic_bytes(compact_bytes: float) -> dict:
+    """Bytes each stage of one steady-state k_search launch reads and writes once, 1080p:
+    * search + mode + AQ of frame t: read reference Y and current Y, write the per-MB records
+      and outputs (8 + 20 B), ln variance and variance sums (12 B), and the luma prediction;
+    * residual of frame t-1: read current YUV, luma prediction, reference chroma (chroma
+      prediction), MB outputs and ln variances (24 B/MB); write the pre-deblock YUV, the
+      coefficients (768 B/MB) and the skip / mask / EOB bytes (5 B/MB);
+    * deblock of frame t-1: read the pre-deblock YUV and the mask, write the reference YUV;
+    * compaction of frame t-1: read and write the compacted side info and coefficients
+      (`compact_bytes`, the bench's measured device->host bytes per frame)."""
+    n = MBS_PER_FRAME
+    search = 2 * Y_BYTES + n * (28 + 12) + Y_BYTES
+    residual = YUV_BYTES + Y_BYTES + Y_BYTES // 2 + n * 24 + YUV_BYTES + n * 768 + n * 5
+    deblock = 2 * YUV_BYTES + n
+    compact = 2 * compact_bytes
+    return {"search_mode_aq": search, "residual": residual, "deblock": deblock, "compaction": int(compact),
+            "total": int(search + residual + deblock + compact)}
+
+
+def roofline_entry(stage_us_per_frame: float, compact_bytes: float):
+    """One k_search launch: the wavefront search of frame t with the previous frame's
+    residual, deblock and compaction in its worker CTAs.  Algorithmic bytes as in
+    launch_algorithmic_bytes; the kernel is bound by the latency of its serial MB chain (120
+    + 2 x 67 = 254 wavefront steps at 1080p), not by HBM, so the step time is reported
+    beside the HBM fraction."""
     peaks = {}
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         peaks = json.load(open(p))
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    alg = 2 * 1920 * 1088 + MBS_PER_FRAME * (8 + 20)
+    parts = launch_algorithmic_bytes(compact_bytes)
+    alg = parts["total"]
     achieved = alg / (stage_us_per_frame * 1e-6) / 1e9
     steps = (1920 // 16) + 2 * (1088 // 16 - 1)
-    return {"bound": "hbm", "kernel": "k_search (motion search + RDO + mode wavefront)", "achieved": achieved,
+    return {"bound": "hbm", "kernel": "k_search (wavefront search + RDO + mode + AQ of frame t; residual, deblock "
+            "and compaction of frame t-1 in the worker CTAs)", "achieved": achieved,
             "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": SEARCH_TRAFFIC_BYTES,
-            "algorithmic_bytes_per_launch": alg, "launch_us": stage_us_per_frame,
+            "algorithmic_bytes_per_launch": alg, "algorithmic_bytes_by_stage": parts, "launch_us": stage_us_per_frame,
             "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
             "critical_path": {"wavefront_steps": steps, "us_per_step": stage_us_per_frame / steps}}
 
@@ -366,7 +393,7 @@ def main():
         "gpu_pipeline_fps": 1e6 / stage[8] if stage[8] > 0 else None,
         "host_ms_per_frame": dict(zip(["submit", "retire", "mv_coding", "dct_coding_sum", "write", "blocked"],
                                       [round((b - a) / K, 3) for a, b in zip(c0["host_ms"], c1["host_ms"])])),
-        "roofline": roofline_entry(stage[2]),
+        "roofline": roofline_entry(stage[2], d2h),
         "cpu_baseline": cpu,
         "clocks": r["clocks"], "clocks_e2e": r["clocks_e2e"],
         "stream_bytes": r["stream_bytes"], "streams_equal_value_vs_e2e": r["streams_equal"],
