@@ -81,6 +81,7 @@ struct SearchParams {
     long long spin_limit;
     long long* prof;  // optional: RIV_PROF_WORDS words per MB (phase stamps, hexagon rounds), nullptr = off
     int nrow_ctas;    // CTAs that own MB rows (row stride); the rest of the grid are table workers
+    int row_helpers;  // row CTAs run worker groups before their row starts and after it ends
     unsigned* tflag;  // fused table: per-MB flag = tag once its table row is written; nullptr = precomputed
     // Prediction and AQ inside the search launch (band + table instantiations): nullptr lnv =
     // done by the separate predict / AQ kernels.
@@ -127,6 +128,7 @@ int launch_rgb_to_yuv(const uint8_t* rgb, int dw, int dh, uint8_t* yuv, int W, i
 struct SearchPlan {
     bool fast;   // band + table instantiation: loader and AQ warps (prediction and AQ in the launch)
     bool fused;
+    bool helpers;  // fused: row CTAs' spare threads and finished row CTAs take worker tasks
     int grid, nrow, threads;
     size_t smem;
 };

@@ -1239,22 +1239,37 @@ __device__ __forceinline__ void pack_mb(int m, int lane, const uint8_t* opt_skip
 // one pack task per MB row (after the scan, published in wq[2BH+1]).
 constexpr int DB_LAG = 3, TAB_LAG = 6;
 constexpr int WK_SCAN_IPT = 8;  // MBs per thread of the in-launch scan (registers are capped)
-__device__ __forceinline__ void frame_worker(const SearchParams& p, uint8_t* sm) {
-    const int groups = blockDim.x / TW_GROUP, g = threadIdx.x / TW_GROUP, tid = threadIdx.x % TW_GROUP;
-    int32_t* sT16 = (int32_t*)sm;
+// Worker region: the residual bases (WK_BASES bytes), `groups` group scratch areas, then a
+// task word and a status word per group.
+__host__ __device__ constexpr int worker_region_bytes(int groups) {
+    return WK_BASES + groups * worker_group_bytes() + 2 * groups * 4;
+}
+// Bases of the deferred residual into a worker region, by threads lo, lo + step, ...
+__device__ __forceinline__ void load_worker_bases(const SearchParams& p, uint8_t* region, int lo, int step) {
+    if (!p.defer) return;
+    int32_t* sT16 = (int32_t*)region;
     int32_t* sT16t = sT16 + 256;
     int32_t* sT8 = sT16t + 256;
-    if (p.defer) {
-        for (int i = threadIdx.x; i < 256; i += blockDim.x) {
-            sT16[i] = c_T16[i];
-            sT16t[(i & 15) * 16 + (i >> 4)] = c_T16[i];
-        }
-        for (int i = threadIdx.x; i < 64; i += blockDim.x) sT8[i] = c_T8[i];
+    for (int i = lo; i < 256; i += step) {
+        sT16[i] = c_T16[i];
+        sT16t[(i & 15) * 16 + (i >> 4)] = c_T16[i];
     }
-    __syncthreads();
-    if (g >= groups) return;
-    uint8_t* gsm = sm + WK_BASES + (size_t)g * worker_group_bytes();
-    volatile int* gtask = (volatile int*)(sm + WK_BASES + (size_t)groups * worker_group_bytes()) + g;
+    for (int i = lo; i < 64; i += step) sT8[i] = c_T8[i];
+}
+
+// The task loop of one 128-thread group: region slot g of `groups`, named barriers keyed
+// by gid (the group's index in its CTA: 1 + gid for the group, 5 + 2 gid + half for the
+// residual halves).  With `stop` the group takes each index only when it will run the
+// task and leaves once *stop is set (no index is held early); without it, it runs until
+// the queue is empty.
+__device__ __forceinline__ void worker_loop(const SearchParams& p, uint8_t* region, int groups, int g, int gid,
+                                            const volatile int* stop) {
+    const int tid = threadIdx.x % TW_GROUP;
+    const int32_t* sT16 = (const int32_t*)region;
+    const int32_t* sT16t = sT16 + 256;
+    const int32_t* sT8 = sT16t + 256;
+    uint8_t* gsm = region + WK_BASES + (size_t)g * worker_group_bytes();
+    volatile int* gtask = (volatile int*)(region + WK_BASES + (size_t)groups * worker_group_bytes()) + g;
     volatile int* gok = gtask + groups;
     const int nr = p.defer ? (p.BW + 1) / 2 : 0;
     const int tb = deblock_tiles_per_band(p.W);
@@ -1263,23 +1278,28 @@ __device__ __forceinline__ void frame_worker(const SearchParams& p, uint8_t* sm)
     const int lag = p.defer ? TAB_LAG : 0;
     const int steps = p.BH + (p.defer ? TAB_LAG : 0);
     const int nmb = p.BW * p.BH;
-    const int bar = 1 + g;
+    const int bar = 1 + gid;
     // Task indices a group takes only grow, so the step cursor (k, first task of step k) only
-    // moves forward.  Thread 0 takes the next index while the group works on the current one;
-    // a group holding index n + 1 still finishes n first, so the smallest unfinished task is
-    // always being worked on and the queue drains.
+    // moves forward.  Thread 0 takes the next index while the group works on the current one
+    // (stoppable groups do not); a group holding index n + 1 still finishes n first, so the
+    // smallest unfinished task is always being worked on and the queue drains.
     int next = 0;
-    if (tid == 0) next = (int)atomicAdd(p.wq, 1u);
+    if (tid == 0 && stop == nullptr) next = (int)atomicAdd(p.wq, 1u);
     int k = 0, base = 0;
     const int csteps = p.defer && p.compact ? 2 : 0;
     unsigned* scan_done = p.wq + 1 + 2 * p.BH;
     for (;;) {
         if (tid == 0) {
-            *gtask = next;
-            next = (int)atomicAdd(p.wq, 1u);
+            if (stop == nullptr) {
+                *gtask = next;
+                next = (int)atomicAdd(p.wq, 1u);
+            } else {
+                *gtask = *stop ? -1 : (int)atomicAdd(p.wq, 1u);
+            }
         }
         group_sync(bar, TW_GROUP);  // (the previous task ended with a group barrier too)
         const int task = *gtask;
+        if (task < 0) return;  // stopped (group-uniform)
         int R = 0, D = 0, T = 0;
         for (; k < steps + csteps; k++) {
             if (k < steps) {
@@ -1306,7 +1326,7 @@ __device__ __forceinline__ void frame_worker(const SearchParams& p, uint8_t* sm)
             const int half = tid >> 6, x = 2 * idx + half;
             if (tid == 0) RIV_GSTAMP(row * p.BW + 2 * idx, 18);
             if (x < p.BW)
-                residual_mb(p.dres, nmb, row * p.BW + x, tid & 63, 5 + 2 * g + half,
+                residual_mb(p.dres, nmb, row * p.BW + x, tid & 63, 5 + 2 * gid + half,
                             *(ResSmem*)(gsm + half * RES_HALF_BYTES), sT16, sT16t, sT8);
             group_sync(bar, TW_GROUP);
             if (tid == 0) {
@@ -1389,10 +1409,21 @@ __device__ __forceinline__ void frame_worker(const SearchParams& p, uint8_t* sm)
     }
 }
 
+// A whole worker CTA (or a row CTA whose rows are done): bases at sm, blockDim / 128 groups.
+__device__ __forceinline__ void frame_worker(const SearchParams& p, uint8_t* sm) {
+    load_worker_bases(p, sm, threadIdx.x, blockDim.x);
+    __syncthreads();
+    const int groups = blockDim.x / TW_GROUP, g = threadIdx.x / TW_GROUP;
+    worker_loop(p, sm, groups, g, g, nullptr);
+}
+
 // ---- mbarrier and bulk-copy helpers (sm_90+ PTX; no multicast)
 __device__ __forceinline__ uint32_t sa32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sa32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_inval(unsigned long long* bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(sa32(bar)) : "memory");
 }
 __device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(sa32(bar)) : "memory");
@@ -1434,8 +1465,10 @@ __host__ __device__ inline int ld_slot_bytes(int tstride) { return 2 * tstride +
 // LD_RING MBs ahead of the search warp, each MB's table row, current block and temporal MV,
 // so that no copy is issued on the search chain.  ctl[0] = MBs the search warp has released,
 // ctl[1] = rows it has finished, ctl[2] = abort.
+// row_live (optional): set once the first row's reference bands are ready, which stops the
+// CTA's helper worker groups from taking further tasks.
 __device__ __forceinline__ void loader_warp(const SearchParams& p, unsigned long long* fullb, unsigned long long* bandb,
-                                            volatile int* ctl, uint8_t* slots, uint8_t* band) {
+                                            volatile int* ctl, uint8_t* slots, uint8_t* band, volatile int* row_live) {
     const int lane = threadIdx.x & 31;
     const int sr = p.sr, WS = 18 + 2 * sr, MARGIN = (sr + 1 + 15) & ~15, BWB = p.W + 2 * MARGIN;
     const int SLOT = ld_slot_bytes(p.tstride);
@@ -1467,6 +1500,7 @@ __device__ __forceinline__ void loader_warp(const SearchParams& p, unsigned long
             asm volatile("fence.proxy.async.global;" ::: "memory");  // generic writes -> bulk-copy reads
             if (!__shfl_sync(0xffffffffu, ok, 0)) { abort = true; break; }
         }
+        if (row_live != nullptr && lane == 0) *row_live = 1;
         // ---- the band: rows wy0 .. wy0+WS-1 (edge-clamped), columns -MARGIN .. W+MARGIN-1
         for (int i = lane; i < WS; i += 32) {
             const int gy = min(max(wy0 + i, 0), p.H - 1);
@@ -1710,7 +1744,16 @@ __device__ __forceinline__ void search_body(const SearchParams& p) {
     if (SMALL)
         for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x) nc32s[i] = p.newcost32[i];
     for (int i = threadIdx.x; i < HAND_RING; i += blockDim.x) hand[i] = 0ull;
+    // Fused launch: threads 128-511 of a row CTA are worker groups 1-3 until the row starts
+    // (region after the row layout: a live flag, then a 3-group worker region), and the
+    // whole CTA joins the worker queue once its rows are done.
+    const bool helpers = FAST && p.tflag != nullptr && p.row_helpers;
+    uint8_t* pre = smem + (((size_t)(refmem - smem) + (size_t)WS * BWB + 16 + 15) & ~(size_t)15);
+    volatile int* row_live = (volatile int*)pre;
+    uint8_t* preg = pre + 16;
+    if (helpers) load_worker_bases(p, preg, threadIdx.x, blockDim.x);
     if (threadIdx.x == 0) {
+        if (helpers) *row_live = 0;
         hand_done[0] = 0;
         hand_done[1] = FAST && p.lnv != nullptr ? 0 : 0x3fffffff;  // no AQ warp: never waited for
         if (FAST) {
@@ -1722,12 +1765,16 @@ __device__ __forceinline__ void search_body(const SearchParams& p) {
     }
     __syncthreads();
     const unsigned long long tagbits = (unsigned long long)(p.tag & 0xffffu) << 48;
+    auto roles = [&]() {
     if (threadIdx.x >= 64) {
         if (FAST && threadIdx.x < 96) {
-            loader_warp(p, fullb, bandb, ld_ctl, slots, refmem);
+            loader_warp(p, fullb, bandb, ld_ctl, slots, refmem, helpers ? row_live : nullptr);
             if (p.lnv != nullptr && blockIdx.x == 0) aq_fold(p, ld_ctl, fold_stage);
         } else if (FAST && threadIdx.x < 128 && p.lnv != nullptr) {
             aq_warp(p, hand, hand_done, ld_ctl, refmem, bandb);
+        } else if (helpers && threadIdx.x >= TW_GROUP) {
+            const int gid = threadIdx.x / TW_GROUP;
+            worker_loop(p, preg, 3, gid - 1, gid, row_live);
         }
         return;
     }
@@ -2335,7 +2382,18 @@ __device__ __forceinline__ void search_body(const SearchParams& p) {
             cp_async_wait0();
         }
     }
+    };
+    roles();
+    if (helpers) {  // the row work is done: the whole CTA takes worker tasks
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int i = 0; i < LD_RING; i++) mbar_inval(fullb + i);
+            mbar_inval(bandb);
+        }
+        frame_worker(p, smem);
+    }
 }
+
 
 // One CTA of 512 threads per SM, at most 120 registers a thread: 61,440 of the SM's 65,536,
 // so a 128-thread CTA of the next frame's input conversion (32 registers) runs beside it.
@@ -2399,7 +2457,12 @@ int search_plan(int sr, int W, int BH, bool table, bool small, SearchPlan* out) 
     if (band && table) {
         // fused: one CTA per SM (the shared-memory request rules out a second), rows first,
         // table workers on the SMs the rows leave free -- used when enough of them remain
-        const size_t smf = sm > (size_t)116 * 1024 ? sm : (size_t)116 * 1024;
+        // row CTAs' helper region (live flag + three worker groups) after the row layout,
+        // where the per-CTA maximum allows it
+        const size_t with_helpers = ((sm + 15) & ~(size_t)15) + 16 + (size_t)worker_region_bytes(3);
+        const bool helpers = with_helpers <= (size_t)227 * 1024;
+        const size_t need = helpers ? with_helpers : sm;
+        const size_t smf = need > (size_t)116 * 1024 ? need : (size_t)116 * 1024;
         int per_sm = 0;
         e = resident(smf, 4 * 128, &per_sm);
         if (e != cudaSuccess) return (int)e;
@@ -2408,6 +2471,7 @@ int search_plan(int sr, int W, int BH, bool table, bool small, SearchPlan* out) 
         const size_t gsm = ((size_t)sad_table_smem(sr) + 15) & ~(size_t)15;
         if (per_sm == 1 && total - nrow >= 32 && 4 * gsm <= smf) {
             pl.fused = true;
+            pl.helpers = helpers;
             pl.threads = 4 * 128;  // row CTAs use three warps; table workers four groups of 128
             pl.smem = smf;
             pl.nrow = nrow;
@@ -2430,6 +2494,7 @@ int launch_search(const SearchParams& p, const SearchPlan& plan, void* stream) {
     const bool band = search_use_band(p.sr, p.W), table = p.tab != nullptr;
     SearchParams q = p;
     q.nrow_ctas = plan.nrow;
+    q.row_helpers = plan.fused && plan.helpers ? 1 : 0;
     if (!plan.fused) q.tflag = nullptr;
     void* args[] = {&q};
     // Cooperative launch: every CTA of the grid is co-resident, so the row-to-row waits
