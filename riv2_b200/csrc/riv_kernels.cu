@@ -1573,7 +1573,7 @@ __device__ __forceinline__ void aq_warp(const SearchParams& p, const unsigned lo
                                         volatile int* ctl, const uint8_t* band, unsigned long long* bandb) {
     const int lane = threadIdx.x & 31;
     const int sr = p.sr, MARGIN = (sr + 1 + 15) & ~15, BWB = p.W + 2 * MARGIN;
-    const int W = p.W, H = p.H, CW = W / 2, CH = H / 2;
+    const int W = p.W, H = p.H;
     uint8_t* PY = p.pred;
     const int yy = lane >> 1, xoff = (lane & 1) * 8;  // luma: row, 8-pixel half
     int n = 0, rows = 0;
@@ -1827,6 +1827,11 @@ __device__ __forceinline__ void search_body(const SearchParams& p) {
             const int idx = r * p.BW + bx;
             RIV_STAMP(0);
             if (lane == 0) RIV_GSTAMP(idx, 16);
+            // Refresh the prefetched top-right record now if it was not published yet when it
+            // was first read: the load's latency then overlaps the slot wait below instead of
+            // sitting on the chain at the wait for the row above.
+            if (r > 0 && lane == 0 && (pref & 0xffff000000000000ull) != tagbits)
+                pref = ld_rec(p.rec + (r - 1) * p.BW + min(bx + 1, p.BW - 1));
             // ---- FAST: wait for the loader's slot; otherwise prefetch MB bx+1 (columns, current
             // block, table row) and wait for MB bx's data
             const uint8_t* lslot = slots + (size_t)(ln & (LD_RING - 1)) * ld_slot_bytes(p.tstride);
