@@ -177,6 +177,12 @@ riv_status riv_debug_frame_state(riv_encoder* enc, int what, void* out, size_t s
 riv_status riv_libm_fixup_counts(uint32_t* nlog, uint32_t* nexp);
 /* The DCT bases the device uses (T16[i][j], T8[i][j]: sample i, frequency j). */
 void riv_dct_tables(int32_t* t16, int32_t* t8);
+/* Test hook (host only, no reference counterpart): the encoder's DCT-coefficient coder on n
+ * dense blocks of 384 i16 (Y 256, U 64, V 64), laid out as the GPU compaction does, with DC
+ * prediction when intra; threads > 0 codes the full rANS batches on a pool of that many
+ * threads, as the pipelined encoder does.  *len = stream size; up to cap bytes copied. */
+riv_status riv_test_dct_encode(const int16_t* blocks, uint32_t n, int intra, uint32_t threads, uint8_t* out, size_t cap,
+                               size_t* len);
 
 /* ---- Decoder (reitero_decode) up to the YUV reconstruction ---- */
 /* DecodeError (dec/error.rs:4-20): Io, InvalidHeader, DecodingFailed, InvalidFrame,

@@ -93,6 +93,8 @@ def lib():
             getattr(L, n).argtypes = [I16, C.c_float, C.c_float, I16]
         for n in ("oracle_idct16_aq", "oracle_idct8_aq"):
             getattr(L, n).argtypes = [I16, C.c_float, I16]
+        L.oracle_dct_encode.restype = C.c_size_t
+        L.oracle_dct_encode.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t]
         L.oracle_rans_roundtrip.restype = C.c_size_t
         L.oracle_rans_roundtrip.argtypes = [U8, U8, C.c_size_t, U8, U8, C.c_size_t]
         _lib = L
@@ -244,6 +246,16 @@ class OracleDecoder:
             self.close()
         except Exception:
             pass
+
+
+def dct_encode(blocks: np.ndarray, intra: bool) -> bytes:
+    """The oracle's DCT-coefficient coder of one frame on dense (n, 384) int16 blocks."""
+    b = np.ascontiguousarray(blocks, dtype=np.int16)
+    n = b.shape[0]
+    size = lib().oracle_dct_encode(b.ctypes.data, n, int(intra), None, 0)
+    out = np.zeros(max(size, 1), np.uint8)
+    lib().oracle_dct_encode(b.ctypes.data, n, int(intra), out.ctypes.data, size)
+    return out[:size].tobytes()
 
 
 def rgb_to_yuv(rgb: np.ndarray, dw: int, dh: int, sw: int, sh: int) -> Frames:

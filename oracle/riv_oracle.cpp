@@ -2143,4 +2143,23 @@ size_t oracle_rans_roundtrip(const uint8_t* bits, const uint8_t* bypass, size_t 
 }
 double oracle_glibc_logf_check(void) { return (double)logf(10.0f); }
 
+size_t oracle_dct_encode(const int16_t* blocks, int n, int intra, uint8_t* stream, size_t cap) {  // res/rans.rs:195-330
+    init_zero_prob();
+    Bytes s;
+    if (n > 0) {
+        RansEnc w(&s);
+        DctCtx ctx;
+        ctx.dcp = intra != 0;
+        for (int b = 0; b < n; b++) {
+            const int16_t* p = blocks + (size_t)b * 384;
+            dct_encode_plane(w, ctx, p, 256, true, 0);
+            dct_encode_plane(w, ctx, p + 256, 64, false, 1);
+            dct_encode_plane(w, ctx, p + 320, 64, false, 2);
+        }
+        w.finish();
+    }
+    if (stream && cap) memcpy(stream, s.data(), std::min(cap, s.size()));
+    return s.size();
+}
+
 }  // extern "C"

@@ -98,6 +98,10 @@ void oracle_idct8_aq(const int16_t* coeffs64, float qs, int16_t* out64);
 size_t oracle_rans_roundtrip(const uint8_t* bits, const uint8_t* bypass, size_t n, uint8_t* out_bits,
                              uint8_t* stream, size_t stream_cap);
 double oracle_glibc_logf_check(void);
+/* DCT-coefficient coder of one frame (res/rans.rs:195-330) on n dense blocks of 384 i16
+ * (Y 256, U 64, V 64), DC prediction when intra; returns the stream size, copies up to cap
+ * bytes. */
+size_t oracle_dct_encode(const int16_t* blocks, int n, int intra, uint8_t* stream, size_t cap);
 
 #ifdef __cplusplus
 }

@@ -111,7 +111,7 @@ EXPORTED_SYMBOLS = (
     "riv_stage_rgb_to_yuv", "riv_stage_deblock", "riv_stage_libm", "riv_libm_fixup_counts", "riv_dct_tables",
     "riv_debug_frame_state", "riv_counters", "riv_host_times", "riv_stage_deblock_noalloc",
     "riv_decoder_new", "riv_decoder_info", "riv_decode_frame_yuv", "riv_decoder_current_frame",
-    "riv_decoder_last_error", "riv_decoder_free",
+    "riv_decoder_last_error", "riv_decoder_free", "riv_test_dct_encode",
 )
 
 
@@ -126,6 +126,7 @@ def lib() -> C.CDLL:
     L.riv_encode_frame_device.argtypes = [P, P, C.c_uint64, C.POINTER(RivFrameStats)]
     L.riv_encode_frame_yuv.argtypes = [P, U8P, U8P, U8P, C.c_uint64, C.POINTER(RivFrameStats)]
     L.riv_finish.argtypes = [P]
+    L.riv_test_dct_encode.argtypes = [P, C.c_uint32, C.c_int, C.c_uint32, P, C.c_size_t, C.POINTER(C.c_size_t)]
     L.riv_encoder_free.argtypes = [P]
     L.riv_last_error.restype = C.c_char_p
     L.riv_last_error.argtypes = [P]
@@ -537,6 +538,20 @@ def stage_libm(which: int, x: np.ndarray) -> np.ndarray:
     if st:
         raise _ERRORS.get(st, EncodeError)("riv_stage_libm failed")
     return out
+
+
+def dct_encode_host(blocks: np.ndarray, intra: bool, threads: int = 0) -> bytes:
+    """The encoder's host DCT-coefficient coder on dense (n, 384) int16 blocks (test hook,
+    no GPU needed); threads > 0 codes the rANS batches on a pool as the pipelined encoder
+    does."""
+    b = np.ascontiguousarray(blocks, dtype=np.int16)
+    n = C.c_size_t(0)
+    st = lib().riv_test_dct_encode(b.ctypes.data, b.shape[0], int(intra), threads, None, 0, C.byref(n))
+    if st != 0:
+        raise EncodingFailed(f"riv_test_dct_encode failed (status {st})")
+    out = np.zeros(max(n.value, 1), np.uint8)
+    lib().riv_test_dct_encode(b.ctypes.data, b.shape[0], int(intra), threads, out.ctypes.data, n.value, C.byref(n))
+    return out[:n.value].tobytes()
 
 
 def libm_fixup_counts():

@@ -1,0 +1,47 @@
+"""The encoder's host DCT-coefficient coder (riv_entropy.cpp, behind riv_test_dct_encode)
+against the oracle's restatement of res/rans.rs:195-330, byte for byte, on CPU: P-frame
+and intra (DC prediction) blocks, frames shorter than one rANS batch and frames of several
+batches, coded inline and with the full batches on a thread pool as the pipelined encoder
+does."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+
+def _blocks(n, seed, density=0.25, big=False):
+    rng = np.random.default_rng(seed)
+    b = np.zeros((n, 384), np.int16)
+    for plane, (lo, hi, d) in enumerate(((0, 256, density), (256, 320, density / 2), (320, 384, density / 2))):
+        width = hi - lo
+        # significance fades with the coefficient index, like quantised DCT blocks
+        p = d * np.exp(-np.arange(width) / (width / 6.0))
+        mask = rng.random((n, width)) < p
+        mag = rng.geometric(0.4, (n, width)).astype(np.int32)
+        if big:
+            mag[rng.random((n, width)) < 0.01] = rng.integers(100, 4000, 1)[0]
+        sign = np.where(rng.random((n, width)) < 0.5, -1, 1)
+        b[:, lo:hi] = np.where(mask, sign * mag, 0).astype(np.int16)
+    b[::7, 0] = rng.integers(-900, 900, b[::7, 0].shape)  # some large DC values
+    return b
+
+
+@pytest.mark.parametrize("intra", [False, True])
+@pytest.mark.parametrize("threads", [0, 3])
+@pytest.mark.parametrize("n,seed", [(1, 1), (37, 2), (3000, 3)])
+def test_dct_coder_matches_oracle(n, seed, threads, intra):
+    from riv2_b200.encoder import dct_encode_host
+    b = _blocks(n, seed, big=seed == 3)
+    assert dct_encode_host(b, intra, threads) == O.dct_encode(b, intra)
+
+
+def test_dct_coder_spans_several_batches_and_all_zero_blocks():
+    from riv2_b200.encoder import dct_encode_host
+    b = _blocks(6000, 9, density=0.6)
+    b[100:200] = 0                      # all-zero blocks are coded too (EOB class 0)
+    ref = O.dct_encode(b, False)
+    # a binary symbol carries at most 8 bits here (probabilities >= 1/256), so more than
+    # 50,000 bytes means more than 3 rANS batches of 16386 symbols
+    assert len(ref) > 50_000
+    assert dct_encode_host(b, False, 0) == ref
+    assert dct_encode_host(b, False, 4) == ref

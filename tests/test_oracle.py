@@ -299,10 +299,9 @@ def test_cabi_config_default_and_validation():
         E.EncoderConfig.new(64, 64, 30).with_keyframe_interval(E.KeyframeInterval.fixed(0)).validate()
 
 
-def test_entropy_coders_match_oracle_on_host():
-    """The product's host rANS/MV coders reproduce the oracle's records for given GPU-side
-    inputs: checked indirectly by the GPU parity tests; here only that the fix-up table
-    and zero-probability setup load without a device."""
+def test_libm_fixup_tables_load_on_host():
+    """The glibc fix-up tables load without a device (the coefficient coder itself is pinned
+    against the oracle in test_entropy_host.py, the MV coder by the GPU parity tests)."""
     from riv2_b200.encoder import libm_fixup_counts
     nlog, nexp = libm_fixup_counts()
     assert 1000 < nlog < 200000 and 1000 < nexp < 500000
