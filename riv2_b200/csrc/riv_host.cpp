@@ -676,10 +676,10 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         CK(cudaEventRecord(s.ev_h2d, e->Hs));
         CK(cudaStreamWaitEvent(Y, s.ev_h2d, 0));
         mark(e, j, EV_START, Y);
-        CK(launch_rgb_to_yuv((const uint8_t*)s.rgb.p, (int)c.display_width, (int)c.display_height, cur, W, H, Y));
+        CK(launch_rgb_to_yuv((const uint8_t*)s.rgb.p, (int)c.display_width, (int)c.display_height, cur, W, H, Y, e->defer_ok));
     } else if (src == 1) {
         mark(e, j, EV_START, Y);
-        CK(launch_rgb_to_yuv((const uint8_t*)a, (int)c.display_width, (int)c.display_height, cur, W, H, Y));
+        CK(launch_rgb_to_yuv((const uint8_t*)a, (int)c.display_width, (int)c.display_height, cur, W, H, Y, e->defer_ok));
     } else {
         uint8_t* d = s.rgb.as<uint8_t>();
         size_t ys = (size_t)W * H, cs = ys / 4;
@@ -1472,6 +1472,41 @@ riv_status riv_libm_fixup_counts(uint32_t* nlog, uint32_t* nexp) {
 }
 
 void riv_dct_tables(int32_t* t16, int32_t* t8) { dct_tables(t16, t8); }
+
+riv_status riv_test_dct_encode(const int16_t* blocks, uint32_t n, int intra, uint32_t threads, uint8_t* out, size_t cap,
+                               size_t* len) {
+    if ((n > 0 && !blocks) || !len) return RIV_ERR_FRAME;
+    entropy_init();
+    // the GPU compaction's layout: per plane the run up to the last non-zero coefficient
+    // (with DC prediction the last non-zero AC coefficient), and that index
+    std::vector<int16_t> packed;
+    std::vector<uint8_t> eobs((size_t)n * 3);
+    static const int base[3] = {0, 256, 320}, len3[3] = {256, 64, 64};
+    for (uint32_t b = 0; b < n; b++)
+        for (int pl = 0; pl < 3; pl++) {
+            const int16_t* p = blocks + (size_t)b * 384 + base[pl];
+            int last = 0;
+            for (int i = len3[pl] - 1; i >= (intra ? 1 : 0); i--)
+                if (p[i] != 0) { last = i; break; }
+            eobs[(size_t)b * 3 + pl] = (uint8_t)last;
+            packed.insert(packed.end(), p, p + last + 1);
+        }
+    std::vector<uint8_t> stream;
+    try {
+        if (threads > 0) {
+            ThreadPool pool(threads);
+            BatchSubmit sub = [&pool](std::function<void()> f) { return pool.submit(std::move(f)); };
+            encode_residual_frame(packed.data(), eobs.data(), (int)n, intra != 0, stream, &sub);
+        } else {
+            encode_residual_frame(packed.data(), eobs.data(), (int)n, intra != 0, stream);
+        }
+    } catch (const std::exception&) {
+        return RIV_ERR_ENCODING_FAILED;
+    }
+    *len = stream.size();
+    if (out && cap) memcpy(out, stream.data(), std::min(cap, stream.size()));
+    return RIV_OK;
+}
 
 }  // extern "C"
 

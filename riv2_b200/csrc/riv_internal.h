@@ -122,7 +122,7 @@ enum StatusBits : unsigned {
 };
 
 // Launchers (riv_kernels.cu).  All are asynchronous on `stream`.
-int launch_rgb_to_yuv(const uint8_t* rgb, int dw, int dh, uint8_t* yuv, int W, int H, void* stream);
+int launch_rgb_to_yuv(const uint8_t* rgb, int dw, int dh, uint8_t* yuv, int W, int H, void* stream, bool beside = false);
 // Launch plan of the search wavefront (chosen once per encoder).  fused: the SAD table is
 // computed inside the same cooperative launch by `grid - nrow` worker CTAs.
 struct SearchPlan {

@@ -57,11 +57,13 @@ __global__ void k_rgb_to_yuv(const uint8_t* __restrict__ rgb, int dw, int dh, ui
         rgb_to_yuv_quad(rgb, dw, dh, Yp, Up, Vp, W, q % cw, q / cw);
 }
 
-int launch_rgb_to_yuv(const uint8_t* rgb, int dw, int dh, uint8_t* yuv, int W, int H, void* stream) {
-    // One 128-thread CTA (4K registers) per SM at most: every SM keeps room for a search CTA
-    // (61,440 registers), so a search launch never waits for a conversion to drain.
-    // Its preferred shared-memory carveout is the search kernel's (maximum shared memory), so
-    // an SM that ran a conversion CTA needs no reconfiguration before the next search CTA.
+// `beside`: the conversion runs while a search launch holds the SMs, so one 128-thread CTA
+// (4K registers) per SM at most: every SM keeps room for a search CTA (61,440 registers) and a
+// search launch never waits for a conversion to drain.  Otherwise one CTA per 128 quads (the
+// conversion alone on the GPU, as fast as it goes).  Either way the preferred shared-memory
+// carveout is the search kernel's (maximum shared memory), so an SM that ran a conversion CTA
+// needs no reconfiguration before the next search CTA.
+int launch_rgb_to_yuv(const uint8_t* rgb, int dw, int dh, uint8_t* yuv, int W, int H, void* stream, bool beside) {
     static int nsm = 0;
     if (nsm == 0) {
         int dev = 0;
@@ -70,7 +72,7 @@ int launch_rgb_to_yuv(const uint8_t* rgb, int dw, int dh, uint8_t* yuv, int W, i
         cudaFuncSetAttribute(k_rgb_to_yuv, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
     }
     const int nq = (W / 2) * (H / 2);
-    const int blk = 128, grd = std::max(1, std::min(nsm, (nq + blk - 1) / blk));
+    const int blk = 128, grd = std::max(1, beside ? std::min(nsm, (nq + blk - 1) / blk) : (nq + blk - 1) / blk);
     uint8_t* Y = yuv;
     uint8_t* U = yuv + (size_t)W * H;
     uint8_t* V = U + (size_t)(W / 2) * (H / 2);
