@@ -205,7 +205,10 @@ riv_dec_status riv_decoder_info(const riv_decoder* dec, uint32_t* dims5, uint64_
 /* Decoder::decode_frame (dec/decoder.rs:174-460) up to the storage-size YUV 4:2:0
  * reconstruction (the reference's final RGB conversion and crop are not on this path).
  * y/u/v (each nullable) receive the planes; the call returns once the frame is decoded.
- * RIV_DEC_END_OF_STREAM after the last frame. */
+ * RIV_DEC_END_OF_STREAM after the last frame.  Records are read up to 8 frames ahead: their
+ * MVs are decoded in order on the calling thread and their coefficient streams on a pool of
+ * host threads; a record that cannot be read is reported by the call for that frame (the
+ * frames before it decode normally). */
 riv_dec_status riv_decode_frame_yuv(riv_decoder* dec, uint8_t* y, uint8_t* u, uint8_t* v, uint32_t* frame_type,
                                     uint64_t* timestamp_ms);
 /* Decoder::current_frame (dec/decoder.rs:475-478). */

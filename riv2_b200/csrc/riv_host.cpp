@@ -1527,24 +1527,46 @@ static uint64_t get_le(const uint8_t* b, int n) {
 }
 }  // namespace
 
+// One record read ahead of the GPU: parsed, its MVs decoded and reconstructed (in order, on
+// the calling thread: the MV coder's contexts and the temporal MVs carry across frames), its
+// coefficients decoding on the pool (each frame's coefficient coder starts from fresh
+// contexts, so several frames decode at once).
+struct DecSlot {
+    bool filled = false;
+    riv_dec_status st = RIV_DEC_OK;  // a record that could not be read: reported when reached
+    std::string msg;
+    int type = 0;
+    uint8_t q = 0;
+    uint64_t ts = 0;
+    HostBuf hcoeffs, hmbout, hskip, hfmask;  // pinned staging for the uploads
+    std::vector<uint8_t> coded;
+    bool coef_ok = false;
+    std::future<void> coef;
+};
+constexpr int DEC_AHEAD = 8;
+
 struct riv_decoder {
     std::vector<uint8_t> data;
-    size_t pos = 36;
     uint32_t dw = 0, dh = 0, sw = 0, sh = 0, fps = 0;
     uint64_t frame_count = 0, current = 0;
     int W = 0, H = 0, BW = 0, BH = 0, N = 0;
     int device = 0;
     std::string err;
-    bool poisoned = false, has_ref = false, has_prev_mvs = false;
+    bool poisoned = false, has_ref = false;
     int ref_cur = 0;
     cudaStream_t S = nullptr;
     DevBuf ref[2], recon_pre, pred, coeffs, mbout, skip, fmask, varsum, lnv, qs, logfix, expfix, ytab, ctab;
-    HostBuf hcoeffs, hmbout, hskip, hfmask;
     int nlog = 0, nexp = 0;
+    // read-ahead state (records up to DEC_AHEAD frames past `current`)
+    DecSlot slots[DEC_AHEAD];
+    uint64_t ahead = 0;       // next frame to read ahead
+    size_t ahead_pos = 36;    // its record's offset
+    bool ahead_stop = false;  // a record could not be read: nothing after it is read
+    bool ahead_ref = false;   // a key frame was read (inter records have a reference)
     riv::MvCoder mvc;
     std::vector<DecMv> prev_mvs, mvs;
     std::vector<riv::MvCodedBlock> blocks;
-    std::vector<uint8_t> coded;
+    std::unique_ptr<ThreadPool> pool;  // coefficient decoding
 };
 
 static riv_dec_status dec_fail(riv_decoder* d, riv_dec_status s, const std::string& m) {
@@ -1552,6 +1574,122 @@ static riv_dec_status dec_fail(riv_decoder* d, riv_dec_status s, const std::stri
     if (s == RIV_DEC_CUDA) d->poisoned = true;
     return s;
 }
+
+// Read frame `d->ahead`'s record into its slot: parse it, decode and reconstruct its MVs (in
+// frame order), and start its coefficient decoding on the pool.  A record that cannot be read
+// is kept in the slot as an error, reported when that frame is requested; nothing after it
+// is read (dec/decoder.rs:174-460).
+static void dec_read_ahead(riv_decoder* d) {
+    DecSlot& sl = d->slots[d->ahead % DEC_AHEAD];
+    d->ahead++;
+    sl.filled = true;
+    sl.st = RIV_DEC_OK;
+    sl.msg.clear();
+    auto stop = [&](riv_dec_status st, const char* m) {
+        sl.st = st;
+        sl.msg = m;
+        d->ahead_stop = true;
+    };
+    const uint8_t* b = d->data.data() + d->ahead_pos;
+    const size_t left = d->data.size() - d->ahead_pos;
+    if (left < 9) return stop(RIV_DEC_IO, "truncated record");
+    sl.ts = get_le(b, 8);
+    sl.type = b[8];
+    const int N = d->N;
+    const uint8_t* cdata = nullptr;
+    size_t clen = 0;
+    if (sl.type == 1) {  // intra (residual.rs:815-887)
+        if (left < 14) return stop(RIV_DEC_IO, "truncated intra record");
+        sl.q = b[9];
+        clen = get_le(b + 10, 4);
+        if (left < 14 + clen) return stop(RIV_DEC_IO, "truncated intra payload");
+        cdata = b + 14;
+        sl.coded.assign(N, 1);
+        d->ahead_pos += 14 + clen;
+        d->prev_mvs.clear();
+        d->mvc.reset();
+        d->ahead_ref = true;
+    } else if (sl.type == 2) {  // inter (residual.rs:889-1079, decoder.rs:255-430)
+        if (left < 17 || !d->ahead_ref) return stop(RIV_DEC_INVALID_FRAME, "inter frame without a reference");
+        sl.q = b[9];
+        const int biasx = (int8_t)b[10], biasy = (int8_t)b[11];
+        const size_t mvs = get_le(b + 13, 4);
+        if (left < 17 + mvs + 4) return stop(RIV_DEC_IO, "truncated motion data");
+        const uint8_t* mvd = b + 17;
+        clen = get_le(b + 17 + mvs, 4);
+        if (left < 21 + mvs + clen) return stop(RIV_DEC_IO, "truncated residual data");
+        cdata = b + 21 + mvs;
+        if (!d->mvc.decode_frame(mvd, mvs, d->BW, d->BH, d->blocks))
+            return stop(RIV_DEC_INVALID_FRAME, "malformed motion data");
+        const bool tm = !d->prev_mvs.empty();
+        // MV reconstruction in raster order from the decoded neighbours (mv_predictor.rs)
+        const int BW = d->BW;
+        d->mvs.assign(N, DecMv{});
+        sl.coded.assign(N, 0);
+        MbOut* mo = sl.hmbout.as<MbOut>();
+        uint8_t* hs = sl.hskip.as<uint8_t>();
+        uint8_t* hf = sl.hfmask.as<uint8_t>();
+        for (int i = 0; i < N; i++) {
+            const riv::MvCodedBlock& cb = d->blocks[i];
+            const int bx = i % BW, by = i / BW;
+            const bool hl = bx > 0, ht = by > 0, htr = by > 0 && bx + 1 < BW, htl = by > 0 && bx > 0;
+            const DecMv L = hl ? d->mvs[i - 1] : DecMv{}, T = ht ? d->mvs[i - BW] : DecMv{};
+            const DecMv TR = htr ? d->mvs[i - BW + 1] : DecMv{}, TL = htl ? d->mvs[i - BW - 1] : DecMv{};
+            const DecMv TM = tm ? d->prev_mvs[i] : DecMv{};
+            DecMv cand[5];
+            int nc = 0;
+            auto add = [&](bool has, const DecMv& m) {
+                if (!has) return;
+                for (int k = 0; k < nc; k++)
+                    if (cand[k] == m) return;
+                cand[nc++] = m;
+            };
+            add(hl, L); add(ht, T); add(htr, TR); add(htl, TL); add(tm, TM);
+            const DecMv nearest = nc > 0 ? cand[0] : DecMv{}, nearm = nc > 1 ? cand[1] : DecMv{};
+            const DecMv temporal = tm ? TM : DecMv{};
+            DecMv base{};
+            switch (cb.mode) {
+                case riv::M_ZERO: break;
+                case riv::M_NEAREST: base = nearest; break;
+                case riv::M_NEAR: base = nearm; break;
+                case riv::M_TOPRIGHT: base = htr ? TR : nearest; break;
+                case riv::M_TOPLEFT: base = htl ? TL : nearest; break;
+                case riv::M_TEMPORAL: base = temporal; break;
+                default:
+                    base = cb.new_base == 0 ? nearest : cb.new_base == 1 ? nearm
+                           : cb.new_base == 2 ? (htr ? TR : nearest)
+                           : cb.new_base == 3 ? (htl ? TL : nearest) : cb.new_base == 4 ? temporal : nearest;
+            }
+            DecMv m;
+            if (cb.mode == riv::M_NEW) {
+                m.dx = sat8i(base.dx + sat8i(cb.dx + biasx));
+                m.dy = sat8i(base.dy + sat8i(cb.dy + biasy));
+                m.sx = cb.spx == riv::SP_PLUS ? 1 : (cb.spx == riv::SP_MINUS ? -1 : 0);
+                m.sy = cb.spy == riv::SP_PLUS ? 1 : (cb.spy == riv::SP_MINUS ? -1 : 0);
+            } else {
+                m = base;
+            }
+            d->mvs[i] = m;
+            MbOut o{};
+            o.raw[0] = m.dx; o.raw[1] = m.dy; o.raw[2] = m.sx; o.raw[3] = m.sy;
+            mo[i] = o;
+            hs[i] = cb.skip ? 1 : 0;
+            hf[i] = (!cb.skip || m.dx || m.dy || m.sx || m.sy) ? 1 : 0;
+            sl.coded[i] = cb.skip ? 0 : 1;
+        }
+        d->ahead_pos += 21 + mvs + clen;
+        d->prev_mvs.swap(d->mvs);
+    } else {
+        return stop(RIV_DEC_INVALID_FRAME, "unknown frame type");
+    }
+    const bool intra = sl.type == 1;
+    DecSlot* ps = &sl;
+    sl.coef_ok = false;
+    sl.coef = d->pool->submit([ps, cdata, clen, N, intra] {
+        ps->coef_ok = riv::decode_residual_frame(cdata, clen, ps->coded.data(), N, intra, ps->hcoeffs.as<int16_t>());
+    });
+}
+
 
 extern "C" {
 
@@ -1601,10 +1739,12 @@ riv_dec_status riv_decoder_new(const uint8_t* data, size_t len, int device, riv_
         d->qs.alloc(N * sizeof(float));
         d->ytab.alloc(256 * 2);
         d->ctab.alloc(64 * 2);
-        d->hcoeffs.alloc(N * 384 * 2);
-        d->hmbout.alloc(N * sizeof(MbOut));
-        d->hskip.alloc(N);
-        d->hfmask.alloc(N);
+        for (DecSlot& sl : d->slots) {
+            sl.hcoeffs.alloc(N * 384 * 2);
+            sl.hmbout.alloc(N * sizeof(MbOut));
+            sl.hskip.alloc(N);
+            sl.hfmask.alloc(N);
+        }
         d->nlog = (int)(F.logf.size() / 2);
         d->nexp = (int)(F.exp2f.size() / 2);
         d->logfix.alloc(F.logf_dev.size() * 4);
@@ -1620,6 +1760,8 @@ riv_dec_status riv_decoder_new(const uint8_t* data, size_t len, int device, riv_
         return RIV_DEC_CUDA;
     }
     riv::entropy_init();
+    const unsigned hw = std::thread::hardware_concurrency();
+    d->pool.reset(new ThreadPool(std::max(1u, std::min((unsigned)DEC_AHEAD, hw > 1 ? hw - 1 : 1u))));
     *out = d;
     return RIV_DEC_OK;
 }
@@ -1641,11 +1783,18 @@ riv_dec_status riv_decode_frame_yuv(riv_decoder* d, uint8_t* y, uint8_t* u, uint
     if (!d) return RIV_DEC_INVALID_HEADER;
     if (d->poisoned) return dec_fail(d, RIV_DEC_CUDA, "decoder unusable after a device failure");
     if (d->current >= d->frame_count) return dec_fail(d, RIV_DEC_END_OF_STREAM, "end of stream");
-    const uint8_t* b = d->data.data() + d->pos;
-    const size_t left = d->data.size() - d->pos;
-    if (left < 9) return dec_fail(d, RIV_DEC_IO, "truncated record");
-    const uint64_t ts = get_le(b, 8);
-    const int type = b[8];
+    try {
+        while (!d->ahead_stop && d->ahead < d->frame_count && d->ahead < d->current + DEC_AHEAD) dec_read_ahead(d);
+    } catch (const std::exception& ex) {
+        return dec_fail(d, RIV_DEC_DECODING_FAILED, ex.what());
+    }
+    DecSlot& sl = d->slots[d->current % DEC_AHEAD];
+    if (!sl.filled) return dec_fail(d, RIV_DEC_IO, "truncated record");
+    if (sl.st != RIV_DEC_OK) return dec_fail(d, sl.st, sl.msg);
+    sl.coef.wait();
+    const int type = sl.type;
+    if (!sl.coef_ok)
+        return dec_fail(d, RIV_DEC_INVALID_FRAME, type == 1 ? "malformed intra coefficient data" : "malformed residual data");
     const int W = d->W, H = d->H, N = d->N;
     const size_t ysz = (size_t)W * H, csz = ysz / 4;
     const int nxt = d->ref_cur ^ 1;
@@ -1653,23 +1802,14 @@ riv_dec_status riv_decode_frame_yuv(riv_decoder* d, uint8_t* y, uint8_t* u, uint
     try {
         CK(cudaSetDevice(d->device));
         cudaStream_t S = d->S;
-        if (type == 1) {  // intra (residual.rs:815-887)
-            if (left < 14) return dec_fail(d, RIV_DEC_IO, "truncated intra record");
-            const uint8_t q = b[9];
-            const size_t sz = get_le(b + 10, 4);
-            if (left < 14 + sz) return dec_fail(d, RIV_DEC_IO, "truncated intra payload");
-            d->coded.assign(N, 1);
-            // the previous frame's copies out of the pinned staging are complete (the last
-            // call synchronised)
-            if (!riv::decode_residual_frame(b + 14, sz, d->coded.data(), N, true, d->hcoeffs.as<int16_t>()))
-                return dec_fail(d, RIV_DEC_INVALID_FRAME, "malformed intra coefficient data");
+        const int level = deblock_level(quant_step(sl.q));
+        uint8_t* target = level > 0 ? d->recon_pre.as<uint8_t>() : recon;
+        if (type == 1) {
             uint16_t yt[256], ct[64];
-            intra_tables(quant_step(q), yt, ct);
+            intra_tables(quant_step(sl.q), yt, ct);
             CK(cudaMemcpyAsync(d->ytab.p, yt, sizeof yt, cudaMemcpyHostToDevice, S));
             CK(cudaMemcpyAsync(d->ctab.p, ct, sizeof ct, cudaMemcpyHostToDevice, S));
-            CK(cudaMemcpyAsync(d->coeffs.p, d->hcoeffs.p, (size_t)N * 768, cudaMemcpyHostToDevice, S));
-            const int level = deblock_level(quant_step(q));
-            uint8_t* target = level > 0 ? d->recon_pre.as<uint8_t>() : recon;
+            CK(cudaMemcpyAsync(d->coeffs.p, sl.hcoeffs.p, (size_t)N * 768, cudaMemcpyHostToDevice, S));
             CK(launch_reconstruct(d->coeffs.as<int16_t>(), nullptr, nullptr, nullptr, 1, d->ytab.as<uint16_t>(),
                                   d->ctab.as<uint16_t>(), target, W, H, S));
             if (level > 0) {
@@ -1677,90 +1817,16 @@ riv_dec_status riv_decode_frame_yuv(riv_decoder* d, uint8_t* y, uint8_t* u, uint
                 deblock_thresholds(level, true, E, I, Hv);
                 CK(launch_deblock_tiled(target, recon, W, H, E, I, Hv, nullptr, S));
             }
-            d->pos += 14 + sz;
-            d->has_prev_mvs = false;
-            d->prev_mvs.clear();
-            d->mvc.reset();
-        } else if (type == 2) {  // inter (residual.rs:889-1079, decoder.rs:255-430)
-            if (left < 17 || !d->has_ref) return dec_fail(d, RIV_DEC_INVALID_FRAME, "inter frame without a reference");
-            const uint8_t q = b[9];
-            const int biasx = (int8_t)b[10], biasy = (int8_t)b[11];
-            const size_t mvs = get_le(b + 13, 4);
-            if (left < 17 + mvs + 4) return dec_fail(d, RIV_DEC_IO, "truncated motion data");
-            const uint8_t* mvd = b + 17;
-            const size_t rs = get_le(b + 17 + mvs, 4);
-            if (left < 21 + mvs + rs) return dec_fail(d, RIV_DEC_IO, "truncated residual data");
-            const uint8_t* rd = b + 21 + mvs;
-            if (!d->mvc.decode_frame(mvd, mvs, d->BW, d->BH, d->blocks))
-                return dec_fail(d, RIV_DEC_INVALID_FRAME, "malformed motion data");
-            // MV reconstruction in raster order from the decoded neighbours (mv_predictor.rs)
-            const int BW = d->BW;
-            d->mvs.assign(N, DecMv{});
-            d->coded.assign(N, 0);
-            MbOut* mo = d->hmbout.as<MbOut>();
-            uint8_t* hs = d->hskip.as<uint8_t>();
-            uint8_t* hf = d->hfmask.as<uint8_t>();
-            const bool tm = d->has_prev_mvs;
-            for (int i = 0; i < N; i++) {
-                const riv::MvCodedBlock& cb = d->blocks[i];
-                const int bx = i % BW, by = i / BW;
-                const bool hl = bx > 0, ht = by > 0, htr = by > 0 && bx + 1 < BW, htl = by > 0 && bx > 0;
-                const DecMv L = hl ? d->mvs[i - 1] : DecMv{}, T = ht ? d->mvs[i - BW] : DecMv{};
-                const DecMv TR = htr ? d->mvs[i - BW + 1] : DecMv{}, TL = htl ? d->mvs[i - BW - 1] : DecMv{};
-                const DecMv TM = tm ? d->prev_mvs[i] : DecMv{};
-                DecMv cand[5];
-                int nc = 0;
-                auto add = [&](bool has, const DecMv& m) {
-                    if (!has) return;
-                    for (int k = 0; k < nc; k++)
-                        if (cand[k] == m) return;
-                    cand[nc++] = m;
-                };
-                add(hl, L); add(ht, T); add(htr, TR); add(htl, TL); add(tm, TM);
-                const DecMv nearest = nc > 0 ? cand[0] : DecMv{}, nearm = nc > 1 ? cand[1] : DecMv{};
-                const DecMv temporal = tm ? TM : DecMv{};
-                DecMv base{};
-                switch (cb.mode) {
-                    case riv::M_ZERO: break;
-                    case riv::M_NEAREST: base = nearest; break;
-                    case riv::M_NEAR: base = nearm; break;
-                    case riv::M_TOPRIGHT: base = htr ? TR : nearest; break;
-                    case riv::M_TOPLEFT: base = htl ? TL : nearest; break;
-                    case riv::M_TEMPORAL: base = temporal; break;
-                    default:
-                        base = cb.new_base == 0 ? nearest : cb.new_base == 1 ? nearm
-                               : cb.new_base == 2 ? (htr ? TR : nearest)
-                               : cb.new_base == 3 ? (htl ? TL : nearest) : cb.new_base == 4 ? temporal : nearest;
-                }
-                DecMv m;
-                if (cb.mode == riv::M_NEW) {
-                    m.dx = sat8i(base.dx + sat8i(cb.dx + biasx));
-                    m.dy = sat8i(base.dy + sat8i(cb.dy + biasy));
-                    m.sx = cb.spx == riv::SP_PLUS ? 1 : (cb.spx == riv::SP_MINUS ? -1 : 0);
-                    m.sy = cb.spy == riv::SP_PLUS ? 1 : (cb.spy == riv::SP_MINUS ? -1 : 0);
-                } else {
-                    m = base;
-                }
-                d->mvs[i] = m;
-                MbOut o{};
-                o.raw[0] = m.dx; o.raw[1] = m.dy; o.raw[2] = m.sx; o.raw[3] = m.sy;
-                mo[i] = o;
-                hs[i] = cb.skip ? 1 : 0;
-                hf[i] = (!cb.skip || m.dx || m.dy || m.sx || m.sy) ? 1 : 0;
-                d->coded[i] = cb.skip ? 0 : 1;
-            }
-            if (!riv::decode_residual_frame(rd, rs, d->coded.data(), N, false, d->hcoeffs.as<int16_t>()))
-                return dec_fail(d, RIV_DEC_INVALID_FRAME, "malformed residual data");
-            CK(cudaMemcpyAsync(d->mbout.p, mo, (size_t)N * sizeof(MbOut), cudaMemcpyHostToDevice, S));
-            CK(cudaMemcpyAsync(d->skip.p, hs, N, cudaMemcpyHostToDevice, S));
-            CK(cudaMemcpyAsync(d->fmask.p, hf, N, cudaMemcpyHostToDevice, S));
-            CK(cudaMemcpyAsync(d->coeffs.p, d->hcoeffs.p, (size_t)N * 768, cudaMemcpyHostToDevice, S));
+        } else {
+            if (!d->has_ref) return dec_fail(d, RIV_DEC_INVALID_FRAME, "inter frame without a reference");
+            CK(cudaMemcpyAsync(d->mbout.p, sl.hmbout.p, (size_t)N * sizeof(MbOut), cudaMemcpyHostToDevice, S));
+            CK(cudaMemcpyAsync(d->skip.p, sl.hskip.p, N, cudaMemcpyHostToDevice, S));
+            CK(cudaMemcpyAsync(d->fmask.p, sl.hfmask.p, N, cudaMemcpyHostToDevice, S));
+            CK(cudaMemcpyAsync(d->coeffs.p, sl.hcoeffs.p, (size_t)N * 768, cudaMemcpyHostToDevice, S));
             const uint8_t* ref = d->ref[d->ref_cur].as<uint8_t>();
             CK(launch_predict(ref, d->mbout.as<MbOut>(), d->pred.as<uint8_t>(), d->varsum.as<uint2>(), W, H, S));
-            CK(launch_aq(d->varsum.as<uint2>(), N, quant_step(q), d->logfix.as<uint32_t>(), d->nlog,
+            CK(launch_aq(d->varsum.as<uint2>(), N, quant_step(sl.q), d->logfix.as<uint32_t>(), d->nlog,
                          d->expfix.as<uint32_t>(), d->nexp, d->lnv.as<float>(), d->qs.as<float>(), S));
-            const int level = deblock_level(quant_step(q));
-            uint8_t* target = level > 0 ? d->recon_pre.as<uint8_t>() : recon;
             CK(launch_reconstruct(d->coeffs.as<int16_t>(), d->pred.as<uint8_t>(), d->skip.as<uint8_t>(),
                                   d->qs.as<float>(), 0, nullptr, nullptr, target, W, H, S));
             if (level > 0) {
@@ -1768,24 +1834,20 @@ riv_dec_status riv_decode_frame_yuv(riv_decoder* d, uint8_t* y, uint8_t* u, uint
                 deblock_thresholds(level, false, E, I, Hv);
                 CK(launch_deblock_tiled(target, recon, W, H, E, I, Hv, d->fmask.as<uint8_t>(), S));
             }
-            d->pos += 21 + mvs + rs;
-            d->prev_mvs.swap(d->mvs);
-            d->has_prev_mvs = true;
-        } else {
-            return dec_fail(d, RIV_DEC_INVALID_FRAME, "unknown frame type");
         }
         if (y) CK(cudaMemcpyAsync(y, recon, ysz, cudaMemcpyDeviceToHost, S));
         if (u) CK(cudaMemcpyAsync(u, recon + ysz, csz, cudaMemcpyDeviceToHost, S));
         if (v) CK(cudaMemcpyAsync(v, recon + ysz + csz, csz, cudaMemcpyDeviceToHost, S));
-        // the pinned staging buffers are rewritten by the next call: finish this frame
+        // the slot's pinned staging is refilled by a later read-ahead: finish this frame
         CK(cudaStreamSynchronize(S));
     } catch (const CudaError& ce) {
         return dec_fail(d, RIV_DEC_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
     }
+    sl.filled = false;
     d->ref_cur = nxt;
     d->has_ref = true;
     if (frame_type) *frame_type = (uint32_t)type;
-    if (timestamp_ms) *timestamp_ms = ts;
+    if (timestamp_ms) *timestamp_ms = sl.ts;
     d->current++;
     return RIV_DEC_OK;
 }
@@ -1797,8 +1859,11 @@ void riv_decoder_free(riv_decoder* d) {
     DevBuf* bufs[] = {&d->ref[0], &d->ref[1], &d->recon_pre, &d->pred, &d->coeffs, &d->mbout, &d->skip, &d->fmask,
                       &d->varsum, &d->lnv, &d->qs, &d->logfix, &d->expfix, &d->ytab, &d->ctab};
     for (DevBuf* x : bufs) x->release();
-    HostBuf* hb[] = {&d->hcoeffs, &d->hmbout, &d->hskip, &d->hfmask};
-    for (HostBuf* x : hb) x->release();
+    d->pool.reset();  // finishes the coefficient decodes still queued (they write the slots)
+    for (DecSlot& sl : d->slots) {
+        HostBuf* hb[] = {&sl.hcoeffs, &sl.hmbout, &sl.hskip, &sl.hfmask};
+        for (HostBuf* x : hb) x->release();
+    }
     if (d->S) cudaStreamDestroy(d->S);
     delete d;
 }
