@@ -1783,11 +1783,16 @@ riv_dec_status riv_decode_frame_yuv(riv_decoder* d, uint8_t* y, uint8_t* u, uint
     if (!d) return RIV_DEC_INVALID_HEADER;
     if (d->poisoned) return dec_fail(d, RIV_DEC_CUDA, "decoder unusable after a device failure");
     if (d->current >= d->frame_count) return dec_fail(d, RIV_DEC_END_OF_STREAM, "end of stream");
-    try {
-        while (!d->ahead_stop && d->ahead < d->frame_count && d->ahead < d->current + DEC_AHEAD) dec_read_ahead(d);
-    } catch (const std::exception& ex) {
-        return dec_fail(d, RIV_DEC_DECODING_FAILED, ex.what());
-    }
+    auto read_ahead = [&](uint64_t upto) -> bool {  // frames before `upto`
+        try {
+            while (!d->ahead_stop && d->ahead < d->frame_count && d->ahead < upto) dec_read_ahead(d);
+        } catch (const std::exception& ex) {
+            dec_fail(d, RIV_DEC_DECODING_FAILED, ex.what());
+            return false;
+        }
+        return true;
+    };
+    if (!read_ahead(d->current + 1)) return RIV_DEC_DECODING_FAILED;  // this frame; the rest while the GPU works
     DecSlot& sl = d->slots[d->current % DEC_AHEAD];
     if (!sl.filled) return dec_fail(d, RIV_DEC_IO, "truncated record");
     if (sl.st != RIV_DEC_OK) return dec_fail(d, sl.st, sl.msg);
@@ -1838,7 +1843,10 @@ riv_dec_status riv_decode_frame_yuv(riv_decoder* d, uint8_t* y, uint8_t* u, uint
         if (y) CK(cudaMemcpyAsync(y, recon, ysz, cudaMemcpyDeviceToHost, S));
         if (u) CK(cudaMemcpyAsync(u, recon + ysz, csz, cudaMemcpyDeviceToHost, S));
         if (v) CK(cudaMemcpyAsync(v, recon + ysz + csz, csz, cudaMemcpyDeviceToHost, S));
-        // the slot's pinned staging is refilled by a later read-ahead: finish this frame
+        // read the next frames while the GPU reconstructs this one (their slots are not this
+        // frame's, whose staging the copies above read), then finish this frame; a failure
+        // here is reported by the next call, which reads its frame first
+        read_ahead(d->current + DEC_AHEAD);
         CK(cudaStreamSynchronize(S));
     } catch (const CudaError& ce) {
         return dec_fail(d, RIV_DEC_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
