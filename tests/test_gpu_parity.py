@@ -240,6 +240,37 @@ def test_encode_pipelined_is_identical():
     assert g0 == o0 == g4
 
 
+def test_deferred_reconstruction_flush_paths():
+    """From pipeline depth 2 a P-frame is reconstructed inside the next P-frame's search
+    launch; before a key frame, for a per-frame-stats call, for last_recon and at finish it
+    is reconstructed with separate kernels instead.  A mix of all of them gives the oracle's
+    stream, last_recon returns the oracle's reconstruction of the frame just submitted, and
+    both kinds of reconstruction occur."""
+    from riv2_b200 import encoder as E
+    frames = _clip("cif", 14, seed=5)
+    gc, oc = _cfgs(352, 288, keyint=5)
+    gc = gc.with_pipeline_depth(16)
+    w = E.VecWriter()
+    enc = E.Encoder.new(gc, w)
+    oenc = O.OracleEncoder(oc)
+    for t, f in enumerate(frames):
+        assert oenc.encode_rgb(f, t * 20) == 0
+        fr = E.Frame(f, 352, 288, t * 20)
+        if t % 6 == 3:
+            assert enc.encode_frame_with_stats(fr).frame_index == t
+        else:
+            enc.encode_frame(fr)
+        if t in (7, 8, 12):
+            y, u, v = enc.last_recon()
+            r = oenc.last("recon")
+            assert np.array_equal(y, r.y) and np.array_equal(u, r.u) and np.array_equal(v, r.v), t
+    enc.finish()
+    c = enc.counters()
+    assert w.into_inner() == oenc.finish()
+    enc.close()
+    assert 0 < c["deferred_pframes"] < c["pframes"]
+
+
 @pytest.mark.parametrize("q", [(85, 80), (95, 90)])
 def test_encode_1080p_matches_oracle(q):
     frames = _clip("1080p", 3, seed=2)
