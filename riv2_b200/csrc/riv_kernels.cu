@@ -358,7 +358,8 @@ __device__ __forceinline__ int argmin8(long long total, bool valid, long long& b
 // Phase stamps, written when p.prof is set: RIV_PROF_WORDS i64 per MB.  Words 0-15 are SM clock
 // cycles (clock64) of the search and mode warps; words 16-27 are %globaltimer nanoseconds,
 // comparable across SMs: 16/17 search warp MB start / slot ready; 18/19 deferred residual of
-// the MB pair starting here; 20/21/22 deblock tile (wait start, work start, end); 23/24/25
+// the MB pair starting here (of MB (r, 1): the AQ fold's end of row r's sum / logs); 30 / 31
+// the mode warp's decision / the AQ warp's variance of the MB; 20/21/22 deblock tile (wait start, work start, end); 23/24/25
 // SAD-table MB (wait start, work start, end); 26/27 the row loader's wait for reference bands.
 __device__ __forceinline__ long long gtimer() {
     unsigned long long t;
@@ -1076,6 +1077,7 @@ __device__ __forceinline__ void mode_warp(const SearchParams& p, const unsigned 
                     make_char4((signed char)coded.dx, (signed char)coded.dy, (signed char)coded.sx, (signed char)coded.sy);
             }
             RIV_STAMP(6);
+            if (lane == 0) RIV_GSTAMP(idx, 30);
             L_cod = coded;
             vTL = vT;
             vT = vTR;
@@ -1289,6 +1291,9 @@ __device__ __forceinline__ void worker_loop(const SearchParams& p, uint8_t* regi
     if (tid == 0 && stop == nullptr) next = (int)atomicAdd(p.wq, 1u);
     int k = 0, base = 0;
     const int csteps = p.defer && p.compact ? 2 : 0;
+    // every kind of task covers each MB row once: a group that takes an index past the end
+    // leaves without walking the steps (row CTAs joining late find the queue empty)
+    const int total = p.BH * (nr + nd + nt) + (csteps ? 1 + p.BH : 0);
     unsigned* scan_done = p.wq + 1 + 2 * p.BH;
     for (;;) {
         if (tid == 0) {
@@ -1301,7 +1306,7 @@ __device__ __forceinline__ void worker_loop(const SearchParams& p, uint8_t* regi
         }
         group_sync(bar, TW_GROUP);  // (the previous task ended with a group barrier too)
         const int task = *gtask;
-        if (task < 0) return;  // stopped (group-uniform)
+        if (task < 0 || task >= total) return;  // stopped, or the queue is empty (group-uniform)
         int R = 0, D = 0, T = 0;
         for (; k < steps + csteps; k++) {
             if (k < steps) {
@@ -1645,6 +1650,7 @@ __device__ __forceinline__ void aq_warp(const SearchParams& p, const unsigned lo
             s = __reduce_add_sync(0xffffffffu, s);
             s2 = __reduce_add_sync(0xffffffffu, s2);
             if (lane == 0) p.varsum[idx] = make_uint2(s, s2);
+            if (lane == 0) RIV_GSTAMP(idx, 31);
         }
         __syncwarp();
         if (lane == 0) {
@@ -1701,8 +1707,10 @@ __device__ __forceinline__ void aq_fold(const SearchParams& p, volatile int* ctl
                 }
             }
             __syncwarp();
+            if (lane == 0) RIV_GSTAMP((size_t)r * p.BW + 1, 19);
             if (lane == 0)
                 for (int i = 0; i < m; i++) part = __fadd_rn(part, stage[i]);
+            if (lane == 0) RIV_GSTAMP((size_t)r * p.BW + 1, 18);
             __syncwarp();
         }
     }
