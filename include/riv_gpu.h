@@ -183,6 +183,14 @@ void riv_dct_tables(int32_t* t16, int32_t* t8);
  * threads, as the pipelined encoder does.  *len = stream size; up to cap bytes copied. */
 riv_status riv_test_dct_encode(const int16_t* blocks, uint32_t n, int intra, uint32_t threads, uint8_t* out, size_t cap,
                                size_t* len);
+/* Test hook (host only, no reference counterpart): the worker-task queue of the fused search
+ * launch for a frame of bw x bh MBs and w storage columns, in the order the kernel hands the
+ * tasks out: 3 int32 per task (kind 0 residual pair / 1 deblock tile / 2 SAD-table MB / 3 scan
+ * / 4 pack row, MB row or band, index), up to cap int32; *n = task count.  defer: the previous
+ * frame's reconstruction is in the queue; deblock: its deblock level is not 0; tables: the
+ * SAD table is computed in the launch; compact: its compaction is in the queue. */
+riv_status riv_test_worker_queue(uint32_t bw, uint32_t bh, uint32_t w, int defer, int deblock, int tables, int compact,
+                                 int32_t* out, size_t cap, size_t* n);
 
 /* ---- Decoder (reitero_decode) up to the YUV reconstruction ---- */
 /* DecodeError (dec/error.rs:4-20): Io, InvalidHeader, DecodingFailed, InvalidFrame,

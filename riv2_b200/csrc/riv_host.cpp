@@ -1473,6 +1473,28 @@ riv_status riv_libm_fixup_counts(uint32_t* nlog, uint32_t* nexp) {
 
 void riv_dct_tables(int32_t* t16, int32_t* t8) { dct_tables(t16, t8); }
 
+riv_status riv_test_worker_queue(uint32_t bw, uint32_t bh, uint32_t w, int defer, int deblock, int tables, int compact,
+                                 int32_t* out, size_t cap, size_t* n) {
+    if (!n || bw == 0 || bh == 0) return RIV_ERR_FRAME;
+    const QueueShape q = queue_shape((int)bw, (int)bh, (int)w, defer != 0, deblock != 0, tables != 0, compact != 0);
+    size_t i = 0;
+    for (int k = 0; k < q.steps + q.csteps; k++) {
+        int R, D, T;
+        queue_step(q, k, R, D, T);
+        for (int t = 0; t < R + D + T; t++, i++) {
+            int kind, row, idx;
+            queue_task(q, k, t, R, D, kind, row, idx);
+            if (out && 3 * i + 2 < cap) {
+                out[3 * i] = kind;
+                out[3 * i + 1] = row;
+                out[3 * i + 2] = idx;
+            }
+        }
+    }
+    *n = i;
+    return i == (size_t)queue_total(q) ? RIV_OK : RIV_ERR_ENCODING_FAILED;
+}
+
 riv_status riv_test_dct_encode(const int16_t* blocks, uint32_t n, int intra, uint32_t threads, uint8_t* out, size_t cap,
                                size_t* len) {
     if ((n > 0 && !blocks) || !len) return RIV_ERR_FRAME;

@@ -163,4 +163,59 @@ int launch_compact(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coef
 // libm device helpers exposed for the exhaustive check
 int launch_libm_eval(int which, const float* in, float* out, size_t n, const uint32_t* fix, int nfix, void* stream);
 
+// ---- the worker-task queue of the fused search launch (used by the kernel and by the
+// riv_test_worker_queue hook).  Step k holds, in this order: the previous frame's residual of
+// MB row k (pairs of MBs), its deblock of band k - DB_LAG (tiles), the SAD-table MBs of row
+// k - lag; after the last step, one scan task and one pack task per MB row (compaction).
+constexpr int DB_TW = 128;  // deblock tile width (luma columns; chroma DB_TW / 2)
+constexpr int DB_LAG = 3, TAB_LAG = 6;
+__host__ __device__ inline int deblock_tiles_per_band(int W) {
+    return (W + DB_TW - 1) / DB_TW + 2 * ((W / 2 + DB_TW / 2 - 1) / (DB_TW / 2));
+}
+struct QueueShape {
+    int BH, nr, nd, nt, lag, steps, csteps;  // rows; residual / deblock / table tasks per row; ...
+};
+__host__ __device__ inline QueueShape queue_shape(int BW, int BH, int W, bool defer, bool deblock, bool tables,
+                                                 bool compact) {
+    QueueShape q;
+    q.BH = BH;
+    q.nr = defer ? (BW + 1) / 2 : 0;
+    q.nd = defer && deblock ? deblock_tiles_per_band(W) : 0;
+    q.nt = tables ? BW : 0;
+    q.lag = defer ? TAB_LAG : 0;
+    q.steps = BH + (defer ? TAB_LAG : 0);
+    q.csteps = defer && compact ? 2 : 0;
+    return q;
+}
+// every kind of task covers each MB row once
+__host__ __device__ inline int queue_total(const QueueShape& q) {
+    return q.BH * (q.nr + q.nd + q.nt) + (q.csteps ? 1 + q.BH : 0);
+}
+// task counts of step k (k < steps + csteps): R residual pairs, D deblock tiles, T table MBs
+// (in the compaction steps: the scan, then the pack rows)
+__host__ __device__ inline void queue_step(const QueueShape& q, int k, int& R, int& D, int& T) {
+    if (k < q.steps) {
+        R = k < q.BH ? q.nr : 0;
+        D = k >= DB_LAG && k - DB_LAG < q.BH ? q.nd : 0;
+        T = k >= q.lag && k - q.lag < q.BH ? q.nt : 0;
+    } else {
+        R = D = 0;
+        T = k == q.steps ? 1 : q.BH;
+    }
+}
+// task t of step k: kind 0 residual pair idx of row, 1 deblock tile idx of band row, 2 table MB
+// idx of row, 3 scan, 4 pack of row
+__host__ __device__ inline void queue_task(const QueueShape& q, int k, int t, int R, int D, int& kind, int& row,
+                                           int& idx) {
+    if (k >= q.steps) {
+        kind = k == q.steps ? 3 : 4;
+        row = t;
+        idx = 0;
+        return;
+    }
+    kind = t < R ? 0 : t < R + D ? 1 : 2;
+    row = kind == 0 ? k : kind == 1 ? k - DB_LAG : k - q.lag;
+    idx = kind == 0 ? t : kind == 1 ? t - R : t - R - D;
+}
+
 }  // namespace riv

@@ -831,7 +831,6 @@ __device__ __forceinline__ void filter_line(int* px, int E, int I, int Hv) {
 // in that pass), then the horizontal edges at the band's top and bottom (their lines are 4+
 // pixels apart, so they touch disjoint pixels), and stores only its own pixels.  That equals
 // the reference's whole-plane vertical pass followed by the whole-plane horizontal pass.
-constexpr int DB_TW = 128;
 constexpr int DB_TILE_BYTES = (16 + 8) * (DB_TW + 8);
 // One tile (plane, t: band-major tile index within the plane) by nthr threads synchronised on
 // group barrier `bar` (0 = the whole CTA); `tile` = DB_TILE_BYTES of shared memory.
@@ -1130,9 +1129,6 @@ __device__ __forceinline__ bool wait_ref_rows(const SearchParams& p, int r, int 
     }
     return true;
 }
-__host__ __device__ inline int deblock_tiles_per_band(int W) {
-    return (W + DB_TW - 1) / DB_TW + 2 * ((W / 2 + DB_TW / 2 - 1) / (DB_TW / 2));
-}
 
 // ---------------------------------------------------------------------------------
 // K8 helpers: per-MB side info and compaction of the coded MBs' coefficients for the host
@@ -1241,7 +1237,6 @@ __device__ __forceinline__ void pack_mb(int m, int lane, const uint8_t* opt_skip
 // wq, per-MB table flags (the frame tag) that the loaders acquire.  With p.compact the queue
 // ends with the previous frame's compaction: one scan task (after every residual row), then
 // one pack task per MB row (after the scan, published in wq[2BH+1]).
-constexpr int DB_LAG = 3, TAB_LAG = 6;
 constexpr int WK_SCAN_IPT = 8;  // MBs per thread of the in-launch scan (registers are capped)
 // Worker region: the residual bases (WK_BASES bytes), `groups` group scratch areas, then a
 // task word and a status word per group.
@@ -1275,12 +1270,8 @@ __device__ __forceinline__ void worker_loop(const SearchParams& p, uint8_t* regi
     uint8_t* gsm = region + WK_BASES + (size_t)g * worker_group_bytes();
     volatile int* gtask = (volatile int*)(region + WK_BASES + (size_t)groups * worker_group_bytes()) + g;
     volatile int* gok = gtask + groups;
-    const int nr = p.defer ? (p.BW + 1) / 2 : 0;
     const int tb = deblock_tiles_per_band(p.W);
-    const int nd = p.defer && p.db_level > 0 ? tb : 0;
-    const int nt = p.tflag != nullptr ? p.BW : 0;
-    const int lag = p.defer ? TAB_LAG : 0;
-    const int steps = p.BH + (p.defer ? TAB_LAG : 0);
+    const QueueShape q = queue_shape(p.BW, p.BH, p.W, p.defer != 0, p.db_level > 0, p.tflag != nullptr, p.compact != 0);
     const int nmb = p.BW * p.BH;
     const int bar = 1 + gid;
     // Task indices a group takes only grow, so the step cursor (k, first task of step k) only
@@ -1290,10 +1281,9 @@ __device__ __forceinline__ void worker_loop(const SearchParams& p, uint8_t* regi
     int next = 0;
     if (tid == 0 && stop == nullptr) next = (int)atomicAdd(p.wq, 1u);
     int k = 0, base = 0;
-    const int csteps = p.defer && p.compact ? 2 : 0;
-    // every kind of task covers each MB row once: a group that takes an index past the end
-    // leaves without walking the steps (row CTAs joining late find the queue empty)
-    const int total = p.BH * (nr + nd + nt) + (csteps ? 1 + p.BH : 0);
+    // a group that takes an index past the end leaves without walking the steps (row CTAs
+    // joining late find the queue empty)
+    const int total = queue_total(q);
     unsigned* scan_done = p.wq + 1 + 2 * p.BH;
     for (;;) {
         if (tid == 0) {
@@ -1308,27 +1298,14 @@ __device__ __forceinline__ void worker_loop(const SearchParams& p, uint8_t* regi
         const int task = *gtask;
         if (task < 0 || task >= total) return;  // stopped, or the queue is empty (group-uniform)
         int R = 0, D = 0, T = 0;
-        for (; k < steps + csteps; k++) {
-            if (k < steps) {
-                R = k < p.BH ? nr : 0;
-                D = k >= DB_LAG && k - DB_LAG < p.BH ? nd : 0;
-                T = k >= lag && k - lag < p.BH ? nt : 0;
-            } else {  // compaction: the scan, then the pack rows (counted as T)
-                R = D = 0;
-                T = k == steps ? 1 : p.BH;
-            }
+        for (; k < q.steps + q.csteps; k++) {
+            queue_step(q, k, R, D, T);
             if (task < base + R + D + T) break;
             base += R + D + T;
         }
-        if (k >= steps + csteps) return;  // the queue is empty
-        const int t = task - base;
-        int kind = t < R ? 0 : t < R + D ? 1 : 2;
-        int row = kind == 0 ? k : kind == 1 ? k - DB_LAG : k - lag;
-        const int idx = kind == 0 ? t : kind == 1 ? t - R : t - R - D;
-        if (k >= steps) {
-            kind = k == steps ? 3 : 4;
-            row = t;
-        }
+        if (k >= q.steps + q.csteps) return;  // the queue is empty
+        int kind, row, idx;
+        queue_task(q, k, task - base, R, D, kind, row, idx);
         if (kind == 0) {  // residual of MBs (row, 2 idx) and (row, 2 idx + 1)
             const int half = tid >> 6, x = 2 * idx + half;
             if (tid == 0) RIV_GSTAMP(row * p.BW + 2 * idx, 18);

@@ -111,7 +111,7 @@ EXPORTED_SYMBOLS = (
     "riv_stage_rgb_to_yuv", "riv_stage_deblock", "riv_stage_libm", "riv_libm_fixup_counts", "riv_dct_tables",
     "riv_debug_frame_state", "riv_counters", "riv_host_times", "riv_stage_deblock_noalloc",
     "riv_decoder_new", "riv_decoder_info", "riv_decode_frame_yuv", "riv_decoder_current_frame",
-    "riv_decoder_last_error", "riv_decoder_free", "riv_test_dct_encode",
+    "riv_decoder_last_error", "riv_decoder_free", "riv_test_dct_encode", "riv_test_worker_queue",
 )
 
 
@@ -127,6 +127,8 @@ def lib() -> C.CDLL:
     L.riv_encode_frame_yuv.argtypes = [P, U8P, U8P, U8P, C.c_uint64, C.POINTER(RivFrameStats)]
     L.riv_finish.argtypes = [P]
     L.riv_test_dct_encode.argtypes = [P, C.c_uint32, C.c_int, C.c_uint32, P, C.c_size_t, C.POINTER(C.c_size_t)]
+    L.riv_test_worker_queue.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_int, C.c_int, C.c_int, P,
+                                        C.c_size_t, C.POINTER(C.c_size_t)]
     L.riv_encoder_free.argtypes = [P]
     L.riv_last_error.restype = C.c_char_p
     L.riv_last_error.argtypes = [P]
@@ -552,6 +554,18 @@ def dct_encode_host(blocks: np.ndarray, intra: bool, threads: int = 0) -> bytes:
     out = np.zeros(max(n.value, 1), np.uint8)
     lib().riv_test_dct_encode(b.ctypes.data, b.shape[0], int(intra), threads, out.ctypes.data, n.value, C.byref(n))
     return out[:n.value].tobytes()
+
+
+def worker_queue(bw: int, bh: int, w: int, defer: bool, deblock: bool, tables: bool, compact: bool) -> np.ndarray:
+    """The fused search launch's worker tasks in hand-out order, (n, 3) int32 rows of (kind,
+    row, index): kind 0 residual pair, 1 deblock tile, 2 SAD-table MB, 3 scan, 4 pack row."""
+    n = C.c_size_t(0)
+    args = (bw, bh, w, int(defer), int(deblock), int(tables), int(compact))
+    if lib().riv_test_worker_queue(*args, None, 0, C.byref(n)) != 0:
+        raise EncodingFailed("riv_test_worker_queue: task count disagrees with the queue total")
+    out = np.zeros((max(n.value, 1), 3), np.int32)
+    lib().riv_test_worker_queue(*args, out.ctypes.data, out.size, C.byref(n))
+    return out[:n.value]
 
 
 def libm_fixup_counts():
