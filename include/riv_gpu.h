@@ -217,6 +217,11 @@ riv_dec_status riv_decoder_info(const riv_decoder* dec, uint32_t* dims5, uint64_
  * MVs are decoded in order on the calling thread and their coefficient streams on a pool of
  * host threads; a record that cannot be read is reported by the call for that frame (the
  * frames before it decode normally). */
+/* Decoder::decode_frame's RGB output (dec/decoder.rs:445-456): the frame as display-size RGB24
+ * (rgb: display w x h x 3 bytes, nullable), converted on the GPU (BT.709 limited range, this
+ * library's definition: the reference uses the `yuv` crate, so byte parity with it is not
+ * established).  Same read-ahead and error behaviour as riv_decode_frame_yuv. */
+riv_dec_status riv_decode_frame_rgb(riv_decoder* dec, uint8_t* rgb, uint32_t* frame_type, uint64_t* timestamp_ms);
 riv_dec_status riv_decode_frame_yuv(riv_decoder* dec, uint8_t* y, uint8_t* u, uint8_t* v, uint32_t* frame_type,
                                     uint64_t* timestamp_ms);
 /* Decoder::current_frame (dec/decoder.rs:475-478). */

@@ -93,6 +93,8 @@ def lib():
             getattr(L, n).argtypes = [I16, C.c_float, C.c_float, I16]
         for n in ("oracle_idct16_aq", "oracle_idct8_aq"):
             getattr(L, n).argtypes = [I16, C.c_float, I16]
+        L.oracle_yuv_to_rgb.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                         C.c_uint32, C.c_void_p]
         L.oracle_dct_encode.restype = C.c_size_t
         L.oracle_dct_encode.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t]
         L.oracle_rans_roundtrip.restype = C.c_size_t
@@ -246,6 +248,14 @@ class OracleDecoder:
             self.close()
         except Exception:
             pass
+
+
+def yuv_to_rgb(f: Frames, dw: int, dh: int) -> np.ndarray:
+    """Decoder output: the frame's YUV 4:2:0 planes to display-size (dh, dw, 3) RGB24."""
+    out = np.zeros((dh, dw, 3), np.uint8)
+    y, u, v = (np.ascontiguousarray(p, dtype=np.uint8) for p in (f.y, f.u, f.v))
+    lib().oracle_yuv_to_rgb(y.ctypes.data, u.ctypes.data, v.ctypes.data, f.w, f.h, dw, dh, out.ctypes.data)
+    return out
 
 
 def dct_encode(blocks: np.ndarray, intra: bool) -> bytes:

@@ -150,6 +150,27 @@ static void rgb_to_yuv420(const uint8_t* rgb, int w, int h, Yuv& out) {
         }
 }
 
+// YUV 4:2:0 -> RGB24 for the decoder's output (dec/decoder.rs:445-456: `to_rgb24`, then
+// `crop_rgb24` to the display size; com/yuv.rs:94-110 calls the `yuv` crate's
+// `yuv420_to_rgb`, limited range, BT.709, absent here).  The project's own definition, the
+// inverse of rgb_to_yuv420: BT.709 (Kr 0.2126, Kb 0.0722) limited range in 13-bit fixed point,
+// each chroma sample covering its 2x2 luma quad.  Parity with the crate is unpinned.
+static const int IY = 9539;                   // round(8192*255/219)
+static const int IRV = 14686, IBU = 17305;    // round(8192*255/224*1.5748), *1.8556
+static const int IGU = 1747, IGV = 4366;      // round(8192*255/224*2Kb(1-Kb)/Kg), *2Kr(1-Kr)/Kg
+static void yuv420_to_rgb24_crop(const Yuv& f, int dw, int dh, uint8_t* rgb) {
+    const int cw = f.w / 2;
+    for (int y = 0; y < dh; y++)
+        for (int x = 0; x < dw; x++) {
+            const int yv = IY * ((int)f.y[(size_t)y * f.w + x] - 16);
+            const int u = (int)f.u[(size_t)(y / 2) * cw + x / 2] - 128, v = (int)f.v[(size_t)(y / 2) * cw + x / 2] - 128;
+            uint8_t* p = rgb + ((size_t)y * dw + x) * 3;
+            p[0] = (uint8_t)clampi((yv + IRV * v + (1 << 12)) >> 13, 0, 255);
+            p[1] = (uint8_t)clampi((yv - IGU * u - IGV * v + (1 << 12)) >> 13, 0, 255);
+            p[2] = (uint8_t)clampi((yv + IBU * u + (1 << 12)) >> 13, 0, 255);
+        }
+}
+
 // ----------------------------------------------------------------------------------
 // Deblocking filter (com/deblock.rs)
 // ----------------------------------------------------------------------------------
@@ -2044,6 +2065,11 @@ void oracle_rgb_to_yuv420(const uint8_t* rgb, uint32_t dw, uint32_t dh, uint32_t
     Yuv f;
     rgb_to_yuv420(pad.data(), (int)sw, (int)sh, f);
     yuv_to(f, y, u, v);
+}
+void oracle_yuv_to_rgb(const uint8_t* y, const uint8_t* u, const uint8_t* v, uint32_t sw, uint32_t sh, uint32_t dw,
+                       uint32_t dh, uint8_t* rgb) {
+    Yuv f = yuv_from(y, u, v, (int)sw, (int)sh);
+    yuv420_to_rgb24_crop(f, (int)dw, (int)dh, rgb);
 }
 void oracle_deblock(uint8_t* y, uint8_t* u, uint8_t* v, uint32_t w, uint32_t h, int level, int intra,
                     const uint8_t* mask) {

@@ -102,6 +102,10 @@ double oracle_glibc_logf_check(void);
  * (Y 256, U 64, V 64), DC prediction when intra; returns the stream size, copies up to cap
  * bytes. */
 size_t oracle_dct_encode(const int16_t* blocks, int n, int intra, uint8_t* stream, size_t cap);
+/* Decoder output: storage-size YUV 4:2:0 to display-size RGB24 (BT.709 limited range, the
+ * project's definition; dec/decoder.rs:445-456). */
+void oracle_yuv_to_rgb(const uint8_t* y, const uint8_t* u, const uint8_t* v, uint32_t sw, uint32_t sh, uint32_t dw,
+                       uint32_t dh, uint8_t* rgb);
 
 #ifdef __cplusplus
 }

@@ -1578,6 +1578,7 @@ struct riv_decoder {
     int ref_cur = 0;
     cudaStream_t S = nullptr;
     DevBuf ref[2], recon_pre, pred, coeffs, mbout, skip, fmask, varsum, lnv, qs, logfix, expfix, ytab, ctab;
+    DevBuf rgbdev;  // display-size RGB24 output, allocated on first use
     int nlog = 0, nexp = 0;
     // read-ahead state (records up to DEC_AHEAD frames past `current`)
     DecSlot slots[DEC_AHEAD];
@@ -1800,8 +1801,9 @@ riv_dec_status riv_decoder_info(const riv_decoder* d, uint32_t* dims5, uint64_t*
 uint64_t riv_decoder_current_frame(const riv_decoder* d) { return d ? d->current : 0; }
 const char* riv_decoder_last_error(const riv_decoder* d) { return d ? d->err.c_str() : "null decoder"; }
 
-riv_dec_status riv_decode_frame_yuv(riv_decoder* d, uint8_t* y, uint8_t* u, uint8_t* v, uint32_t* frame_type,
-                                    uint64_t* timestamp_ms) {
+// One frame: the YUV planes and / or the display-size RGB24 (each nullable).
+static riv_dec_status dec_frame(riv_decoder* d, uint8_t* y, uint8_t* u, uint8_t* v, uint8_t* rgb, uint32_t* frame_type,
+                                uint64_t* timestamp_ms) {
     if (!d) return RIV_DEC_INVALID_HEADER;
     if (d->poisoned) return dec_fail(d, RIV_DEC_CUDA, "decoder unusable after a device failure");
     if (d->current >= d->frame_count) return dec_fail(d, RIV_DEC_END_OF_STREAM, "end of stream");
@@ -1865,6 +1867,12 @@ riv_dec_status riv_decode_frame_yuv(riv_decoder* d, uint8_t* y, uint8_t* u, uint
         if (y) CK(cudaMemcpyAsync(y, recon, ysz, cudaMemcpyDeviceToHost, S));
         if (u) CK(cudaMemcpyAsync(u, recon + ysz, csz, cudaMemcpyDeviceToHost, S));
         if (v) CK(cudaMemcpyAsync(v, recon + ysz + csz, csz, cudaMemcpyDeviceToHost, S));
+        if (rgb) {  // dec/decoder.rs:445-456: to RGB24, cropped to the display size
+            const size_t rgb_bytes = (size_t)d->dw * d->dh * 3;
+            if (!d->rgbdev.p) d->rgbdev.alloc(rgb_bytes);
+            CK(launch_yuv_to_rgb(recon, W, H, (int)d->dw, (int)d->dh, d->rgbdev.as<uint8_t>(), S));
+            CK(cudaMemcpyAsync(rgb, d->rgbdev.p, rgb_bytes, cudaMemcpyDeviceToHost, S));
+        }
         // read the next frames while the GPU reconstructs this one (their slots are not this
         // frame's, whose staging the copies above read), then finish this frame; a failure
         // here is reported by the next call, which reads its frame first
@@ -1882,12 +1890,21 @@ riv_dec_status riv_decode_frame_yuv(riv_decoder* d, uint8_t* y, uint8_t* u, uint
     return RIV_DEC_OK;
 }
 
+riv_dec_status riv_decode_frame_yuv(riv_decoder* d, uint8_t* y, uint8_t* u, uint8_t* v, uint32_t* frame_type,
+                                    uint64_t* timestamp_ms) {
+    return dec_frame(d, y, u, v, nullptr, frame_type, timestamp_ms);
+}
+
+riv_dec_status riv_decode_frame_rgb(riv_decoder* d, uint8_t* rgb, uint32_t* frame_type, uint64_t* timestamp_ms) {
+    return dec_frame(d, nullptr, nullptr, nullptr, rgb, frame_type, timestamp_ms);
+}
+
 void riv_decoder_free(riv_decoder* d) {
     if (!d) return;
     cudaSetDevice(d->device);
     if (d->S) cudaStreamSynchronize(d->S);
     DevBuf* bufs[] = {&d->ref[0], &d->ref[1], &d->recon_pre, &d->pred, &d->coeffs, &d->mbout, &d->skip, &d->fmask,
-                      &d->varsum, &d->lnv, &d->qs, &d->logfix, &d->expfix, &d->ytab, &d->ctab};
+                      &d->varsum, &d->lnv, &d->qs, &d->logfix, &d->expfix, &d->ytab, &d->ctab, &d->rgbdev};
     for (DevBuf* x : bufs) x->release();
     d->pool.reset();  // finishes the coefficient decodes still queued (they write the slots)
     for (DecSlot& sl : d->slots) {

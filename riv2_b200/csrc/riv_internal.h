@@ -123,6 +123,7 @@ enum StatusBits : unsigned {
 
 // Launchers (riv_kernels.cu).  All are asynchronous on `stream`.
 int launch_rgb_to_yuv(const uint8_t* rgb, int dw, int dh, uint8_t* yuv, int W, int H, void* stream, bool beside = false);
+int launch_yuv_to_rgb(const uint8_t* yuv, int W, int H, int dw, int dh, uint8_t* rgb, void* stream);
 // Launch plan of the search wavefront (chosen once per encoder).  fused: the SAD table is
 // computed inside the same cooperative launch by `grid - nrow` worker CTAs.
 struct SearchPlan {

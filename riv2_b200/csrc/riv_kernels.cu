@@ -57,6 +57,30 @@ __global__ void k_rgb_to_yuv(const uint8_t* __restrict__ rgb, int dw, int dh, ui
         rgb_to_yuv_quad(rgb, dw, dh, Yp, Up, Vp, W, q % cw, q / cw);
 }
 
+// Decoder output (dec/decoder.rs:445-456: `to_rgb24` then `crop_rgb24`): storage-size YUV
+// 4:2:0 to display-size RGB24, BT.709 limited range in 13-bit fixed point (the inverse of
+// k_rgb_to_yuv; 8192*255/219, 8192*255/224 * 1.5748, 0.18732, 0.46812, 1.8556), each chroma
+// sample covering its 2x2 luma quad.  One thread per output pixel.
+__global__ void k_yuv_to_rgb(const uint8_t* __restrict__ Yp, const uint8_t* __restrict__ Up,
+                             const uint8_t* __restrict__ Vp, int W, int dw, int dh, uint8_t* __restrict__ rgb) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= dw || y >= dh) return;
+    const int yv = 9539 * ((int)Yp[(size_t)y * W + x] - 16);
+    const size_t ci = (size_t)(y >> 1) * (W / 2) + (x >> 1);
+    const int u = (int)Up[ci] - 128, v = (int)Vp[ci] - 128;
+    uint8_t* p = rgb + ((size_t)y * dw + x) * 3;
+    p[0] = (uint8_t)min(max((yv + 14686 * v + (1 << 12)) >> 13, 0), 255);
+    p[1] = (uint8_t)min(max((yv - 1747 * u - 4366 * v + (1 << 12)) >> 13, 0), 255);
+    p[2] = (uint8_t)min(max((yv + 17305 * u + (1 << 12)) >> 13, 0), 255);
+}
+int launch_yuv_to_rgb(const uint8_t* yuv, int W, int H, int dw, int dh, uint8_t* rgb, void* stream) {
+    const uint8_t* Y = yuv;
+    const uint8_t* U = yuv + (size_t)W * H;
+    const uint8_t* V = U + (size_t)(W / 2) * (H / 2);
+    k_yuv_to_rgb<<<dim3((dw + 127) / 128, dh), 128, 0, (cudaStream_t)stream>>>(Y, U, V, W, dw, dh, rgb);
+    return (int)cudaGetLastError();
+}
+
 // `beside`: the conversion runs while a search launch holds the SMs, so one 128-thread CTA
 // (4K registers) per SM at most: every SM keeps room for a search CTA (61,440 registers) and a
 // search launch never waits for a conversion to drain.  Otherwise one CTA per 128 quads (the

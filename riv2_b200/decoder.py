@@ -72,6 +72,15 @@ class DecodedFrame:
     frame_type: int  # 1 intra, 2 inter
 
 
+@dataclasses.dataclass
+class DecodedRgbFrame:
+    """decoder.rs:34-50: the frame as display-size RGB24 (dec/decoder.rs:445-456)."""
+    rgb: np.ndarray  # (display_height, display_width, 3) uint8
+    timestamp: int
+    frame_index: int
+    frame_type: int  # 1 intra, 2 inter
+
+
 class Decoder:
     def __init__(self, handle, data):
         self._h = handle
@@ -117,6 +126,22 @@ class Decoder:
             msg = lib().riv_decoder_last_error(self._h)
             raise _ERRORS.get(st, DecodeError)(msg.decode() if msg else "decode failed")
         return DecodedFrame(y, u, v, ts.value, idx, t.value) if copy_out else None
+
+    def decode_frame_rgb(self) -> DecodedRgbFrame:
+        """Decoder::decode_frame (decoder.rs:174-460) with its RGB output: the reconstruction
+        converted to RGB24 on the GPU (BT.709 limited range, this library's definition; the
+        reference uses the `yuv` crate, so byte parity with it is not established) and
+        cropped to the display size."""
+        hd = self._header
+        rgb = np.empty((hd.display_height, hd.display_width, 3), np.uint8)
+        t = C.c_uint32()
+        ts = C.c_uint64()
+        idx = self.current_frame()
+        st = lib().riv_decode_frame_rgb(self._h, rgb.ctypes.data_as(C.POINTER(C.c_uint8)), C.byref(t), C.byref(ts))
+        if st:
+            msg = lib().riv_decoder_last_error(self._h)
+            raise _ERRORS.get(st, DecodeError)(msg.decode() if msg else "decode failed")
+        return DecodedRgbFrame(rgb, ts.value, idx, t.value)
 
     def close(self) -> None:
         if self._h:

@@ -110,7 +110,7 @@ EXPORTED_SYMBOLS = (
     "riv_memwriter_new", "riv_memwriter_vtable", "riv_memwriter_size", "riv_memwriter_data", "riv_memwriter_free",
     "riv_stage_rgb_to_yuv", "riv_stage_deblock", "riv_stage_libm", "riv_libm_fixup_counts", "riv_dct_tables",
     "riv_debug_frame_state", "riv_counters", "riv_host_times", "riv_stage_deblock_noalloc",
-    "riv_decoder_new", "riv_decoder_info", "riv_decode_frame_yuv", "riv_decoder_current_frame",
+    "riv_decoder_new", "riv_decoder_info", "riv_decode_frame_yuv", "riv_decode_frame_rgb", "riv_decoder_current_frame",
     "riv_decoder_last_error", "riv_decoder_free", "riv_test_dct_encode", "riv_test_worker_queue",
 )
 
@@ -156,6 +156,7 @@ def lib() -> C.CDLL:
     L.riv_decoder_new.argtypes = [U8P, C.c_size_t, C.c_int, C.POINTER(P)]
     L.riv_decoder_info.argtypes = [P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]
     L.riv_decode_frame_yuv.argtypes = [P, U8P, U8P, U8P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]
+    L.riv_decode_frame_rgb.argtypes = [P, U8P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]
     L.riv_decoder_current_frame.restype = C.c_uint64
     L.riv_decoder_current_frame.argtypes = [P]
     L.riv_decoder_last_error.restype = C.c_char_p

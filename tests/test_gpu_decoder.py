@@ -117,3 +117,31 @@ def test_decode_truncated_stream_reports_io():
     with pytest.raises(IoError):
         dec.decode_frame()
     dec.close()
+
+
+def test_oracle_rgb_output_inverts_the_input_conversion():
+    """The decoder's RGB output definition (BT.709 limited range, each chroma sample on its 2x2
+    quad) inverts the input conversion: on colours constant over each 2x2 quad, RGB -> YUV ->
+    RGB is within the limited-range quantisation (at most 3 levels per channel)."""
+    rng = np.random.default_rng(1)
+    quads = rng.integers(0, 256, (18, 22, 3), dtype=np.uint8)
+    rgb = np.repeat(np.repeat(quads, 2, axis=0), 2, axis=1)  # 36 x 44, constant per quad
+    f = O.rgb_to_yuv(rgb, 44, 36, 48, 48)
+    back = O.yuv_to_rgb(f, 44, 36)
+    assert back.shape == (36, 44, 3)
+    assert np.abs(back.astype(int) - rgb.astype(int)).max() <= 3
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("w,h", [(352, 288), (100, 70)])
+def test_decode_rgb_output_matches_oracle(w, h):
+    from riv2_b200.decoder import Decoder
+    data, _ = _stream("cif", 5, w, h, keyint=3)
+    dec = Decoder.new(data)
+    odec = O.OracleDecoder(data)
+    for t in range(5):
+        f = dec.decode_frame_rgb()
+        typ, o = odec.next()
+        assert f.frame_index == t and f.frame_type == typ and f.rgb.shape == (h, w, 3)
+        assert np.array_equal(f.rgb, O.yuv_to_rgb(o, w, h)), t
+    dec.close()
