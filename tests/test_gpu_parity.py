@@ -240,22 +240,23 @@ def test_encode_pipelined_is_identical():
     assert g0 == o0 == g4
 
 
-def test_deferred_reconstruction_flush_paths():
+@pytest.mark.parametrize("w,h", [(352, 288), (100, 70), (16, 16)])
+def test_deferred_reconstruction_flush_paths(w, h):
     """From pipeline depth 2 a P-frame is reconstructed inside the next P-frame's search
     launch; before a key frame, for a per-frame-stats call, for last_recon and at finish it
     is reconstructed with separate kernels instead.  A mix of all of them gives the oracle's
     stream, last_recon returns the oracle's reconstruction of the frame just submitted, and
     both kinds of reconstruction occur."""
     from riv2_b200 import encoder as E
-    frames = _clip("cif", 14, seed=5)
-    gc, oc = _cfgs(352, 288, keyint=5)
+    frames = _clip("cif", 14, seed=5, width=w, height=h)
+    gc, oc = _cfgs(w, h, keyint=5)
     gc = gc.with_pipeline_depth(16)
-    w = E.VecWriter()
-    enc = E.Encoder.new(gc, w)
+    wr = E.VecWriter()
+    enc = E.Encoder.new(gc, wr)
     oenc = O.OracleEncoder(oc)
     for t, f in enumerate(frames):
         assert oenc.encode_rgb(f, t * 20) == 0
-        fr = E.Frame(f, 352, 288, t * 20)
+        fr = E.Frame(f, w, h, t * 20)
         if t % 6 == 3:
             assert enc.encode_frame_with_stats(fr).frame_index == t
         else:
@@ -266,7 +267,7 @@ def test_deferred_reconstruction_flush_paths():
             assert np.array_equal(y, r.y) and np.array_equal(u, r.u) and np.array_equal(v, r.v), t
     enc.finish()
     c = enc.counters()
-    assert w.into_inner() == oenc.finish()
+    assert wr.into_inner() == oenc.finish()
     enc.close()
     assert 0 < c["deferred_pframes"] < c["pframes"]
 
