@@ -1581,7 +1581,7 @@ __device__ __forceinline__ void aq_warp(const SearchParams& p, const unsigned lo
                                         volatile int* ctl, const uint8_t* band, unsigned long long* bandb) {
     const int lane = threadIdx.x & 31;
     const int sr = p.sr, MARGIN = (sr + 1 + 15) & ~15, BWB = p.W + 2 * MARGIN;
-    const int W = p.W, H = p.H;
+    const int W = p.W;
     uint8_t* PY = p.pred;
     const int yy = lane >> 1, xoff = (lane & 1) * 8;  // luma: row, 8-pixel half
     int n = 0, rows = 0;
