@@ -3,6 +3,8 @@
 * CIF 352x288, 60 frames, q 85/80: the GPU stream equals the oracle's byte for byte.
 * 1080p, 120 frames, q 85/80 and 95/90, frames in flight: byte-identical to the oracle, and
   the oracle decoder reproduces the GPU's last reconstruction.
+* 720p, 30 frames, and CIF at search range 15, 20 frames, both 16 frames in flight:
+  byte-identical to the oracle.
 * 4K 3840x2160 high-motion stress, 60 frames, q 95/90 and 75/70: the oracle decoder decodes
   the GPU stream to the GPU's reconstruction of every frame (a size-independent property),
   and the first frames are byte-identical to the oracle encoder's.
@@ -77,6 +79,27 @@ def test_1080p_120_frames_byte_identical(q):
         assert typ > 0
     typ, f = dec.next()
     assert typ == 2 and _same_frame(f, last)
+
+
+def test_720p_pipelined_byte_identical():
+    """720p (80 x 45 MBs: other worker-queue counts and deblock tiling) at depth 16, where each
+    P-frame is reconstructed inside the next frame's search launch."""
+    from riv2_b200.synth import SynthClip
+    clip = SynthClip("720p", seed=31)
+    gc, oc = _configs(1280, 720, 30, 85, 80, depth=16)
+    g, _, _ = _gpu_stream(clip, 30, gc)
+    assert g == _oracle_stream(clip, 30, oc, 30)
+
+
+def test_cif_search_range_15_pipelined_byte_identical():
+    """Search range 15 (the largest SAD-table window and reference band) at depth 16."""
+    from riv2_b200.synth import SynthClip
+    clip = SynthClip("cif", seed=17)
+    gc, oc = _configs(352, 288, 30, 85, 80, depth=16)
+    gc = gc._with(search_range=15)
+    oc.search_range = 15
+    g, _, _ = _gpu_stream(clip, 20, gc)
+    assert g == _oracle_stream(clip, 20, oc, 30)
 
 
 @pytest.mark.parametrize("q", [(95, 90), (75, 70)])
