@@ -382,7 +382,7 @@ __device__ __forceinline__ int argmin8(long long total, bool valid, long long& b
 // Phase stamps, written when p.prof is set: RIV_PROF_WORDS i64 per MB.  Words 0-15 are SM clock
 // cycles (clock64) of the search and mode warps; words 16-27 are %globaltimer nanoseconds,
 // comparable across SMs: 16/17 search warp MB start / slot ready; 18/19 deferred residual of
-// the MB pair starting here (of MB (r, 1): the AQ fold's end of row r's sum / logs); 30 / 31
+// the MB pair starting here (of MB (r, 1): the AQ fold's end of row r's sum / loads); 30 / 31
 // the mode warp's decision / the AQ warp's variance of the MB; 20/21/22 deblock tile (wait start, work start, end); 23/24/25
 // SAD-table MB (wait start, work start, end); 26/27 the row loader's wait for reference bands.
 __device__ __forceinline__ long long gtimer() {
@@ -1575,8 +1575,10 @@ __device__ __forceinline__ void loader_warp(const SearchParams& p, unsigned long
 // (build_predicted, com/fast_motion.rs:103-352) from the row's reference band, where the
 // replicated edges give the same samples as the reference's clamped coordinates, and the
 // predicted-luma sums (sum, sum of squares) for the MB's variance (compute_aq_quant_steps,
-// res/residual.rs:116-153).  Chroma prediction is left to the residual kernel.  After each row it publishes row_done[r] = tag.  ctl[3] = rows it has finished (the loader refills
-// the band only after both the search warp and this warp are done with it).
+// res/residual.rs:116-153).  Chroma prediction is left to the residual kernel.  After each row
+// it sets ctl[3] = rows it has finished (the loader refills the band only after both the search
+// warp and this warp are done with it), computes the row's ln variances into lnv and publishes
+// row_done[r] = tag.
 __device__ __forceinline__ void aq_warp(const SearchParams& p, const unsigned long long* hand, volatile int* hand_done,
                                         volatile int* ctl, const uint8_t* band, unsigned long long* bandb) {
     const int lane = threadIdx.x & 31;
@@ -1654,19 +1656,41 @@ __device__ __forceinline__ void aq_warp(const SearchParams& p, const unsigned lo
             if (lane == 0) RIV_GSTAMP(idx, 31);
         }
         __syncwarp();
-        if (lane == 0) {
-            __threadfence();
-            st_release_u32(p.row_done + r, p.tag);
-            ctl[3] = rows + 1;
+        if (lane == 0) ctl[3] = rows + 1;  // the band is free for the loader
+        // the row's ln variances (res/residual.rs:134-153) from the sums lane 0 wrote above
+        // (visible to the warp after __syncwarp), then row_done[r] for the fold
+        for (int b0 = 0; b0 < p.BW; b0 += 4 * 32) {
+            float v4[4], l4[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int i = b0 + j * 32 + lane;
+                float var = 4.0f;
+                if (i < p.BW) {
+                    const uint2 vs = p.varsum[(size_t)r * p.BW + i];
+                    const unsigned long long N = 256ull * vs.y - (unsigned long long)vs.x * vs.x;
+                    var = __fdiv_rn(__ull2float_rn(N), 65536.0f);
+                    var = var < 4.0f ? 4.0f : var;
+                }
+                v4[j] = var;
+            }
+            glibc_logf_batch<4>(v4, l4, p.logfix, p.nlog);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int i = b0 + j * 32 + lane;
+                if (i < p.BW) p.lnv[(size_t)r * p.BW + i] = l4[j];
+            }
         }
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) st_release_u32(p.row_done + r, p.tag);
         rows++;
     }
 }
 
-// The per-MB ln variances and their Iterator::sum, strictly left to right in raster order,
-// while the rows are still being searched: one warp waits for each row's row_done flag,
-// computes the row's glibc-exact ln variances in parallel, stages them in shared memory and
-// its lane 0 folds them.  Then avg = sum / n (res/residual.rs:116-167).
+// The Iterator::sum of the per-MB ln variances, strictly left to right in raster order, while
+// the rows are still being searched: one warp waits for each row's row_done flag (set by the
+// row's AQ warp once the row's glibc-exact ln variances are written), stages the row's values
+// in shared memory and its lane 0 folds them.  Then avg = sum / n (res/residual.rs:116-167).
 __device__ __forceinline__ void aq_fold(const SearchParams& p, volatile int* ctl, float* stage) {
     const int lane = threadIdx.x & 31;
     float part = 0.0f;
@@ -1683,30 +1707,7 @@ __device__ __forceinline__ void aq_fold(const SearchParams& p, volatile int* ctl
         }
         for (int c0 = 0; c0 < p.BW; c0 += 256) {
             const int m = min(256, p.BW - c0);
-            for (int b0 = 0; b0 < m; b0 += 4 * 32) {  // ln variance of each MB (res/residual.rs:134-153)
-                float v4[4], l4[4];
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const int i = b0 + j * 32 + lane;
-                    float var = 4.0f;
-                    if (i < m) {
-                        const uint2 vs = p.varsum[(size_t)r * p.BW + c0 + i];
-                        const unsigned long long N = 256ull * vs.y - (unsigned long long)vs.x * vs.x;
-                        var = __fdiv_rn(__ull2float_rn(N), 65536.0f);
-                        var = var < 4.0f ? 4.0f : var;
-                    }
-                    v4[j] = var;
-                }
-                glibc_logf_batch<4>(v4, l4, p.logfix, p.nlog);
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const int i = b0 + j * 32 + lane;
-                    if (i < m) {
-                        p.lnv[(size_t)r * p.BW + c0 + i] = l4[j];
-                        stage[i] = l4[j];
-                    }
-                }
-            }
+            for (int i = lane; i < m; i += 32) stage[i] = p.lnv[(size_t)r * p.BW + c0 + i];
             __syncwarp();
             if (lane == 0) RIV_GSTAMP((size_t)r * p.BW + 1, 19);
             if (lane == 0)
