@@ -307,10 +307,10 @@ def cpu_baseline_all_cores(seed, nframes, iq, pq, workers):
 
 # dram__bytes_read.sum + dram__bytes_write.sum of one steady-state k_search launch at this
 # workload (ncu --set full, caches flushed before each pass, launch 7 of the bench
-# command): 9,851,648 + 39,680 bytes.  The SAD table, the prediction, the pre-deblock
+# command): 9,853,184 + 59,904 bytes.  The SAD table, the prediction, the pre-deblock
 # reconstruction and the coefficients are produced and consumed inside the launch (or by the
 # next one) and stay in L2.
-SEARCH_TRAFFIC_BYTES = 9_851_648 + 39_680
+SEARCH_TRAFFIC_BYTES = 9_853_184 + 59_904
 
 Y_BYTES = 1920 * 1088            # one luma plane (storage size)
 YUV_BYTES = Y_BYTES * 3 // 2     # one 4:2:0 frame
