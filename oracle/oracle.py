@@ -259,10 +259,13 @@ def yuv_to_rgb(f: Frames, dw: int, dh: int) -> np.ndarray:
 
 
 def dct_encode(blocks: np.ndarray, intra: bool) -> bytes:
-    """The oracle's DCT-coefficient coder of one frame on dense (n, 384) int16 blocks."""
+    """The oracle's DCT-coefficient coder of one frame on dense (n, 384) int16 blocks.
+    Raises ValueError where the reference encoder panics (a magnitude class above 13)."""
     b = np.ascontiguousarray(blocks, dtype=np.int16)
     n = b.shape[0]
     size = lib().oracle_dct_encode(b.ctypes.data, n, int(intra), None, 0)
+    if size == C.c_size_t(-1).value:
+        raise ValueError("magnitude class above 13: the reference encoder panics")
     out = np.zeros(max(size, 1), np.uint8)
     lib().oracle_dct_encode(b.ctypes.data, n, int(intra), out.ctypes.data, size)
     return out[:size].tobytes()

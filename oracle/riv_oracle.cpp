@@ -979,9 +979,12 @@ static inline int eob_class(unsigned v) { return v <= 1 ? (int)v : 32 - __builti
 static inline int luma_band(int p) { return p == 0 ? 0 : (p < 16 ? 1 : (p < 64 ? 2 : 3)); }
 static inline int chroma_band(int p) { return p == 0 ? 0 : (p < 8 ? 1 : 2); }
 static bool g_overflow = false;  // set where the reference would panic (index out of bounds)
+// Class nctx is still coded (nctx continue bits, no stop bit), as the reference does,
+// although its decoder stops at class nctx - 1; from class nctx + 1 the reference indexes
+// contexts[nctx] and panics (reitero_residual/src/rans.rs:81-83).
 static void enc_class_value(RansEnc& w, unsigned value, BinProb* ctx, int nctx) {  // :72-98,133-159
     int maxc = nctx - 1, cls = eob_class(value);
-    if (cls > maxc) { g_overflow = true; return; }  // the reference panics here
+    if (cls > nctx) { g_overflow = true; return; }  // the reference panics here
     for (int c = 0; c < cls; c++) w.put(true, ctx[c]);
     if (cls < maxc) w.put(false, ctx[cls]);
     if (cls >= 2) {
@@ -2169,8 +2172,10 @@ size_t oracle_rans_roundtrip(const uint8_t* bits, const uint8_t* bypass, size_t 
 }
 double oracle_glibc_logf_check(void) { return (double)logf(10.0f); }
 
+// Returns SIZE_MAX where the reference encoder panics (a magnitude class above 13).
 size_t oracle_dct_encode(const int16_t* blocks, int n, int intra, uint8_t* stream, size_t cap) {  // res/rans.rs:195-330
     init_zero_prob();
+    g_overflow = false;
     Bytes s;
     if (n > 0) {
         RansEnc w(&s);
@@ -2184,6 +2189,7 @@ size_t oracle_dct_encode(const int16_t* blocks, int n, int intra, uint8_t* strea
         }
         w.finish();
     }
+    if (g_overflow) return SIZE_MAX;
     if (stream && cap) memcpy(stream, s.data(), std::min(cap, s.size()));
     return s.size();
 }

@@ -2,6 +2,9 @@
 #include "riv_entropy.h"
 
 #include <algorithm>
+#include <atomic>
+#include <exception>
+#include <stdexcept>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -49,6 +52,10 @@ static inline void observe(BinProb& b, bool bit) {  // com/rans.rs:73-84
 }
 
 static const int BATCH = 16386;  // com/rans.rs:201
+// The parallel coefficient coder takes frames of 16K to 2M coded coefficients: below, its
+// fork and join cost more than they save; above, its symbol lists (up to about 26 symbols per
+// coefficient) would take hundreds of MB.
+static const uint32_t PARALLEL_MIN_COEFFS = 16384, PARALLEL_MAX_COEFFS = 2u << 20;
 
 RansWriter::RansWriter(std::vector<uint8_t>* sink, const BatchSubmit* submit)
     : sink_(sink), stack_(BATCH), sp_(BATCH), submit_(submit) {}
@@ -204,13 +211,63 @@ static inline int bit_len(unsigned v) { return v <= 1 ? (int)v : 32 - __builtin_
 static inline int luma_band(int p) { return p == 0 ? 0 : (p < 16 ? 1 : (p < 64 ? 2 : 3)); }
 static inline int chroma_band(int p) { return p == 0 ? 0 : (p < 8 ? 1 : 2); }
 
-static inline void put_class_value(RansWriter& w, unsigned value, BinProb* ctx, int nctx) {
+// The coder's adaptive models as one flat array of ids: sig_y[256], sig_c[64], mag_y[4][13],
+// mag_c[3][13], eob_y[9], eob_c[7] (res/rans.rs:195-248).  CX_BYPASS marks a bypass symbol.
+constexpr int CX_SIG_Y = 0, CX_SIG_C = 256, CX_MAG_Y = 320, CX_MAG_C = 372, CX_EOB_Y = 411, CX_EOB_C = 420,
+              CX_COUNT = 427, CX_BYPASS = 511;
+
+// The binary symbols of the coefficient stream, in coding order, for any sink W with
+// put(bit, model id), bypass(bit) and a flag `bad`: the class/value code
+// (reitero_residual/src/rans.rs:72-98, 133-159).  Class nctx is coded with nctx continue
+// bits and no stop bit, as the reference does; above it the reference indexes past its
+// models and panics, so the sink is marked bad and the frame fails.
+template <class W>
+static inline void class_value_syms(W& w, unsigned value, int cx0, int nctx) {
     int maxc = nctx - 1, cls = bit_len(value);
-    for (int c = 0; c < cls; c++) w.put(true, ctx[c]);
-    if (cls < maxc) w.put(false, ctx[cls]);
+    if (cls > nctx) {
+        w.bad = true;
+        return;
+    }
+    for (int c = 0; c < cls; c++) w.put(true, cx0 + c);
+    if (cls < maxc) w.put(false, cx0 + cls);
     if (cls >= 2) {
         unsigned off = value - (1u << (cls - 1));
-        for (int b = cls - 2; b >= 0; b--) w.put_bypass((off >> b) & 1);
+        for (int b = cls - 2; b >= 0; b--) w.bypass((off >> b) & 1);
+    }
+}
+// ... one plane block: EOB class, then per coefficient up to it the significance flag, sign
+// and magnitude class (res/rans.rs:250-278); intra DC values are coded against the previous
+// block's (prev_dc, per plane) ...
+template <class W>
+static void plane_syms(W& w, int16_t* prev_dc, const int16_t* pl, int last, bool luma, int pi, bool dcp) {
+    int16_t dcv = pl[0];
+    if (dcp) {
+        dcv = (int16_t)(pl[0] - prev_dc[pi]);
+        prev_dc[pi] = pl[0];
+    }
+    class_value_syms(w, (unsigned)last, luma ? CX_EOB_Y : CX_EOB_C, luma ? 9 : 7);
+    const int sig0 = luma ? CX_SIG_Y : CX_SIG_C;
+    for (int i = 0; i <= last; i++) {
+        int16_t v = i == 0 ? dcv : pl[i];
+        w.put(v != 0, sig0 + i);
+        if (v != 0) {
+            w.bypass(v < 0);
+            unsigned a = (unsigned)std::abs((int)v) - 1;
+            class_value_syms(w, a, luma ? CX_MAG_Y + 13 * luma_band(i) : CX_MAG_C + 13 * chroma_band(i), 13);
+        }
+    }
+}
+// ... and blocks [b0, b1) of the compact layout starting at p (Y, U, V per MB).
+template <class W>
+static void blocks_syms(W& w, int16_t* prev_dc, const int16_t* p, const uint8_t* eobs, int b0, int b1, bool intra) {
+    for (int b = b0; b < b1; b++) {
+        const uint8_t* e = eobs + 3 * b;
+        plane_syms(w, prev_dc, p, e[0], true, 0, intra);
+        p += e[0] + 1;
+        plane_syms(w, prev_dc, p, e[1], false, 1, intra);
+        p += e[1] + 1;
+        plane_syms(w, prev_dc, p, e[2], false, 2, intra);
+        p += e[2] + 1;
     }
 }
 
@@ -219,48 +276,192 @@ struct DctContexts {
     int16_t prev_dc[3] = {0, 0, 0};
 };
 
-static void encode_plane(RansWriter& w, DctContexts& c, const int16_t* pl, int last, bool luma, int pi, bool dcp) {
-    int16_t dcv = pl[0];
-    if (dcp) {
-        dcv = (int16_t)(pl[0] - c.prev_dc[pi]);
-        c.prev_dc[pi] = pl[0];
+// Sequential sink: models the symbols into a RansWriter.
+struct ModelSink {
+    RansWriter& w;
+    BinProb* cx;
+    bool bad = false;
+    void put(bool bit, int id) { w.put(bit, cx[id]); }
+    void bypass(bool bit) { w.put_bypass(bit); }
+};
+// Enumerating sink: model id | bit << 15 per symbol, and how often each model is used.
+struct SymList {
+    std::vector<uint16_t> s;
+    uint32_t cnt[CX_COUNT] = {};
+    bool bad = false;
+    void put(bool bit, int id) {
+        s.push_back((uint16_t)(id | (bit ? 0x8000 : 0)));
+        cnt[id]++;
     }
-    if (luma) put_class_value(w, (unsigned)last, c.eob_y, 9);
-    else put_class_value(w, (unsigned)last, c.eob_c, 7);
-    BinProb* sig = luma ? c.sig_y : c.sig_c;
-    for (int i = 0; i <= last; i++) {
-        int16_t v = i == 0 ? dcv : pl[i];
-        w.put(v != 0, sig[i]);
-        if (v != 0) {
-            w.put_bypass(v < 0);
-            unsigned a = (unsigned)std::abs((int)v) - 1;
-            BinProb* mc = luma ? c.mag_y[luma_band(i)] : c.mag_c[chroma_band(i)];
-            put_class_value(w, a, mc, 13);
+    void bypass(bool bit) { s.push_back((uint16_t)(CX_BYPASS | (bit ? 0x8000 : 0))); }
+};
+
+struct ParallelWork {
+    std::vector<SymList> lists;
+    std::vector<uint16_t> stacks;
+    std::vector<uint32_t> occ;
+    std::vector<std::vector<uint8_t>> bytes;
+};
+
+static const char* const MAG_CLASS_ERROR = "coefficient magnitude class above 13 (the reference encoder panics)";
+
+// Runs f(0) here and f(1 .. parts-1) through submit; returns when all have ended.
+static void run_parts(const BatchSubmit& submit, int parts, const std::function<void(int)>& f) {
+    std::vector<std::future<void>> fs;
+    std::exception_ptr err;
+    try {
+        for (int t = 1; t < parts; t++) fs.push_back(submit([&f, t] { f(t); }));
+        f(0);
+    } catch (...) {
+        err = std::current_exception();
+    }
+    for (auto& x : fs) {
+        try {
+            x.get();
+        } catch (...) {
+            if (!err) err = std::current_exception();
         }
     }
+    if (err) std::rethrow_exception(err);
+}
+
+// Stack slot of the symbol at stream position k: batch k / BATCH, whose stack holds its
+// oldest symbol at the top (RansWriter::put pushes downwards).
+static inline size_t stack_slot(size_t k) { return (k / BATCH) * BATCH + (BATCH - 1 - k % BATCH); }
+
+// The same stream as the sequential coder, with the work split `parts` ways.  A model's
+// probability at each of its symbols depends only on the bits it saw before, so: (1) each
+// part lists the symbols (model id, bit) of a range of blocks; (2) the symbols are grouped
+// by model (counting sort, positions in stream order); (3) each part runs a set of models
+// over their own symbols and writes each symbol's (probability, bit) into its rANS batch
+// stack; (4) the batches, which start from fresh states, are coded in parallel and
+// appended in order.
+static void encode_residual_parallel(const int16_t* packed, const uint8_t* eobs, int nblocks, bool intra,
+                                     const std::vector<uint32_t>& off, std::vector<uint8_t>& out,
+                                     const BatchSubmit& submit, int parts) {
+    std::vector<int> bstart(parts + 1);
+    for (int t = 0; t <= parts; t++)
+        bstart[t] = (int)(std::lower_bound(off.begin(), off.end(), (uint32_t)((uint64_t)off[nblocks] * t / parts)) -
+                          off.begin());
+    bstart[0] = 0;
+    bstart[parts] = nblocks;
+    // buffers of the calling thread, kept from frame to frame (no page faults, no zeroing)
+    thread_local ParallelWork ws;
+    std::vector<SymList>& lists = ws.lists;
+    lists.resize(parts);
+    run_parts(submit, parts, [&](int t) {
+        const int b0 = bstart[t], b1 = std::max(bstart[t], bstart[t + 1]);
+        SymList& L = lists[t];
+        L.s.clear();
+        std::fill(L.cnt, L.cnt + CX_COUNT, 0u);
+        L.bad = false;
+        L.s.reserve((size_t)(off[b1] - off[b0]) * 2 + (size_t)(b1 - b0) * 12);
+        int16_t prev_dc[3] = {0, 0, 0};
+        if (intra && b0 > 0) {
+            const int16_t* q = packed + off[b0 - 1];
+            const uint8_t* e = eobs + 3 * (b0 - 1);
+            prev_dc[0] = q[0];
+            prev_dc[1] = q[e[0] + 1];
+            prev_dc[2] = q[e[0] + 1 + e[1] + 1];
+        }
+        blocks_syms(L, prev_dc, packed + off[b0], eobs, b0, b1, intra);
+    });
+    std::vector<size_t> sbase(parts + 1, 0);
+    for (int t = 0; t < parts; t++) {
+        if (lists[t].bad) throw std::runtime_error(MAG_CLASS_ERROR);
+        sbase[t + 1] = sbase[t] + lists[t].s.size();
+    }
+    const size_t N = sbase[parts], nb = (N + BATCH - 1) / BATCH;
+    std::vector<uint32_t> cbase(CX_COUNT + 1), cstart((size_t)parts * CX_COUNT);
+    uint32_t acc = 0;
+    for (int c = 0; c < CX_COUNT; c++) {
+        cbase[c] = acc;
+        for (int t = 0; t < parts; t++) {
+            cstart[(size_t)t * CX_COUNT + c] = acc;
+            acc += lists[t].cnt[c];
+        }
+    }
+    cbase[CX_COUNT] = acc;
+    std::vector<uint16_t>& stacks = ws.stacks;
+    std::vector<uint32_t>& occ = ws.occ;  // per model, in stream order: position | bit << 31
+    if (stacks.size() < nb * BATCH) stacks.resize(nb * BATCH);
+    if (occ.size() < acc) occ.resize(acc);
+    run_parts(submit, parts, [&](int t) {
+        uint32_t* cs = cstart.data() + (size_t)t * CX_COUNT;
+        size_t k = sbase[t];
+        for (uint16_t e : lists[t].s) {
+            const int c = e & 0x1ff;
+            const uint32_t bit = e >> 15;
+            if (c == CX_BYPASS) stacks[stack_slot(k)] = (uint16_t)(128 | bit << 8);
+            else occ[cs[c]++] = (uint32_t)k | bit << 31;
+            k++;
+        }
+    });
+    // models to parts, largest first onto the least loaded part
+    std::vector<int> order(CX_COUNT);
+    for (int c = 0; c < CX_COUNT; c++) order[c] = c;
+    std::sort(order.begin(), order.end(), [&](int a, int b) {
+        const uint32_t na = cbase[a + 1] - cbase[a], nb_ = cbase[b + 1] - cbase[b];
+        return na != nb_ ? na > nb_ : a < b;
+    });
+    std::vector<std::vector<int>> groups(parts);
+    std::vector<uint64_t> load(parts, 0);
+    for (int c : order) {
+        const uint32_t n = cbase[c + 1] - cbase[c];
+        if (n == 0) break;
+        const int t = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        groups[t].push_back(c);
+        load[t] += n;
+    }
+    run_parts(submit, parts, [&](int t) {
+        for (int c : groups[t]) {
+            BinProb st;
+            for (uint32_t i = cbase[c]; i < cbase[c + 1]; i++) {
+                const uint32_t e = occ[i];
+                const bool bit = (e >> 31) != 0;
+                stacks[stack_slot(e & 0x7fffffffu)] = (uint16_t)(prob_zero(st) | (bit ? 0x100 : 0));
+                observe(st, bit);
+            }
+        }
+    });
+    std::vector<std::vector<uint8_t>>& bytes = ws.bytes;
+    if (bytes.size() < nb) bytes.resize(nb);
+    for (size_t j = 0; j < nb; j++) bytes[j].clear();
+    std::atomic<size_t> next{0};
+    run_parts(submit, parts, [&](int) {
+        for (size_t j; (j = next.fetch_add(1)) < nb;) {
+            const size_t len = std::min<size_t>(BATCH, N - j * BATCH);
+            code_batch(stacks.data() + j * BATCH, (int)(BATCH - len), bytes[j]);
+        }
+    });
+    out.clear();
+    for (size_t j = 0; j < nb; j++) out.insert(out.end(), bytes[j].begin(), bytes[j].end());
 }
 
 void encode_residual_frame(const int16_t* packed, const uint8_t* eobs, int nblocks, bool intra,
-                           std::vector<uint8_t>& out, const BatchSubmit* submit) {
+                           std::vector<uint8_t>& out, const BatchSubmit* submit, int parts) {
     out.clear();
     if (nblocks == 0) return;  // the reference never instantiates the coder
-    RansWriter w(&out, submit);
-    DctContexts* c = new DctContexts();
-    const int16_t* p = packed;
-    for (int b = 0; b < nblocks; b++) {
-        const uint8_t* e = eobs + 3 * b;
-        // With DC prediction the coded range ends at the last non-zero AC coefficient
-        // (res/rans.rs:250-262); the GPU's last-non-zero index already equals it.  The
-        // compact layout holds each plane block only up to that index.
-        encode_plane(w, *c, p, e[0], true, 0, intra);
-        p += e[0] + 1;
-        encode_plane(w, *c, p, e[1], false, 1, intra);
-        p += e[1] + 1;
-        encode_plane(w, *c, p, e[2], false, 2, intra);
-        p += e[2] + 1;
+    // With DC prediction the coded range ends at the last non-zero AC coefficient
+    // (res/rans.rs:250-262); the GPU's last-non-zero index already equals it.  The compact
+    // layout holds each plane block only up to that index.
+    if (submit != nullptr && parts > 1) {
+        std::vector<uint32_t> off((size_t)nblocks + 1);
+        off[0] = 0;
+        for (int b = 0; b < nblocks; b++)
+            off[b + 1] = off[b] + eobs[3 * b] + eobs[3 * b + 1] + eobs[3 * b + 2] + 3;
+        if (off[nblocks] >= PARALLEL_MIN_COEFFS && off[nblocks] <= PARALLEL_MAX_COEFFS) {
+            encode_residual_parallel(packed, eobs, nblocks, intra, off, out, *submit, parts);
+            return;
+        }
     }
+    RansWriter w(&out, submit);
+    std::vector<BinProb> cx(CX_COUNT);
+    int16_t prev_dc[3] = {0, 0, 0};
+    ModelSink sink{w, cx.data()};
+    blocks_syms(sink, prev_dc, packed, eobs, 0, nblocks, intra);
+    if (sink.bad) throw std::runtime_error(MAG_CLASS_ERROR);
     w.finish();
-    delete c;
 }
 
 static inline unsigned get_class_value(RansReader& r, BinProb* ctx, int nctx) {

@@ -79,9 +79,12 @@ bool decode_residual_frame(const uint8_t* data, size_t len, const uint8_t* coded
 
 // Coded MBs in the GPU's compact layout: per MB, the Y, U and V blocks each truncated
 // after its last non-zero coefficient (eobs = those three indices per MB).
-// `submit` (optional) codes the full rANS batches on other threads.
+// `submit` (optional) codes the full rANS batches on other threads; with parts > 1 as well,
+// frames of 16K to 2M coded coefficients are coded by `parts` threads at once (this one and
+// parts - 1 jobs given to submit, which must not run them on this thread), same bytes.
+// Throws std::runtime_error where the reference encoder panics (a magnitude class above 13).
 void encode_residual_frame(const int16_t* packed, const uint8_t* eobs, int nblocks, bool intra,
-                           std::vector<uint8_t>& out, const BatchSubmit* submit = nullptr);
+                           std::vector<uint8_t>& out, const BatchSubmit* submit = nullptr, int parts = 0);
 
 enum MvMode { M_ZERO = 0, M_NEAREST = 1, M_NEAR = 2, M_TOPRIGHT = 3, M_TOPLEFT = 4, M_NEW = 5, M_TEMPORAL = 6 };
 enum Subpel { SP_ZERO = 0, SP_PLUS = 1, SP_MINUS = 2 };

@@ -383,8 +383,10 @@ struct riv_encoder {
     MvCoder mvc;
     std::unique_ptr<ThreadPool> pool;
     std::unique_ptr<ThreadPool> mv_exec;  // one thread: MV coding strictly in frame order
-    std::unique_ptr<ThreadPool> rans_pool;  // rANS coding of full coefficient batches (never waits)
+    std::unique_ptr<ThreadPool> rans_pool;  // coefficient-coder jobs (never wait)
     BatchSubmit rans_submit;
+    int rans_parts = 1;  // threads that code one frame's coefficients: rans_pool's and the caller
+    bool draining = false;  // inside drain_all: the newest frame is coded by rans_parts threads
     double host_ms[6] = {0};  // submit, retire, mv coding, dct coding (summed), write, blocked
     std::mutex stat_mu;
     float last_times[NSTAGE + 1] = {0};
@@ -567,6 +569,7 @@ static void setup_device(riv_encoder* e) {
     e->pool.reset(new ThreadPool(nt));
     e->mv_exec.reset(new ThreadPool(1));
     e->rans_pool.reset(new ThreadPool(std::max(2u, nt / 2)));
+    e->rans_parts = (int)std::max(2u, nt / 2) + 1;
     {
         ThreadPool* rp = e->rans_pool.get();
         e->rans_submit = [rp](std::function<void()> f) { return rp->submit(std::move(f)); };
@@ -956,9 +959,13 @@ static riv_status retire(riv_encoder* e, Job& j) {
     const uint8_t* peobs = s.peobs.as<uint8_t>();
     uint32_t count = j.count;
     bool intra = j.type == 1;
-    j.fut = e->pool->submit([jp, ep, packed, peobs, count, intra] {
+    // The newest frame of a drain is coded by all of rans_pool's threads (no later frame will
+    // be coded beside it); the others model on one pool thread and hand their full rANS
+    // batches to rans_pool, which keeps the CPU cost per frame lowest while frames overlap.
+    const int parts = e->draining && &j == &e->jobs.back() ? e->rans_parts : 1;
+    j.fut = e->pool->submit([jp, ep, packed, peobs, count, intra, parts] {
         double d0 = now_ms();
-        encode_residual_frame(packed, peobs, (int)count, intra, jp->res_bytes, &ep->rans_submit);
+        encode_residual_frame(packed, peobs, (int)count, intra, jp->res_bytes, &ep->rans_submit, parts);
         double dt = now_ms() - d0;
         std::lock_guard<std::mutex> g(ep->stat_mu);
         ep->host_ms[3] += dt;
@@ -1048,6 +1055,11 @@ static riv_status pump(riv_encoder* e, bool block_front) {
 
 static riv_status drain_all(riv_encoder* e) {
     flush_pending(e);  // no later launch is coming: reconstruct now, before the host work queued ahead of it
+    struct Draining {
+        riv_encoder* e;
+        ~Draining() { e->draining = false; }
+    } guard{e};
+    e->draining = true;
     while (!e->jobs.empty()) {
         riv_status st = pump(e, true);
         if (st) return st;
@@ -1518,7 +1530,7 @@ riv_status riv_test_dct_encode(const int16_t* blocks, uint32_t n, int intra, uin
         if (threads > 0) {
             ThreadPool pool(threads);
             BatchSubmit sub = [&pool](std::function<void()> f) { return pool.submit(std::move(f)); };
-            encode_residual_frame(packed.data(), eobs.data(), (int)n, intra != 0, stream, &sub);
+            encode_residual_frame(packed.data(), eobs.data(), (int)n, intra != 0, stream, &sub, (int)threads + 1);
         } else {
             encode_residual_frame(packed.data(), eobs.data(), (int)n, intra != 0, stream);
         }

@@ -1,7 +1,8 @@
 """The encoder's host DCT-coefficient coder (riv_entropy.cpp, behind riv_test_dct_encode)
 against the oracle's restatement of res/rans.rs:195-330, byte for byte, on CPU: P-frame
 and intra (DC prediction) blocks, frames shorter than one rANS batch and frames of several
-batches, coded inline and with the full batches on a thread pool as the pipelined encoder
+batches, coded inline, with the full batches on a thread pool, and by the parallel coder
+(block ranges, models evolved per thread, batches in parallel) as the pipelined encoder
 does."""
 import numpy as np
 import pytest
@@ -45,3 +46,33 @@ def test_dct_coder_spans_several_batches_and_all_zero_blocks():
     assert len(ref) > 50_000
     assert dct_encode_host(b, False, 0) == ref
     assert dct_encode_host(b, False, 4) == ref
+
+
+@pytest.mark.parametrize("intra", [False, True])
+@pytest.mark.parametrize("threads", [1, 2, 6])
+def test_parallel_dct_coder_matches_oracle(threads, intra):
+    """Frames of 16K to 2M coded coefficients are split over threads + 1 parts: the symbols
+    of block ranges are listed in parallel, grouped by model, each model's probabilities
+    evolved on one thread, and the rANS batches coded in parallel.  Same bytes, including
+    the intra DC prediction across range boundaries and all-zero blocks."""
+    from riv2_b200.encoder import dct_encode_host
+    b = _blocks(2500, 11 + threads, density=0.4, big=True)
+    b[300:340] = 0
+    assert dct_encode_host(b, intra, threads) == O.dct_encode(b, intra)
+
+
+@pytest.mark.parametrize("threads", [0, 3])
+def test_magnitude_classes_13_and_14(threads):
+    """A magnitude of class 13 (|v| - 1 in [4096, 8191]) is coded with 13 continue bits and
+    no stop bit, as the reference's encode_magnitude does (reitero_residual/src/rans.rs:72-98);
+    from class 14 the reference indexes past its 13 models and panics, and the frame fails."""
+    from riv2_b200.encoder import dct_encode_host, EncodingFailed
+    b = _blocks(400, 21, density=0.5)
+    b[5, 3] = 5000
+    b[200, 260] = -8000
+    assert dct_encode_host(b, False, threads) == O.dct_encode(b, False)
+    b[300, 40] = 9000
+    with pytest.raises(ValueError):
+        O.dct_encode(b, False)
+    with pytest.raises(EncodingFailed):
+        dct_encode_host(b, False, threads)
