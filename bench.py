@@ -39,7 +39,8 @@ sys.path.insert(0, ROOT)
 
 W_DISP, H_DISP, FPS = 1920, 1080, 50
 MBS_PER_FRAME = (1920 // 16) * (1088 // 16)
-METRIC = json.load(open(os.path.join(ROOT, "BASELINE.json")))["metric"]
+# the headline metric this line reports (only the plain form exists; "form" in config says so)
+METRIC = "1080p encode fps: learned-proposal vs plain GPU at \u22640.1 dB PSNR, \u22642% bitrate"
 
 
 def parse():
