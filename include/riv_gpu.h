@@ -179,8 +179,11 @@ riv_status riv_libm_fixup_counts(uint32_t* nlog, uint32_t* nexp);
 void riv_dct_tables(int32_t* t16, int32_t* t8);
 /* Test hook (host only, no reference counterpart): the encoder's DCT-coefficient coder on n
  * dense blocks of 384 i16 (Y 256, U 64, V 64), laid out as the GPU compaction does, with DC
- * prediction when intra; threads > 0 codes the full rANS batches on a pool of that many
- * threads, as the pipelined encoder does.  *len = stream size; up to cap bytes copied. */
+ * prediction when intra; threads > 0 codes it in parallel on this thread and a pool of that
+ * many threads, as the encoder does for the newest frame of a drain (frames of 16K to 2M
+ * coded coefficients; smaller ones model here and hand the full rANS batches to the pool).
+ * *len = stream size; up to cap bytes copied.  RIV_ERR_ENCODING_FAILED where the reference
+ * encoder panics (a magnitude class above 13). */
 riv_status riv_test_dct_encode(const int16_t* blocks, uint32_t n, int intra, uint32_t threads, uint8_t* out, size_t cap,
                                size_t* len);
 /* Test hook (host only, no reference counterpart): the worker-task queue of the fused search
