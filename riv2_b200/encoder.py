@@ -545,8 +545,9 @@ def stage_libm(which: int, x: np.ndarray) -> np.ndarray:
 
 def dct_encode_host(blocks: np.ndarray, intra: bool, threads: int = 0) -> bytes:
     """The encoder's host DCT-coefficient coder on dense (n, 384) int16 blocks (test hook,
-    no GPU needed); threads > 0 codes the rANS batches on a pool as the pipelined encoder
-    does."""
+    no GPU needed); threads > 0 runs its parallel form on this thread and a pool of that many
+    threads (frames of 16K to 2M coded coefficients), as the encoder does for the newest
+    frame of a drain.  Raises EncodingFailed where the reference encoder panics."""
     b = np.ascontiguousarray(blocks, dtype=np.int16)
     n = C.c_size_t(0)
     st = lib().riv_test_dct_encode(b.ctypes.data, b.shape[0], int(intra), threads, None, 0, C.byref(n))
