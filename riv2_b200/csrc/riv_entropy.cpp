@@ -56,6 +56,7 @@ static const int BATCH = 16386;  // com/rans.rs:201
 // fork and join cost more than they save; above, its symbol lists (up to about 26 symbols per
 // coefficient) would take hundreds of MB.
 static const uint32_t PARALLEL_MIN_COEFFS = 16384, PARALLEL_MAX_COEFFS = 2u << 20;
+static const size_t WORK_KEEP_BYTES = 64u << 20;  // parallel coder buffers kept per thread
 
 RansWriter::RansWriter(std::vector<uint8_t>* sink, const BatchSubmit* submit)
     : sink_(sink), stack_(BATCH), sp_(BATCH), submit_(submit) {}
@@ -436,6 +437,11 @@ static void encode_residual_parallel(const int16_t* packed, const uint8_t* eobs,
     });
     out.clear();
     for (size_t j = 0; j < nb; j++) out.insert(out.end(), bytes[j].begin(), bytes[j].end());
+    // keep the buffers for the next frame only while they are small (a frame of huge
+    // coefficients must not pin hundreds of MB on every thread that ever coded one)
+    size_t held = ws.stacks.capacity() * 2 + ws.occ.capacity() * 4;
+    for (const SymList& L : ws.lists) held += L.s.capacity() * 2;
+    if (held > WORK_KEEP_BYTES) ws = ParallelWork();
 }
 
 void encode_residual_frame(const int16_t* packed, const uint8_t* eobs, int nblocks, bool intra,
