@@ -12,9 +12,22 @@
 namespace riv {
 
 static uint8_t g_zero_prob[65536];
+static uint16_t g_next[2][65536];  // BinProb state after a 0 / a 1
 static uint64_t g_rcp_m[256];
 static uint32_t g_rcp_s[256];
 static std::once_flag g_once;
+
+// BinProb update after one bit (com/rans.rs:73-84); tabulated in g_next.
+static uint16_t observe_calc(uint16_t packed, bool bit) {
+    uint16_t rot = bit ? (uint16_t)((packed << 8) | (packed >> 8)) : packed;
+    uint32_t sum = (uint32_t)rot + 0x100u;
+    uint16_t upd = (uint16_t)sum;
+    if (sum > 0xFFFFu) {
+        uint16_t mask = rot == 0xff01 ? 0xff00 : 0x8100;
+        upd = (uint16_t)((uint16_t)(rot + 0x101) >> 1) | mask;
+    }
+    return bit ? (uint16_t)((upd << 8) | (upd >> 8)) : upd;
+}
 
 void entropy_init() {
     std::call_once(g_once, [] {
@@ -25,6 +38,10 @@ void entropy_init() {
             int zeros = i >> 8, ones = i & 0xff;
             uint8_t p = (uint8_t)((zeros << 8) / (zeros + ones));
             g_zero_prob[i] = p ? p : 1;
+        }
+        for (uint32_t st = 0; st < 65536; st++) {
+            g_next[0][st] = observe_calc((uint16_t)st, false);
+            g_next[1][st] = observe_calc((uint16_t)st, true);
         }
         // Exact reciprocals for r / f, f in [1,255], r < 2^32 (round-up multiplier with
         // s = 32 + ceil(log2 f) fraction bits).
@@ -40,16 +57,7 @@ void entropy_init() {
 }
 
 static inline uint8_t prob_zero(const BinProb& b) { return g_zero_prob[b.packed]; }
-static inline void observe(BinProb& b, bool bit) {  // com/rans.rs:73-84
-    uint16_t rot = bit ? (uint16_t)((b.packed << 8) | (b.packed >> 8)) : b.packed;
-    uint32_t sum = (uint32_t)rot + 0x100u;
-    uint16_t upd = (uint16_t)sum;
-    if (sum > 0xFFFFu) {
-        uint16_t mask = rot == 0xff01 ? 0xff00 : 0x8100;
-        upd = (uint16_t)((uint16_t)(rot + 0x101) >> 1) | mask;
-    }
-    b.packed = bit ? (uint16_t)((upd << 8) | (upd >> 8)) : upd;
-}
+static inline void observe(BinProb& b, bool bit) { b.packed = g_next[bit][b.packed]; }
 
 static const int BATCH = 16386;  // com/rans.rs:201
 // The parallel coefficient coder takes frames of 16K to 2M coded coefficients: below, its
