@@ -186,6 +186,12 @@ void riv_dct_tables(int32_t* t16, int32_t* t8);
  * encoder panics (a magnitude class above 13). */
 riv_status riv_test_dct_encode(const int16_t* blocks, uint32_t n, int intra, uint32_t threads, uint8_t* out, size_t cap,
                                size_t* len);
+/* Test hook (host only, no reference counterpart): the decoder's DCT-coefficient decoder on one
+ * frame's coefficient stream; n blocks of 384 i16 out, blocks with coded[b] == 0 are not in the
+ * stream and stay zero; DC prediction when intra.  RIV_OK, or RIV_ERR_FRAME where the stream is
+ * malformed (read past its end, an EOB beyond the plane: the reference decoder panics). */
+riv_status riv_test_dct_decode(const uint8_t* data, size_t len, const uint8_t* coded, uint32_t n, int intra,
+                               int16_t* out);
 /* Test hook (host only, no reference counterpart): the worker-task queue of the fused search
  * launch for a frame of bw x bh MBs and w storage columns, in the order the kernel hands the
  * tasks out: 3 int32 per task (kind 0 residual pair / 1 deblock tile / 2 SAD-table MB / 3 scan

@@ -97,6 +97,7 @@ def lib():
                                          C.c_uint32, C.c_void_p]
         L.oracle_dct_encode.restype = C.c_size_t
         L.oracle_dct_encode.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t]
+        L.oracle_dct_decode.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         L.oracle_rans_roundtrip.restype = C.c_size_t
         L.oracle_rans_roundtrip.argtypes = [U8, U8, C.c_size_t, U8, U8, C.c_size_t]
         _lib = L
@@ -269,6 +270,16 @@ def dct_encode(blocks: np.ndarray, intra: bool) -> bytes:
     out = np.zeros(max(size, 1), np.uint8)
     lib().oracle_dct_encode(b.ctypes.data, n, int(intra), out.ctypes.data, size)
     return out[:size].tobytes()
+
+
+def dct_decode(data: bytes, coded: np.ndarray, intra: bool):
+    """The oracle's coefficient decoder of one frame: (dense (n, 384) int16 blocks, ok), ok
+    False where the stream is malformed (the reference decoder panics there)."""
+    c = np.ascontiguousarray(coded, dtype=np.uint8)
+    out = np.zeros((c.size, 384), np.int16)
+    buf = np.frombuffer(data, np.uint8) if len(data) else np.zeros(1, np.uint8)
+    st = lib().oracle_dct_decode(buf.ctypes.data, len(data), c.ctypes.data, c.size, int(intra), out.ctypes.data)
+    return out, st == 0
 
 
 def rgb_to_yuv(rgb: np.ndarray, dw: int, dh: int, sw: int, sh: int) -> Frames:

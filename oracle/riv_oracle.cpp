@@ -2172,6 +2172,27 @@ size_t oracle_rans_roundtrip(const uint8_t* bits, const uint8_t* bypass, size_t 
 }
 double oracle_glibc_logf_check(void) { return (double)logf(10.0f); }
 
+// The coefficient decoder of one frame (res/rans.rs:340-459): blocks with coded[b] == 0 are
+// not in the stream and stay zero.  Returns 1 where the stream is malformed (read past its
+// end, an EOB beyond the plane), where the reference decoder panics; the blocks then hold
+// what was decoded.
+int oracle_dct_decode(const uint8_t* d, size_t len, const uint8_t* coded, int n, int intra, int16_t* out) {
+    init_zero_prob();
+    std::fill(out, out + (size_t)n * 384, (int16_t)0);
+    if (len == 0) return 0;
+    RansDec r(d, len);
+    DctCtx ctx;
+    ctx.dcp = intra != 0;
+    for (int b = 0; b < n && !r.err; b++) {
+        if (!coded[b]) continue;
+        int16_t* p = out + (size_t)b * 384;
+        dct_decode_plane(r, ctx, p, 256, true, 0);
+        if (!r.err) dct_decode_plane(r, ctx, p + 256, 64, false, 1);
+        if (!r.err) dct_decode_plane(r, ctx, p + 320, 64, false, 2);
+    }
+    return r.err ? 1 : 0;
+}
+
 // Returns SIZE_MAX where the reference encoder panics (a magnitude class above 13).
 size_t oracle_dct_encode(const int16_t* blocks, int n, int intra, uint8_t* stream, size_t cap) {  // res/rans.rs:195-330
     init_zero_prob();

@@ -1507,6 +1507,13 @@ riv_status riv_test_worker_queue(uint32_t bw, uint32_t bh, uint32_t w, int defer
     return i == (size_t)queue_total(q) ? RIV_OK : RIV_ERR_ENCODING_FAILED;
 }
 
+riv_status riv_test_dct_decode(const uint8_t* data, size_t len, const uint8_t* coded, uint32_t n, int intra,
+                               int16_t* out) {
+    if ((len > 0 && !data) || (n > 0 && (!coded || !out))) return RIV_ERR_FRAME;
+    entropy_init();
+    return decode_residual_frame(data, len, coded, (int)n, intra != 0, out) ? RIV_OK : RIV_ERR_FRAME;
+}
+
 riv_status riv_test_dct_encode(const int16_t* blocks, uint32_t n, int intra, uint32_t threads, uint8_t* out, size_t cap,
                                size_t* len) {
     if ((n > 0 && !blocks) || !len) return RIV_ERR_FRAME;

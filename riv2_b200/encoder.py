@@ -111,7 +111,7 @@ EXPORTED_SYMBOLS = (
     "riv_stage_rgb_to_yuv", "riv_stage_deblock", "riv_stage_libm", "riv_libm_fixup_counts", "riv_dct_tables",
     "riv_debug_frame_state", "riv_counters", "riv_host_times", "riv_stage_deblock_noalloc",
     "riv_decoder_new", "riv_decoder_info", "riv_decode_frame_yuv", "riv_decode_frame_rgb", "riv_decoder_current_frame",
-    "riv_decoder_last_error", "riv_decoder_free", "riv_test_dct_encode", "riv_test_worker_queue",
+    "riv_decoder_last_error", "riv_decoder_free", "riv_test_dct_encode", "riv_test_dct_decode", "riv_test_worker_queue",
 )
 
 
@@ -127,6 +127,7 @@ def lib() -> C.CDLL:
     L.riv_encode_frame_yuv.argtypes = [P, U8P, U8P, U8P, C.c_uint64, C.POINTER(RivFrameStats)]
     L.riv_finish.argtypes = [P]
     L.riv_test_dct_encode.argtypes = [P, C.c_uint32, C.c_int, C.c_uint32, P, C.c_size_t, C.POINTER(C.c_size_t)]
+    L.riv_test_dct_decode.argtypes = [P, C.c_size_t, P, C.c_uint32, C.c_int, P]
     L.riv_test_worker_queue.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_int, C.c_int, C.c_int, P,
                                         C.c_size_t, C.POINTER(C.c_size_t)]
     L.riv_encoder_free.argtypes = [P]
@@ -556,6 +557,16 @@ def dct_encode_host(blocks: np.ndarray, intra: bool, threads: int = 0) -> bytes:
     out = np.zeros(max(n.value, 1), np.uint8)
     lib().riv_test_dct_encode(b.ctypes.data, b.shape[0], int(intra), threads, out.ctypes.data, n.value, C.byref(n))
     return out[:n.value].tobytes()
+
+
+def dct_decode_host(data: bytes, coded: np.ndarray, intra: bool):
+    """The decoder's host DCT-coefficient decoder on one frame's stream (test hook, no GPU
+    needed): (dense (n, 384) int16 blocks, ok), ok False where the stream is malformed."""
+    c = np.ascontiguousarray(coded, dtype=np.uint8)
+    out = np.zeros((c.size, 384), np.int16)
+    buf = np.frombuffer(data, np.uint8) if len(data) else np.zeros(1, np.uint8)
+    st = lib().riv_test_dct_decode(buf.ctypes.data, len(data), c.ctypes.data, c.size, int(intra), out.ctypes.data)
+    return out, st == 0
 
 
 def worker_queue(bw: int, bh: int, w: int, defer: bool, deblock: bool, tables: bool, compact: bool) -> np.ndarray:

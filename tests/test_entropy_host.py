@@ -76,3 +76,41 @@ def test_magnitude_classes_13_and_14(threads):
         O.dct_encode(b, False)
     with pytest.raises(EncodingFailed):
         dct_encode_host(b, False, threads)
+
+
+@pytest.mark.parametrize("intra", [False, True])
+def test_dct_decoder_round_trip_and_oracle(intra):
+    """The decoder's host coefficient decoder (riv_entropy.cpp, behind riv_test_dct_decode)
+    inverts the coder, leaves the blocks outside the coded mask zero, and agrees with the
+    oracle's restatement of the reference decoder (res/rans.rs:340-459)."""
+    from riv2_b200.encoder import dct_encode_host, dct_decode_host
+    rng = np.random.default_rng(5)
+    n = 900
+    coded = (rng.random(n) < 0.7).astype(np.uint8)
+    b = _blocks(int(coded.sum()), 31, density=0.4, big=not intra)
+    data = dct_encode_host(b, intra, 0)
+    got, ok = dct_decode_host(data, coded, intra)
+    assert ok
+    assert np.array_equal(got[coded == 1], b) and not got[coded == 0].any()
+    ref, ref_ok = O.dct_decode(data, coded, intra)
+    assert ref_ok and np.array_equal(got, ref)
+
+
+def test_dct_decoder_class_13_and_malformed_streams_match_oracle():
+    """A class-13 magnitude is written with 13 continue bits but read back, as by the
+    reference decoder, as class 12: the rest of the frame decodes to the same wrong values on
+    both sides.  A truncated stream is malformed for both."""
+    from riv2_b200.encoder import dct_encode_host, dct_decode_host
+    b = _blocks(300, 41, density=0.3)
+    b[10, 5] = 5000
+    coded = np.ones(300, np.uint8)
+    data = dct_encode_host(b, False, 0)
+    got, ok = dct_decode_host(data, coded, False)
+    ref, ref_ok = O.dct_decode(data, coded, False)
+    assert ok == ref_ok
+    if ok:
+        assert np.array_equal(got, ref)
+    assert not np.array_equal(got, b)
+    short, short_ok = dct_decode_host(data[: len(data) // 3], coded, False)
+    _, short_ref_ok = O.dct_decode(data[: len(data) // 3], coded, False)
+    assert not short_ok and not short_ref_ok
