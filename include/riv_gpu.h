@@ -192,6 +192,18 @@ riv_status riv_test_dct_encode(const int16_t* blocks, uint32_t n, int intra, uin
  * malformed (read past its end, an EOB beyond the plane: the reference decoder panics). */
 riv_status riv_test_dct_decode(const uint8_t* data, size_t len, const uint8_t* coded, uint32_t n, int intra,
                                int16_t* out);
+/* Test hooks (host only, no reference counterpart): the MV coder over nframes frames with one
+ * coder (contexts and candidate history carry across frames, res/mv_rans/encoder.rs:60-412).
+ * Frame f has dims[2f] x dims[2f+1] blocks; a block is 7 bytes: mode (MvMode order: Zero,
+ * Nearest, Near, TopRight, TopLeft, New, Temporal), NEW base, dx (i8), dy (i8), subpel x,
+ * subpel y (Zero, PlusHalf, MinusHalf), skip.  Encode: *len = total size, frame_len[f] = each
+ * frame's size, up to cap bytes copied; RIV_ERR_ENCODING_FAILED on a NEW block with a raw
+ * -1/2 subpel (the reference panics).  Decode: the inverse with a fresh coder (decoder.rs);
+ * RIV_ERR_FRAME on malformed data. */
+riv_status riv_test_mv_encode(const uint8_t* blocks, const uint32_t* dims, uint32_t nframes, uint8_t* out, size_t cap,
+                              size_t* len, uint32_t* frame_len);
+riv_status riv_test_mv_decode(const uint8_t* data, const uint32_t* frame_len, const uint32_t* dims, uint32_t nframes,
+                              uint8_t* blocks);
 /* Test hook (host only, no reference counterpart): the worker-task queue of the fused search
  * launch for a frame of bw x bh MBs and w storage columns, in the order the kernel hands the
  * tasks out: 3 int32 per task (kind 0 residual pair / 1 deblock tile / 2 SAD-table MB / 3 scan

@@ -98,6 +98,9 @@ def lib():
         L.oracle_dct_encode.restype = C.c_size_t
         L.oracle_dct_encode.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t]
         L.oracle_dct_decode.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        L.oracle_mv_encode.restype = C.c_size_t
+        L.oracle_mv_encode.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]
+        L.oracle_mv_decode.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
         L.oracle_rans_roundtrip.restype = C.c_size_t
         L.oracle_rans_roundtrip.argtypes = [U8, U8, C.c_size_t, U8, U8, C.c_size_t]
         _lib = L
@@ -280,6 +283,39 @@ def dct_decode(data: bytes, coded: np.ndarray, intra: bool):
     buf = np.frombuffer(data, np.uint8) if len(data) else np.zeros(1, np.uint8)
     st = lib().oracle_dct_decode(buf.ctypes.data, len(data), c.ctypes.data, c.size, int(intra), out.ctypes.data)
     return out, st == 0
+
+
+def mv_encode(blocks: np.ndarray, dims) -> list:
+    """The oracle's MV coder over a sequence of frames, one coder throughout: blocks is
+    (total blocks, 7) uint8 (mode, NEW base, dx, dy, subpel x, subpel y, skip), dims the
+    (bw, bh) of each frame.  Returns each frame's bytes; raises ValueError where the reference
+    encoder panics (a NEW block with a raw -1/2 subpel)."""
+    b = np.ascontiguousarray(blocks, dtype=np.uint8)
+    d = np.ascontiguousarray(np.asarray(dims, dtype=np.uint32).reshape(-1))
+    nf = d.size // 2
+    fl = np.zeros(max(nf, 1), np.uint32)
+    total = lib().oracle_mv_encode(b.ctypes.data, d.ctypes.data, nf, None, 0, fl.ctypes.data)
+    if total == C.c_size_t(-1).value:
+        raise ValueError("raw -0.5 subpixel: the reference encoder panics")
+    out = np.zeros(max(total, 1), np.uint8)
+    lib().oracle_mv_encode(b.ctypes.data, d.ctypes.data, nf, out.ctypes.data, total, fl.ctypes.data)
+    frames, pos = [], 0
+    for f in range(nf):
+        frames.append(out[pos:pos + int(fl[f])].tobytes())
+        pos += int(fl[f])
+    return frames
+
+
+def mv_decode(frames: list, dims):
+    """Inverse of mv_encode with a fresh coder: ((total blocks, 7) uint8, ok)."""
+    d = np.ascontiguousarray(np.asarray(dims, dtype=np.uint32).reshape(-1))
+    nf = d.size // 2
+    fl = np.array([len(f) for f in frames] or [0], np.uint32)
+    data = np.frombuffer(b"".join(frames) or b"\0", np.uint8)
+    n = int(sum(int(d[2 * f]) * int(d[2 * f + 1]) for f in range(nf)))
+    out = np.zeros((max(n, 1), 7), np.uint8)
+    st = lib().oracle_mv_decode(data.ctypes.data, fl.ctypes.data, d.ctypes.data, nf, out.ctypes.data)
+    return out[:n], st == 0
 
 
 def rgb_to_yuv(rgb: np.ndarray, dw: int, dh: int, sw: int, sh: int) -> Frames:

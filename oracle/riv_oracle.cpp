@@ -2193,6 +2193,67 @@ int oracle_dct_decode(const uint8_t* d, size_t len, const uint8_t* coded, int n,
     return r.err ? 1 : 0;
 }
 
+// The MV coder over nframes frames with one coder (res/mv_rans/encoder.rs:60-412): frame f
+// has dims[2f] x dims[2f+1] blocks of 7 bytes (mode, NEW base, dx, dy, subpel x, subpel y,
+// skip).  Returns the total size (frame_len[f] per frame, up to cap bytes copied), SIZE_MAX
+// where the reference encoder panics: a NEW block with a raw -1/2 subpel reaches
+// encode_fractional (:335-336), no candidate ever holding one (:379-381).
+static Coded oracle_coded(const uint8_t* r) {
+    Coded b;
+    b.mode = r[0];
+    b.base = r[1];
+    b.dx = (int8_t)r[2];
+    b.dy = (int8_t)r[3];
+    b.spx = r[4];
+    b.spy = r[5];
+    b.skip = r[6] != 0;
+    return b;
+}
+size_t oracle_mv_encode(const uint8_t* blk, const uint32_t* dims, int nframes, uint8_t* out, size_t cap,
+                        uint32_t* frame_len) {
+    init_zero_prob();
+    MvCoder c;
+    Bytes all;
+    size_t k = 0;
+    for (int f = 0; f < nframes; f++) {
+        const size_t n = (size_t)dims[2 * f] * dims[2 * f + 1];
+        std::vector<Coded> v(n);
+        for (size_t i = 0; i < n; i++, k++) {
+            v[i] = oracle_coded(blk + 7 * k);
+            if (v[i].mode == NEW && (v[i].spx == SM || v[i].spy == SM)) return SIZE_MAX;
+        }
+        Bytes fb = c.encode_frame(v, (int)dims[2 * f]);
+        frame_len[f] = (uint32_t)fb.size();
+        all.insert(all.end(), fb.begin(), fb.end());
+    }
+    if (out && cap) memcpy(out, all.data(), std::min(cap, all.size()));
+    return all.size();
+}
+// Inverse of oracle_mv_encode with a fresh coder (res/mv_rans/decoder.rs:149-283); 1 where
+// the data is malformed.
+int oracle_mv_decode(const uint8_t* data, const uint32_t* frame_len, const uint32_t* dims, int nframes,
+                     uint8_t* blk) {
+    init_zero_prob();
+    MvCoder c;
+    std::vector<Coded> v;
+    size_t pos = 0, k = 0;
+    for (int f = 0; f < nframes; f++) {
+        if (!c.decode_frame(data + pos, frame_len[f], (int)dims[2 * f], (int)dims[2 * f + 1], v)) return 1;
+        pos += frame_len[f];
+        for (const Coded& b : v) {
+            uint8_t* r = blk + 7 * k++;
+            r[0] = (uint8_t)b.mode;
+            r[1] = (uint8_t)b.base;
+            r[2] = (uint8_t)b.dx;
+            r[3] = (uint8_t)b.dy;
+            r[4] = (uint8_t)b.spx;
+            r[5] = (uint8_t)b.spy;
+            r[6] = b.skip ? 1 : 0;
+        }
+    }
+    return 0;
+}
+
 // Returns SIZE_MAX where the reference encoder panics (a magnitude class above 13).
 size_t oracle_dct_encode(const int16_t* blocks, int n, int intra, uint8_t* stream, size_t cap) {  // res/rans.rs:195-330
     init_zero_prob();

@@ -99,6 +99,7 @@ struct MvCodedBlock {  // res/mv_rans.rs:65-78
 class MvCoder {  // res/mv_rans/encoder.rs:60-412
 public:
     void reset();
+    // Throws std::runtime_error on a NEW block with a raw -1/2 subpel (the reference panics).
     void encode_frame(const std::vector<MvCodedBlock>& blocks, int bw, std::vector<uint8_t>& out);
     // res/mv_rans/decoder.rs:149-283; the same context and candidate-history state as the
     // encoder, so a decoder instance follows the encoder's across frames.  false on bad data.

@@ -1507,6 +1507,68 @@ riv_status riv_test_worker_queue(uint32_t bw, uint32_t bh, uint32_t w, int defer
     return i == (size_t)queue_total(q) ? RIV_OK : RIV_ERR_ENCODING_FAILED;
 }
 
+static riv::MvCodedBlock mv_block_from(const uint8_t* r) {
+    riv::MvCodedBlock b;
+    b.mode = r[0];
+    b.new_base = r[1];
+    b.dx = (int8_t)r[2];
+    b.dy = (int8_t)r[3];
+    b.spx = r[4];
+    b.spy = r[5];
+    b.skip = r[6] != 0;
+    return b;
+}
+
+riv_status riv_test_mv_encode(const uint8_t* blocks, const uint32_t* dims, uint32_t nframes, uint8_t* out, size_t cap,
+                              size_t* len, uint32_t* frame_len) {
+    if (!len || (nframes > 0 && (!blocks || !dims || !frame_len))) return RIV_ERR_FRAME;
+    entropy_init();
+    riv::MvCoder coder;
+    std::vector<uint8_t> all, fb;
+    size_t k = 0;
+    try {
+        for (uint32_t f = 0; f < nframes; f++) {
+            const size_t n = (size_t)dims[2 * f] * dims[2 * f + 1];
+            std::vector<riv::MvCodedBlock> v(n);
+            for (size_t i = 0; i < n; i++, k++) v[i] = mv_block_from(blocks + 7 * k);
+            coder.encode_frame(v, (int)dims[2 * f], fb);
+            frame_len[f] = (uint32_t)fb.size();
+            all.insert(all.end(), fb.begin(), fb.end());
+        }
+    } catch (const std::exception&) {
+        return RIV_ERR_ENCODING_FAILED;
+    }
+    *len = all.size();
+    if (out && cap) memcpy(out, all.data(), std::min(cap, all.size()));
+    return RIV_OK;
+}
+
+riv_status riv_test_mv_decode(const uint8_t* data, const uint32_t* frame_len, const uint32_t* dims, uint32_t nframes,
+                              uint8_t* blocks) {
+    if (nframes > 0 && (!frame_len || !dims || !blocks)) return RIV_ERR_FRAME;
+    entropy_init();
+    riv::MvCoder coder;
+    std::vector<riv::MvCodedBlock> v;
+    size_t pos = 0, k = 0;
+    for (uint32_t f = 0; f < nframes; f++) {
+        if (frame_len[f] > 0 && !data) return RIV_ERR_FRAME;
+        if (!coder.decode_frame(data + pos, frame_len[f], (int)dims[2 * f], (int)dims[2 * f + 1], v))
+            return RIV_ERR_FRAME;
+        pos += frame_len[f];
+        for (const riv::MvCodedBlock& b : v) {
+            uint8_t* r = blocks + 7 * k++;
+            r[0] = b.mode;
+            r[1] = b.new_base;
+            r[2] = (uint8_t)b.dx;
+            r[3] = (uint8_t)b.dy;
+            r[4] = b.spx;
+            r[5] = b.spy;
+            r[6] = b.skip ? 1 : 0;
+        }
+    }
+    return RIV_OK;
+}
+
 riv_status riv_test_dct_decode(const uint8_t* data, size_t len, const uint8_t* coded, uint32_t n, int intra,
                                int16_t* out) {
     if ((len > 0 && !data) || (n > 0 && (!coded || !out))) return RIV_ERR_FRAME;

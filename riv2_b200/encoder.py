@@ -111,7 +111,8 @@ EXPORTED_SYMBOLS = (
     "riv_stage_rgb_to_yuv", "riv_stage_deblock", "riv_stage_libm", "riv_libm_fixup_counts", "riv_dct_tables",
     "riv_debug_frame_state", "riv_counters", "riv_host_times", "riv_stage_deblock_noalloc",
     "riv_decoder_new", "riv_decoder_info", "riv_decode_frame_yuv", "riv_decode_frame_rgb", "riv_decoder_current_frame",
-    "riv_decoder_last_error", "riv_decoder_free", "riv_test_dct_encode", "riv_test_dct_decode", "riv_test_worker_queue",
+    "riv_decoder_last_error", "riv_decoder_free", "riv_test_dct_encode", "riv_test_dct_decode", "riv_test_mv_encode",
+    "riv_test_mv_decode", "riv_test_worker_queue",
 )
 
 
@@ -128,6 +129,8 @@ def lib() -> C.CDLL:
     L.riv_finish.argtypes = [P]
     L.riv_test_dct_encode.argtypes = [P, C.c_uint32, C.c_int, C.c_uint32, P, C.c_size_t, C.POINTER(C.c_size_t)]
     L.riv_test_dct_decode.argtypes = [P, C.c_size_t, P, C.c_uint32, C.c_int, P]
+    L.riv_test_mv_encode.argtypes = [P, P, C.c_uint32, P, C.c_size_t, C.POINTER(C.c_size_t), P]
+    L.riv_test_mv_decode.argtypes = [P, P, P, C.c_uint32, P]
     L.riv_test_worker_queue.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_int, C.c_int, C.c_int, P,
                                         C.c_size_t, C.POINTER(C.c_size_t)]
     L.riv_encoder_free.argtypes = [P]
@@ -567,6 +570,41 @@ def dct_decode_host(data: bytes, coded: np.ndarray, intra: bool):
     buf = np.frombuffer(data, np.uint8) if len(data) else np.zeros(1, np.uint8)
     st = lib().riv_test_dct_decode(buf.ctypes.data, len(data), c.ctypes.data, c.size, int(intra), out.ctypes.data)
     return out, st == 0
+
+
+def mv_encode_host(blocks: np.ndarray, dims) -> list:
+    """The encoder's host MV coder over a sequence of frames, one coder throughout (test hook,
+    no GPU needed): blocks is (total blocks, 7) uint8 (mode, NEW base, dx, dy, subpel x,
+    subpel y, skip), dims the (bw, bh) of each frame.  Returns each frame's bytes; raises
+    EncodingFailed where the reference encoder panics (a NEW block with a raw -1/2 subpel)."""
+    b = np.ascontiguousarray(blocks, dtype=np.uint8)
+    d = np.ascontiguousarray(np.asarray(dims, dtype=np.uint32).reshape(-1))
+    nf = d.size // 2
+    fl = np.zeros(max(nf, 1), np.uint32)
+    n = C.c_size_t(0)
+    st = lib().riv_test_mv_encode(b.ctypes.data, d.ctypes.data, nf, None, 0, C.byref(n), fl.ctypes.data)
+    if st != 0:
+        raise _ERRORS.get(st, EncodeError)(f"riv_test_mv_encode failed (status {st})")
+    out = np.zeros(max(n.value, 1), np.uint8)
+    lib().riv_test_mv_encode(b.ctypes.data, d.ctypes.data, nf, out.ctypes.data, n.value, C.byref(n), fl.ctypes.data)
+    frames, pos = [], 0
+    for f in range(nf):
+        frames.append(out[pos:pos + int(fl[f])].tobytes())
+        pos += int(fl[f])
+    return frames
+
+
+def mv_decode_host(frames: list, dims):
+    """The decoder's host MV decoder over a sequence of frames with a fresh coder (test hook):
+    ((total blocks, 7) uint8, ok), ok False on malformed data."""
+    d = np.ascontiguousarray(np.asarray(dims, dtype=np.uint32).reshape(-1))
+    nf = d.size // 2
+    fl = np.array([len(f) for f in frames] or [0], np.uint32)
+    data = np.frombuffer(b"".join(frames) or b"\0", np.uint8)
+    n = int(sum(int(d[2 * f]) * int(d[2 * f + 1]) for f in range(nf)))
+    out = np.zeros((max(n, 1), 7), np.uint8)
+    st = lib().riv_test_mv_decode(data.ctypes.data, fl.ctypes.data, d.ctypes.data, nf, out.ctypes.data)
+    return out[:n], st == 0
 
 
 def worker_queue(bw: int, bh: int, w: int, defer: bool, deblock: bool, tables: bool, compact: bool) -> np.ndarray:

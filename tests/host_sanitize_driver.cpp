@@ -2,7 +2,8 @@
 // tests/test_host_sanitizers.py with -fsanitize=address,undefined and with -fsanitize=thread).
 // On seeded random coefficient frames it checks that the coefficient coder gives the same
 // bytes inline, with its full rANS batches on a pool, and in its parallel form; that the
-// decoder inverts it; and that a magnitude class above 13 fails in every form.
+// decoder inverts it; that a magnitude class above 13 fails in every form; and that the MV
+// decoder inverts the MV coder over frames with a candidate history.
 #include <cmath>
 #include <condition_variable>
 #include <cstdio>
@@ -153,6 +154,39 @@ int main(int argc, char** argv) {
             threw = true;
         }
         if (!threw) return fail("magnitude class 14 did not fail", form);
+    }
+    // the MV coder: frames of every mode with a candidate history, encoded by one coder and
+    // decoded by another that follows it
+    {
+        riv::MvCoder enc, dec;
+        std::uniform_int_distribution<int> mode(0, 6), base(0, 4), delta(-128, 127), sub(0, 1), few(0, 3);
+        std::bernoulli_distribution coin(0.5);
+        const int bw = 24, bh = 16;
+        for (int f = 0; f < 30; f++) {
+            std::vector<riv::MvCodedBlock> v((size_t)bw * bh), back;
+            for (riv::MvCodedBlock& b : v) {
+                b = riv::MvCodedBlock{};
+                b.mode = (uint8_t)mode(rng);
+                b.skip = coin(rng);
+                if (b.mode == riv::M_NEW) {
+                    static const int8_t common[4] = {-3, 0, 2, 5};
+                    b.new_base = (uint8_t)base(rng);
+                    b.dx = coin(rng) ? common[few(rng)] : (int8_t)delta(rng);
+                    b.dy = coin(rng) ? common[few(rng)] : (int8_t)delta(rng);
+                    b.spx = (uint8_t)sub(rng);
+                    b.spy = (uint8_t)sub(rng);
+                }
+            }
+            std::vector<uint8_t> bytes;
+            enc.encode_frame(v, bw, bytes);
+            if (!dec.decode_frame(bytes.data(), bytes.size(), bw, bh, back)) return fail("MV decoder: malformed", f);
+            for (size_t i = 0; i < v.size(); i++) {
+                const riv::MvCodedBlock &a = v[i], &c = back[i];
+                if (a.mode != c.mode || a.new_base != c.new_base || a.dx != c.dx || a.dy != c.dy || a.spx != c.spx ||
+                    a.spy != c.spy || a.skip != c.skip)
+                    return fail("MV decoder does not invert the coder", f);
+            }
+        }
     }
     std::printf("host entropy sanitizer driver: ok\n");
     return 0;
