@@ -192,6 +192,9 @@ riv_status riv_test_dct_encode(const int16_t* blocks, uint32_t n, int intra, uin
  * malformed (read past its end, an EOB beyond the plane: the reference decoder panics). */
 riv_status riv_test_dct_decode(const uint8_t* data, size_t len, const uint8_t* coded, uint32_t n, int intra,
                                int16_t* out);
+/* Test hook (host only, no reference counterpart): the NEW-delta bias the encoder writes in
+ * each P-frame record (compute_delta_bias_for_new, enc/encoder.rs:984-1048) over n raw deltas. */
+riv_status riv_test_delta_bias(const int8_t* dx, const int8_t* dy, uint32_t n, int8_t* bx, int8_t* by);
 /* Test hooks (host only, no reference counterpart): the MV coder over nframes frames with one
  * coder (contexts and candidate history carry across frames, res/mv_rans/encoder.rs:60-412).
  * Frame f has dims[2f] x dims[2f+1] blocks; a block is 7 bytes: mode (MvMode order: Zero,

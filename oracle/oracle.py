@@ -98,6 +98,7 @@ def lib():
         L.oracle_dct_encode.restype = C.c_size_t
         L.oracle_dct_encode.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t]
         L.oracle_dct_decode.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        L.oracle_delta_bias.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
         L.oracle_mv_encode.restype = C.c_size_t
         L.oracle_mv_encode.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]
         L.oracle_mv_decode.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
@@ -283,6 +284,15 @@ def dct_decode(data: bytes, coded: np.ndarray, intra: bool):
     buf = np.frombuffer(data, np.uint8) if len(data) else np.zeros(1, np.uint8)
     st = lib().oracle_dct_decode(buf.ctypes.data, len(data), c.ctypes.data, c.size, int(intra), out.ctypes.data)
     return out, st == 0
+
+
+def delta_bias(dx: np.ndarray, dy: np.ndarray):
+    """The oracle's compute_delta_bias_for_new over NEW-block raw deltas: (bias x, bias y)."""
+    x = np.ascontiguousarray(dx, dtype=np.int8)
+    y = np.ascontiguousarray(dy, dtype=np.int8)
+    bx, by = C.c_int8(0), C.c_int8(0)
+    lib().oracle_delta_bias(x.ctypes.data, y.ctypes.data, x.size, C.byref(bx), C.byref(by))
+    return bx.value, by.value
 
 
 def mv_encode(blocks: np.ndarray, dims) -> list:

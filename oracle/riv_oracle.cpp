@@ -2254,6 +2254,13 @@ int oracle_mv_decode(const uint8_t* data, const uint32_t* frame_len, const uint3
     return 0;
 }
 
+// compute_delta_bias_for_new (enc/encoder.rs:984-1048) over n NEW-block raw deltas.
+void oracle_delta_bias(const int8_t* dx, const int8_t* dy, uint32_t n, int8_t* bx, int8_t* by) {
+    std::vector<std::pair<int8_t, int8_t>> d(n);
+    for (uint32_t i = 0; i < n; i++) d[i] = {dx[i], dy[i]};
+    compute_bias(d, *bx, *by);
+}
+
 // Returns SIZE_MAX where the reference encoder panics (a magnitude class above 13).
 size_t oracle_dct_encode(const int16_t* blocks, int n, int intra, uint8_t* stream, size_t cap) {  // res/rans.rs:195-330
     init_zero_prob();

@@ -1507,6 +1507,14 @@ riv_status riv_test_worker_queue(uint32_t bw, uint32_t bh, uint32_t w, int defer
     return i == (size_t)queue_total(q) ? RIV_OK : RIV_ERR_ENCODING_FAILED;
 }
 
+riv_status riv_test_delta_bias(const int8_t* dx, const int8_t* dy, uint32_t n, int8_t* bx, int8_t* by) {
+    if (!bx || !by || (n > 0 && (!dx || !dy))) return RIV_ERR_FRAME;
+    std::vector<std::pair<int8_t, int8_t>> d(n);
+    for (uint32_t i = 0; i < n; i++) d[i] = {dx[i], dy[i]};
+    riv::compute_delta_bias(d, *bx, *by);
+    return RIV_OK;
+}
+
 static riv::MvCodedBlock mv_block_from(const uint8_t* r) {
     riv::MvCodedBlock b;
     b.mode = r[0];

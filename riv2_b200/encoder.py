@@ -112,7 +112,7 @@ EXPORTED_SYMBOLS = (
     "riv_debug_frame_state", "riv_counters", "riv_host_times", "riv_stage_deblock_noalloc",
     "riv_decoder_new", "riv_decoder_info", "riv_decode_frame_yuv", "riv_decode_frame_rgb", "riv_decoder_current_frame",
     "riv_decoder_last_error", "riv_decoder_free", "riv_test_dct_encode", "riv_test_dct_decode", "riv_test_mv_encode",
-    "riv_test_mv_decode", "riv_test_worker_queue",
+    "riv_test_mv_decode", "riv_test_delta_bias", "riv_test_worker_queue",
 )
 
 
@@ -131,6 +131,7 @@ def lib() -> C.CDLL:
     L.riv_test_dct_decode.argtypes = [P, C.c_size_t, P, C.c_uint32, C.c_int, P]
     L.riv_test_mv_encode.argtypes = [P, P, C.c_uint32, P, C.c_size_t, C.POINTER(C.c_size_t), P]
     L.riv_test_mv_decode.argtypes = [P, P, P, C.c_uint32, P]
+    L.riv_test_delta_bias.argtypes = [P, P, C.c_uint32, P, P]
     L.riv_test_worker_queue.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_int, C.c_int, C.c_int, P,
                                         C.c_size_t, C.POINTER(C.c_size_t)]
     L.riv_encoder_free.argtypes = [P]
@@ -570,6 +571,16 @@ def dct_decode_host(data: bytes, coded: np.ndarray, intra: bool):
     buf = np.frombuffer(data, np.uint8) if len(data) else np.zeros(1, np.uint8)
     st = lib().riv_test_dct_decode(buf.ctypes.data, len(data), c.ctypes.data, c.size, int(intra), out.ctypes.data)
     return out, st == 0
+
+
+def delta_bias_host(dx: np.ndarray, dy: np.ndarray):
+    """The encoder's NEW-delta bias over raw deltas (test hook, no GPU needed): (bias x, bias y)."""
+    x = np.ascontiguousarray(dx, dtype=np.int8)
+    y = np.ascontiguousarray(dy, dtype=np.int8)
+    bx, by = C.c_int8(0), C.c_int8(0)
+    if lib().riv_test_delta_bias(x.ctypes.data, y.ctypes.data, x.size, C.byref(bx), C.byref(by)) != 0:
+        raise EncodingFailed("riv_test_delta_bias failed")
+    return bx.value, by.value
 
 
 def mv_encode_host(blocks: np.ndarray, dims) -> list:

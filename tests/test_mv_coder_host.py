@@ -118,3 +118,24 @@ def test_truncated_mv_stream_is_malformed_for_both():
     short = [got[0][: len(got[0]) // 4]]
     assert not mv_decode_host(short, [(40, 30)])[1]
     assert not O.mv_decode(short, [(40, 30)])[1]
+
+
+@pytest.mark.parametrize("case", ["empty", "random", "clustered", "extremes"])
+def test_delta_bias_matches_oracle(case):
+    """The encoder's NEW-delta bias (compute_delta_bias_for_new, enc/encoder.rs:984-1048) is
+    computed from per-axis histograms; the oracle restates the reference's loop over the
+    deltas.  Same bias on both axes, including the -128 wrap of i8::abs and the clamp."""
+    from riv2_b200.encoder import delta_bias_host
+    rng = np.random.default_rng(11)
+    if case == "empty":
+        dx = dy = np.zeros(0, np.int8)
+    elif case == "random":
+        dx, dy = rng.integers(-128, 128, 5000), rng.integers(-128, 128, 5000)
+    elif case == "clustered":
+        dx = np.clip(np.round(rng.normal(7, 3, 8160)), -128, 127)
+        dy = np.clip(np.round(rng.normal(-19, 5, 8160)), -128, 127)
+    else:
+        dx = rng.choice([-128, -127, -105, 104, 127, 0], 3000)
+        dy = rng.choice([-128, 127, -24, 24, 1], 3000)
+    dx, dy = np.asarray(dx, np.int8), np.asarray(dy, np.int8)
+    assert delta_bias_host(dx, dy) == O.delta_bias(dx, dy)
