@@ -338,6 +338,7 @@ struct riv_encoder {
     riv_writer_vtable wr;
     std::string err;
     bool poisoned = false;
+    std::string poison_msg;  // the failure that made the encoder unusable
     uint64_t header_pos = 0, frame_count = 0, submitted = 0;
     int W = 0, H = 0, BW = 0, BH = 0, NMB = 0;
     size_t yuv_bytes = 0;
@@ -404,8 +405,23 @@ namespace {
 
 static riv_status fail(riv_encoder* e, riv_status s, const std::string& msg) {
     e->err = msg;
-    if (s == RIV_ERR_CUDA || s == RIV_ERR_DEVICE_TIMEOUT) e->poisoned = true;
+    if (s == RIV_ERR_CUDA || s == RIV_ERR_DEVICE_TIMEOUT) {
+        e->poisoned = true;
+        e->poison_msg = msg;
+    }
     return s;
+}
+// A failure that leaves the pipeline unusable (a device failure, or an exception from a
+// coder where the reference panics): later calls report it instead of running on.
+static riv_status fail_poison(riv_encoder* e, riv_status s, const std::string& msg) {
+    e->poisoned = true;
+    e->poison_msg = msg;
+    e->err = msg;
+    return s;
+}
+static riv_status poisoned_status(riv_encoder* e) {
+    e->err = "encoder unusable after an earlier failure: " + e->poison_msg;
+    return RIV_ERR_ENCODING_FAILED;
 }
 
 static riv_status validate(const riv_config& c, std::string& msg) {  // enc/config.rs:129-164
@@ -1046,6 +1062,9 @@ static riv_status pump(riv_encoder* e, bool block_front) {
                        f.fut_mv.wait_for(std::chrono::seconds(0)) != std::future_status::ready))
             break;
         riv_status st = write_job(e, f);
+        // a record the writer refused is lost and not counted, as when the reference's
+        // write fails (enc/encoder.rs:248-253); later frames go on
+        if (st == RIV_ERR_IO) e->jobs.pop_front();
         if (st) return st;
         e->jobs.pop_front();
         block = false;
@@ -1069,7 +1088,7 @@ static riv_status drain_all(riv_encoder* e) {
 
 static riv_status encode_common(riv_encoder* e, int src, const void* a, const void* b, const void* c3,
                                 uint64_t ts, riv_frame_stats* stats) {
-    if (e->poisoned) return fail(e, RIV_ERR_ENCODING_FAILED, "encoder unusable after an earlier device failure: " + e->err);
+    if (e->poisoned) return poisoned_status(e);
     try {
         CK(cudaSetDevice(e->cfg.device));
         size_t cap = e->slots.size();
@@ -1108,7 +1127,7 @@ static riv_status encode_common(riv_encoder* e, int src, const void* a, const vo
     } catch (const CudaError& ce) {
         return fail(e, RIV_ERR_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
     } catch (const std::exception& ex) {
-        return fail(e, RIV_ERR_ENCODING_FAILED, ex.what());
+        return fail_poison(e, RIV_ERR_ENCODING_FAILED, ex.what());
     }
     return RIV_OK;
 }
@@ -1209,12 +1228,15 @@ riv_status riv_encode_frame_yuv(riv_encoder* e, const uint8_t* y, const uint8_t*
 
 riv_status riv_finish(riv_encoder* e) {  // enc/encoder.rs:950-961
     if (!e) return RIV_ERR_INVALID_CONFIG;
+    if (e->poisoned) return poisoned_status(e);
     try {
         CK(cudaSetDevice(e->cfg.device));
         riv_status st = drain_all(e);
         if (st) return st;
     } catch (const CudaError& ce) {
         return fail(e, RIV_ERR_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
+    } catch (const std::exception& ex) {
+        return fail_poison(e, RIV_ERR_ENCODING_FAILED, ex.what());
     }
     uint64_t end = e->wr.position(e->wr.user);
     if (e->wr.seek(e->wr.user, e->header_pos) != 0) return fail(e, RIV_ERR_IO, "writer.seek failed");
@@ -1289,6 +1311,8 @@ riv_status riv_last_recon(riv_encoder* e, uint8_t* y, uint8_t* u, uint8_t* v) {
         CK(cudaMemcpy(v, d + ys + cs, cs, cudaMemcpyDeviceToHost));
     } catch (const CudaError& ce) {
         return fail(e, RIV_ERR_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
+    } catch (const std::exception& ex) {
+        return fail_poison(e, RIV_ERR_ENCODING_FAILED, ex.what());
     }
     return RIV_OK;
 }
@@ -1316,6 +1340,8 @@ riv_status riv_debug_frame_state(riv_encoder* e, int what, void* out, size_t siz
         CK(cudaMemcpy(out, b->p, b->n, cudaMemcpyDeviceToHost));
     } catch (const CudaError& ce) {
         return fail(e, RIV_ERR_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
+    } catch (const std::exception& ex) {
+        return fail_poison(e, RIV_ERR_ENCODING_FAILED, ex.what());
     }
     return RIV_OK;
 }
@@ -1870,6 +1896,9 @@ riv_dec_status riv_decoder_new(const uint8_t* data, size_t len, int device, riv_
         d->err = std::string(ce.where) + ": " + cudaGetErrorString(ce.e);
         riv_decoder_free(d);
         return RIV_DEC_CUDA;
+    } catch (const std::exception&) {  // host allocation failures
+        riv_decoder_free(d);
+        return RIV_DEC_DECODING_FAILED;
     }
     riv::entropy_init();
     const unsigned hw = std::thread::hardware_concurrency();
@@ -1969,6 +1998,8 @@ static riv_dec_status dec_frame(riv_decoder* d, uint8_t* y, uint8_t* u, uint8_t*
         CK(cudaStreamSynchronize(S));
     } catch (const CudaError& ce) {
         return dec_fail(d, RIV_DEC_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
+    } catch (const std::exception& ex) {
+        return dec_fail(d, RIV_DEC_DECODING_FAILED, ex.what());
     }
     sl.filled = false;
     d->ref_cur = nxt;
