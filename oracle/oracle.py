@@ -304,6 +304,8 @@ def mv_encode(blocks: np.ndarray, dims) -> list:
     d = np.ascontiguousarray(np.asarray(dims, dtype=np.uint32).reshape(-1))
     nf = d.size // 2
     fl = np.zeros(max(nf, 1), np.uint32)
+    if b.ndim != 2 or b.shape[1] != 7 or b.shape[0] != int(sum(int(d[2 * f]) * int(d[2 * f + 1]) for f in range(nf))):
+        raise ValueError("blocks must be (sum of bw * bh over the frames, 7)")
     total = lib().oracle_mv_encode(b.ctypes.data, d.ctypes.data, nf, None, 0, fl.ctypes.data)
     if total == C.c_size_t(-1).value:
         raise ValueError("raw -0.5 subpixel: the reference encoder panics")

@@ -592,6 +592,8 @@ def mv_encode_host(blocks: np.ndarray, dims) -> list:
     d = np.ascontiguousarray(np.asarray(dims, dtype=np.uint32).reshape(-1))
     nf = d.size // 2
     fl = np.zeros(max(nf, 1), np.uint32)
+    if b.ndim != 2 or b.shape[1] != 7 or b.shape[0] != int(sum(int(d[2 * f]) * int(d[2 * f + 1]) for f in range(nf))):
+        raise ValueError("blocks must be (sum of bw * bh over the frames, 7)")
     n = C.c_size_t(0)
     st = lib().riv_test_mv_encode(b.ctypes.data, d.ctypes.data, nf, None, 0, C.byref(n), fl.ctypes.data)
     if st != 0:
