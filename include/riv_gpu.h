@@ -3,8 +3,8 @@
  *
  * Each declaration names the reference interface it replaces (paths relative to the
  * reference project root; enc/ = reitero_video/reitero_encode/src/).  A Rust caller
- * binds these through an `extern "C"` block; Python binds them
- * with ctypes (riv2_b200/encoder.py).  No CUDA or torch types appear here: buffers
+ * binds these through an `extern "C"` block; Python binds them with ctypes
+ * (riv2_b200/encoder.py).  No CUDA or torch types appear here: buffers
  * are plain pointers and sizes.
  *
  * Threading: one encoder per host thread.  riv_encode_frame may keep up to
@@ -153,8 +153,10 @@ riv_status riv_stage_deblock(uint8_t* yuv, uint32_t w, uint32_t h, int level, in
  * RIV_DEBLOCK_NOALLOC_MAX_BYTES (4 MiB: storage sizes up to 1920x1088); larger requests
  * return RIV_ERR_FRAME and write the reason to errbuf (nullable, errbuf_len bytes).
  * Set-up: the first call on a device looks up the scratch address
- * (cudaGetSymbolAddress, device current); make that first call before any stream
- * capture on that device.
+ * (cudaGetSymbolAddress, device current) and keeps it for the life of the process; make
+ * that first call before any stream capture on that device.  The kept address belongs to
+ * the device's primary context: after cudaDeviceReset, or with another context current,
+ * it is stale, so do not call this entry point after either.
  * Zero state: nothing in the scratch has to start at zero; each call writes every byte
  * it reads.
  * Calls that overlap on one device (from several host threads) share the scratch and
@@ -162,6 +164,22 @@ riv_status riv_stage_deblock(uint8_t* yuv, uint32_t w, uint32_t h, int level, in
 #define RIV_DEBLOCK_NOALLOC_MAX_BYTES (4u << 20)
 riv_status riv_stage_deblock_noalloc(uint8_t* yuv, uint32_t w, uint32_t h, int level, int intra,
                                      const uint8_t* mask, char* errbuf, size_t errbuf_len);
+/* build_predicted (com/fast_motion.rs:103-352) and compute_aq_quant_steps
+ * (res/residual.rs:116-167): the motion-compensated prediction of storage-size planes
+ * ref_yuv (Y, U, V contiguous) for one MV per MB (mv4: dx, dy, sx, sy as i8, raster order),
+ * then the per-MB AQ steps (qs, nullable) from the prediction's luma with the base step of
+ * `quality` (quant_step_from_quality, res/residual.rs:13-23). */
+riv_status riv_stage_predict(const uint8_t* ref_yuv, const int8_t* mv4, uint32_t w, uint32_t h, uint8_t quality,
+                             uint8_t* pred_yuv, float* qs);
+/* The residual part of ResidualEncoder::encode_inter (res/residual.rs:520-752): current minus
+ * prediction, 16x16 / 8x8 FDCT, dead-zone quantisation with the per-MB steps qs, optimized
+ * skip of all-zero MBs, dequantisation, inverse transforms and the pre-deblock
+ * reconstruction.  rdo_skip: one byte per MB (RDO-skipped MBs keep the prediction);
+ * coded4 (nullable): coded MVs, for the deblock mask (fmask, nullable: 1 where the MB is
+ * coded or its MV is not zero).  coeffs: 384 i16 per MB (Y 16x16, U 8x8, V 8x8, row-major). */
+riv_status riv_stage_residual(const uint8_t* cur_yuv, const uint8_t* pred_yuv, const float* qs, const uint8_t* rdo_skip,
+                              const int8_t* coded4, float dead_zone, uint32_t w, uint32_t h, int16_t* coeffs,
+                              uint8_t* opt_skip, uint8_t* recon_yuv, uint8_t* fmask);
 /* glibc-exact logf (which=0) / exp2f (which=1) on the device over n inputs. */
 riv_status riv_stage_libm(int which, const float* in, float* out, size_t n);
 /* Test hook: device state left by the most recent frame (synchronises the device; meant
@@ -173,6 +191,19 @@ riv_status riv_stage_libm(int which, const float* in, float* out, size_t n);
  * the encoder was created with RIV_PROFILE_SEARCH set in the environment).
  * Returns RIV_ERR_FRAME if `size` is short. */
 riv_status riv_debug_frame_state(riv_encoder* enc, int what, void* out, size_t size);
+/* Test hook (no reference counterpart): the device logf (which=0), exp2f (which=1) and the
+ * four-wide batched logf of the AQ warps (which=2) on every f32 whose bit pattern lies in
+ * [lo_bits, hi_bits], compared bit for bit with the host's glibc logf / exp2f (the functions
+ * f32::ln / f32::exp2 call on linux-gnu, res/residual.rs:116-167).  *mismatches = number of
+ * inputs that differ, *first_bad_bits = the smallest such bit pattern (0 if none). */
+riv_status riv_test_libm_range(int which, uint32_t lo_bits, uint32_t hi_bits, uint64_t* mismatches,
+                               uint32_t* first_bad_bits);
+/* Test hook (no reference counterpart): runs the bounded device waits of the search launch
+ * on flags nothing sets (which: 0 wavefront record, 1 worker-queue counter, 2 search -> mode
+ * hand-off slot, 3 mbarrier phase) with a spin limit of spin_limit polls (1 .. 2^20).  The
+ * waits give up, the kernel returns, and the status word (*status_word) carries the same
+ * timeout bit the encoder maps to RIV_ERR_DEVICE_TIMEOUT, which this call returns. */
+riv_status riv_test_wait_expiry(int which, int64_t spin_limit, uint32_t* status_word);
 /* Number of glibc fix-up entries loaded for logf / exp2f. */
 riv_status riv_libm_fixup_counts(uint32_t* nlog, uint32_t* nexp);
 /* The DCT bases the device uses (T16[i][j], T8[i][j]: sample i, frequency j). */
@@ -241,13 +272,13 @@ riv_dec_status riv_decoder_info(const riv_decoder* dec, uint32_t* dims5, uint64_
  * MVs are decoded in order on the calling thread and their coefficient streams on a pool of
  * host threads; a record that cannot be read is reported by the call for that frame (the
  * frames before it decode normally). */
+riv_dec_status riv_decode_frame_yuv(riv_decoder* dec, uint8_t* y, uint8_t* u, uint8_t* v, uint32_t* frame_type,
+                                    uint64_t* timestamp_ms);
 /* Decoder::decode_frame's RGB output (dec/decoder.rs:445-456): the frame as display-size RGB24
  * (rgb: display w x h x 3 bytes, nullable), converted on the GPU (BT.709 limited range, this
  * library's definition: the reference uses the `yuv` crate, so byte parity with it is not
  * established).  Same read-ahead and error behaviour as riv_decode_frame_yuv. */
 riv_dec_status riv_decode_frame_rgb(riv_decoder* dec, uint8_t* rgb, uint32_t* frame_type, uint64_t* timestamp_ms);
-riv_dec_status riv_decode_frame_yuv(riv_decoder* dec, uint8_t* y, uint8_t* u, uint8_t* v, uint32_t* frame_type,
-                                    uint64_t* timestamp_ms);
 /* Decoder::current_frame (dec/decoder.rs:475-478). */
 uint64_t riv_decoder_current_frame(const riv_decoder* dec);
 const char* riv_decoder_last_error(const riv_decoder* dec);

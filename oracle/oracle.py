@@ -87,6 +87,7 @@ def lib():
             getattr(L, n).argtypes = [U8, U8, C.c_uint32, C.c_uint32, C.c_int, C.c_int, C.c_int, C.c_int,
                                       C.c_int64, C.c_int]
         L.oracle_aq_steps.argtypes = [U8, C.c_uint32, C.c_uint32, C.c_float, F32]
+        L.oracle_residual_inter.argtypes = [U8, U8, C.c_uint32, C.c_uint32, U8, F32, C.c_float, I16, U8, U8]
         L.oracle_rdo_lambda.restype = C.c_double
         L.oracle_rdo_lambda.argtypes = [C.c_uint8, C.c_double]
         for n in ("oracle_fdct16_quant", "oracle_fdct8_quant"):
@@ -351,3 +352,23 @@ def build_predicted(prev: Frames, mvs4: np.ndarray, reference: bool = False) -> 
     fn = lib().oracle_reference_build_predicted if reference else lib().oracle_build_predicted
     fn(*prev.ptrs(), prev.w, prev.h, i8(m), *o.ptrs())
     return o
+
+
+def aq_steps(pred_y: np.ndarray, w: int, h: int, base: float) -> np.ndarray:
+    """compute_aq_quant_steps (res/residual.rs:116-167) on a luma prediction plane."""
+    out = np.zeros((w // 16) * (h // 16), np.float32)
+    lib().oracle_aq_steps(u8(np.ascontiguousarray(pred_y, dtype=np.uint8)), w, h, base, _p(out, C.c_float))
+    return out
+
+
+def residual_inter(cur: np.ndarray, pred: np.ndarray, w: int, h: int, skip: np.ndarray, qs: np.ndarray, dz: float):
+    """encode_inter's residual, transforms, quantisation and reconstruction (res/residual.rs:520-752)
+    for given AQ steps: returns (coefficients n x 384, optimized skip n, reconstruction planes)."""
+    n = (w // 16) * (h // 16)
+    co = np.zeros((n, 384), np.int16)
+    os_ = np.zeros(n, np.uint8)
+    rec = np.zeros(w * h * 3 // 2, np.uint8)
+    lib().oracle_residual_inter(u8(np.ascontiguousarray(cur, np.uint8)), u8(np.ascontiguousarray(pred, np.uint8)),
+                                w, h, u8(np.ascontiguousarray(skip, np.uint8)),
+                                _p(np.ascontiguousarray(qs, np.float32), C.c_float), dz, i16(co), u8(os_), u8(rec))
+    return co, os_, rec

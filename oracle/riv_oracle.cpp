@@ -1470,18 +1470,15 @@ static Bytes encode_intra(const Yuv& cur, uint8_t quality, Yuv& recon, std::vect
 }
 
 // ResidualEncoder::encode_inter (res/residual.rs:396-809)
-static Bytes encode_inter(const Yuv& cur, const Yuv& pred, const std::vector<bool>& skip_mask, uint8_t quality,
-                          float dz, Yuv& recon, std::vector<bool>& opt_skip, std::vector<float>& qsv,
-                          std::vector<int16_t>& all) {
+// Residual, transforms, quantisation and reconstruction of encode_inter (residual.rs:520-752)
+// for given AQ steps; the coefficient coding of the coded MBs follows separately, in MB order.
+static void residual_inter(const Yuv& cur, const Yuv& pred, const std::vector<bool>& skip_mask,
+                           const std::vector<float>& qsv, float dz, Yuv& recon, std::vector<bool>& opt_skip,
+                           std::vector<int16_t>& all) {
     init_tables();
     int w = cur.w, h = cur.h, cw = w / 2, bw = w / 16, bh = h / 16, n = bw * bh;
-    float base = quant_step_from_quality(quality);
-    aq_steps(pred.y.data(), w, w, h, base, qsv);
     all.assign((size_t)n * 384, 0);
     opt_skip.assign(n, true);
-    Bytes data;
-    RansEnc* w_ = nullptr;
-    DctCtx ctx;
     for (int b = 0; b < n; b++) {
         if (skip_mask[b]) continue;
         int bx = b % bw, by = b / bw;
@@ -1513,10 +1510,6 @@ static Bytes encode_inter(const Yuv& cur, const Yuv& pred, const std::vector<boo
         if (zero) continue;
         opt_skip[b] = false;
         memcpy(&all[(size_t)b * 384], tmp, sizeof(tmp));
-        if (!w_) w_ = new RansEnc(&data);
-        dct_encode_plane(*w_, ctx, tmp, 256, true, 0);
-        dct_encode_plane(*w_, ctx, tmp + 256, 64, false, 1);
-        dct_encode_plane(*w_, ctx, tmp + 320, 64, false, 2);
     }
     recon = pred;
     for (int b = 0; b < n; b++) {
@@ -1549,6 +1542,26 @@ static Bytes encode_inter(const Yuv& cur, const Yuv& pred, const std::vector<boo
                     P[i] = (uint8_t)clampi((int)P[i] + r8[y * 8 + x], 0, 255);
                 }
         }
+    }
+}
+
+static Bytes encode_inter(const Yuv& cur, const Yuv& pred, const std::vector<bool>& skip_mask, uint8_t quality,
+                          float dz, Yuv& recon, std::vector<bool>& opt_skip, std::vector<float>& qsv,
+                          std::vector<int16_t>& all) {  // residual.rs:396-809
+    const int n = (cur.w / 16) * (cur.h / 16);
+    aq_steps(pred.y.data(), cur.w, cur.w, cur.h, quant_step_from_quality(quality), qsv);
+    residual_inter(cur, pred, skip_mask, qsv, dz, recon, opt_skip, all);
+    // the inline DCT-rANS coder (residual.rs:618-674) sees the coded MBs in raster order
+    Bytes data;
+    RansEnc* w_ = nullptr;
+    DctCtx ctx;
+    for (int b = 0; b < n; b++) {
+        if (opt_skip[b]) continue;
+        const int16_t* tmp = &all[(size_t)b * 384];
+        if (!w_) w_ = new RansEnc(&data);
+        dct_encode_plane(*w_, ctx, tmp, 256, true, 0);
+        dct_encode_plane(*w_, ctx, tmp + 256, 64, false, 1);
+        dct_encode_plane(*w_, ctx, tmp + 320, 64, false, 2);
     }
     if (w_) {
         w_->finish();
@@ -2124,6 +2137,21 @@ void oracle_aq_steps(const uint8_t* py, uint32_t w, uint32_t h, float base, floa
     memcpy(out, v.data(), v.size() * sizeof(float));
 }
 double oracle_rdo_lambda(uint8_t q, double mult) { return lambda_for_quality(q, mult).lambda; }
+void oracle_residual_inter(const uint8_t* cur_yuv, const uint8_t* pred_yuv, uint32_t w, uint32_t h, const uint8_t* skip,
+                           const float* qs, float dz, int16_t* coeffs, uint8_t* opt_skip, uint8_t* recon_yuv) {
+    const size_t ys = (size_t)w * h, cs = ys / 4;
+    const int n = (int)((w / 16) * (h / 16));
+    Yuv c = yuv_from(cur_yuv, cur_yuv + ys, cur_yuv + ys + cs, (int)w, (int)h);
+    Yuv p = yuv_from(pred_yuv, pred_yuv + ys, pred_yuv + ys + cs, (int)w, (int)h), r;
+    std::vector<bool> sk(n), os;
+    for (int b = 0; b < n; b++) sk[b] = skip[b] != 0;
+    std::vector<float> q(qs, qs + n);
+    std::vector<int16_t> all;
+    residual_inter(c, p, sk, q, dz, r, os, all);
+    memcpy(coeffs, all.data(), all.size() * 2);
+    for (int b = 0; b < n; b++) opt_skip[b] = os[b] ? 1 : 0;
+    yuv_to(r, recon_yuv, recon_yuv + ys, recon_yuv + ys + cs);
+}
 void oracle_fdct16_quant(const int16_t* blk, float qs, float dz, int16_t* out) {
     init_tables();
     int32_t b[256], c[256];

@@ -88,6 +88,11 @@ int64_t oracle_sad_int(const uint8_t* prev_y, const uint8_t* curr_y, uint32_t w,
 int64_t oracle_sad_halfpel(const uint8_t* prev_y, const uint8_t* curr_y, uint32_t w, uint32_t h, int x0,
                            int y0, int dx_hp, int dy_hp, int64_t limit, int force_scalar);
 void oracle_aq_steps(const uint8_t* pred_y, uint32_t w, uint32_t h, float base, float* out);
+/* Residual, 16x16/8x8 FDCT, dead-zone quantisation, optimized skip and reconstruction of
+ * encode_inter (res/residual.rs:520-752) for given per-MB AQ steps; skip = RDO-skipped MBs;
+ * coeffs: 384 per MB; planes contiguous Y, U, V. */
+void oracle_residual_inter(const uint8_t* cur_yuv, const uint8_t* pred_yuv, uint32_t w, uint32_t h, const uint8_t* skip,
+                           const float* qs, float dz, int16_t* coeffs, uint8_t* opt_skip, uint8_t* recon_yuv);
 double oracle_rdo_lambda(uint8_t inter_quality, double mult);
 /* forward transforms + quant of one block; inverse of one block */
 void oracle_fdct16_quant(const int16_t* blk256, float qs, float dead_zone, int16_t* out256);

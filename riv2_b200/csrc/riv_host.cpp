@@ -1079,11 +1079,20 @@ static riv_status drain_all(riv_encoder* e) {
         ~Draining() { e->draining = false; }
     } guard{e};
     e->draining = true;
+    // A record the writer refuses is dropped (pump pops it) and the drain goes on, so that
+    // every later record is still written and the header can be patched; the refusal is
+    // reported once the queue is empty.
+    riv_status io = RIV_OK;
     while (!e->jobs.empty()) {
         riv_status st = pump(e, true);
+        if (st == RIV_ERR_IO) {
+            io = st;
+            continue;
+        }
         if (st) return st;
     }
-    return RIV_OK;
+    if (io) e->err = "writer.write failed for at least one record; the others were written";
+    return io;
 }
 
 static riv_status encode_common(riv_encoder* e, int src, const void* a, const void* b, const void* c3,
@@ -1229,10 +1238,12 @@ riv_status riv_encode_frame_yuv(riv_encoder* e, const uint8_t* y, const uint8_t*
 riv_status riv_finish(riv_encoder* e) {  // enc/encoder.rs:950-961
     if (!e) return RIV_ERR_INVALID_CONFIG;
     if (e->poisoned) return poisoned_status(e);
+    riv_status dropped = RIV_OK;  // RIV_ERR_IO: a record was refused, the rest were written
     try {
         CK(cudaSetDevice(e->cfg.device));
         riv_status st = drain_all(e);
-        if (st) return st;
+        if (st && st != RIV_ERR_IO) return st;
+        dropped = st;
     } catch (const CudaError& ce) {
         return fail(e, RIV_ERR_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
     } catch (const std::exception& ex) {
@@ -1244,7 +1255,7 @@ riv_status riv_finish(riv_encoder* e) {  // enc/encoder.rs:950-961
     if (e->wr.write(e->wr.user, h.data(), h.size()) != 0) return fail(e, RIV_ERR_IO, "writer.write failed");
     if (e->wr.seek(e->wr.user, end) != 0) return fail(e, RIV_ERR_IO, "writer.seek failed");
     if (e->wr.flush(e->wr.user) != 0) return fail(e, RIV_ERR_IO, "writer.flush failed");
-    return RIV_OK;
+    return dropped;
 }
 
 void riv_encoder_free(riv_encoder* e) {
@@ -1414,6 +1425,101 @@ riv_status riv_stage_rgb_to_yuv(const uint8_t* rgb, uint32_t dw, uint32_t dh, ui
     return st;
 }
 
+// Device buffers of one stage call, freed together.
+struct StageBufs {
+    std::vector<void*> ps;
+    void* get(size_t n) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, n ? n : 1) != cudaSuccess) throw CudaError{cudaErrorMemoryAllocation, "cudaMalloc"};
+        ps.push_back(p);
+        return p;
+    }
+    void* up(const void* h, size_t n) {
+        void* p = get(n);
+        CK(cudaMemcpy(p, h, n, cudaMemcpyHostToDevice));
+        return p;
+    }
+    ~StageBufs() {
+        for (void* p : ps) cudaFree(p);
+    }
+};
+
+riv_status riv_stage_predict(const uint8_t* ref_yuv, const int8_t* mv4, uint32_t w, uint32_t h, uint8_t quality,
+                             uint8_t* pred_yuv, float* qs) {
+    if (!ref_yuv || !mv4 || !pred_yuv || w == 0 || h == 0 || w % 16 || h % 16) return RIV_ERR_FRAME;
+    LibmFix& F = libm_fix();
+    if (!F.ok) return RIV_ERR_ENCODING_FAILED;
+    const int n = (int)((w / 16) * (h / 16));
+    const size_t yuv = (size_t)w * h * 3 / 2;
+    std::vector<MbOut> mb(n);
+    for (int i = 0; i < n; i++) {
+        memset(&mb[i], 0, sizeof(MbOut));
+        memcpy(mb[i].raw, mv4 + 4 * i, 4);
+        memcpy(mb[i].coded, mv4 + 4 * i, 4);
+    }
+    try {
+        StageBufs B;
+        auto* dref = (const uint8_t*)B.up(ref_yuv, yuv);
+        auto* dmb = (const MbOut*)B.up(mb.data(), n * sizeof(MbOut));
+        auto* dpred = (uint8_t*)B.get(yuv);
+        auto* dvs = (uint2*)B.get((size_t)n * sizeof(uint2));
+        auto* dlnv = (float*)B.get((size_t)(n + 1) * 4);
+        auto* dqs = (float*)B.get((size_t)n * 4);
+        auto* dlog = (const uint32_t*)B.up(F.logf_dev.data(), F.logf_dev.size() * 4);
+        auto* dexp = (const uint32_t*)B.up(F.exp2f_dev.data(), F.exp2f_dev.size() * 4);
+        CK((cudaError_t)launch_predict(dref, dmb, dpred, dvs, (int)w, (int)h, 0));
+        CK((cudaError_t)launch_aq(dvs, n, quant_step(quality), dlog, (int)(F.logf.size() / 2), dexp,
+                                  (int)(F.exp2f.size() / 2), dlnv, dqs, 0));
+        CK(cudaMemcpy(pred_yuv, dpred, yuv, cudaMemcpyDeviceToHost));
+        if (qs) CK(cudaMemcpy(qs, dqs, (size_t)n * 4, cudaMemcpyDeviceToHost));
+    } catch (const CudaError&) {
+        return RIV_ERR_CUDA;
+    }
+    return RIV_OK;
+}
+
+riv_status riv_stage_residual(const uint8_t* cur_yuv, const uint8_t* pred_yuv, const float* qs, const uint8_t* rdo_skip,
+                              const int8_t* coded4, float dead_zone, uint32_t w, uint32_t h, int16_t* coeffs,
+                              uint8_t* opt_skip, uint8_t* recon_yuv, uint8_t* fmask) {
+    if (!cur_yuv || !pred_yuv || !qs || !rdo_skip || !coeffs || !opt_skip || !recon_yuv || w == 0 || h == 0 || w % 16 ||
+        h % 16)
+        return RIV_ERR_FRAME;
+    const int n = (int)((w / 16) * (h / 16));
+    const size_t yuv = (size_t)w * h * 3 / 2;
+    std::vector<MbOut> mb(n);
+    for (int i = 0; i < n; i++) {
+        memset(&mb[i], 0, sizeof(MbOut));
+        if (coded4) memcpy(mb[i].coded, coded4 + 4 * i, 4);
+        mb[i].rdo_skip = rdo_skip[i] ? 1 : 0;
+    }
+    try {
+        StageBufs B;
+        ResidualParams rp{};
+        rp.cur = (const uint8_t*)B.up(cur_yuv, yuv);
+        rp.pred = (const uint8_t*)B.up(pred_yuv, yuv);
+        rp.recon = (uint8_t*)B.get(yuv);
+        rp.coeffs = (int16_t*)B.get((size_t)n * 384 * 2);
+        rp.opt_skip = (uint8_t*)B.get(n);
+        rp.fmask = (uint8_t*)B.get(n);
+        rp.eobs = (uint8_t*)B.get((size_t)n * 3);
+        rp.mb = (const MbOut*)B.up(mb.data(), n * sizeof(MbOut));
+        rp.qs = (const float*)B.up(qs, (size_t)n * 4);
+        rp.dead_zone = dead_zone;
+        rp.W = (int)w;
+        rp.H = (int)h;
+        rp.BW = (int)w / 16;
+        rp.intra = 0;
+        CK((cudaError_t)launch_residual(rp, n, 0));
+        CK(cudaMemcpy(coeffs, rp.coeffs, (size_t)n * 384 * 2, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(opt_skip, rp.opt_skip, n, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(recon_yuv, rp.recon, yuv, cudaMemcpyDeviceToHost));
+        if (fmask) CK(cudaMemcpy(fmask, rp.fmask, n, cudaMemcpyDeviceToHost));
+    } catch (const CudaError&) {
+        return RIV_ERR_CUDA;
+    }
+    return RIV_OK;
+}
+
 riv_status riv_stage_deblock(uint8_t* yuv, uint32_t w, uint32_t h, int level, int intra, const uint8_t* mask) {
     if (!yuv || w % 16 || h % 16) return RIV_ERR_FRAME;
     if (level <= 0) return RIV_OK;
@@ -1499,6 +1605,108 @@ riv_status riv_stage_libm(int which, const float* in, float* out, size_t n) {
     cudaFree(dout);
     cudaFree(df);
     return st;
+}
+
+// Exhaustive check of the device logf / exp2f against the host's glibc: every f32 with bit
+// pattern in [lo_bits, hi_bits], in chunks computed on the device while the host threads
+// compare the previous chunk bit for bit.
+riv_status riv_test_libm_range(int which, uint32_t lo_bits, uint32_t hi_bits, uint64_t* mismatches,
+                               uint32_t* first_bad_bits) {
+    if (!mismatches || !first_bad_bits || which < 0 || which > 2 || hi_bits < lo_bits) return RIV_ERR_FRAME;
+    *mismatches = 0;
+    *first_bad_bits = 0;
+    LibmFix& F = libm_fix();
+    if (!F.ok) return RIV_ERR_ENCODING_FAILED;
+    const std::vector<uint32_t>& fx = which == 1 ? F.exp2f_dev : F.logf_dev;
+    const int npairs = (int)((which == 1 ? F.exp2f : F.logf).size() / 2);
+    const uint32_t CH = 1u << 25;
+    void *df = nullptr, *dout[2] = {nullptr, nullptr}, *hout[2] = {nullptr, nullptr};
+    cudaStream_t st = nullptr;
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    riv_status rs = RIV_OK;
+    std::atomic<uint64_t> bad{0};
+    std::atomic<uint32_t> first{0xffffffffu};
+    const unsigned nthr = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    auto compare = [&](const float* got, uint32_t base, uint32_t n) {
+        std::vector<std::thread> ts;
+        for (unsigned t = 0; t < nthr; t++)
+            ts.emplace_back([&, t] {
+                const uint32_t a = (uint32_t)((uint64_t)n * t / nthr), b = (uint32_t)((uint64_t)n * (t + 1) / nthr);
+                uint64_t nb = 0;
+                uint32_t fb = 0xffffffffu;
+                for (uint32_t i = a; i < b; i++) {
+                    const uint32_t bits = base + i;
+                    float x;
+                    memcpy(&x, &bits, 4);
+                    const float want = which == 1 ? exp2f(x) : logf(x);
+                    uint32_t wb, gb;
+                    memcpy(&wb, &want, 4);
+                    memcpy(&gb, got + i, 4);
+                    if (wb != gb && !(want != want && got[i] != got[i])) {
+                        nb++;
+                        fb = std::min(fb, bits);
+                    }
+                }
+                bad += nb;
+                uint32_t cur = first.load();
+                while (fb < cur && !first.compare_exchange_weak(cur, fb)) {}
+            });
+        for (auto& t : ts) t.join();
+    };
+    if (cudaMalloc(&df, fx.size() * 4 + 4) || cudaMemcpy(df, fx.data(), fx.size() * 4, cudaMemcpyHostToDevice) ||
+        cudaMalloc(&dout[0], (size_t)CH * 4) || cudaMalloc(&dout[1], (size_t)CH * 4) ||
+        cudaMallocHost(&hout[0], (size_t)CH * 4) || cudaMallocHost(&hout[1], (size_t)CH * 4) ||
+        cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) ||
+        cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming) ||
+        cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming))
+        rs = RIV_ERR_CUDA;
+    const uint64_t total = (uint64_t)hi_bits - lo_bits + 1;
+    const uint64_t nch = (total + CH - 1) / CH;
+    auto enqueue = [&](uint64_t c) {
+        const int k = (int)(c & 1);
+        const uint32_t base = (uint32_t)(lo_bits + c * CH);
+        const uint32_t n = (uint32_t)std::min<uint64_t>(CH, total - c * CH);
+        return launch_libm_range(which, base, n, (float*)dout[k], (const uint32_t*)df, npairs, st) == 0 &&
+               cudaMemcpyAsync(hout[k], dout[k], (size_t)n * 4, cudaMemcpyDeviceToHost, st) == cudaSuccess &&
+               cudaEventRecord(done[k], st) == cudaSuccess;
+    };
+    if (!rs && !enqueue(0)) rs = RIV_ERR_CUDA;
+    for (uint64_t c = 0; !rs && c < nch; c++) {
+        if (c + 1 < nch && !enqueue(c + 1)) { rs = RIV_ERR_CUDA; break; }
+        if (cudaEventSynchronize(done[c & 1]) != cudaSuccess) { rs = RIV_ERR_CUDA; break; }
+        compare((const float*)hout[c & 1], (uint32_t)(lo_bits + c * CH), (uint32_t)std::min<uint64_t>(CH, total - c * CH));
+    }
+    if (st) cudaStreamSynchronize(st);
+    for (int k = 0; k < 2; k++) {
+        cudaFree(dout[k]);
+        cudaFreeHost(hout[k]);
+        if (done[k]) cudaEventDestroy(done[k]);
+    }
+    cudaFree(df);
+    if (st) cudaStreamDestroy(st);
+    *mismatches = bad.load();
+    *first_bad_bits = bad.load() ? first.load() : 0;
+    return rs;
+}
+
+riv_status riv_test_wait_expiry(int which, int64_t spin_limit, uint32_t* status_word) {
+    if (which < 0 || which > 3 || spin_limit < 1 || spin_limit > (1 << 20) || !status_word) return RIV_ERR_FRAME;
+    *status_word = 0;
+    try {
+        StageBufs B;
+        auto* rec = (unsigned long long*)B.get(4 * 8);
+        auto* cnt = (unsigned*)B.get(4 * 4);
+        auto* st = (unsigned*)B.get(4);
+        CK(cudaMemset(rec, 0, 4 * 8));
+        CK(cudaMemset(cnt, 0, 4 * 4));
+        CK(cudaMemset(st, 0, 4));
+        CK((cudaError_t)launch_wait_expiry(which, rec, cnt, (long long)spin_limit, st, 0));
+        CK(cudaDeviceSynchronize());
+        CK(cudaMemcpy(status_word, st, 4, cudaMemcpyDeviceToHost));
+    } catch (const CudaError&) {
+        return RIV_ERR_CUDA;
+    }
+    return (*status_word & ST_WAIT_TIMEOUT) ? RIV_ERR_DEVICE_TIMEOUT : RIV_OK;
 }
 
 riv_status riv_libm_fixup_counts(uint32_t* nlog, uint32_t* nexp) {
@@ -1835,8 +2043,14 @@ riv_dec_status riv_decoder_new(const uint8_t* data, size_t len, int device, riv_
     if (!out) return RIV_DEC_INVALID_HEADER;
     *out = nullptr;
     if (!data || len < 36 || memcmp(data, "RIV\0", 4) != 0 || get_le(data + 4, 4) != 5) return RIV_DEC_INVALID_HEADER;
-    riv_decoder* d = new riv_decoder();
-    d->data.assign(data, data + len);
+    riv_decoder* d = nullptr;
+    try {  // a large stream may not fit in host memory: no exception crosses the C ABI
+        d = new riv_decoder();
+        d->data.assign(data, data + len);
+    } catch (const std::exception&) {
+        delete d;
+        return RIV_DEC_DECODING_FAILED;
+    }
     d->dw = (uint32_t)get_le(data + 8, 4);
     d->dh = (uint32_t)get_le(data + 12, 4);
     d->sw = (uint32_t)get_le(data + 16, 4);

@@ -163,6 +163,9 @@ int launch_compact(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coef
                    uint32_t* hhdr, void* stream);
 // libm device helpers exposed for the exhaustive check
 int launch_libm_eval(int which, const float* in, float* out, size_t n, const uint32_t* fix, int nfix, void* stream);
+int launch_libm_range(int which, uint32_t lo, uint32_t n, float* out, const uint32_t* fix, int nfix, void* stream);
+int launch_wait_expiry(int which, const unsigned long long* rec, const unsigned* counter, long long limit,
+                       unsigned* status, void* stream);
 
 // ---- the worker-task queue of the fused search launch (used by the kernel and by the
 // riv_test_worker_queue hook).  Step k holds, in this order: the previous frame's residual of

@@ -1463,6 +1463,41 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                  : "memory");
 }
 
+// Expiry of the bounded waits, on flags nothing sets (test hook).  which: 0 a wavefront record
+// (rec_wait), 1 a worker-queue counter (wait_at_least), 2 a search -> mode hand-off slot
+// (hand_get), 3 an mbarrier phase that never completes (mbar_wait_warp).  Each waiting warp
+// gives up after `limit` polls and reports ST_WAIT_TIMEOUT in *status, as the search launch
+// does; the kernel then returns normally.
+__global__ void k_wait_expiry(int which, const unsigned long long* rec, const unsigned* counter, long long limit,
+                              unsigned* status) {
+    __shared__ unsigned long long bar;
+    __shared__ unsigned long long hand[HAND_RING];
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    for (int i = threadIdx.x; i < HAND_RING; i += blockDim.x) hand[i] = 0;
+    __syncthreads();
+    bool ok = true;
+    if (which == 0) {
+        unsigned long long v = 0;
+        if (lane == 0) ok = rec_wait(rec + blockIdx.x, 0x5a5aull << 48, v, limit);
+    } else if (which == 1) {
+        if (lane == 0) ok = wait_at_least(counter + blockIdx.x, 1u, limit);
+    } else if (which == 2) {
+        unsigned long long w = 0;
+        if (lane == 0) ok = hand_get(hand, 0, w, limit);
+    } else {
+        ok = mbar_wait_warp(&bar, 0u, limit);
+    }
+    if (lane == 0 && !ok) atomicOr(status, ST_WAIT_TIMEOUT);
+    __syncthreads();
+    if (threadIdx.x == 0) mbar_inval(&bar);
+}
+int launch_wait_expiry(int which, const unsigned long long* rec, const unsigned* counter, long long limit,
+                       unsigned* status, void* stream) {
+    k_wait_expiry<<<4, 64, 0, (cudaStream_t)stream>>>(which, rec, counter, limit, status);
+    return (int)cudaGetLastError();
+}
+
 // Staging ring of the band+table search (LD_RING MBs ahead): per slot the MB's SAD-table row
 // (2*tstride bytes), its 16x16 current block and the previous frame's coded MV (4 bytes).
 constexpr int LD_RING = 4;
@@ -2594,6 +2629,32 @@ __global__ void k_libm_eval(int which, const float* in, float* out, size_t n, co
 }
 int launch_libm_eval(int which, const float* in, float* out, size_t n, const uint32_t* fix, int nfix, void* stream) {
     k_libm_eval<<<1184, 256, 0, (cudaStream_t)stream>>>(which, in, out, n, fix, nfix);
+    return (int)cudaGetLastError();
+}
+
+// Every f32 whose bit pattern lies in [lo, lo + n): out[i] = f(bits lo + i).  which: 0 logf,
+// 1 exp2f, 2 logf through the four-wide batched search the AQ warps use.
+__global__ void k_libm_range(int which, uint32_t lo, uint32_t n, float* out, const uint32_t* fix, int nfix) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    if (which == 2) {
+        for (uint32_t i = 4 * (blockIdx.x * blockDim.x + threadIdx.x); i < n; i += 4 * stride) {
+            float x[4], y[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) x[j] = __uint_as_float(lo + min(i + j, n - 1));
+            glibc_logf_batch<4>(x, y, fix, nfix);
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (i + j < n) out[i + j] = y[j];
+        }
+        return;
+    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float x = __uint_as_float(lo + i);
+        out[i] = which == 0 ? glibc_logf(x, fix, nfix) : glibc_exp2f(x, fix, nfix);
+    }
+}
+int launch_libm_range(int which, uint32_t lo, uint32_t n, float* out, const uint32_t* fix, int nfix, void* stream) {
+    k_libm_range<<<148 * 8, 256, 0, (cudaStream_t)stream>>>(which, lo, n, out, fix, nfix);
     return (int)cudaGetLastError();
 }
 

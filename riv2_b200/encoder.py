@@ -112,7 +112,8 @@ EXPORTED_SYMBOLS = (
     "riv_debug_frame_state", "riv_counters", "riv_host_times", "riv_stage_deblock_noalloc",
     "riv_decoder_new", "riv_decoder_info", "riv_decode_frame_yuv", "riv_decode_frame_rgb", "riv_decoder_current_frame",
     "riv_decoder_last_error", "riv_decoder_free", "riv_test_dct_encode", "riv_test_dct_decode", "riv_test_mv_encode",
-    "riv_test_mv_decode", "riv_test_delta_bias", "riv_test_worker_queue",
+    "riv_test_mv_decode", "riv_test_delta_bias", "riv_test_worker_queue", "riv_test_libm_range",
+    "riv_stage_predict", "riv_stage_residual", "riv_test_wait_expiry",
 )
 
 
@@ -154,6 +155,11 @@ def lib() -> C.CDLL:
                                             C.c_size_t]
     L.riv_stage_libm.argtypes = [C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_size_t]
     L.riv_libm_fixup_counts.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+    L.riv_stage_predict.argtypes = [U8P, P, C.c_uint32, C.c_uint32, C.c_uint8, U8P, C.POINTER(C.c_float)]
+    L.riv_stage_residual.argtypes = [U8P, U8P, C.POINTER(C.c_float), U8P, P, C.c_float, C.c_uint32, C.c_uint32, P,
+                                     U8P, U8P, U8P]
+    L.riv_test_wait_expiry.argtypes = [C.c_int, C.c_int64, C.POINTER(C.c_uint32)]
+    L.riv_test_libm_range.argtypes = [C.c_int, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]
     L.riv_dct_tables.argtypes = [C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     L.riv_debug_frame_state.argtypes = [P, C.c_int, P, C.c_size_t]
     L.riv_counters.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
@@ -546,6 +552,40 @@ def stage_libm(which: int, x: np.ndarray) -> np.ndarray:
     if st:
         raise _ERRORS.get(st, EncodeError)("riv_stage_libm failed")
     return out
+
+
+def stage_predict(ref_yuv: np.ndarray, mv4: np.ndarray, w: int, h: int, quality: int):
+    """build_predicted + compute_aq_quant_steps on the GPU: (prediction planes, AQ steps)."""
+    ref = np.ascontiguousarray(ref_yuv, dtype=np.uint8)
+    mv = np.ascontiguousarray(mv4, dtype=np.int8)
+    pred = np.empty(w * h * 3 // 2, np.uint8)
+    qs = np.empty((w // 16) * (h // 16), np.float32)
+    st = lib().riv_stage_predict(_u8(ref), mv.ctypes.data, w, h, quality, _u8(pred),
+                                 qs.ctypes.data_as(C.POINTER(C.c_float)))
+    if st:
+        raise _ERRORS.get(st, EncodeError)("riv_stage_predict failed")
+    return pred, qs
+
+
+def stage_residual(cur_yuv, pred_yuv, qs, rdo_skip, w: int, h: int, dead_zone: float, coded4=None):
+    """encode_inter's residual path on the GPU: (coefficients n x 384, optimized skip,
+    pre-deblock reconstruction planes, deblock mask)."""
+    n = (w // 16) * (h // 16)
+    cur = np.ascontiguousarray(cur_yuv, dtype=np.uint8)
+    pred = np.ascontiguousarray(pred_yuv, dtype=np.uint8)
+    q = np.ascontiguousarray(qs, dtype=np.float32)
+    sk = np.ascontiguousarray(rdo_skip, dtype=np.uint8)
+    cd = None if coded4 is None else np.ascontiguousarray(coded4, dtype=np.int8)
+    co = np.empty((n, 384), np.int16)
+    os_ = np.empty(n, np.uint8)
+    rec = np.empty(w * h * 3 // 2, np.uint8)
+    fm = np.empty(n, np.uint8)
+    st = lib().riv_stage_residual(_u8(cur), _u8(pred), q.ctypes.data_as(C.POINTER(C.c_float)), _u8(sk),
+                                  None if cd is None else cd.ctypes.data, dead_zone, w, h, co.ctypes.data, _u8(os_),
+                                  _u8(rec), _u8(fm))
+    if st:
+        raise _ERRORS.get(st, EncodeError)("riv_stage_residual failed")
+    return co, os_, rec, fm
 
 
 def dct_encode_host(blocks: np.ndarray, intra: bool, threads: int = 0) -> bytes:

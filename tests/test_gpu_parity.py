@@ -287,3 +287,41 @@ def test_encode_1080p_matches_oracle(q):
     frames = _clip("1080p", 3, seed=2)
     gc, oc = _cfgs(1920, 1080, *q)
     _check(*_encode_both(frames, gc, oc))
+
+
+# ---------------------------------------------------------------------------------------
+# Whole-encode parity on content and qualities the synthetic clips do not reach
+# ---------------------------------------------------------------------------------------
+
+def _noise_clip(n, w, h, seed):
+    rng = np.random.default_rng(seed)
+    return [rng.integers(0, 256, (h, w, 3), dtype=np.uint8) for _ in range(n)]
+
+
+def _step_clip(n, w, h, seed):
+    """Full-range 0/255 blocks that move by a few pixels per frame (MVs up to the range)."""
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:h + 64, 0:w + 64]
+    base = np.where(((yy // 13) + (xx // 11)) % 2 == 0, 0, 255).astype(np.uint8)
+    out = []
+    for t in range(n):
+        dy, dx = int(rng.integers(0, 32)), int(rng.integers(0, 32))
+        f = base[dy:dy + h, dx:dx + w]
+        out.append(np.stack([f, 255 - f, f], axis=-1).copy())
+    return out
+
+
+@pytest.mark.parametrize("case", ["q1", "q100", "noise_q100", "noise_q1", "steps_q100", "steps_sr31"])
+def test_encode_extreme_content_and_quality_matches_oracle(case):
+    w, h, kw = 352, 288, {}
+    if case in ("q1", "q100"):
+        frames = _clip("cif", 6, seed=21)
+    elif case.startswith("noise"):
+        frames = _noise_clip(4, w, h, seed=22)
+    else:
+        frames = _step_clip(5, w, h, seed=23)
+    q = 1 if case.endswith("q1") else 100
+    if case == "steps_sr31":
+        q, kw = 90, {"search_range": 31}
+    gc, oc = _cfgs(w, h, q, q, **kw)
+    _check(*_encode_both(frames, gc, oc))

@@ -74,10 +74,21 @@ def test_noalloc_matches_existing_entry_point_twice(w, h, with_mask):
 
 @pytest.mark.gpu
 def test_noalloc_at_the_size_limit_edge():
-    # largest storage size the scratch takes with a mask: 1920x1088 (3,141,600 bytes)
-    w, h = 1920, 1088
-    assert w * h * 3 // 2 + (w // 16) * (h // 16) <= MAX_BYTES
-    yuv = _planes(w, h, seed=3)
-    st0, ref = _existing(yuv, w, h, 0, False, None)
-    st1, out, _ = _noalloc(yuv, w, h, 0, False, None)  # level 0: nothing to do
-    assert st0 == st1 == 0 and np.array_equal(out, yuv) and np.array_equal(ref, yuv)
+    # 2048x1360 with a mask fills the scratch to within 5.5 KB of its end (4,188,800 of
+    # 4,194,304 bytes): the planes and the mask both sit at the scratch's far end
+    w, h = 2048, 1360
+    need = w * h * 3 // 2 + (w // 16) * (h // 16)
+    assert MAX_BYTES - 8192 < need <= MAX_BYTES
+    rng = np.random.default_rng(5)
+    for call in range(2):
+        yuv = _planes(w, h, seed=11 + call)
+        mask = rng.integers(0, 2, size=(w // 16) * (h // 16)).astype(np.uint8)
+        mask[-64:] = 1  # the last MB rows (the mask's last bytes) are filtered
+        st0, ref = _existing(yuv, w, h, 36, False, mask)
+        st1, out, msg = _noalloc(yuv, w, h, 36, False, mask)
+        assert st0 == 0 and st1 == 0, msg
+        assert not np.array_equal(ref, yuv)
+        assert np.array_equal(out, ref), f"call {call}: {(out != ref).sum()} samples differ"
+    # one 16-pixel row more no longer fits
+    st, _, msg = _noalloc(np.zeros(w * (h + 16) * 3 // 2, np.uint8), w, h + 16, 36, False, mask)
+    assert st == 5 and "RIV_DEBLOCK_NOALLOC_MAX_BYTES" in msg
