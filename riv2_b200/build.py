@@ -17,7 +17,7 @@ CSRC = os.path.join(PKG_DIR, "csrc")
 REPO = os.path.dirname(PKG_DIR)
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUDA_SOURCES = ["riv_kernels.cu", "riv_host.cpp", "riv_entropy.cpp"]
+CUDA_SOURCES = ["riv_kernels.cu", "riv_nn.cu", "riv_host.cpp", "riv_entropy.cpp"]
 HOST_FLAGS = "-fPIC,-fwrapv,-ffp-contract=off,-fno-fast-math,-O2"
 
 
@@ -37,7 +37,7 @@ def _run(cmd: list[str]) -> None:
 def build_cuda(force: bool = False) -> str:
     os.makedirs(LIB_DIR, exist_ok=True)
     out = os.path.join(LIB_DIR, "libriv2_b200.so")
-    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(REPO, "include", "riv_gpu.h")]
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(REPO, "include", h) for h in ("riv_gpu.h", "riv_nn.h")]
     if not force and not _stale(out, deps):
         return out
     objs = []

@@ -1098,11 +1098,18 @@ static riv_status drain_all(riv_encoder* e) {
 static riv_status encode_common(riv_encoder* e, int src, const void* a, const void* b, const void* c3,
                                 uint64_t ts, riv_frame_stats* stats) {
     if (e->poisoned) return poisoned_status(e);
+    // A record the writer refuses while this call makes room is lost (pump drops it); this
+    // frame is still encoded and queued, and the refusal is reported when the call returns.
+    riv_status refused = RIV_OK;
     try {
         CK(cudaSetDevice(e->cfg.device));
         size_t cap = e->slots.size();
         while (e->jobs.size() >= cap) {
             riv_status st = pump(e, true);
+            if (st == RIV_ERR_IO) {
+                refused = st;
+                continue;
+            }
             if (st) return st;
         }
         // frame type (enc/encoder.rs:265-291)
@@ -1138,7 +1145,8 @@ static riv_status encode_common(riv_encoder* e, int src, const void* a, const vo
     } catch (const std::exception& ex) {
         return fail_poison(e, RIV_ERR_ENCODING_FAILED, ex.what());
     }
-    return RIV_OK;
+    if (refused) e->err = "writer.write failed for an earlier frame's record; that record is lost";
+    return refused;
 }
 
 }  // namespace

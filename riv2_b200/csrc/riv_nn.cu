@@ -1,0 +1,825 @@
+// riv_nn.cu -- tensor-core kernels of the motion-proposal network (sm_100a).
+//
+// Both kernels accumulate bf16 x bf16 products in f32 tensor memory with tcgen05.mma, issued
+// by one thread of the CTA, operands read from shared memory through 64-bit matrix
+// descriptors (K-major, 128-byte or 64-byte swizzle), completion tracked by tcgen05.commit on
+// mbarriers, the accumulator read back with tcgen05.ld for the epilogue.
+//
+//  * k_nn_gemm: D = A . B^T with both operands staged by TMA (cp.async.bulk.tensor) through a
+//    four-deep ring: warp 0 issues the copies, warp 1 the MMAs, all four warps run the
+//    epilogue (warp w owns accumulator rows 32w .. 32w+31, the TMEM lanes it may read).
+//  * k_nn_conv: implicit-GEMM 3x3 convolution.  The weights come in once by TMA and stay in
+//    shared memory; each 128-row tile of output positions is gathered (im2col) by the CTA's
+//    threads straight into the swizzled operand layout, one k-block per ring stage, while the
+//    tensor core consumes the previous stage.  Persistent CTAs, one per SM.
+//
+// Every wait is bounded; an expired wait sets bit 0 of *err and the kernel runs to its end
+// without waiting again (tensor memory is always released).
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+
+#include "../../include/riv_nn.h"
+#include "riv_nn.h"
+
+namespace {
+
+constexpr long long NN_SPIN = 1ll << 26;
+
+__device__ __forceinline__ uint32_t s32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// ---- mbarriers
+__device__ __forceinline__ void mb_init(uint64_t* b, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mb_expect_tx(uint64_t* b, unsigned tx) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(s32(b)), "r"(tx) : "memory");
+}
+__device__ __forceinline__ bool mb_try(uint64_t* b, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(s32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for the completion of the phase with the given parity.  `dead` short-cuts all
+// later waits once one has expired.
+__device__ __forceinline__ bool mb_wait(uint64_t* b, unsigned parity, unsigned* err, bool& dead) {
+    if (dead) return false;
+    long long n = 0;
+    while (!mb_try(b, parity)) {
+        if (++n > NN_SPIN) {
+            atomicOr(err, 1u);
+            dead = true;
+            return false;
+        }
+    }
+    return true;
+}
+
+// ---- TMA
+__device__ __forceinline__ void tma_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            s32(dst)),
+        "l"((uint64_t)map), "r"(x), "r"(y), "r"(s32(bar))
+        : "memory");
+}
+
+// ---- tensor memory and tcgen05
+__device__ __forceinline__ void tm_alloc(uint32_t* slot, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(s32(slot)), "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tm_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// K-major shared-memory matrix descriptor: rows of 128 (or 64) bytes, 16-byte chunks XOR
+// swizzled by the row within 8-row groups that lie 1024 (512) bytes apart.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, int swz) {
+    uint64_t d = (uint64_t)((saddr & 0x3FFFFu) >> 4);
+    d |= (uint64_t)1 << 16;                                   // leading offset: unused when swizzled
+    d |= (uint64_t)((swz == 128 ? 1024u : 512u) >> 4) << 32;  // stride between 8-row groups
+    d |= (uint64_t)1 << 46;                                   // descriptor version of sm_100
+    d |= (uint64_t)(swz == 128 ? 2u : 4u) << 61;              // swizzle mode
+    return d;
+}
+// Instruction descriptor: bf16 A and B (K-major), f32 accumulator, M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void umma(uint32_t dtm, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dtm),
+        "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+        : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(s32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tm_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+        "[%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *(uint32_t*)&h;
+}
+
+// =====================================================================================
+// GEMM
+// =====================================================================================
+constexpr int GEMM_STAGES = 4;
+
+struct GemmArgs {
+    int M, N, nkb_total, kb_per_cta, ntile;
+    float* d;
+    __nv_bfloat16* dh;
+    int ldd;
+    const float* bias;
+    int relu, mode;
+    unsigned* err;
+};
+
+template <int BK>
+__global__ void __launch_bounds__(128, 1)
+    k_nn_gemm(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, GemmArgs g) {
+    constexpr int SWZ = BK * 2;  // bytes per operand row
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* sm = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    const int BN = g.ntile;
+    const int a_bytes = 128 * SWZ, b_bytes = BN * SWZ;
+    const int stage_bytes = (a_bytes + b_bytes + 1023) & ~1023;
+    uint64_t* full = (uint64_t*)(sm + GEMM_STAGES * stage_bytes);
+    uint64_t* empty = full + GEMM_STAGES;
+    uint64_t* accum = empty + GEMM_STAGES;
+    uint32_t* slot = (uint32_t*)(accum + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * 128, n0 = blockIdx.z * BN;
+    const int kb0 = blockIdx.y * g.kb_per_cta;
+    const int nkb = min(g.kb_per_cta, g.nkb_total - kb0);
+    uint32_t ncols = 32;
+    while ((int)ncols < BN) ncols <<= 1;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < GEMM_STAGES; s++) {
+            mb_init(&full[s], 1);
+            mb_init(&empty[s], 1);
+        }
+        mb_init(accum, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) tm_alloc(slot, ncols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tacc = *slot;
+    bool dead = false;
+    if (nkb > 0) {
+        if (warp == 0 && lane == 0) {  // TMA producer
+            for (int i = 0; i < nkb && !dead; i++) {
+                const int s = i % GEMM_STAGES;
+                if (i >= GEMM_STAGES) mb_wait(&empty[s], ((i / GEMM_STAGES) - 1) & 1, g.err, dead);
+                if (dead) break;
+                uint8_t* st = sm + s * stage_bytes;
+                mb_expect_tx(&full[s], (unsigned)(a_bytes + b_bytes));
+                tma_2d(st, &ta, (kb0 + i) * BK, m0, &full[s]);
+                tma_2d(st + a_bytes, &tb, (kb0 + i) * BK, n0, &full[s]);
+            }
+        } else if (warp == 1 && lane == 0) {  // MMA issuer
+            const uint32_t idesc = idesc_bf16(128, BN);
+            for (int i = 0; i < nkb && !dead; i++) {
+                const int s = i % GEMM_STAGES;
+                if (!mb_wait(&full[s], (i / GEMM_STAGES) & 1, g.err, dead)) break;
+                tc_fence_after();
+                const uint32_t sa = s32(sm + s * stage_bytes);
+                const uint64_t ad = sdesc(sa, SWZ), bd = sdesc(sa + a_bytes, SWZ);
+#pragma unroll
+                for (int k = 0; k < BK / 16; k++) umma(tacc, ad + 2 * k, bd + 2 * k, idesc, (i | k) != 0);
+                umma_commit(&empty[s]);
+            }
+            umma_commit(accum);  // arrives once every MMA issued above is complete
+        }
+        __syncwarp();
+        // epilogue: warp w reads accumulator rows 32w + lane
+        mb_wait(accum, 0, g.err, dead);
+        __syncwarp();
+        tc_fence_after();
+        const int row = m0 + warp * 32 + lane;
+        for (int c = 0; c < BN; c += 16) {
+            __syncwarp();  // tcgen05.ld is warp-collective
+            uint32_t r[16];
+            tm_ld16(tacc + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, r);
+            if (row >= g.M || dead) continue;
+            float v[16];
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                v[j] = __uint_as_float(r[j]);
+                if (g.bias) v[j] += g.bias[n0 + c + j];
+                if (g.relu) v[j] = fmaxf(v[j], 0.0f);
+            }
+            const size_t o = (size_t)row * g.ldd + n0 + c;
+            if (g.mode == 0) {
+#pragma unroll
+                for (int j = 0; j < 16; j += 4) *(float4*)(g.d + o + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+            } else if (g.mode == 1) {
+#pragma unroll
+                for (int j = 0; j < 16; j++) atomicAdd(g.d + o + j, v[j]);
+            } else {
+                uint4 p0 = make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]),
+                                      pack_bf16(v[6], v[7]));
+                uint4 p1 = make_uint4(pack_bf16(v[8], v[9]), pack_bf16(v[10], v[11]), pack_bf16(v[12], v[13]),
+                                      pack_bf16(v[14], v[15]));
+                *(uint4*)(g.dh + o) = p0;
+                *(uint4*)(g.dh + o + 8) = p1;
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tm_dealloc(tacc, ncols);
+}
+
+// =====================================================================================
+// Implicit-GEMM convolution
+// =====================================================================================
+constexpr int CONV_STAGES = 3;
+
+struct ConvArgs {
+    const __nv_bfloat16* in;
+    __nv_bfloat16* out;
+    const float* bias;
+    int in_mb, out_mb, out_ld;
+    int nmb, hin, hout, stride;
+    unsigned* err;
+};
+
+// CIN = 2 (conv1: one k-block of 32, 64-byte rows) or 32 (five k-blocks of 64: two taps each).
+template <int CIN>
+__global__ void __launch_bounds__(128, 1) k_nn_conv(const __grid_constant__ CUtensorMap tw, ConvArgs a) {
+    constexpr int BK = CIN == 2 ? 32 : 64;
+    constexpr int SWZ = BK * 2;
+    constexpr int NKB = CIN == 2 ? 1 : 5;
+    constexpr int W_TILE = 32 * SWZ;   // one k-block of the weights: 32 rows
+    constexpr int A_TILE = 128 * SWZ;  // one k-block of the gathered operand
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* sm = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* sw = sm;                                           // NKB weight tiles
+    uint8_t* sa = sm + ((NKB * W_TILE + 1023) & ~1023);         // CONV_STAGES operand tiles
+    uint64_t* wfull = (uint64_t*)(sa + CONV_STAGES * A_TILE);
+    uint64_t* empty = wfull + 1;
+    uint64_t* accum = empty + CONV_STAGES;
+    uint32_t* slot = (uint32_t*)(accum + 1);
+    float* sbias = (float*)(slot + 4);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    if (tid == 0) {
+        mb_init(wfull, 1);
+        for (int s = 0; s < CONV_STAGES; s++) mb_init(&empty[s], 1);
+        mb_init(accum, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (tid < 32) sbias[tid] = a.bias[tid];
+    if (warp == 0) tm_alloc(slot, 32);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tacc = *slot;
+    bool dead = false;
+    if (tid == 0) {
+        mb_expect_tx(wfull, (unsigned)(NKB * W_TILE));
+        for (int kb = 0; kb < NKB; kb++) tma_2d(sw + kb * W_TILE, &tw, kb * BK, 0, wfull);
+    }
+    mb_wait(wfull, 0, a.err, dead);
+    const int pos = a.hout * a.hout;
+    const long long rows = (long long)a.nmb * pos;
+    const int ntiles = (int)((rows + 127) / 128);
+    const uint32_t idesc = idesc_bf16(128, 32);
+    int it = 0, nt = 0;
+    for (int tile = blockIdx.x; tile < ntiles && !dead; tile += gridDim.x, nt++) {
+        const long long m = (long long)tile * 128 + tid;
+        const bool valid = m < rows;
+        const int b = valid ? (int)(m / pos) : 0, p = valid ? (int)(m % pos) : 0;
+        const int oy = p / a.hout, ox = p % a.hout;
+        const __nv_bfloat16* inb = a.in + (size_t)b * a.in_mb;
+        for (int kb = 0; kb < NKB; kb++, it++) {
+            const int s = it % CONV_STAGES;
+            if (it >= CONV_STAGES && !mb_wait(&empty[s], ((it / CONV_STAGES) - 1) & 1, a.err, dead)) break;
+            uint8_t* rowp = sa + s * A_TILE + tid * SWZ;
+            if (CIN == 2) {
+                // k = tap * 2 + channel for the nine taps, zeros from k = 18
+                uint32_t w[16];
+#pragma unroll
+                for (int t = 0; t < 16; t++) w[t] = 0u;
+#pragma unroll
+                for (int t = 0; t < 9; t++) {
+                    const int iy = oy * a.stride + t / 3 - 1, ix = ox * a.stride + t % 3 - 1;
+                    if (valid && iy >= 0 && iy < a.hin && ix >= 0 && ix < a.hin)
+                        w[t] = *(const uint32_t*)(inb + ((size_t)iy * a.hin + ix) * 2);
+                }
+                const int x = (tid >> 1) & 3;
+#pragma unroll
+                for (int c = 0; c < 4; c++)
+                    *(uint4*)(rowp + ((c ^ x) << 4)) = make_uint4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]);
+            } else {
+                const int x = tid & 7;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int t = 2 * kb + h;
+                    const int iy = oy * a.stride + t / 3 - 1, ix = ox * a.stride + t % 3 - 1;
+                    const bool in = valid && t < 9 && iy >= 0 && iy < a.hin && ix >= 0 && ix < a.hin;
+                    const uint4* src = (const uint4*)(inb + ((size_t)(in ? iy : 0) * a.hin + (in ? ix : 0)) * 32);
+#pragma unroll
+                    for (int c = 0; c < 4; c++) {
+                        const uint4 v = in ? src[c] : make_uint4(0u, 0u, 0u, 0u);
+                        *(uint4*)(rowp + (((4 * h + c) ^ x) << 4)) = v;
+                    }
+                }
+            }
+            fence_async_smem();
+            tc_fence_before();
+            __syncthreads();
+            if (tid == 0) {
+                tc_fence_after();
+                const uint64_t ad = sdesc(s32(sa + s * A_TILE), SWZ), bd = sdesc(s32(sw + kb * W_TILE), SWZ);
+#pragma unroll
+                for (int k = 0; k < BK / 16; k++) umma(tacc, ad + 2 * k, bd + 2 * k, idesc, (kb | k) != 0);
+                umma_commit(&empty[s]);
+                if (kb == NKB - 1) umma_commit(accum);
+            }
+        }
+        if (dead) break;
+        // epilogue: bias, ReLU, bf16, one 64-byte output row per thread
+        mb_wait(accum, nt & 1, a.err, dead);
+        __syncwarp();  // tcgen05.ld is warp-collective
+        tc_fence_after();
+        uint32_t r0[16], r1[16];
+        tm_ld16(tacc + ((uint32_t)(warp * 32) << 16), r0);
+        tm_ld16(tacc + ((uint32_t)(warp * 32) << 16) + 16u, r1);
+        tc_fence_before();
+        if (valid && !dead) {
+            uint32_t o[16];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                o[j] = pack_bf16(fmaxf(__uint_as_float(r0[2 * j]) + sbias[2 * j], 0.0f),
+                                 fmaxf(__uint_as_float(r0[2 * j + 1]) + sbias[2 * j + 1], 0.0f));
+                o[8 + j] = pack_bf16(fmaxf(__uint_as_float(r1[2 * j]) + sbias[16 + 2 * j], 0.0f),
+                                     fmaxf(__uint_as_float(r1[2 * j + 1]) + sbias[16 + 2 * j + 1], 0.0f));
+            }
+            uint4* dst = (uint4*)(a.out + (size_t)b * a.out_mb + (size_t)p * a.out_ld);
+#pragma unroll
+            for (int c = 0; c < 4; c++) dst[c] = make_uint4(o[4 * c], o[4 * c + 1], o[4 * c + 2], o[4 * c + 3]);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tm_dealloc(tacc, 32);
+}
+
+// ---- host side: tensor maps
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    });
+    return fn;
+}
+
+// 2-D bf16 map over rows x cols (row pitch ld elements), box of `box_rows` rows x bk columns.
+bool make_map(CUtensorMap* m, const void* base, uint64_t rows, uint64_t cols, uint64_t ld, uint32_t box_rows,
+              uint32_t bk) {
+    auto fn = encode_fn();
+    if (!fn || ((uintptr_t)base & 15) || (ld * 2) % 16) return false;
+    cuuint64_t dims[2] = {cols, rows};
+    cuuint64_t strides[1] = {ld * 2};
+    cuuint32_t box[2] = {bk, box_rows};
+    cuuint32_t es[2] = {1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, bk == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+int num_sms() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+}  // namespace
+
+int nn_gemm(const void* A, int lda, const void* B, int ldb, void* D, int ldd, const float* bias, int M, int N, int K,
+            int bk, int mode, int relu, int ksplit, int ntile, unsigned* err, void* stream) {
+    if (M <= 0 || N <= 0 || K <= 0 || N % 16 || (bk != 64 && bk != 32) || ksplit < 1 || ntile < 16 || ntile > 256 ||
+        ntile % 16 || N % ntile || mode < 0 || mode > 2)
+        return (int)cudaErrorInvalidValue;
+    CUtensorMap ta, tb;
+    if (!make_map(&ta, A, (uint64_t)M, (uint64_t)K, (uint64_t)lda, 128, (uint32_t)bk) ||
+        !make_map(&tb, B, (uint64_t)N, (uint64_t)K, (uint64_t)ldb, (uint32_t)ntile, (uint32_t)bk))
+        return (int)cudaErrorInvalidValue;
+    GemmArgs g{};
+    g.M = M;
+    g.N = N;
+    g.nkb_total = (K + bk - 1) / bk;
+    g.kb_per_cta = (g.nkb_total + ksplit - 1) / ksplit;
+    const int splits = (g.nkb_total + g.kb_per_cta - 1) / g.kb_per_cta;  // every CTA gets >= 1 k-block
+    g.ntile = ntile;
+    g.d = (float*)D;
+    g.dh = (__nv_bfloat16*)D;
+    g.ldd = ldd;
+    g.bias = bias;
+    g.relu = relu;
+    g.mode = mode;
+    g.err = err;
+    const int stage = (128 * bk * 2 + ntile * bk * 2 + 1023) & ~1023;
+    const size_t smem = 1024 + (size_t)GEMM_STAGES * stage + 256;
+    const void* fn = bk == 64 ? (const void*)k_nn_gemm<64> : (const void*)k_nn_gemm<32>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    dim3 grid((M + 127) / 128, splits, N / ntile);
+    if (bk == 64)
+        k_nn_gemm<64><<<grid, 128, smem, (cudaStream_t)stream>>>(ta, tb, g);
+    else
+        k_nn_gemm<32><<<grid, 128, smem, (cudaStream_t)stream>>>(ta, tb, g);
+    return (int)cudaGetLastError();
+}
+
+int nn_conv(int layer, const void* in, int in_mb, const void* W, const float* bias, void* out, int out_mb, int out_ld,
+            int nmb, unsigned* err, void* stream) {
+    static const int HIN[5] = {0, 24, 12, 6, 6}, HOUT[5] = {0, 12, 6, 6, 3}, STRIDE[5] = {0, 2, 2, 1, 2};
+    if (layer < 1 || layer > 4 || nmb <= 0) return (int)cudaErrorInvalidValue;
+    const int cin = layer == 1 ? 2 : 32, bk = layer == 1 ? 32 : 64, k = layer == 1 ? nn::K1 : nn::KC;
+    CUtensorMap tw;
+    if (!make_map(&tw, W, 32, (uint64_t)k, (uint64_t)k, 32, (uint32_t)bk)) return (int)cudaErrorInvalidValue;
+    ConvArgs a{};
+    a.in = (const __nv_bfloat16*)in;
+    a.out = (__nv_bfloat16*)out;
+    a.bias = bias;
+    a.in_mb = in_mb;
+    a.out_mb = out_mb;
+    a.out_ld = out_ld;
+    a.nmb = nmb;
+    a.hin = HIN[layer];
+    a.hout = HOUT[layer];
+    a.stride = STRIDE[layer];
+    a.err = err;
+    const int nkb = cin == 2 ? 1 : 5;
+    const size_t smem = 1024 + (((size_t)nkb * 32 * bk * 2 + 1023) & ~(size_t)1023) + (size_t)CONV_STAGES * 128 * bk * 2 +
+                        256 + 128;
+    const void* fn = cin == 2 ? (const void*)k_nn_conv<2> : (const void*)k_nn_conv<32>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    const long long rows = (long long)nmb * a.hout * a.hout;
+    const int ntiles = (int)((rows + 127) / 128);
+    const int grid = ntiles < num_sms() ? ntiles : num_sms();
+    if (cin == 2)
+        k_nn_conv<2><<<grid, 128, smem, (cudaStream_t)stream>>>(tw, a);
+    else
+        k_nn_conv<32><<<grid, 128, smem, (cudaStream_t)stream>>>(tw, a);
+    return (int)cudaGetLastError();
+}
+
+// =====================================================================================
+// Network input: correlation volume, predictor prior map and predictor values
+// =====================================================================================
+// Per MB (one 128-thread CTA): the 64x64 reference window at (x0 - 24, y0 - 24) and the 16x16
+// current block, both averaged over 2x2 (rounded), coordinates clamped to the plane; the sum of
+// absolute differences of the 8x8 current block against the 32x32 window at the 24x24 offsets
+// (u, v) = half-resolution displacement (u - 12, v - 12) becomes channel 0, 1 - min(V, 2048) / 1024;
+// channel 1 marks the offsets the seven predictor MVs round to.  The predictor MVs come from the
+// previous P-frame's coded MVs around the MB (left, top, top-right, top-left, co-located, zero,
+// median of the first three; absent neighbours count as zero), in half-pel units / 64, written
+// to fc1's input row (columns 288 .. 303; 304 .. 319 zero).
+__device__ __forceinline__ int med3(int a, int b, int c) { return max(min(a, b), min(max(a, b), c)); }
+
+__global__ void __launch_bounds__(128) k_prop_features(const uint8_t* __restrict__ cur, const uint8_t* __restrict__ ref,
+                                                       int W, int H, const int8_t* __restrict__ prev_coded, int mb0,
+                                                       int nmb, __nv_bfloat16* __restrict__ feat,
+                                                       __nv_bfloat16* __restrict__ x1) {
+    __shared__ uint8_t R[32][33];
+    __shared__ uint8_t Cb[8][8];
+    __shared__ int pu[nn::NPRED], pv[nn::NPRED], ph[2 * nn::NPRED];
+    const int i = blockIdx.x;
+    if (i >= nmb) return;
+    const int mb = mb0 + i;
+    const int BW = W / 16, BH = H / 16;
+    const int bx = mb % BW, by = mb / BW, x0 = bx * 16, y0 = by * 16;
+    const int t = threadIdx.x;
+    for (int k = t; k < 32 * 32; k += 128) {
+        const int j = k >> 5, c = k & 31;
+        const int X = x0 - nn::WIN_OFF + 2 * c, Y = y0 - nn::WIN_OFF + 2 * j;
+        const int xa = min(max(X, 0), W - 1), xb = min(max(X + 1, 0), W - 1);
+        const int ya = min(max(Y, 0), H - 1), yb = min(max(Y + 1, 0), H - 1);
+        R[j][c] = (uint8_t)((ref[(size_t)ya * W + xa] + ref[(size_t)ya * W + xb] + ref[(size_t)yb * W + xa] +
+                             ref[(size_t)yb * W + xb] + 2) >> 2);
+    }
+    if (t < 64) {
+        const int j = t >> 3, c = t & 7;
+        const uint8_t* p = cur + (size_t)(y0 + 2 * j) * W + x0 + 2 * c;
+        Cb[j][c] = (uint8_t)((p[0] + p[1] + p[W] + p[W + 1] + 2) >> 2);
+    }
+    if (t == 0) {
+        int px[nn::NPRED] = {0}, py[nn::NPRED] = {0};
+        if (prev_coded) {
+            auto get = [&](int xx, int yy, int& hx, int& hy) {
+                if (xx < 0 || yy < 0 || xx >= BW || yy >= BH) { hx = hy = 0; return; }
+                const int8_t* c = prev_coded + 4 * ((size_t)yy * BW + xx);
+                hx = 2 * c[0] + c[2];
+                hy = 2 * c[1] + c[3];
+            };
+            get(bx - 1, by, px[0], py[0]);
+            get(bx, by - 1, px[1], py[1]);
+            get(bx + 1, by - 1, px[2], py[2]);
+            get(bx - 1, by - 1, px[3], py[3]);
+            get(bx, by, px[4], py[4]);
+            px[6] = med3(px[0], px[1], px[2]);
+            py[6] = med3(py[0], py[1], py[2]);
+        }
+        for (int k = 0; k < nn::NPRED; k++) {
+            // nearest half-resolution offset of the MV (half-pel units / 4, rounded half up)
+            pu[k] = ((px[k] + 2) >> 2) + 12;
+            pv[k] = ((py[k] + 2) >> 2) + 12;
+            ph[2 * k] = px[k];
+            ph[2 * k + 1] = py[k];
+        }
+    }
+    __syncthreads();
+    __nv_bfloat16* f = feat + (size_t)i * (nn::FEAT * nn::FEAT * 2);
+    for (int k = t; k < nn::FEAT * nn::FEAT; k += 128) {
+        const int v = k / nn::FEAT, u = k % nn::FEAT;
+        int sad = 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+#pragma unroll
+            for (int c = 0; c < 8; c++) sad += abs((int)Cb[j][c] - (int)R[v + j][u + c]);
+        const float f0 = 1.0f - (float)min(sad, 2048) * (1.0f / 1024.0f);
+        float f1 = 0.0f;
+#pragma unroll
+        for (int q = 0; q < nn::NPRED; q++)
+            if (pu[q] == u && pv[q] == v) f1 = 1.0f;
+        *(uint32_t*)(f + 2 * k) = pack_bf16(f0, f1);
+    }
+    if (t < 16) {
+        const float v = t < 2 * nn::NPRED ? (float)ph[t] * (1.0f / 64.0f) : 0.0f;
+        x1[(size_t)i * nn::F1 + 288 + t] = __float2bfloat16_rn(v);
+        x1[(size_t)i * nn::F1 + 304 + t] = __float2bfloat16_rn(0.0f);
+    }
+}
+
+// =====================================================================================
+// Training kernels
+// =====================================================================================
+// im2col^T of a 3x3 convolution: out[k][m] (k = tap * cin + channel, m = MB * hout^2 + position)
+// for k < 9 * cin; rows 9 * cin .. kpad - 1 are zero.  One thread per (k, m) pair, m fastest.
+__global__ void k_nn_im2col_t(const __nv_bfloat16* __restrict__ in, int in_mb, int cin, int hin, int hout, int stride,
+                              int nmb, int kpad, __nv_bfloat16* __restrict__ out) {
+    const long long M = (long long)nmb * hout * hout;
+    const long long n = M * kpad;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(idx / M);
+        const long long m = idx - (long long)k * M;
+        __nv_bfloat16 v = __float2bfloat16_rn(0.0f);
+        if (k < 9 * cin) {
+            const int tap = k / cin, c = k % cin;
+            const int b = (int)(m / (hout * hout)), p = (int)(m % (hout * hout));
+            const int iy = (p / hout) * stride + tap / 3 - 1, ix = (p % hout) * stride + tap % 3 - 1;
+            if (iy >= 0 && iy < hin && ix >= 0 && ix < hin) v = in[(size_t)b * in_mb + ((size_t)iy * hin + ix) * cin + c];
+        }
+        out[idx] = v;
+    }
+}
+
+// col2im of the input gradient of a 3x3 convolution (dcol: [m][kpad] f32, k = tap * 32 + channel),
+// times the ReLU derivative of the input activation (act, NHWC bf16 with per-MB stride act_mb),
+// written as bf16 in two layouts: dz[mi][32] (mi = MB * hin^2 + position) and dzt[32][Mi].
+__global__ void k_nn_col2im(const float* __restrict__ dcol, int kpad, int hin, int hout, int stride, int nmb,
+                            const __nv_bfloat16* __restrict__ act, int act_mb, __nv_bfloat16* __restrict__ dz,
+                            __nv_bfloat16* __restrict__ dzt) {
+    const long long Mi = (long long)nmb * hin * hin;
+    const long long n = Mi * 32;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
+        const long long mi = idx >> 5;
+        const int c = (int)(idx & 31);
+        const int b = (int)(mi / (hin * hin)), p = (int)(mi % (hin * hin));
+        const int iy = p / hin, ix = p % hin;
+        float g = 0.0f;
+        for (int tap = 0; tap < 9; tap++) {
+            const int ny = iy + 1 - tap / 3, nx = ix + 1 - tap % 3;  // = o * stride
+            if (ny < 0 || nx < 0 || ny % stride || nx % stride) continue;
+            const int oy = ny / stride, ox = nx / stride;
+            if (oy >= hout || ox >= hout) continue;
+            const long long m = (long long)b * hout * hout + oy * hout + ox;
+            g += dcol[m * kpad + tap * 32 + c];
+        }
+        const float a = __bfloat162float(act[(size_t)b * act_mb + (size_t)p * 32 + c]);
+        const float d = a > 0.0f ? g : 0.0f;
+        dz[idx] = __float2bfloat16_rn(d);
+        dzt[(size_t)c * Mi + mi] = __float2bfloat16_rn(d);
+    }
+}
+
+// ReLU derivative of a layer's output: d (f32) times (act > 0) (act bf16), as bf16 rows x n (dz)
+// and n x rows (dzt).  Rows come in groups of grp: row r, column c lies at
+// (r / grp) * ld + (r % grp) * n + c, with ld = ldd for d and lda for act (grp = 1: plain rows).
+__global__ void k_nn_relu_bwd(const float* __restrict__ d, int ldd, const __nv_bfloat16* __restrict__ act, int lda,
+                              int rows, int n, int grp, __nv_bfloat16* __restrict__ dz, __nv_bfloat16* __restrict__ dzt) {
+    const long long total = (long long)rows * n;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(idx / n), c = (int)(idx % n);
+        const int g = r / grp, q = r - g * grp;
+        const float a = __bfloat162float(act[(size_t)g * lda + (size_t)q * n + c]);
+        const float v = a > 0.0f ? d[(size_t)g * ldd + (size_t)q * n + c] : 0.0f;
+        dz[idx] = __float2bfloat16_rn(v);
+        dzt[(size_t)c * rows + r] = __float2bfloat16_rn(v);
+    }
+}
+
+// bf16 transpose: in rows x cols (pitch ld) -> out cols x rows.
+__global__ void k_nn_transpose(const __nv_bfloat16* __restrict__ in, int ld, int rows, int cols,
+                               __nv_bfloat16* __restrict__ out) {
+    __shared__ __nv_bfloat16 tile[32][33];
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int j = ty; j < 32; j += 8) {
+        const int r = r0 + j, c = c0 + tx;
+        if (r < rows && c < cols) tile[j][tx] = in[(size_t)r * ld + c];
+    }
+    __syncthreads();
+    for (int j = ty; j < 32; j += 8) {
+        const int c = c0 + j, r = r0 + tx;
+        if (r < rows && c < cols) out[(size_t)c * rows + r] = tile[tx][j];
+    }
+}
+
+// Column sums of a bf16 matrix (rows x n, pitch ld) added into out[n] (bias gradients).
+__global__ void k_nn_colsum(const __nv_bfloat16* __restrict__ z, int ld, long long rows, int n, float* __restrict__ out) {
+    const int c = threadIdx.x % n, lanes = blockDim.x / n;
+    float acc = 0.0f;
+    for (long long r = (long long)blockIdx.x * lanes + threadIdx.x / n; r < rows; r += (long long)gridDim.x * lanes)
+        acc += __bfloat162float(z[r * ld + c]);
+    if ((int)threadIdx.x < lanes * n) atomicAdd(out + c, acc);
+}
+
+// Loss of the head and its gradient.  o: rows x 16 f32 (fc3 output); target MV (half-pel) and
+// skip flag per row.  Candidates k = 0..3 are (o[2k], o[2k+1]) * 32 half-pel; each axis error is
+// a Huber loss with a one-half-pel knee; the closest candidate takes weight 1, the others 0.05;
+// the skip logit o[8] a logistic loss with weight 0.5.  Mean over the rows.  dout: rows x 32
+// bf16 (columns 16 .. 31 zero), doutt: 16 x rows bf16; loss_sum accumulates the summed loss.
+__global__ void k_nn_head_loss(const float* __restrict__ o, const int16_t* __restrict__ tmv,
+                               const uint8_t* __restrict__ tskip, int rows, __nv_bfloat16* __restrict__ dout,
+                               __nv_bfloat16* __restrict__ doutt, float* __restrict__ loss_sum) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.0f;
+    if (r < rows) {
+        const float* q = o + (size_t)r * 16;
+        const float tx = tmv[2 * r] * (1.0f / 32.0f), ty = tmv[2 * r + 1] * (1.0f / 32.0f);
+        const float dl = 1.0f / 32.0f;
+        float h[4], gx[4], gy[4];
+        int best = 0;
+        for (int k = 0; k < 4; k++) {
+            const float ex = q[2 * k] - tx, ey = q[2 * k + 1] - ty;
+            const float hx = fabsf(ex) < dl ? 0.5f * ex * ex / dl : fabsf(ex) - 0.5f * dl;
+            const float hy = fabsf(ey) < dl ? 0.5f * ey * ey / dl : fabsf(ey) - 0.5f * dl;
+            h[k] = hx + hy;
+            gx[k] = fabsf(ex) < dl ? ex / dl : (ex > 0.0f ? 1.0f : -1.0f);
+            gy[k] = fabsf(ey) < dl ? ey / dl : (ey > 0.0f ? 1.0f : -1.0f);
+            if (h[k] < h[best]) best = k;
+        }
+        const float z = q[8], y = tskip[r] ? 1.0f : 0.0f;
+        const float sg = 1.0f / (1.0f + __expf(-z));
+        const float bce = fmaxf(z, 0.0f) - z * y + log1pf(__expf(-fabsf(z)));
+        const float inv = 1.0f / (float)rows;
+        float g[16];
+        for (int k = 0; k < 16; k++) g[k] = 0.0f;
+        for (int k = 0; k < 4; k++) {
+            const float w = k == best ? 1.0f : 0.05f;
+            l += w * h[k];
+            g[2 * k] = w * gx[k] * inv;
+            g[2 * k + 1] = w * gy[k] * inv;
+        }
+        l += 0.5f * bce;
+        g[8] = 0.5f * (sg - y) * inv;
+        for (int k = 0; k < 16; k++) {
+            dout[(size_t)r * 32 + k] = __float2bfloat16_rn(g[k]);
+            dout[(size_t)r * 32 + 16 + k] = __float2bfloat16_rn(0.0f);
+            doutt[(size_t)k * rows + r] = __float2bfloat16_rn(g[k]);
+        }
+    }
+    for (int off = 16; off; off >>= 1) l += __shfl_xor_sync(0xffffffffu, l, off);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss_sum, l);
+}
+
+// AdamW over n parameters: f32 master weights p, gradients g (scaled by gscale), moments m, v;
+// bf16 copy pb (nullable).  Decoupled weight decay wd (applied where decay != 0).
+__global__ void k_nn_adamw(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                           float* __restrict__ v, __nv_bfloat16* __restrict__ pb, long long n, float lr, float b1,
+                           float b2, float eps, float wd, float c1, float c2, int decay) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi;
+        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        float w = p[i];
+        if (decay) w -= lr * wd * w;
+        w -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        p[i] = w;
+        if (pb) pb[i] = __float2bfloat16_rn(w);
+    }
+}
+
+// =====================================================================================
+// C ABI (device pointers; the network's training driver and tests call these)
+// =====================================================================================
+extern "C" {
+
+int riv_nn_gemm(const void* A, int lda, const void* B, int ldb, void* D, int ldd, const float* bias, int M, int N,
+                int K, int bk, int mode, int relu, int ksplit, int ntile, unsigned* err, void* stream) {
+    return nn_gemm(A, lda, B, ldb, D, ldd, bias, M, N, K, bk, mode, relu, ksplit, ntile, err, stream);
+}
+
+int riv_nn_conv(int layer, const void* in, int in_mb, const void* W, const float* bias, void* out, int out_mb,
+                int out_ld, int nmb, unsigned* err, void* stream) {
+    return nn_conv(layer, in, in_mb, W, bias, out, out_mb, out_ld, nmb, err, stream);
+}
+
+static int grid_for(long long n, int per = 256) {
+    long long g = (n + per - 1) / per;
+    return (int)(g < 148 * 32 ? (g < 1 ? 1 : g) : 148 * 32);
+}
+
+int riv_nn_features(const uint8_t* cur_y, const uint8_t* ref_y, int W, int H, const int8_t* prev_coded, int mb0,
+                    int nmb, void* feat, void* x1, void* stream) {
+    if (W <= 0 || H <= 0 || W % 16 || H % 16 || nmb <= 0 || mb0 < 0 || mb0 + nmb > (W / 16) * (H / 16))
+        return (int)cudaErrorInvalidValue;
+    k_prop_features<<<nmb, 128, 0, (cudaStream_t)stream>>>(cur_y, ref_y, W, H, prev_coded, mb0, nmb,
+                                                           (__nv_bfloat16*)feat, (__nv_bfloat16*)x1);
+    return (int)cudaGetLastError();
+}
+
+int riv_nn_im2col_t(int layer, const void* in, int in_mb, int nmb, void* out, void* stream) {
+    static const int HIN[5] = {0, 24, 12, 6, 6}, HOUT[5] = {0, 12, 6, 6, 3}, STRIDE[5] = {0, 2, 2, 1, 2};
+    if (layer < 1 || layer > 4 || nmb <= 0) return (int)cudaErrorInvalidValue;
+    const int cin = layer == 1 ? 2 : 32, kpad = layer == 1 ? nn::K1 : nn::KC;
+    const long long n = (long long)nmb * HOUT[layer] * HOUT[layer] * kpad;
+    k_nn_im2col_t<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)in, in_mb, cin, HIN[layer],
+                                                                 HOUT[layer], STRIDE[layer], nmb, kpad,
+                                                                 (__nv_bfloat16*)out);
+    return (int)cudaGetLastError();
+}
+
+int riv_nn_col2im(int layer, const float* dcol, int nmb, const void* act, int act_mb, void* dz, void* dzt,
+                  void* stream) {
+    static const int HIN[5] = {0, 24, 12, 6, 6}, HOUT[5] = {0, 12, 6, 6, 3}, STRIDE[5] = {0, 2, 2, 1, 2};
+    if (layer < 2 || layer > 4 || nmb <= 0) return (int)cudaErrorInvalidValue;
+    const long long n = (long long)nmb * HIN[layer] * HIN[layer] * 32;
+    k_nn_col2im<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(dcol, nn::KC, HIN[layer], HOUT[layer], STRIDE[layer], nmb,
+                                                               (const __nv_bfloat16*)act, act_mb, (__nv_bfloat16*)dz,
+                                                               (__nv_bfloat16*)dzt);
+    return (int)cudaGetLastError();
+}
+
+int riv_nn_relu_bwd(const float* d, int ldd, const void* act, int lda, int rows, int n, int grp, void* dz, void* dzt,
+                    void* stream) {
+    if (grp < 1 || n <= 0 || rows <= 0) return (int)cudaErrorInvalidValue;
+    k_nn_relu_bwd<<<grid_for((long long)rows * n), 256, 0, (cudaStream_t)stream>>>(
+        d, ldd, (const __nv_bfloat16*)act, lda, rows, n, grp, (__nv_bfloat16*)dz, (__nv_bfloat16*)dzt);
+    return (int)cudaGetLastError();
+}
+
+int riv_nn_transpose(const void* in, int ld, int rows, int cols, void* out, void* stream) {
+    dim3 grid((cols + 31) / 32, (rows + 31) / 32);
+    k_nn_transpose<<<grid, 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)in, ld, rows, cols,
+                                                          (__nv_bfloat16*)out);
+    return (int)cudaGetLastError();
+}
+
+int riv_nn_colsum(const void* z, int ld, long long rows, int n, float* out, void* stream) {
+    if (n <= 0 || n > 256) return (int)cudaErrorInvalidValue;
+    const int per = 256 / n * n;
+    k_nn_colsum<<<grid_for(rows, per / n), per, 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)z, ld, rows, n, out);
+    return (int)cudaGetLastError();
+}
+
+int riv_nn_head_loss(const float* o, const int16_t* tmv, const uint8_t* tskip, int rows, void* dout, void* doutt,
+                     float* loss_sum, void* stream) {
+    k_nn_head_loss<<<(rows + 127) / 128, 128, 0, (cudaStream_t)stream>>>(o, tmv, tskip, rows, (__nv_bfloat16*)dout,
+                                                                         (__nv_bfloat16*)doutt, loss_sum);
+    return (int)cudaGetLastError();
+}
+
+int riv_nn_adamw(float* p, const float* g, float* m, float* v, void* pb, long long n, float lr, float b1, float b2,
+                 float eps, float wd, int step, int decay, void* stream) {
+    const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+    k_nn_adamw<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(p, g, m, v, (__nv_bfloat16*)pb, n, lr, b1, b2, eps, wd,
+                                                             c1, c2, decay);
+    return (int)cudaGetLastError();
+}
+
+}  // extern "C"

@@ -269,12 +269,14 @@ def test_oracle_rejects_bad_config():
 
 def test_cabi_exports_every_declared_symbol():
     from riv2_b200 import encoder as E
-    header = open(os.path.join(ROOT, "include", "riv_gpu.h")).read()
-    declared = set(re.findall(r"\b(riv_\w+)\s*\(", header))
-    assert declared == set(E.EXPORTED_SYMBOLS)
-    L = E.lib()
-    for s in declared:
-        assert getattr(L, s) is not None
+    from riv2_b200 import proposal as P
+    for name, listed in (("riv_gpu.h", E.EXPORTED_SYMBOLS), ("riv_nn.h", P.EXPORTED_SYMBOLS)):
+        header = open(os.path.join(ROOT, "include", name)).read()
+        declared = set(re.findall(r"\b(riv_\w+)\s*\(", header))
+        assert declared == set(listed), name
+        L = E.lib()
+        for s in declared:
+            assert getattr(L, s) is not None
 
 
 def test_cabi_config_default_and_validation():
