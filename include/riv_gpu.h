@@ -53,8 +53,22 @@ typedef struct {
     int32_t device;          /* CUDA device ordinal */
     uint32_t pipeline_depth; /* frames in flight (0 = synchronous, like the reference) */
     uint32_t entropy_threads;/* host threads for the DCT-coefficient rANS coder (0 = auto) */
-    uint32_t _pad2[2];
+    /* Encode form (riv_encode_form; no counterpart in the reference, which has only the plain
+     * search).  The plain form reproduces the reference encoder byte for byte; the learned
+     * form seeds a parallel search with the proposal network (riv_encoder_set_proposal) and
+     * writes a different, equally valid stream.  proposal_margin: SAD margin above which a
+     * macroblock's proposals count as failed and it falls back to the hexagon search. */
+    uint32_t encode_form;
+    uint32_t proposal_margin;
 } riv_config;
+
+/* RIV_FORM_PLAIN: the reference's raster-order search (byte-identical streams).
+ * RIV_FORM_LEARNED: every MB searched at once from the proposal network's four candidates and
+ * the previous P-frame's MV predictors (short diamond + half-pel; hexagon search as fallback);
+ * mode decisions for all MBs at once.  Needs search_range <= 63 and riv_encoder_set_proposal.
+ * RIV_FORM_PARALLEL: the same parallel search without the network: every MB runs the hexagon
+ * search from its best predictor (the learned form's method without its network). */
+typedef enum { RIV_FORM_PLAIN = 0, RIV_FORM_LEARNED = 1, RIV_FORM_PARALLEL = 2 } riv_encode_form;
 
 /* EncoderConfig::new (enc/config.rs:56-77): defaults, storage rounded up to 16. */
 void riv_config_default(riv_config* cfg, uint32_t width, uint32_t height, uint32_t fps);
@@ -99,6 +113,15 @@ riv_status riv_encode_frame_yuv(riv_encoder* enc, const uint8_t* y, const uint8_
 /* Encoder::finish (enc/encoder.rs:950-961): drains, rewrites frame_count, flushes. */
 riv_status riv_finish(riv_encoder* enc);
 void riv_encoder_free(riv_encoder* enc);
+/* No counterpart in the reference.  Loads the proposal network's parameters for
+ * RIV_FORM_LEARNED: n = 146,592 f32 values (bf16-rounded weights of conv1..4, fc1..3, then
+ * their biases; the layout of riv_nn.h), as written by this library's trainer.  Call before
+ * the first P-frame; RIV_ERR_INVALID_CONFIG when n does not match. */
+riv_status riv_encoder_set_proposal(riv_encoder* enc, const float* params, size_t n);
+/* No counterpart in the reference.  Learned and parallel forms: P-frame MBs searched so far,
+ * MBs that fell back to the hexagon search, MBs that kept an unrefined whole-pixel candidate
+ * (the network's skip shortcut).  Synchronises the device. */
+riv_status riv_learned_counters(riv_encoder* enc, uint64_t* mbs, uint64_t* fallbacks, uint64_t* shortcuts);
 /* Message of the last failure ("" if none). */
 const char* riv_last_error(const riv_encoder* enc);
 uint64_t riv_frame_count(const riv_encoder* enc);

@@ -26,8 +26,10 @@
 #include <vector>
 
 #include "../../include/riv_gpu.h"
+#include "../../include/riv_nn.h"
 #include "riv_entropy.h"
 #include "riv_internal.h"
+#include "riv_nn.h"
 
 extern "C" int riv_upload_dct_tables(const int32_t* t16, const int32_t* t8);
 
@@ -399,6 +401,11 @@ struct riv_encoder {
     DevBuf tflag;           // fused table: per-MB "table row written" flags (frame tag)
     DevBuf rowdone;         // AQ inside the search: per-row "ln variances written" flags (frame tag)
     uint64_t h2d_bytes = 0, d2h_bytes = 0, pframes = 0, launches = 0, pdeferred = 0, ptimed = 0;
+    // learned / parallel forms: the proposal network's parameters (bf16 weights, f32 biases),
+    // its activations, the per-MB search result and the fallback / shortcut counters
+    bool learned = false, nn_loaded = false;
+    DevBuf nn_w, nn_b, nn_feat, nn_a1, nn_a2, nn_a3, nn_x1, nn_h1, nn_h2, nn_o, lmv, lcount;
+    uint64_t learned_mbs = 0;
 };
 
 namespace {
@@ -439,6 +446,11 @@ static riv_status validate(const riv_config& c, std::string& msg) {  // enc/conf
     }
     if (c.keyframe_mode > 2) { msg = "unknown keyframe mode"; return RIV_ERR_INVALID_CONFIG; }
     if (c.storage_width % 16 || c.storage_height % 16) { msg = "storage dimensions must be multiples of 16"; return RIV_ERR_INVALID_CONFIG; }
+    if (c.encode_form > RIV_FORM_PARALLEL) { msg = "unknown encode_form"; return RIV_ERR_INVALID_CONFIG; }
+    if (c.encode_form != RIV_FORM_PLAIN && c.search_range > 63) {
+        msg = "the learned and parallel forms need search_range <= 63";
+        return RIV_ERR_INVALID_CONFIG;
+    }
     return RIV_OK;
 }
 
@@ -533,7 +545,25 @@ static void setup_device(riv_encoder* e) {
     CK(search_plan(c.search_range, (int)c.storage_width, e->BH, e->table_ok, e->small_costs, &e->splan));
     if (e->splan.grid <= 0) throw std::runtime_error("search kernel cannot be made resident");
     // P-frame reconstruction folded into the next P-frame's search launch (its worker CTAs)
-    e->defer_ok = e->splan.fused && e->splan.fast && e->table_ok && c.pipeline_depth > 1;
+    e->learned = c.encode_form != RIV_FORM_PLAIN;
+    e->defer_ok = !e->learned && e->splan.fused && e->splan.fast && e->table_ok && c.pipeline_depth > 1;
+    if (e->learned) {
+        e->lmv.alloc((size_t)N * 8);
+        e->lcount.alloc(2 * sizeof(unsigned));
+        e->lcount.zero(e->S);
+    }
+    if (c.encode_form == RIV_FORM_LEARNED) {
+        e->nn_w.alloc(nn::ParamLayout::nweights * 2);
+        e->nn_b.alloc(nn::ParamLayout::nbias * 4);
+        e->nn_feat.alloc((size_t)N * nn::FEAT * nn::FEAT * 2 * 2);
+        e->nn_a1.alloc((size_t)N * 144 * 32 * 2);
+        e->nn_a2.alloc((size_t)N * 36 * 32 * 2);
+        e->nn_a3.alloc((size_t)N * 36 * 32 * 2);
+        e->nn_x1.alloc((size_t)N * nn::F1 * 2);
+        e->nn_h1.alloc((size_t)N * nn::HID * 2);
+        e->nn_h2.alloc((size_t)N * nn::HID * 2);
+        e->nn_o.alloc((size_t)N * nn::OUT * 4);
+    }
     if (e->splan.fused) {
         e->tflag.alloc((size_t)N * sizeof(unsigned));
         e->tflag.zero(e->S);
@@ -667,6 +697,31 @@ static void flush_pending(riv_encoder* e) {
                     e->fmaskb[e->pend.ck].as<uint8_t>(), e->pend.recon);
 }
 
+// The proposal network over every MB of a P-frame (learned form): network input, four
+// convolutions (implicit GEMM on tcgen05) and the three fully connected layers (TMA-fed
+// tcgen05 GEMMs), leaving 16 outputs per MB in nn_o.  Expired device waits set bit 0 of the
+// status word (RIV_ERR_DEVICE_TIMEOUT).
+static void proposal_forward(riv_encoder* e, const uint8_t* cur_y, const uint8_t* ref_y, const int8_t* prev_coded,
+                             cudaStream_t S) {
+    using PL = nn::ParamLayout;
+    const int N = e->NMB;
+    const uint16_t* W = e->nn_w.as<uint16_t>();
+    const float* B = e->nn_b.as<float>();
+    unsigned* err = e->status.as<unsigned>();
+    void *feat = e->nn_feat.p, *a1 = e->nn_a1.p, *a2 = e->nn_a2.p, *a3 = e->nn_a3.p, *x1 = e->nn_x1.p;
+    CK((cudaError_t)riv_nn_features(cur_y, ref_y, e->W, e->H, prev_coded, 0, N, feat, x1, S));
+    CK((cudaError_t)nn_conv(1, feat, nn::FEAT * nn::FEAT * 2, W + PL::w1, B, a1, 144 * 32, 32, N, err, S));
+    CK((cudaError_t)nn_conv(2, a1, 144 * 32, W + PL::w2, B + 32, a2, 36 * 32, 32, N, err, S));
+    CK((cudaError_t)nn_conv(3, a2, 36 * 32, W + PL::w3, B + 64, a3, 36 * 32, 32, N, err, S));
+    CK((cudaError_t)nn_conv(4, a3, 36 * 32, W + PL::w4, B + 96, x1, nn::F1, 32, N, err, S));
+    CK((cudaError_t)nn_gemm(x1, nn::F1, W + PL::f1, nn::F1, e->nn_h1.p, nn::HID, B + 128, N, nn::HID, nn::F1, 64, 2, 1,
+                            1, nn::HID, err, S));
+    CK((cudaError_t)nn_gemm(e->nn_h1.p, nn::HID, W + PL::f2, nn::HID, e->nn_h2.p, nn::HID, B + 256, N, nn::HID, nn::HID,
+                            64, 2, 1, 1, nn::HID, err, S));
+    CK((cudaError_t)nn_gemm(e->nn_h2.p, nn::HID, W + PL::f3, nn::HID, e->nn_o.p, nn::OUT, B + 384, N, nn::OUT, nn::HID,
+                            64, 0, 0, 1, nn::OUT, err, S));
+}
+
 // Enqueue the GPU work of one frame.  `src` = 0 host RGB, 1 device RGB, 2 host YUV.
 static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const void* b, const void* c3) {
     const riv_config& c = e->cfg;
@@ -775,7 +830,7 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         sp.wq = e->wq.as<unsigned>() + (size_t)e->wq_par * e->wq_words;
         sp.wq_next = e->wq.as<unsigned>() + (size_t)(e->wq_par ^ 1) * e->wq_words;
         sp.wq_words = e->wq_words;
-        if (e->table_ok) {
+        if (e->table_ok && !e->learned) {
             sp.tstride = sad_table_stride(c.search_range);
             sp.tab = e->sadtab.as<uint16_t>();
             if (e->splan.fused) sp.tflag = e->tflag.as<unsigned>();  // computed inside the search launch
@@ -786,7 +841,7 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         // coded MVs of this frame become next frame's temporal predictors
         const int cn = e->coded_cur ^ 1;
         sp.coded_out = e->coded[cn].as<int8_t>();
-        const bool aq_in_search = e->splan.fast && e->table_ok;
+        const bool aq_in_search = e->splan.fast && e->table_ok && !e->learned;
         if (aq_in_search) {  // prediction, variances and ln inside the search launch
             sp.pred = e->predb[ck].as<uint8_t>();
             sp.varsum = e->varsum.as<uint2>();
@@ -817,7 +872,18 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         }
         e->pend.active = false;
         CK(cudaStreamWaitEvent(S, e->ev_mbout_free[ck], 0));  // compaction of the frame NPAR back
-        CK(launch_search(sp, e->splan, S));
+        if (e->learned) {
+            if (c.encode_form == RIV_FORM_LEARNED) {
+                if (!e->nn_loaded) throw std::runtime_error("learned form: no proposal network loaded (riv_encoder_set_proposal)");
+                proposal_forward(e, cur, sp.ref_y, sp.prev_coded, S);
+            }
+            e->launches += (c.encode_form == RIV_FORM_LEARNED ? 8 : 0) + 2;
+            CK((cudaError_t)launch_learned(sp, c.encode_form == RIV_FORM_LEARNED ? e->nn_o.as<float>() : nullptr,
+                                           (int)c.proposal_margin, 2.2f, e->lmv.p, e->lcount.as<unsigned>(), S));
+            e->learned_mbs += (uint64_t)N;
+        } else {
+            CK(launch_search(sp, e->splan, S));
+        }
         e->wq_par ^= 1;
         mark(e, j, EV_SEARCH, S);
         CK(cudaEventRecord(e->ev_search_done, S));
@@ -1210,6 +1276,47 @@ riv_status riv_encoder_new(const riv_config* cfg, const riv_writer_vtable* write
     return RIV_OK;
 }
 
+riv_status riv_encoder_set_proposal(riv_encoder* e, const float* params, size_t n) {
+    using PL = nn::ParamLayout;
+    if (!e || !params) return RIV_ERR_INVALID_CONFIG;
+    if (e->cfg.encode_form != RIV_FORM_LEARNED) return fail(e, RIV_ERR_INVALID_CONFIG, "encoder is not in the learned form");
+    if (n != PL::nweights + PL::nbias) return fail(e, RIV_ERR_INVALID_CONFIG, "proposal parameters: wrong count");
+    if (e->poisoned) return poisoned_status(e);
+    std::vector<uint16_t> wb(PL::nweights);
+    for (size_t i = 0; i < PL::nweights; i++) {  // round to the nearest bf16, ties to even
+        uint32_t u;
+        memcpy(&u, params + i, 4);
+        wb[i] = (uint16_t)((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);
+    }
+    try {
+        CK(cudaSetDevice(e->cfg.device));
+        CK(cudaMemcpy(e->nn_w.p, wb.data(), wb.size() * 2, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(e->nn_b.p, params + PL::nweights, PL::nbias * 4, cudaMemcpyHostToDevice));
+    } catch (const CudaError& ce) {
+        return fail(e, RIV_ERR_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
+    }
+    e->nn_loaded = true;
+    return RIV_OK;
+}
+
+riv_status riv_learned_counters(riv_encoder* e, uint64_t* mbs, uint64_t* fallbacks, uint64_t* shortcuts) {
+    if (!e || !mbs || !fallbacks || !shortcuts) return RIV_ERR_INVALID_CONFIG;
+    *mbs = *fallbacks = *shortcuts = 0;
+    if (!e->learned) return RIV_OK;
+    unsigned h[2] = {0, 0};
+    try {
+        CK(cudaSetDevice(e->cfg.device));
+        CK(cudaStreamSynchronize(e->S));
+        CK(cudaMemcpy(h, e->lcount.p, sizeof(h), cudaMemcpyDeviceToHost));
+    } catch (const CudaError& ce) {
+        return fail(e, RIV_ERR_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
+    }
+    *mbs = e->learned_mbs;
+    *fallbacks = h[0];
+    *shortcuts = h[1];
+    return RIV_OK;
+}
+
 riv_status riv_encode_frame(riv_encoder* e, const uint8_t* rgb, uint32_t w, uint32_t h, uint64_t ts,
                             riv_frame_stats* stats) {
     if (!e) return RIV_ERR_INVALID_CONFIG;
@@ -1298,7 +1405,9 @@ void riv_encoder_free(riv_encoder* e) {
             b->release();
     DevBuf* bufs[] = {&e->ref[0], &e->ref[1], &e->recon_pre, &e->wq, &e->coded[0], &e->coded[1], &e->rec,
                       &e->varsum, &e->qs, &e->status,
-                      &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset, &e->lcindex, &e->lcoffset, &e->sadtab, &e->prof, &e->tflag, &e->rowdone, &e->newcost, &e->newcost32};
+                      &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset, &e->lcindex, &e->lcoffset, &e->sadtab, &e->prof, &e->tflag, &e->rowdone, &e->newcost, &e->newcost32,
+                      &e->nn_w, &e->nn_b, &e->nn_feat, &e->nn_a1, &e->nn_a2, &e->nn_a3, &e->nn_x1, &e->nn_h1, &e->nn_h2,
+                      &e->nn_o, &e->lmv, &e->lcount};
     for (DevBuf* b : bufs) b->release();
     if (e->S) cudaStreamDestroy(e->S);
     if (e->C) cudaStreamDestroy(e->C);

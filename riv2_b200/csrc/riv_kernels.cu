@@ -965,6 +965,83 @@ __device__ __forceinline__ bool rec_wait(const unsigned long long* rp, unsigned 
     return true;
 }
 
+// RDO skip (enc/rdo.rs:140-178) and the MV mode decision of one MB on its coded neighbours
+// (enc/encoder.rs:459-733, res/mv_predictor.rs:59-272): mode, NEW base and raw delta, flags
+// and the coded (reconstructed) MV.
+struct MbDecision {
+    MvT coded;
+    int mode, chosen, rdx, rdy;
+    uint8_t flags;
+    bool rdo_skip;
+};
+__device__ __forceinline__ MbDecision decide_mb(const SearchParams& p, const MvT& raw, long long best_sad, bool has_l,
+                                                bool has_t, bool has_tr, bool has_tl, bool has_tm, const MvT& L_cod,
+                                                const MvT& cT, const MvT& cTR, const MvT& cTL, const MvT& Tm_cod) {
+    // ---- RDO skip decision (enc/rdo.rs:140-178)
+    bool int_al = raw.sx == 0 && raw.sy == 0;
+    double satd = (double)best_sad;
+    double skip_cost = __dadd_rn(satd, __dmul_rn(p.rdo_lambda, p.rdo_skip_bits));
+    double est = __dadd_rn(p.rdo_icpt, __dmul_rn(p.rdo_slope, satd));
+    if (est < 0.0) est = 0.0;
+    double coded_cost = __dadd_rn(__dmul_rn(satd, p.rdo_ret), __dmul_rn(p.rdo_lambda, __dadd_rn(p.rdo_keep_bits, est)));
+    bool rdo_skip = p.rdo_allow && int_al && !(satd > p.rdo_guard) && (skip_cost <= coded_cost);
+
+    // ---- mode decision on the coded neighbours
+    const MvT zero{0, 0, 0, 0};
+    MvT nearest = zero, nearm = zero;
+    {
+        const MvT CS[5] = {L_cod, cT, cTR, cTL, Tm_cod};
+        const bool PV[5] = {has_l, has_t, has_tr, has_tl, has_tm};
+        int nu = 0;
+#pragma unroll
+        for (int i = 0; i < 5; i++) {
+            bool take = PV[i] && (nu == 0 || (nu == 1 && !mv_eq(CS[i], nearest)));
+            if (take && nu == 0) nearest = CS[i];
+            else if (take && nu == 1) nearm = CS[i];
+            nu += take ? 1 : 0;
+        }
+    }
+    MvT temporal = has_tm ? Tm_cod : zero;
+    const int mx = raw.dx * 2 + raw.sx, my = raw.dy * 2 + raw.sy;
+    auto hpeq = [&](const MvT& t) { return mx == t.dx * 2 + t.sx && my == t.dy * 2 + t.sy; };
+    int mode;
+    if (raw.dx == 0 && raw.dy == 0 && raw.sx == 0 && raw.sy == 0) mode = 0;  // Zero
+    else if (hpeq(nearest)) mode = 1;
+    else if (hpeq(nearm)) mode = 2;
+    else if (has_tr && hpeq(cTR)) mode = 3;
+    else if (has_tl && hpeq(cTL)) mode = 4;
+    else if (hpeq(temporal)) mode = 6;
+    else mode = 5;  // New
+    int chosen = 0, rdx = 0, rdy = 0;
+    MvT coded = raw;
+    if (mode == 5) {
+        const MvT bases[5] = {nearest, nearm, cTR, cTL, temporal};
+        const bool hasb[5] = {true, true, has_tr, has_tl, true};
+        const int selbits[5] = {1, 2, 3, 4, 4};
+        unsigned best = 0xffffffffu;
+        int bbx = nearest.dx, bby = nearest.dy;
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            if (!hasb[k]) continue;
+            int ddx = sat8(raw.dx - bases[k].dx), ddy = sat8(raw.dy - bases[k].dy);
+            unsigned cst = (unsigned)(selbits[k] + comp_bits(ddx) + comp_bits(ddy));
+            if (cst < best) { best = cst; chosen = k; bbx = bases[k].dx; bby = bases[k].dy; }
+        }
+        rdx = sat8(raw.dx - bbx);
+        rdy = sat8(raw.dy - bby);
+        coded.dx = sat8(bbx + rdx);
+        coded.dy = sat8(bby + rdy);
+    } else if (mode == 1) coded = nearest;
+    else if (mode == 2) coded = nearm;
+    else if (mode == 3) coded = cTR;
+    else if (mode == 4) coded = cTL;
+    else if (mode == 6) coded = temporal;
+    uint8_t flags = 0;
+    if (mode == 5) flags = (raw.sx == 1 ? 0x01 : 0) | (raw.sy == 1 ? 0x04 : 0);
+    if (rdo_skip) flags |= 0x40;
+    return MbDecision{coded, mode, chosen, rdx, rdy, flags, rdo_skip};
+}
+
 // The second warp of each row CTA: RDO skip (enc/rdo.rs:140-178) and the MV mode decision on
 // the coded (reconstructed) neighbours (enc/encoder.rs:459-733, res/mv_predictor.rs:59-272)
 // for the MBs the search warp hands over, in raster order.  It publishes the coded-MV records
@@ -1015,70 +1092,14 @@ __device__ __forceinline__ void mode_warp(const SearchParams& p, const unsigned 
                 Tm_cod = MvT{pc.x, pc.y, pc.z, pc.w};
             }
 
-            // ---- RDO skip decision (enc/rdo.rs:140-178)
-            bool int_al = raw.sx == 0 && raw.sy == 0;
-            double satd = (double)best_sad;
-            double skip_cost = __dadd_rn(satd, __dmul_rn(p.rdo_lambda, p.rdo_skip_bits));
-            double est = __dadd_rn(p.rdo_icpt, __dmul_rn(p.rdo_slope, satd));
-            if (est < 0.0) est = 0.0;
-            double coded_cost = __dadd_rn(__dmul_rn(satd, p.rdo_ret), __dmul_rn(p.rdo_lambda, __dadd_rn(p.rdo_keep_bits, est)));
-            bool rdo_skip = p.rdo_allow && int_al && !(satd > p.rdo_guard) && (skip_cost <= coded_cost);
-
-            // ---- mode decision on the coded neighbours
-            MvT cT = has_t ? rec_cod(vT) : MvT{0, 0, 0, 0}, cTR = has_tr ? rec_cod(vTR) : MvT{0, 0, 0, 0},
-                cTL = has_tl ? rec_cod(vTL) : MvT{0, 0, 0, 0};
-            const MvT zero{0, 0, 0, 0};
-            MvT nearest = zero, nearm = zero;
-            {
-                const MvT CS[5] = {L_cod, cT, cTR, cTL, Tm_cod};
-                const bool PV[5] = {has_l, has_t, has_tr, has_tl, has_tm};
-                int nu = 0;
-#pragma unroll
-                for (int i = 0; i < 5; i++) {
-                    bool take = PV[i] && (nu == 0 || (nu == 1 && !mv_eq(CS[i], nearest)));
-                    if (take && nu == 0) nearest = CS[i];
-                    else if (take && nu == 1) nearm = CS[i];
-                    nu += take ? 1 : 0;
-                }
-            }
-            MvT temporal = has_tm ? Tm_cod : zero;
-            const int mx = raw.dx * 2 + raw.sx, my = raw.dy * 2 + raw.sy;
-            auto hpeq = [&](const MvT& t) { return mx == t.dx * 2 + t.sx && my == t.dy * 2 + t.sy; };
-            int mode;
-            if (raw.dx == 0 && raw.dy == 0 && raw.sx == 0 && raw.sy == 0) mode = 0;  // Zero
-            else if (hpeq(nearest)) mode = 1;
-            else if (hpeq(nearm)) mode = 2;
-            else if (has_tr && hpeq(cTR)) mode = 3;
-            else if (has_tl && hpeq(cTL)) mode = 4;
-            else if (hpeq(temporal)) mode = 6;
-            else mode = 5;  // New
-            int chosen = 0, rdx = 0, rdy = 0;
-            MvT coded = raw;
-            if (mode == 5) {
-                const MvT bases[5] = {nearest, nearm, cTR, cTL, temporal};
-                const bool hasb[5] = {true, true, has_tr, has_tl, true};
-                const int selbits[5] = {1, 2, 3, 4, 4};
-                unsigned best = 0xffffffffu;
-                int bbx = nearest.dx, bby = nearest.dy;
-#pragma unroll
-                for (int k = 0; k < 5; k++) {
-                    if (!hasb[k]) continue;
-                    int ddx = sat8(raw.dx - bases[k].dx), ddy = sat8(raw.dy - bases[k].dy);
-                    unsigned cst = (unsigned)(selbits[k] + comp_bits(ddx) + comp_bits(ddy));
-                    if (cst < best) { best = cst; chosen = k; bbx = bases[k].dx; bby = bases[k].dy; }
-                }
-                rdx = sat8(raw.dx - bbx);
-                rdy = sat8(raw.dy - bby);
-                coded.dx = sat8(bbx + rdx);
-                coded.dy = sat8(bby + rdy);
-            } else if (mode == 1) coded = nearest;
-            else if (mode == 2) coded = nearm;
-            else if (mode == 3) coded = cTR;
-            else if (mode == 4) coded = cTL;
-            else if (mode == 6) coded = temporal;
-            uint8_t flags = 0;
-            if (mode == 5) flags = (raw.sx == 1 ? 0x01 : 0) | (raw.sy == 1 ? 0x04 : 0);
-            if (rdo_skip) flags |= 0x40;
+            const MbDecision md = decide_mb(p, raw, best_sad, has_l, has_t, has_tr, has_tl, has_tm, L_cod,
+                                             has_t ? rec_cod(vT) : MvT{0, 0, 0, 0},
+                                             has_tr ? rec_cod(vTR) : MvT{0, 0, 0, 0},
+                                             has_tl ? rec_cod(vTL) : MvT{0, 0, 0, 0}, Tm_cod);
+            const MvT coded = md.coded;
+            const int mode = md.mode, chosen = md.chosen, rdx = md.rdx, rdy = md.rdy;
+            const uint8_t flags = md.flags;
+            const bool rdo_skip = md.rdo_skip;
 
             RIV_STAMP(5);
             // ---- publish
@@ -2554,6 +2575,281 @@ int launch_search(const SearchParams& p, const SearchPlan& plan, void* stream) {
     cudaError_t e = cudaLaunchCooperativeKernel(search_fn(band, table, table && p.small), dim3(plan.grid),
                                                 dim3(plan.threads), args, plan.smem, (cudaStream_t)stream);
     return (int)e;
+}
+
+// ---------------------------------------------------------------------------------
+// Learned-proposal form: a parallel search seeded by the proposal network, and the mode
+// decision of every MB in parallel.
+//
+// No MB waits for another.  Each MB's search uses, as predictors and as the basis of its MV
+// cost (estimate_mv_cost, enc/motion/scalar.rs:453-544), the previous P-frame's coded MVs
+// around it (left, top, top-right, top-left, co-located, zero, median of the first three)
+// instead of the current frame's neighbours, so every MB can be searched at once.
+//   candidates: the network's four proposals (rounded to whole pixels) and the predictors;
+//   refinement: small-diamond rounds from the best candidate, then the nine half-pel
+//   positions around it (floor-averaged samples, as the plain search scores them, with the
+//   fractional penalty of refine_halfpel, enc/motion/scalar.rs:759-839);
+//   fallback: when the best proposal's SAD exceeds the best predictor's SAD by more than
+//   `margin`, the hexagon search of process_block_hex (enc/motion/scalar.rs:546-636) from
+//   the best candidate instead of the short diamond;
+//   shortcut: an MB whose skip probability exceeds `skip_prob` keeps its best whole-pixel
+//   candidate without refinement.
+// Every MV stays within +-search range (<= 63), so a NEW delta never saturates and each MB's
+// coded MV equals its search MV: the mode decision then needs only the neighbours' search
+// MVs, and runs for all MBs at once (k_learned_mode).
+// ---------------------------------------------------------------------------------
+constexpr int LS_MBS = 4;  // MBs (warps) per CTA: consecutive MBs of one row
+
+struct LearnedMv {
+    int8_t raw[4];  // dx, dy, sx, sy (canonical)
+    int32_t sad;    // SAD of the chosen position (half-pel SAD when fractional)
+};
+static_assert(sizeof(LearnedMv) == 8, "LearnedMv layout");
+
+struct LearnedParams {
+    SearchParams sp;
+    const float* net;  // per MB 16 network outputs (nullptr: predictors only, every MB refined by the hexagon search)
+    int margin;
+    float skip_logit;  // shortcut when the skip logit exceeds this (a probability threshold, as a logit)
+    LearnedMv* out;
+    unsigned* counters;  // [0] fallbacks to the hexagon search, [1] shortcuts
+};
+
+// SAD of the 16x16 block at whole-pixel offset (dx, dy) over the window; lane l covers row l/2,
+// eight pixels, current samples in c0, c1.
+__device__ __forceinline__ unsigned ls_sad(const uint8_t* win, int ws, int ox, int oy, int dx, int dy, int lane,
+                                           uint32_t c0, uint32_t c1) {
+    const uint8_t* r = win + (oy + (lane >> 1) + dy) * ws + ox + (lane & 1) * 8 + dx;
+    const unsigned s = __vsadu4(lds_u32(r), c0) + __vsadu4(lds_u32(r + 4), c1);
+    return __reduce_add_sync(0xffffffffu, s);
+}
+// SAD at half-pel offset (hx, hy) with floor-averaged samples.
+__device__ __forceinline__ unsigned ls_sad_hp(const uint8_t* win, int ws, int ox, int oy, int hx, int hy, int lane,
+                                              uint32_t c0, uint32_t c1) {
+    const int ix = hx >> 1, iy = hy >> 1, fx = hx & 1, fy = hy & 1;
+    const uint8_t* r = win + (oy + (lane >> 1) + iy) * ws + ox + (lane & 1) * 8 + ix;
+    uint32_t a0 = lds_u32(r), a1 = lds_u32(r + 4);
+    if (fx && fy) {
+        a0 = favg4(a0, lds_u32(r + 1), lds_u32(r + ws), lds_u32(r + ws + 1));
+        a1 = favg4(a1, lds_u32(r + 5), lds_u32(r + ws + 4), lds_u32(r + ws + 5));
+    } else if (fx) {
+        a0 = favg(a0, lds_u32(r + 1));
+        a1 = favg(a1, lds_u32(r + 5));
+    } else if (fy) {
+        a0 = favg(a0, lds_u32(r + ws));
+        a1 = favg(a1, lds_u32(r + ws + 4));
+    }
+    const unsigned s = __vsadu4(a0, c0) + __vsadu4(a1, c1);
+    return __reduce_add_sync(0xffffffffu, s);
+}
+
+__global__ void __launch_bounds__(32 * LS_MBS) k_learned_search(LearnedParams lp) {
+    const SearchParams& p = lp.sp;
+    extern __shared__ __align__(16) uint8_t lsm[];
+    const int sr = p.sr, M = sr + 2;
+    const int bx0 = blockIdx.x * LS_MBS, by = blockIdx.y;
+    const int nmb_here = min(LS_MBS, p.BW - bx0);
+    const int wx0 = bx0 * 16 - M, wy0 = by * 16 - M;
+    const int ws = ((16 * LS_MBS + 2 * M + 3) & ~3) + 4, wh = 16 + 2 * M + 1;
+    // stage the window with coordinates clamped to the plane (replicated borders)
+    for (int i = threadIdx.x; i < ws * wh; i += blockDim.x) {
+        const int y = i / ws, x = i - y * ws;
+        const int fy = min(max(wy0 + y, 0), p.H - 1), fx = min(max(wx0 + x, 0), p.W - 1);
+        lsm[i] = p.ref_y[(size_t)fy * p.W + fx];
+    }
+    __syncthreads();
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (w >= nmb_here) return;
+    const int bx = bx0 + w, mb = by * p.BW + bx;
+    const int x0 = bx * 16, y0 = by * 16;
+    const int ox = x0 - wx0, oy = y0 - wy0;
+    // this lane's 8 current samples
+    const uint8_t* cp = p.cur_y + (size_t)(y0 + (lane >> 1)) * p.W + x0 + (lane & 1) * 8;
+    const uint32_t c0 = *(const uint32_t*)cp, c1 = *(const uint32_t*)(cp + 4);
+    // predictors from the previous P-frame's coded MVs (whole-pixel parts, within +-sr)
+    int px[7] = {0, 0, 0, 0, 0, 0, 0}, py[7] = {0, 0, 0, 0, 0, 0, 0};
+    bool av[5] = {false, false, false, false, false};
+    if (p.prev_coded) {
+        const int nx[5] = {bx - 1, bx, bx + 1, bx - 1, bx}, ny[5] = {by, by - 1, by - 1, by - 1, by};
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            if (nx[k] < 0 || ny[k] < 0 || nx[k] >= p.BW || ny[k] >= p.BH) continue;
+            const char4 c = *(const char4*)(p.prev_coded + 4 * ((size_t)ny[k] * p.BW + nx[k]));
+            px[k] = min(max((int)c.x, -sr), sr);
+            py[k] = min(max((int)c.y, -sr), sr);
+            av[k] = true;
+        }
+        px[6] = median3(px[0], px[1], px[2]);
+        py[6] = median3(py[0], py[1], py[2]);
+    }
+    // cost basis: nearest / near = first two distinct available predictors, median of L, T, TR
+    CostCtx cc{0, 0, 0, 0, px[6], py[6]};
+    {
+        int nu = 0;
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            if (!av[k]) continue;
+            if (nu == 0) { cc.nx = px[k]; cc.ny = py[k]; nu = 1; }
+            else if (nu == 1 && (px[k] != cc.nx || py[k] != cc.ny)) { cc.rx = px[k]; cc.ry = py[k]; nu = 2; }
+        }
+    }
+    auto cost = [&](int dx, int dy, unsigned sad) { return (long long)sad + mv_cost<false>(dx, dy, cc, p, p.mvbits, nullptr); };
+    // candidates: 4 proposals, then the 7 predictors
+    int cx[11], cy[11];
+    int ncand = 0;
+    bool shortcut = false;
+    if (lp.net) {
+        const float* o = lp.net + (size_t)mb * 16;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const float hx = o[2 * k] * 32.0f, hy = o[2 * k + 1] * 32.0f;  // half-pel units
+            cx[k] = min(max(__float2int_rn(hx * 0.5f), -sr), sr);
+            cy[k] = min(max(__float2int_rn(hy * 0.5f), -sr), sr);
+        }
+        ncand = 4;
+        shortcut = o[8] > lp.skip_logit;
+    }
+    const int npro = ncand;
+#pragma unroll
+    for (int k = 0; k < 7; k++) { cx[ncand + k] = px[k]; cy[ncand + k] = py[k]; }
+    ncand += 7;
+    long long best = LLONG_MAX, bestp = LLONG_MAX, bestq = LLONG_MAX;
+    unsigned bsad = 0, bsp = 0xffffffffu, bsq = 0xffffffffu;
+    int bdx = 0, bdy = 0;
+    for (int k = 0; k < ncand; k++) {
+        const unsigned sad = ls_sad(lsm, ws, ox, oy, cx[k], cy[k], lane, c0, c1);
+        const long long c = cost(cx[k], cy[k], sad);
+        if (k < npro) bsp = min(bsp, sad); else bsq = min(bsq, sad);
+        if (c < best) { best = c; bsad = sad; bdx = cx[k]; bdy = cy[k]; }
+    }
+    (void)bestp; (void)bestq;
+    const bool fallback = !lp.net || bsp > bsq + (unsigned)lp.margin;
+    if (fallback) shortcut = false;
+    if (!shortcut) {
+        // whole-pixel refinement: hexagon rounds (fallback) then small-diamond rounds
+        const int HX[6] = {2, 1, -1, -2, -1, 1}, HY[6] = {0, 2, 2, 0, -2, -2};
+        const int DX[4] = {1, -1, 0, 0}, DY[4] = {0, 0, 1, -1};
+        if (fallback) {
+            for (int round = 0; round < 64; round++) {
+                int nbx = bdx, nby = bdy;
+                long long nb = best;
+                unsigned ns = bsad;
+#pragma unroll
+                for (int k = 0; k < 6; k++) {
+                    const int dx = bdx + HX[k], dy = bdy + HY[k];
+                    if (dx < -sr || dx > sr || dy < -sr || dy > sr) continue;
+                    const unsigned sad = ls_sad(lsm, ws, ox, oy, dx, dy, lane, c0, c1);
+                    const long long c = cost(dx, dy, sad);
+                    if (c < nb) { nb = c; ns = sad; nbx = dx; nby = dy; }
+                }
+                if (nbx == bdx && nby == bdy) break;
+                best = nb; bsad = ns; bdx = nbx; bdy = nby;
+            }
+        }
+        for (int round = 0; round < (fallback ? 64 : 8); round++) {
+            int nbx = bdx, nby = bdy;
+            long long nb = best;
+            unsigned ns = bsad;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int dx = bdx + DX[k], dy = bdy + DY[k];
+                if (dx < -sr || dx > sr || dy < -sr || dy > sr) continue;
+                const unsigned sad = ls_sad(lsm, ws, ox, oy, dx, dy, lane, c0, c1);
+                const long long c = cost(dx, dy, sad);
+                if (c < nb) { nb = c; ns = sad; nbx = dx; nby = dy; }
+            }
+            if (nbx == bdx && nby == bdy) break;
+            best = nb; bsad = ns; bdx = nbx; bdy = nby;
+        }
+    }
+    // half-pel refinement around the whole-pixel best (the centre with no penalty)
+    int hx = 2 * bdx, hy = 2 * bdy;
+    unsigned hsad = bsad;
+    if (!shortcut) {
+        hsad = ls_sad_hp(lsm, ws, ox, oy, hx, hy, lane, c0, c1);
+        long long hbest = hsad;
+        int bhx = hx, bhy = hy;
+        for (int sy = -1; sy <= 1; sy++)
+            for (int sx = -1; sx <= 1; sx++) {
+                if (!sx && !sy) continue;
+                const unsigned sad = ls_sad_hp(lsm, ws, ox, oy, hx + sx, hy + sy, lane, c0, c1);
+                const long long c = (long long)sad + p.c15;
+                if (c < hbest) { hbest = c; bhx = hx + sx; bhy = hy + sy; hsad = sad; }
+            }
+        hx = bhx;
+        hy = bhy;
+    }
+    if (lane == 0) {
+        // canonical form: a -1/2 component becomes +1/2 of the whole pixel below
+        LearnedMv r;
+        r.raw[0] = (int8_t)(hx >> 1);
+        r.raw[1] = (int8_t)(hy >> 1);
+        r.raw[2] = (int8_t)(hx & 1);
+        r.raw[3] = (int8_t)(hy & 1);
+        r.sad = (int32_t)hsad;
+        lp.out[mb] = r;
+        if (fallback && lp.net) atomicAdd(lp.counters, 1u);
+        if (shortcut) atomicAdd(lp.counters + 1, 1u);
+    }
+}
+
+// Mode decision of every MB at once (coded MV = search MV, see above): RDO skip, mode, NEW base
+// and delta through decide_mb, the same routine the wavefront's mode warp runs.
+__global__ void __launch_bounds__(128) k_learned_mode(SearchParams p, const LearnedMv* __restrict__ lm) {
+    const int mb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mb >= p.BW * p.BH) return;
+    const int bx = mb % p.BW, by = mb / p.BW;
+    auto get = [&](int x, int y) {
+        const LearnedMv& m = lm[(size_t)y * p.BW + x];
+        return MvT{m.raw[0], m.raw[1], m.raw[2], m.raw[3]};
+    };
+    const MvT zero{0, 0, 0, 0};
+    const bool has_t = by > 0, has_l = bx > 0, has_tl = by > 0 && bx > 0, has_tr = by > 0 && bx + 1 < p.BW;
+    const bool has_tm = p.prev_coded != nullptr;
+    MvT Tm{0, 0, 0, 0};
+    if (has_tm) {
+        const char4 pc = *(const char4*)(p.prev_coded + 4 * (size_t)mb);
+        Tm = MvT{pc.x, pc.y, pc.z, pc.w};
+    }
+    const MvT raw = get(bx, by);
+    const MbDecision md = decide_mb(p, raw, (long long)lm[mb].sad, has_l, has_t, has_tr, has_tl, has_tm,
+                                    has_l ? get(bx - 1, by) : zero, has_t ? get(bx, by - 1) : zero,
+                                    has_tr ? get(bx + 1, by - 1) : zero, has_tl ? get(bx - 1, by - 1) : zero, Tm);
+    MbOut o;
+    o.raw[0] = (int8_t)raw.dx; o.raw[1] = (int8_t)raw.dy; o.raw[2] = (int8_t)raw.sx; o.raw[3] = (int8_t)raw.sy;
+    o.coded[0] = (int8_t)md.coded.dx; o.coded[1] = (int8_t)md.coded.dy;
+    o.coded[2] = (int8_t)md.coded.sx; o.coded[3] = (int8_t)md.coded.sy;
+    o.rdelta[0] = (int8_t)md.rdx; o.rdelta[1] = (int8_t)md.rdy;
+    o.mode = (uint8_t)md.mode; o.base = (uint8_t)md.chosen; o.flags = md.flags; o.rdo_skip = md.rdo_skip ? 1 : 0;
+    o.pad[0] = o.pad[1] = 0;
+    o.best_sad = lm[mb].sad;
+    p.out[mb] = o;
+    *(char4*)(p.coded_out + 4 * (size_t)mb) =
+        make_char4((signed char)md.coded.dx, (signed char)md.coded.dy, (signed char)md.coded.sx, (signed char)md.coded.sy);
+    // a search MV outside +-63 would break coded == search MV for the neighbours: flag it
+    if (md.coded.dx != raw.dx || md.coded.dy != raw.dy || md.coded.sx != raw.sx || md.coded.sy != raw.sy)
+        atomicOr(p.status, ST_HEX_CAP);
+}
+
+int launch_learned(const SearchParams& sp, const float* net, int margin, float skip_logit, void* lmv,
+                   unsigned* counters, void* stream) {
+    LearnedParams lp{};
+    lp.sp = sp;
+    lp.net = net;
+    lp.margin = margin;
+    lp.skip_logit = skip_logit;
+    lp.out = (LearnedMv*)lmv;
+    lp.counters = counters;
+    const int M = sp.sr + 2;
+    const int ws = ((16 * LS_MBS + 2 * M + 3) & ~3) + 4, wh = 16 + 2 * M + 1;
+    const size_t smem = (size_t)ws * wh + 16;
+    dim3 grid((sp.BW + LS_MBS - 1) / LS_MBS, sp.BH);
+    k_learned_search<<<grid, 32 * LS_MBS, smem, (cudaStream_t)stream>>>(lp);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return (int)e;
+    const int n = sp.BW * sp.BH;
+    k_learned_mode<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(sp, (const LearnedMv*)lmv);
+    return (int)cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------------

@@ -77,7 +77,7 @@ class RivConfig(C.Structure):
         ("me_zero_mv_threshold", C.c_int64), ("me_predictor_threshold", C.c_int64),
         ("rdo_lambda_mult", C.c_double), ("inter_dead_zone", C.c_float),
         ("device", C.c_int32), ("pipeline_depth", C.c_uint32), ("entropy_threads", C.c_uint32),
-        ("_pad2", C.c_uint32 * 2),
+        ("encode_form", C.c_uint32), ("proposal_margin", C.c_uint32),
     ]
 
 
@@ -113,7 +113,8 @@ EXPORTED_SYMBOLS = (
     "riv_decoder_new", "riv_decoder_info", "riv_decode_frame_yuv", "riv_decode_frame_rgb", "riv_decoder_current_frame",
     "riv_decoder_last_error", "riv_decoder_free", "riv_test_dct_encode", "riv_test_dct_decode", "riv_test_mv_encode",
     "riv_test_mv_decode", "riv_test_delta_bias", "riv_test_worker_queue", "riv_test_libm_range",
-    "riv_stage_predict", "riv_stage_residual", "riv_test_wait_expiry",
+    "riv_stage_predict", "riv_stage_residual", "riv_test_wait_expiry", "riv_encoder_set_proposal",
+    "riv_learned_counters",
 )
 
 
@@ -158,6 +159,8 @@ def lib() -> C.CDLL:
     L.riv_stage_predict.argtypes = [U8P, P, C.c_uint32, C.c_uint32, C.c_uint8, U8P, C.POINTER(C.c_float)]
     L.riv_stage_residual.argtypes = [U8P, U8P, C.POINTER(C.c_float), U8P, P, C.c_float, C.c_uint32, C.c_uint32, P,
                                      U8P, U8P, U8P]
+    L.riv_encoder_set_proposal.argtypes = [P, C.POINTER(C.c_float), C.c_size_t]
+    L.riv_learned_counters.argtypes = [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.riv_test_wait_expiry.argtypes = [C.c_int, C.c_int64, C.POINTER(C.c_uint32)]
     L.riv_test_libm_range.argtypes = [C.c_int, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]
     L.riv_dct_tables.argtypes = [C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
@@ -227,6 +230,8 @@ class EncoderConfig:
     device: int = 0
     pipeline_depth: int = 0
     entropy_threads: int = 0
+    encode_form: int = 0      # 0 plain (reference-identical), 1 learned proposal, 2 parallel without the network
+    proposal_margin: int = 256
 
     @staticmethod
     def new(width: int, height: int, fps: int) -> "EncoderConfig":
@@ -247,6 +252,8 @@ class EncoderConfig:
     def with_me_zero_mv_threshold(self, v: int): return self._with(me_zero_mv_threshold=v)
     def with_me_predictor_threshold(self, v: int): return self._with(me_predictor_threshold=v)
     def with_pipeline_depth(self, v: int): return self._with(pipeline_depth=v)
+    def with_encode_form(self, v: int): return self._with(encode_form=v)
+    def with_proposal_margin(self, v: int): return self._with(proposal_margin=v)
     def with_device(self, v: int): return self._with(device=v)
 
     def validate(self) -> None:
@@ -263,13 +270,17 @@ class EncoderConfig:
             raise InvalidConfig("mv_deflate_level must be in 0..=10")
         if self.keyframe_interval.mode == 2 and self.keyframe_interval.interval == 0:
             raise InvalidConfig("Keyframe interval must be greater than 0")
+        if self.encode_form not in (0, 1, 2):
+            raise InvalidConfig("encode_form must be 0 (plain), 1 (learned) or 2 (parallel)")
+        if self.encode_form and self.search_range > 63:
+            raise InvalidConfig("the learned and parallel forms need search_range <= 63")
 
     def to_c(self) -> RivConfig:
         c = RivConfig()
         for f in ("display_width", "display_height", "storage_width", "storage_height", "fps", "intra_quality",
                   "inter_quality", "search_range", "mv_deflate_level", "skip_threshold", "me_zero_mv_threshold",
                   "me_predictor_threshold", "rdo_lambda_mult", "inter_dead_zone", "device", "pipeline_depth",
-                  "entropy_threads"):
+                  "entropy_threads", "encode_form", "proposal_margin"):
             setattr(c, f, getattr(self, f))
         c.keyframe_mode = self.keyframe_interval.mode
         c.keyframe_interval = self.keyframe_interval.interval
@@ -462,6 +473,18 @@ class Encoder:
         self._check(lib().riv_encode_frame_device(self._h, C.c_void_p(ptr), timestamp,
                                                   C.byref(s) if s is not None else None))
         return EncodeFrameStats.from_c(s) if s is not None else None
+
+    def set_proposal(self, params: np.ndarray) -> None:
+        """Load the proposal network's parameters (learned form), e.g. from
+        riv2_b200.proposal.load_params()."""
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        self._check(lib().riv_encoder_set_proposal(self._h, p.ctypes.data_as(C.POINTER(C.c_float)), p.size))
+
+    def learned_counters(self) -> dict:
+        """Learned / parallel forms: MBs searched, hexagon fallbacks, skip shortcuts."""
+        a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        self._check(lib().riv_learned_counters(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return {"mbs": a.value, "fallbacks": b.value, "shortcuts": c.value}
 
     def encode_frame_yuv(self, y: np.ndarray, u: np.ndarray, v: np.ndarray, timestamp: int) -> None:
         y, u, v = (np.ascontiguousarray(p, dtype=np.uint8) for p in (y, u, v))
