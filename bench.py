@@ -1,18 +1,24 @@
 #!/usr/bin/env python3
-"""Benchmark: 1080p P-frame encode throughput of the B200 riv2 encoder.
+"""Benchmark: 1080p P-frame encode throughput of the B200 riv2 encoder, learned-proposal form
+against the plain form.
 
 Workload: a seeded synthetic 1920x1080 RGB24 clip (16 rectangles, sides 64-384 px,
 velocities +-16 px/frame at 0.5 px steps, pan +-4, noise sigma 2), quality 85/80, one
 key frame at frame 0, encoder defaults otherwise (search range 12, skip threshold 3,
 lambda multiplier 0.49, dead zone 0.75).  A step is one P-frame.
 
-* ``value``: frames/s of the whole encode (GPU hot path + host rANS coding + record
-  writes, pipelined) with the RGB frames already resident in HBM.
+* ``value``: frames/s of the whole encode in the learned-proposal form (proposal network on
+  the tensor cores, parallel proposal-seeded search, parallel mode decision; the network
+  weights riv2_b200/weights/proposal.bin, trained by riv2_b200.train_proposal) with the RGB
+  frames already resident in HBM.  ``plain`` holds the same for the plain form (the
+  reference-identical path), and ``learned_vs_plain`` the fps ratio and the quality deltas
+  of the two streams of the timed frames (PSNR-Y and size, both streams decoded on the GPU).
 * ``e2e``: the same through ``riv_encode_frame`` with pinned host RGB buffers; the
   host->device copy of each frame and the device->host copy of its side info and
   coefficients are inside the timed region.
-* ``roofline``: the dominant kernel (the search/mode wavefront), achieved bytes/s over
-  its algorithmic bytes against the measured HBM copy bandwidth.
+* ``roofline``: the plain form's dominant kernel (the search/mode wavefront), achieved
+  bytes/s over its algorithmic bytes against the measured HBM copy bandwidth; the learned
+  form's GPU stages are in ``learned_stage_us_per_pframe``.
 * ``cpu_baseline``: the CPU oracle (single-threaded restatement of the reference encoder,
   library-default raster-serial search) on a bounded sample of the same clip.
 
@@ -39,8 +45,9 @@ sys.path.insert(0, ROOT)
 
 W_DISP, H_DISP, FPS = 1920, 1080, 50
 MBS_PER_FRAME = (1920 // 16) * (1088 // 16)
-# the headline metric this line reports (only the plain form exists; "form" in config says so)
+# the headline metric this line reports: learned-proposal fps, with the plain form beside it
 METRIC = "1080p encode fps: learned-proposal vs plain GPU at \u22640.1 dB PSNR, \u22642% bitrate"
+WEIGHTS = os.path.join(ROOT, "riv2_b200", "weights", "proposal.bin")
 
 
 def parse():
@@ -55,6 +62,8 @@ def parse():
     ap.add_argument("--cpu-sample-frames", type=int, default=12)
     ap.add_argument("--cpu-workers", type=int, default=96, help="cap on the reference arm's host threads")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--weights", default=WEIGHTS)
+    ap.add_argument("--margin", type=int, default=256, help="learned form: proposal fallback SAD margin")
     return ap.parse_args()
 
 
@@ -167,13 +176,27 @@ def make_frames(n: int, seed: int, clip: int) -> np.ndarray:
     return SynthClip("1080p", seed=seed, clip=clip).frames(n)
 
 
-def config(iq: int, pq: int, depth: int, device: int):
+def config(iq: int, pq: int, depth: int, device: int, form: int = 0, margin: int = 256):
     from riv2_b200 import encoder as E
     return (E.EncoderConfig.new(W_DISP, H_DISP, FPS).with_intra_quality(iq).with_inter_quality(pq)
-            .with_keyframe_interval(E.KeyframeInterval.fixed(1 << 40)).with_pipeline_depth(depth).with_device(device))
+            .with_keyframe_interval(E.KeyframeInterval.fixed(1 << 40)).with_pipeline_depth(depth).with_device(device)
+            .with_encode_form(form).with_proposal_margin(margin))
 
 
-def run_ours(args, frames_host, dev_index, dist):
+def psnr_y_of_stream(stream: bytes, src_y, dev_index: int):
+    """Mean PSNR-Y (display area) of a stream decoded on the GPU against the source luma."""
+    from riv2_b200.decoder import Decoder
+    dec = Decoder.new(stream, dev_index)
+    vals = []
+    for ys in src_y:
+        y = dec.decode_frame().y[:H_DISP, :W_DISP].astype(np.float64)
+        mse = float(np.mean((y - ys[:H_DISP, :W_DISP]) ** 2))
+        vals.append(99.0 if mse == 0 else 10.0 * np.log10(255.0 ** 2 / mse))
+    dec.close()
+    return float(np.mean(vals))
+
+
+def run_ours(args, frames_host, dev_index, dist, form=0, params=None):
     import torch
 
     from riv2_b200 import encoder as E
@@ -188,7 +211,9 @@ def run_ours(args, frames_host, dev_index, dist):
 
     def session(device_inputs: bool):
         w = E.VecWriter()
-        enc = E.Encoder.new(config(iq, pq, args.pipeline_depth, dev_index), w)
+        enc = E.Encoder.new(config(iq, pq, args.pipeline_depth, dev_index, form, args.margin), w)
+        if form == 1:
+            enc.set_proposal(params)
         base = frames_dev.data_ptr() if device_inputs else pinned.data_ptr()
 
         def put(t, drain=False):
@@ -219,16 +244,18 @@ def run_ours(args, frames_host, dev_index, dist):
         barrier(dist, dev)
         ms = ev0.elapsed_time(ev1)
         c1 = enc.counters()
+        lc = enc.learned_counters()
         data = w.into_inner()
         enc.close()
-        return ms, c0, c1, clk, data
+        return ms, c0, c1, clk, data, lc
 
-    ms_v, c0v, c1v, clk_v, data_v = session(True)
-    dec = decode_rate(data_v, dev_index)
-    ms_e, c0e, c1e, clk_e, data_e = session(False)
+    ms_v, c0v, c1v, clk_v, data_v, lc = session(True)
+    dec = decode_rate(data_v, dev_index) if form == 0 else None
+    ms_e, c0e, c1e, clk_e, data_e, _ = session(False)
     del frames_dev
     return {"ms_value": ms_v, "ms_e2e": ms_e, "c0": c0v, "c1": c1v, "c0e": c0e, "c1e": c1e, "clocks": clk_v,
-            "clocks_e2e": clk_e, "stream_bytes": len(data_v), "streams_equal": data_v == data_e, "decode": dec}
+            "clocks_e2e": clk_e, "stream_bytes": len(data_v), "streams_equal": data_v == data_e, "decode": dec,
+            "stream": data_v, "learned_counters": lc}
 
 
 def decode_rate(stream: bytes, dev_index: int):
@@ -407,54 +434,102 @@ def main():
     import torch
     dev_index = local if torch.cuda.device_count() > 1 else 0
     frames = make_frames(K + Wm + 1, args.seed, rank)
-    r = run_ours(args, frames, dev_index, dist)
-    ms_v = max_over_ranks(r["ms_value"], dist, torch.device("cuda", dev_index))
-    ms_e = max_over_ranks(r["ms_e2e"], dist, torch.device("cuda", dev_index))
-    c0, c1 = r["c0"], r["c1"]
-    pf = c1["pframes"] - c0["pframes"]
-    ptimed = c1["timed_pframes"] - c0["timed_pframes"]  # stage timing events ride on sampled frames
-    stage = [(b - a) / max(ptimed, 1) for a, b in zip(c0["stage_us_sum"], c1["stage_us_sum"])]
-    launches = c1["launches"] - c0["launches"]
-    deferred = (c1["deferred_pframes"] - c0["deferred_pframes"]) / max(pf, 1)
-    h2d = (r["c1e"]["h2d_bytes"] - r["c0e"]["h2d_bytes"]) / K
-    d2h = (r["c1e"]["d2h_bytes"] - r["c0e"]["d2h_bytes"]) / K
+    params = None
+    if os.path.exists(args.weights):
+        from riv2_b200 import proposal as P
+        params = P.load_params(args.weights)
+    forms = {"plain": run_ours(args, frames, dev_index, dist, 0)}
+    if params is not None:
+        forms["learned"] = run_ours(args, frames, dev_index, dist, 1, params)
+    dvc = torch.device("cuda", dev_index)
+    res = {}
+    for name, r in forms.items():
+        ms_v = max_over_ranks(r["ms_value"], dist, dvc)
+        ms_e = max_over_ranks(r["ms_e2e"], dist, dvc)
+        c0, c1 = r["c0"], r["c1"]
+        pf = c1["pframes"] - c0["pframes"]
+        ptimed = c1["timed_pframes"] - c0["timed_pframes"]  # stage timing events ride on sampled frames
+        stage = [(b - a) / max(ptimed, 1) for a, b in zip(c0["stage_us_sum"], c1["stage_us_sum"])]
+        res[name] = {
+            "ms_v": ms_v, "ms_e": ms_e, "stage": stage, "launches": c1["launches"] - c0["launches"],
+            "deferred": (c1["deferred_pframes"] - c0["deferred_pframes"]) / max(pf, 1),
+            "h2d": (r["c1e"]["h2d_bytes"] - r["c0e"]["h2d_bytes"]) / K,
+            "d2h": (r["c1e"]["d2h_bytes"] - r["c0e"]["d2h_bytes"]) / K,
+            "host": dict(zip(["submit", "retire", "mv_coding", "dct_coding_sum", "write", "blocked"],
+                             [round((b - a) / K, 3) for a, b in zip(c0["host_ms"], c1["host_ms"])])),
+            "value": ws * K / (ms_v / 1000.0), "e2e": ws * K / (ms_e / 1000.0),
+        }
+    # quality of the two forms' streams of the same frames (decoded on the GPU; rank 0's clip)
+    quality = None
+    if "learned" in forms and rank == 0:
+        from riv2_b200 import encoder as E
+        sw, sh = W_DISP, (H_DISP + 15) // 16 * 16
+        src_y = [E.stage_rgb_to_yuv(f, W_DISP, H_DISP, sw, sh)[: sw * sh].reshape(sh, sw) for f in frames]
+        pp = psnr_y_of_stream(forms["plain"]["stream"], src_y, dev_index)
+        pl = psnr_y_of_stream(forms["learned"]["stream"], src_y, dev_index)
+        lc = forms["learned"]["learned_counters"]
+        quality = {"psnr_y_plain_db": pp, "psnr_y_learned_db": pl, "delta_psnr_db": pl - pp,
+                   "bytes_plain": forms["plain"]["stream_bytes"], "bytes_learned": forms["learned"]["stream_bytes"],
+                   "delta_bitrate": forms["learned"]["stream_bytes"] / forms["plain"]["stream_bytes"] - 1.0,
+                   "fallback_rate": lc["fallbacks"] / max(lc["mbs"], 1),
+                   "shortcut_rate": lc["shortcuts"] / max(lc["mbs"], 1),
+                   "frames": len(frames), "what": "the timed clip's key frame and P-frames, both streams decoded on "
+                                                   "the GPU decoder, PSNR of the luma display area"}
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
         return
-    value = ws * K / (ms_v / 1000.0)
-    e2e = ws * K / (ms_e / 1000.0)
+    head = res.get("learned", res["plain"])
     cpu = None
     if ws == 1 and not args.no_cpu_baseline:
         fps, dt = cpu_baseline(frames, args.cpu_sample_frames, iq, pq)
         cpu = {"value": fps, "unit": "frames/s", "cores": 1, "kind": "port",
                "sample": f"{args.cpu_sample_frames} P-frames of the same 1080p clip after its key frame ({dt:.1f} s)"}
     names = ["rgb_to_yuv", "sad_table", "search", "predict", "aq", "residual", "deblock", "compact", "total"]
+    lnames = ["rgb_to_yuv", "proposal_network", "search_and_mode", "predict", "aq", "residual", "deblock", "compact",
+              "total"]
+    rp = res["plain"]
+    learned = "learned" in res
     line = {
-        "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": ws, "steps": K, "warmup": Wm,
-        "ms_per_step": ms_v / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "u8/i16/i32 (f32 AQ, f64 RDO)", "data": "synthetic",
-        "config": {"workload": "1080p synthetic clip (1920x1080, 16 moving textured rects, pan, noise), plain GPU "
-                               "P-frame encode, q %d/%d, search range 12, one key frame" % (iq, pq),
+        "metric": METRIC, "value": head["value"] if learned else None, "unit": "frames/s", "n_gpus": ws, "steps": K,
+        "warmup": Wm, "ms_per_step": head["ms_v"] / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8/i16/i32 (f32 AQ, f64 RDO); bf16 network, f32 accumulation",
+        "data": "synthetic",
+        "config": {"workload": "1080p synthetic clip (1920x1080, 16 moving textured rects, pan, noise), GPU P-frame "
+                               "encode, q %d/%d, search range 12, one key frame" % (iq, pq),
                    "global_batch": ws, "seq_len": K, "parallelism": f"replicas x{ws} (one clip per GPU)",
-                   "form": "plain (learned-proposal form not built)",
+                   "form": ("learned proposal (network %s, fallback margin %d) vs plain"
+                            % (os.path.relpath(args.weights, ROOT), args.margin)) if learned
+                           else "plain only: no proposal-network weights at %s" % args.weights,
                    "pipeline_depth": args.pipeline_depth,
                    "l2": "inputs larger than L2: %d distinct RGB frames (%.0f MB) resident in HBM"
                          % (K + Wm + 1, (K + Wm + 1) * W_DISP * H_DISP * 3 / 1e6),
-                   "macroblocks_per_s": value * MBS_PER_FRAME},
-        "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-        "gpu_launches": int(launches),
-        "gpu_stage_us_per_pframe": dict(zip(names, [round(x, 2) for x in stage])),
-        "pframes_reconstructed_in_next_launch": round(deferred, 3),
-        "gpu_pipeline_fps": 1e6 / stage[8] if stage[8] > 0 else None,
-        "host_ms_per_frame": dict(zip(["submit", "retire", "mv_coding", "dct_coding_sum", "write", "blocked"],
-                                      [round((b - a) / K, 3) for a, b in zip(c0["host_ms"], c1["host_ms"])])),
-        "roofline": roofline_entry(stage[2], d2h),
+                   "macroblocks_per_s": head["value"] * MBS_PER_FRAME},
+        "e2e": {"value": head["e2e"], "unit": "frames/s", "h2d_bytes_per_step": int(head["h2d"]),
+                "d2h_bytes_per_step": int(head["d2h"])},
+        "plain": {"value": rp["value"], "e2e": rp["e2e"], "ms_per_step": rp["ms_v"] / K,
+                  "macroblocks_per_s": rp["value"] * MBS_PER_FRAME,
+                  "gpu_stage_us_per_pframe": dict(zip(names, [round(x, 2) for x in rp["stage"]])),
+                  "pframes_reconstructed_in_next_launch": round(rp["deferred"], 3),
+                  "gpu_pipeline_fps": 1e6 / rp["stage"][8] if rp["stage"][8] > 0 else None,
+                  "host_ms_per_frame": rp["host"], "gpu_launches": int(rp["launches"]),
+                  "stream_bytes": forms["plain"]["stream_bytes"],
+                  "streams_equal_value_vs_e2e": forms["plain"]["streams_equal"]},
+        "gpu_launches": int(head["launches"]),
+        "roofline": roofline_entry(rp["stage"][2], rp["d2h"]),
         "cpu_baseline": cpu,
-        "clocks": r["clocks"], "clocks_e2e": r["clocks_e2e"],
-        "stream_bytes": r["stream_bytes"], "streams_equal_value_vs_e2e": r["streams_equal"],
-        "decode": r["decode"],
+        "clocks": forms["learned" if learned else "plain"]["clocks"],
+        "clocks_e2e": forms["learned" if learned else "plain"]["clocks_e2e"],
+        "decode": forms["plain"]["decode"],
     }
+    if learned:
+        rl = res["learned"]
+        line["learned_vs_plain"] = dict({"value_ratio": rl["value"] / rp["value"], "e2e_ratio": rl["e2e"] / rp["e2e"]},
+                                        **(quality or {}))
+        line["learned_stage_us_per_pframe"] = dict(zip(lnames, [round(x, 2) for x in rl["stage"]]))
+        line["learned_gpu_pipeline_fps"] = 1e6 / rl["stage"][8] if rl["stage"][8] > 0 else None
+        line["learned_host_ms_per_frame"] = rl["host"]
+        line["learned_streams_equal_value_vs_e2e"] = forms["learned"]["streams_equal"]
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

@@ -131,8 +131,9 @@ uint64_t riv_frame_count(const riv_encoder* enc);
 riv_status riv_last_recon(riv_encoder* enc, uint8_t* y, uint8_t* u, uint8_t* v);
 /* Per-frame GPU timing of the last completed frame that carried stage timing events (every
  * frame at pipeline_depth 0 or with per-frame stats, else one in 8), microseconds: [0] rgb->yuv
- * [1] integer-SAD table [2] search/mode wavefront [3] predict [4] aq [5] residual
- * [6] deblock [7] compact [8] total */
+ * [1] integer-SAD table (plain form) or proposal network (learned form) [2] search/mode
+ * (the wavefront, or the learned forms' parallel search + mode decision) [3] predict [4] aq
+ * [5] residual [6] deblock [7] compact [8] total */
 riv_status riv_last_kernel_times(riv_encoder* enc, float* us9);
 
 /* Cumulative counters since riv_encoder_new: us9 = per-stage GPU time summed over all

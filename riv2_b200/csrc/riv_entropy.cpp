@@ -556,14 +556,15 @@ static void enc_comp(RansWriter& w, int8_t delta, BinProb* cls, BinProb& sign, B
     for (unsigned b = 0; b < bits; b++) w.put((off >> b) & 1, mag[b]);
 }
 
-void MvCoder::encode_frame(const std::vector<MvCodedBlock>& blocks, int bw, std::vector<uint8_t>& out) {
+void MvCoder::encode_frame(const std::vector<MvCodedBlock>& blocks, int bw, std::vector<uint8_t>& out,
+                           const BatchSubmit* submit) {
     out.clear();
     // a NEW block with a raw -1/2 subpel: the reference panics ("raw -0.5 subpixel is
     // disallowed", res/mv_rans/encoder.rs:335-336; no candidate holds one, :379-381)
     for (const MvCodedBlock& b : blocks)
         if (b.mode == M_NEW && (b.spx == SP_MINUS || b.spy == SP_MINUS))
             throw std::runtime_error("raw -0.5 subpixel is disallowed");
-    RansWriter w(&out);
+    RansWriter w(&out, submit);
     std::vector<uint8_t> modes, hits;
     modes.reserve(blocks.size());
     hits.reserve(blocks.size());

@@ -100,7 +100,10 @@ class MvCoder {  // res/mv_rans/encoder.rs:60-412
 public:
     void reset();
     // Throws std::runtime_error on a NEW block with a raw -1/2 subpel (the reference panics).
-    void encode_frame(const std::vector<MvCodedBlock>& blocks, int bw, std::vector<uint8_t>& out);
+    // submit (nullable): full rANS batches are coded there while the context modelling goes on
+    // (same bytes; see RansWriter).
+    void encode_frame(const std::vector<MvCodedBlock>& blocks, int bw, std::vector<uint8_t>& out,
+                      const BatchSubmit* submit = nullptr);
     // res/mv_rans/decoder.rs:149-283; the same context and candidate-history state as the
     // encoder, so a decoder instance follows the encoder's across frames.  false on bad data.
     bool decode_frame(const uint8_t* data, size_t len, int bw, int bh, std::vector<MvCodedBlock>& out);

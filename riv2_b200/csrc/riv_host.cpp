@@ -735,7 +735,8 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
     const bool defer_this = j.type == 2 && e->defer_ok;
     if (j.type == 1) flush_pending(e);  // key frames reconstruct immediately
     // kernels per frame: rgb->yuv, (search, predict, 3 x aq), residual, deblock, scan + pack
-    const int p_launches = 1 + (e->table_ok && !e->splan.fused ? 1 : 0) + (e->splan.fast && e->table_ok ? 0 : 4);
+    const int p_launches = e->learned ? (c.encode_form == RIV_FORM_LEARNED ? 8 : 0) + 2 + 4
+                                      : 1 + (e->table_ok && !e->splan.fused ? 1 : 0) + (e->splan.fast && e->table_ok ? 0 : 4);
     e->launches += (src == 2 ? 0 : 1) + (j.type == 2 ? p_launches : 0);  // + residual / deblock / compaction below
     if (src == 0) e->h2d_bytes += (uint64_t)c.display_width * c.display_height * 3;
     if (src == 2) e->h2d_bytes += e->yuv_bytes;
@@ -830,6 +831,10 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         sp.wq = e->wq.as<unsigned>() + (size_t)e->wq_par * e->wq_words;
         sp.wq_next = e->wq.as<unsigned>() + (size_t)(e->wq_par ^ 1) * e->wq_words;
         sp.wq_words = e->wq_words;
+        if (e->learned && c.encode_form == RIV_FORM_LEARNED) {  // stage 1 of the learned form: the network
+            if (!e->nn_loaded) throw std::runtime_error("learned form: no proposal network loaded (riv_encoder_set_proposal)");
+            proposal_forward(e, cur, sp.ref_y, sp.prev_coded, S);
+        }
         if (e->table_ok && !e->learned) {
             sp.tstride = sad_table_stride(c.search_range);
             sp.tab = e->sadtab.as<uint16_t>();
@@ -873,11 +878,6 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         e->pend.active = false;
         CK(cudaStreamWaitEvent(S, e->ev_mbout_free[ck], 0));  // compaction of the frame NPAR back
         if (e->learned) {
-            if (c.encode_form == RIV_FORM_LEARNED) {
-                if (!e->nn_loaded) throw std::runtime_error("learned form: no proposal network loaded (riv_encoder_set_proposal)");
-                proposal_forward(e, cur, sp.ref_y, sp.prev_coded, S);
-            }
-            e->launches += (c.encode_form == RIV_FORM_LEARNED ? 8 : 0) + 2;
             CK((cudaError_t)launch_learned(sp, c.encode_form == RIV_FORM_LEARNED ? e->nn_o.as<float>() : nullptr,
                                            (int)c.proposal_margin, 2.2f, e->lmv.p, e->lcount.as<unsigned>(), S));
             e->learned_mbs += (uint64_t)N;
@@ -1025,7 +1025,7 @@ static riv_status retire(riv_encoder* e, Job& j) {
                 S.mv_mode_counts[b.mode]++;
                 if (b.skip) S.blocks_skipped++;
             }
-            ep->mvc.encode_frame(blocks, ep->BW, jp->mv_bytes);
+            ep->mvc.encode_frame(blocks, ep->BW, jp->mv_bytes, &ep->rans_submit);
             S.mv_bias_dx = jp->bias[0];
             S.mv_bias_dy = jp->bias[1];
             S.rdo_lambda = ep->L.lambda;

@@ -29,7 +29,7 @@
 
 namespace {
 
-constexpr long long NN_SPIN = 1ll << 26;
+constexpr long long NN_SPIN = 1ll << 22;  // polls of mbarrier.try_wait (a few seconds at most)
 
 __device__ __forceinline__ uint32_t s32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
