@@ -63,6 +63,7 @@ def parse():
     ap.add_argument("--cpu-workers", type=int, default=96, help="cap on the reference arm's host threads")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--weights", default=WEIGHTS)
+    ap.add_argument("--no-secondary", action="store_true", help="skip the secondary measurement points")
     ap.add_argument("--margin", type=int, default=256, help="learned form: proposal fallback SAD margin")
     return ap.parse_args()
 
@@ -281,9 +282,66 @@ def decode_rate(stream: bytes, dev_index: int):
             "what": "P-frames of the bench stream through the GPU decoder (YUV reconstruction, no copy-out)"}
 
 
+def quick_fps(frames_dev, w, h, iq, pq, depth, form, params, steps, warmup, sr=12, margin=256):
+    """Frames/s of a secondary configuration: device-resident RGB frames, `warmup` untimed
+    frames, then `steps` frames timed with CUDA events up to the last record's write."""
+    import torch
+
+    from riv2_b200 import encoder as E
+    cfg = (E.EncoderConfig.new(w, h, FPS).with_intra_quality(iq).with_inter_quality(pq).with_search_range(sr)
+           .with_keyframe_interval(E.KeyframeInterval.fixed(1 << 40)).with_pipeline_depth(depth)
+           .with_encode_form(form).with_proposal_margin(margin))
+    enc = E.Encoder.new(cfg, E.VecWriter())
+    if form == 1:
+        enc.set_proposal(params)
+    stride = w * h * 3
+    base = frames_dev.data_ptr()
+    for t in range(warmup):
+        enc.encode_frame_device(base + t * stride, t * 20)
+    enc.encode_frame_device(base + warmup * stride, warmup * 20, drain=True)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for t in range(warmup + 1, warmup + 1 + steps):
+        enc.encode_frame_device(base + t * stride, t * 20)
+    enc.finish()
+    ev1.record()
+    torch.cuda.synchronize()
+    enc.close()
+    return steps / (ev0.elapsed_time(ev1) / 1000.0)
+
+
+def secondary_points(frames_host, dev_index, params, steps, warmup, depth):
+    """The other measurement points of the 1080p workload (quality 95/90, search range 31,
+    pipeline depth 0 = the reference's one record per call) and the CIF workload, each for
+    the plain form and, where a network is loaded, the learned form."""
+    import torch
+
+    from riv2_b200.synth import SynthClip
+    dev = torch.device("cuda", dev_index)
+    n = steps + warmup + 1
+    f1080 = torch.from_numpy(frames_host[:n]).to(dev)
+    cif = torch.from_numpy(SynthClip("cif", seed=2026).frames(max(n, 61))).to(dev)
+    points = {"1080p_q95_90": (f1080, 1920, 1080, 95, 90, depth, 12, steps),
+              "1080p_sr31": (f1080, 1920, 1080, 85, 80, depth, 31, steps),
+              "1080p_depth0": (f1080, 1920, 1080, 85, 80, 0, 12, steps),
+              "cif_q85_80": (cif, 352, 288, 85, 80, depth, 12, 60)}
+    out = {}
+    for name, (fr, w, h, iq, pq, d, sr, k) in points.items():
+        k = min(k, fr.shape[0] - warmup - 1)
+        row = {"plain": quick_fps(fr, w, h, iq, pq, d, 0, None, k, warmup, sr), "steps": k,
+               "pipeline_depth": d, "search_range": sr, "quality": f"{iq}/{pq}"}
+        if params is not None:
+            row["learned"] = quick_fps(fr, w, h, iq, pq, d, 1, params, k, warmup, sr)
+        out[name] = row
+    return out
+
+
 def cpu_baseline(frames_host, nframes, iq, pq):
-    """The oracle (single-threaded restatement of the reference encoder) on a sample."""
+    """The oracle (single-threaded restatement of the reference encoder, built here with
+    -O3 -march=native) on a sample."""
     from oracle import oracle as O
+    O.use_native_build()
     cfg = O.default_config(W_DISP, H_DISP, FPS)
     cfg.intra_quality, cfg.inter_quality = iq, pq
     cfg.keyframe_mode, cfg.keyframe_interval = 2, 1 << 40
@@ -301,6 +359,7 @@ def _cpu_stream_worker(seed, nframes, iq, pq, barrier, results):
     timed from a barrier that all workers pass together."""
     frames = make_frames(nframes + 1, seed, 0)
     from oracle import oracle as O
+    O.use_native_build()
     cfg = O.default_config(W_DISP, H_DISP, FPS)
     cfg.intra_quality, cfg.inter_quality = iq, pq
     cfg.keyframe_mode, cfg.keyframe_interval = 2, 1 << 40
@@ -416,6 +475,8 @@ def main():
                                  f"({n} P-frames each, timed from a common start; slowest {slowest:.1f} s)"}
         except Exception as ex:  # the single-stream figure above stands on its own
             all_cores = {"unavailable": f"{type(ex).__name__}: {ex}"}
+        from oracle import oracle as O
+        model = O.cpu_model()
         line = {"impl": "reference", "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": ws, "steps": K,
                 "warmup": Wm, "ms_per_step": 1000.0 / fps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "u8/i16/i32 (f32 AQ, f64 RDO)", "data": "synthetic",
@@ -424,7 +485,9 @@ def main():
                                           "(raster-serial search, library-default features), so one thread is "
                                           "all this configuration can use"},
                 "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": 1, "kind": "port",
-                                 "sample": f"{n} P-frames of the 1080p clip after its key frame, x{len(steps_vals)}"},
+                                 "sample": f"{n} P-frames of the 1080p clip after its key frame, x{len(steps_vals)}",
+                                 "cpu_model": model, "host_threads": ncpu,
+                                 "build": "g++ -O3 -march=native -fwrapv -ffp-contract=off -fno-fast-math"},
                 "cpu_all_cores": all_cores,
                 "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -483,8 +546,10 @@ def main():
     cpu = None
     if ws == 1 and not args.no_cpu_baseline:
         fps, dt = cpu_baseline(frames, args.cpu_sample_frames, iq, pq)
+        from oracle import oracle as O
         cpu = {"value": fps, "unit": "frames/s", "cores": 1, "kind": "port",
-               "sample": f"{args.cpu_sample_frames} P-frames of the same 1080p clip after its key frame ({dt:.1f} s)"}
+               "sample": f"{args.cpu_sample_frames} P-frames of the same 1080p clip after its key frame ({dt:.1f} s)",
+               "cpu_model": O.cpu_model(), "build": "g++ -O3 -march=native -fwrapv -ffp-contract=off -fno-fast-math"}
     names = ["rgb_to_yuv", "sad_table", "search", "predict", "aq", "residual", "deblock", "compact", "total"]
     lnames = ["rgb_to_yuv", "proposal_network", "search_and_mode", "predict", "aq", "residual", "deblock", "compact",
               "total"]
@@ -530,6 +595,8 @@ def main():
         line["learned_gpu_pipeline_fps"] = 1e6 / rl["stage"][8] if rl["stage"][8] > 0 else None
         line["learned_host_ms_per_frame"] = rl["host"]
         line["learned_streams_equal_value_vs_e2e"] = forms["learned"]["streams_equal"]
+    if ws == 1 and not args.no_secondary:
+        line["secondary"] = secondary_points(frames, dev_index, params, min(K, 20), min(Wm, 3), args.pipeline_depth)
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

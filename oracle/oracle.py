@@ -38,6 +38,30 @@ def build() -> str:
     return _LIB_PATH
 
 
+def use_native_build() -> str:
+    """Switch this process to the -O3 -march=native build of the same source (compiled here,
+    for this host's CPU), for the timed CPU baseline.  Returns the CPU model it targets."""
+    import hashlib
+    global _LIB_PATH, _lib
+    model = cpu_model()
+    out = "_ref/liboracle_native_%s.so" % hashlib.sha1(model.encode()).hexdigest()[:10]
+    subprocess.run(["make", "-s", "-C", _HERE, "native", "NATIVE_OUT=" + out], check=True)
+    _LIB_PATH = os.path.join(_HERE, out)
+    _lib = None
+    return model
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 _lib = None
 
 
