@@ -114,7 +114,7 @@ riv_status riv_encode_frame_yuv(riv_encoder* enc, const uint8_t* y, const uint8_
 riv_status riv_finish(riv_encoder* enc);
 void riv_encoder_free(riv_encoder* enc);
 /* No counterpart in the reference.  Loads the proposal network's parameters for
- * RIV_FORM_LEARNED: n = 146,592 f32 values (bf16-rounded weights of conv1..4, fc1..3, then
+ * RIV_FORM_LEARNED: n = 91,536 f32 values (bf16-rounded weights of conv1..4, fc1..3, then
  * their biases; the layout of riv_nn.h), as written by this library's trainer.  Call before
  * the first P-frame; RIV_ERR_INVALID_CONFIG when n does not match. */
 riv_status riv_encoder_set_proposal(riv_encoder* enc, const float* params, size_t n);

@@ -735,7 +735,7 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
     const bool defer_this = j.type == 2 && e->defer_ok;
     if (j.type == 1) flush_pending(e);  // key frames reconstruct immediately
     // kernels per frame: rgb->yuv, (search, predict, 3 x aq), residual, deblock, scan + pack
-    const int p_launches = e->learned ? (c.encode_form == RIV_FORM_LEARNED ? 8 : 0) + 2 + 4
+    const int p_launches = e->learned ? (c.encode_form == RIV_FORM_LEARNED ? 8 : 0) + 3
                                       : 1 + (e->table_ok && !e->splan.fused ? 1 : 0) + (e->splan.fast && e->table_ok ? 0 : 4);
     e->launches += (src == 2 ? 0 : 1) + (j.type == 2 ? p_launches : 0);  // + residual / deblock / compaction below
     if (src == 0) e->h2d_bytes += (uint64_t)c.display_width * c.display_height * 3;
@@ -846,7 +846,9 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         // coded MVs of this frame become next frame's temporal predictors
         const int cn = e->coded_cur ^ 1;
         sp.coded_out = e->coded[cn].as<int8_t>();
-        const bool aq_in_search = e->splan.fast && e->table_ok && !e->learned;
+        // prediction, variances and ln inside the search launch (plain fused form), or inside the
+        // learned forms' parallel search (their launch also folds the mean)
+        const bool aq_in_search = (e->splan.fast && e->table_ok) || e->learned;
         if (aq_in_search) {  // prediction, variances and ln inside the search launch
             sp.pred = e->predb[ck].as<uint8_t>();
             sp.varsum = e->varsum.as<uint2>();

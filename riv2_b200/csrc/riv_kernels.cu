@@ -182,6 +182,14 @@ __device__ __forceinline__ uint32_t favg4(uint32_t a, uint32_t b, uint32_t c, ui
     return ((lo >> 2) & M) | (((hi >> 2) & M) << 8);
 }
 
+// (a+b+c+d+2)>>2 per byte (build_predicted's rounded four-tap average), via 16-bit lanes
+__device__ __forceinline__ uint32_t ravg4(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+    const uint32_t M = 0x00FF00FFu;
+    uint32_t lo = (a & M) + (b & M) + (c & M) + (d & M) + 0x00020002u;
+    uint32_t hi = ((a >> 8) & M) + ((b >> 8) & M) + ((c >> 8) & M) + ((d >> 8) & M) + 0x00020002u;
+    return ((lo >> 2) & M) | (((hi >> 2) & M) << 8);
+}
+
 // Reference samples of one MB: byte at frame (fx, fy) = org[(fy - wy0) * stride + fx - x0].
 // Replicated borders: positions outside the frame hold the nearest frame sample.
 struct RefView {
@@ -2730,7 +2738,7 @@ __global__ void __launch_bounds__(32 * LS_MBS) k_learned_search(LearnedParams lp
         const int HX[6] = {2, 1, -1, -2, -1, 1}, HY[6] = {0, 2, 2, 0, -2, -2};
         const int DX[4] = {1, -1, 0, 0}, DY[4] = {0, 0, 1, -1};
         if (fallback) {
-            for (int round = 0; round < 64; round++) {
+            for (int round = 0; round < 16; round++) {  // a bounded hexagon walk (+-32 pixels)
                 int nbx = bdx, nby = bdy;
                 long long nb = best;
                 unsigned ns = bsad;
@@ -2746,7 +2754,7 @@ __global__ void __launch_bounds__(32 * LS_MBS) k_learned_search(LearnedParams lp
                 best = nb; bsad = ns; bdx = nbx; bdy = nby;
             }
         }
-        for (int round = 0; round < (fallback ? 64 : 8); round++) {
+        for (int round = 0; round < (fallback ? 16 : 8); round++) {
             int nbx = bdx, nby = bdy;
             long long nb = best;
             unsigned ns = bsad;
@@ -2778,6 +2786,42 @@ __global__ void __launch_bounds__(32 * LS_MBS) k_learned_search(LearnedParams lp
             }
         hx = bhx;
         hy = bhy;
+    }
+    if (p.pred != nullptr) {
+        // luma prediction of the chosen MV with build_predicted's rounded bilinear rule
+        // (com/fast_motion.rs:103-262; the window's replicated borders equal its coordinate
+        // clamps), then the MB's variance and its glibc-exact ln (compute_aq_quant_steps,
+        // res/residual.rs:116-167) for the AQ fold
+        const int ix = hx >> 1, iy = hy >> 1, fx = hx & 1, fy = hy & 1;
+        const uint8_t* r = lsm + (oy + (lane >> 1) + iy) * ws + ox + (lane & 1) * 8 + ix;
+        uint32_t q[2];
+#pragma unroll
+        for (int h2 = 0; h2 < 2; h2++) {
+            const uint8_t* rr = r + 4 * h2;
+            const uint32_t a = lds_u32(rr);
+            if (fx && fy) q[h2] = ravg4(a, lds_u32(rr + 1), lds_u32(rr + ws), lds_u32(rr + ws + 1));
+            else if (fx) q[h2] = __vavgu4(a, lds_u32(rr + 1));
+            else if (fy) q[h2] = __vavgu4(a, lds_u32(rr + ws));
+            else q[h2] = a;
+        }
+        *(uint2*)(p.pred + (size_t)(y0 + (lane >> 1)) * p.W + x0 + (lane & 1) * 8) = make_uint2(q[0], q[1]);
+        unsigned sv = 0, sv2 = 0;
+#pragma unroll
+        for (int h2 = 0; h2 < 2; h2++)
+#pragma unroll
+            for (int b = 0; b < 4; b++) {
+                const unsigned v = (q[h2] >> (8 * b)) & 255u;
+                sv += v;
+                sv2 += v * v;
+            }
+        sv = __reduce_add_sync(0xffffffffu, sv);
+        sv2 = __reduce_add_sync(0xffffffffu, sv2);
+        if (lane == 0) {
+            const unsigned long long NN = 256ull * sv2 - (unsigned long long)sv * sv;
+            float var = __fdiv_rn(__ull2float_rn(NN), 65536.0f);
+            var = var < 4.0f ? 4.0f : var;
+            p.lnv[mb] = glibc_logf(var, p.logfix, p.nlog);
+        }
     }
     if (lane == 0) {
         // canonical form: a -1/2 component becomes +1/2 of the whole pixel below
@@ -2831,6 +2875,8 @@ __global__ void __launch_bounds__(128) k_learned_mode(SearchParams p, const Lear
         atomicOr(p.status, ST_HEX_CAP);
 }
 
+__global__ void __launch_bounds__(1024) k_aq_sum(const float* __restrict__ lnv, int n, float* avg_out);
+
 int launch_learned(const SearchParams& sp, const float* net, int margin, float skip_logit, void* lmv,
                    unsigned* counters, void* stream) {
     LearnedParams lp{};
@@ -2849,6 +2895,10 @@ int launch_learned(const SearchParams& sp, const float* net, int margin, float s
     if (e != cudaSuccess) return (int)e;
     const int n = sp.BW * sp.BH;
     k_learned_mode<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(sp, (const LearnedMv*)lmv);
+    e = cudaGetLastError();
+    if (e != cudaSuccess || sp.lnv == nullptr) return (int)e;
+    // the strictly sequential f32 mean of the ln variances (Iterator::sum), at lnv[n]
+    k_aq_sum<<<1, 1024, 8192 * sizeof(float), (cudaStream_t)stream>>>(sp.lnv, n, sp.lnv + n);
     return (int)cudaGetLastError();
 }
 

@@ -241,7 +241,14 @@ __global__ void __launch_bounds__(128, 1)
 // =====================================================================================
 // Implicit-GEMM convolution
 // =====================================================================================
-constexpr int CONV_STAGES = 3;
+// Warp roles (288 threads): warps 0-3 gather the operand (one output position per thread,
+// cp.async straight into the swizzled K-major layout, zero-filled padding taps) into a ring of
+// CV_STAGES k-blocks and mark each stage full on an mbarrier once their copies have landed;
+// warp 4 holds the tensor memory and its lane 0 issues the MMAs; warps 5-8 run the epilogue
+// (warp w reads TMEM lanes 32 (w % 4) .. +31).  The accumulator is double-buffered (2 x 32
+// columns), so a tile's epilogue overlaps the next tile's MMAs and gathers.
+constexpr int CV_THREADS = 288;
+constexpr int CV_LAG = 2;  // k-blocks a gathering thread keeps in flight before marking one full
 
 struct ConvArgs {
     const __nv_bfloat16* in;
@@ -252,125 +259,178 @@ struct ConvArgs {
     unsigned* err;
 };
 
-// CIN = 2 (conv1: one k-block of 32, 64-byte rows) or 32 (five k-blocks of 64: two taps each).
 template <int CIN>
-__global__ void __launch_bounds__(128, 1) k_nn_conv(const __grid_constant__ CUtensorMap tw, ConvArgs a) {
-    constexpr int BK = CIN == 2 ? 32 : 64;
-    constexpr int SWZ = BK * 2;
-    constexpr int NKB = CIN == 2 ? 1 : 5;
-    constexpr int W_TILE = 32 * SWZ;   // one k-block of the weights: 32 rows
-    constexpr int A_TILE = 128 * SWZ;  // one k-block of the gathered operand
+struct ConvCfg {
+    static constexpr int BK = CIN == 2 ? 32 : 64;      // k-block width (elements)
+    static constexpr int SWZ = BK * 2;                 // bytes per operand row
+    static constexpr int NKB = CIN == 2 ? 1 : 5;       // k-blocks per tile
+    static constexpr int STAGES = CIN == 2 ? 8 : 5;    // operand ring depth
+    static constexpr int W_TILE = 32 * SWZ;
+    static constexpr int A_TILE = 128 * SWZ;
+    static constexpr size_t smem() {
+        return 1024 + ((NKB * W_TILE + 1023) & ~1023) + (size_t)STAGES * A_TILE + 512;
+    }
+};
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, unsigned bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src, unsigned bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void mb_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(s32(b)) : "memory");
+}
+
+template <int CIN>
+__global__ void __launch_bounds__(CV_THREADS, 2) k_nn_conv(const __grid_constant__ CUtensorMap tw, ConvArgs a) {
+    using CF = ConvCfg<CIN>;
+    constexpr int BK = CF::BK, SWZ = CF::SWZ, NKB = CF::NKB, S = CF::STAGES;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* sm = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    uint8_t* sw = sm;                                           // NKB weight tiles
-    uint8_t* sa = sm + ((NKB * W_TILE + 1023) & ~1023);         // CONV_STAGES operand tiles
-    uint64_t* wfull = (uint64_t*)(sa + CONV_STAGES * A_TILE);
-    uint64_t* empty = wfull + 1;
-    uint64_t* accum = empty + CONV_STAGES;
-    uint32_t* slot = (uint32_t*)(accum + 1);
+    uint8_t* sw = sm;                                        // NKB weight tiles
+    uint8_t* sa = sm + ((NKB * CF::W_TILE + 1023) & ~1023);  // S operand stages
+    uint64_t* wfull = (uint64_t*)(sa + S * CF::A_TILE);
+    uint64_t* full = wfull + 1;
+    uint64_t* empty = full + S;
+    uint64_t* accf = empty + S;
+    uint64_t* acce = accf + 2;
+    uint32_t* slot = (uint32_t*)(acce + 2);
     float* sbias = (float*)(slot + 4);
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
         mb_init(wfull, 1);
-        for (int s = 0; s < CONV_STAGES; s++) mb_init(&empty[s], 1);
-        mb_init(accum, 1);
+        for (int k = 0; k < S; k++) {
+            mb_init(&full[k], 128);
+            mb_init(&empty[k], 1);
+        }
+        for (int k = 0; k < 2; k++) {
+            mb_init(&accf[k], 1);
+            mb_init(&acce[k], 128);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (tid < 32) sbias[tid] = a.bias[tid];
-    if (warp == 0) tm_alloc(slot, 32);
+    if (warp == 4) tm_alloc(slot, 64);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tacc = *slot;
     bool dead = false;
-    if (tid == 0) {
-        mb_expect_tx(wfull, (unsigned)(NKB * W_TILE));
-        for (int kb = 0; kb < NKB; kb++) tma_2d(sw + kb * W_TILE, &tw, kb * BK, 0, wfull);
-    }
-    mb_wait(wfull, 0, a.err, dead);
     const int pos = a.hout * a.hout;
     const long long rows = (long long)a.nmb * pos;
     const int ntiles = (int)((rows + 127) / 128);
-    const uint32_t idesc = idesc_bf16(128, 32);
-    int it = 0, nt = 0;
-    for (int tile = blockIdx.x; tile < ntiles && !dead; tile += gridDim.x, nt++) {
-        const long long m = (long long)tile * 128 + tid;
-        const bool valid = m < rows;
-        const int b = valid ? (int)(m / pos) : 0, p = valid ? (int)(m % pos) : 0;
-        const int oy = p / a.hout, ox = p % a.hout;
-        const __nv_bfloat16* inb = a.in + (size_t)b * a.in_mb;
-        for (int kb = 0; kb < NKB; kb++, it++) {
-            const int s = it % CONV_STAGES;
-            if (it >= CONV_STAGES && !mb_wait(&empty[s], ((it / CONV_STAGES) - 1) & 1, a.err, dead)) break;
-            uint8_t* rowp = sa + s * A_TILE + tid * SWZ;
-            if (CIN == 2) {
-                // k = tap * 2 + channel for the nine taps, zeros from k = 18
-                uint32_t w[16];
+
+    if (warp < 4) {
+        // ---- gather: row `tid` of every tile, one ring stage per k-block
+        const uint32_t sa0 = s32(sa);
+        int it = 0;
+        for (int tile = blockIdx.x; tile < ntiles && !dead; tile += gridDim.x) {
+            const long long m = (long long)tile * 128 + tid;
+            const bool valid = m < rows;
+            const int b = valid ? (int)(m / pos) : 0, p = valid ? (int)(m % pos) : 0;
+            const int oy = p / a.hout, ox = p % a.hout;
+            const __nv_bfloat16* inb = a.in + (size_t)b * a.in_mb;
+            for (int kb = 0; kb < NKB; kb++, it++) {
+                const int s = it % S;
+                if (it >= S && !mb_wait(&empty[s], ((it / S) - 1) & 1, a.err, dead)) break;
+                const uint32_t row = sa0 + (uint32_t)(s * CF::A_TILE + tid * SWZ);
+                if (CIN == 2) {  // k = tap * 2 + channel: taps 0..8, zeros from tap 9
+                    const int x = (tid >> 1) & 3;
 #pragma unroll
-                for (int t = 0; t < 16; t++) w[t] = 0u;
+                    for (int t = 0; t < 16; t++) {
+                        const int iy = oy * a.stride + t / 3 - 1, ix = ox * a.stride + t % 3 - 1;
+                        const bool in = valid && t < 9 && iy >= 0 && iy < a.hin && ix >= 0 && ix < a.hin;
+                        const __nv_bfloat16* src = in ? inb + ((size_t)iy * a.hin + ix) * 2 : a.in;
+                        cp_async4(row + ((((t >> 2) ^ x)) << 4) + (t & 3) * 4, src, in ? 4u : 0u);
+                    }
+                } else {  // two taps of 32 channels per k-block
+                    const int x = tid & 7;
 #pragma unroll
-                for (int t = 0; t < 9; t++) {
-                    const int iy = oy * a.stride + t / 3 - 1, ix = ox * a.stride + t % 3 - 1;
-                    if (valid && iy >= 0 && iy < a.hin && ix >= 0 && ix < a.hin)
-                        w[t] = *(const uint32_t*)(inb + ((size_t)iy * a.hin + ix) * 2);
-                }
-                const int x = (tid >> 1) & 3;
+                    for (int h = 0; h < 2; h++) {
+                        const int t = 2 * kb + h;
+                        const int iy = oy * a.stride + t / 3 - 1, ix = ox * a.stride + t % 3 - 1;
+                        const bool in = valid && t < 9 && iy >= 0 && iy < a.hin && ix >= 0 && ix < a.hin;
+                        const __nv_bfloat16* src = in ? inb + ((size_t)iy * a.hin + ix) * 32 : a.in;
 #pragma unroll
-                for (int c = 0; c < 4; c++)
-                    *(uint4*)(rowp + ((c ^ x) << 4)) = make_uint4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]);
-            } else {
-                const int x = tid & 7;
-#pragma unroll
-                for (int h = 0; h < 2; h++) {
-                    const int t = 2 * kb + h;
-                    const int iy = oy * a.stride + t / 3 - 1, ix = ox * a.stride + t % 3 - 1;
-                    const bool in = valid && t < 9 && iy >= 0 && iy < a.hin && ix >= 0 && ix < a.hin;
-                    const uint4* src = (const uint4*)(inb + ((size_t)(in ? iy : 0) * a.hin + (in ? ix : 0)) * 32);
-#pragma unroll
-                    for (int c = 0; c < 4; c++) {
-                        const uint4 v = in ? src[c] : make_uint4(0u, 0u, 0u, 0u);
-                        *(uint4*)(rowp + (((4 * h + c) ^ x) << 4)) = v;
+                        for (int c = 0; c < 4; c++)
+                            cp_async16(row + ((((4 * h + c) ^ x)) << 4), in ? src + 8 * c : src, in ? 16u : 0u);
                     }
                 }
-            }
-            fence_async_smem();
-            tc_fence_before();
-            __syncthreads();
-            if (tid == 0) {
-                tc_fence_after();
-                const uint64_t ad = sdesc(s32(sa + s * A_TILE), SWZ), bd = sdesc(s32(sw + kb * W_TILE), SWZ);
-#pragma unroll
-                for (int k = 0; k < BK / 16; k++) umma(tacc, ad + 2 * k, bd + 2 * k, idesc, (kb | k) != 0);
-                umma_commit(&empty[s]);
-                if (kb == NKB - 1) umma_commit(accum);
+                cp_commit();
+                if (it >= CV_LAG) {  // the stage of CV_LAG k-blocks ago has landed: hand it over
+                    cp_wait<CV_LAG>();
+                    fence_async_smem();
+                    mb_arrive(&full[(it - CV_LAG) % S]);
+                }
             }
         }
-        if (dead) break;
-        // epilogue: bias, ReLU, bf16, one 64-byte output row per thread
-        mb_wait(accum, nt & 1, a.err, dead);
-        __syncwarp();  // tcgen05.ld is warp-collective
-        tc_fence_after();
-        uint32_t r0[16], r1[16];
-        tm_ld16(tacc + ((uint32_t)(warp * 32) << 16), r0);
-        tm_ld16(tacc + ((uint32_t)(warp * 32) << 16) + 16u, r1);
-        tc_fence_before();
-        if (valid && !dead) {
-            uint32_t o[16];
+        cp_wait<0>();
+        fence_async_smem();
+        for (int k = it - CV_LAG < 0 ? 0 : it - CV_LAG; k < it; k++) mb_arrive(&full[k % S]);
+    } else if (warp == 4) {
+        // ---- MMA issue (lane 0); the weights by TMA first
+        if (lane == 0) {
+            mb_expect_tx(wfull, (unsigned)(NKB * CF::W_TILE));
+            for (int kb = 0; kb < NKB; kb++) tma_2d(sw + kb * CF::W_TILE, &tw, kb * BK, 0, wfull);
+            mb_wait(wfull, 0, a.err, dead);
+            const uint32_t idesc = idesc_bf16(128, 32);
+            int it = 0, nt = 0;
+            for (int tile = blockIdx.x; tile < ntiles && !dead; tile += gridDim.x, nt++) {
+                const int buf = nt & 1;
+                if (nt >= 2 && !mb_wait(&acce[buf], ((nt >> 1) - 1) & 1, a.err, dead)) break;
+                tc_fence_after();
+                for (int kb = 0; kb < NKB; kb++, it++) {
+                    const int s = it % S;
+                    if (!mb_wait(&full[s], (it / S) & 1, a.err, dead)) break;
+                    tc_fence_after();
+                    const uint64_t ad = sdesc(s32(sa + s * CF::A_TILE), SWZ), bd = sdesc(s32(sw + kb * CF::W_TILE), SWZ);
 #pragma unroll
-            for (int j = 0; j < 8; j++) {
-                o[j] = pack_bf16(fmaxf(__uint_as_float(r0[2 * j]) + sbias[2 * j], 0.0f),
-                                 fmaxf(__uint_as_float(r0[2 * j + 1]) + sbias[2 * j + 1], 0.0f));
-                o[8 + j] = pack_bf16(fmaxf(__uint_as_float(r1[2 * j]) + sbias[16 + 2 * j], 0.0f),
-                                     fmaxf(__uint_as_float(r1[2 * j + 1]) + sbias[16 + 2 * j + 1], 0.0f));
+                    for (int k = 0; k < BK / 16; k++)
+                        umma(tacc + (uint32_t)(buf * 32), ad + 2 * k, bd + 2 * k, idesc, (kb | k) != 0);
+                    umma_commit(&empty[s]);
+                }
+                umma_commit(&accf[buf]);
             }
-            uint4* dst = (uint4*)(a.out + (size_t)b * a.out_mb + (size_t)p * a.out_ld);
+        }
+        __syncwarp();
+    } else {
+        // ---- epilogue: bias, ReLU, bf16, one 64-byte output row per thread
+        const int g = warp & 3, r = g * 32 + lane;
+        int nt = 0;
+        for (int tile = blockIdx.x; tile < ntiles && !dead; tile += gridDim.x, nt++) {
+            const int buf = nt & 1;
+            mb_wait(&accf[buf], (nt >> 1) & 1, a.err, dead);
+            __syncwarp();
+            tc_fence_after();
+            uint32_t r0[16], r1[16];
+            tm_ld16(tacc + ((uint32_t)(g * 32) << 16) + (uint32_t)(buf * 32), r0);
+            tm_ld16(tacc + ((uint32_t)(g * 32) << 16) + (uint32_t)(buf * 32 + 16), r1);
+            tc_fence_before();
+            mb_arrive(&acce[buf]);
+            const long long m = (long long)tile * 128 + r;
+            if (m < rows && !dead) {
+                const int b = (int)(m / pos), p = (int)(m % pos);
+                uint32_t o[16];
 #pragma unroll
-            for (int c = 0; c < 4; c++) dst[c] = make_uint4(o[4 * c], o[4 * c + 1], o[4 * c + 2], o[4 * c + 3]);
+                for (int j = 0; j < 8; j++) {
+                    o[j] = pack_bf16(fmaxf(__uint_as_float(r0[2 * j]) + sbias[2 * j], 0.0f),
+                                     fmaxf(__uint_as_float(r0[2 * j + 1]) + sbias[2 * j + 1], 0.0f));
+                    o[8 + j] = pack_bf16(fmaxf(__uint_as_float(r1[2 * j]) + sbias[16 + 2 * j], 0.0f),
+                                         fmaxf(__uint_as_float(r1[2 * j + 1]) + sbias[16 + 2 * j + 1], 0.0f));
+                }
+                uint4* dst = (uint4*)(a.out + (size_t)b * a.out_mb + (size_t)p * a.out_ld);
+#pragma unroll
+                for (int c = 0; c < 4; c++) dst[c] = make_uint4(o[4 * c], o[4 * c + 1], o[4 * c + 2], o[4 * c + 3]);
+            }
         }
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == 0) tm_dealloc(tacc, 32);
+    if (warp == 4) tm_dealloc(tacc, 64);
 }
 
 // ---- host side: tensor maps
@@ -453,7 +513,9 @@ int nn_gemm(const void* A, int lda, const void* B, int ldb, void* D, int ldd, co
 int nn_conv(int layer, const void* in, int in_mb, const void* W, const float* bias, void* out, int out_mb, int out_ld,
             int nmb, unsigned* err, void* stream) {
     static const int HIN[5] = {0, 24, 12, 6, 6}, HOUT[5] = {0, 12, 6, 6, 3}, STRIDE[5] = {0, 2, 2, 1, 2};
-    if (layer < 1 || layer > 4 || nmb <= 0) return (int)cudaErrorInvalidValue;
+    if (layer < 1 || layer > 4 || nmb <= 0 || ((uintptr_t)in & 15) || ((uintptr_t)out & 15) || out_ld % 8 || in_mb % 8 ||
+        out_mb % 8)
+        return (int)cudaErrorInvalidValue;
     const int cin = layer == 1 ? 2 : 32, bk = layer == 1 ? 32 : 64, k = layer == 1 ? nn::K1 : nn::KC;
     CUtensorMap tw;
     if (!make_map(&tw, W, 32, (uint64_t)k, (uint64_t)k, 32, (uint32_t)bk)) return (int)cudaErrorInvalidValue;
@@ -469,19 +531,22 @@ int nn_conv(int layer, const void* in, int in_mb, const void* W, const float* bi
     a.hout = HOUT[layer];
     a.stride = STRIDE[layer];
     a.err = err;
-    const int nkb = cin == 2 ? 1 : 5;
-    const size_t smem = 1024 + (((size_t)nkb * 32 * bk * 2 + 1023) & ~(size_t)1023) + (size_t)CONV_STAGES * 128 * bk * 2 +
-                        256 + 128;
+    const size_t smem = cin == 2 ? ConvCfg<2>::smem() : ConvCfg<32>::smem();
     const void* fn = cin == 2 ? (const void*)k_nn_conv<2> : (const void*)k_nn_conv<32>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
     const long long rows = (long long)nmb * a.hout * a.hout;
     const int ntiles = (int)((rows + 127) / 128);
-    const int grid = ntiles < num_sms() ? ntiles : num_sms();
+    // persistent CTAs: as many per SM as shared memory allows (64 TMEM columns each), at most 2
+    // (288 threads of at most 96 registers each)
+    int per_sm = (int)((227 * 1024) / (smem + 1024));
+    per_sm = per_sm < 1 ? 1 : (per_sm > 2 ? 2 : per_sm);
+    const int cap = num_sms() * per_sm;
+    const int grid = ntiles < cap ? ntiles : cap;
     if (cin == 2)
-        k_nn_conv<2><<<grid, 128, smem, (cudaStream_t)stream>>>(tw, a);
+        k_nn_conv<2><<<grid, CV_THREADS, smem, (cudaStream_t)stream>>>(tw, a);
     else
-        k_nn_conv<32><<<grid, 128, smem, (cudaStream_t)stream>>>(tw, a);
+        k_nn_conv<32><<<grid, CV_THREADS, smem, (cudaStream_t)stream>>>(tw, a);
     return (int)cudaGetLastError();
 }
 
@@ -502,8 +567,9 @@ __global__ void __launch_bounds__(128) k_prop_features(const uint8_t* __restrict
                                                        int W, int H, const int8_t* __restrict__ prev_coded, int mb0,
                                                        int nmb, __nv_bfloat16* __restrict__ feat,
                                                        __nv_bfloat16* __restrict__ x1) {
-    __shared__ uint8_t R[32][33];
-    __shared__ uint8_t Cb[8][8];
+    __shared__ __align__(16) uint32_t win[64][16];  // the 64x64 reference window
+    __shared__ __align__(16) uint32_t R[32][9];     // its 2x2 averages, 32 bytes + 4 of slack per row
+    __shared__ __align__(16) uint32_t Cb[8][2];     // the current block's 2x2 averages
     __shared__ int pu[nn::NPRED], pv[nn::NPRED], ph[2 * nn::NPRED];
     const int i = blockIdx.x;
     if (i >= nmb) return;
@@ -511,18 +577,29 @@ __global__ void __launch_bounds__(128) k_prop_features(const uint8_t* __restrict
     const int BW = W / 16, BH = H / 16;
     const int bx = mb % BW, by = mb / BW, x0 = bx * 16, y0 = by * 16;
     const int t = threadIdx.x;
-    for (int k = t; k < 32 * 32; k += 128) {
-        const int j = k >> 5, c = k & 31;
-        const int X = x0 - nn::WIN_OFF + 2 * c, Y = y0 - nn::WIN_OFF + 2 * j;
-        const int xa = min(max(X, 0), W - 1), xb = min(max(X + 1, 0), W - 1);
-        const int ya = min(max(Y, 0), H - 1), yb = min(max(Y + 1, 0), H - 1);
-        R[j][c] = (uint8_t)((ref[(size_t)ya * W + xa] + ref[(size_t)ya * W + xb] + ref[(size_t)yb * W + xa] +
-                             ref[(size_t)yb * W + xb] + 2) >> 2);
+    const int wx = x0 - nn::WIN_OFF, wy = y0 - nn::WIN_OFF;
+    if (wx >= 0 && wy >= 0 && wx + 64 <= W && wy + 64 <= H) {  // inside the frame: word loads
+        for (int k = t; k < 64 * 16; k += 128) {
+            const int r = k >> 4, c = k & 15;
+            win[r][c] = *(const uint32_t*)(ref + (size_t)(wy + r) * W + wx + 4 * c);
+        }
+    } else {  // at a border: coordinates clamped per sample
+        for (int k = t; k < 64 * 16; k += 128) {
+            const int r = k >> 4, c = k & 15;
+            const int yy = min(max(wy + r, 0), H - 1);
+            uint32_t v = 0;
+#pragma unroll
+            for (int b = 0; b < 4; b++) {
+                const int xx = min(max(wx + 4 * c + b, 0), W - 1);
+                v |= (uint32_t)ref[(size_t)yy * W + xx] << (8 * b);
+            }
+            win[r][c] = v;
+        }
     }
     if (t < 64) {
         const int j = t >> 3, c = t & 7;
         const uint8_t* p = cur + (size_t)(y0 + 2 * j) * W + x0 + 2 * c;
-        Cb[j][c] = (uint8_t)((p[0] + p[1] + p[W] + p[W + 1] + 2) >> 2);
+        ((uint8_t*)Cb)[j * 8 + c] = (uint8_t)((p[0] + p[1] + p[W] + p[W + 1] + 2) >> 2);
     }
     if (t == 0) {
         int px[nn::NPRED] = {0}, py[nn::NPRED] = {0};
@@ -550,15 +627,37 @@ __global__ void __launch_bounds__(128) k_prop_features(const uint8_t* __restrict
         }
     }
     __syncthreads();
+    // 2x2 rounded averages of the window: thread t makes 8 of the 1024 (two output words)
+    for (int k = t; k < 32 * 8; k += 128) {
+        const int j = k >> 3, c = k & 7;  // output row j, output word c (columns 4c .. 4c+3)
+        const uint8_t* a = (const uint8_t*)win[2 * j] + 8 * c;
+        const uint8_t* b = (const uint8_t*)win[2 * j + 1] + 8 * c;
+        uint32_t v = 0;
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            v |= (uint32_t)((a[2 * q] + a[2 * q + 1] + b[2 * q] + b[2 * q + 1] + 2) >> 2) << (8 * q);
+        R[j][c] = v;
+    }
+    if (t < 32) R[t][8] = 0u;
+    __syncthreads();
     __nv_bfloat16* f = feat + (size_t)i * (nn::FEAT * nn::FEAT * 2);
+    const uint32_t c00 = Cb[0][0], c01 = Cb[0][1], c10 = Cb[1][0], c11 = Cb[1][1], c20 = Cb[2][0], c21 = Cb[2][1],
+                   c30 = Cb[3][0], c31 = Cb[3][1], c40 = Cb[4][0], c41 = Cb[4][1], c50 = Cb[5][0], c51 = Cb[5][1],
+                   c60 = Cb[6][0], c61 = Cb[6][1], c70 = Cb[7][0], c71 = Cb[7][1];
+    const uint32_t cw[8][2] = {{c00, c01}, {c10, c11}, {c20, c21}, {c30, c31},
+                               {c40, c41}, {c50, c51}, {c60, c61}, {c70, c71}};
     for (int k = t; k < nn::FEAT * nn::FEAT; k += 128) {
         const int v = k / nn::FEAT, u = k % nn::FEAT;
-        int sad = 0;
+        const int wq = u >> 2, sh = (u & 3) * 8;
+        unsigned sad = 0;
 #pragma unroll
-        for (int j = 0; j < 8; j++)
-#pragma unroll
-            for (int c = 0; c < 8; c++) sad += abs((int)Cb[j][c] - (int)R[v + j][u + c]);
-        const float f0 = 1.0f - (float)min(sad, 2048) * (1.0f / 1024.0f);
+        for (int j = 0; j < 8; j++) {
+            const uint32_t* row = R[v + j];
+            const uint32_t w0 = row[wq], w1 = row[wq + 1], w2 = row[wq + 2];
+            sad += __vsadu4(__funnelshift_r(w0, w1, sh), cw[j][0]);
+            sad += __vsadu4(__funnelshift_r(w1, w2, sh), cw[j][1]);
+        }
+        const float f0 = 1.0f - (float)min((int)sad, 2048) * (1.0f / 1024.0f);
         float f1 = 0.0f;
 #pragma unroll
         for (int q = 0; q < nn::NPRED; q++)
