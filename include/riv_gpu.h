@@ -260,6 +260,11 @@ riv_status riv_test_delta_bias(const int8_t* dx, const int8_t* dy, uint32_t n, i
  * RIV_ERR_FRAME on malformed data. */
 riv_status riv_test_mv_encode(const uint8_t* blocks, const uint32_t* dims, uint32_t nframes, uint8_t* out, size_t cap,
                               size_t* len, uint32_t* frame_len);
+/* Test hook (host only, no reference counterpart): riv_test_mv_encode with the encoder's parallel
+ * form of the MV coder (the calling thread and a pool of `threads` threads; 0: the sequential
+ * form).  Same bytes. */
+riv_status riv_test_mv_encode_threads(const uint8_t* blocks, const uint32_t* dims, uint32_t nframes, uint32_t threads,
+                                      uint8_t* out, size_t cap, size_t* len, uint32_t* frame_len);
 riv_status riv_test_mv_decode(const uint8_t* data, const uint32_t* frame_len, const uint32_t* dims, uint32_t nframes,
                               uint8_t* blocks);
 /* Test hook (host only, no reference counterpart): the worker-task queue of the fused search

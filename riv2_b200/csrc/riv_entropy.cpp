@@ -536,7 +536,8 @@ static inline int mv_class(unsigned mag) {  // res/mv_rans.rs:80-86
 
 void MvCoder::reset() { *this = MvCoder(); }
 
-static void enc_class(RansWriter& w, BinProb* ctx, int cls) {
+template <class W>
+static void enc_class(W& w, BinProb* ctx, int cls) {
     int lo = 0, hi = 10, d = 0;
     while (lo < hi) {
         int mid = (lo + hi) / 2;
@@ -546,7 +547,8 @@ static void enc_class(RansWriter& w, BinProb* ctx, int cls) {
         d++;
     }
 }
-static void enc_comp(RansWriter& w, int8_t delta, BinProb* cls, BinProb& sign, BinProb* mag) {
+template <class W>
+static void enc_comp(W& w, int8_t delta, BinProb* cls, BinProb& sign, BinProb* mag) {
     unsigned m = (unsigned)std::abs((int)delta);
     int c = mv_class(m);
     enc_class(w, cls, c);
@@ -556,96 +558,214 @@ static void enc_comp(RansWriter& w, int8_t delta, BinProb* cls, BinProb& sign, B
     for (unsigned b = 0; b < bits; b++) w.put((off >> b) & 1, mag[b]);
 }
 
-void MvCoder::encode_frame(const std::vector<MvCodedBlock>& blocks, int bw, std::vector<uint8_t>& out,
-                           const BatchSubmit* submit) {
-    out.clear();
-    // a NEW block with a raw -1/2 subpel: the reference panics ("raw -0.5 subpixel is
-    // disallowed", res/mv_rans/encoder.rs:335-336; no candidate holds one, :379-381)
-    for (const MvCodedBlock& b : blocks)
-        if (b.mode == M_NEW && (b.spx == SP_MINUS || b.spy == SP_MINUS))
-            throw std::runtime_error("raw -0.5 subpixel is disallowed");
-    RansWriter w(&out, submit);
-    std::vector<uint8_t> modes, hits;
-    modes.reserve(blocks.size());
-    hits.reserve(blocks.size());
+// Candidate-history hit of every block (a NEW block whose MV is in the frame's candidate
+// list, res/mv_rans/encoder.rs:199-230); the hit context of a block reads its left and top
+// neighbours' flags.
+std::vector<uint8_t> MvCoder::hit_flags(const std::vector<MvCodedBlock>& blocks) const {
+    std::vector<uint8_t> hits(blocks.size(), 0);
+    if (cands_.empty()) return hits;
     for (size_t i = 0; i < blocks.size(); i++) {
         const MvCodedBlock& b = blocks[i];
+        if (b.mode != M_NEW) continue;
+        const uint32_t key = cand_key(b.dx, b.dy, b.spx, b.spy);
+        for (uint32_t k : cands_)
+            if (k == key) { hits[i] = 1; break; }
+    }
+    return hits;
+}
+
+// The symbols of blocks b0 .. b1-1 (res/mv_rans/encoder.rs:145-255), in stream order, to w
+// (w.put(bit, model)); modes and hits of the neighbours come from the whole frame.
+template <class W>
+void MvCoder::emit(W& w, const std::vector<MvCodedBlock>& blocks, const std::vector<uint8_t>& hits, int bw,
+                   size_t b0, size_t b1) {
+    for (size_t i = b0; i < b1; i++) {
+        const MvCodedBlock& b = blocks[i];
         int bx = (int)(i % bw), by = (int)(i / bw);
-        w.put(b.skip, skip_);
+        w.put(b.skip, c_.skip);
         // mv_mode_context (res/mv_predictor.rs:275-308)
         int score = 0;
         auto sc = [](int m) { return m == M_ZERO ? 2 : (m == M_NEW ? 0 : 1); };
-        if (bx > 0) score += sc(modes[i - 1]);
-        if (by > 0) score += sc(modes[i - bw]);
+        if (bx > 0) score += sc(blocks[i - 1].mode);
+        if (by > 0) score += sc(blocks[i - bw].mode);
         int ctx = std::min(score, 3);
         bool is_new = b.mode == M_NEW;
-        w.put(is_new, m_new_[ctx]);
+        w.put(is_new, c_.m_new[ctx]);
         if (!is_new) {
             bool nz = b.mode != M_ZERO;
-            w.put(nz, m_nz_[ctx]);
+            w.put(nz, c_.m_nz[ctx]);
             if (nz) {
                 bool nr = b.mode == M_NEAR;
-                w.put(nr, m_near_[ctx]);
+                w.put(nr, c_.m_near[ctx]);
                 if (!nr) {
                     bool tm = b.mode == M_TEMPORAL;
-                    w.put(tm, m_tmp_[ctx]);
+                    w.put(tm, c_.m_tmp[ctx]);
                     if (!tm) {
                         bool tr = b.mode == M_TOPRIGHT;
-                        w.put(tr, m_tr_[ctx]);
-                        if (!tr) w.put(b.mode == M_TOPLEFT, m_tl_[ctx]);
+                        w.put(tr, c_.m_tr[ctx]);
+                        if (!tr) w.put(b.mode == M_TOPLEFT, c_.m_tl[ctx]);
                     }
                 }
             }
-            hits.push_back(0);
         } else {
             bool e0 = b.new_base == 0;
-            w.put(e0, b_nearest_[ctx]);
+            w.put(e0, c_.b_nearest[ctx]);
             if (!e0) {
                 bool e1 = b.new_base == 1;
-                w.put(e1, b_near_[ctx]);
+                w.put(e1, c_.b_near[ctx]);
                 if (!e1) {
                     bool e2 = b.new_base == 2;
-                    w.put(e2, b_tr_[ctx]);
-                    if (!e2) w.put(b.new_base == 3, b_tl_[ctx]);
+                    w.put(e2, c_.b_tr[ctx]);
+                    if (!e2) w.put(b.new_base == 3, c_.b_tl[ctx]);
                 }
             }
             bool via = false;
             if (!cands_.empty()) {
-                uint32_t key = cand_key(b.dx, b.dy, b.spx, b.spy);
-                int ci = -1;
-                for (size_t k = 0; k < cands_.size(); k++)
-                    if (cands_[k] == key) { ci = (int)k; break; }
-                bool hit = ci >= 0;
+                const bool hit = hits[i] != 0;
                 int lh = bx > 0 ? hits[i - 1] : 0, th = by > 0 ? hits[i - bw] : 0;
-                w.put(hit, hit_[lh + th]);
+                w.put(hit, c_.hit[lh + th]);
                 if (hit) {
+                    const uint32_t key = cand_key(b.dx, b.dy, b.spx, b.spy);
+                    int ci = 0;
+                    while (cands_[ci] != key) ci++;
                     int lo = 0, hi = 16, d = 0;
                     while (hi - lo > 1) {
                         int mid = (lo + hi) / 2;
                         bool g = ci >= mid;
-                        w.put(g, cidx_[d]);
+                        w.put(g, c_.cidx[d]);
                         if (g) lo = mid; else hi = mid;
                         d++;
                     }
                     via = true;
                 } else {
-                    enc_comp(w, b.dx, cls_x_, sign_x_, mag_x_);
-                    enc_comp(w, b.dy, cls_y_, sign_y_, mag_y_);
+                    enc_comp(w, b.dx, c_.cls_x, c_.sign_x, c_.mag_x);
+                    enc_comp(w, b.dy, c_.cls_y, c_.sign_y, c_.mag_y);
                 }
-                hits.push_back(hit ? 1 : 0);
             } else {
-                enc_comp(w, b.dx, cls_x_, sign_x_, mag_x_);
-                enc_comp(w, b.dy, cls_y_, sign_y_, mag_y_);
-                hits.push_back(0);
+                enc_comp(w, b.dx, c_.cls_x, c_.sign_x, c_.mag_x);
+                enc_comp(w, b.dy, c_.cls_y, c_.sign_y, c_.mag_y);
             }
             if (!via) {
-                w.put(b.spx != SP_ZERO, sub_x_);
-                w.put(b.spy != SP_ZERO, sub_y_);
+                w.put(b.spx != SP_ZERO, c_.sub_x);
+                w.put(b.spy != SP_ZERO, c_.sub_y);
             }
         }
-        modes.push_back(b.mode);
     }
+}
+
+static void check_subpels(const std::vector<MvCodedBlock>& blocks) {
+    // a NEW block with a raw -1/2 subpel: the reference panics ("raw -0.5 subpixel is
+    // disallowed", res/mv_rans/encoder.rs:335-336; no candidate holds one, :379-381)
+    for (const MvCodedBlock& b : blocks)
+        if (b.mode == M_NEW && (b.spx == SP_MINUS || b.spy == SP_MINUS))
+            throw std::runtime_error("raw -0.5 subpixel is disallowed");
+}
+
+void MvCoder::encode_frame(const std::vector<MvCodedBlock>& blocks, int bw, std::vector<uint8_t>& out,
+                           const BatchSubmit* submit) {
+    out.clear();
+    check_subpels(blocks);
+    RansWriter w(&out, submit);
+    const std::vector<uint8_t> hits = hit_flags(blocks);
+    emit(w, blocks, hits, bw, 0, blocks.size());
     w.finish();
+    update(blocks);
+}
+
+namespace {
+constexpr int MV_NMODELS = 80;  // the models of MvCoder::Models
+// Lists the (model, bit) symbols of a block range without touching the models.
+struct MvSymList {
+    const BinProb* base;
+    std::vector<uint16_t> s;  // model | bit << 15
+    uint32_t cnt[MV_NMODELS];
+    void put(bool bit, const BinProb& m) {
+        const int id = (int)(&m - base);
+        s.push_back((uint16_t)(id | (bit ? 0x8000 : 0)));
+        cnt[id]++;
+    }
+};
+}  // namespace
+
+void MvCoder::encode_frame_parallel(const std::vector<MvCodedBlock>& blocks, int bw, std::vector<uint8_t>& out,
+                                    const BatchSubmit& submit, int parts) {
+    static_assert(sizeof(Models) == MV_NMODELS * sizeof(BinProb), "the models must be contiguous");
+    out.clear();
+    check_subpels(blocks);
+    const std::vector<uint8_t> hits = hit_flags(blocks);
+    const size_t nb_ = blocks.size();
+    parts = std::max(1, std::min(parts, (int)std::max<size_t>(1, nb_ / 256)));
+    const BinProb* base = &c_.skip;
+    std::vector<MvSymList> lists(parts);
+    run_parts(submit, parts, [&](int t) {
+        MvSymList& L = lists[t];
+        L.base = base;
+        std::fill(L.cnt, L.cnt + MV_NMODELS, 0u);
+        const size_t b0 = nb_ * t / parts, b1 = nb_ * (t + 1) / parts;
+        L.s.reserve((b1 - b0) * 8);
+        emit(L, blocks, hits, bw, b0, b1);
+    });
+    std::vector<size_t> sbase(parts + 1, 0);
+    for (int t = 0; t < parts; t++) sbase[t + 1] = sbase[t] + lists[t].s.size();
+    const size_t N = sbase[parts], nbatch = (N + BATCH - 1) / BATCH;
+    if (N == 0) {
+        update(blocks);
+        return;
+    }
+    std::vector<uint32_t> cbase(MV_NMODELS + 1), cstart((size_t)parts * MV_NMODELS);
+    uint32_t acc = 0;
+    for (int c = 0; c < MV_NMODELS; c++) {
+        cbase[c] = acc;
+        for (int t = 0; t < parts; t++) {
+            cstart[(size_t)t * MV_NMODELS + c] = acc;
+            acc += lists[t].cnt[c];
+        }
+    }
+    cbase[MV_NMODELS] = acc;
+    std::vector<uint16_t> stacks(nbatch * BATCH);
+    std::vector<uint32_t> occ(acc);  // per model, in stream order: position | bit << 31
+    run_parts(submit, parts, [&](int t) {
+        uint32_t* cs = cstart.data() + (size_t)t * MV_NMODELS;
+        size_t k = sbase[t];
+        for (uint16_t e : lists[t].s) occ[cs[e & 0x7fff]++] = (uint32_t)k++ | (uint32_t)(e >> 15) << 31;
+    });
+    // each model over its own symbols, from its state left by the previous frame
+    BinProb* models = &c_.skip;
+    std::vector<int> order;
+    for (int c = 0; c < MV_NMODELS; c++)
+        if (cbase[c + 1] > cbase[c]) order.push_back(c);
+    std::sort(order.begin(), order.end(), [&](int a, int b) {
+        const uint32_t na = cbase[a + 1] - cbase[a], nb2 = cbase[b + 1] - cbase[b];
+        return na != nb2 ? na > nb2 : a < b;
+    });
+    std::vector<std::vector<int>> groups(parts);
+    std::vector<uint64_t> load(parts, 0);
+    for (int c : order) {
+        const int t = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        groups[t].push_back(c);
+        load[t] += cbase[c + 1] - cbase[c];
+    }
+    run_parts(submit, parts, [&](int t) {
+        for (int c : groups[t]) {
+            BinProb st = models[c];
+            for (uint32_t i = cbase[c]; i < cbase[c + 1]; i++) {
+                const uint32_t e = occ[i];
+                const bool bit = (e >> 31) != 0;
+                stacks[stack_slot(e & 0x7fffffffu)] = (uint16_t)(prob_zero(st) | (bit ? 0x100 : 0));
+                observe(st, bit);
+            }
+            models[c] = st;
+        }
+    });
+    std::vector<std::vector<uint8_t>> bytes(nbatch);
+    std::atomic<size_t> next{0};
+    run_parts(submit, parts, [&](int) {
+        for (size_t j; (j = next.fetch_add(1)) < nbatch;) {
+            const size_t len = std::min<size_t>(BATCH, N - j * BATCH);
+            code_batch(stacks.data() + j * BATCH, (int)(BATCH - len), bytes[j]);
+        }
+    });
+    for (size_t j = 0; j < nbatch; j++) out.insert(out.end(), bytes[j].begin(), bytes[j].end());
     update(blocks);
 }
 
@@ -679,19 +799,19 @@ bool MvCoder::decode_frame(const uint8_t* data, size_t len, int bw, int bh, std:
     for (int i = 0; i < n; i++) {
         const int bx = i % bw, by = i / bw;
         MvCodedBlock& b = out[i];
-        b.skip = r.get(skip_);
+        b.skip = r.get(c_.skip);
         int score = 0;
         auto sc = [](int m) { return m == M_ZERO ? 2 : (m == M_NEW ? 0 : 1); };
         if (bx > 0) score += sc(modes[i - 1]);
         if (by > 0) score += sc(modes[i - bw]);
         const int ctx = std::min(score, 3);
         int mode;
-        if (r.get(m_new_[ctx])) mode = M_NEW;
-        else if (!r.get(m_nz_[ctx])) mode = M_ZERO;
-        else if (r.get(m_near_[ctx])) mode = M_NEAR;
-        else if (r.get(m_tmp_[ctx])) mode = M_TEMPORAL;
-        else if (r.get(m_tr_[ctx])) mode = M_TOPRIGHT;
-        else if (r.get(m_tl_[ctx])) mode = M_TOPLEFT;
+        if (r.get(c_.m_new[ctx])) mode = M_NEW;
+        else if (!r.get(c_.m_nz[ctx])) mode = M_ZERO;
+        else if (r.get(c_.m_near[ctx])) mode = M_NEAR;
+        else if (r.get(c_.m_tmp[ctx])) mode = M_TEMPORAL;
+        else if (r.get(c_.m_tr[ctx])) mode = M_TOPRIGHT;
+        else if (r.get(c_.m_tl[ctx])) mode = M_TOPLEFT;
         else mode = M_NEAREST;
         b.mode = (uint8_t)mode;
         b.new_base = 0;
@@ -699,19 +819,19 @@ bool MvCoder::decode_frame(const uint8_t* data, size_t len, int bw, int bh, std:
         b.spx = b.spy = SP_ZERO;
         hits[i] = 0;
         if (mode == M_NEW) {
-            if (r.get(b_nearest_[ctx])) b.new_base = 0;
-            else if (r.get(b_near_[ctx])) b.new_base = 1;
-            else if (r.get(b_tr_[ctx])) b.new_base = 2;
-            else b.new_base = r.get(b_tl_[ctx]) ? 3 : 4;
+            if (r.get(c_.b_nearest[ctx])) b.new_base = 0;
+            else if (r.get(c_.b_near[ctx])) b.new_base = 1;
+            else if (r.get(c_.b_tr[ctx])) b.new_base = 2;
+            else b.new_base = r.get(c_.b_tl[ctx]) ? 3 : 4;
             bool via = false;
             if (!cands_.empty()) {
                 const int lh = bx > 0 ? hits[i - 1] : 0, th = by > 0 ? hits[i - bw] : 0;
-                const bool hit = r.get(hit_[lh + th]);
+                const bool hit = r.get(c_.hit[lh + th]);
                 if (hit) {
                     int lo = 0, hi = 16, d = 0;
                     while (hi - lo > 1) {
                         const int mid = (lo + hi) / 2;
-                        if (r.get(cidx_[d])) lo = mid;
+                        if (r.get(c_.cidx[d])) lo = mid;
                         else hi = mid;
                         d++;
                     }
@@ -724,17 +844,17 @@ bool MvCoder::decode_frame(const uint8_t* data, size_t len, int bw, int bh, std:
                         via = true;
                     }
                 } else {
-                    b.dx = dec_comp(r, cls_x_, sign_x_, mag_x_);
-                    b.dy = dec_comp(r, cls_y_, sign_y_, mag_y_);
+                    b.dx = dec_comp(r, c_.cls_x, c_.sign_x, c_.mag_x);
+                    b.dy = dec_comp(r, c_.cls_y, c_.sign_y, c_.mag_y);
                 }
                 hits[i] = hit ? 1 : 0;
             } else {
-                b.dx = dec_comp(r, cls_x_, sign_x_, mag_x_);
-                b.dy = dec_comp(r, cls_y_, sign_y_, mag_y_);
+                b.dx = dec_comp(r, c_.cls_x, c_.sign_x, c_.mag_x);
+                b.dy = dec_comp(r, c_.cls_y, c_.sign_y, c_.mag_y);
             }
             if (!via) {
-                b.spx = r.get(sub_x_) ? SP_PLUS : SP_ZERO;
-                b.spy = r.get(sub_y_) ? SP_PLUS : SP_ZERO;
+                b.spx = r.get(c_.sub_x) ? SP_PLUS : SP_ZERO;
+                b.spy = r.get(c_.sub_y) ? SP_PLUS : SP_ZERO;
             }
         }
         modes[i] = (uint8_t)mode;
@@ -744,28 +864,55 @@ bool MvCoder::decode_frame(const uint8_t* data, size_t len, int bw, int bh, std:
     return true;
 }
 
+// dense index of a candidate key (cand_key): (dx, dy) bytes and the two subpels (0..2)
+static inline uint32_t key_index(uint32_t key) {
+    return ((key >> 16) * 3 + ((key >> 8) & 0xff)) * 3 + (key & 0xff);
+}
+
 void MvCoder::update(const std::vector<MvCodedBlock>& blocks) {  // encoder.rs:370-412
-    for (auto& kv : counts_) kv.second = (kv.second * 7) / 8;
+    if (cnt_.empty()) {
+        cnt_.assign(65536u * 9u, 0u);
+        listed_.assign(65536u * 9u, 0);
+    }
+    for (uint32_t k : active_) {
+        uint32_t& c = cnt_[key_index(k)];
+        c = (c * 7) / 8;
+    }
     total_ = (total_ * 7) / 8;
     for (auto& b : blocks)
         if (b.mode == M_NEW) {
-            counts_[cand_key(b.dx, b.dy, b.spx, b.spy)] += 1;
+            const uint32_t key = cand_key(b.dx, b.dy, b.spx, b.spy), i = key_index(key);
+            if (!listed_[i]) {
+                listed_[i] = 1;
+                active_.push_back(key);
+            }
+            cnt_[i] += 1;
             total_++;
         }
-    for (auto it = counts_.begin(); it != counts_.end();)
-        if (it->second == 0) it = counts_.erase(it); else ++it;
+    // drop the keys whose count decayed to zero (the reference removes them)
+    size_t w = 0;
+    for (uint32_t k : active_) {
+        const uint32_t i = key_index(k);
+        if (cnt_[i]) active_[w++] = k;
+        else listed_[i] = 0;
+    }
+    active_.resize(w);
     cands_.clear();
     if (total_ < 100) return;
-    std::vector<std::pair<uint32_t, uint32_t>> s(counts_.begin(), counts_.end());
-    std::sort(s.begin(), s.end(), [](const std::pair<uint32_t, uint32_t>& a, const std::pair<uint32_t, uint32_t>& b) {
+    // the 16 most frequent keys above 1 % of the total, ties to the smaller key
+    const uint32_t thr = total_ / 100;
+    std::vector<std::pair<uint32_t, uint32_t>> s;
+    for (uint32_t k : active_) {
+        const uint32_t c = cnt_[key_index(k)];
+        if (c > thr) s.emplace_back(k, c);
+    }
+    auto better = [](const std::pair<uint32_t, uint32_t>& a, const std::pair<uint32_t, uint32_t>& b) {
         if (a.second != b.second) return a.second > b.second;
         return a.first < b.first;
-    });
-    uint32_t thr = total_ / 100;
-    for (auto& e : s) {
-        if (cands_.size() >= 16) break;
-        if (e.second > thr) cands_.push_back(e.first);
-    }
+    };
+    const size_t take = std::min<size_t>(16, s.size());
+    std::partial_sort(s.begin(), s.begin() + take, s.end(), better);
+    for (size_t k = 0; k < take; k++) cands_.push_back(s[k].first);
 }
 
 void compute_delta_bias(const std::vector<std::pair<int8_t, int8_t>>& d, int8_t& bx, int8_t& by) {

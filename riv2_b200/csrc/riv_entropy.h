@@ -108,13 +108,30 @@ public:
     // encoder, so a decoder instance follows the encoder's across frames.  false on bad data.
     bool decode_frame(const uint8_t* data, size_t len, int bw, int bh, std::vector<MvCodedBlock>& out);
 
+    // The same bytes as encode_frame, with the context modelling split `parts` ways (this
+    // thread and submit): each part lists the (model, bit) symbols of a range of MBs, each
+    // model then runs over its own symbols from its state of the previous frame, and the rANS
+    // batches are coded in parallel.
+    void encode_frame_parallel(const std::vector<MvCodedBlock>& blocks, int bw, std::vector<uint8_t>& out,
+                               const BatchSubmit& submit, int parts);
+
 private:
     void update(const std::vector<MvCodedBlock>& blocks);
-    BinProb skip_, m_new_[4], m_nz_[4], m_near_[4], m_tmp_[4], m_tr_[4], m_tl_[4], b_nearest_[4], b_near_[4],
-        b_tr_[4], b_tl_[4], cls_x_[4], cls_y_[4], sign_x_, sign_y_, mag_x_[10], mag_y_[10], sub_x_, sub_y_,
-        hit_[3], cidx_[4];
+    template <class W>
+    void emit(W& w, const std::vector<MvCodedBlock>& blocks, const std::vector<uint8_t>& hits, int bw, size_t b0,
+              size_t b1);
+    std::vector<uint8_t> hit_flags(const std::vector<MvCodedBlock>& blocks) const;
+    // every adaptive model of the coder, contiguous (a model's index is its position here)
+    struct Models {
+        BinProb skip, m_new[4], m_nz[4], m_near[4], m_tmp[4], m_tr[4], m_tl[4], b_nearest[4], b_near[4], b_tr[4],
+            b_tl[4], cls_x[4], cls_y[4], sign_x, sign_y, mag_x[10], mag_y[10], sub_x, sub_y, hit[3], cidx[4];
+    } c_;
     std::vector<uint32_t> cands_;  // packed keys
-    std::unordered_map<uint32_t, uint32_t> counts_;
+    // candidate-history counts: one counter per (dx, dy, subpel x, subpel y) (allocated on first
+    // use), and the keys whose counter is listed (non-zero, or decayed to zero this frame)
+    std::vector<uint32_t> cnt_;
+    std::vector<uint8_t> listed_;
+    std::vector<uint32_t> active_;
     uint32_t total_ = 0;
 };
 

@@ -1882,17 +1882,29 @@ static riv::MvCodedBlock mv_block_from(const uint8_t* r) {
 
 riv_status riv_test_mv_encode(const uint8_t* blocks, const uint32_t* dims, uint32_t nframes, uint8_t* out, size_t cap,
                               size_t* len, uint32_t* frame_len) {
+    return riv_test_mv_encode_threads(blocks, dims, nframes, 0, out, cap, len, frame_len);
+}
+
+riv_status riv_test_mv_encode_threads(const uint8_t* blocks, const uint32_t* dims, uint32_t nframes, uint32_t threads,
+                                      uint8_t* out, size_t cap, size_t* len, uint32_t* frame_len) {
     if (!len || (nframes > 0 && (!blocks || !dims || !frame_len))) return RIV_ERR_FRAME;
     entropy_init();
     riv::MvCoder coder;
     std::vector<uint8_t> all, fb;
+    std::unique_ptr<ThreadPool> pool(threads > 0 ? new ThreadPool(threads) : nullptr);
+    BatchSubmit submit;
+    if (pool) {
+        ThreadPool* tp = pool.get();
+        submit = [tp](std::function<void()> f) { return tp->submit(std::move(f)); };
+    }
     size_t k = 0;
     try {
         for (uint32_t f = 0; f < nframes; f++) {
             const size_t n = (size_t)dims[2 * f] * dims[2 * f + 1];
             std::vector<riv::MvCodedBlock> v(n);
             for (size_t i = 0; i < n; i++, k++) v[i] = mv_block_from(blocks + 7 * k);
-            coder.encode_frame(v, (int)dims[2 * f], fb);
+            if (pool) coder.encode_frame_parallel(v, (int)dims[2 * f], fb, submit, (int)threads + 1);
+            else coder.encode_frame(v, (int)dims[2 * f], fb);
             frame_len[f] = (uint32_t)fb.size();
             all.insert(all.end(), fb.begin(), fb.end());
         }

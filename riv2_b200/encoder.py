@@ -114,7 +114,7 @@ EXPORTED_SYMBOLS = (
     "riv_decoder_last_error", "riv_decoder_free", "riv_test_dct_encode", "riv_test_dct_decode", "riv_test_mv_encode",
     "riv_test_mv_decode", "riv_test_delta_bias", "riv_test_worker_queue", "riv_test_libm_range",
     "riv_stage_predict", "riv_stage_residual", "riv_test_wait_expiry", "riv_encoder_set_proposal",
-    "riv_learned_counters",
+    "riv_learned_counters", "riv_test_mv_encode_threads",
 )
 
 
@@ -133,6 +133,7 @@ def lib() -> C.CDLL:
     L.riv_test_dct_decode.argtypes = [P, C.c_size_t, P, C.c_uint32, C.c_int, P]
     L.riv_test_mv_encode.argtypes = [P, P, C.c_uint32, P, C.c_size_t, C.POINTER(C.c_size_t), P]
     L.riv_test_mv_decode.argtypes = [P, P, P, C.c_uint32, P]
+    L.riv_test_mv_encode_threads.argtypes = [P, P, C.c_uint32, C.c_uint32, P, C.c_size_t, C.POINTER(C.c_size_t), P]
     L.riv_test_delta_bias.argtypes = [P, P, C.c_uint32, P, P]
     L.riv_test_worker_queue.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_int, C.c_int, C.c_int, P,
                                         C.c_size_t, C.POINTER(C.c_size_t)]
@@ -646,10 +647,11 @@ def delta_bias_host(dx: np.ndarray, dy: np.ndarray):
     return bx.value, by.value
 
 
-def mv_encode_host(blocks: np.ndarray, dims) -> list:
+def mv_encode_host(blocks: np.ndarray, dims, threads: int = 0) -> list:
     """The encoder's host MV coder over a sequence of frames, one coder throughout (test hook,
     no GPU needed): blocks is (total blocks, 7) uint8 (mode, NEW base, dx, dy, subpel x,
-    subpel y, skip), dims the (bw, bh) of each frame.  Returns each frame's bytes; raises
+    subpel y, skip), dims the (bw, bh) of each frame.  threads > 0: the parallel form the
+    encoder runs (this thread and a pool of that many).  Returns each frame's bytes; raises
     EncodingFailed where the reference encoder panics (a NEW block with a raw -1/2 subpel)."""
     b = np.ascontiguousarray(blocks, dtype=np.uint8)
     d = np.ascontiguousarray(np.asarray(dims, dtype=np.uint32).reshape(-1))
@@ -658,11 +660,13 @@ def mv_encode_host(blocks: np.ndarray, dims) -> list:
     if b.ndim != 2 or b.shape[1] != 7 or b.shape[0] != int(sum(int(d[2 * f]) * int(d[2 * f + 1]) for f in range(nf))):
         raise ValueError("blocks must be (sum of bw * bh over the frames, 7)")
     n = C.c_size_t(0)
-    st = lib().riv_test_mv_encode(b.ctypes.data, d.ctypes.data, nf, None, 0, C.byref(n), fl.ctypes.data)
+    st = lib().riv_test_mv_encode_threads(b.ctypes.data, d.ctypes.data, nf, threads, None, 0, C.byref(n),
+                                          fl.ctypes.data)
     if st != 0:
         raise _ERRORS.get(st, EncodeError)(f"riv_test_mv_encode failed (status {st})")
     out = np.zeros(max(n.value, 1), np.uint8)
-    lib().riv_test_mv_encode(b.ctypes.data, d.ctypes.data, nf, out.ctypes.data, n.value, C.byref(n), fl.ctypes.data)
+    lib().riv_test_mv_encode_threads(b.ctypes.data, d.ctypes.data, nf, threads, out.ctypes.data, n.value, C.byref(n),
+                                     fl.ctypes.data)
     frames, pos = [], 0
     for f in range(nf):
         frames.append(out[pos:pos + int(fl[f])].tobytes())

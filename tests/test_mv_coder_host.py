@@ -139,3 +139,44 @@ def test_delta_bias_matches_oracle(case):
         dy = rng.choice([-128, 127, -24, 24, 1], 3000)
     dx, dy = np.asarray(dx, np.int8), np.asarray(dy, np.int8)
     assert delta_bias_host(dx, dy) == O.delta_bias(dx, dy)
+
+
+def _random_sequence(nf, bw, bh, seed):
+    """Frames of every mode, NEW blocks drawn from a small set of MVs so that the candidate
+    history fills (hits, candidate indices) and carries across frames."""
+    rng = np.random.default_rng(seed)
+    frames = []
+    pool = [(int(a), int(b), int(c), int(d)) for a, b, c, d in zip(rng.integers(-20, 21, 24), rng.integers(-20, 21, 24),
+                                                                 rng.integers(0, 2, 24), rng.integers(0, 2, 24))]
+    for _ in range(nf):
+        n = bw * bh
+        f = np.zeros((n, 7), np.uint8)
+        f[:, 0] = rng.choice([ZERO, NEAREST, NEAR, TOPRIGHT, TOPLEFT, NEW, TEMPORAL], n,
+                             p=[0.2, 0.3, 0.1, 0.05, 0.05, 0.25, 0.05])
+        new = f[:, 0] == NEW
+        f[new, 1] = rng.integers(0, 5, new.sum())
+        pick = rng.integers(0, len(pool), new.sum())
+        for j, (i, k) in enumerate(zip(np.nonzero(new)[0], pick)):
+            dx, dy, sx, sy = pool[k] if rng.random() < 0.7 else (int(rng.integers(-100, 101)), int(rng.integers(-100, 101)),
+                                                                int(rng.integers(0, 2)), int(rng.integers(0, 2)))
+            f[i, 2:6] = (dx & 0xFF, dy & 0xFF, sx, sy)
+        f[:, 6] = rng.random(n) < 0.3
+        frames.append(f)
+    return frames
+
+
+@pytest.mark.parametrize("threads", [1, 2, 3, 7])
+def test_parallel_mv_coder_is_byte_identical(threads):
+    """The encoder's parallel MV coder (symbol lists per MB range, each model over its own
+    symbols, rANS batches in parallel) writes the sequential coder's bytes, and the oracle's,
+    frame after frame (contexts and candidate history carried), for frames of one rANS batch
+    and of several."""
+    from riv2_b200.encoder import mv_encode_host
+    for bw, bh, nf in ((120, 68, 4), (16, 9, 6), (240, 135, 2)):
+        frames = _random_sequence(nf, bw, bh, seed=bw + threads)
+        blocks = np.concatenate(frames)
+        dims = [(bw, bh)] * nf
+        seq = mv_encode_host(blocks, dims)
+        par = mv_encode_host(blocks, dims, threads=threads)
+        assert par == seq, (bw, bh)
+        assert seq == O.mv_encode(blocks, dims)
