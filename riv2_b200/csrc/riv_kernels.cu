@@ -2607,6 +2607,10 @@ int launch_search(const SearchParams& p, const SearchPlan& plan, void* stream) {
 // MVs, and runs for all MBs at once (k_learned_mode).
 // ---------------------------------------------------------------------------------
 constexpr int LS_MBS = 4;  // MBs (warps) per CTA: consecutive MBs of one row
+// Width of the shared reference window of a CTA: its MBs, +-(sr + 2) columns, up to 3 more on
+// the left (the left edge is rounded down to a 4-byte boundary) and 4 bytes of slack for the
+// unaligned word reads; a multiple of 4.
+__host__ __device__ constexpr int ls_window_width(int sr) { return ((16 * LS_MBS + 2 * (sr + 2) + 3 + 3) & ~3) + 4; }
 
 struct LearnedMv {
     int8_t raw[4];  // dx, dy, sx, sy (canonical)
@@ -2657,13 +2661,22 @@ __global__ void __launch_bounds__(32 * LS_MBS) k_learned_search(LearnedParams lp
     const int sr = p.sr, M = sr + 2;
     const int bx0 = blockIdx.x * LS_MBS, by = blockIdx.y;
     const int nmb_here = min(LS_MBS, p.BW - bx0);
-    const int wx0 = bx0 * 16 - M, wy0 = by * 16 - M;
-    const int ws = ((16 * LS_MBS + 2 * M + 3) & ~3) + 4, wh = 16 + 2 * M + 1;
-    // stage the window with coordinates clamped to the plane (replicated borders)
-    for (int i = threadIdx.x; i < ws * wh; i += blockDim.x) {
-        const int y = i / ws, x = i - y * ws;
-        const int fy = min(max(wy0 + y, 0), p.H - 1), fx = min(max(wx0 + x, 0), p.W - 1);
-        lsm[i] = p.ref_y[(size_t)fy * p.W + fx];
+    const int wx0 = (bx0 * 16 - M) & ~3, wy0 = by * 16 - M;  // left edge on a 4-byte boundary
+    const int ws = ls_window_width(sr), wh = 16 + 2 * M + 1;
+    // stage the window with coordinates clamped to the plane (replicated borders); word loads
+    // when it lies inside the plane
+    if (wx0 >= 0 && wy0 >= 0 && wx0 + ws <= p.W && wy0 + wh <= p.H) {
+        const int wpr = ws / 4;
+        for (int i = threadIdx.x; i < wpr * wh; i += blockDim.x) {
+            const int y = i / wpr, x = i - y * wpr;
+            ((uint32_t*)lsm)[i] = *(const uint32_t*)(p.ref_y + (size_t)(wy0 + y) * p.W + wx0 + 4 * x);
+        }
+    } else {
+        for (int i = threadIdx.x; i < ws * wh; i += blockDim.x) {
+            const int y = i / ws, x = i - y * ws;
+            const int fy = min(max(wy0 + y, 0), p.H - 1), fx = min(max(wx0 + x, 0), p.W - 1);
+            lsm[i] = p.ref_y[(size_t)fy * p.W + fx];
+        }
     }
     __syncthreads();
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -2887,7 +2900,7 @@ int launch_learned(const SearchParams& sp, const float* net, int margin, float s
     lp.out = (LearnedMv*)lmv;
     lp.counters = counters;
     const int M = sp.sr + 2;
-    const int ws = ((16 * LS_MBS + 2 * M + 3) & ~3) + 4, wh = 16 + 2 * M + 1;
+    const int ws = ls_window_width(sp.sr), wh = 16 + 2 * M + 1;
     const size_t smem = (size_t)ws * wh + 16;
     dim3 grid((sp.BW + LS_MBS - 1) / LS_MBS, sp.BH);
     k_learned_search<<<grid, 32 * LS_MBS, smem, (cudaStream_t)stream>>>(lp);

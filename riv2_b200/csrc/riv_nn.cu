@@ -401,10 +401,13 @@ __global__ void __launch_bounds__(CV_THREADS, 2) k_nn_conv(const __grid_constant
         // ---- epilogue: bias, ReLU, bf16, one 64-byte output row per thread
         const int g = warp & 3, r = g * 32 + lane;
         int nt = 0;
-        for (int tile = blockIdx.x; tile < ntiles && !dead; tile += gridDim.x, nt++) {
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, nt++) {
             const int buf = nt & 1;
-            mb_wait(&accf[buf], (nt >> 1) & 1, a.err, dead);
-            __syncwarp();
+            const bool ok = mb_wait(&accf[buf], (nt >> 1) & 1, a.err, dead);
+            if (!__all_sync(0xffffffffu, ok)) {  // warp-uniform: tcgen05.ld is warp-collective
+                dead = true;
+                break;
+            }
             tc_fence_after();
             uint32_t r0[16], r1[16];
             tm_ld16(tacc + ((uint32_t)(g * 32) << 16) + (uint32_t)(buf * 32), r0);
@@ -563,29 +566,34 @@ int nn_conv(int layer, const void* in, int in_mb, const void* W, const float* bi
 // to fc1's input row (columns 288 .. 303; 304 .. 319 zero).
 __device__ __forceinline__ int med3(int a, int b, int c) { return max(min(a, b), min(max(a, b), c)); }
 
-__global__ void __launch_bounds__(128) k_prop_features(const uint8_t* __restrict__ cur, const uint8_t* __restrict__ ref,
+constexpr int PF_MBS = 4;               // MBs of a row per CTA
+constexpr int PF_WW = 16 * PF_MBS + 48;  // window width shared by them (full resolution)
+
+__global__ void __launch_bounds__(256) k_prop_features(const uint8_t* __restrict__ cur, const uint8_t* __restrict__ ref,
                                                        int W, int H, const int8_t* __restrict__ prev_coded, int mb0,
                                                        int nmb, __nv_bfloat16* __restrict__ feat,
                                                        __nv_bfloat16* __restrict__ x1) {
-    __shared__ __align__(16) uint32_t win[64][16];  // the 64x64 reference window
-    __shared__ __align__(16) uint32_t R[32][9];     // its 2x2 averages, 32 bytes + 4 of slack per row
-    __shared__ __align__(16) uint32_t Cb[8][2];     // the current block's 2x2 averages
-    __shared__ int pu[nn::NPRED], pv[nn::NPRED], ph[2 * nn::NPRED];
-    const int i = blockIdx.x;
-    if (i >= nmb) return;
-    const int mb = mb0 + i;
+    __shared__ __align__(16) uint32_t win[64][PF_WW / 4];   // reference window, 4 MBs wide
+    __shared__ __align__(16) uint32_t R[32][PF_WW / 8 + 1];  // its 2x2 averages (+ a word of slack)
+    __shared__ __align__(16) uint32_t Cb[PF_MBS][8][2];     // the current blocks' 2x2 averages
+    __shared__ int pu[PF_MBS][nn::NPRED], pv[PF_MBS][nn::NPRED], ph[PF_MBS][2 * nn::NPRED];
     const int BW = W / 16, BH = H / 16;
-    const int bx = mb % BW, by = mb / BW, x0 = bx * 16, y0 = by * 16;
     const int t = threadIdx.x;
-    const int wx = x0 - nn::WIN_OFF, wy = y0 - nn::WIN_OFF;
-    if (wx >= 0 && wy >= 0 && wx + 64 <= W && wy + 64 <= H) {  // inside the frame: word loads
-        for (int k = t; k < 64 * 16; k += 128) {
-            const int r = k >> 4, c = k & 15;
+    // the CTA's MBs: PF_MBS consecutive MBs of one row, starting at raster index first
+    const int rows_groups = (BW + PF_MBS - 1) / PF_MBS;
+    const int gi = blockIdx.x, by = gi / rows_groups, bx0 = (gi % rows_groups) * PF_MBS;
+    const int nhere = min(PF_MBS, BW - bx0);
+    const int first = by * BW + bx0;
+    if (first + nhere <= mb0 || first >= mb0 + nmb) return;
+    const int wx = bx0 * 16 - nn::WIN_OFF, wy = by * 16 - nn::WIN_OFF;
+    if (wx >= 0 && wy >= 0 && wx + PF_WW <= W && wy + 64 <= H) {  // inside the frame: word loads
+        for (int k = t; k < 64 * (PF_WW / 4); k += 256) {
+            const int r = k / (PF_WW / 4), c = k % (PF_WW / 4);
             win[r][c] = *(const uint32_t*)(ref + (size_t)(wy + r) * W + wx + 4 * c);
         }
     } else {  // at a border: coordinates clamped per sample
-        for (int k = t; k < 64 * 16; k += 128) {
-            const int r = k >> 4, c = k & 15;
+        for (int k = t; k < 64 * (PF_WW / 4); k += 256) {
+            const int r = k / (PF_WW / 4), c = k % (PF_WW / 4);
             const int yy = min(max(wy + r, 0), H - 1);
             uint32_t v = 0;
 #pragma unroll
@@ -596,12 +604,13 @@ __global__ void __launch_bounds__(128) k_prop_features(const uint8_t* __restrict
             win[r][c] = v;
         }
     }
-    if (t < 64) {
-        const int j = t >> 3, c = t & 7;
-        const uint8_t* p = cur + (size_t)(y0 + 2 * j) * W + x0 + 2 * c;
-        ((uint8_t*)Cb)[j * 8 + c] = (uint8_t)((p[0] + p[1] + p[W] + p[W + 1] + 2) >> 2);
+    if (t < 64 * nhere) {
+        const int m = t >> 6, j = (t >> 3) & 7, c = t & 7;
+        const uint8_t* p = cur + (size_t)(by * 16 + 2 * j) * W + (bx0 + m) * 16 + 2 * c;
+        ((uint8_t*)Cb[m])[j * 8 + c] = (uint8_t)((p[0] + p[1] + p[W] + p[W + 1] + 2) >> 2);
     }
-    if (t == 0) {
+    if (t < nhere) {
+        const int bx = bx0 + t;
         int px[nn::NPRED] = {0}, py[nn::NPRED] = {0};
         if (prev_coded) {
             auto get = [&](int xx, int yy, int& hx, int& hy) {
@@ -620,54 +629,55 @@ __global__ void __launch_bounds__(128) k_prop_features(const uint8_t* __restrict
         }
         for (int k = 0; k < nn::NPRED; k++) {
             // nearest half-resolution offset of the MV (half-pel units / 4, rounded half up)
-            pu[k] = ((px[k] + 2) >> 2) + 12;
-            pv[k] = ((py[k] + 2) >> 2) + 12;
-            ph[2 * k] = px[k];
-            ph[2 * k + 1] = py[k];
+            pu[t][k] = ((px[k] + 2) >> 2) + 12;
+            pv[t][k] = ((py[k] + 2) >> 2) + 12;
+            ph[t][2 * k] = px[k];
+            ph[t][2 * k + 1] = py[k];
         }
     }
     __syncthreads();
-    // 2x2 rounded averages of the window: thread t makes 8 of the 1024 (two output words)
-    for (int k = t; k < 32 * 8; k += 128) {
-        const int j = k >> 3, c = k & 7;  // output row j, output word c (columns 4c .. 4c+3)
-        const uint8_t* a = (const uint8_t*)win[2 * j] + 8 * c;
-        const uint8_t* b = (const uint8_t*)win[2 * j + 1] + 8 * c;
-        uint32_t v = 0;
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-            v |= (uint32_t)((a[2 * q] + a[2 * q + 1] + b[2 * q] + b[2 * q + 1] + 2) >> 2) << (8 * q);
-        R[j][c] = v;
+    // 2x2 rounded averages of the window, four output bytes per step
+    for (int k = t; k < 32 * (PF_WW / 8); k += 256) {
+        const int j = k / (PF_WW / 8), c = k % (PF_WW / 8);  // output row j, output word c
+        const uint32_t a0 = win[2 * j][2 * c], a1 = win[2 * j][2 * c + 1];
+        const uint32_t b0 = win[2 * j + 1][2 * c], b1 = win[2 * j + 1][2 * c + 1];
+        const uint32_t M = 0x00FF00FFu;
+        // pair sums of adjacent bytes in 16-bit lanes: lane 0 = bytes 0+1, lane 1 = bytes 2+3
+        const uint32_t s0 = (a0 & M) + ((a0 >> 8) & M) + (b0 & M) + ((b0 >> 8) & M) + 0x00020002u;
+        const uint32_t s1 = (a1 & M) + ((a1 >> 8) & M) + (b1 & M) + ((b1 >> 8) & M) + 0x00020002u;
+        R[j][c] = ((s0 >> 2) & 0xFFu) | (((s0 >> 18) & 0xFFu) << 8) | (((s1 >> 2) & 0xFFu) << 16) |
+                  (((s1 >> 18) & 0xFFu) << 24);
     }
-    if (t < 32) R[t][8] = 0u;
+    if (t < 32) R[t][PF_WW / 8] = 0u;
     __syncthreads();
-    __nv_bfloat16* f = feat + (size_t)i * (nn::FEAT * nn::FEAT * 2);
-    const uint32_t c00 = Cb[0][0], c01 = Cb[0][1], c10 = Cb[1][0], c11 = Cb[1][1], c20 = Cb[2][0], c21 = Cb[2][1],
-                   c30 = Cb[3][0], c31 = Cb[3][1], c40 = Cb[4][0], c41 = Cb[4][1], c50 = Cb[5][0], c51 = Cb[5][1],
-                   c60 = Cb[6][0], c61 = Cb[6][1], c70 = Cb[7][0], c71 = Cb[7][1];
-    const uint32_t cw[8][2] = {{c00, c01}, {c10, c11}, {c20, c21}, {c30, c31},
-                               {c40, c41}, {c50, c51}, {c60, c61}, {c70, c71}};
-    for (int k = t; k < nn::FEAT * nn::FEAT; k += 128) {
-        const int v = k / nn::FEAT, u = k % nn::FEAT;
-        const int wq = u >> 2, sh = (u & 3) * 8;
+    for (int k = t; k < nhere * nn::FEAT * nn::FEAT; k += 256) {
+        const int m = k / (nn::FEAT * nn::FEAT), kk = k % (nn::FEAT * nn::FEAT);
+        const int mb = first + m;
+        if (mb < mb0 || mb >= mb0 + nmb) continue;
+        const int v = kk / nn::FEAT, u = kk % nn::FEAT;
+        const int uu = 8 * m + u, wq = uu >> 2, sh = (uu & 3) * 8;
         unsigned sad = 0;
 #pragma unroll
         for (int j = 0; j < 8; j++) {
             const uint32_t* row = R[v + j];
             const uint32_t w0 = row[wq], w1 = row[wq + 1], w2 = row[wq + 2];
-            sad += __vsadu4(__funnelshift_r(w0, w1, sh), cw[j][0]);
-            sad += __vsadu4(__funnelshift_r(w1, w2, sh), cw[j][1]);
+            sad += __vsadu4(__funnelshift_r(w0, w1, sh), Cb[m][j][0]);
+            sad += __vsadu4(__funnelshift_r(w1, w2, sh), Cb[m][j][1]);
         }
         const float f0 = 1.0f - (float)min((int)sad, 2048) * (1.0f / 1024.0f);
         float f1 = 0.0f;
 #pragma unroll
         for (int q = 0; q < nn::NPRED; q++)
-            if (pu[q] == u && pv[q] == v) f1 = 1.0f;
-        *(uint32_t*)(f + 2 * k) = pack_bf16(f0, f1);
+            if (pu[m][q] == u && pv[m][q] == v) f1 = 1.0f;
+        *(uint32_t*)(feat + (size_t)(mb - mb0) * (nn::FEAT * nn::FEAT * 2) + 2 * kk) = pack_bf16(f0, f1);
     }
-    if (t < 16) {
-        const float v = t < 2 * nn::NPRED ? (float)ph[t] * (1.0f / 64.0f) : 0.0f;
-        x1[(size_t)i * nn::F1 + 288 + t] = __float2bfloat16_rn(v);
-        x1[(size_t)i * nn::F1 + 304 + t] = __float2bfloat16_rn(0.0f);
+    if (t < 16 * nhere) {
+        const int m = t >> 4, q = t & 15, mb = first + m;
+        if (mb >= mb0 && mb < mb0 + nmb) {
+            const float v = q < 2 * nn::NPRED ? (float)ph[m][q] * (1.0f / 64.0f) : 0.0f;
+            x1[(size_t)(mb - mb0) * nn::F1 + 288 + q] = __float2bfloat16_rn(v);
+            x1[(size_t)(mb - mb0) * nn::F1 + 304 + q] = __float2bfloat16_rn(0.0f);
+        }
     }
 }
 
@@ -857,8 +867,10 @@ int riv_nn_features(const uint8_t* cur_y, const uint8_t* ref_y, int W, int H, co
                     int nmb, void* feat, void* x1, void* stream) {
     if (W <= 0 || H <= 0 || W % 16 || H % 16 || nmb <= 0 || mb0 < 0 || mb0 + nmb > (W / 16) * (H / 16))
         return (int)cudaErrorInvalidValue;
-    k_prop_features<<<nmb, 128, 0, (cudaStream_t)stream>>>(cur_y, ref_y, W, H, prev_coded, mb0, nmb,
-                                                           (__nv_bfloat16*)feat, (__nv_bfloat16*)x1);
+    // CTAs over groups of PF_MBS MBs of a row; those outside mb0 .. mb0+nmb-1 return at once
+    const int BW = W / 16, groups = (BW + PF_MBS - 1) / PF_MBS * (H / 16);
+    k_prop_features<<<groups, 256, 0, (cudaStream_t)stream>>>(cur_y, ref_y, W, H, prev_coded, mb0, nmb,
+                                                              (__nv_bfloat16*)feat, (__nv_bfloat16*)x1);
     return (int)cudaGetLastError();
 }
 
