@@ -304,7 +304,7 @@ struct MappedBuf {
 // Per-frame timing events: Y = input stream, S = main chain, K = compaction stream.
 constexpr int NPAR = 3;  // rotation depth of the per-frame device buffers
 constexpr uint64_t TIMING_SAMPLE = 8;  // pipelined frames carry stage timing events one in this many
-enum { EV_START, EV_YUV, EV_S0, EV_TABLE, EV_SEARCH, EV_PRED, EV_AQ, EV_RES, EV_DEBLOCK, EV_K0, EV_COMPACT, EV_N };
+enum { EV_START, EV_YUV, EV_S0, EV_TABLE, EV_SEARCH, EV_PRED, EV_AQ, EV_RES, EV_DEBLOCK, EV_K0, EV_COMPACT, EV_NET0, EV_NET1, EV_N };
 static const int NSTAGE = 8;  // rgb->yuv, table, search, predict, aq, residual, deblock, compact (+ total)
 
 struct Slot {
@@ -404,8 +404,18 @@ struct riv_encoder {
     // learned / parallel forms: the proposal network's parameters (bf16 weights, f32 biases),
     // its activations, the per-MB search result and the fallback / shortcut counters
     bool learned = false, nn_loaded = false;
-    DevBuf nn_w, nn_b, nn_feat, nn_a1, nn_a2, nn_a3, nn_x1, nn_h1, nn_h2, nn_o, lmv, lcount;
+    DevBuf nn_w, nn_b, nn_feat, nn_a1, nn_a2, nn_a3, nn_x1, nn_h1, nn_h2, nn_o[2], lmv, lcount;
     uint64_t learned_mbs = 0;
+    // The network of P-frame t runs on its own stream N while frame t-1 is still searched,
+    // reconstructed and deblocked: its inputs are the converted input planes of frames t and
+    // t-1 and the coded MVs of frame t-2, none of which frame t-1's work changes.  Its output
+    // is double-buffered (by frame parity); the search of frame t waits for ev_net_out[t & 1],
+    // the network of frame t+2 for ev_net_read[t & 1] (the search that read it), and the
+    // conversion into cur[k] for ev_net_cur[k] (the last network that read cur[k]).
+    cudaStream_t N = nullptr;
+    cudaEvent_t ev_net_out[2] = {}, ev_net_read[2] = {}, ev_net_cur[NPAR] = {};
+    bool has_prev2_mvs = false;  // the frame two back was a P-frame (its coded MVs are in coded[coded_cur ^ 1])
+    uint64_t nn_frames = 0;
 };
 
 namespace {
@@ -465,6 +475,12 @@ static void setup_device(riv_encoder* e) {
     CK(cudaStreamCreateWithFlags(&e->Hs, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&e->Y, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&e->K, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&e->N, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; k++) {
+        CK(cudaEventCreateWithFlags(&e->ev_net_out[k], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&e->ev_net_read[k], cudaEventDisableTiming));
+    }
+    for (int k = 0; k < NPAR; k++) CK(cudaEventCreateWithFlags(&e->ev_net_cur[k], cudaEventDisableTiming));
     for (int k = 0; k < NPAR; k++) {
         CK(cudaEventCreateWithFlags(&e->ev_cur_free[k], cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&e->ev_mbout_free[k], cudaEventDisableTiming));
@@ -562,7 +578,8 @@ static void setup_device(riv_encoder* e) {
         e->nn_x1.alloc((size_t)N * nn::F1 * 2);
         e->nn_h1.alloc((size_t)N * nn::HID * 2);
         e->nn_h2.alloc((size_t)N * nn::HID * 2);
-        e->nn_o.alloc((size_t)N * nn::OUT * 4);
+        e->nn_o[0].alloc((size_t)N * nn::OUT * 4);
+        e->nn_o[1].alloc((size_t)N * nn::OUT * 4);
     }
     if (e->splan.fused) {
         e->tflag.alloc((size_t)N * sizeof(unsigned));
@@ -702,7 +719,7 @@ static void flush_pending(riv_encoder* e) {
 // tcgen05 GEMMs), leaving 16 outputs per MB in nn_o.  Expired device waits set bit 0 of the
 // status word (RIV_ERR_DEVICE_TIMEOUT).
 static void proposal_forward(riv_encoder* e, const uint8_t* cur_y, const uint8_t* ref_y, const int8_t* prev_coded,
-                             cudaStream_t S) {
+                             void* out, cudaStream_t S) {
     using PL = nn::ParamLayout;
     const int N = e->NMB;
     const uint16_t* W = e->nn_w.as<uint16_t>();
@@ -718,7 +735,7 @@ static void proposal_forward(riv_encoder* e, const uint8_t* cur_y, const uint8_t
                             1, nn::HID, err, S));
     CK((cudaError_t)nn_gemm(e->nn_h1.p, nn::HID, W + PL::f2, nn::HID, e->nn_h2.p, nn::HID, B + 256, N, nn::HID, nn::HID,
                             64, 2, 1, 1, nn::HID, err, S));
-    CK((cudaError_t)nn_gemm(e->nn_h2.p, nn::HID, W + PL::f3, nn::HID, e->nn_o.p, nn::OUT, B + 384, N, nn::OUT, nn::HID,
+    CK((cudaError_t)nn_gemm(e->nn_h2.p, nn::HID, W + PL::f3, nn::HID, out, nn::OUT, B + 384, N, nn::OUT, nn::HID,
                             64, 0, 0, 1, nn::OUT, err, S));
 }
 
@@ -743,6 +760,7 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
     // ---- input conversion on Y, overlapping the previous frame's main chain; cur[ck] is
     // free once the residual of the frame NPAR back has read it
     CK(cudaStreamWaitEvent(Y, e->ev_cur_free[ck], 0));
+    if (e->learned) CK(cudaStreamWaitEvent(Y, e->ev_net_cur[ck], 0));
     // without deferral: after the previous search launch, i.e. beside that frame's residual;
     // with it the conversion runs in the gap between two launches, one frame ahead
     if (!e->defer_ok) CK(cudaStreamWaitEvent(Y, e->ev_search_done, 0));
@@ -793,6 +811,7 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         if (e->intra_level > 0) rp.recon = e->recon_pre.as<uint8_t>();
         reconstruct_now(e, j, rp, e->intra_level, e->intra_E, e->intra_I, e->intra_H, nullptr, recon);
         e->has_prev_mvs = false;
+        e->has_prev2_mvs = false;
     } else {
         SearchParams sp{};
         sp.ref_y = e->ref[e->ref_cur].as<uint8_t>();
@@ -831,9 +850,20 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         sp.wq = e->wq.as<unsigned>() + (size_t)e->wq_par * e->wq_words;
         sp.wq_next = e->wq.as<unsigned>() + (size_t)(e->wq_par ^ 1) * e->wq_words;
         sp.wq_words = e->wq_words;
-        if (e->learned && c.encode_form == RIV_FORM_LEARNED) {  // stage 1 of the learned form: the network
+        const int nbuf = (int)(e->nn_frames & 1);
+        if (e->learned && c.encode_form == RIV_FORM_LEARNED) {
+            // stage 1 of the learned form: the network, on stream N (see riv_encoder::N)
             if (!e->nn_loaded) throw std::runtime_error("learned form: no proposal network loaded (riv_encoder_set_proposal)");
-            proposal_forward(e, cur, sp.ref_y, sp.prev_coded, S);
+            cudaStream_t Nn = e->N;
+            CK(cudaStreamWaitEvent(Nn, s.ev_yuv, 0));                // this frame's planes converted
+            CK(cudaStreamWaitEvent(Nn, e->ev_net_read[nbuf], 0));    // the search two frames back read nn_o[nbuf]
+            if (j.timed) CK(cudaEventRecord(s.ev_k[EV_NET0], Nn));
+            proposal_forward(e, cur, e->curb[e->last_par].as<uint8_t>(),
+                             e->has_prev2_mvs ? e->coded[e->coded_cur ^ 1].as<int8_t>() : nullptr, e->nn_o[nbuf].p, Nn);
+            if (j.timed) CK(cudaEventRecord(s.ev_k[EV_NET1], Nn));
+            CK(cudaEventRecord(e->ev_net_out[nbuf], Nn));
+            CK(cudaEventRecord(e->ev_net_cur[e->last_par], Nn));     // cur of the previous frame read
+            CK(cudaStreamWaitEvent(S, e->ev_net_out[nbuf], 0));
         }
         if (e->table_ok && !e->learned) {
             sp.tstride = sad_table_stride(c.search_range);
@@ -880,8 +910,10 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         e->pend.active = false;
         CK(cudaStreamWaitEvent(S, e->ev_mbout_free[ck], 0));  // compaction of the frame NPAR back
         if (e->learned) {
-            CK((cudaError_t)launch_learned(sp, c.encode_form == RIV_FORM_LEARNED ? e->nn_o.as<float>() : nullptr,
+            CK((cudaError_t)launch_learned(sp, c.encode_form == RIV_FORM_LEARNED ? e->nn_o[nbuf].as<float>() : nullptr,
                                            (int)c.proposal_margin, 2.2f, e->lmv.p, e->lcount.as<unsigned>(), S));
+            CK(cudaEventRecord(e->ev_net_read[nbuf], S));
+            e->nn_frames++;
             e->learned_mbs += (uint64_t)N;
         } else {
             CK(launch_search(sp, e->splan, S));
@@ -930,6 +962,7 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
                             recon);
         }
         e->coded_cur = cn;
+        e->has_prev2_mvs = e->has_prev_mvs;
         e->has_prev_mvs = true;
     }
     e->ref_cur = nxt;
@@ -966,8 +999,10 @@ static riv_status retire(riv_encoder* e, Job& j) {
     e->d2h_bytes += (uint64_t)e->NMB * 7 + 12 + std::max(coef_bytes, s.prefetched);
     float t[NSTAGE + 1] = {0};
     CK(cudaEventSynchronize(s.ev_recon));  // the D2H did not wait for the deblock
-    const int spans[NSTAGE + 1][2] = {{EV_START, EV_YUV},   {EV_S0, EV_TABLE},  {EV_TABLE, EV_SEARCH},
-                                      {EV_SEARCH, EV_PRED}, {EV_PRED, EV_AQ},   {EV_AQ, EV_RES},
+    // stage 1 of the learned form is its network, on stream N
+    const bool net = j.type == 2 && e->cfg.encode_form == RIV_FORM_LEARNED;
+    const int spans[NSTAGE + 1][2] = {{EV_START, EV_YUV},   {net ? EV_NET0 : EV_S0, net ? EV_NET1 : EV_TABLE},
+                                      {EV_TABLE, EV_SEARCH}, {EV_SEARCH, EV_PRED}, {EV_PRED, EV_AQ},   {EV_AQ, EV_RES},
                                       {EV_RES, EV_DEBLOCK}, {EV_K0, EV_COMPACT}, {EV_S0, EV_DEBLOCK}};
     if (j.timed) {
         for (int k = 0; k <= NSTAGE; k++) cudaEventElapsedTime(&t[k], s.ev_k[spans[k][0]], s.ev_k[spans[k][1]]);
@@ -1409,8 +1444,16 @@ void riv_encoder_free(riv_encoder* e) {
                       &e->varsum, &e->qs, &e->status,
                       &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset, &e->lcindex, &e->lcoffset, &e->sadtab, &e->prof, &e->tflag, &e->rowdone, &e->newcost, &e->newcost32,
                       &e->nn_w, &e->nn_b, &e->nn_feat, &e->nn_a1, &e->nn_a2, &e->nn_a3, &e->nn_x1, &e->nn_h1, &e->nn_h2,
-                      &e->nn_o, &e->lmv, &e->lcount};
+                      &e->nn_o[0], &e->nn_o[1], &e->lmv, &e->lcount};
     for (DevBuf* b : bufs) b->release();
+    if (e->N) cudaStreamSynchronize(e->N);
+    for (int k = 0; k < 2; k++) {
+        if (e->ev_net_out[k]) cudaEventDestroy(e->ev_net_out[k]);
+        if (e->ev_net_read[k]) cudaEventDestroy(e->ev_net_read[k]);
+    }
+    for (int k = 0; k < NPAR; k++)
+        if (e->ev_net_cur[k]) cudaEventDestroy(e->ev_net_cur[k]);
+    if (e->N) cudaStreamDestroy(e->N);
     if (e->S) cudaStreamDestroy(e->S);
     if (e->C) cudaStreamDestroy(e->C);
     if (e->Hs) cudaStreamDestroy(e->Hs);

@@ -1,11 +1,13 @@
 """Training of the motion-proposal network on records logged by the plain GPU encoder.
 
-Records: for every P-frame of seeded synthetic clips, every MB's network input (computed on
-the GPU by the same kernel the learned encoder runs: correlation volume of the current block
-against the previous reconstruction, predictor prior map, the previous P-frame's coded MVs
-around it) and the plain encoder's choice for it (its search MV in half-pel units and its RDO
-skip decision).  The plain encoder is the reference-identical path, so the network learns to
-propose what the reference's search would pick.
+Records: for every P-frame of seeded synthetic clips, every MB's network input, computed on
+the GPU by the same kernel and from the same planes the learned encoder uses (the correlation
+volume of the current input block against the previous frame's input planes, the predictor
+prior map and values from the coded MVs of the frame two back: the encoder runs the network of
+frame t while frame t-1 is still being reconstructed), and the plain encoder's choice for it
+(its search MV in half-pel units and its RDO skip decision).  The plain encoder is the
+reference-identical path, so the network learns to propose what the reference's search would
+pick.
 
 Training: AdamW (lr 1e-3, batch 4096 MBs) with this library's forward, backward and optimizer
 kernels (riv2_b200.proposal); the parameters are written with proposal.save_params.
@@ -48,18 +50,19 @@ def log_records(clips: int, frames: int, preset: str = "720p", keep: float = 1.0
         enc = E.Encoder.new(cfg, E.VecWriter())
         sw, sh = cfg.storage_width, cfg.storage_height
         nmb = (sw // 16) * (sh // 16)
-        prev_recon, prev_coded = None, None
+        prev_in, coded1, coded2 = None, None, None  # input luma of t-1; coded MVs of t-1 and t-2
         for t in range(frames):
             enc.encode_frame(E.Frame(clip.frame(t), w, h, t * 33))
+            cur = np.ascontiguousarray(enc.debug_state(3)[: sw * sh])
+            coded_t = None
             if t >= 1:
                 mbo = enc.debug_state(0).reshape(nmb, 20)
-                cur = enc.debug_state(3)[: sw * sh]
                 raw = mbo[:, 0:4].view(np.int8).astype(np.int16)
                 keep_idx = np.nonzero(rng.random(nmb) < keep)[0].astype(np.int64)
                 if keep_idx.size:
-                    cur_d = torch.from_numpy(cur.copy()).to(dev)
-                    ref_d = torch.from_numpy(prev_recon).to(dev)
-                    pc_d = None if prev_coded is None else torch.from_numpy(prev_coded).to(dev)
+                    cur_d = torch.from_numpy(cur).to(dev)
+                    ref_d = torch.from_numpy(prev_in).to(dev)
+                    pc_d = None if coded2 is None else torch.from_numpy(coded2).to(dev)
                     f = torch.empty((nmb, 24, 24, 2), dtype=torch.bfloat16, device=dev)
                     x = torch.zeros((nmb, 320), dtype=torch.bfloat16, device=dev)
                     rc = P.lib().riv_nn_features(cur_d.data_ptr(), ref_d.data_ptr(), sw, sh,
@@ -73,9 +76,9 @@ def log_records(clips: int, frames: int, preset: str = "720p", keep: float = 1.0
                     tm = np.stack([2 * raw[:, 0] + raw[:, 2], 2 * raw[:, 1] + raw[:, 3]], axis=1).astype(np.int16)
                     tmvs.append(torch.from_numpy(tm[keep_idx]).to(dev))
                     tskips.append(torch.from_numpy(mbo[keep_idx, 13].copy()).to(dev))  # rdo_skip byte
-                prev_coded = np.ascontiguousarray(mbo[:, 4:8].view(np.int8))
-            y, _, _ = enc.last_recon()
-            prev_recon = np.ascontiguousarray(y)
+                coded_t = np.ascontiguousarray(mbo[:, 4:8].view(np.int8))
+            coded1, coded2 = coded_t, coded1
+            prev_in = cur
         enc.close()
         if verbose and (ci + 1) % 16 == 0:
             print(f"  logged {ci + 1}/{clips} clips ({time.time() - t0:.1f} s)", flush=True)
