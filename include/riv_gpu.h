@@ -149,6 +149,50 @@ riv_status riv_counters(riv_encoder* enc, double* us9, uint64_t* io2, uint64_t* 
  * [4] record writes, [5] waiting for a frame's entropy coding to finish. */
 riv_status riv_host_times(riv_encoder* enc, double* ms6);
 
+/* ---- Multi-clip encoding.  No counterpart in the reference (one stream per Encoder). ----
+ * A batch holds n independent clips -- each with its own config (any mix of sizes, qualities
+ * and keyframe settings; plain form; one device) and its own writer -- whose frames are
+ * encoded together one step at a time.  A step takes at most one frame per clip; its GPU work
+ * is one launch per stage over every clip of the step (conversion, SAD tables, the search --
+ * one cooperative launch in which each clip's CTAs run its MB rows as a wavefront --,
+ * prediction, AQ mean, residual, deblock, compaction), so the clips fill the SMs that one
+ * clip's wavefront leaves idle; each clip's entropy coding and records then run as in
+ * riv_encode_frame, on thread pools the clips share.  Every clip's stream is byte-identical
+ * to what riv_encoder_new + riv_encode_frame + riv_finish write for that clip alone.
+ * Tile shapes (search CTAs, MBs per residual CTA, deblock tile width) are chosen by an
+ * autotuner during the first all-P-frame steps (they do not change the output), or fixed by
+ * riv_batch_set_tune. */
+#define RIV_BATCH_MAX_CLIPS 256
+typedef struct riv_batch riv_batch;
+typedef struct {
+    int32_t search_rows_pct; /* search CTAs per step, percent of what fits on the device (1..100) */
+    int32_t res_mbs;         /* MBs per residual CTA: 2, 4 or 8 */
+    int32_t db_tw;           /* deblock tile width, luma columns: 64, 128 or 256 */
+} riv_batch_tune;
+/* cfgs[i] / writers[i]: clip i (n <= RIV_BATCH_MAX_CLIPS).  Headers are written now. */
+riv_status riv_batch_new(const riv_config* cfgs, const riv_writer_vtable* writers, uint32_t n, riv_batch** out);
+/* One step: frames[i] = clip i's next RGB24 frame (display size, host memory, read during
+ * the call) or NULL when clip i has none in this step; ts[i] its timestamp. */
+riv_status riv_batch_encode(riv_batch* b, const uint8_t* const* frames, const uint64_t* ts);
+/* The same with the frames already in device memory. */
+riv_status riv_batch_encode_device(riv_batch* b, const void* const* d_frames, const uint64_t* ts);
+/* Encoder::finish of every clip (drains, rewrites each header's frame count, flushes). */
+riv_status riv_batch_finish(riv_batch* b);
+void riv_batch_free(riv_batch* b);
+const char* riv_batch_last_error(const riv_batch* b);
+/* Fixes the tile shapes (the autotuner stops); RIV_ERR_INVALID_CONFIG for values not listed. */
+riv_status riv_batch_set_tune(riv_batch* b, const riv_batch_tune* t);
+/* The shapes in use; *tuned = 0 still tuning, 1 chosen by the autotuner, 2 fixed. */
+riv_status riv_batch_get_tune(const riv_batch* b, riv_batch_tune* t, int* tuned);
+/* c7 = {steps, frames, MBs, kernel launches, timed steps, host->device bytes, device->host
+ * bytes}; stage_us10 = mean GPU microseconds per timed step: conversion, SAD tables, search,
+ * prediction, AQ mean, residual, deblock, scan, pack, whole step.  Either may be NULL. */
+riv_status riv_batch_counters(const riv_batch* b, uint64_t* c7, double* stage_us10);
+/* Reconstruction (storage-size planes) of clip `clip`'s last submitted frame.  Synchronises. */
+riv_status riv_batch_last_recon(riv_batch* b, uint32_t clip, uint8_t* y, uint8_t* u, uint8_t* v);
+/* Records written so far for clip `clip`, and its host milliseconds (as riv_host_times). */
+riv_status riv_batch_clip_counters(const riv_batch* b, uint32_t clip, uint64_t* frames_written, double* host_ms6);
+
 /* In-memory writer (VecWriter, enc/writer.rs:20-69). */
 typedef struct riv_memwriter riv_memwriter;
 riv_memwriter* riv_memwriter_new(void);

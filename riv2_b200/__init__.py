@@ -3,6 +3,7 @@
 Public API mirrors reitero_encode: EncoderConfig / KeyframeInterval / Frame / VecWriter /
 Encoder (new, encode_frame, encode_frame_with_stats, finish) and the EncodeError family.
 """
+from .batch import Batch  # noqa: F401
 from .encoder import (  # noqa: F401
     CudaError,
     DeviceTimeout,

@@ -324,6 +324,9 @@ struct Job {
     bool tail_done = true;  // compaction and copies enqueued (false while the frame is pending)
     bool deferred = false;  // reconstructed inside the next P-frame's search launch
     bool timed = false;     // stage timing events recorded for this frame
+    // multi-clip step (riv_batch): one event marks the step's GPU work and copies done, in
+    // place of the slot's ev_gpu / ev_recon / ev_d2h
+    cudaEvent_t xev = nullptr;
     int ck = 0;             // double-buffer parity of the frame's buffers
     uint32_t count = 0;
     std::future<void> fut, fut_mv;
@@ -384,12 +387,13 @@ struct riv_encoder {
     std::vector<Slot> slots;
     std::deque<Job> jobs;
     MvCoder mvc;
-    std::unique_ptr<ThreadPool> pool;
-    std::unique_ptr<ThreadPool> mv_exec;  // one thread: MV coding strictly in frame order
-    std::unique_ptr<ThreadPool> rans_pool;  // coefficient-coder jobs (never wait)
+    std::shared_ptr<ThreadPool> pool;       // coefficient modelling (shared by the clips of a batch)
+    std::unique_ptr<ThreadPool> mv_exec;    // one thread: MV coding strictly in frame order
+    std::shared_ptr<ThreadPool> rans_pool;  // coefficient-coder jobs (never wait)
     BatchSubmit rans_submit;
     int rans_parts = 1;  // threads that code one frame's coefficients: rans_pool's and the caller
     bool draining = false;  // inside drain_all: the newest frame is coded by rans_parts threads
+    bool batched = false;   // a clip of a riv_batch: only the batch submits its frames
     double host_ms[6] = {0};  // submit, retire, mv coding, dct coding (summed), write, blocked
     std::mutex stat_mu;
     float last_times[NSTAGE + 1] = {0};
@@ -739,6 +743,43 @@ static void proposal_forward(riv_encoder* e, const uint8_t* cur_y, const uint8_t
                             64, 0, 0, 1, nn::OUT, err, S));
 }
 
+// The search parameters of a P-frame of `e` (current planes `cur`, per-MB output `mbo`) against
+// its last reconstruction, with a new frame tag; the caller sets the table, AQ, worker-queue
+// and launch-shape fields.
+static void frame_search_params(riv_encoder* e, const uint8_t* cur, MbOut* mbo, SearchParams& sp) {
+    const riv_config& c = e->cfg;
+    sp.ref_y = e->ref[e->ref_cur].as<uint8_t>();
+    sp.cur_y = cur;
+    sp.W = e->W; sp.H = e->H; sp.BW = e->BW; sp.BH = e->BH; sp.sr = c.search_range;
+    sp.prev_coded = e->has_prev_mvs ? e->coded[e->coded_cur].as<int8_t>() : nullptr;
+    sp.zthr = c.me_zero_mv_threshold;
+    sp.pthr = c.me_predictor_threshold;
+    double lam = e->L.lambda;
+    sp.lam2 = lam * 2.0;
+    sp.c15 = f64_as_i64(lam * 2.0 * 1.5);
+    sp.c05 = f64_as_i64(lam * 2.0 * 0.5);
+    sp.lambda_zero = lam == 0.0;
+    sp.mvbits = e->mvbits.as<double>();
+    sp.newcost = e->newcost.as<long long>();
+    sp.newcost32 = e->newcost32.as<int>();
+    sp.small = e->small_costs ? 1 : 0;
+    sp.rdo_lambda = lam;
+    sp.rdo_skip_bits = e->L.skip_bits;
+    sp.rdo_keep_bits = e->L.keep_bits;
+    sp.rdo_icpt = e->L.icpt;
+    sp.rdo_slope = e->L.slope;
+    sp.rdo_ret = e->L.ret;
+    sp.rdo_guard = 768.0 * (double)c.skip_threshold;
+    sp.rdo_allow = c.skip_threshold > 0;
+    sp.rec = e->rec.as<MbRec>();
+    e->tag = (e->tag + 1) & 0xffffu;
+    if (e->tag == 0) e->tag = 1;
+    sp.tag = e->tag;
+    sp.out = mbo;
+    sp.status = e->status.as<unsigned>();
+    sp.spin_limit = 1ll << 22;  // ~ a few seconds, far above any legitimate wait
+}
+
 // Enqueue the GPU work of one frame.  `src` = 0 host RGB, 1 device RGB, 2 host YUV.
 static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const void* b, const void* c3) {
     const riv_config& c = e->cfg;
@@ -814,36 +855,7 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         e->has_prev2_mvs = false;
     } else {
         SearchParams sp{};
-        sp.ref_y = e->ref[e->ref_cur].as<uint8_t>();
-        sp.cur_y = cur;
-        sp.W = W; sp.H = H; sp.BW = e->BW; sp.BH = e->BH; sp.sr = c.search_range;
-        sp.prev_coded = e->has_prev_mvs ? e->coded[e->coded_cur].as<int8_t>() : nullptr;
-        sp.zthr = c.me_zero_mv_threshold;
-        sp.pthr = c.me_predictor_threshold;
-        double lam = e->L.lambda;
-        sp.lam2 = lam * 2.0;
-        sp.c15 = f64_as_i64(lam * 2.0 * 1.5);
-        sp.c05 = f64_as_i64(lam * 2.0 * 0.5);
-        sp.lambda_zero = lam == 0.0;
-        sp.mvbits = e->mvbits.as<double>();
-        sp.newcost = e->newcost.as<long long>();
-        sp.newcost32 = e->newcost32.as<int>();
-        sp.small = e->small_costs ? 1 : 0;
-        sp.rdo_lambda = lam;
-        sp.rdo_skip_bits = e->L.skip_bits;
-        sp.rdo_keep_bits = e->L.keep_bits;
-        sp.rdo_icpt = e->L.icpt;
-        sp.rdo_slope = e->L.slope;
-        sp.rdo_ret = e->L.ret;
-        sp.rdo_guard = 768.0 * (double)c.skip_threshold;
-        sp.rdo_allow = c.skip_threshold > 0;
-        sp.rec = e->rec.as<MbRec>();
-        e->tag = (e->tag + 1) & 0xffffu;
-        if (e->tag == 0) e->tag = 1;
-        sp.tag = e->tag;
-        sp.out = mbo;
-        sp.status = e->status.as<unsigned>();
-        sp.spin_limit = 1ll << 22;  // ~ a few seconds, far above any legitimate wait
+        frame_search_params(e, cur, mbo, sp);
         sp.tab = nullptr;
         sp.tstride = 0;
         sp.tflag = nullptr;
@@ -980,7 +992,7 @@ static double now_ms() {
 static riv_status retire(riv_encoder* e, Job& j) {
     Slot& s = e->slots[j.slot];
     double t0 = now_ms();
-    CK(cudaEventSynchronize(s.ev_d2h));
+    CK(cudaEventSynchronize(j.xev ? j.xev : s.ev_d2h));
     const uint32_t* hdr = s.hdr.host<uint32_t>();
     unsigned st = hdr[2];
     if (st) {
@@ -998,7 +1010,7 @@ static riv_status retire(riv_encoder* e, Job& j) {
     e->coef_guess = coef_bytes + coef_bytes / 4 + 65536;
     e->d2h_bytes += (uint64_t)e->NMB * 7 + 12 + std::max(coef_bytes, s.prefetched);
     float t[NSTAGE + 1] = {0};
-    CK(cudaEventSynchronize(s.ev_recon));  // the D2H did not wait for the deblock
+    if (!j.xev) CK(cudaEventSynchronize(s.ev_recon));  // the D2H did not wait for the deblock
     // stage 1 of the learned form is its network, on stream N
     const bool net = j.type == 2 && e->cfg.encode_form == RIV_FORM_LEARNED;
     const int spans[NSTAGE + 1][2] = {{EV_START, EV_YUV},   {net ? EV_NET0 : EV_S0, net ? EV_NET1 : EV_TABLE},
@@ -1149,7 +1161,7 @@ static riv_status pump(riv_encoder* e, bool block_front) {
             flush_pending(e);
         }
         if (!block) {
-            cudaError_t q = cudaEventQuery(e->slots[j.slot].ev_gpu);
+            cudaError_t q = cudaEventQuery(j.xev ? j.xev : e->slots[j.slot].ev_gpu);
             if (q == cudaErrorNotReady) break;
             if (q != cudaSuccess) throw CudaError{q, "cudaEventQuery"};
         }
@@ -1198,6 +1210,17 @@ static riv_status drain_all(riv_encoder* e) {
     return io;
 }
 
+// Frame type of the next frame (enc/encoder.rs:265-291).
+static bool next_is_key(const riv_encoder* e) {
+    const riv_config& c = e->cfg;
+    const uint64_t n = e->submitted;
+    bool intra;
+    if (c.keyframe_mode == RIV_KEYFRAME_ALL_INTRA) intra = true;
+    else if (c.keyframe_mode == RIV_KEYFRAME_AUTOMATIC) intra = n % 30 == 0;
+    else intra = n % c.keyframe_interval == 0;
+    return intra || !e->has_ref;
+}
+
 static riv_status encode_common(riv_encoder* e, int src, const void* a, const void* b, const void* c3,
                                 uint64_t ts, riv_frame_stats* stats) {
     if (e->poisoned) return poisoned_status(e);
@@ -1215,14 +1238,8 @@ static riv_status encode_common(riv_encoder* e, int src, const void* a, const vo
             }
             if (st) return st;
         }
-        // frame type (enc/encoder.rs:265-291)
-        const riv_config& c = e->cfg;
-        bool intra;
-        uint64_t n = e->submitted;
-        if (c.keyframe_mode == RIV_KEYFRAME_ALL_INTRA) intra = true;
-        else if (c.keyframe_mode == RIV_KEYFRAME_AUTOMATIC) intra = n % 30 == 0;
-        else intra = n % c.keyframe_interval == 0;
-        if (!e->has_ref) intra = true;
+        const uint64_t n = e->submitted;
+        const bool intra = next_is_key(e);
         e->jobs.emplace_back();
         Job& j = e->jobs.back();
         j.index = n;
@@ -2421,6 +2438,653 @@ void riv_decoder_free(riv_decoder* d) {
     }
     if (d->S) cudaStreamDestroy(d->S);
     delete d;
+}
+
+}  // extern "C"
+
+// =====================================================================================
+// Multi-clip encoding (riv_batch).  No counterpart in the reference, which encodes one
+// stream per Encoder.  A batch owns one encoder per clip (its config, writer, buffers, MV
+// coder and record pipeline); a step takes at most one frame per clip and runs its GPU work
+// as one launch per stage over every clip of the step on one stream (riv_batch.cuh), then
+// hands each clip's frame to that clip's host pipeline (retire / write_job), exactly as
+// riv_encode_frame does.  Each clip's stream is therefore byte-identical to a single-clip
+// encode of the clip.
+// =====================================================================================
+namespace {
+constexpr int BT_BOUNDS = BS_N + 3;  // timing marks: start, then one after each stage
+enum { TB_START, TB_CONVERT, TB_TABLE, TB_SEARCH, TB_PREDICT, TB_AQSUM, TB_RESIDUAL, TB_DEBLOCK, TB_SCAN, TB_PACK };
+constexpr int BT_NSTAGE = 9;  // convert, table, search, predict, aq mean, residual, deblock, scan, pack
+// Autotuner candidates (one dimension per timed stage; the streams do not depend on them).
+constexpr int TUNE_ROWS_PCT[3] = {100, 75, 50};
+constexpr int TUNE_RES_MBS[3] = {4, 2, 8};
+constexpr int TUNE_DB_TW[3] = {128, 64, 256};
+constexpr int TUNE_ROUNDS = 2;  // all-P-frame steps measured per candidate
+}  // namespace
+
+struct riv_batch {
+    int device = 0;
+    std::vector<riv_encoder*> clips;
+    std::shared_ptr<ThreadPool> pool, rans_pool;
+    cudaStream_t B = nullptr, Hs = nullptr, C = nullptr;  // GPU chain, host->device, device->host
+    cudaEvent_t ev_h2d = nullptr, ev_gpu = nullptr;
+    std::vector<cudaEvent_t> ev_step;  // per step in flight: its GPU work and copies done
+    // stage timing marks of timed steps, two sets: a step's marks are read one timed step later
+    // (or at the end), so that reading them rarely waits for the GPU
+    cudaEvent_t ev_t[2][BT_BOUNDS] = {};
+    struct TimedStep {
+        bool pending = false, tuning = false;
+        int cand = 0;
+        uint64_t mbs = 0, pmbs = 0;
+    } tpend[2];
+    int tpar = 0;
+    // step descriptors: pinned staging (double-buffered), one device copy
+    HostBuf hdesc[2];
+    cudaEvent_t ev_desc[2] = {};
+    DevBuf ddesc;
+    size_t off_sp = 0, off_start = 0, off_sstart = 0, desc_bytes = 0;
+    int dpar = 0;
+    int max_sr = 0;
+    // search capacity per variant: 0 table + small costs, 1 table, 2 no table
+    int cap[3] = {0, 0, 0}, sthreads[3] = {0, 0, 0};
+    size_t ssmem[3] = {0, 0, 0};
+    // tile shapes and the autotuner
+    BatchTune tune{4, 128, 100};
+    bool fixed = false, tuned = false;
+    int tune_step = 0;          // tuning steps submitted (candidate = (tune_step / ROUNDS) % 3)
+    double tune_us[3][3] = {};  // [dimension][candidate] summed microseconds per MB
+    int tune_n[3] = {0, 0, 0};  // all-P-frame steps measured per candidate
+    uint64_t steps = 0, frames = 0, mbs = 0, launches = 0, timed = 0;
+    double stage_us[BT_NSTAGE + 1] = {};  // sums over timed steps (last: whole step)
+    uint64_t h2d_bytes = 0, d2h_bytes = 0;
+    std::string err;
+    bool poisoned = false;
+};
+
+namespace {
+
+static int search_variant(const riv_encoder* e) { return e->table_ok ? (e->small_costs ? 0 : 1) : 2; }
+
+// Row CTAs of each clip of one search launch: about proportional to its MBs, at least one, at
+// most its MB rows, `total` in all (>= the number of clips).
+static void spread_rows(const std::vector<int>& nmb, const std::vector<int>& bh, int total, std::vector<int>& out) {
+    const size_t n = nmb.size();
+    out.assign(n, 1);
+    double sum = 0;
+    for (size_t i = 0; i < n; i++) sum += nmb[i];
+    int used = 0;
+    for (size_t i = 0; i < n; i++) {
+        out[i] = std::max(1, std::min(bh[i], (int)((double)total * nmb[i] / sum)));
+        used += out[i];
+    }
+    while (used > total) {  // the minimum of one may overshoot: take from the largest
+        size_t k = 0;
+        for (size_t i = 1; i < n; i++)
+            if (out[i] > out[k]) k = i;
+        if (out[k] <= 1) break;
+        out[k]--;
+        used--;
+    }
+    while (used < total) {  // hand out what rounding left, to the clip with most MBs per CTA
+        size_t k = n;
+        double worst = 0;
+        for (size_t i = 0; i < n; i++) {
+            if (out[i] >= bh[i]) continue;
+            const double load = (double)nmb[i] / out[i];
+            if (k == n || load > worst) { worst = load; k = i; }
+        }
+        if (k == n) break;
+        out[k]++;
+        used++;
+    }
+}
+
+static riv_status batch_fail(riv_batch* b, riv_status s, const std::string& msg) {
+    b->err = msg;
+    if (s == RIV_ERR_CUDA || s == RIV_ERR_DEVICE_TIMEOUT) b->poisoned = true;
+    return s;
+}
+
+// The frame of clip `e` in this step: descriptor, search parameters and state updates, like
+// submit_gpu but without launching anything.  src: 0 host RGB (copied on `hs`), 1 device RGB.
+static void batch_collect(riv_encoder* e, Job& j, int src, const void* frame, cudaStream_t hs, BatchClip& k,
+                          SearchParams& sp) {
+    const riv_config& c = e->cfg;
+    Slot& s = e->slots[j.slot];
+    const int W = e->W, H = e->H, N = e->NMB;
+    const int ck = e->fpar;
+    j.ck = ck;
+    uint8_t* cur = e->curb[ck].as<uint8_t>();
+    MbOut* mbo = e->mboutb[ck].as<MbOut>();
+    memset(&k, 0, sizeof(k));
+    k.W = W; k.H = H; k.BW = e->BW; k.NMB = N;
+    k.intra = j.type == 1 ? 1 : 0;
+    k.dw = (int)c.display_width;
+    k.dh = (int)c.display_height;
+    k.cur = cur;
+    if (src == 0) {
+        CK(cudaMemcpyAsync(s.rgb.p, frame, (size_t)c.display_width * c.display_height * 3, cudaMemcpyHostToDevice, hs));
+        k.rgb = s.rgb.as<uint8_t>();
+        e->h2d_bytes += (uint64_t)c.display_width * c.display_height * 3;
+    } else {
+        k.rgb = (const uint8_t*)frame;
+    }
+    const int nxt = e->ref_cur ^ 1;
+    uint8_t* recon = e->ref[nxt].as<uint8_t>();
+    ResidualParams& rp = k.rp;
+    rp.cur = cur;
+    rp.pred = e->predb[ck].as<uint8_t>();
+    rp.coeffs = e->coeffsb[ck].as<int16_t>();
+    rp.opt_skip = e->optskipb[ck].as<uint8_t>();
+    rp.fmask = e->fmaskb[ck].as<uint8_t>();
+    rp.eobs = e->eobsb[ck].as<uint8_t>();
+    rp.dead_zone = c.inter_dead_zone;
+    rp.W = W; rp.H = H; rp.BW = e->BW;
+    const int level = j.type == 1 ? e->intra_level : e->inter_level;
+    rp.recon = level > 0 ? e->recon_pre.as<uint8_t>() : recon;
+    k.db_level = level;
+    k.db_src = e->recon_pre.as<uint8_t>();
+    k.db_dst = recon;
+    if (j.type == 1) {
+        rp.intra = 1;
+        rp.intra_ytab = e->ytab.as<uint16_t>();
+        rp.intra_ctab = e->ctab.as<uint16_t>();
+        k.db_E = e->intra_E; k.db_I = e->intra_I; k.db_H = e->intra_H;
+        k.db_mask = nullptr;
+        e->has_prev_mvs = false;
+        e->has_prev2_mvs = false;
+    } else {
+        memset(&sp, 0, sizeof(sp));
+        frame_search_params(e, cur, mbo, sp);
+        if (e->table_ok) {
+            sp.tstride = sad_table_stride(c.search_range);
+            sp.tab = e->sadtab.as<uint16_t>();
+        }
+        const int cn = e->coded_cur ^ 1;
+        sp.coded_out = e->coded[cn].as<int8_t>();
+        k.ref = e->ref[e->ref_cur].as<uint8_t>();
+        k.tab = e->table_ok ? e->sadtab.as<uint16_t>() : nullptr;
+        k.tstride = sp.tstride;
+        k.sr = c.search_range;
+        k.mbo = mbo;
+        k.pred = e->predb[ck].as<uint8_t>();
+        k.lnv = e->lnvb[ck].as<float>();
+        k.logfix = e->logfix.as<uint32_t>();
+        k.nlog = e->nlog;
+        rp.intra = 0;
+        rp.mb = mbo;
+        rp.qs = e->qs.as<float>();
+        rp.lnv = k.lnv;  // the residual derives the steps from the ln variances and their mean
+        rp.aq_base = e->inter_base;
+        rp.expfix = e->expfix.as<uint32_t>();
+        rp.nexp = e->nexp;
+        rp.qs_out = e->qs.as<float>();
+        k.db_E = e->inter_E; k.db_I = e->inter_I; k.db_H = e->inter_H;
+        k.db_mask = rp.fmask;
+        e->coded_cur = cn;
+        e->has_prev2_mvs = e->has_prev_mvs;
+        e->has_prev_mvs = true;
+    }
+    k.c_index = e->cindex.as<int32_t>();
+    k.c_offset = e->coffset.as<int32_t>();
+    k.c_side = s.dside.as<uint32_t>();
+    k.c_packed = s.dpacked.as<int16_t>();
+    k.c_peobs = s.dpeobs.as<uint8_t>();
+    k.c_hdr = s.hdr.dev<uint32_t>();
+    k.status = e->status.as<unsigned>();
+    e->ref_cur = nxt;
+    e->has_ref = true;
+    e->last_par = ck;
+    e->fpar = (ck + 1) % NPAR;
+}
+
+// The shapes of this step: while tuning, candidate (tune_step / ROUNDS) % 3 of every dimension
+// at once (each dimension is timed by its own stage).
+static BatchTune batch_step_tune(riv_batch* b, bool& tuning, int& cand) {
+    tuning = !b->fixed && !b->tuned;
+    BatchTune t = b->tune;
+    cand = (b->tune_step / TUNE_ROUNDS) % 3;
+    if (tuning) {
+        t.row_ctas = TUNE_ROWS_PCT[cand];
+        t.res_mbs = TUNE_RES_MBS[cand];
+        t.db_tw = TUNE_DB_TW[cand];
+    }
+    return t;
+}
+
+// Stage times of the timed step held by timing set `par` (if any): accumulated, and fed to the
+// autotuner when that step ran candidate shapes.  Waits for that step's work to end.
+static void batch_read_times(riv_batch* b, int par) {
+    riv_batch::TimedStep& t = b->tpend[par];
+    if (!t.pending) return;
+    t.pending = false;
+    cudaEvent_t* ev = b->ev_t[par];
+    CK(cudaEventSynchronize(ev[TB_PACK]));
+    float ms[BT_NSTAGE + 1] = {0};
+    for (int s = 0; s < BT_NSTAGE; s++) CK(cudaEventElapsedTime(&ms[s], ev[s], ev[s + 1]));
+    CK(cudaEventElapsedTime(&ms[BT_NSTAGE], ev[TB_START], ev[TB_PACK]));
+    for (int s = 0; s <= BT_NSTAGE; s++) b->stage_us[s] += 1000.0 * ms[s];
+    b->timed++;
+    if (!t.tuning || b->tuned || b->fixed) return;
+    if (t.pmbs == t.mbs && t.pmbs > 0) {  // P-frames only: comparable steps
+        b->tune_us[0][t.cand] += 1000.0 * ms[2] / (double)t.pmbs;  // search
+        b->tune_us[1][t.cand] += 1000.0 * ms[5] / (double)t.mbs;   // residual
+        b->tune_us[2][t.cand] += 1000.0 * ms[6] / (double)t.mbs;   // deblock
+        b->tune_n[t.cand]++;
+    }
+    for (int q = 0; q < 3; q++)
+        if (b->tune_n[q] < TUNE_ROUNDS) return;
+    auto pick = [&](int d) {
+        int k = 0;
+        for (int q = 1; q < 3; q++)
+            if (b->tune_us[d][q] / b->tune_n[q] < b->tune_us[d][k] / b->tune_n[k]) k = q;
+        return k;
+    };
+    b->tune.row_ctas = TUNE_ROWS_PCT[pick(0)];
+    b->tune.res_mbs = TUNE_RES_MBS[pick(1)];
+    b->tune.db_tw = TUNE_DB_TW[pick(2)];
+    b->tuned = true;
+}
+
+static riv_status batch_step(riv_batch* b, int src, const void* const* frames, const uint64_t* ts) {
+    if (b->poisoned) {
+        b->err = "batch unusable after an earlier failure: " + b->err;
+        return RIV_ERR_ENCODING_FAILED;
+    }
+    const int n = (int)b->clips.size();
+    riv_status refused = RIV_OK;
+    try {
+        CK(cudaSetDevice(b->device));
+        // ---- jobs, in clip order
+        std::vector<int> act;
+        std::vector<Job*> jobs;
+        for (int i = 0; i < n; i++) {
+            if (!frames[i]) continue;
+            riv_encoder* e = b->clips[i];
+            if (e->poisoned) return batch_fail(b, poisoned_status(e), "clip " + std::to_string(i) + ": " + e->err);
+            const size_t cap = e->slots.size();
+            while (e->jobs.size() >= cap) {
+                riv_status st = pump(e, true);
+                if (st == RIV_ERR_IO) { refused = st; continue; }
+                if (st) return batch_fail(b, st, "clip " + std::to_string(i) + ": " + e->err);
+            }
+            const uint64_t idx = e->submitted;
+            const bool intra = next_is_key(e);
+            e->jobs.emplace_back();
+            Job& j = e->jobs.back();
+            j.index = idx;
+            j.ts = ts[i];
+            j.type = intra ? 1 : 2;
+            j.slot = (int)(idx % cap);
+            j.timed = false;
+            act.push_back(i);
+            jobs.push_back(&j);
+        }
+        if (act.empty()) return refused;
+        const int m = (int)act.size();
+        bool tuning = false;
+        int cand = 0;
+        BatchTune t = batch_step_tune(b, tuning, cand);
+        const bool timed = tuning || b->steps % 8 == 0;
+        // staging buffer of this step (its previous copy to the device is done)
+        uint8_t* hd = b->hdesc[b->dpar].as<uint8_t>();
+        CK(cudaEventSynchronize(b->ev_desc[b->dpar]));
+        BatchClip* kc = (BatchClip*)hd;
+        SearchParams* kp = (SearchParams*)(hd + b->off_sp);
+        int* kst = (int*)(hd + b->off_start);
+        int* kss = (int*)(hd + b->off_sstart);
+        std::vector<int> pvar(m, -1);  // search variant of each P clip
+        std::vector<SearchParams> sps(m);
+        uint64_t step_mbs = 0, step_pmbs = 0;
+        for (int a = 0; a < m; a++) {
+            riv_encoder* e = b->clips[act[a]];
+            batch_collect(e, *jobs[a], src, frames[act[a]], b->Hs, kc[a], sps[a]);
+            step_mbs += (uint64_t)e->NMB;
+            if (jobs[a]->type == 2) {
+                pvar[a] = search_variant(e);
+                step_pmbs += (uint64_t)e->NMB;
+            }
+        }
+        // stage ranges
+        int tot[BS_N];
+        for (int s = 0; s < BS_N; s++) {
+            int* st = kst + s * (m + 1);
+            st[0] = 0;
+            for (int a = 0; a < m; a++) st[a + 1] = st[a] + batch_ctas_host(s, kc[a], t);
+            tot[s] = st[m];
+        }
+        // search launches, one per variant present; each variant's parameters contiguous in kp,
+        // its row CTAs spread over its clips
+        int stot[3] = {0, 0, 0}, sfirst[3] = {0, 0, 0}, scount[3] = {0, 0, 0};
+        int pos = 0;
+        for (int v = 0; v < 3; v++) {
+            std::vector<int> mem, nmb, bh, rows;
+            for (int a = 0; a < m; a++)
+                if (pvar[a] == v) { mem.push_back(a); nmb.push_back(kc[a].NMB); bh.push_back(kc[a].H / 16); }
+            if (mem.empty()) continue;
+            if ((int)mem.size() > b->cap[v]) throw std::runtime_error("more P-frame clips in one step than search CTAs fit");
+            const int total = std::max((int)mem.size(), b->cap[v] * t.row_ctas / 100);
+            spread_rows(nmb, bh, total, rows);
+            int* ss = kss + v * (n + 1);
+            ss[0] = 0;
+            sfirst[v] = pos;
+            scount[v] = (int)mem.size();
+            for (size_t q = 0; q < mem.size(); q++) {
+                SearchParams& sp = kp[pos++];
+                sp = sps[mem[q]];
+                sp.nrow_ctas = rows[q];
+                sp.cta0 = ss[q];
+                ss[q + 1] = ss[q] + rows[q];
+            }
+            stot[v] = ss[mem.size()];
+        }
+        // ---- the step's GPU work on B: the host->device copies, the descriptors, the stages
+        cudaStream_t B = b->B;
+        if (src == 0) {
+            CK(cudaEventRecord(b->ev_h2d, b->Hs));
+            CK(cudaStreamWaitEvent(B, b->ev_h2d, 0));
+        }
+        CK(cudaMemcpyAsync(b->ddesc.p, hd, b->desc_bytes, cudaMemcpyHostToDevice, B));
+        CK(cudaEventRecord(b->ev_desc[b->dpar], B));
+        b->dpar ^= 1;
+        const uint8_t* dd = b->ddesc.as<uint8_t>();
+        BatchLaunch L{(const BatchClip*)dd, (const int*)(dd + b->off_start), m};
+        cudaEvent_t* evt = b->ev_t[b->tpar];
+        auto mark = [&](int k) {
+            if (timed) CK(cudaEventRecord(evt[k], B));
+        };
+        auto stage = [&](int s, int tb) {
+            CK(launch_batch_stage(s, L, t, tot[s], b->max_sr, B));
+            if (tot[s] > 0) b->launches++;
+            mark(tb);
+        };
+        mark(TB_START);
+        stage(BS_CONVERT, TB_CONVERT);
+        stage(BS_TABLE, TB_TABLE);
+        for (int v = 0; v < 3; v++) {
+            if (!stot[v]) continue;
+            const SearchParams* dps = (const SearchParams*)(dd + b->off_sp) + sfirst[v];
+            const int* dss = (const int*)(dd + b->off_sstart) + v * (n + 1);
+            CK(launch_search_multi(dps, dss, scount[v], stot[v], v < 2, v == 0, b->ssmem[v], b->sthreads[v], B));
+            b->launches++;
+        }
+        mark(TB_SEARCH);
+        stage(BS_PREDICT, TB_PREDICT);
+        stage(BS_AQSUM, TB_AQSUM);
+        stage(BS_RESIDUAL, TB_RESIDUAL);
+        stage(BS_DEBLOCK, TB_DEBLOCK);
+        stage(BS_SCAN, TB_SCAN);
+        stage(BS_PACK, TB_PACK);
+        CK(cudaEventRecord(b->ev_gpu, B));
+        // ---- copies back: side info, EOBs and a bounded prefix of the coefficients per clip
+        cudaEvent_t xev = b->ev_step[b->steps % b->ev_step.size()];
+        CK(cudaStreamWaitEvent(b->C, b->ev_gpu, 0));
+        for (int a = 0; a < m; a++) {
+            riv_encoder* e = b->clips[act[a]];
+            Slot& s = e->slots[jobs[a]->slot];
+            const int N = e->NMB;
+            CK(cudaMemcpyAsync(s.side.p, s.dside.p, (size_t)N * 4, cudaMemcpyDeviceToHost, b->C));
+            CK(cudaMemcpyAsync(s.peobs.p, s.dpeobs.p, (size_t)N * 3, cudaMemcpyDeviceToHost, b->C));
+            s.prefetched = std::min(e->coef_guess, (size_t)N * 384 * 2);
+            CK(cudaMemcpyAsync(s.packed.p, s.dpacked.p, s.prefetched, cudaMemcpyDeviceToHost, b->C));
+            b->d2h_bytes += (uint64_t)N * 7 + s.prefetched;
+        }
+        CK(cudaEventRecord(xev, b->C));
+        if (src == 0) {
+            for (int a = 0; a < m; a++) {
+                const riv_config& c = b->clips[act[a]]->cfg;
+                b->h2d_bytes += (uint64_t)c.display_width * c.display_height * 3;
+            }
+            CK(cudaEventSynchronize(b->ev_h2d));  // the caller's buffers are reusable
+        }
+        for (int a = 0; a < m; a++) {
+            riv_encoder* e = b->clips[act[a]];
+            Job& j = *jobs[a];
+            j.xev = xev;
+            j.tail_done = true;
+            e->submitted++;
+        }
+        b->steps++;
+        b->frames += (uint64_t)m;
+        b->mbs += step_mbs;
+        if (timed) {
+            riv_batch::TimedStep& tsp = b->tpend[b->tpar];
+            tsp.pending = true;
+            tsp.tuning = tuning;
+            tsp.cand = cand;
+            tsp.mbs = step_mbs;
+            tsp.pmbs = step_pmbs;
+            b->tpar ^= 1;
+            if (tuning) b->tune_step++;
+            batch_read_times(b, b->tpar);  // the other set: the previous timed step
+        }
+        // ---- each clip's host pipeline advances
+        for (int a = 0; a < m; a++) {
+            riv_encoder* e = b->clips[act[a]];
+            riv_status st = pump(e, false);
+            if (st == RIV_ERR_IO) { refused = st; continue; }
+            if (st) return batch_fail(b, st, "clip " + std::to_string(act[a]) + ": " + e->err);
+        }
+    } catch (const CudaError& ce) {
+        const std::string msg = std::string(ce.where) + ": " + cudaGetErrorString(ce.e);
+        for (riv_encoder* e : b->clips) {
+            e->poisoned = true;
+            e->poison_msg = msg;
+        }
+        return batch_fail(b, RIV_ERR_CUDA, msg);
+    } catch (const std::exception& ex) {
+        b->poisoned = true;
+        return batch_fail(b, RIV_ERR_ENCODING_FAILED, ex.what());
+    }
+    if (refused) b->err = "writer.write failed for a record of at least one clip; that record is lost";
+    return refused;
+}
+
+}  // namespace
+
+extern "C" {
+
+riv_status riv_batch_new(const riv_config* cfgs, const riv_writer_vtable* writers, uint32_t n, riv_batch** out) {
+    if (!cfgs || !writers || !out || n == 0 || n > RIV_BATCH_MAX_CLIPS) return RIV_ERR_INVALID_CONFIG;
+    *out = nullptr;
+    for (uint32_t i = 0; i < n; i++)
+        if (cfgs[i].device != cfgs[0].device || cfgs[i].encode_form != RIV_FORM_PLAIN) return RIV_ERR_INVALID_CONFIG;
+    riv_batch* b = new riv_batch();
+    b->device = cfgs[0].device;
+    try {
+        CK(cudaSetDevice(b->device));
+        const unsigned hw = std::max(2u, std::thread::hardware_concurrency());
+        b->pool = std::make_shared<ThreadPool>(hw - 1);
+        b->rans_pool = std::make_shared<ThreadPool>(std::max(2u, hw / 2));
+        size_t maxcap = 1;
+        for (uint32_t i = 0; i < n; i++) {
+            riv_config c = cfgs[i];
+            c.entropy_threads = 1;  // the clips share the batch's pools (set below)
+            riv_encoder* e = nullptr;
+            riv_status st = riv_encoder_new(&c, &writers[i], &e);
+            if (st) {
+                riv_batch_free(b);
+                return st;
+            }
+            e->cfg.entropy_threads = cfgs[i].entropy_threads;
+            e->batched = true;
+            e->defer_ok = false;  // each step reconstructs its frames itself
+            e->pool = b->pool;
+            e->rans_pool = b->rans_pool;
+            ThreadPool* rp = b->rans_pool.get();
+            e->rans_submit = [rp](std::function<void()> f) { return rp->submit(std::move(f)); };
+            e->rans_parts = (int)std::max(2u, hw / 2) + 1;
+            b->clips.push_back(e);
+            b->max_sr = std::max(b->max_sr, (int)c.search_range);
+            maxcap = std::max(maxcap, e->slots.size());
+        }
+        CK(cudaStreamCreateWithFlags(&b->B, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&b->Hs, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&b->C, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&b->ev_h2d, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&b->ev_gpu, cudaEventDisableTiming));
+        b->ev_step.resize(maxcap + 2);
+        for (auto& ev : b->ev_step) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        for (int q = 0; q < 2; q++)
+            for (int k = 0; k < BT_BOUNDS; k++) CK(cudaEventCreate(&b->ev_t[q][k]));
+        for (int k = 0; k < 2; k++) {
+            CK(cudaEventCreateWithFlags(&b->ev_desc[k], cudaEventDisableTiming));
+            CK(cudaEventRecord(b->ev_desc[k], b->B));
+        }
+        auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+        b->off_sp = al((size_t)n * sizeof(BatchClip));
+        b->off_start = b->off_sp + al((size_t)n * sizeof(SearchParams));
+        b->off_sstart = b->off_start + al((size_t)BS_N * (n + 1) * sizeof(int));
+        b->desc_bytes = b->off_sstart + al((size_t)3 * (n + 1) * sizeof(int));
+        for (int k = 0; k < 2; k++) {
+            b->hdesc[k].alloc(b->desc_bytes);
+            memset(b->hdesc[k].p, 0, b->desc_bytes);
+        }
+        b->ddesc.alloc(b->desc_bytes);
+        int dev = 0, nsm = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        for (int v = 0; v < 3; v++) {
+            int per_sm = 0;
+            CK(search_multi_capacity(v < 2, v == 0, b->max_sr, &per_sm, &b->ssmem[v], &b->sthreads[v]));
+            b->cap[v] = per_sm * nsm;
+        }
+        CK(cudaStreamSynchronize(b->B));
+    } catch (const CudaError& ce) {
+        fprintf(stderr, "riv_batch_new: %s: %s\n", ce.where, cudaGetErrorString(ce.e));
+        riv_batch_free(b);
+        return RIV_ERR_CUDA;
+    } catch (const std::exception& ex) {
+        fprintf(stderr, "riv_batch_new: %s\n", ex.what());
+        riv_batch_free(b);
+        return RIV_ERR_ENCODING_FAILED;
+    }
+    *out = b;
+    return RIV_OK;
+}
+
+riv_status riv_batch_encode(riv_batch* b, const uint8_t* const* frames, const uint64_t* ts) {
+    if (!b || !frames || !ts) return RIV_ERR_FRAME;
+    return batch_step(b, 0, (const void* const*)frames, ts);
+}
+
+riv_status riv_batch_encode_device(riv_batch* b, const void* const* d_frames, const uint64_t* ts) {
+    if (!b || !d_frames || !ts) return RIV_ERR_FRAME;
+    return batch_step(b, 1, d_frames, ts);
+}
+
+riv_status riv_batch_finish(riv_batch* b) {
+    if (!b) return RIV_ERR_INVALID_CONFIG;
+    try {
+        CK(cudaSetDevice(b->device));
+        batch_read_times(b, 0);
+        batch_read_times(b, 1);
+    } catch (const CudaError& ce) {
+        return batch_fail(b, RIV_ERR_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
+    }
+    riv_status first = RIV_OK;
+    for (size_t i = 0; i < b->clips.size(); i++) {
+        riv_status st = riv_finish(b->clips[i]);
+        if (st && !first) {
+            first = st;
+            b->err = "clip " + std::to_string(i) + ": " + b->clips[i]->err;
+        }
+    }
+    return first;
+}
+
+void riv_batch_free(riv_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->B) cudaStreamSynchronize(b->B);
+    if (b->C) cudaStreamSynchronize(b->C);
+    if (b->Hs) cudaStreamSynchronize(b->Hs);
+    for (riv_encoder* e : b->clips) riv_encoder_free(e);
+    b->clips.clear();
+    b->pool.reset();
+    b->rans_pool.reset();
+    for (auto& ev : b->ev_step)
+        if (ev) cudaEventDestroy(ev);
+    for (int q = 0; q < 2; q++)
+        for (int k = 0; k < BT_BOUNDS; k++)
+            if (b->ev_t[q][k]) cudaEventDestroy(b->ev_t[q][k]);
+    for (int k = 0; k < 2; k++) {
+        if (b->ev_desc[k]) cudaEventDestroy(b->ev_desc[k]);
+        b->hdesc[k].release();
+    }
+    if (b->ev_h2d) cudaEventDestroy(b->ev_h2d);
+    if (b->ev_gpu) cudaEventDestroy(b->ev_gpu);
+    b->ddesc.release();
+    if (b->B) cudaStreamDestroy(b->B);
+    if (b->C) cudaStreamDestroy(b->C);
+    if (b->Hs) cudaStreamDestroy(b->Hs);
+    delete b;
+}
+
+const char* riv_batch_last_error(const riv_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+riv_status riv_batch_set_tune(riv_batch* b, const riv_batch_tune* t) {
+    if (!b || !t) return RIV_ERR_INVALID_CONFIG;
+    if ((t->res_mbs != 2 && t->res_mbs != 4 && t->res_mbs != 8) || (t->db_tw != 64 && t->db_tw != 128 && t->db_tw != 256) ||
+        t->search_rows_pct < 1 || t->search_rows_pct > 100)
+        return RIV_ERR_INVALID_CONFIG;
+    b->tune.row_ctas = t->search_rows_pct;
+    b->tune.res_mbs = t->res_mbs;
+    b->tune.db_tw = t->db_tw;
+    b->fixed = true;
+    return RIV_OK;
+}
+
+riv_status riv_batch_get_tune(const riv_batch* b, riv_batch_tune* t, int* tuned) {
+    if (!b || !t) return RIV_ERR_INVALID_CONFIG;
+    t->search_rows_pct = b->tune.row_ctas;
+    t->res_mbs = b->tune.res_mbs;
+    t->db_tw = b->tune.db_tw;
+    if (tuned) *tuned = b->fixed ? 2 : (b->tuned ? 1 : 0);
+    return RIV_OK;
+}
+
+riv_status riv_batch_counters(const riv_batch* b, uint64_t* c7, double* stage_us10) {
+    if (!b) return RIV_ERR_INVALID_CONFIG;
+    if (c7) {
+        c7[0] = b->steps;
+        c7[1] = b->frames;
+        c7[2] = b->mbs;
+        c7[3] = b->launches;
+        c7[4] = b->timed;
+        c7[5] = b->h2d_bytes;
+        c7[6] = b->d2h_bytes;
+    }
+    if (stage_us10)
+        for (int s = 0; s <= BT_NSTAGE; s++) stage_us10[s] = b->timed ? b->stage_us[s] / (double)b->timed : 0.0;
+    return RIV_OK;
+}
+
+riv_status riv_batch_last_recon(riv_batch* b, uint32_t clip, uint8_t* y, uint8_t* u, uint8_t* v) {
+    if (!b || clip >= b->clips.size()) return RIV_ERR_INVALID_CONFIG;
+    riv_encoder* e = b->clips[clip];
+    if (!e->has_ref) return RIV_ERR_FRAME;
+    try {
+        CK(cudaSetDevice(b->device));
+        CK(cudaStreamSynchronize(b->B));
+        const uint8_t* d = e->ref[e->ref_cur].as<uint8_t>();
+        const size_t ys = (size_t)e->W * e->H, cs = ys / 4;
+        CK(cudaMemcpy(y, d, ys, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(u, d + ys, cs, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(v, d + ys + cs, cs, cudaMemcpyDeviceToHost));
+    } catch (const CudaError& ce) {
+        return batch_fail(b, RIV_ERR_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
+    }
+    return RIV_OK;
+}
+
+riv_status riv_batch_clip_counters(const riv_batch* b, uint32_t clip, uint64_t* frames_written, double* host_ms6) {
+    if (!b || clip >= b->clips.size()) return RIV_ERR_INVALID_CONFIG;
+    const riv_encoder* e = b->clips[clip];
+    if (frames_written) *frames_written = e->frame_count;
+    if (host_ms6)
+        for (int k = 0; k < 6; k++) host_ms6[k] = e->host_ms[k];
+    return RIV_OK;
 }
 
 }  // extern "C"

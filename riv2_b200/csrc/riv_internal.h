@@ -81,6 +81,7 @@ struct SearchParams {
     long long spin_limit;
     long long* prof;  // optional: RIV_PROF_WORDS words per MB (phase stamps, hexagon rounds), nullptr = off
     int nrow_ctas;    // CTAs that own MB rows (row stride); the rest of the grid are table workers
+    int cta0;         // first CTA of this clip in a multi-clip launch (0 for a single clip)
     int row_helpers;  // row CTAs run worker groups before their row starts and after it ends
     unsigned* tflag;  // fused table: per-MB flag = tag once its table row is written; nullptr = precomputed
     // Prediction and AQ inside the search launch (band + table instantiations): nullptr lnv =
@@ -115,6 +116,59 @@ struct SearchParams {
     uint32_t* c_hdr;
 };
 
+
+// ---- multi-clip steps (riv_batch): one launch per stage over every clip of the step.
+// One clip's frame in a step.
+struct BatchClip {
+    int W, H, BW, NMB;  // storage size
+    int intra;          // 1 key frame, 0 P-frame
+    // conversion: display-size RGB24 (nullptr: cur already holds the frame's planes)
+    const uint8_t* rgb;
+    int dw, dh;
+    uint8_t* cur;  // planar YUV of the frame
+    // P-frames: the previous frame's deblocked reconstruction, the SAD table, the search's
+    // per-MB output, the prediction and the ln variances (NMB values, then their mean)
+    const uint8_t* ref;
+    uint16_t* tab;
+    int tstride, sr;
+    const MbOut* mbo;
+    uint8_t* pred;
+    float* lnv;
+    const uint32_t* logfix;
+    int nlog;
+    ResidualParams rp;  // residual (steps from lnv for P-frames, intra tables for key frames)
+    // deblock (db_level > 0): db_src -> db_dst
+    int db_level, db_E, db_I, db_H;
+    const uint8_t* db_src;
+    uint8_t* db_dst;
+    const uint8_t* db_mask;
+    // compaction into the slot's buffers; c_hdr = mapped host words (coded MBs, coefficients,
+    // status)
+    int32_t* c_index;
+    int32_t* c_offset;
+    uint32_t* c_side;
+    int16_t* c_packed;
+    uint8_t* c_peobs;
+    uint32_t* c_hdr;
+    const unsigned* status;
+};
+enum BatchStage { BS_CONVERT, BS_TABLE, BS_PREDICT, BS_AQSUM, BS_RESIDUAL, BS_DEBLOCK, BS_SCAN, BS_PACK, BS_N };
+// Tile shapes of a step (chosen by the batch's autotuner; the output does not depend on them).
+struct BatchTune {
+    int res_mbs;   // MBs per residual CTA: 2, 4 or 8
+    int db_tw;     // deblock tile width in luma columns: 64, 128 or 256
+    int row_ctas;  // search: percent of the device's capacity of search CTAs used by a step
+};
+struct BatchLaunch {
+    const BatchClip* clips;  // device, nclips
+    const int* start;        // device, BS_N x (nclips + 1) CTA prefix sums
+    int nclips;
+};
+int batch_ctas_host(int stage, const BatchClip& k, const BatchTune& t);
+int launch_batch_stage(int stage, const BatchLaunch& b, const BatchTune& t, int total_ctas, int max_sr, void* stream);
+int search_multi_capacity(bool table, bool small, int max_sr, int* per_sm, size_t* smem, int* threads);
+int launch_search_multi(const SearchParams* dparams, const int* dstart, int nclips, int total_ctas, bool table,
+                        bool small, size_t smem, int threads, void* stream);
 
 enum StatusBits : unsigned {
     ST_WAIT_TIMEOUT = 1u,

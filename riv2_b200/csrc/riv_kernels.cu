@@ -866,10 +866,13 @@ __device__ __forceinline__ void filter_line(int* px, int E, int I, int Hv) {
 constexpr int DB_TILE_BYTES = (16 + 8) * (DB_TW + 8);
 // One tile (plane, t: band-major tile index within the plane) by nthr threads synchronised on
 // group barrier `bar` (0 = the whole CTA); `tile` = DB_TILE_BYTES of shared memory.
+// TW: tile width in luma columns (DB_TW everywhere but the tuned multi-clip launch), tile =
+// (16 + 8) * (TW + 8) bytes.
+template <int TW = DB_TW>
 __device__ __forceinline__ void deblock_tile(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, int W, int H,
                                              int BW, int E, int I, int Hv, const uint8_t* mask, int plane, int t,
                                              uint8_t* tile, int tid, int nthr, int bar) {
-    const int w = plane ? W / 2 : W, h = plane ? H / 2 : H, g = plane ? 8 : 16, tw = plane ? DB_TW / 2 : DB_TW;
+    const int w = plane ? W / 2 : W, h = plane ? H / 2 : H, g = plane ? 8 : 16, tw = plane ? TW / 2 : TW;
     const size_t poff = plane == 0 ? 0 : (size_t)W * H + (plane == 2 ? (size_t)(W / 2) * (H / 2) : 0);
     const uint8_t* pl = src + poff;
     uint8_t* po = dst + poff;
@@ -877,7 +880,7 @@ __device__ __forceinline__ void deblock_tile(const uint8_t* __restrict__ src, ui
     const int band = t / tpb, X0 = (t % tpb) * tw, X1 = min(X0 + tw, w);
     const int Y0 = band * g, Y1 = Y0 + g;
     const int ry0 = max(Y0 - 4, 0), ry1 = min(Y1 + 4, h), cx0 = max(X0 - 4, 0), cx1 = min(X1 + 4, w);
-    const int TS = DB_TW + 8, oy = Y0 - 4, ox = X0 - 4;  // tile row stride and origin
+    const int TS = TW + 8, oy = Y0 - 4, ox = X0 - 4;  // tile row stride and origin
     const int nrow = ry1 - ry0, ncol = cx1 - cx0;
     for (int i = tid; i < nrow * ncol; i += nthr) {
         const int r = i / ncol, c = i - r * ncol;
@@ -923,6 +926,11 @@ __device__ __forceinline__ void deblock_tile(const uint8_t* __restrict__ src, ui
         po[(size_t)(Y0 + r) * w + X0 + c] = tile[(Y0 + r - oy) * TS + X0 + c - ox];
     }
 }
+
+// This CTA's index within its clip's part of the grid: a single-clip launch owns the whole
+// grid (cta0 = 0); a multi-clip launch gives each clip a contiguous range of CTAs starting
+// at cta0.
+__device__ __forceinline__ int row_cta(const SearchParams& p) { return (int)blockIdx.x - p.cta0; }
 
 // ---- search warp -> mode warp handoff through a shared-memory ring (one CTA per MB row)
 // Slot word: [63:49] (n + 1) mod 2^15 for the n-th MB of the CTA, [48] failure, [47:32] best
@@ -1064,7 +1072,7 @@ __device__ __forceinline__ void mode_warp(const SearchParams& p, const unsigned 
     };
     const bool has_tm = p.prev_coded != nullptr;
     int n = 0;
-    for (int r = blockIdx.x; r < p.BH; r += p.nrow_ctas) {
+    for (int r = row_cta(p); r < p.BH; r += p.nrow_ctas) {
         MvT L_cod{0, 0, 0, 0};
         unsigned long long vT = 0, vTL = 0;
         for (int bx = 0; bx < p.BW; bx++) {
@@ -1558,7 +1566,7 @@ __device__ __forceinline__ void loader_warp(const SearchParams& p, unsigned long
         }
         return __shfl_sync(0xffffffffu, ok, 0) != 0;
     };
-    for (int r = blockIdx.x; r < p.BH && !abort; r += p.nrow_ctas) {
+    for (int r = row_cta(p); r < p.BH && !abort; r += p.nrow_ctas) {
         const int wy0 = r * 16 - sr - 1;
         if (rows > 0 && !(wait_ctl(1, rows) && (p.lnv == nullptr || wait_ctl(3, rows)))) { abort = true; break; }
         if (p.defer) {  // the previous frame's bands r-1 .. r+1 must be deblocked (written by workers)
@@ -1651,7 +1659,7 @@ __device__ __forceinline__ void aq_warp(const SearchParams& p, const unsigned lo
     uint8_t* PY = p.pred;
     const int yy = lane >> 1, xoff = (lane & 1) * 8;  // luma: row, 8-pixel half
     int n = 0, rows = 0;
-    for (int r = blockIdx.x; r < p.BH; r += p.nrow_ctas) {
+    for (int r = row_cta(p); r < p.BH; r += p.nrow_ctas) {
         const int y0 = r * 16, wy0 = y0 - sr - 1;
         // observe the band fill of this row (the loader refills only after this warp is done)
         if (!mbar_wait_warp(bandb, (unsigned)(rows & 1), p.spin_limit)) {
@@ -1789,7 +1797,7 @@ __device__ __forceinline__ void search_body(const SearchParams& p) {
     // search warp stages its own data with cp.async and the third warp is not launched.
     constexpr bool FAST = BAND && TABLE;
     extern __shared__ __align__(16) uint8_t smem[];
-    if (FAST && p.tflag != nullptr && (int)blockIdx.x >= p.nrow_ctas) {
+    if (FAST && p.tflag != nullptr && row_cta(p) >= p.nrow_ctas) {
         frame_worker(p, smem);
         return;
     }
@@ -1845,7 +1853,7 @@ __device__ __forceinline__ void search_body(const SearchParams& p) {
     if (threadIdx.x >= 64) {
         if (FAST && threadIdx.x < 96) {
             loader_warp(p, fullb, bandb, ld_ctl, slots, refmem, helpers ? row_live : nullptr);
-            if (p.lnv != nullptr && blockIdx.x == 0) aq_fold(p, ld_ctl, fold_stage);
+            if (p.lnv != nullptr && row_cta(p) == 0) aq_fold(p, ld_ctl, fold_stage);
         } else if (FAST && threadIdx.x < 128 && p.lnv != nullptr) {
             aq_warp(p, hand, hand_done, ld_ctl, refmem, bandb);
         } else if (helpers && threadIdx.x >= TW_GROUP) {
@@ -1868,7 +1876,7 @@ __device__ __forceinline__ void search_body(const SearchParams& p) {
     bool failed = false;
     int hn = 0;  // MBs handed to the mode warp so far
 
-    for (int r = blockIdx.x; r < p.BH; r += p.nrow_ctas) {
+    for (int r = row_cta(p); r < p.BH; r += p.nrow_ctas) {
         const int y0 = r * 16;
         const int wy0 = y0 - sr - 1;
         __syncwarp();
@@ -2922,10 +2930,12 @@ int launch_learned(const SearchParams& sp, const float* net, int margin, float s
 // chroma: copy at the truncated (x0+dx)/2 origin for in-bounds integer MVs, else
 // rounded bilinear at chroma half-pel (2c + (mv_hp >> 1)).
 // ---------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_predict(const uint8_t* __restrict__ ref, const MbOut* __restrict__ mbo,
-                                                 uint8_t* __restrict__ pred, uint2* __restrict__ varsum, int W, int H) {
+// MB mb by 256 threads; returns the luma (sum, sum of squares) to thread 0 (ws, ws2: 8 words
+// of shared memory each).
+__device__ __forceinline__ uint2 predict_mb(const uint8_t* __restrict__ ref, const MbOut* __restrict__ mbo,
+                                            uint8_t* __restrict__ pred, int W, int H, int mb, unsigned* ws,
+                                            unsigned* ws2) {
     const int BW = W / 16;
-    const int mb = blockIdx.x;
     const int bx = mb % BW, by = mb / BW;
     const int x0 = bx * 16, y0 = by * 16;
     const int t = threadIdx.x;
@@ -2959,14 +2969,18 @@ __global__ void __launch_bounds__(256) k_predict(const uint8_t* __restrict__ ref
     unsigned s = (unsigned)v, s2 = (unsigned)(v * v);
     s = __reduce_add_sync(0xffffffffu, s);
     s2 = __reduce_add_sync(0xffffffffu, s2);
-    __shared__ unsigned ws[8], ws2[8];
     if ((t & 31) == 0) { ws[t >> 5] = s; ws2[t >> 5] = s2; }
     __syncthreads();
-    if (t == 0) {
-        unsigned a = 0, b = 0;
+    unsigned a = 0, b = 0;
+    if (t == 0)
         for (int i = 0; i < 8; i++) { a += ws[i]; b += ws2[i]; }
-        varsum[mb] = make_uint2(a, b);
-    }
+    return make_uint2(a, b);
+}
+__global__ void __launch_bounds__(256) k_predict(const uint8_t* __restrict__ ref, const MbOut* __restrict__ mbo,
+                                                 uint8_t* __restrict__ pred, uint2* __restrict__ varsum, int W, int H) {
+    __shared__ unsigned ws[8], ws2[8];
+    const uint2 vs = predict_mb(ref, mbo, pred, W, H, blockIdx.x, ws, ws2);
+    if (threadIdx.x == 0) varsum[blockIdx.x] = vs;
 }
 
 int launch_predict(const uint8_t* ref, const MbOut* mb, uint8_t* pred, uint2* varsum, int W, int H, void* stream) {
@@ -3034,8 +3048,7 @@ __global__ void k_aq_log(const uint2* __restrict__ varsum, int n, const uint32_t
 }
 // The strictly sequential f32 sum (Iterator::sum folds left to right): staged through
 // shared memory by the whole CTA, folded by one thread.
-__global__ void __launch_bounds__(1024) k_aq_sum(const float* __restrict__ lnv, int n, float* avg_out) {
-    extern __shared__ float sl[];
+__device__ __forceinline__ void aq_sum_cta(const float* __restrict__ lnv, int n, float* avg_out, float* sl) {
     __shared__ float part;
     if (threadIdx.x == 0) part = 0.0f;
     const int CH = 8192;
@@ -3058,6 +3071,10 @@ __global__ void __launch_bounds__(1024) k_aq_sum(const float* __restrict__ lnv, 
     }
     __syncthreads();
     if (threadIdx.x == 0) *avg_out = __fdiv_rn(part, (float)n);
+}
+__global__ void __launch_bounds__(1024) k_aq_sum(const float* __restrict__ lnv, int n, float* avg_out) {
+    extern __shared__ float sl[];
+    aq_sum_cta(lnv, n, avg_out, sl);
 }
 __global__ void k_aq_steps(const float* __restrict__ lnv, int n, const float* avg_in, float base,
                            const uint32_t* expfix, int nexp, float* qs) {
@@ -3273,6 +3290,9 @@ int launch_compact(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coef
     k_pack<<<(nmb + 7) / 8, 256, 0, st>>>(opt_skip, mb, coeffs, eobs, index, offset, intra, nmb, dside, dpacked, dpeobs);
     return (int)cudaGetLastError();
 }
+
+// Multi-clip launches of the stages above (riv_batch).
+#include "riv_batch.cuh"
 
 }  // namespace riv
 

@@ -115,6 +115,9 @@ EXPORTED_SYMBOLS = (
     "riv_test_mv_decode", "riv_test_delta_bias", "riv_test_worker_queue", "riv_test_libm_range",
     "riv_stage_predict", "riv_stage_residual", "riv_test_wait_expiry", "riv_encoder_set_proposal",
     "riv_learned_counters", "riv_test_mv_encode_threads",
+    "riv_batch_new", "riv_batch_encode", "riv_batch_encode_device", "riv_batch_finish", "riv_batch_free",
+    "riv_batch_last_error", "riv_batch_set_tune", "riv_batch_get_tune", "riv_batch_counters", "riv_batch_last_recon",
+    "riv_batch_clip_counters",
 )
 
 

@@ -47,3 +47,29 @@ def test_decoder_without_device_raises():
     stream = enc.finish()
     with pytest.raises(D.CudaError):
         D.Decoder.new(stream)
+
+
+def test_batch_without_device_raises_cuda_error():
+    if _device_present():
+        pytest.skip("a CUDA device is visible")
+    from riv2_b200 import encoder as E
+    from riv2_b200.batch import Batch
+    cfgs = [E.EncoderConfig.new(64, 48, 30), E.EncoderConfig.new(352, 288, 30)]
+    ws = [E.VecWriter(), E.VecWriter()]
+    with pytest.raises(E.CudaError):
+        Batch.new(cfgs, ws)
+    assert all(w.into_inner() == b"" for w in ws)
+
+
+def test_batch_rejects_bad_clip_sets():
+    # checked before any device call
+    from riv2_b200 import encoder as E
+    from riv2_b200.batch import Batch
+    with pytest.raises(E.InvalidConfig):
+        Batch.new([], [])
+    learned = E.EncoderConfig.new(64, 48, 30).with_encode_form(1)
+    with pytest.raises(E.InvalidConfig):
+        Batch.new([E.EncoderConfig.new(64, 48, 30), learned], [E.VecWriter(), E.VecWriter()])
+    other_dev = E.EncoderConfig.new(64, 48, 30).with_device(1)
+    with pytest.raises(E.InvalidConfig):
+        Batch.new([E.EncoderConfig.new(64, 48, 30), other_dev], [E.VecWriter(), E.VecWriter()])
