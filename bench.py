@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--weights", default=WEIGHTS)
     ap.add_argument("--no-secondary", action="store_true", help="skip the secondary measurement points")
+    ap.add_argument("--batch-steps", type=int, default=12, help="timed steps of the multi-clip point (0: skip it)")
+    ap.add_argument("--workload", default="single", choices=["single", "batch"],
+                    help="batch: only the 64-clip multi-clip workload over its whole length, one JSON line")
     ap.add_argument("--margin", type=int, default=256, help="learned form: proposal fallback SAD margin")
     return ap.parse_args()
 
@@ -311,10 +314,106 @@ def quick_fps(frames_dev, w, h, iq, pq, depth, form, params, steps, warmup, sr=1
     return steps / (ev0.elapsed_time(ev1) / 1000.0)
 
 
+BATCH_SIZES = (("cif", 352, 288), ("720p", 640, 360), ("720p", 1280, 720), ("1080p", 1920, 1080))
+
+
+def batch_clips(seed: int):
+    """The multi-clip workload: 16 clips at each of 352x288, 640x360, 1280x720 and 1920x1080
+    with 30-90 frames each (uniform per clip, seeded), generator presets of their size class."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k, (preset, w, h) in enumerate(BATCH_SIZES):
+        for i in range(16):
+            out.append({"preset": preset, "w": w, "h": h, "frames": int(rng.integers(30, 91)),
+                        "seed": seed * 100 + 16 * k + i})
+    return out
+
+
+def batch_point(dev_index: int, seed: int, steps: int, warmup: int, full: bool = False, check: int = 4):
+    """Aggregate throughput of the multi-clip encoder on the 64-clip mixed-resolution workload:
+    RGB frames resident in device memory, one frame per clip per step, `warmup` untimed steps,
+    then the timed steps up to the last record's write (riv_batch_finish inside the timed
+    region).  `full`: every clip's whole length (up to 90 steps); otherwise `steps` steps (every
+    clip has at least 30 frames, so all 64 clips are in every step).  `check` clips (the first of
+    each size class) are encoded again alone by the single-clip encoder and their streams
+    compared byte for byte."""
+    import torch
+
+    from riv2_b200 import encoder as E
+    from riv2_b200.batch import Batch
+    from riv2_b200.synth import SynthClip
+    dev = torch.device("cuda", dev_index)
+    clips = batch_clips(seed)
+    nsteps = max(c["frames"] for c in clips) if full else warmup + steps
+    t0 = time.perf_counter()
+    dframes = []
+    for c in clips:
+        n = min(c["frames"], nsteps)
+        sc = SynthClip(c["preset"], seed=c["seed"], width=c["w"], height=c["h"])
+        dframes.append(torch.from_numpy(sc.frames(n)).to(dev))
+    gen_s = time.perf_counter() - t0
+    cfgs = [(E.EncoderConfig.new(c["w"], c["h"], 30).with_intra_quality(85).with_inter_quality(80)
+             .with_keyframe_interval(E.KeyframeInterval.fixed(1 << 40)).with_pipeline_depth(4).with_device(dev_index))
+            for c in clips]
+    writers = [E.VecWriter() for _ in clips]
+    b = Batch.new(cfgs, writers)
+    strides = [c["w"] * c["h"] * 3 for c in clips]
+
+    def step(k):
+        ptrs = [f.data_ptr() + k * s if k < f.shape[0] else 0 for f, s in zip(dframes, strides)]
+        b.encode_step_device(ptrs, [k * 33] * len(clips))
+
+    for k in range(warmup):
+        step(k)
+    torch.cuda.synchronize()
+    c0 = b.counters()
+    clk = ClockSampler(dev_index)
+    clk.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
+    ev0.record()
+    for k in range(warmup, nsteps):
+        step(k)
+    b.finish()
+    ev1.record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - w0
+    clocks = clk.stop()
+    ms = ev0.elapsed_time(ev1)
+    c1 = b.counters()
+    tune = b.tune()
+    mbs = c1["mbs"] - c0["mbs"]
+    frames = c1["frames"] - c0["frames"]
+    b.close()
+    streams = [w.into_inner() for w in writers]
+    checked = []
+    for k in range(min(check, len(BATCH_SIZES))):
+        i = 16 * k
+        n = min(clips[i]["frames"], nsteps)
+        enc = E.Encoder.new(cfgs[i], E.VecWriter())
+        for t in range(n):
+            enc.encode_frame_device(dframes[i].data_ptr() + t * strides[i], t * 33)
+        enc.finish()
+        checked.append(enc.writer.into_inner() == streams[i])
+        enc.close()
+    del dframes
+    torch.cuda.empty_cache()
+    return {"macroblocks_per_s": mbs / (ms / 1000.0), "frames_per_s": frames / (ms / 1000.0),
+            "per_clip_fps": (nsteps - warmup) / (ms / 1000.0), "ms": ms, "wall_s": wall, "steps": nsteps - warmup,
+            "warmup": warmup, "clips": len(clips), "frames": frames, "mbs": mbs, "tune": tune,
+            "gpu_stage_us_per_step": {k: round(v, 1) for k, v in c1["stage_us"].items()},
+            "launches_per_step": (c1["launches"] - c0["launches"]) / max(1, nsteps - warmup),
+            "streams_identical_to_single_clip": f"{sum(checked)}/{len(checked)}", "clocks": clocks,
+            "frame_generation_s": round(gen_s, 1),
+            "what": "64 clips (16 each at 352x288, 640x360, 1280x720, 1920x1080; 30-90 frames), q 85/80, one "
+                    "frame per clip per step, RGB resident in device memory" + (", whole clips" if full else "")}
+
+
 def secondary_points(frames_host, dev_index, params, steps, warmup, depth):
     """The other measurement points of the 1080p workload (quality 95/90, search range 31,
-    pipeline depth 0 = the reference's one record per call) and the CIF workload, each for
-    the plain form and, where a network is loaded, the learned form."""
+    pipeline depth 0 = the reference's one record per call), the CIF workload and the
+    high-motion 4K stress clip at q 95/90 and 75/70, each for the plain form and, where a
+    network is loaded, the learned form."""
     import torch
 
     from riv2_b200.synth import SynthClip
@@ -322,10 +421,14 @@ def secondary_points(frames_host, dev_index, params, steps, warmup, depth):
     n = steps + warmup + 1
     f1080 = torch.from_numpy(frames_host[:n]).to(dev)
     cif = torch.from_numpy(SynthClip("cif", seed=2026).frames(max(n, 61))).to(dev)
+    k4 = min(steps, 12)
+    f4k = torch.from_numpy(SynthClip("4k", seed=2026).frames(k4 + warmup + 1)).to(dev)
     points = {"1080p_q95_90": (f1080, 1920, 1080, 95, 90, depth, 12, steps),
               "1080p_sr31": (f1080, 1920, 1080, 85, 80, depth, 31, steps),
               "1080p_depth0": (f1080, 1920, 1080, 85, 80, 0, 12, steps),
-              "cif_q85_80": (cif, 352, 288, 85, 80, depth, 12, 60)}
+              "cif_q85_80": (cif, 352, 288, 85, 80, depth, 12, 60),
+              "4k_q95_90": (f4k, 3840, 2160, 95, 90, depth, 12, k4),
+              "4k_q75_70": (f4k, 3840, 2160, 75, 70, depth, 12, k4)}
     out = {}
     for name, (fr, w, h, iq, pq, d, sr, k) in points.items():
         k = min(k, fr.shape[0] - warmup - 1)
@@ -496,6 +599,19 @@ def main():
     dist = init_dist(ws, "nccl")
     import torch
     dev_index = local if torch.cuda.device_count() > 1 else 0
+    if args.workload == "batch":  # the multi-clip workload alone, every clip over its whole length
+        r = batch_point(dev_index, args.seed + rank, 0, Wm, full=True)
+        ms = max_over_ranks(r["ms"], dist, torch.device("cuda", dev_index))
+        if rank == 0:
+            print(json.dumps({"metric": "multi-clip encode macroblocks/s (64 mixed-resolution clips, plain form)",
+                              "value": r["mbs"] * ws / (ms / 1000.0), "unit": "macroblocks/s", "n_gpus": ws,
+                              "steps": r["steps"], "warmup": Wm, "ms_per_step": ms / max(r["steps"], 1),
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                              "dtype": "u8/i16/i32 (f32 AQ, f64 RDO)", "data": "synthetic",
+                              "config": {"workload": r["what"], "parallelism": f"replicas x{ws}"}, "batch": r}))
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     frames = make_frames(K + Wm + 1, args.seed, rank)
     params = None
     if os.path.exists(args.weights):
@@ -597,6 +713,8 @@ def main():
         line["learned_streams_equal_value_vs_e2e"] = forms["learned"]["streams_equal"]
     if ws == 1 and not args.no_secondary:
         line["secondary"] = secondary_points(frames, dev_index, params, min(K, 20), min(Wm, 3), args.pipeline_depth)
+        if args.batch_steps > 0:
+            line["secondary"]["batch_64_clips"] = batch_point(dev_index, args.seed, args.batch_steps, 3)
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
