@@ -82,18 +82,35 @@ typedef struct {
     void* user;
 } riv_writer_vtable;
 
-/* A subset of EncodeFrameStats (enc/encoder.rs:58-124). */
+/* EncodeFrameStats (enc/encoder.rs:58-124), field for field except `rle_stats` (its sizes are
+ * resi_raw / resi_rans).  Option fields: -1 = None.  The fields marked (*) need the frame's
+ * per-MB search results and are filled only for the frame whose riv_encode_frame call passed
+ * a stats pointer (the others leave them 0); the rest are filled for every frame. */
 typedef struct {
     uint64_t frame_index, timestamp_ms;
     uint32_t frame_type; /* 1 = intra, 2 = inter (FrameType, com/format.rs:12-20) */
-    uint32_t total_bytes, mv_bytes, residual_bytes;
+    uint32_t total_bytes, mv_bytes, mv_raw_bytes, residual_bytes;
     uint32_t storage_width, storage_height;
-    uint32_t blocks_total, blocks_skipped, rdo_blocks_selected_skip;
+    uint32_t blocks_total, blocks_skipped;
+    uint32_t mv_zero_delta_blocks;
     uint32_t mv_mode_counts[7];
+    uint32_t mv_new_zero_pre_bias, mv_new_zero_post_bias, mv_new_zero_axes_x, mv_new_zero_axes_y;
     uint32_t mv_new_base_counts[5];
-    uint32_t mv_new_blocks;
+    uint32_t mv_new_best_ref_counts[5];      /* (*) */
+    uint64_t mv_new_best_ref_l1_saved_sum;   /* (*) */
+    uint32_t mv_new_blocks, mv_new_delta_count;
+    double mv_new_delta_mag_sum, mv_new_delta_mag_sq_sum;
+    uint64_t mv_class_histogram[11];
     int32_t mv_bias_dx, mv_bias_dy;
+    uint32_t mv_candidate_unique_total, mv_candidate_unique_samples; /* (*) */
+    uint32_t mv_candidate_unique_min, mv_candidate_unique_max;       /* (*) */
+    uint32_t mv_match_source_counts[6];                              /* (*) */
+    uint32_t mv_match_nonzero_blocks, mv_match_any_spatial, mv_match_any_temporal; /* (*) */
+    int64_t resi_raw, resi_rans;
     double rdo_lambda;
+    uint32_t rdo_blocks_evaluated, rdo_blocks_selected_skip;                    /* (*) */
+    uint32_t rdo_forced_fractional, rdo_forced_threshold, rdo_forced_disabled; /* (*) */
+    double rdo_avg_skip_cost, rdo_avg_coded_cost;                               /* (*) */
 } riv_frame_stats;
 
 typedef struct riv_encoder riv_encoder;

@@ -90,6 +90,8 @@ def lib():
         L.oracle_enc_last_qsteps.argtypes = [P, F32]
         L.oracle_enc_last_coeffs.argtypes = [P, I16]
         L.oracle_enc_last_bias.argtypes = [P, I8]
+        L.oracle_enc_last_stats.argtypes = [P, C.POINTER(C.c_double), C.c_size_t]
+        L.oracle_enc_last_stats.restype = C.c_size_t
         L.oracle_enc_last_record.restype = C.c_size_t
         L.oracle_enc_last_record.argtypes = [P, C.POINTER(U8)]
         L.oracle_dec_new.restype = P
@@ -172,6 +174,23 @@ class Frames:
         return (np.array_equal(self.y, o.y) and np.array_equal(self.u, o.u) and np.array_equal(self.v, o.v))
 
 
+# oracle_enc_last_stats's layout (riv_oracle.h): (field, width)
+STATS_FIELDS = (
+    ("frame_type", 1), ("total_bytes", 1), ("mv_bytes", 1), ("mv_raw_bytes", 1), ("residual_bytes", 1),
+    ("blocks_total", 1), ("blocks_skipped", 1), ("mv_zero_delta_blocks", 1), ("mv_mode_counts", 7),
+    ("mv_new_zero_pre_bias", 1), ("mv_new_zero_post_bias", 1), ("mv_new_zero_axes_x", 1), ("mv_new_zero_axes_y", 1),
+    ("mv_new_base_counts", 5), ("mv_new_best_ref_counts", 5), ("mv_new_best_ref_l1_saved_sum", 1),
+    ("mv_new_blocks", 1), ("mv_new_delta_count", 1), ("mv_new_delta_mag_sum", 1), ("mv_new_delta_mag_sq_sum", 1),
+    ("mv_class_histogram", 11), ("mv_bias_dx", 1), ("mv_bias_dy", 1), ("mv_candidate_unique_total", 1),
+    ("mv_candidate_unique_samples", 1), ("mv_candidate_unique_min", 1), ("mv_candidate_unique_max", 1),
+    ("mv_match_source_counts", 6), ("mv_match_nonzero_blocks", 1), ("mv_match_any_spatial", 1),
+    ("mv_match_any_temporal", 1), ("resi_raw", 1), ("resi_rans", 1), ("rdo_lambda", 1), ("rdo_blocks_evaluated", 1),
+    ("rdo_blocks_selected_skip", 1), ("rdo_forced_fractional", 1), ("rdo_forced_threshold", 1),
+    ("rdo_forced_disabled", 1), ("rdo_avg_skip_cost", 1), ("rdo_avg_coded_cost", 1),
+)
+STATS_N = sum(w for _, w in STATS_FIELDS)
+
+
 class OracleEncoder:
     """Oracle encoder: Encoder::new / encode_frame / finish over an in-memory writer."""
 
@@ -239,6 +258,22 @@ class OracleEncoder:
         b = np.zeros(2, np.int8)
         lib().oracle_enc_last_bias(self.h, i8(b))
         return int(b[0]), int(b[1])
+
+    def last_stats(self) -> dict:
+        """EncodeFrameStats of the last frame (enc/encoder.rs:58-124), arrays as tuples,
+        Options as None."""
+        v = np.zeros(STATS_N, np.float64)
+        got = lib().oracle_enc_last_stats(self.h, v.ctypes.data_as(C.POINTER(C.c_double)), STATS_N)
+        assert got == STATS_N, got
+        out, k = {}, 0
+        for name, width in STATS_FIELDS:
+            vals = v[k:k + width]
+            out[name] = tuple(vals.tolist()) if width > 1 else float(vals[0])
+            k += width
+        for name in ("resi_raw", "resi_rans"):
+            if out[name] < 0:
+                out[name] = None
+        return out
 
     def close(self):
         if self.h:

@@ -1356,6 +1356,117 @@ static Bytes header_bytes(const oracle_config& c, uint64_t frame_count) {  // :6
 // ----------------------------------------------------------------------------------
 // Encoder (enc/encoder.rs)
 // ----------------------------------------------------------------------------------
+// EncodeFrameStats of a P-frame (enc/encoder.rs:436-733 mode loop telemetry, :768-800 delta
+// statistics after the bias, :822 mv_raw_bytes, :873-884 zero deltas, :886-941 the rest), in
+// the order of oracle_enc_last_stats.  mvs: raw search MVs, coded: coded_prefix, prev: the
+// previous P-frame's coded MVs or nullptr, modes / bases / deltas: the mode decision's
+// outputs, opt: the optimized skip mask.
+static std::vector<double> inter_stats(int bw, int bh, const std::vector<MV>& mvs, const std::vector<MV>& coded,
+                                       const MV* prev, const std::vector<int64_t>& sads, const Lambda& L, bool allow,
+                                       double guard, const std::vector<uint8_t>& modes, const std::vector<uint8_t>& bases,
+                                       const std::vector<std::pair<int8_t, int8_t>>& raw_delta, int8_t biasx, int8_t biasy,
+                                       const std::vector<bool>& opt, size_t mv_bytes, size_t res_bytes, size_t total) {
+    const int n = bw * bh;
+    double mode_counts[7] = {0}, base_counts[5] = {0}, best_ref[5] = {0}, cls[11] = {0}, match[6] = {0};
+    double saved = 0, new_blocks = 0, zero_pre = 0, zero_post = 0, axes_x = 0, axes_y = 0, mag_sum = 0, mag_sq = 0;
+    double uniq_total = 0, uniq_samples = 0, uniq_min = 1e30, uniq_max = 0, nonzero = 0, any_sp = 0, any_tm = 0;
+    double evaluated = 0, chosen = 0, f_frac = 0, f_thr = 0, f_dis = 0, tot_skip = 0.0, tot_coded = 0.0;
+    double zero_delta = 0, skipped = 0;
+    for (int i = 0; i < n; i++) {
+        const MV& mv = mvs[i];
+        const int bx = i % bw, by = i / bw;
+        // RdoContext::decide + RdoTelemetry::record (enc/rdo.rs:140-178, :220-234)
+        double satd = (double)std::max<int64_t>(sads[i], 0);
+        double skip_cost = satd + L.lambda * L.skip_bits;
+        double est = L.icpt + L.slope * satd;
+        if (est < 0.0) est = 0.0;
+        double coded_cost = satd * L.retention + L.lambda * (L.keep_bits + est);
+        evaluated += 1;
+        if (!allow) f_dis += 1;
+        else if (mv.sx != 0 || mv.sy != 0) f_frac += 1;
+        else if (satd > guard) f_thr += 1;
+        else if (skip_cost <= coded_cost) chosen += 1;
+        tot_skip += skip_cost;
+        tot_coded += coded_cost;
+        // derive_mv_predictors_with_stats (res/mv_predictor.rs:135-163) on coded_prefix
+        std::vector<MV> before(coded.begin(), coded.begin() + i);
+        Neigh ng = gather_neighbors(before, prev, bw, bx, by);
+        std::vector<Tup> c;
+        auto add = [&](bool has, const Tup& t) {
+            if (!has) return;
+            for (auto& e : c)
+                if (e == t) return;
+            c.push_back(t);
+        };
+        add(ng.has_l, ng.l); add(ng.has_t, ng.t); add(ng.has_tr, ng.tr); add(ng.has_tl, ng.tl); add(ng.has_tm, ng.tm);
+        double u = c.empty() ? 1 : (double)c.size();
+        uniq_total += u; uniq_samples += 1;
+        uniq_min = std::min(uniq_min, u); uniq_max = std::max(uniq_max, u);
+        Preds P = derive_predictors(ng);
+        Tup act = tup(mv);
+        bool zero_el = mv.dx == 0 && mv.dy == 0 && mv.sx == 0 && mv.sy == 0;
+        if (!zero_el) {  // :483-515
+            nonzero += 1;
+            bool ml = ng.has_l && ng.l == act, mt = ng.has_t && ng.t == act, mtr = ng.has_tr && ng.tr == act,
+                 mtl = ng.has_tl && ng.tl == act, mtm = ng.has_tm && ng.tm == act;
+            if (ml || mt || mtr || mtl) any_sp += 1;
+            if (mtm) any_tm += 1;
+            match[ml ? 0 : mt ? 1 : mtr ? 2 : mtl ? 3 : mtm ? 4 : 5] += 1;
+        }
+        int mode = modes[i];
+        mode_counts[mode] += 1;
+        if (mode == NEW) {  // :567-660
+            int ax = mv.dx, ay = mv.dy;
+            auto l1 = [&](const Tup& b) { return (uint32_t)(std::abs(ax - b.dx) + std::abs(ay - b.dy)); };
+            uint32_t cn = l1(P.nearest), cr = l1(P.near);
+            bool has[5] = {true, true, ng.has_tr, ng.has_tl, true};
+            uint32_t cost[5] = {cn, cr, ng.has_tr ? l1(ng.tr) : 0u, ng.has_tl ? l1(ng.tl) : 0u, l1(P.temporal)};
+            int best = 0;
+            uint32_t bc = cn;
+            for (int k = 0; k < 5; k++)
+                if (has[k] && cost[k] < bc) { bc = cost[k]; best = k; }
+            best_ref[best] += 1;
+            uint32_t cur = std::min(cn, cr);
+            if (bc < cur) saved += (double)(cur - bc);
+            base_counts[bases[i]] += 1;
+            new_blocks += 1;
+            if (raw_delta[i].first == 0 && raw_delta[i].second == 0) zero_pre += 1;
+            // after the bias (:776-798)
+            int8_t dx = sat_i8(raw_delta[i].first - biasx), dy = sat_i8(raw_delta[i].second - biasy);
+            double fx = (double)dx, fy = (double)dy, mag = sqrt(fx * fx + fy * fy);
+            mag_sum += mag;
+            mag_sq += mag * mag;
+            cls[mv_class((unsigned)std::abs((int)dx))] += 1;
+            cls[mv_class((unsigned)std::abs((int)dy))] += 1;
+            if (dx == 0) axes_x += 1;
+            if (dy == 0) axes_y += 1;
+            if (dx == 0 && dy == 0) zero_post += 1;
+            if (raw_delta[i].first == 0 && raw_delta[i].second == 0) zero_delta += 1;  // :873-884
+        } else {
+            zero_delta += 1;
+        }
+        if (opt[i]) skipped += 1;
+    }
+    std::vector<double> o;
+    auto put = [&](double v) { o.push_back(v); };
+    put(2); put((double)total); put((double)mv_bytes); put((double)(n * 2 + new_blocks * 2)); put((double)res_bytes);
+    put(n); put(skipped); put(zero_delta);
+    for (double v : mode_counts) put(v);
+    put(zero_pre); put(zero_post); put(axes_x); put(axes_y);
+    for (double v : base_counts) put(v);
+    for (double v : best_ref) put(v);
+    put(saved); put(new_blocks); put(new_blocks); put(mag_sum); put(mag_sq);
+    for (double v : cls) put(v);
+    put(biasx); put(biasy);
+    put(uniq_total); put(uniq_samples); put(uniq_samples ? uniq_min : 0); put(uniq_max);
+    for (double v : match) put(v);
+    put(nonzero); put(any_sp); put(any_tm);
+    put((double)((n - skipped) * 384 * 2)); put((double)res_bytes);
+    put(L.lambda); put(evaluated); put(chosen); put(f_frac); put(f_thr); put(f_dis);
+    put(evaluated ? tot_skip / evaluated : 0.0); put(evaluated ? tot_coded / evaluated : 0.0);
+    return o;
+}
+
 struct Encoder {
     oracle_config cfg;
     Bytes out;
@@ -1375,6 +1486,7 @@ struct Encoder {
     std::vector<int16_t> coeffs;
     int8_t bias[2] = {0, 0};
     Bytes record;
+    std::vector<double> stats;  // EncodeFrameStats of the last frame, ORACLE_STATS_* order
 
     void write(const Bytes& b) {  // VecWriter semantics (enc/writer.rs:49-69)
         if (pos + b.size() > out.size()) out.resize(pos + b.size(), 0);
@@ -1598,6 +1710,13 @@ static int encode_frame_yuv(Encoder& E, Yuv& cur, uint64_t ts) {  // encoder.rs:
         E.prev_mvs.clear();
         E.mvc.reset();
         E.last_type = 1;
+        {  // EncodeFrameStats of a key frame (enc/encoder.rs:338-385): sizes only, Options None
+            const int n = (w / 16) * (h / 16);
+            const size_t total = data.size() + 14;
+            E.stats.assign(ORACLE_STATS_N, 0.0);
+            E.stats[0] = 1; E.stats[1] = (double)total; E.stats[4] = (double)data.size(); E.stats[5] = n;
+            E.stats[ORACLE_STATS_RESI_RAW] = -1; E.stats[ORACLE_STATS_RESI_RAW + 1] = -1;
+        }
         E.raw.assign(n, MV()); E.coded.assign(n, MV()); E.sads.assign(n, 0);
         E.side.assign((size_t)n * 8, 0);
         E.qs.assign(n, 0.0f);
@@ -1702,6 +1821,8 @@ static int encode_frame_yuv(Encoder& E, Yuv& cur, uint64_t ts) {  // encoder.rs:
             b.skip = opt[i];
         }
         Bytes mvdata = E.mvc.encode_frame(blocks, bw);
+        E.stats = inter_stats(bw, h / 16, mvs, coded, pm, sads, L, allow, guard, modes, bases, raw_delta, bx_, by_, opt,
+                              mvdata.size(), data.size(), 8 + 1 + 1 + 2 + 1 + 4 + mvdata.size() + 4 + data.size());
         std::vector<uint8_t> fmask(n);
         for (int i = 0; i < n; i++)
             fmask[i] = (!opt[i] || coded[i].dx != 0 || coded[i].dy != 0 || coded[i].sx != 0 || coded[i].sy != 0) ? 1 : 0;
@@ -2034,6 +2155,11 @@ void oracle_enc_last_qsteps(void* h, float* qs) {
 void oracle_enc_last_coeffs(void* h, int16_t* c) {
     Encoder& E = *(Encoder*)h;
     memcpy(c, E.coeffs.data(), E.coeffs.size() * sizeof(int16_t));
+}
+size_t oracle_enc_last_stats(void* h, double* out, size_t n) {
+    Encoder& E = *(Encoder*)h;
+    for (size_t i = 0; i < n && i < E.stats.size(); i++) out[i] = E.stats[i];
+    return E.stats.size();
 }
 void oracle_enc_last_bias(void* h, int8_t* b) {
     Encoder& E = *(Encoder*)h;

@@ -60,6 +60,18 @@ void oracle_enc_last_side(void* h, uint8_t* side);
 void oracle_enc_last_qsteps(void* h, float* qs);
 void oracle_enc_last_coeffs(void* h, int16_t* coeffs); /* 384 per MB: Y256,U64,V64 */
 void oracle_enc_last_bias(void* h, int8_t* bias2);
+/* EncodeFrameStats of the last frame as ORACLE_STATS_N doubles: frame_type, total_bytes,
+ * mv_bytes, mv_raw_bytes, residual_bytes, blocks_total, blocks_skipped, mv_zero_delta_blocks,
+ * mv_mode_counts[7], mv_new_zero_pre_bias, _post_bias, _axes_x, _axes_y, mv_new_base_counts[5],
+ * mv_new_best_ref_counts[5], mv_new_best_ref_l1_saved_sum, mv_new_blocks, mv_new_delta_count,
+ * mv_new_delta_mag_sum, _sq_sum, mv_class_histogram[11], mv_bias_dx, _dy,
+ * mv_candidate_unique_total, _samples, _min, _max, mv_match_source_counts[6],
+ * mv_match_nonzero_blocks, _any_spatial, _any_temporal, resi_raw, resi_rans (-1 = None),
+ * rdo_lambda, rdo_blocks_evaluated, rdo_blocks_selected_skip, rdo_forced_fractional,
+ * _threshold, _disabled, rdo_avg_skip_cost, rdo_avg_coded_cost.  Returns the count written. */
+#define ORACLE_STATS_N 70
+#define ORACLE_STATS_RESI_RAW 60
+size_t oracle_enc_last_stats(void* h, double* out, size_t n);
 size_t oracle_enc_last_record(void* h, const uint8_t** data);
 
 void* oracle_dec_new(const uint8_t* stream, size_t len, int* status);

@@ -12,6 +12,7 @@
 #include <dlfcn.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <condition_variable>
@@ -172,6 +173,13 @@ static Lambda lambda_for(uint8_t quality, double mult) {
     L.keep_bits = 1.20 + nq * 0.35;
     return L;
 }
+// mv_class_from_magnitude (res/mv_rans.rs:80-86): 0 for 0, else the bit length, at most 10.
+static int mv_class_of(int mag) {
+    if (mag == 0) return 0;
+    int b = 0;
+    while ((mag >> b) > 1) b++;
+    return std::min(b + 1, 10);
+}
 static int64_t f64_as_i64(double d) {
     if (std::isnan(d)) return 0;
     if (d <= -9223372036854775808.0) return INT64_MIN;
@@ -327,6 +335,10 @@ struct Job {
     // multi-clip step (riv_batch): one event marks the step's GPU work and copies done, in
     // place of the slot's ev_gpu / ev_recon / ev_d2h
     cudaEvent_t xev = nullptr;
+    // per-MB statistics requested for this frame: the coded MVs of the frame before (buffer
+    // prev_buf when prev_valid) and the frame's search output are read back in retire
+    bool want_stats = false, prev_valid = false;
+    int prev_buf = 0;
     int ck = 0;             // double-buffer parity of the frame's buffers
     uint32_t count = 0;
     std::future<void> fut, fut_mv;
@@ -989,6 +1001,93 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
 static double now_ms() {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
+// The per-MB statistics of a P-frame that need its search output (EncodeFrameStats,
+// enc/encoder.rs:436-733): RDO telemetry (RdoTelemetry, enc/rdo.rs:195-258), the number of
+// distinct predictor candidates (derive_mv_predictors_with_stats, res/mv_predictor.rs:135-163),
+// which raw neighbour a non-zero MV repeats (gather_mv_neighbor_set, :59-118) and the
+// L1-closest NEW base.  mb: the frame's search output in raster order (raw MV, coded MV, best
+// SAD); prev: the previous P-frame's coded MVs (4 bytes per MB) or nullptr.
+static void search_stats(const riv_encoder* e, const MbOut* mb, const int8_t* prev, riv_frame_stats& S) {
+    const riv_config& c = e->cfg;
+    const int bw = e->BW, n = e->NMB;
+    const Lambda& L = e->L;
+    const bool allow = c.skip_threshold > 0;
+    const double guard = 768.0 * (double)c.skip_threshold;
+    double tot_skip = 0.0, tot_coded = 0.0;
+    uint32_t umin = UINT32_MAX, umax = 0;
+    typedef std::array<int, 4> Tup;
+    auto coded = [&](int i) { return Tup{mb[i].coded[0], mb[i].coded[1], mb[i].coded[2], mb[i].coded[3]}; };
+    for (int i = 0; i < n; i++) {
+        const int bx = i % bw, by = i / bw;
+        const MbOut& m = mb[i];
+        // RdoContext::decide (enc/rdo.rs:140-178) as telemetry
+        const double satd = (double)std::max<int32_t>(m.best_sad, 0);
+        const double skip_cost = satd + L.lambda * L.skip_bits;
+        double est = L.icpt + L.slope * satd;
+        if (est < 0.0) est = 0.0;
+        const double coded_cost = satd * L.ret + L.lambda * (L.keep_bits + est);
+        const bool int_al = m.raw[2] == 0 && m.raw[3] == 0;
+        if (!allow) S.rdo_forced_disabled++;
+        else if (!int_al) S.rdo_forced_fractional++;
+        else if (satd > guard) S.rdo_forced_threshold++;
+        else if (skip_cost <= coded_cost) S.rdo_blocks_selected_skip++;
+        S.rdo_blocks_evaluated++;
+        tot_skip += skip_cost;
+        tot_coded += coded_cost;
+        // neighbours among the coded MVs of this frame and the previous one
+        bool hl = bx > 0, ht = by > 0, htr = by > 0 && bx + 1 < bw, htl = by > 0 && bx > 0, htm = prev != nullptr;
+        Tup l{}, t{}, tr{}, tl{}, tm{};
+        if (hl) l = coded(i - 1);
+        if (ht) t = coded(i - bw);
+        if (htr) tr = coded(i - bw + 1);
+        if (htl) tl = coded(i - bw - 1);
+        if (htm) tm = Tup{prev[4 * i], prev[4 * i + 1], prev[4 * i + 2], prev[4 * i + 3]};
+        Tup cand[5];
+        int nc = 0;
+        auto add = [&](bool has, const Tup& v) {
+            if (!has) return;
+            for (int k = 0; k < nc; k++)
+                if (cand[k] == v) return;
+            cand[nc++] = v;
+        };
+        add(hl, l); add(ht, t); add(htr, tr); add(htl, tl); add(htm, tm);
+        const uint32_t unique = nc == 0 ? 1u : (uint32_t)nc;
+        S.mv_candidate_unique_total += unique;
+        S.mv_candidate_unique_samples++;
+        umin = std::min(umin, unique);
+        umax = std::max(umax, unique);
+        const Tup zero{0, 0, 0, 0};
+        const Tup nearest = nc > 0 ? cand[0] : zero, near = nc > 1 ? cand[1] : zero, temporal = htm ? tm : zero;
+        const Tup actual{m.raw[0], m.raw[1], m.raw[2], m.raw[3]};
+        if (actual != zero) {  // attribution of exact matches to raw neighbours
+            S.mv_match_nonzero_blocks++;
+            const bool ml = hl && l == actual, mt = ht && t == actual, mtr = htr && tr == actual, mtl = htl && tl == actual,
+                       mtm = htm && tm == actual;
+            if (ml || mt || mtr || mtl) S.mv_match_any_spatial++;
+            if (mtm) S.mv_match_any_temporal++;
+            S.mv_match_source_counts[ml ? 0 : mt ? 1 : mtr ? 2 : mtl ? 3 : mtm ? 4 : 5]++;
+        }
+        if (m.mode == M_NEW) {  // the L1-closest integer base and what it would save over nearest/near
+            const int ax = m.raw[0], ay = m.raw[1];
+            auto l1 = [&](const Tup& b) { return (uint32_t)(std::abs(ax - b[0]) + std::abs(ay - b[1])); };
+            const uint32_t cn = l1(nearest), cr = l1(near);
+            const bool has[5] = {true, true, htr, htl, true};
+            const uint32_t cost[5] = {cn, cr, htr ? l1(tr) : 0u, htl ? l1(tl) : 0u, l1(temporal)};
+            int best = 0;
+            uint32_t bc = cn;
+            for (int k = 0; k < 5; k++)
+                if (has[k] && cost[k] < bc) { bc = cost[k]; best = k; }
+            S.mv_new_best_ref_counts[best]++;
+            const uint32_t cur = std::min(cn, cr);
+            if (bc < cur) S.mv_new_best_ref_l1_saved_sum += cur - bc;
+        }
+    }
+    S.mv_candidate_unique_min = umin == UINT32_MAX ? 0 : umin;
+    S.mv_candidate_unique_max = umax;
+    S.rdo_avg_skip_cost = S.rdo_blocks_evaluated ? tot_skip / (double)S.rdo_blocks_evaluated : 0.0;
+    S.rdo_avg_coded_cost = S.rdo_blocks_evaluated ? tot_coded / (double)S.rdo_blocks_evaluated : 0.0;
+}
+
 static riv_status retire(riv_encoder* e, Job& j) {
     Slot& s = e->slots[j.slot];
     double t0 = now_ms();
@@ -1044,8 +1143,18 @@ static riv_status retire(riv_encoder* e, Job& j) {
     Job* jp = &j;
     riv_encoder* ep = e;
     const uint32_t* side = s.side.as<uint32_t>();
+    std::shared_ptr<std::vector<MbOut>> mbh;
+    std::shared_ptr<std::vector<int8_t>> prevh;
+    if (j.type == 2 && j.want_stats) {  // the frame's search output (and the MVs it predicted from)
+        mbh = std::make_shared<std::vector<MbOut>>(N);
+        CK(cudaMemcpy(mbh->data(), e->mboutb[j.ck].p, (size_t)N * sizeof(MbOut), cudaMemcpyDeviceToHost));
+        if (j.prev_valid) {
+            prevh = std::make_shared<std::vector<int8_t>>((size_t)N * 4);
+            CK(cudaMemcpy(prevh->data(), e->coded[j.prev_buf].p, (size_t)N * 4, cudaMemcpyDeviceToHost));
+        }
+    }
     if (j.type == 2) {
-        j.fut_mv = e->mv_exec->submit([ep, jp, side, N] {
+        j.fut_mv = e->mv_exec->submit([ep, jp, side, N, mbh, prevh] {
             double m0 = now_ms();
             riv_frame_stats& S = jp->stats;
             std::vector<std::pair<int8_t, int8_t>> nd;
@@ -1064,16 +1173,36 @@ static riv_status retire(riv_encoder* e, Job& j) {
                 b.dx = b.dy = 0;
                 b.spx = b.spy = SP_ZERO;
                 if (b.mode == M_NEW) {
-                    b.dx = (int8_t)std::min(std::max((int)(int8_t)(v >> 8) - jp->bias[0], -128), 127);
-                    b.dy = (int8_t)std::min(std::max((int)(int8_t)(v >> 16) - jp->bias[1], -128), 127);
+                    const int rdx = (int8_t)(v >> 8), rdy = (int8_t)(v >> 16);
+                    b.dx = (int8_t)std::min(std::max(rdx - jp->bias[0], -128), 127);
+                    b.dy = (int8_t)std::min(std::max(rdy - jp->bias[1], -128), 127);
                     b.spx = ((v >> 6) & 1) ? SP_PLUS : SP_ZERO;
                     b.spy = ((v >> 7) & 1) ? SP_PLUS : SP_ZERO;
                     S.mv_new_blocks++;
                     S.mv_new_base_counts[std::min<int>(b.new_base, 4)]++;
+                    // delta statistics before and after the bias (enc/encoder.rs:768-800, 873-884)
+                    if (rdx == 0 && rdy == 0) {
+                        S.mv_new_zero_pre_bias++;
+                        S.mv_zero_delta_blocks++;
+                    }
+                    const double fx = (double)b.dx, fy = (double)b.dy, mag = std::sqrt(fx * fx + fy * fy);
+                    S.mv_new_delta_mag_sum += mag;
+                    S.mv_new_delta_mag_sq_sum += mag * mag;
+                    S.mv_class_histogram[mv_class_of(std::abs((int)b.dx))]++;
+                    S.mv_class_histogram[mv_class_of(std::abs((int)b.dy))]++;
+                    if (b.dx == 0) S.mv_new_zero_axes_x++;
+                    if (b.dy == 0) S.mv_new_zero_axes_y++;
+                    if (b.dx == 0 && b.dy == 0) S.mv_new_zero_post_bias++;
+                } else {
+                    S.mv_zero_delta_blocks++;
                 }
                 S.mv_mode_counts[b.mode]++;
                 if (b.skip) S.blocks_skipped++;
             }
+            S.mv_new_delta_count = S.mv_new_blocks;
+            S.mv_raw_bytes = (uint32_t)(2 * N + 2 * S.mv_new_blocks);
+            S.resi_raw = (int64_t)(N - (int)S.blocks_skipped) * 384 * 2;
+            if (mbh) search_stats(ep, mbh->data(), prevh ? prevh->data() : nullptr, S);
             ep->mvc.encode_frame(blocks, ep->BW, jp->mv_bytes, &ep->rans_submit);
             S.mv_bias_dx = jp->bias[0];
             S.mv_bias_dy = jp->bias[1];
@@ -1136,6 +1265,8 @@ static riv_status write_job(riv_encoder* e, Job& j) {
     j.stats.total_bytes = (uint32_t)rec.size();
     j.stats.mv_bytes = (uint32_t)j.mv_bytes.size();
     j.stats.residual_bytes = (uint32_t)j.res_bytes.size();
+    j.stats.resi_rans = j.type == 2 ? (int64_t)j.res_bytes.size() : -1;
+    if (j.type != 2) j.stats.resi_raw = -1;
     if (e->wr.write(e->wr.user, rec.data(), rec.size()) != 0) return fail(e, RIV_ERR_IO, "writer.write failed");
     e->host_ms[4] += now_ms() - w0;
     e->frame_count++;
@@ -1247,8 +1378,11 @@ static riv_status encode_common(riv_encoder* e, int src, const void* a, const vo
         j.type = intra ? 1 : 2;
         j.slot = (int)(n % cap);
         j.timed = e->cfg.pipeline_depth == 0 || stats != nullptr || n % TIMING_SAMPLE == 0;
+        j.want_stats = stats != nullptr;
         double s0 = now_ms();
         submit_gpu(e, j, src, a, b, c3);
+        j.prev_valid = e->has_prev2_mvs;  // the temporal predictors this P-frame used
+        j.prev_buf = e->coded_cur ^ 1;
         e->submitted++;
         e->host_ms[0] += now_ms() - s0;
         if (src == 0 || src == 2) CK(cudaEventSynchronize(e->slots[j.slot].ev_h2d));  // caller buffer reusable

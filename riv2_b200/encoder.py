@@ -95,11 +95,22 @@ class RivWriterVtable(C.Structure):
 class RivFrameStats(C.Structure):
     _fields_ = [
         ("frame_index", C.c_uint64), ("timestamp_ms", C.c_uint64), ("frame_type", C.c_uint32),
-        ("total_bytes", C.c_uint32), ("mv_bytes", C.c_uint32), ("residual_bytes", C.c_uint32),
-        ("storage_width", C.c_uint32), ("storage_height", C.c_uint32), ("blocks_total", C.c_uint32),
-        ("blocks_skipped", C.c_uint32), ("rdo_blocks_selected_skip", C.c_uint32),
-        ("mv_mode_counts", C.c_uint32 * 7), ("mv_new_base_counts", C.c_uint32 * 5), ("mv_new_blocks", C.c_uint32),
-        ("mv_bias_dx", C.c_int32), ("mv_bias_dy", C.c_int32), ("rdo_lambda", C.c_double),
+        ("total_bytes", C.c_uint32), ("mv_bytes", C.c_uint32), ("mv_raw_bytes", C.c_uint32),
+        ("residual_bytes", C.c_uint32), ("storage_width", C.c_uint32), ("storage_height", C.c_uint32),
+        ("blocks_total", C.c_uint32), ("blocks_skipped", C.c_uint32), ("mv_zero_delta_blocks", C.c_uint32),
+        ("mv_mode_counts", C.c_uint32 * 7), ("mv_new_zero_pre_bias", C.c_uint32), ("mv_new_zero_post_bias", C.c_uint32),
+        ("mv_new_zero_axes_x", C.c_uint32), ("mv_new_zero_axes_y", C.c_uint32), ("mv_new_base_counts", C.c_uint32 * 5),
+        ("mv_new_best_ref_counts", C.c_uint32 * 5), ("mv_new_best_ref_l1_saved_sum", C.c_uint64),
+        ("mv_new_blocks", C.c_uint32), ("mv_new_delta_count", C.c_uint32), ("mv_new_delta_mag_sum", C.c_double),
+        ("mv_new_delta_mag_sq_sum", C.c_double), ("mv_class_histogram", C.c_uint64 * 11),
+        ("mv_bias_dx", C.c_int32), ("mv_bias_dy", C.c_int32), ("mv_candidate_unique_total", C.c_uint32),
+        ("mv_candidate_unique_samples", C.c_uint32), ("mv_candidate_unique_min", C.c_uint32),
+        ("mv_candidate_unique_max", C.c_uint32), ("mv_match_source_counts", C.c_uint32 * 6),
+        ("mv_match_nonzero_blocks", C.c_uint32), ("mv_match_any_spatial", C.c_uint32),
+        ("mv_match_any_temporal", C.c_uint32), ("resi_raw", C.c_int64), ("resi_rans", C.c_int64),
+        ("rdo_lambda", C.c_double), ("rdo_blocks_evaluated", C.c_uint32), ("rdo_blocks_selected_skip", C.c_uint32),
+        ("rdo_forced_fractional", C.c_uint32), ("rdo_forced_threshold", C.c_uint32),
+        ("rdo_forced_disabled", C.c_uint32), ("rdo_avg_skip_cost", C.c_double), ("rdo_avg_coded_cost", C.c_double),
     ]
 
 
@@ -389,29 +400,65 @@ class _PyWriterBridge:
 
 @dataclasses.dataclass
 class EncodeFrameStats:
+    """EncodeFrameStats (enc/encoder.rs:58-124): every field of the reference except
+    ``rle_stats``, whose sizes are ``resi_raw`` / ``resi_rans`` (None when absent)."""
     frame_index: int
     timestamp_ms: int
     frame_type: int
     total_bytes: int
     mv_bytes: int
+    mv_raw_bytes: int
     residual_bytes: int
     storage_width: int
     storage_height: int
     blocks_total: int
     blocks_skipped: int
+    mv_zero_delta_blocks: int
     mv_mode_counts: tuple
+    mv_new_zero_pre_bias: int
+    mv_new_zero_post_bias: int
+    mv_new_zero_axes_x: int
+    mv_new_zero_axes_y: int
     mv_new_base_counts: tuple
+    mv_new_best_ref_counts: tuple
+    mv_new_best_ref_l1_saved_sum: int
     mv_new_blocks: int
+    mv_new_delta_count: int
+    mv_new_delta_mag_sum: float
+    mv_new_delta_mag_sq_sum: float
+    mv_class_histogram: tuple
     mv_bias_dx: int
     mv_bias_dy: int
+    mv_candidate_unique_total: int
+    mv_candidate_unique_samples: int
+    mv_candidate_unique_min: int
+    mv_candidate_unique_max: int
+    mv_match_source_counts: tuple
+    mv_match_nonzero_blocks: int
+    mv_match_any_spatial: int
+    mv_match_any_temporal: int
+    resi_raw: Optional[int]
+    resi_rans: Optional[int]
     rdo_lambda: float
+    rdo_blocks_evaluated: int
+    rdo_blocks_selected_skip: int
+    rdo_forced_fractional: int
+    rdo_forced_threshold: int
+    rdo_forced_disabled: int
+    rdo_avg_skip_cost: float
+    rdo_avg_coded_cost: float
 
     @staticmethod
     def from_c(s: RivFrameStats) -> "EncodeFrameStats":
-        return EncodeFrameStats(s.frame_index, s.timestamp_ms, s.frame_type, s.total_bytes, s.mv_bytes,
-                                s.residual_bytes, s.storage_width, s.storage_height, s.blocks_total, s.blocks_skipped,
-                                tuple(s.mv_mode_counts), tuple(s.mv_new_base_counts), s.mv_new_blocks, s.mv_bias_dx,
-                                s.mv_bias_dy, s.rdo_lambda)
+        kw = {}
+        for f in dataclasses.fields(EncodeFrameStats):
+            v = getattr(s, f.name)
+            if isinstance(v, C.Array):
+                v = tuple(v)
+            if f.name in ("resi_raw", "resi_rans") and v < 0:
+                v = None
+            kw[f.name] = v
+        return EncodeFrameStats(**kw)
 
 
 class Encoder:

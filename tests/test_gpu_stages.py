@@ -95,8 +95,8 @@ CASES = [
     ("noise", "noise", 80, 1.0, 0.75),
     ("steps", "flat", 100, 1.0, 0.75),
     ("steps", "noise", 1, 1.0, 0.75),
-    ("noise", "flat", 100, 0.05, 0.75),   # tiny steps: quantised values saturate at +-32767
-    ("steps", "flat", 100, 0.01, 0.0),    # no dead zone, saturation
+    ("noise", "flat", 100, 0.002, 0.75),  # tiny steps: quantised values saturate at +-32767
+    ("steps", "flat", 100, 0.002, 0.0),   # no dead zone, saturation
     ("noise", "noise", 1, 400.0, 0.75),   # huge steps: every MB quantises to zero (optimized skip)
     ("noise", "steps", 95, 1.0, 0.0),
 ]
@@ -122,7 +122,7 @@ def test_residual_matches_oracle(cur_kind, pred_kind, q, scale, dz):
     assert np.array_equal(rec, wrec), f"{(rec != wrec).sum()} reconstructed samples differ"
     # the deblock mask of enc/encoder.rs:831-841: coded, or a non-zero MV
     assert np.array_equal(fm, ((1 - osk) | (coded != 0).any(axis=1)).astype(np.uint8))
-    if scale <= 0.05:
+    if scale <= 0.002:
         assert (np.abs(co.astype(np.int32)) >= 32767).any(), "expected saturated coefficients"
     if scale >= 400:
         assert osk.all()
