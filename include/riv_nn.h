@@ -38,6 +38,13 @@ int riv_nn_conv(int layer, const void* in, int in_mb, const void* W, const float
  * P-frame's coded MVs (4 x i8 per MB, NULL when there is none). */
 int riv_nn_features(const uint8_t* cur_y, const uint8_t* ref_y, int W, int H, const int8_t* prev_coded, int mb0,
                     int nmb, void* feat, void* x1, void* stream);
+/* Inference front end: the network input of riv_nn_features kept on chip and conv1 (+ bias b1,
+ * ReLU) applied to it at once: a1 = nmb x 144 x 32 bf16 (conv1's output, 16-byte aligned), x1's
+ * predictor columns as riv_nn_features writes them; w1 = conv1's [32][32] bf16 weights.  The
+ * same function as riv_nn_features followed by riv_nn_conv(1, ...) up to the order of the f32
+ * accumulation. */
+int riv_nn_front(const uint8_t* cur_y, const uint8_t* ref_y, int W, int H, const int8_t* prev_coded, int mb0, int nmb,
+                 const void* w1, const float* b1, void* a1, void* x1, void* stream);
 /* Training: im2col^T of layer `layer`'s input (K x nmb*positions bf16). */
 int riv_nn_im2col_t(int layer, const void* in, int in_mb, int nmb, void* out, void* stream);
 /* Training: col2im of layer `layer`'s input gradient (f32 [positions][320]) times the ReLU

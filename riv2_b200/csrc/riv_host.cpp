@@ -420,7 +420,7 @@ struct riv_encoder {
     // learned / parallel forms: the proposal network's parameters (bf16 weights, f32 biases),
     // its activations, the per-MB search result and the fallback / shortcut counters
     bool learned = false, nn_loaded = false;
-    DevBuf nn_w, nn_b, nn_feat, nn_a1, nn_a2, nn_a3, nn_x1, nn_h1, nn_h2, nn_o[2], lmv, lcount;
+    DevBuf nn_w, nn_b, nn_feat, nn_a1, nn_a2, nn_a3, nn_x1, nn_h1, nn_h2, nn_o[2], lmv, lcount, lrowcnt;
     uint64_t learned_mbs = 0;
     // The network of P-frame t runs on its own stream N while frame t-1 is still searched,
     // reconstructed and deblocked: its inputs are the converted input planes of frames t and
@@ -583,6 +583,8 @@ static void setup_device(riv_encoder* e) {
         e->lmv.alloc((size_t)N * 8);
         e->lcount.alloc(2 * sizeof(unsigned));
         e->lcount.zero(e->S);
+        e->lrowcnt.alloc((size_t)e->BH * sizeof(unsigned));
+        e->lrowcnt.zero(e->S);
     }
     if (c.encode_form == RIV_FORM_LEARNED) {
         e->nn_w.alloc(nn::ParamLayout::nweights * 2);
@@ -742,8 +744,9 @@ static void proposal_forward(riv_encoder* e, const uint8_t* cur_y, const uint8_t
     const float* B = e->nn_b.as<float>();
     unsigned* err = e->status.as<unsigned>();
     void *feat = e->nn_feat.p, *a1 = e->nn_a1.p, *a2 = e->nn_a2.p, *a3 = e->nn_a3.p, *x1 = e->nn_x1.p;
-    CK((cudaError_t)riv_nn_features(cur_y, ref_y, e->W, e->H, prev_coded, 0, N, feat, x1, S));
-    CK((cudaError_t)nn_conv(1, feat, nn::FEAT * nn::FEAT * 2, W + PL::w1, B, a1, 144 * 32, 32, N, err, S));
+    // network input and conv1 in one kernel (the input stays on chip), then conv2..4 and fc1..3
+    (void)feat;
+    CK((cudaError_t)riv_nn_front(cur_y, ref_y, e->W, e->H, prev_coded, 0, N, W + PL::w1, B, a1, x1, S));
     CK((cudaError_t)nn_conv(2, a1, 144 * 32, W + PL::w2, B + 32, a2, 36 * 32, 32, N, err, S));
     CK((cudaError_t)nn_conv(3, a2, 36 * 32, W + PL::w3, B + 64, a3, 36 * 32, 32, N, err, S));
     CK((cudaError_t)nn_conv(4, a3, 36 * 32, W + PL::w4, B + 96, x1, nn::F1, 32, N, err, S));
@@ -935,7 +938,8 @@ static void submit_gpu(riv_encoder* e, Job& j, int src, const void* a, const voi
         CK(cudaStreamWaitEvent(S, e->ev_mbout_free[ck], 0));  // compaction of the frame NPAR back
         if (e->learned) {
             CK((cudaError_t)launch_learned(sp, c.encode_form == RIV_FORM_LEARNED ? e->nn_o[nbuf].as<float>() : nullptr,
-                                           (int)c.proposal_margin, 2.2f, e->lmv.p, e->lcount.as<unsigned>(), S));
+                                           (int)c.proposal_margin, 2.2f, e->lmv.p, e->lcount.as<unsigned>(),
+                                           e->lrowcnt.as<unsigned>(), S));
             CK(cudaEventRecord(e->ev_net_read[nbuf], S));
             e->nn_frames++;
             e->learned_mbs += (uint64_t)N;
@@ -1595,7 +1599,7 @@ void riv_encoder_free(riv_encoder* e) {
                       &e->varsum, &e->qs, &e->status,
                       &e->mvbits, &e->logfix, &e->expfix, &e->ytab, &e->ctab, &e->cindex, &e->coffset, &e->lcindex, &e->lcoffset, &e->sadtab, &e->prof, &e->tflag, &e->rowdone, &e->newcost, &e->newcost32,
                       &e->nn_w, &e->nn_b, &e->nn_feat, &e->nn_a1, &e->nn_a2, &e->nn_a3, &e->nn_x1, &e->nn_h1, &e->nn_h2,
-                      &e->nn_o[0], &e->nn_o[1], &e->lmv, &e->lcount};
+                      &e->nn_o[0], &e->nn_o[1], &e->lmv, &e->lcount, &e->lrowcnt};
     for (DevBuf* b : bufs) b->release();
     if (e->N) cudaStreamSynchronize(e->N);
     for (int k = 0; k < 2; k++) {

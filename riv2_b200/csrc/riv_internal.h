@@ -219,8 +219,9 @@ int launch_compact(const uint8_t* opt_skip, const MbOut* mb, const int16_t* coef
 int launch_libm_eval(int which, const float* in, float* out, size_t n, const uint32_t* fix, int nfix, void* stream);
 // Learned-proposal form of the P-frame search and mode decision (riv_kernels.cu): lmv holds 8
 // bytes per MB; counters[0] += fallbacks to the hexagon search, counters[1] += shortcuts.
+// rowcnt (BH words, zero; nullable): the ln-variance mean is folded inside the search launch.
 int launch_learned(const SearchParams& sp, const float* net, int margin, float skip_logit, void* lmv,
-                   unsigned* counters, void* stream);
+                   unsigned* counters, unsigned* rowcnt, void* stream);
 int launch_libm_range(int which, uint32_t lo, uint32_t n, float* out, const uint32_t* fix, int nfix, void* stream);
 int launch_wait_expiry(int which, const unsigned long long* rec, const unsigned* counter, long long limit,
                        unsigned* status, void* stream);

@@ -2633,7 +2633,49 @@ struct LearnedParams {
     float skip_logit;  // shortcut when the skip logit exceeds this (a probability threshold, as a logit)
     LearnedMv* out;
     unsigned* counters;  // [0] fallbacks to the hexagon search, [1] shortcuts
+    // per MB row: MBs whose ln variance is written (zero between frames); non-null: the
+    // launch's extra fold CTA sums the ln variances in raster order while the rows finish
+    unsigned* rowcnt;
 };
+
+// The strictly sequential f32 sum of the ln variances (Iterator::sum, res/residual.rs:154-167)
+// and their mean at lnv[n], by one warp of the launch's first CTA while the search CTAs run:
+// row r is folded once all its MBs have published (release: fence + count; acquire: the
+// count's load), lane 0 adding the values left to right.  Each row's count goes back to zero
+// for the next frame.  A wait past the spin limit sets ST_WAIT_TIMEOUT and ends the fold.
+__device__ __forceinline__ void learned_fold(const LearnedParams& lp) {
+    __shared__ float fb[256];
+    const SearchParams& p = lp.sp;
+    const int lane = threadIdx.x & 31;
+    float sum = 0.0f;
+    bool failed = false;
+    for (int r = 0; r < p.BH && !failed; r++) {
+        if (lane == 0) {
+            long long spins = 0;
+            while (ld_acquire_u32(lp.rowcnt + r) < (unsigned)p.BW) {
+                if (++spins > p.spin_limit) {
+                    atomicOr(p.status, ST_WAIT_TIMEOUT);
+                    failed = true;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        failed = __shfl_sync(0xffffffffu, (int)failed, 0) != 0;
+        if (failed) break;
+        __syncwarp();
+        for (int b0 = 0; b0 < p.BW; b0 += 256) {
+            const int m = min(256, p.BW - b0);
+            for (int i = lane; i < m; i += 32) fb[i] = __ldcg(p.lnv + (size_t)r * p.BW + b0 + i);
+            __syncwarp();
+            if (lane == 0)
+                for (int i = 0; i < m; i++) sum = __fadd_rn(sum, fb[i]);
+            __syncwarp();
+        }
+        if (lane == 0) lp.rowcnt[r] = 0u;
+    }
+    if (lane == 0 && !failed) p.lnv[p.BW * p.BH] = __fdiv_rn(sum, (float)(p.BW * p.BH));
+}
 
 // SAD of the 16x16 block at whole-pixel offset (dx, dy) over the window; lane l covers row l/2,
 // eight pixels, current samples in c0, c1.
@@ -2666,8 +2708,16 @@ __device__ __forceinline__ unsigned ls_sad_hp(const uint8_t* win, int ws, int ox
 __global__ void __launch_bounds__(32 * LS_MBS) k_learned_search(LearnedParams lp) {
     const SearchParams& p = lp.sp;
     extern __shared__ __align__(16) uint8_t lsm[];
+    // with the fold: grid row 0 is the fold CTA (x = 0; the rest of that row returns), MB row r
+    // is grid row r + 1.  The fold CTA comes first and waits only for search CTAs, which never
+    // wait, so every CTA finishes.
+    const int yoff = lp.rowcnt != nullptr ? 1 : 0;
+    if ((int)blockIdx.y < yoff) {
+        if (blockIdx.x == 0 && threadIdx.x < 32) learned_fold(lp);
+        return;
+    }
     const int sr = p.sr, M = sr + 2;
-    const int bx0 = blockIdx.x * LS_MBS, by = blockIdx.y;
+    const int bx0 = blockIdx.x * LS_MBS, by = (int)blockIdx.y - yoff;
     const int nmb_here = min(LS_MBS, p.BW - bx0);
     const int wx0 = (bx0 * 16 - M) & ~3, wy0 = by * 16 - M;  // left edge on a 4-byte boundary
     const int ws = ls_window_width(sr), wh = 16 + 2 * M + 1;
@@ -2842,6 +2892,10 @@ __global__ void __launch_bounds__(32 * LS_MBS) k_learned_search(LearnedParams lp
             float var = __fdiv_rn(__ull2float_rn(NN), 65536.0f);
             var = var < 4.0f ? 4.0f : var;
             p.lnv[mb] = glibc_logf(var, p.logfix, p.nlog);
+            if (lp.rowcnt != nullptr) {  // publish for the fold CTA
+                __threadfence();
+                atomicAdd(lp.rowcnt + by, 1u);
+            }
         }
     }
     if (lane == 0) {
@@ -2899,7 +2953,7 @@ __global__ void __launch_bounds__(128) k_learned_mode(SearchParams p, const Lear
 __global__ void __launch_bounds__(1024) k_aq_sum(const float* __restrict__ lnv, int n, float* avg_out);
 
 int launch_learned(const SearchParams& sp, const float* net, int margin, float skip_logit, void* lmv,
-                   unsigned* counters, void* stream) {
+                   unsigned* counters, unsigned* rowcnt, void* stream) {
     LearnedParams lp{};
     lp.sp = sp;
     lp.net = net;
@@ -2907,17 +2961,18 @@ int launch_learned(const SearchParams& sp, const float* net, int margin, float s
     lp.skip_logit = skip_logit;
     lp.out = (LearnedMv*)lmv;
     lp.counters = counters;
+    lp.rowcnt = sp.lnv != nullptr ? rowcnt : nullptr;
     const int M = sp.sr + 2;
     const int ws = ls_window_width(sp.sr), wh = 16 + 2 * M + 1;
     const size_t smem = (size_t)ws * wh + 16;
-    dim3 grid((sp.BW + LS_MBS - 1) / LS_MBS, sp.BH);
+    dim3 grid((sp.BW + LS_MBS - 1) / LS_MBS, sp.BH + (lp.rowcnt != nullptr ? 1 : 0));
     k_learned_search<<<grid, 32 * LS_MBS, smem, (cudaStream_t)stream>>>(lp);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return (int)e;
     const int n = sp.BW * sp.BH;
     k_learned_mode<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(sp, (const LearnedMv*)lmv);
     e = cudaGetLastError();
-    if (e != cudaSuccess || sp.lnv == nullptr) return (int)e;
+    if (e != cudaSuccess || sp.lnv == nullptr || lp.rowcnt != nullptr) return (int)e;
     // the strictly sequential f32 mean of the ln variances (Iterator::sum), at lnv[n]
     k_aq_sum<<<1, 1024, 8192 * sizeof(float), (cudaStream_t)stream>>>(sp.lnv, n, sp.lnv + n);
     return (int)cudaGetLastError();

@@ -569,10 +569,33 @@ __device__ __forceinline__ int med3(int a, int b, int c) { return max(min(a, b),
 constexpr int PF_MBS = 4;               // MBs of a row per CTA
 constexpr int PF_WW = 16 * PF_MBS + 48;  // window width shared by them (full resolution)
 
-__global__ void __launch_bounds__(256) k_prop_features(const uint8_t* __restrict__ cur, const uint8_t* __restrict__ ref,
-                                                       int W, int H, const int8_t* __restrict__ prev_coded, int mb0,
-                                                       int nmb, __nv_bfloat16* __restrict__ feat,
-                                                       __nv_bfloat16* __restrict__ x1) {
+// bf16 tensor-core product of one 16x16 A fragment and one 16x8 B fragment, f32 accumulate
+// (mma.sync m16n8k16; register layouts of the PTX ISA).
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// FRONT = false: the network input to global memory (feat, x1).  FRONT = true: the input stays
+// in shared memory and conv1 (+ bias, ReLU) runs on it at once, writing its output a1
+// (nmb x 144 positions x 32 channels bf16) and x1's predictor columns: the 24x24x2 input never
+// goes to global memory.  conv1's reduction is 9 taps x 2 channels (k = 2 tap + channel, zero
+// from k = 18), too small for a tcgen05 tile of its own, so each warp runs it with mma.sync on
+// 16 output positions at a time: A rows = positions, the fragment's k pairs = one tap's two
+// channels (one 32-bit word of the shared input), B = W1 (32 x 32, bf16), f32 accumulation.
+template <bool FRONT>
+__global__ void __launch_bounds__(256) k_prop_input(const uint8_t* __restrict__ cur, const uint8_t* __restrict__ ref,
+                                                    int W, int H, const int8_t* __restrict__ prev_coded, int mb0,
+                                                    int nmb, __nv_bfloat16* __restrict__ feat,
+                                                    __nv_bfloat16* __restrict__ x1,
+                                                    const __nv_bfloat16* __restrict__ w1, const float* __restrict__ b1,
+                                                    __nv_bfloat16* __restrict__ a1) {
+    constexpr int NF = nn::FEAT * nn::FEAT;
+    __shared__ __align__(16) uint32_t F[FRONT ? PF_MBS * NF : 1];      // the input, one word per pixel
+    __shared__ __align__(16) uint32_t O[FRONT ? 8 * 16 * 16 : 1];      // per warp: 16 output rows of 64 bytes
     __shared__ __align__(16) uint32_t win[64][PF_WW / 4];   // reference window, 4 MBs wide
     __shared__ __align__(16) uint32_t R[32][PF_WW / 8 + 1];  // its 2x2 averages (+ a word of slack)
     __shared__ __align__(16) uint32_t Cb[PF_MBS][8][2];     // the current blocks' 2x2 averages
@@ -669,7 +692,8 @@ __global__ void __launch_bounds__(256) k_prop_features(const uint8_t* __restrict
 #pragma unroll
         for (int q = 0; q < nn::NPRED; q++)
             if (pu[m][q] == u && pv[m][q] == v) f1 = 1.0f;
-        *(uint32_t*)(feat + (size_t)(mb - mb0) * (nn::FEAT * nn::FEAT * 2) + 2 * kk) = pack_bf16(f0, f1);
+        if (FRONT) F[m * NF + kk] = pack_bf16(f0, f1);
+        else *(uint32_t*)(feat + (size_t)(mb - mb0) * (nn::FEAT * nn::FEAT * 2) + 2 * kk) = pack_bf16(f0, f1);
     }
     if (t < 16 * nhere) {
         const int m = t >> 4, q = t & 15, mb = first + m;
@@ -677,6 +701,59 @@ __global__ void __launch_bounds__(256) k_prop_features(const uint8_t* __restrict
             const float v = q < 2 * nn::NPRED ? (float)ph[m][q] * (1.0f / 64.0f) : 0.0f;
             x1[(size_t)(mb - mb0) * nn::F1 + 288 + q] = __float2bfloat16_rn(v);
             x1[(size_t)(mb - mb0) * nn::F1 + 304 + q] = __float2bfloat16_rn(0.0f);
+        }
+    }
+    if constexpr (FRONT) {
+        __syncthreads();
+        const int warp = t >> 5, lane = t & 31, g = lane >> 2, tig = lane & 3;
+        // B fragments of W1 ([32 out][32 k]): k-step s, n-tile nt: (k = 16 s + 2 tig (+8), n = 8 nt + g)
+        uint32_t bw[2][4][2];
+#pragma unroll
+        for (int ks = 0; ks < 2; ks++)
+#pragma unroll
+            for (int nt = 0; nt < 4; nt++) {
+                const __nv_bfloat16* wr = w1 + (size_t)(8 * nt + g) * nn::K1 + 16 * ks + 2 * tig;
+                bw[ks][nt][0] = __ldg((const unsigned int*)wr);
+                bw[ks][nt][1] = __ldg((const unsigned int*)(wr + 8));
+            }
+        float bias[4][2];
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++) {
+            bias[nt][0] = __ldg(b1 + 8 * nt + 2 * tig);
+            bias[nt][1] = __ldg(b1 + 8 * nt + 2 * tig + 1);
+        }
+        uint32_t* ob = O + warp * 256;
+        // 9 tiles of 16 positions per MB; warp w takes tiles w, w + 8, ...
+        for (int tile = warp; tile < nhere * 9; tile += 8) {
+            const int m = tile / 9, p0 = (tile % 9) * 16, mb = first + m;
+            if (mb < mb0 || mb >= mb0 + nmb) continue;  // warp-uniform
+            const uint32_t* fm = F + m * NF;
+            // the input word of position p (row of A) at tap: zero outside the 24x24 input
+            auto px = [&](int p, int tap) -> uint32_t {
+                const int oy = p / 12, ox = p % 12;
+                const int y = 2 * oy + tap / 3 - 1, x = 2 * ox + tap % 3 - 1;
+                return (y >= 0 && y < nn::FEAT && x >= 0 && x < nn::FEAT) ? fm[y * nn::FEAT + x] : 0u;
+            };
+            const int r0 = p0 + g, r1 = p0 + g + 8;
+            const uint32_t a0[4] = {px(r0, tig), px(r1, tig), px(r0, tig + 4), px(r1, tig + 4)};
+            const uint32_t a1f[4] = {tig == 0 ? px(r0, 8) : 0u, tig == 0 ? px(r1, 8) : 0u, 0u, 0u};
+#pragma unroll
+            for (int nt = 0; nt < 4; nt++) {
+                float d[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                mma_bf16_16816(d, a0, bw[0][nt][0], bw[0][nt][1]);
+                mma_bf16_16816(d, a1f, bw[1][nt][0], bw[1][nt][1]);
+                // rows g and g + 8, channels 8 nt + 2 tig (+1): one 32-bit word each
+                ob[g * 16 + 4 * nt + tig] = pack_bf16(fmaxf(d[0] + bias[nt][0], 0.0f), fmaxf(d[1] + bias[nt][1], 0.0f));
+                ob[(g + 8) * 16 + 4 * nt + tig] =
+                    pack_bf16(fmaxf(d[2] + bias[nt][0], 0.0f), fmaxf(d[3] + bias[nt][1], 0.0f));
+            }
+            __syncwarp();
+            // the tile's 16 rows are 1 KB contiguous in a1: two 16-byte stores per lane
+            uint4* dst = (uint4*)(a1 + ((size_t)(mb - mb0) * 144 + p0) * 32);
+            const uint4* src = (const uint4*)ob;
+            dst[lane] = src[lane];
+            dst[lane + 32] = src[lane + 32];
+            __syncwarp();
         }
     }
 }
@@ -869,8 +946,21 @@ int riv_nn_features(const uint8_t* cur_y, const uint8_t* ref_y, int W, int H, co
         return (int)cudaErrorInvalidValue;
     // CTAs over groups of PF_MBS MBs of a row; those outside mb0 .. mb0+nmb-1 return at once
     const int BW = W / 16, groups = (BW + PF_MBS - 1) / PF_MBS * (H / 16);
-    k_prop_features<<<groups, 256, 0, (cudaStream_t)stream>>>(cur_y, ref_y, W, H, prev_coded, mb0, nmb,
-                                                              (__nv_bfloat16*)feat, (__nv_bfloat16*)x1);
+    k_prop_input<false><<<groups, 256, 0, (cudaStream_t)stream>>>(cur_y, ref_y, W, H, prev_coded, mb0, nmb,
+                                                                  (__nv_bfloat16*)feat, (__nv_bfloat16*)x1, nullptr,
+                                                                  nullptr, nullptr);
+    return (int)cudaGetLastError();
+}
+
+int riv_nn_front(const uint8_t* cur_y, const uint8_t* ref_y, int W, int H, const int8_t* prev_coded, int mb0, int nmb,
+                 const void* w1, const float* b1, void* a1, void* x1, void* stream) {
+    if (W <= 0 || H <= 0 || W % 16 || H % 16 || nmb <= 0 || mb0 < 0 || mb0 + nmb > (W / 16) * (H / 16) ||
+        ((uintptr_t)a1 & 15) || ((uintptr_t)w1 & 3))
+        return (int)cudaErrorInvalidValue;
+    const int BW = W / 16, groups = (BW + PF_MBS - 1) / PF_MBS * (H / 16);
+    k_prop_input<true><<<groups, 256, 0, (cudaStream_t)stream>>>(cur_y, ref_y, W, H, prev_coded, mb0, nmb, nullptr,
+                                                                 (__nv_bfloat16*)x1, (const __nv_bfloat16*)w1, b1,
+                                                                 (__nv_bfloat16*)a1);
     return (int)cudaGetLastError();
 }
 

@@ -34,7 +34,8 @@ NB = sum(n for _, n in BIASES)
 MAGIC = b"RIVPROP1"
 # Every symbol include/riv_nn.h declares (checked by the CPU test suite).
 EXPORTED_SYMBOLS = ("riv_nn_gemm", "riv_nn_conv", "riv_nn_features", "riv_nn_im2col_t", "riv_nn_col2im",
-                    "riv_nn_relu_bwd", "riv_nn_transpose", "riv_nn_colsum", "riv_nn_head_loss", "riv_nn_adamw")
+                    "riv_nn_relu_bwd", "riv_nn_transpose", "riv_nn_colsum", "riv_nn_head_loss", "riv_nn_adamw",
+                    "riv_nn_front")
 
 
 def weight_offsets():
@@ -97,6 +98,7 @@ def lib():
         L.riv_nn_gemm.argtypes = [P, I, P, I, P, I, P, I, I, I, I, I, I, I, I, P, P]
         L.riv_nn_conv.argtypes = [I, P, I, P, P, P, I, I, I, P, P]
         L.riv_nn_features.argtypes = [P, P, I, I, P, I, I, P, P, P]
+        L.riv_nn_front.argtypes = [P, P, I, I, P, I, I, P, P, P, P, P]
         L.riv_nn_im2col_t.argtypes = [I, P, I, I, P, P]
         L.riv_nn_col2im.argtypes = [I, P, I, P, I, P, P, P]
         L.riv_nn_relu_bwd.argtypes = [P, I, P, I, I, I, I, P, P, P]

@@ -138,6 +138,53 @@ def test_features_match_oracle():
         assert not x1[:, 304:].float().abs().sum().item()
 
 
+def test_front_equals_features_then_conv1():
+    """riv_nn_front (input on chip + conv1 on mma.sync) against riv_nn_features followed by the
+    tcgen05 conv1, and against the float64 oracle's conv1: the same bf16 outputs up to one
+    rounding step (the two sum the nine taps' f32 products in different orders)."""
+    from oracle import oracle as O
+    from riv2_b200 import proposal as P
+    from riv2_b200.synth import SynthClip
+    clip = SynthClip("cif", seed=9)
+    f0 = O.rgb_to_yuv(clip.frame(0), 352, 288, 352, 288)
+    f1 = O.rgb_to_yuv(clip.frame(2), 352, 288, 352, 288)
+    rng = np.random.default_rng(3)
+    n = 396
+    coded = np.zeros((n, 4), np.int8)
+    coded[:, 0:2] = rng.integers(-13, 13, (n, 2))
+    coded[:, 2:4] = rng.integers(0, 2, (n, 2))
+    net = P.ProposalNet(_params())
+    w1, b1 = net.w("w1"), net.bias("b1")
+    cur = torch.from_numpy(f1.y.copy()).cuda()
+    ref = torch.from_numpy(f0.y.copy()).cuda()
+    for prev, (mb0, cnt) in ((None, (0, n)), (coded, (5, 300))):
+        pc = None if prev is None else torch.from_numpy(prev).cuda()
+        pcp = None if pc is None else pc.data_ptr()
+        feat = torch.empty((cnt, 24, 24, 2), dtype=torch.bfloat16, device="cuda")
+        xa = torch.zeros((cnt, 320), dtype=torch.bfloat16, device="cuda")
+        xb = torch.zeros((cnt, 320), dtype=torch.bfloat16, device="cuda")
+        a_ref = torch.empty((cnt, 144, 32), dtype=torch.bfloat16, device="cuda")
+        a_new = torch.full((cnt, 144, 32), 7.0, dtype=torch.bfloat16, device="cuda")
+        L = P.lib()
+        assert L.riv_nn_features(cur.data_ptr(), ref.data_ptr(), 352, 288, pcp, mb0, cnt, feat.data_ptr(),
+                                 xa.data_ptr(), None) == 0
+        assert L.riv_nn_conv(1, feat.data_ptr(), 24 * 24 * 2, w1.data_ptr(), b1.data_ptr(), a_ref.data_ptr(),
+                             144 * 32, 32, cnt, net.err.data_ptr(), None) == 0
+        assert L.riv_nn_front(cur.data_ptr(), ref.data_ptr(), 352, 288, pcp, mb0, cnt, w1.data_ptr(), b1.data_ptr(),
+                              a_new.data_ptr(), xb.data_ptr(), None) == 0
+        torch.cuda.synchronize()
+        net.check()
+        assert torch.equal(xa[:, 288:], xb[:, 288:])
+        r, q = a_ref.float().cpu().numpy(), a_new.float().cpu().numpy()
+        assert np.abs(r - q).max() <= 2 ** -7 * max(1.0, np.abs(r).max())
+        assert (r != q).mean() < 0.01  # nearly all equal; the rest one bf16 step apart
+        # and the float64 oracle's conv1 on the same input
+        Pm = PO.unpack(net.params_numpy(), _layout())
+        cols = PO.im2col(feat.float().cpu().numpy().astype(np.float64), 1)
+        want = PO.bf16(np.maximum(cols @ Pm["w1"].T + Pm["b1"], 0.0)).reshape(cnt, 144, 32)
+        assert np.abs(q - want).max() <= 2 ** -7 * max(1.0, np.abs(want).max())
+
+
 def test_forward_matches_oracle():
     from riv2_b200 import proposal as P
     p = _params()
