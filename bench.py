@@ -382,6 +382,10 @@ def batch_point(dev_index: int, seed: int, steps: int, warmup: int, full: bool =
     ms = ev0.elapsed_time(ev1)
     c1 = b.counters()
     tune = b.tune()
+    host = {k: round(v, 1) for k, v in b.host_times().items()}
+    clip_host = np.sum([b.clip_counters(i)["host_ms"] for i in range(len(clips))], axis=0)
+    host_clips = dict(zip(["submit", "retire", "mv_coding", "dct_coding_sum", "write", "blocked"],
+                          [round(float(x), 1) for x in clip_host]))
     mbs = c1["mbs"] - c0["mbs"]
     frames = c1["frames"] - c0["frames"]
     b.close()
@@ -403,6 +407,7 @@ def batch_point(dev_index: int, seed: int, steps: int, warmup: int, full: bool =
             "warmup": warmup, "clips": len(clips), "frames": frames, "mbs": mbs, "tune": tune,
             "gpu_stage_us_per_step": {k: round(v, 1) for k, v in c1["stage_us"].items()},
             "launches_per_step": (c1["launches"] - c0["launches"]) / max(1, nsteps - warmup),
+            "host_ms_total": host, "clips_host_ms_total": host_clips,
             "streams_identical_to_single_clip": f"{sum(checked)}/{len(checked)}", "clocks": clocks,
             "frame_generation_s": round(gen_s, 1),
             "what": "64 clips (16 each at 352x288, 640x360, 1280x720, 1920x1080; 30-90 frames), q 85/80, one "

@@ -176,15 +176,16 @@ riv_status riv_host_times(riv_encoder* enc, double* ms6);
  * clip's wavefront leaves idle; each clip's entropy coding and records then run as in
  * riv_encode_frame, on thread pools the clips share.  Every clip's stream is byte-identical
  * to what riv_encoder_new + riv_encode_frame + riv_finish write for that clip alone.
- * Tile shapes (search CTAs, MBs per residual CTA, deblock tile width) are chosen by an
- * autotuner during the first all-P-frame steps (they do not change the output), or fixed by
- * riv_batch_set_tune. */
+ * Tile shapes (search CTAs, SAD table or not, MBs per residual CTA, deblock tile width) are
+ * chosen by an autotuner during the first all-P-frame steps (they do not change the output),
+ * or fixed by riv_batch_set_tune. */
 #define RIV_BATCH_MAX_CLIPS 256
 typedef struct riv_batch riv_batch;
 typedef struct {
     int32_t search_rows_pct; /* search CTAs per step, percent of what fits on the device (1..100) */
     int32_t res_mbs;         /* MBs per residual CTA: 2, 4 or 8 */
     int32_t db_tw;           /* deblock tile width, luma columns: 64, 128 or 256 */
+    int32_t sad_table;       /* 1: search from an exhaustive SAD table (search ranges <= 15), 0: SADs on the way */
 } riv_batch_tune;
 /* cfgs[i] / writers[i]: clip i (n <= RIV_BATCH_MAX_CLIPS).  Headers are written now. */
 riv_status riv_batch_new(const riv_config* cfgs, const riv_writer_vtable* writers, uint32_t n, riv_batch** out);
@@ -205,6 +206,10 @@ riv_status riv_batch_get_tune(const riv_batch* b, riv_batch_tune* t, int* tuned)
  * bytes}; stage_us10 = mean GPU microseconds per timed step: conversion, SAD tables, search,
  * prediction, AQ mean, residual, deblock, scan, pack, whole step.  Either may be NULL. */
 riv_status riv_batch_counters(const riv_batch* b, uint64_t* c7, double* stage_us10);
+/* Cumulative host milliseconds: [0] waiting for a clip's earlier records before its next
+ * frame (pipeline full), [1] descriptors and launches, [2] copies back and bookkeeping,
+ * [3] advancing the clips' pipelines after each step, [4] riv_batch_finish. */
+riv_status riv_batch_host_times(const riv_batch* b, double* ms5);
 /* Reconstruction (storage-size planes) of clip `clip`'s last submitted frame.  Synchronises. */
 riv_status riv_batch_last_recon(riv_batch* b, uint32_t clip, uint8_t* y, uint8_t* u, uint8_t* v);
 /* Records written so far for clip `clip`, and its host milliseconds (as riv_host_times). */

@@ -26,7 +26,8 @@ STAGES = ["convert", "sad_table", "search", "predict", "aq_mean", "residual", "d
 
 
 class RivBatchTune(C.Structure):
-    _fields_ = [("search_rows_pct", C.c_int32), ("res_mbs", C.c_int32), ("db_tw", C.c_int32)]
+    _fields_ = [("search_rows_pct", C.c_int32), ("res_mbs", C.c_int32), ("db_tw", C.c_int32),
+                ("sad_table", C.c_int32)]
 
 
 def _lib() -> C.CDLL:
@@ -46,6 +47,7 @@ def _lib() -> C.CDLL:
     L.riv_batch_counters.argtypes = [P, C.POINTER(C.c_uint64), C.POINTER(C.c_double)]
     L.riv_batch_last_recon.argtypes = [P, C.c_uint32, U8P, U8P, U8P]
     L.riv_batch_clip_counters.argtypes = [P, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_double)]
+    L.riv_batch_host_times.argtypes = [P, C.POINTER(C.c_double)]
     L._riv_batch_typed = True
     return L
 
@@ -118,8 +120,8 @@ class Batch:
     def finish(self) -> None:
         self._check(_lib().riv_batch_finish(self._h))
 
-    def set_tune(self, search_rows_pct: int, res_mbs: int, db_tw: int) -> None:
-        t = RivBatchTune(search_rows_pct, res_mbs, db_tw)
+    def set_tune(self, search_rows_pct: int, res_mbs: int, db_tw: int, sad_table: int = 1) -> None:
+        t = RivBatchTune(search_rows_pct, res_mbs, db_tw, sad_table)
         self._check(_lib().riv_batch_set_tune(self._h, C.byref(t)))
 
     def tune(self) -> dict:
@@ -127,7 +129,7 @@ class Batch:
         s = C.c_int()
         self._check(_lib().riv_batch_get_tune(self._h, C.byref(t), C.byref(s)))
         return {"search_rows_pct": t.search_rows_pct, "res_mbs": t.res_mbs, "db_tw": t.db_tw,
-                "state": {0: "tuning", 1: "autotuned", 2: "fixed"}[s.value]}
+                "sad_table": t.sad_table, "state": {0: "tuning", 1: "autotuned", 2: "fixed"}[s.value]}
 
     def counters(self) -> dict:
         c = (C.c_uint64 * 7)()
@@ -135,6 +137,12 @@ class Batch:
         self._check(_lib().riv_batch_counters(self._h, c, us))
         return {"steps": c[0], "frames": c[1], "mbs": c[2], "launches": c[3], "timed_steps": c[4], "h2d_bytes": c[5],
                 "d2h_bytes": c[6], "stage_us": dict(zip(STAGES, list(us)))}
+
+    def host_times(self) -> dict:
+        """Cumulative host milliseconds of the batch's own thread."""
+        ms = (C.c_double * 5)()
+        self._check(_lib().riv_batch_host_times(self._h, ms))
+        return dict(zip(["making_room", "launch", "copies_back", "advance", "finish"], list(ms)))
 
     def clip_counters(self, i: int) -> dict:
         n = C.c_uint64()

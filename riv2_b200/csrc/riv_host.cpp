@@ -2594,7 +2594,11 @@ constexpr int BT_BOUNDS = BS_N + 3;  // timing marks: start, then one after each
 enum { TB_START, TB_CONVERT, TB_TABLE, TB_SEARCH, TB_PREDICT, TB_AQSUM, TB_RESIDUAL, TB_DEBLOCK, TB_SCAN, TB_PACK };
 constexpr int BT_NSTAGE = 9;  // convert, table, search, predict, aq mean, residual, deblock, scan, pack
 // Autotuner candidates (one dimension per timed stage; the streams do not depend on them).
-constexpr int TUNE_ROWS_PCT[3] = {100, 75, 50};
+// The search has six candidates (CTA share x SAD table or not, timed as table + search stages),
+// the residual and the deblock three each (cycled twice as often).
+constexpr int TUNE_NCAND = 6;
+constexpr int TUNE_ROWS_PCT[TUNE_NCAND] = {100, 75, 50, 100, 75, 50};
+constexpr int TUNE_TABLE[TUNE_NCAND] = {1, 1, 1, 0, 0, 0};
 constexpr int TUNE_RES_MBS[3] = {4, 2, 8};
 constexpr int TUNE_DB_TW[3] = {128, 64, 256};
 constexpr int TUNE_ROUNDS = 2;  // all-P-frame steps measured per candidate
@@ -2627,14 +2631,18 @@ struct riv_batch {
     int cap[3] = {0, 0, 0}, sthreads[3] = {0, 0, 0};
     size_t ssmem[3] = {0, 0, 0};
     // tile shapes and the autotuner
-    BatchTune tune{4, 128, 100};
+    BatchTune tune{4, 128, 100, 1};
     bool fixed = false, tuned = false;
     int tune_step = 0;          // tuning steps submitted (candidate = (tune_step / ROUNDS) % 3)
-    double tune_us[3][3] = {};  // [dimension][candidate] summed microseconds per MB
-    int tune_n[3] = {0, 0, 0};  // all-P-frame steps measured per candidate
+    double tune_us[3][TUNE_NCAND] = {};  // [dimension][candidate] summed microseconds per MB
+    int tune_n[3][TUNE_NCAND] = {};      // all-P-frame steps measured per candidate
     uint64_t steps = 0, frames = 0, mbs = 0, launches = 0, timed = 0;
     double stage_us[BT_NSTAGE + 1] = {};  // sums over timed steps (last: whole step)
     uint64_t h2d_bytes = 0, d2h_bytes = 0;
+    // host milliseconds: [0] making room (earlier records of a clip written before its next
+    // frame), [1] descriptors and launches, [2] copies back and step bookkeeping, [3] advancing
+    // the clips' pipelines after the step, [4] finish
+    double host_ms[5] = {0, 0, 0, 0, 0};
     std::string err;
     bool poisoned = false;
 };
@@ -2776,16 +2784,17 @@ static void batch_collect(riv_encoder* e, Job& j, int src, const void* frame, cu
     e->fpar = (ck + 1) % NPAR;
 }
 
-// The shapes of this step: while tuning, candidate (tune_step / ROUNDS) % 3 of every dimension
-// at once (each dimension is timed by its own stage).
+// The shapes of this step: while tuning, search candidate c = (tune_step / ROUNDS) % 6 and
+// residual / deblock candidate c % 3 (each dimension is timed by its own stages).
 static BatchTune batch_step_tune(riv_batch* b, bool& tuning, int& cand) {
     tuning = !b->fixed && !b->tuned;
     BatchTune t = b->tune;
-    cand = (b->tune_step / TUNE_ROUNDS) % 3;
+    cand = (b->tune_step / TUNE_ROUNDS) % TUNE_NCAND;
     if (tuning) {
         t.row_ctas = TUNE_ROWS_PCT[cand];
-        t.res_mbs = TUNE_RES_MBS[cand];
-        t.db_tw = TUNE_DB_TW[cand];
+        t.table = TUNE_TABLE[cand];
+        t.res_mbs = TUNE_RES_MBS[cand % 3];
+        t.db_tw = TUNE_DB_TW[cand % 3];
     }
     return t;
 }
@@ -2805,22 +2814,27 @@ static void batch_read_times(riv_batch* b, int par) {
     b->timed++;
     if (!t.tuning || b->tuned || b->fixed) return;
     if (t.pmbs == t.mbs && t.pmbs > 0) {  // P-frames only: comparable steps
-        b->tune_us[0][t.cand] += 1000.0 * ms[2] / (double)t.pmbs;  // search
-        b->tune_us[1][t.cand] += 1000.0 * ms[5] / (double)t.mbs;   // residual
-        b->tune_us[2][t.cand] += 1000.0 * ms[6] / (double)t.mbs;   // deblock
-        b->tune_n[t.cand]++;
+        const int c3 = t.cand % 3;
+        b->tune_us[0][t.cand] += 1000.0 * (ms[1] + ms[2]) / (double)t.pmbs;  // SAD table + search
+        b->tune_us[1][c3] += 1000.0 * ms[5] / (double)t.mbs;                 // residual
+        b->tune_us[2][c3] += 1000.0 * ms[6] / (double)t.mbs;                 // deblock
+        b->tune_n[0][t.cand]++;
+        b->tune_n[1][c3]++;
+        b->tune_n[2][c3]++;
     }
-    for (int q = 0; q < 3; q++)
-        if (b->tune_n[q] < TUNE_ROUNDS) return;
-    auto pick = [&](int d) {
+    for (int q = 0; q < TUNE_NCAND; q++)
+        if (b->tune_n[0][q] < TUNE_ROUNDS) return;
+    auto pick = [&](int d, int nc) {
         int k = 0;
-        for (int q = 1; q < 3; q++)
-            if (b->tune_us[d][q] / b->tune_n[q] < b->tune_us[d][k] / b->tune_n[k]) k = q;
+        for (int q = 1; q < nc; q++)
+            if (b->tune_us[d][q] / b->tune_n[d][q] < b->tune_us[d][k] / b->tune_n[d][k]) k = q;
         return k;
     };
-    b->tune.row_ctas = TUNE_ROWS_PCT[pick(0)];
-    b->tune.res_mbs = TUNE_RES_MBS[pick(1)];
-    b->tune.db_tw = TUNE_DB_TW[pick(2)];
+    const int sc = pick(0, TUNE_NCAND);
+    b->tune.row_ctas = TUNE_ROWS_PCT[sc];
+    b->tune.table = TUNE_TABLE[sc];
+    b->tune.res_mbs = TUNE_RES_MBS[pick(1, 3)];
+    b->tune.db_tw = TUNE_DB_TW[pick(2, 3)];
     b->tuned = true;
 }
 
@@ -2833,6 +2847,8 @@ static riv_status batch_step(riv_batch* b, int src, const void* const* frames, c
     riv_status refused = RIV_OK;
     try {
         CK(cudaSetDevice(b->device));
+        const double h0 = now_ms();
+        double room = 0.0;
         // ---- jobs, in clip order
         std::vector<int> act;
         std::vector<Job*> jobs;
@@ -2841,11 +2857,13 @@ static riv_status batch_step(riv_batch* b, int src, const void* const* frames, c
             riv_encoder* e = b->clips[i];
             if (e->poisoned) return batch_fail(b, poisoned_status(e), "clip " + std::to_string(i) + ": " + e->err);
             const size_t cap = e->slots.size();
+            const double r0 = now_ms();
             while (e->jobs.size() >= cap) {
                 riv_status st = pump(e, true);
                 if (st == RIV_ERR_IO) { refused = st; continue; }
                 if (st) return batch_fail(b, st, "clip " + std::to_string(i) + ": " + e->err);
             }
+            room += now_ms() - r0;
             const uint64_t idx = e->submitted;
             const bool intra = next_is_key(e);
             e->jobs.emplace_back();
@@ -2879,7 +2897,12 @@ static riv_status batch_step(riv_batch* b, int src, const void* const* frames, c
             batch_collect(e, *jobs[a], src, frames[act[a]], b->Hs, kc[a], sps[a]);
             step_mbs += (uint64_t)e->NMB;
             if (jobs[a]->type == 2) {
-                pvar[a] = search_variant(e);
+                if (!t.table) {  // SADs computed by the search itself
+                    sps[a].tab = nullptr;
+                    sps[a].tstride = 0;
+                    kc[a].tab = nullptr;
+                }
+                pvar[a] = t.table ? search_variant(e) : 2;
                 step_pmbs += (uint64_t)e->NMB;
             }
         }
@@ -2954,6 +2977,9 @@ static riv_status batch_step(riv_batch* b, int src, const void* const* frames, c
         stage(BS_SCAN, TB_SCAN);
         stage(BS_PACK, TB_PACK);
         CK(cudaEventRecord(b->ev_gpu, B));
+        const double h1 = now_ms();
+        b->host_ms[0] += room;
+        b->host_ms[1] += h1 - h0 - room;
         // ---- copies back: side info, EOBs and a bounded prefix of the coefficients per clip
         cudaEvent_t xev = b->ev_step[b->steps % b->ev_step.size()];
         CK(cudaStreamWaitEvent(b->C, b->ev_gpu, 0));
@@ -2996,7 +3022,14 @@ static riv_status batch_step(riv_batch* b, int src, const void* const* frames, c
             if (tuning) b->tune_step++;
             batch_read_times(b, b->tpar);  // the other set: the previous timed step
         }
+        const double h2 = now_ms();
+        b->host_ms[2] += h2 - h1;
         // ---- each clip's host pipeline advances
+        struct Tail {
+            riv_batch* b;
+            double t;
+            ~Tail() { b->host_ms[3] += now_ms() - t; }
+        } tail{b, h2};
         for (int a = 0; a < m; a++) {
             riv_encoder* e = b->clips[act[a]];
             riv_status st = pump(e, false);
@@ -3121,6 +3154,12 @@ riv_status riv_batch_finish(riv_batch* b) {
         return batch_fail(b, RIV_ERR_CUDA, std::string(ce.where) + ": " + cudaGetErrorString(ce.e));
     }
     riv_status first = RIV_OK;
+    const double f0 = now_ms();
+    struct Fin {
+        riv_batch* b;
+        double t;
+        ~Fin() { b->host_ms[4] += now_ms() - t; }
+    } fin{b, f0};
     for (size_t i = 0; i < b->clips.size(); i++) {
         riv_status st = riv_finish(b->clips[i]);
         if (st && !first) {
@@ -3164,11 +3203,12 @@ const char* riv_batch_last_error(const riv_batch* b) { return b ? b->err.c_str()
 riv_status riv_batch_set_tune(riv_batch* b, const riv_batch_tune* t) {
     if (!b || !t) return RIV_ERR_INVALID_CONFIG;
     if ((t->res_mbs != 2 && t->res_mbs != 4 && t->res_mbs != 8) || (t->db_tw != 64 && t->db_tw != 128 && t->db_tw != 256) ||
-        t->search_rows_pct < 1 || t->search_rows_pct > 100)
+        t->search_rows_pct < 1 || t->search_rows_pct > 100 || (t->sad_table != 0 && t->sad_table != 1))
         return RIV_ERR_INVALID_CONFIG;
     b->tune.row_ctas = t->search_rows_pct;
     b->tune.res_mbs = t->res_mbs;
     b->tune.db_tw = t->db_tw;
+    b->tune.table = t->sad_table ? 1 : 0;
     b->fixed = true;
     return RIV_OK;
 }
@@ -3178,6 +3218,7 @@ riv_status riv_batch_get_tune(const riv_batch* b, riv_batch_tune* t, int* tuned)
     t->search_rows_pct = b->tune.row_ctas;
     t->res_mbs = b->tune.res_mbs;
     t->db_tw = b->tune.db_tw;
+    t->sad_table = b->tune.table;
     if (tuned) *tuned = b->fixed ? 2 : (b->tuned ? 1 : 0);
     return RIV_OK;
 }
@@ -3195,6 +3236,12 @@ riv_status riv_batch_counters(const riv_batch* b, uint64_t* c7, double* stage_us
     }
     if (stage_us10)
         for (int s = 0; s <= BT_NSTAGE; s++) stage_us10[s] = b->timed ? b->stage_us[s] / (double)b->timed : 0.0;
+    return RIV_OK;
+}
+
+riv_status riv_batch_host_times(const riv_batch* b, double* ms5) {
+    if (!b || !ms5) return RIV_ERR_INVALID_CONFIG;
+    for (int k = 0; k < 5; k++) ms5[k] = b->host_ms[k];
     return RIV_OK;
 }
 

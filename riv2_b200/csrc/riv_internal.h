@@ -158,6 +158,7 @@ struct BatchTune {
     int res_mbs;   // MBs per residual CTA: 2, 4 or 8
     int db_tw;     // deblock tile width in luma columns: 64, 128 or 256
     int row_ctas;  // search: percent of the device's capacity of search CTAs used by a step
+    int table;     // search from an exhaustive SAD table (search ranges <= 15) or SADs computed on the way
 };
 struct BatchLaunch {
     const BatchClip* clips;  // device, nclips

@@ -2644,7 +2644,7 @@ struct LearnedParams {
 // count's load), lane 0 adding the values left to right.  Each row's count goes back to zero
 // for the next frame.  A wait past the spin limit sets ST_WAIT_TIMEOUT and ends the fold.
 __device__ __forceinline__ void learned_fold(const LearnedParams& lp) {
-    __shared__ float fb[256];
+    __shared__ __align__(16) float fb[256];
     const SearchParams& p = lp.sp;
     const int lane = threadIdx.x & 31;
     float sum = 0.0f;
@@ -2668,8 +2668,16 @@ __device__ __forceinline__ void learned_fold(const LearnedParams& lp) {
             const int m = min(256, p.BW - b0);
             for (int i = lane; i < m; i += 32) fb[i] = __ldcg(p.lnv + (size_t)r * p.BW + b0 + i);
             __syncwarp();
-            if (lane == 0)
-                for (int i = 0; i < m; i++) sum = __fadd_rn(sum, fb[i]);
+            if (lane == 0) {  // eight values per pair of vector loads, the adds strictly in order
+                int i = 0;
+                for (; i + 8 <= m; i += 8) {
+                    const float4 a = *(const float4*)(fb + i), b = *(const float4*)(fb + i + 4);
+                    sum = __fadd_rn(sum, a.x); sum = __fadd_rn(sum, a.y); sum = __fadd_rn(sum, a.z);
+                    sum = __fadd_rn(sum, a.w); sum = __fadd_rn(sum, b.x); sum = __fadd_rn(sum, b.y);
+                    sum = __fadd_rn(sum, b.z); sum = __fadd_rn(sum, b.w);
+                }
+                for (; i < m; i++) sum = __fadd_rn(sum, fb[i]);
+            }
             __syncwarp();
         }
         if (lane == 0) lp.rowcnt[r] = 0u;

@@ -587,7 +587,7 @@ __device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a
 // 16 output positions at a time: A rows = positions, the fragment's k pairs = one tap's two
 // channels (one 32-bit word of the shared input), B = W1 (32 x 32, bf16), f32 accumulation.
 template <bool FRONT>
-__global__ void __launch_bounds__(256) k_prop_input(const uint8_t* __restrict__ cur, const uint8_t* __restrict__ ref,
+__global__ void __launch_bounds__(256, 4) k_prop_input(const uint8_t* __restrict__ cur, const uint8_t* __restrict__ ref,
                                                     int W, int H, const int8_t* __restrict__ prev_coded, int mb0,
                                                     int nmb, __nv_bfloat16* __restrict__ feat,
                                                     __nv_bfloat16* __restrict__ x1,

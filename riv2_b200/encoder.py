@@ -128,7 +128,7 @@ EXPORTED_SYMBOLS = (
     "riv_learned_counters", "riv_test_mv_encode_threads",
     "riv_batch_new", "riv_batch_encode", "riv_batch_encode_device", "riv_batch_finish", "riv_batch_free",
     "riv_batch_last_error", "riv_batch_set_tune", "riv_batch_get_tune", "riv_batch_counters", "riv_batch_last_recon",
-    "riv_batch_clip_counters",
+    "riv_batch_clip_counters", "riv_batch_host_times",
 )
 
 

@@ -99,7 +99,7 @@ def test_batch_clip_matches_oracle():
     assert streams[0] == oe.finish()
 
 
-@pytest.mark.parametrize("tune", [(100, 2, 64), (50, 8, 256), (1, 4, 128)])
+@pytest.mark.parametrize("tune", [(100, 2, 64, 1), (50, 8, 256, 0), (1, 4, 128, 1), (75, 4, 128, 0)])
 def test_batch_tile_shapes_do_not_change_the_streams(tune):
     from riv2_b200.synth import SynthClip
     cfgs = [_cfg(352, 288), _cfg(1280, 720), _cfg(640, 360)]
@@ -114,8 +114,9 @@ def test_batch_autotuner_settles_and_keeps_streams():
     from riv2_b200.synth import SynthClip
     cfgs = [_cfg(352, 288), _cfg(352, 288), _cfg(640, 360)]
     clips = [SynthClip("cif", seed=61), SynthClip("cif", seed=62), SynthClip("720p", seed=63, width=640, height=360)]
-    spans = [(0, 12), (0, 12), (0, 12)]
+    spans = [(0, 18), (0, 18), (0, 18)]
     streams, recons, info = _run_batch(cfgs, clips, spans)
     assert info["tune"]["state"] == "autotuned", info
+    assert info["tune"]["sad_table"] in (0, 1)
     assert info["tune"]["res_mbs"] in (2, 4, 8) and info["tune"]["db_tw"] in (64, 128, 256)
     _check_against_single(cfgs, clips, spans, streams, recons)
