@@ -2639,50 +2639,56 @@ struct LearnedParams {
 };
 
 // The strictly sequential f32 sum of the ln variances (Iterator::sum, res/residual.rs:154-167)
-// and their mean at lnv[n], by one warp of the launch's first CTA while the search CTAs run:
-// row r is folded once all its MBs have published (release: fence + count; acquire: the
-// count's load), lane 0 adding the values left to right.  Each row's count goes back to zero
-// for the next frame.  A wait past the spin limit sets ST_WAIT_TIMEOUT and ends the fold.
+// and their mean at lnv[n], by one warp of the launch's first CTA while the search CTAs run.
+// Each round, lane i checks whether row r + i has published all its MBs (release: fence +
+// count; acquire: the count's load), the warp takes every finished row from r on at once,
+// stages their values through shared memory in chunks and lane 0 adds them left to right, so
+// the L2 round trips are paid per batch of rows, not per row.  Each row's count goes back to
+// zero for the next frame.  A wait past the spin limit sets ST_WAIT_TIMEOUT and ends the fold.
 __device__ __forceinline__ void learned_fold(const LearnedParams& lp) {
-    __shared__ __align__(16) float fb[256];
+    constexpr int CH = 1024;
+    __shared__ __align__(16) float fb[CH];
     const SearchParams& p = lp.sp;
     const int lane = threadIdx.x & 31;
     float sum = 0.0f;
-    bool failed = false;
-    for (int r = 0; r < p.BH && !failed; r++) {
-        if (lane == 0) {
-            long long spins = 0;
-            while (ld_acquire_u32(lp.rowcnt + r) < (unsigned)p.BW) {
-                if (++spins > p.spin_limit) {
-                    atomicOr(p.status, ST_WAIT_TIMEOUT);
-                    failed = true;
-                    break;
-                }
-                __nanosleep(32);
+    long long spins = 0;
+    int r = 0;
+    while (r < p.BH) {
+        const bool done = r + lane < p.BH && ld_acquire_u32(lp.rowcnt + r + lane) >= (unsigned)p.BW;
+        const unsigned m = __ballot_sync(0xffffffffu, done);
+        const int ready = m == 0xffffffffu ? 32 : __ffs(~m) - 1;  // finished rows r, r + 1, ...
+        if (ready == 0) {
+            if (++spins > p.spin_limit) {
+                if (lane == 0) atomicOr(p.status, ST_WAIT_TIMEOUT);
+                return;
             }
+            __nanosleep(64);
+            continue;
         }
-        failed = __shfl_sync(0xffffffffu, (int)failed, 0) != 0;
-        if (failed) break;
+        spins = 0;
         __syncwarp();
-        for (int b0 = 0; b0 < p.BW; b0 += 256) {
-            const int m = min(256, p.BW - b0);
-            for (int i = lane; i < m; i += 32) fb[i] = __ldcg(p.lnv + (size_t)r * p.BW + b0 + i);
+        const size_t base = (size_t)r * p.BW;
+        const int total = ready * p.BW;
+        for (int c0 = 0; c0 < total; c0 += CH) {
+            const int m2 = min(CH, total - c0);
+            for (int i = lane; i < m2; i += 32) fb[i] = __ldcg(p.lnv + base + c0 + i);
             __syncwarp();
             if (lane == 0) {  // eight values per pair of vector loads, the adds strictly in order
                 int i = 0;
-                for (; i + 8 <= m; i += 8) {
+                for (; i + 8 <= m2; i += 8) {
                     const float4 a = *(const float4*)(fb + i), b = *(const float4*)(fb + i + 4);
                     sum = __fadd_rn(sum, a.x); sum = __fadd_rn(sum, a.y); sum = __fadd_rn(sum, a.z);
                     sum = __fadd_rn(sum, a.w); sum = __fadd_rn(sum, b.x); sum = __fadd_rn(sum, b.y);
                     sum = __fadd_rn(sum, b.z); sum = __fadd_rn(sum, b.w);
                 }
-                for (; i < m; i++) sum = __fadd_rn(sum, fb[i]);
+                for (; i < m2; i++) sum = __fadd_rn(sum, fb[i]);
             }
             __syncwarp();
         }
-        if (lane == 0) lp.rowcnt[r] = 0u;
+        if (lane < ready) lp.rowcnt[r + lane] = 0u;
+        r += ready;
     }
-    if (lane == 0 && !failed) p.lnv[p.BW * p.BH] = __fdiv_rn(sum, (float)(p.BW * p.BH));
+    if (lane == 0) p.lnv[p.BW * p.BH] = __fdiv_rn(sum, (float)(p.BW * p.BH));
 }
 
 // SAD of the 16x16 block at whole-pixel offset (dx, dy) over the window; lane l covers row l/2,

@@ -272,8 +272,10 @@ struct ConvCfg {
     }
 };
 
+// L1-allocating: the 3x3 windows of neighbouring output rows share most of their input
+// pixels, so a tile's repeated reads hit L1 instead of going back to L2.
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, unsigned bytes) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
 }
 __device__ __forceinline__ void cp_async4(uint32_t dst, const void* src, unsigned bytes) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
