@@ -3251,22 +3251,27 @@ int launch_residual(const ResidualParams& p, int nmb, void* stream) {
 // x-4..x+3 and writes x-3..x+2, edges are >= 8 px apart), so a thread per edge line
 // reproduces the reference's sequential loops exactly.
 // ---------------------------------------------------------------------------------
+// TW: luma tile width (256 for this standalone launch: fewer, wider tiles measured faster than
+// the worker tasks' DB_TW; the output does not depend on it).
+constexpr int DB_TW_STANDALONE = 256;
+template <int TW>
 __global__ void __launch_bounds__(128) k_deblock_tiled(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, int W,
                                                        int H, int BW, int E, int I, int Hv, const uint8_t* mask,
                                                        int ntiles_y) {
-    __shared__ uint8_t tile[DB_TILE_BYTES];
+    __shared__ uint8_t tile[(16 + 8) * (TW + 8)];
     int t = blockIdx.x;
     int plane = t < ntiles_y ? 0 : (t - ntiles_y) % 2 + 1;
     if (plane > 0) t = (t - ntiles_y) / 2;
-    deblock_tile(src, dst, W, H, BW, E, I, Hv, mask, plane, t, tile, threadIdx.x, blockDim.x, 0);
+    deblock_tile<TW>(src, dst, W, H, BW, E, I, Hv, mask, plane, t, tile, threadIdx.x, blockDim.x, 0);
 }
 
 int launch_deblock_tiled(const uint8_t* src, uint8_t* dst, int W, int H, int E, int I, int Hv, const uint8_t* mask,
                          void* stream) {
+    constexpr int TW = DB_TW_STANDALONE;
     const int BW = W / 16;
-    const int ty = (H / 16) * ((W + DB_TW - 1) / DB_TW);
-    const int tc = ((H / 2) / 8) * ((W / 2 + DB_TW / 2 - 1) / (DB_TW / 2));
-    k_deblock_tiled<<<ty + 2 * tc, 128, 0, (cudaStream_t)stream>>>(src, dst, W, H, BW, E, I, Hv, mask, ty);
+    const int ty = (H / 16) * ((W + TW - 1) / TW);
+    const int tc = ((H / 2) / 8) * ((W / 2 + TW / 2 - 1) / (TW / 2));
+    k_deblock_tiled<TW><<<ty + 2 * tc, 128, 0, (cudaStream_t)stream>>>(src, dst, W, H, BW, E, I, Hv, mask, ty);
     return (int)cudaGetLastError();
 }
 

@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(128, 1)
 // (warp w reads TMEM lanes 32 (w % 4) .. +31).  The accumulator is double-buffered (2 x 32
 // columns), so a tile's epilogue overlaps the next tile's MMAs and gathers.
 constexpr int CV_THREADS = 288;
-constexpr int CV_LAG = 2;  // k-blocks a gathering thread keeps in flight before marking one full
+constexpr int CV_LAG = 3;  // k-blocks a gathering thread keeps in flight before marking one full
 
 struct ConvArgs {
     const __nv_bfloat16* in;
@@ -272,10 +272,8 @@ struct ConvCfg {
     }
 };
 
-// L1-allocating: the 3x3 windows of neighbouring output rows share most of their input
-// pixels, so a tile's repeated reads hit L1 instead of going back to L2.
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, unsigned bytes) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
 }
 __device__ __forceinline__ void cp_async4(uint32_t dst, const void* src, unsigned bytes) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
@@ -675,27 +673,39 @@ __global__ void __launch_bounds__(256, 4) k_prop_input(const uint8_t* __restrict
     }
     if (t < 32) R[t][PF_WW / 8] = 0u;
     __syncthreads();
-    for (int k = t; k < nhere * nn::FEAT * nn::FEAT; k += 256) {
-        const int m = k / (nn::FEAT * nn::FEAT), kk = k % (nn::FEAT * nn::FEAT);
+    // four horizontally adjacent offsets per item: they share the reference words of each row
+    // (shifted by 0, 8, 16, 24 bits) and the current block's words
+    constexpr int NG = nn::FEAT / 4;  // groups of four offsets per row of the volume
+    for (int k = t; k < nhere * nn::FEAT * NG; k += 256) {
+        const int m = k / (nn::FEAT * NG), kg = k % (nn::FEAT * NG);
         const int mb = first + m;
         if (mb < mb0 || mb >= mb0 + nmb) continue;
-        const int v = kk / nn::FEAT, u = kk % nn::FEAT;
-        const int uu = 8 * m + u, wq = uu >> 2, sh = (uu & 3) * 8;
-        unsigned sad = 0;
+        const int v = kg / NG, u0 = 4 * (kg % NG);
+        const int wq = (8 * m + u0) >> 2;  // 8 m + u0 is a multiple of 4
+        unsigned sad[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
         for (int j = 0; j < 8; j++) {
             const uint32_t* row = R[v + j];
             const uint32_t w0 = row[wq], w1 = row[wq + 1], w2 = row[wq + 2];
-            sad += __vsadu4(__funnelshift_r(w0, w1, sh), Cb[m][j][0]);
-            sad += __vsadu4(__funnelshift_r(w1, w2, sh), Cb[m][j][1]);
-        }
-        const float f0 = 1.0f - (float)min((int)sad, 2048) * (1.0f / 1024.0f);
-        float f1 = 0.0f;
+            const uint32_t c0 = Cb[m][j][0], c1 = Cb[m][j][1];
+            sad[0] += __vsadu4(w0, c0) + __vsadu4(w1, c1);
 #pragma unroll
-        for (int q = 0; q < nn::NPRED; q++)
-            if (pu[m][q] == u && pv[m][q] == v) f1 = 1.0f;
-        if (FRONT) F[m * NF + kk] = pack_bf16(f0, f1);
-        else *(uint32_t*)(feat + (size_t)(mb - mb0) * (nn::FEAT * nn::FEAT * 2) + 2 * kk) = pack_bf16(f0, f1);
+            for (int q = 1; q < 4; q++)
+                sad[q] += __vsadu4(__funnelshift_r(w0, w1, 8 * q), c0) + __vsadu4(__funnelshift_r(w1, w2, 8 * q), c1);
+        }
+        uint32_t o[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const float f0 = 1.0f - (float)min((int)sad[q], 2048) * (1.0f / 1024.0f);
+            float f1 = 0.0f;
+#pragma unroll
+            for (int pq = 0; pq < nn::NPRED; pq++)
+                if (pu[m][pq] == u0 + q && pv[m][pq] == v) f1 = 1.0f;
+            o[q] = pack_bf16(f0, f1);
+        }
+        const int kk = v * nn::FEAT + u0;  // 16-byte aligned word index
+        if (FRONT) *(uint4*)(F + m * NF + kk) = make_uint4(o[0], o[1], o[2], o[3]);
+        else *(uint4*)(feat + (size_t)(mb - mb0) * (nn::FEAT * nn::FEAT * 2) + 2 * kk) = make_uint4(o[0], o[1], o[2], o[3]);
     }
     if (t < 16 * nhere) {
         const int m = t >> 4, q = t & 15, mb = first + m;
