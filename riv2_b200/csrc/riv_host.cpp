@@ -404,6 +404,7 @@ struct riv_encoder {
     std::shared_ptr<ThreadPool> rans_pool;  // coefficient-coder jobs (never wait)
     BatchSubmit rans_submit;
     int rans_parts = 1;  // threads that code one frame's coefficients: rans_pool's and the caller
+    int mv_parts = 1;    // threads that model one frame's MVs (1: the sequential coder)
     bool draining = false;  // inside drain_all: the newest frame is coded by rans_parts threads
     bool batched = false;   // a clip of a riv_batch: only the batch submits its frames
     double host_ms[6] = {0};  // submit, retire, mv coding, dct coding (summed), write, blocked
@@ -651,6 +652,7 @@ static void setup_device(riv_encoder* e) {
     e->mv_exec.reset(new ThreadPool(1));
     e->rans_pool.reset(new ThreadPool(std::max(2u, nt / 2)));
     e->rans_parts = (int)std::max(2u, nt / 2) + 1;
+    if (const char* v = getenv("RIV_MV_PARTS")) e->mv_parts = std::max(1, std::min(8, atoi(v)));
     {
         ThreadPool* rp = e->rans_pool.get();
         e->rans_submit = [rp](std::function<void()> f) { return rp->submit(std::move(f)); };
@@ -1207,7 +1209,10 @@ static riv_status retire(riv_encoder* e, Job& j) {
             S.mv_raw_bytes = (uint32_t)(2 * N + 2 * S.mv_new_blocks);
             S.resi_raw = (int64_t)(N - (int)S.blocks_skipped) * 384 * 2;
             if (mbh) search_stats(ep, mbh->data(), prevh ? prevh->data() : nullptr, S);
-            ep->mvc.encode_frame(blocks, ep->BW, jp->mv_bytes, &ep->rans_submit);
+            // the MV coder's modelling split mv_parts ways when set (same bytes; shorter on
+            // the ordered thread, which is serial across frames)
+            if (ep->mv_parts > 1) ep->mvc.encode_frame_parallel(blocks, ep->BW, jp->mv_bytes, ep->rans_submit, ep->mv_parts);
+            else ep->mvc.encode_frame(blocks, ep->BW, jp->mv_bytes, &ep->rans_submit);
             S.mv_bias_dx = jp->bias[0];
             S.mv_bias_dy = jp->bias[1];
             S.rdo_lambda = ep->L.lambda;
