@@ -517,7 +517,8 @@ __global__ void __launch_bounds__(CV_THREADS, 1) k_nn_conv_s(const __grid_consta
         };
         if (tid == 0 && (int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
         const uint32_t sa0 = s32(sa);
-        const int x = tid & 7;
+        const int c8 = tid & 7, h8 = c8 >> 2, c4 = c8 & 3, rsub = tid >> 3;
+        const int x = rsub & 7;  // swizzle phase of this thread's rows (rsub + 16 q) & 7
         int it = 0, nt = 0;
         for (int tile = blockIdx.x; tile < ntiles && !dead; tile += gridDim.x, nt++) {
             const int buf = nt & 1;
@@ -530,26 +531,33 @@ __global__ void __launch_bounds__(CV_THREADS, 1) k_nn_conv_s(const __grid_consta
             if (!mb_wait(&ibar[buf], (unsigned)((nt >> 1) & 1), a.err, dead)) break;
             int b0, b1;
             tile_mbs(tile, b0, b1);
-            const long long m = (long long)tile * 128 + tid;
-            const bool valid = m < rows;
-            const int b = valid ? (int)(m / pos) : b0, p = valid ? (int)(m % pos) : 0;
-            const int oy = p / a.hout, ox = p % a.hout;
-            const uint8_t* in_b = ibuf + (size_t)buf * ib_bytes + (size_t)(b - b0) * mb_bytes;
+            // thread t copies 16-byte piece c8 = t % 8 of rows t / 8 + 16 i (i = 0..7): eight
+            // neighbouring threads fill one row (two taps of 64 bytes each), so their loads from
+            // the input buffer are contiguous and their stores fill one swizzled 128-byte row
+            const uint8_t* ib = ibuf + (size_t)buf * ib_bytes;
+            int roff[8], ry[8], rx[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const long long m = (long long)tile * 128 + rsub + 16 * q;
+                const bool valid = m < rows;
+                const int b = valid ? (int)(m / pos) : b0, p = valid ? (int)(m % pos) : 0;
+                roff[q] = (int)((size_t)(b - b0) * mb_bytes);
+                ry[q] = valid ? (p / a.hout) * a.stride - 1 : -1000;  // -1000: never inside
+                rx[q] = (p % a.hout) * a.stride - 1;
+            }
             for (int kb = 0; kb < NKB; kb++, it++) {
                 const int s = it % S;
                 if (it >= S && !mb_wait(&empty[s], ((it / S) - 1) & 1, a.err, dead)) break;
-                uint8_t* row = sa + (size_t)s * A_TILE + (size_t)tid * SWZ;
+                uint8_t* stage = sa + (size_t)s * A_TILE;
+                const int t = 2 * kb + h8;  // this thread's tap (9: zero padding of K)
+                const int ty = t / 3, tx = t % 3;
 #pragma unroll
-                for (int h = 0; h < 2; h++) {  // two taps of 32 channels (64 bytes each) per k-block
-                    const int t = 2 * kb + h;
-                    const int iy = oy * a.stride + t / 3 - 1, ix = ox * a.stride + t % 3 - 1;
-                    const bool in = valid && t < 9 && iy >= 0 && iy < a.hin && ix >= 0 && ix < a.hin;
-                    const uint4* src = (const uint4*)(in_b + (size_t)(iy * a.hin + ix) * 64);
-#pragma unroll
-                    for (int c = 0; c < 4; c++) {
-                        const uint4 v = in ? src[c] : make_uint4(0u, 0u, 0u, 0u);
-                        *(uint4*)(row + (((4 * h + c) ^ x) << 4)) = v;
-                    }
+                for (int q = 0; q < 8; q++) {
+                    const int iy = ry[q] + ty, ix = rx[q] + tx;
+                    const bool in = t < 9 && iy >= 0 && iy < a.hin && ix >= 0 && ix < a.hin;
+                    const uint4 v = in ? *(const uint4*)(ib + roff[q] + (iy * a.hin + ix) * 64 + c4 * 16)
+                                       : make_uint4(0u, 0u, 0u, 0u);
+                    *(uint4*)(stage + (size_t)(rsub + 16 * q) * SWZ + ((c8 ^ x) << 4)) = v;
                 }
                 fence_async_smem();
                 mb_arrive(&full[s]);
