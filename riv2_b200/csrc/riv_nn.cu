@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(128, 1)
 // (warp w reads TMEM lanes 32 (w % 4) .. +31).  The accumulator is double-buffered (2 x 32
 // columns), so a tile's epilogue overlaps the next tile's MMAs and gathers.
 constexpr int CV_THREADS = 288;
-constexpr int CV_LAG = 3;  // k-blocks a gathering thread keeps in flight before marking one full
+constexpr int CV_LAG = 2;  // k-blocks a gathering thread keeps in flight before marking one full
 
 struct ConvArgs {
     const __nv_bfloat16* in;
@@ -436,199 +436,6 @@ __global__ void __launch_bounds__(CV_THREADS, 2) k_nn_conv(const __grid_constant
     if (warp == 4) tm_dealloc(tacc, 64);
 }
 
-// ---- Implicit-GEMM convolution with the input staged in shared memory (layers 2-4).
-// A 128-row tile of output positions covers at most mbs_per_tile consecutive MBs, whose inputs
-// are contiguous in global memory: one bulk copy (cp.async.bulk, TMA engine) brings them into
-// one of two input buffers while the previous tile is built, and the gather warps then build
-// each k-block of the im2col operand from shared memory (16-byte loads and stores into the
-// swizzled K-major layout, zeros for padding taps), so no gather waits on L2.  MMA and epilogue
-// warps as in k_nn_conv.  Smem: weights (5 k-blocks), SS operand stages, 2 input buffers.
-constexpr int CS_STAGES = 4;
-__host__ __device__ inline int conv_s_mbs_per_tile(int pos) { return 127 / pos + 2; }
-__host__ __device__ inline size_t conv_s_ib_bytes(int pos, int in_mb) {
-    return ((size_t)conv_s_mbs_per_tile(pos) * in_mb * 2 + 127) & ~(size_t)127;
-}
-__host__ __device__ inline size_t conv_s_smem(int pos, int in_mb) {
-    return 1024 + 5 * 32 * 128 + (size_t)CS_STAGES * 128 * 128 + 2 * conv_s_ib_bytes(pos, in_mb) + 1024;
-}
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, unsigned bytes, uint64_t* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                 "l"(src), "r"(bytes), "r"(s32(bar))
-                 : "memory");
-}
-
-__global__ void __launch_bounds__(CV_THREADS, 1) k_nn_conv_s(const __grid_constant__ CUtensorMap tw, ConvArgs a) {
-    constexpr int NKB = 5, S = CS_STAGES, SWZ = 128, A_TILE = 128 * 128, W_TILE = 32 * 128;
-    extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint8_t* sm = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const int pos = a.hout * a.hout;
-    const size_t ib_bytes = conv_s_ib_bytes(pos, a.in_mb);
-    uint8_t* sw = sm;                      // weights
-    uint8_t* sa = sm + NKB * W_TILE;       // operand stages (1024-byte aligned)
-    uint8_t* ibuf = sa + S * A_TILE;       // two input buffers
-    uint64_t* wfull = (uint64_t*)(ibuf + 2 * ib_bytes);
-    uint64_t* full = wfull + 1;
-    uint64_t* empty = full + S;
-    uint64_t* accf = empty + S;
-    uint64_t* acce = accf + 2;
-    uint64_t* ibar = acce + 2;   // input buffer b filled (bulk copy)
-    uint64_t* ifree = ibar + 2;  // input buffer b released by all 128 gather threads
-    uint32_t* slot = (uint32_t*)(ifree + 2);
-    float* sbias = (float*)(slot + 4);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (tid == 0) {
-        mb_init(wfull, 1);
-        for (int k = 0; k < S; k++) {
-            mb_init(&full[k], 128);
-            mb_init(&empty[k], 1);
-        }
-        for (int k = 0; k < 2; k++) {
-            mb_init(&accf[k], 1);
-            mb_init(&acce[k], 128);
-            mb_init(&ibar[k], 1);
-            mb_init(&ifree[k], 128);
-        }
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    if (tid < 32) sbias[tid] = a.bias[tid];
-    if (warp == 4) tm_alloc(slot, 64);
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tacc = *slot;
-    bool dead = false;
-    const long long rows = (long long)a.nmb * pos;
-    const int ntiles = (int)((rows + 127) / 128);
-    const size_t mb_bytes = (size_t)a.in_mb * 2;
-
-    if (warp < 4) {
-        // the MBs of tile t: b0 .. b1, all inside the frame's nmb
-        auto tile_mbs = [&](int t, int& b0, int& b1) {
-            const long long m0 = (long long)t * 128, m1 = min(rows, m0 + 128) - 1;
-            b0 = (int)(m0 / pos);
-            b1 = (int)(m1 / pos);
-        };
-        auto issue = [&](int t, int buf) {  // thread 0: the bulk copy of tile t's input into buf
-            int b0, b1;
-            tile_mbs(t, b0, b1);
-            const unsigned bytes = (unsigned)((size_t)(b1 - b0 + 1) * mb_bytes);
-            mb_expect_tx(&ibar[buf], bytes);
-            bulk_g2s(s32(ibuf + (size_t)buf * ib_bytes), (const uint8_t*)a.in + (size_t)b0 * mb_bytes, bytes, &ibar[buf]);
-        };
-        if (tid == 0 && (int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
-        const uint32_t sa0 = s32(sa);
-        const int c8 = tid & 7, h8 = c8 >> 2, c4 = c8 & 3, rsub = tid >> 3;
-        const int x = rsub & 7;  // swizzle phase of this thread's rows (rsub + 16 q) & 7
-        int it = 0, nt = 0;
-        for (int tile = blockIdx.x; tile < ntiles && !dead; tile += gridDim.x, nt++) {
-            const int buf = nt & 1;
-            // the next tile's input goes into the other buffer once every gather thread has
-            // released it (its previous use was tile nt - 1)
-            if (tid == 0 && tile + (int)gridDim.x < ntiles) {
-                if (nt >= 1 && !mb_wait(&ifree[buf ^ 1], (unsigned)(((nt - 1) >> 1) & 1), a.err, dead)) break;
-                issue(tile + gridDim.x, buf ^ 1);
-            }
-            if (!mb_wait(&ibar[buf], (unsigned)((nt >> 1) & 1), a.err, dead)) break;
-            int b0, b1;
-            tile_mbs(tile, b0, b1);
-            // thread t copies 16-byte piece c8 = t % 8 of rows t / 8 + 16 i (i = 0..7): eight
-            // neighbouring threads fill one row (two taps of 64 bytes each), so their loads from
-            // the input buffer are contiguous and their stores fill one swizzled 128-byte row
-            const uint8_t* ib = ibuf + (size_t)buf * ib_bytes;
-            int roff[8], ry[8], rx[8];
-#pragma unroll
-            for (int q = 0; q < 8; q++) {
-                const long long m = (long long)tile * 128 + rsub + 16 * q;
-                const bool valid = m < rows;
-                const int b = valid ? (int)(m / pos) : b0, p = valid ? (int)(m % pos) : 0;
-                roff[q] = (int)((size_t)(b - b0) * mb_bytes);
-                ry[q] = valid ? (p / a.hout) * a.stride - 1 : -1000;  // -1000: never inside
-                rx[q] = (p % a.hout) * a.stride - 1;
-            }
-            for (int kb = 0; kb < NKB; kb++, it++) {
-                const int s = it % S;
-                if (it >= S && !mb_wait(&empty[s], ((it / S) - 1) & 1, a.err, dead)) break;
-                uint8_t* stage = sa + (size_t)s * A_TILE;
-                const int t = 2 * kb + h8;  // this thread's tap (9: zero padding of K)
-                const int ty = t / 3, tx = t % 3;
-#pragma unroll
-                for (int q = 0; q < 8; q++) {
-                    const int iy = ry[q] + ty, ix = rx[q] + tx;
-                    const bool in = t < 9 && iy >= 0 && iy < a.hin && ix >= 0 && ix < a.hin;
-                    const uint4 v = in ? *(const uint4*)(ib + roff[q] + (iy * a.hin + ix) * 64 + c4 * 16)
-                                       : make_uint4(0u, 0u, 0u, 0u);
-                    *(uint4*)(stage + (size_t)(rsub + 16 * q) * SWZ + ((c8 ^ x) << 4)) = v;
-                }
-                fence_async_smem();
-                mb_arrive(&full[s]);
-            }
-            mb_arrive(&ifree[buf]);  // this thread is done with the tile's input buffer
-        }
-        (void)sa0;
-    } else if (warp == 4) {
-        // ---- MMA issue (lane 0); the weights by TMA first
-        if (lane == 0) {
-            mb_expect_tx(wfull, (unsigned)(NKB * W_TILE));
-            for (int kb = 0; kb < NKB; kb++) tma_2d(sw + kb * W_TILE, &tw, kb * 64, 0, wfull);
-            mb_wait(wfull, 0, a.err, dead);
-            const uint32_t idesc = idesc_bf16(128, 32);
-            int it = 0, nt = 0;
-            for (int tile = blockIdx.x; tile < ntiles && !dead; tile += gridDim.x, nt++) {
-                const int buf = nt & 1;
-                if (nt >= 2 && !mb_wait(&acce[buf], ((nt >> 1) - 1) & 1, a.err, dead)) break;
-                tc_fence_after();
-                for (int kb = 0; kb < NKB; kb++, it++) {
-                    const int s = it % S;
-                    if (!mb_wait(&full[s], (it / S) & 1, a.err, dead)) break;
-                    tc_fence_after();
-                    const uint64_t ad = sdesc(s32(sa + s * A_TILE), SWZ), bd = sdesc(s32(sw + kb * W_TILE), SWZ);
-#pragma unroll
-                    for (int k = 0; k < 4; k++) umma(tacc + (uint32_t)(buf * 32), ad + 2 * k, bd + 2 * k, idesc, (kb | k) != 0);
-                    umma_commit(&empty[s]);
-                }
-                umma_commit(&accf[buf]);
-            }
-        }
-        __syncwarp();
-    } else {
-        // ---- epilogue: bias, ReLU, bf16, one 64-byte output row per thread
-        const int g = warp & 3, r = g * 32 + lane;
-        int nt = 0;
-        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, nt++) {
-            const int buf = nt & 1;
-            const bool ok = mb_wait(&accf[buf], (nt >> 1) & 1, a.err, dead);
-            if (!__all_sync(0xffffffffu, ok)) {  // warp-uniform: tcgen05.ld is warp-collective
-                dead = true;
-                break;
-            }
-            tc_fence_after();
-            uint32_t r0[16], r1[16];
-            tm_ld16(tacc + ((uint32_t)(g * 32) << 16) + (uint32_t)(buf * 32), r0);
-            tm_ld16(tacc + ((uint32_t)(g * 32) << 16) + (uint32_t)(buf * 32 + 16), r1);
-            tc_fence_before();
-            mb_arrive(&acce[buf]);
-            const long long m = (long long)tile * 128 + r;
-            if (m < rows && !dead) {
-                const int b = (int)(m / pos), p = (int)(m % pos);
-                uint32_t o[16];
-#pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    o[j] = pack_bf16(fmaxf(__uint_as_float(r0[2 * j]) + sbias[2 * j], 0.0f),
-                                     fmaxf(__uint_as_float(r0[2 * j + 1]) + sbias[2 * j + 1], 0.0f));
-                    o[8 + j] = pack_bf16(fmaxf(__uint_as_float(r1[2 * j]) + sbias[16 + 2 * j], 0.0f),
-                                         fmaxf(__uint_as_float(r1[2 * j + 1]) + sbias[16 + 2 * j + 1], 0.0f));
-                }
-                uint4* dst = (uint4*)(a.out + (size_t)b * a.out_mb + (size_t)p * a.out_ld);
-#pragma unroll
-                for (int c = 0; c < 4; c++) dst[c] = make_uint4(o[4 * c], o[4 * c + 1], o[4 * c + 2], o[4 * c + 3]);
-            }
-        }
-    }
-    tc_fence_before();
-    __syncthreads();
-    if (warp == 4) tm_dealloc(tacc, 64);
-}
-
 // ---- host side: tensor maps
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -729,22 +536,8 @@ int nn_conv(int layer, const void* in, int in_mb, const void* W, const float* bi
     a.err = err;
     const long long rows = (long long)nmb * a.hout * a.hout;
     const int ntiles = (int)((rows + 127) / 128);
-    if (cin == 32) {  // layers 2-4: the input staged in shared memory by bulk copies
-        const int pos = a.hout * a.hout;
-        const size_t sm2 = conv_s_smem(pos, in_mb);
-        if (sm2 > (size_t)227 * 1024) return (int)cudaErrorInvalidValue;
-        cudaError_t e2 = cudaFuncSetAttribute(k_nn_conv_s, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
-        if (e2 != cudaSuccess) return (int)e2;
-        int per_sm = 0;
-        e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_nn_conv_s, CV_THREADS, sm2);
-        if (e2 != cudaSuccess) return (int)e2;
-        per_sm = per_sm < 1 ? 1 : (per_sm > 2 ? 2 : per_sm);  // 64 TMEM columns each
-        const int cap2 = num_sms() * per_sm;
-        k_nn_conv_s<<<ntiles < cap2 ? ntiles : cap2, CV_THREADS, sm2, (cudaStream_t)stream>>>(tw, a);
-        return (int)cudaGetLastError();
-    }
-    const size_t smem = ConvCfg<2>::smem();
-    const void* fn = (const void*)k_nn_conv<2>;
+    const size_t smem = cin == 2 ? ConvCfg<2>::smem() : ConvCfg<32>::smem();
+    const void* fn = cin == 2 ? (const void*)k_nn_conv<2> : (const void*)k_nn_conv<32>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
     // persistent CTAs: as many per SM as shared memory allows (64 TMEM columns each), at most 2
@@ -753,7 +546,10 @@ int nn_conv(int layer, const void* in, int in_mb, const void* W, const float* bi
     per_sm = per_sm < 1 ? 1 : (per_sm > 2 ? 2 : per_sm);
     const int cap = num_sms() * per_sm;
     const int grid = ntiles < cap ? ntiles : cap;
-    k_nn_conv<2><<<grid, CV_THREADS, smem, (cudaStream_t)stream>>>(tw, a);
+    if (cin == 2)
+        k_nn_conv<2><<<grid, CV_THREADS, smem, (cudaStream_t)stream>>>(tw, a);
+    else
+        k_nn_conv<32><<<grid, CV_THREADS, smem, (cudaStream_t)stream>>>(tw, a);
     return (int)cudaGetLastError();
 }
 
