@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(64 * NM) kb_residual(BatchLaunch b) {
 // ---- out-of-place deblock (deblock_tile), TW luma columns per tile
 template <int TW>
 __global__ void __launch_bounds__(128) kb_deblock(BatchLaunch b) {
-    __shared__ uint8_t tile[(16 + 8) * (TW + 8)];
+    __shared__ __align__(16) uint8_t tile[(16 + 8) * (TW + 8)];
     const int* st = b.start + BS_DEBLOCK * (b.nclips + 1);
     const int c = batch_clip(st, b.nclips, blockIdx.x);
     const BatchClip& k = b.clips[c];

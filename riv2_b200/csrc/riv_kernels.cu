@@ -882,9 +882,13 @@ __device__ __forceinline__ void deblock_tile(const uint8_t* __restrict__ src, ui
     const int ry0 = max(Y0 - 4, 0), ry1 = min(Y1 + 4, h), cx0 = max(X0 - 4, 0), cx1 = min(X1 + 4, w);
     const int TS = TW + 8, oy = Y0 - 4, ox = X0 - 4;  // tile row stride and origin
     const int nrow = ry1 - ry0, ncol = cx1 - cx0;
-    for (int i = tid; i < nrow * ncol; i += nthr) {
-        const int r = i / ncol, c = i - r * ncol;
-        tile[(ry0 + r - oy) * TS + cx0 + c - ox] = pl[(size_t)(ry0 + r) * w + cx0 + c];
+    // 32-bit words: cx0, cx1, w and the tile's row stride and origin are multiples of 4 (tile
+    // widths and plane widths are multiples of 8), and `tile` is 16-byte aligned
+    const int ncw = ncol >> 2;
+    for (int i = tid; i < nrow * ncw; i += nthr) {
+        const int r = i / ncw, c = i - r * ncw;
+        *(uint32_t*)(tile + (ry0 + r - oy) * TS + cx0 + 4 * c - ox) =
+            *(const uint32_t*)(pl + (size_t)(ry0 + r) * w + cx0 + 4 * c);
     }
     group_sync(bar, nthr);
     // vertical edges x = k*g (1 <= k < w/g) with X0 <= x <= X1, on every loaded row
@@ -920,10 +924,10 @@ __device__ __forceinline__ void deblock_tile(const uint8_t* __restrict__ src, ui
         for (int q = 1; q < 7; q++) sp[q * TS] = (uint8_t)px[q];
     }
     group_sync(bar, nthr);
-    const int ow = X1 - X0;
-    for (int i = tid; i < g * ow; i += nthr) {
-        const int r = i / ow, c = i - r * ow;
-        po[(size_t)(Y0 + r) * w + X0 + c] = tile[(Y0 + r - oy) * TS + X0 + c - ox];
+    const int oww = (X1 - X0) >> 2;
+    for (int i = tid; i < g * oww; i += nthr) {
+        const int r = i / oww, c = i - r * oww;
+        *(uint32_t*)(po + (size_t)(Y0 + r) * w + X0 + 4 * c) = *(const uint32_t*)(tile + (Y0 + r - oy) * TS + X0 + 4 * c - ox);
     }
 }
 
@@ -3258,7 +3262,7 @@ template <int TW>
 __global__ void __launch_bounds__(128) k_deblock_tiled(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, int W,
                                                        int H, int BW, int E, int I, int Hv, const uint8_t* mask,
                                                        int ntiles_y) {
-    __shared__ uint8_t tile[(16 + 8) * (TW + 8)];
+    __shared__ __align__(16) uint8_t tile[(16 + 8) * (TW + 8)];
     int t = blockIdx.x;
     int plane = t < ntiles_y ? 0 : (t - ntiles_y) % 2 + 1;
     if (plane > 0) t = (t - ntiles_y) / 2;
