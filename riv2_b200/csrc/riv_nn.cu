@@ -21,6 +21,7 @@
 #include <cudaTypedefs.h>
 
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
@@ -436,7 +437,182 @@ __global__ void __launch_bounds__(CV_THREADS, 2) k_nn_conv(const __grid_constant
     if (warp == 4) tm_dealloc(tacc, 64);
 }
 
+// =====================================================================================
+// Implicit-GEMM convolution with the operand loaded by the TMA's im2col mode (32 channels in)
+// =====================================================================================
+// The input is a 4-D tensor {C = 32, W = hin, H = hin, N = MBs} (NHWC per MB, MBs back to
+// back).  Its im2col tensor map walks output positions in (MB, y, x) order: the bounding box of
+// a layer with padding 1 and a 3x3 filter spans base positions -1 .. hin - 2 in x and y
+// (corners -1, -1), stepped by the layer's stride, and wraps to the next MB at its end.  One
+// load fetches the 32 channels of 128 consecutive output positions for one tap (im2col
+// offsets kx, ky added to every base position; positions outside the MB read zeros) as a
+// 128 x 64-byte K-major tile in the 64-byte swizzle, so a tile's operand is nine such loads
+// and nothing is gathered by threads.  The MMA for tap t reads that tile as A (K = 32: two
+// instructions) and the weights' columns 32t .. 32t + 31 as B, in the same K order as the
+// k-block kernel above, so both kernels accumulate identically.
+// Warp roles (192 threads): warp 0 lane 0 issues the loads (weights first), warp 1 holds the
+// tensor memory and its lane 0 the MMAs, warps 2-5 run the epilogue of k_nn_conv.
+constexpr int CI_THREADS = 192;
+constexpr int CI_STAGES = 10;       // ring of tap tiles
+constexpr int CI_TAP = 128 * 64;    // one tap tile: 128 positions x 32 channels bf16
+constexpr int CI_WKB = 32 * 128;    // one weight k-block: 32 rows x 64 elements, 128-byte swizzle
+constexpr size_t ci_smem() { return 1024 + 5 * (size_t)CI_WKB + (size_t)CI_STAGES * CI_TAP + 512; }
+
+__device__ __forceinline__ void tma_im2col_4d(void* dst, const CUtensorMap* map, int c, int w, int h, int n,
+                                              uint16_t off_w, uint16_t off_h, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.im2col.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6], {%7, %8};" ::"r"(s32(dst)),
+        "l"((uint64_t)map), "r"(c), "r"(w), "r"(h), "r"(n), "r"(s32(bar)), "h"(off_w), "h"(off_h)
+        : "memory");
+}
+
+__global__ void __launch_bounds__(CI_THREADS, 2)
+    k_nn_conv_i2c(const __grid_constant__ CUtensorMap tw, const __grid_constant__ CUtensorMap tin, ConvArgs a) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* sm = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* sw = sm;                 // 5 weight k-blocks
+    uint8_t* sa = sm + 5 * CI_WKB;    // CI_STAGES tap tiles
+    uint64_t* wfull = (uint64_t*)(sa + CI_STAGES * CI_TAP);
+    uint64_t* full = wfull + 1;
+    uint64_t* empty = full + CI_STAGES;
+    uint64_t* accf = empty + CI_STAGES;
+    uint64_t* acce = accf + 2;
+    uint32_t* slot = (uint32_t*)(acce + 2);
+    float* sbias = (float*)(slot + 4);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        mb_init(wfull, 1);
+        for (int k = 0; k < CI_STAGES; k++) {
+            mb_init(&full[k], 1);
+            mb_init(&empty[k], 1);
+        }
+        for (int k = 0; k < 2; k++) {
+            mb_init(&accf[k], 1);
+            mb_init(&acce[k], 128);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (tid < 32) sbias[tid] = a.bias[tid];
+    if (warp == 1) tm_alloc(slot, 64);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tacc = *slot;
+    bool dead = false;
+    const int pos = a.hout * a.hout;
+    const long long rows = (long long)a.nmb * pos;
+    const int ntiles = (int)((rows + 127) / 128);
+
+    if (warp == 0) {
+        // ---- loads: the weights, then nine tap tiles per output tile
+        if (lane == 0) {
+            mb_expect_tx(wfull, (unsigned)(5 * CI_WKB));
+            for (int kb = 0; kb < 5; kb++) tma_2d(sw + kb * CI_WKB, &tw, kb * 64, 0, wfull);
+            int it = 0;
+            for (int tile = blockIdx.x; tile < ntiles && !dead; tile += gridDim.x) {
+                const long long m0 = (long long)tile * 128;
+                const int n = (int)(m0 / pos), p = (int)(m0 % pos);
+                const int w0 = (p % a.hout) * a.stride - 1, h0 = (p / a.hout) * a.stride - 1;
+                for (int t = 0; t < 9; t++, it++) {
+                    const int s = it % CI_STAGES;
+                    if (it >= CI_STAGES && !mb_wait(&empty[s], ((it / CI_STAGES) - 1) & 1, a.err, dead)) break;
+                    mb_expect_tx(&full[s], (unsigned)CI_TAP);
+                    tma_im2col_4d(sa + s * CI_TAP, &tin, 0, w0, h0, n, (uint16_t)(t % 3), (uint16_t)(t / 3), &full[s]);
+                }
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ---- MMA issue
+        if (lane == 0 && mb_wait(wfull, 0, a.err, dead)) {
+            const uint32_t idesc = idesc_bf16(128, 32);
+            int it = 0, nt = 0;
+            for (int tile = blockIdx.x; tile < ntiles && !dead; tile += gridDim.x, nt++) {
+                const int buf = nt & 1;
+                if (nt >= 2 && !mb_wait(&acce[buf], ((nt >> 1) - 1) & 1, a.err, dead)) break;
+                tc_fence_after();
+                for (int t = 0; t < 9; t++, it++) {
+                    const int s = it % CI_STAGES;
+                    if (!mb_wait(&full[s], (it / CI_STAGES) & 1, a.err, dead)) break;
+                    tc_fence_after();
+                    const uint64_t ad = sdesc(s32(sa + s * CI_TAP), 64);
+                    const uint64_t bd = sdesc(s32(sw + (t >> 1) * CI_WKB), 128) + (uint64_t)((t & 1) * 4);
+                    umma(tacc + (uint32_t)(buf * 32), ad, bd, idesc, t != 0);
+                    umma(tacc + (uint32_t)(buf * 32), ad + 2, bd + 2, idesc, 1);
+                    umma_commit(&empty[s]);
+                }
+                umma_commit(&accf[buf]);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---- epilogue: bias, ReLU, bf16, one 64-byte output row per thread
+        const int g = warp & 3, r = g * 32 + lane;
+        int nt = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, nt++) {
+            const int buf = nt & 1;
+            const bool ok = mb_wait(&accf[buf], (nt >> 1) & 1, a.err, dead);
+            if (!__all_sync(0xffffffffu, ok)) {  // warp-uniform: tcgen05.ld is warp-collective
+                dead = true;
+                break;
+            }
+            tc_fence_after();
+            uint32_t r0[16], r1[16];
+            tm_ld16(tacc + ((uint32_t)(g * 32) << 16) + (uint32_t)(buf * 32), r0);
+            tm_ld16(tacc + ((uint32_t)(g * 32) << 16) + (uint32_t)(buf * 32 + 16), r1);
+            tc_fence_before();
+            mb_arrive(&acce[buf]);
+            const long long m = (long long)tile * 128 + r;
+            if (m < rows && !dead) {
+                const int b = (int)(m / pos), p = (int)(m % pos);
+                uint32_t o[16];
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    o[j] = pack_bf16(fmaxf(__uint_as_float(r0[2 * j]) + sbias[2 * j], 0.0f),
+                                     fmaxf(__uint_as_float(r0[2 * j + 1]) + sbias[2 * j + 1], 0.0f));
+                    o[8 + j] = pack_bf16(fmaxf(__uint_as_float(r1[2 * j]) + sbias[16 + 2 * j], 0.0f),
+                                         fmaxf(__uint_as_float(r1[2 * j + 1]) + sbias[16 + 2 * j + 1], 0.0f));
+                }
+                uint4* dst = (uint4*)(a.out + (size_t)b * a.out_mb + (size_t)p * a.out_ld);
+#pragma unroll
+                for (int c = 0; c < 4; c++) dst[c] = make_uint4(o[4 * c], o[4 * c + 1], o[4 * c + 2], o[4 * c + 3]);
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) tm_dealloc(tacc, 64);
+}
+
 // ---- host side: tensor maps
+PFN_cuTensorMapEncodeIm2col_v12000 encode_im2col_fn() {
+    static PFN_cuTensorMapEncodeIm2col_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeIm2col", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeIm2col_v12000)p;
+    });
+    return fn;
+}
+
+// im2col map over nmb MBs of hin x hin x 32 bf16 (in_mb elements apart): 128 positions x 32
+// channels per load, 64-byte swizzle, base positions -1 .. hin - 2 stepped by `stride`.
+bool make_im2col_map(CUtensorMap* m, const void* base, int hin, int in_mb, int nmb, int stride) {
+    auto fn = encode_im2col_fn();
+    if (!fn || ((uintptr_t)base & 15) || (in_mb * 2) % 16) return false;
+    cuuint64_t dims[4] = {32, (cuuint64_t)hin, (cuuint64_t)hin, (cuuint64_t)nmb};
+    cuuint64_t strides[3] = {64, (cuuint64_t)hin * 64, (cuuint64_t)in_mb * 2};
+    int lower[2] = {-1, -1}, upper[2] = {-1, -1};
+    cuuint32_t es[4] = {1, (cuuint32_t)stride, (cuuint32_t)stride, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, lower, upper, 32, 128, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     static std::once_flag once;
@@ -536,6 +712,18 @@ int nn_conv(int layer, const void* in, int in_mb, const void* W, const float* bi
     a.err = err;
     const long long rows = (long long)nmb * a.hout * a.hout;
     const int ntiles = (int)((rows + 127) / 128);
+    const char* gv = getenv("RIV_CONV_GATHER");
+    if (cin == 32 && !(gv && gv[0] == '1')) {
+        CUtensorMap tin;
+        if (!make_im2col_map(&tin, in, a.hin, in_mb, nmb, a.stride)) return (int)cudaErrorInvalidValue;
+        const size_t smem = ci_smem();
+        cudaError_t e = cudaFuncSetAttribute(k_nn_conv_i2c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+        const int cap = num_sms() * 2;
+        const int grid = ntiles < cap ? ntiles : cap;
+        k_nn_conv_i2c<<<grid, CI_THREADS, smem, (cudaStream_t)stream>>>(tw, tin, a);
+        return (int)cudaGetLastError();
+    }
     const size_t smem = cin == 2 ? ConvCfg<2>::smem() : ConvCfg<32>::smem();
     const void* fn = cin == 2 ? (const void*)k_nn_conv<2> : (const void*)k_nn_conv<32>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -185,6 +185,42 @@ def test_front_equals_features_then_conv1():
         assert np.abs(q - want).max() <= 2 ** -7 * max(1.0, np.abs(want).max())
 
 
+@pytest.mark.parametrize("layer,nmb", [(2, 1), (2, 37), (3, 300), (4, 257), (2, 1000), (3, 4), (4, 8160)])
+def test_conv_layers_match_oracle(layer, nmb, monkeypatch):
+    """conv2-4 (im2col-TMA operand) against the float64 oracle's convolution of the same bf16
+    input, with MB counts whose tiles end mid-MB and a ragged last tile; conv4 writes into
+    fc1's input rows (320 columns per MB), leaving the predictor columns alone.  The k-block
+    gather kernel (same K order of the f32 accumulation) gives the same bits."""
+    from riv2_b200 import proposal as P
+    hin, hout = {2: (12, 6), 3: (6, 6), 4: (6, 3)}[layer]
+    net = P.ProposalNet(_params())
+    rng = np.random.default_rng(100 * layer + nmb)
+    x = np.maximum(rng.standard_normal((nmb, hin, hin, 32)), 0.0) * rng.uniform(0.5, 2.0, (nmb, 1, 1, 1))
+    xin = _bf(x.reshape(nmb, hin * hin * 32))
+    out_mb = 320 if layer == 4 else hout * hout * 32
+    L = P.lib()
+
+    def run():
+        out = torch.full((nmb, out_mb), 3.0, dtype=torch.bfloat16, device="cuda")
+        assert L.riv_nn_conv(layer, xin.data_ptr(), hin * hin * 32, net.w(f"w{layer}").data_ptr(),
+                             net.bias(f"b{layer}").data_ptr(), out.data_ptr(), out_mb, 32, nmb, net.err.data_ptr(),
+                             None) == 0
+        torch.cuda.synchronize()
+        net.check()
+        return out.float().cpu().numpy()
+
+    got = run()
+    Pm = PO.unpack(net.params_numpy(), _layout())
+    cols = PO.im2col(xin.float().cpu().numpy().astype(np.float64).reshape(nmb, hin, hin, 32), layer)
+    want = PO.bf16(np.maximum(cols @ Pm[f"w{layer}"].T + Pm[f"b{layer}"], 0.0)).reshape(nmb, hout * hout * 32)
+    q = got[:, :hout * hout * 32]
+    assert np.abs(q - want).max() <= 2 ** -7 * max(1.0, np.abs(want).max())
+    assert (q != want).mean() < 0.02
+    assert (got[:, hout * hout * 32:] == 3.0).all()
+    monkeypatch.setenv("RIV_CONV_GATHER", "1")
+    assert np.array_equal(run(), got)
+
+
 def test_forward_matches_oracle():
     from riv2_b200 import proposal as P
     p = _params()
