@@ -11,14 +11,17 @@
 
 namespace riv {
 
-static uint8_t g_zero_prob[65536];
-static uint16_t g_next[2][65536];  // BinProb state after a 0 / a 1
+// ceil(2^32 / d) for d = 1 .. 510 (0 for d = 0): (zeros << 8) / (zeros + ones) of every
+// BinProb state by one multiply (exact for dividends below 2^16, checked for all 65536 states
+// by entropy_init)
+static uint32_t g_div_m[512];
 static uint64_t g_rcp_m[256];
 static uint32_t g_rcp_s[256];
 static std::once_flag g_once;
 
-// BinProb update after one bit (com/rans.rs:73-84); tabulated in g_next.
-static uint16_t observe_calc(uint16_t packed, bool bit) {
+// BinProb update after one bit (com/rans.rs:73-84).  Computed, not tabulated: a state moves
+// by 256 entries per update, so a 65536-entry table misses the L1 cache on nearly every symbol.
+static inline uint16_t observe_calc(uint16_t packed, bool bit) {
     uint16_t rot = bit ? (uint16_t)((packed << 8) | (packed >> 8)) : packed;
     uint32_t sum = (uint32_t)rot + 0x100u;
     uint16_t upd = (uint16_t)sum;
@@ -29,19 +32,24 @@ static uint16_t observe_calc(uint16_t packed, bool bit) {
     return bit ? (uint16_t)((upd << 8) | (upd >> 8)) : upd;
 }
 
+static inline uint8_t prob_zero(const BinProb& b) {
+    const uint32_t z = (uint32_t)b.packed >> 8, d = z + (b.packed & 0xffu);
+    const uint8_t p = (uint8_t)(((uint64_t)(z << 8) * g_div_m[d]) >> 32);
+    return p ? p : 1;
+}
+static inline void observe(BinProb& b, bool bit) { b.packed = observe_calc(b.packed, bit); }
+
 void entropy_init() {
     std::call_once(g_once, [] {
-        // BinProb zero-probability table (com/rans.rs:30-44): p = zeros*256/(zeros+ones)
-        // truncated to u8, with 0 mapped to 1.
-        g_zero_prob[0] = 1;
-        for (int i = 1; i < 65536; i++) {
-            int zeros = i >> 8, ones = i & 0xff;
-            uint8_t p = (uint8_t)((zeros << 8) / (zeros + ones));
-            g_zero_prob[i] = p ? p : 1;
-        }
-        for (uint32_t st = 0; st < 65536; st++) {
-            g_next[0][st] = observe_calc((uint16_t)st, false);
-            g_next[1][st] = observe_calc((uint16_t)st, true);
+        // BinProb zero probability (com/rans.rs:30-44): p = zeros*256/(zeros+ones) truncated
+        // to u8, with 0 mapped to 1; the division by the reciprocal multiply of prob_zero
+        for (uint32_t d = 1; d < 512; d++) g_div_m[d] = (uint32_t)((((uint64_t)1 << 32) + d - 1) / d);
+        for (int i = 0; i < 65536; i++) {
+            const int zeros = i >> 8, ones = i & 0xff;
+            const uint8_t want = i == 0 ? 1 : ((uint8_t)((zeros << 8) / (zeros + ones)) ? (uint8_t)((zeros << 8) / (zeros + ones)) : 1);
+            BinProb b;
+            b.packed = (uint16_t)i;
+            if (prob_zero(b) != want) std::abort();  // cannot happen: the reciprocals are exact here
         }
         // Exact reciprocals for r / f, f in [1,255], r < 2^32 (round-up multiplier with
         // s = 32 + ceil(log2 f) fraction bits).
@@ -56,8 +64,6 @@ void entropy_init() {
     });
 }
 
-static inline uint8_t prob_zero(const BinProb& b) { return g_zero_prob[b.packed]; }
-static inline void observe(BinProb& b, bool bit) { b.packed = g_next[bit][b.packed]; }
 
 static const int BATCH = 16386;  // com/rans.rs:201
 // The parallel coefficient coder takes frames of 16K to 2M coded coefficients: below, its
@@ -72,11 +78,11 @@ RansWriter::RansWriter(std::vector<uint8_t>* sink, const BatchSubmit* submit)
 inline void RansWriter::put(bool bit, BinProb& ctx) {
     uint8_t p = prob_zero(ctx);
     observe(ctx, bit);
-    if (sp_ == 0) drain();
+    if (__builtin_expect(sp_ == 0, 0)) drain();
     stack_[--sp_] = (uint16_t)(p | (bit ? 0x100 : 0));
 }
 inline void RansWriter::put_bypass(bool bit) {
-    if (sp_ == 0) drain();
+    if (__builtin_expect(sp_ == 0, 0)) drain();
     stack_[--sp_] = (uint16_t)(128 | (bit ? 0x100 : 0));
 }
 
@@ -535,6 +541,14 @@ static inline int mv_class(unsigned mag) {  // res/mv_rans.rs:80-86
 }
 
 void MvCoder::reset() { *this = MvCoder(); }
+void MvCoder::reset_history() {
+    cands_.clear();
+    cnt_.clear();
+    listed_.clear();
+    active_.clear();
+    total_ = 0;
+}
+void MvCoder::reset_models() { c_ = Models(); }
 
 template <class W>
 static void enc_class(W& w, BinProb* ctx, int cls) {
@@ -664,12 +678,43 @@ static void check_subpels(const std::vector<MvCodedBlock>& blocks) {
 void MvCoder::encode_frame(const std::vector<MvCodedBlock>& blocks, int bw, std::vector<uint8_t>& out,
                            const BatchSubmit* submit) {
     out.clear();
+    MvSymbols syms;
+    prepare(blocks, bw, syms);
+    code(syms, out, submit);
+}
+
+namespace {
+// Symbols of one block at most: skip, NEW, four base bits, the hit flag, then either four index
+// bits or two components of at most 4 class + 1 sign + 9 magnitude bits, and two subpel flags.
+constexpr size_t MV_MAX_SYMS_PER_BLOCK = 40;
+struct MvRawSink {  // lists symbols into a buffer sized for the frame
+    const BinProb* base;
+    uint16_t* p;
+    void put(bool bit, const BinProb& m) { *p++ = (uint16_t)((&m - base) | (bit ? 0x8000 : 0)); }
+};
+}  // namespace
+
+void MvCoder::prepare(const std::vector<MvCodedBlock>& blocks, int bw, MvSymbols& syms) {
     check_subpels(blocks);
-    RansWriter w(&out, submit);
     const std::vector<uint8_t> hits = hit_flags(blocks);
-    emit(w, blocks, hits, bw, 0, blocks.size());
-    w.finish();
+    const size_t need = blocks.size() * MV_MAX_SYMS_PER_BLOCK;
+    if (syms.cap < need) {
+        syms.s.reset(new uint16_t[need]);
+        syms.cap = need;
+    }
+    MvRawSink k{&c_.skip, syms.s.get()};
+    emit(k, blocks, hits, bw, 0, blocks.size());
+    syms.n = (size_t)(k.p - syms.s.get());
     update(blocks);
+}
+
+void MvCoder::code(const MvSymbols& syms, std::vector<uint8_t>& out, const BatchSubmit* submit) {
+    out.clear();
+    RansWriter w(&out, submit);
+    BinProb* m = &c_.skip;
+    const uint16_t* s = syms.s.get();
+    for (size_t i = 0; i < syms.n; i++) w.put((s[i] >> 15) != 0, m[s[i] & 0x7fff]);
+    w.finish();
 }
 
 namespace {
@@ -923,11 +968,14 @@ void compute_delta_bias(const std::vector<std::pair<int8_t, int8_t>>& d, int8_t&
         hx[p.first + 128]++;
         hy[p.second + 128]++;
     }
+    int vs[256], nv = 0;  // the occupied bins, in increasing order
+    for (int v = 0; v < 256; v++)
+        if (hx[v] || hy[v]) vs[nv++] = v;
     int64_t bzx = -1, bzy = -1, bcx = INT64_MAX, bcy = INT64_MAX;
     for (int b = -24; b <= 24; b++) {
         int64_t zx = 0, cx = 0, zy = 0, cy = 0;
-        for (int v = 0; v < 256; v++) {
-            if (!hx[v] && !hy[v]) continue;
+        for (int k = 0; k < nv; k++) {
+            const int v = vs[k];
             int a = std::min(std::max(v - 128 - b, -128), 127);
             // `adj.abs() as i32` on i8 wraps at -128 in the release build.
             int64_t ab = a == -128 ? -128 : std::abs(a);

@@ -7,6 +7,7 @@
 #include <deque>
 #include <functional>
 #include <future>
+#include <memory>
 #include <tuple>
 #include <unordered_map>
 #include <vector>
@@ -38,7 +39,8 @@ public:
     void finish();
 
 private:
-    void drain();
+    // out of line and cold: inlined into put it costs the symbol loop its registers
+    __attribute__((noinline, cold)) void drain();
     std::vector<uint8_t>* sink_;
     std::vector<uint16_t> stack_;  // entry = p | bit << 8; stack_[BATCH-1] is the oldest
     int sp_;
@@ -96,9 +98,24 @@ struct MvCodedBlock {  // res/mv_rans.rs:65-78
     bool skip;
 };
 
+// A frame's MV symbols in stream order (model index | bit << 15), as MvCoder::prepare lists them.
+struct MvSymbols {
+    std::unique_ptr<uint16_t[]> s;
+    size_t n = 0, cap = 0;
+};
+
 class MvCoder {  // res/mv_rans/encoder.rs:60-412
 public:
     void reset();
+    // The coder in two stages that touch disjoint state, so that two threads can run them on
+    // consecutive frames: prepare lists a frame's (model, bit) symbols, which depend on the
+    // candidate history but on no adaptive model, then advances the history (encoder.rs:370-412);
+    // code runs the adaptive models over a listed frame and codes it.  prepare and code each in
+    // frame order give encode_frame's bytes.  prepare throws where encode_frame does.
+    void prepare(const std::vector<MvCodedBlock>& blocks, int bw, MvSymbols& syms);
+    void code(const MvSymbols& syms, std::vector<uint8_t>& out, const BatchSubmit* submit = nullptr);
+    void reset_history();  // prepare's state, as reset() leaves it
+    void reset_models();   // code's state, as reset() leaves it
     // Throws std::runtime_error on a NEW block with a raw -1/2 subpel (the reference panics).
     // submit (nullable): full rANS batches are coded there while the context modelling goes on
     // (same bytes; see RansWriter).

@@ -10,6 +10,9 @@
 // reitero_video/reitero_encode/src/).
 #include <cuda_runtime.h>
 #include <dlfcn.h>
+#include <sys/resource.h>
+#include <sys/syscall.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <array>
@@ -51,10 +54,18 @@ struct CudaError {
         if (e_ != cudaSuccess) throw CudaError{e_, #x};         \
     } while (0)
 
+constexpr int BULK_NICE = 5;  // the coefficient coders' workers, below the serial stages
+
 class ThreadPool {
 public:
-    explicit ThreadPool(unsigned n) {
-        for (unsigned i = 0; i < n; i++) workers_.emplace_back([this] { run(); });
+    // nice > 0: the workers run below the process's other threads (bulk work that must not
+    // preempt the serial stages of the pipeline; a refused priority change is ignored)
+    explicit ThreadPool(unsigned n, int nice = 0) {
+        for (unsigned i = 0; i < n; i++)
+            workers_.emplace_back([this, nice] {
+                if (nice > 0) (void)setpriority(PRIO_PROCESS, (id_t)syscall(SYS_gettid), nice);
+                run();
+            });
     }
     ~ThreadPool() {
         {
@@ -64,12 +75,14 @@ public:
         cv_.notify_all();
         for (auto& t : workers_) t.join();
     }
-    std::future<void> submit(std::function<void()> f) {
+    // urgent: ahead of every queued job (latency-critical work behind bulk work)
+    std::future<void> submit(std::function<void()> f, bool urgent = false) {
         auto task = std::make_shared<std::packaged_task<void()>>(std::move(f));
         std::future<void> fut = task->get_future();
         {
             std::lock_guard<std::mutex> g(m_);
-            q_.push_back([task] { (*task)(); });
+            if (urgent) q_.push_front([task] { (*task)(); });
+            else q_.push_back([task] { (*task)(); });
         }
         cv_.notify_one();
         return fut;
@@ -341,8 +354,14 @@ struct Job {
     int prev_buf = 0;
     int ck = 0;             // double-buffer parity of the frame's buffers
     uint32_t count = 0;
-    std::future<void> fut, fut_mv;
+    std::future<void> fut, fut_mv, fut_prep;
     std::vector<uint8_t> res_bytes, mv_bytes;
+    std::vector<MvCodedBlock> mv_blocks;  // the P-frame's MV coder input
+    // host timeline (milliseconds, steady clock), kept when the encoder traces: submitted; MV
+    // input assembly started / done; MV listing started / done; MV coding started / done; DCT
+    // coding started / done; written
+    double tr[10] = {0};
+    MvSymbols mv_syms;
     int8_t bias[2] = {0, 0};
     riv_frame_stats stats{};
     float times[NSTAGE + 1] = {0};
@@ -401,13 +420,19 @@ struct riv_encoder {
     MvCoder mvc;
     std::shared_ptr<ThreadPool> pool;       // coefficient modelling (shared by the clips of a batch)
     std::unique_ptr<ThreadPool> mv_exec;    // one thread: MV coding strictly in frame order
+    std::unique_ptr<ThreadPool> mv_prep;    // one thread: MV symbol listing strictly in frame order
+    std::shared_ptr<ThreadPool> mv_pool;    // rANS batches of the MV coder (shared by the clips of a batch)
     std::shared_ptr<ThreadPool> rans_pool;  // coefficient-coder jobs (never wait)
     BatchSubmit rans_submit;
+    BatchSubmit mv_submit;  // mv_pool: the MV coder is serial across frames, its batches wait for no bulk work
     int rans_parts = 1;  // threads that code one frame's coefficients: rans_pool's and the caller
-    int mv_parts = 1;    // threads that model one frame's MVs (1: the sequential coder)
     bool draining = false;  // inside drain_all: the newest frame is coded by rans_parts threads
     bool batched = false;   // a clip of a riv_batch: only the batch submits its frames
     double host_ms[6] = {0};  // submit, retire, mv coding, dct coding (summed), write, blocked
+    // RIV_TRACE=<file>: every written frame's host timeline (Job::tr), appended to the file as
+    // CSV when the encoder is freed
+    std::string trace_path;
+    std::vector<std::array<double, 11>> trace;
     std::mutex stat_mu;
     float last_times[NSTAGE + 1] = {0};
     bool have_times = false;
@@ -648,14 +673,18 @@ static void setup_device(riv_encoder* e) {
         e->sadtab.alloc((size_t)N * sad_table_stride(c.search_range) * sizeof(uint16_t));
     unsigned nt = c.entropy_threads;
     if (nt == 0) nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency() > 1 ? std::thread::hardware_concurrency() - 1 : 1u));
-    e->pool.reset(new ThreadPool(nt));
+    e->pool.reset(new ThreadPool(nt, BULK_NICE));
     e->mv_exec.reset(new ThreadPool(1));
-    e->rans_pool.reset(new ThreadPool(std::max(2u, nt / 2)));
+    e->mv_prep.reset(new ThreadPool(1));
+    e->mv_pool.reset(new ThreadPool(2));
+    e->rans_pool.reset(new ThreadPool(std::max(2u, nt / 2), BULK_NICE));
     e->rans_parts = (int)std::max(2u, nt / 2) + 1;
-    if (const char* v = getenv("RIV_MV_PARTS")) e->mv_parts = std::max(1, std::min(8, atoi(v)));
+    if (const char* v = getenv("RIV_TRACE")) e->trace_path = v;
     {
         ThreadPool* rp = e->rans_pool.get();
         e->rans_submit = [rp](std::function<void()> f) { return rp->submit(std::move(f)); };
+        ThreadPool* mp = e->mv_pool.get();
+        e->mv_submit = [mp](std::function<void()> f) { return mp->submit(std::move(f)); };
     }
     CK(cudaStreamSynchronize(e->S));
 }
@@ -1094,6 +1123,70 @@ static void search_stats(const riv_encoder* e, const MbOut* mb, const int8_t* pr
     S.rdo_avg_coded_cost = S.rdo_blocks_evaluated ? tot_coded / (double)S.rdo_blocks_evaluated : 0.0;
 }
 
+// The MV coder's input of a P-frame (MvCodedBlock assembly, enc/encoder.rs:774-818) after the
+// delta bias (compute_delta_bias_for_new, enc/encoder.rs:984-1048), and the frame's MV
+// statistics; none of it depends on the coder's state carried across frames.
+static void assemble_mv(riv_encoder* e, Job& j, const uint32_t* side, int N, const std::vector<MbOut>* mbh,
+                        const std::vector<int8_t>* prevh) {
+    double m0 = now_ms();
+    j.tr[1] = m0;
+    riv_frame_stats& S = j.stats;
+    std::vector<std::pair<int8_t, int8_t>> nd;
+    nd.reserve(N);
+    for (int i = 0; i < N; i++)
+        if ((side[i] & 7) == M_NEW) nd.emplace_back((int8_t)(side[i] >> 8), (int8_t)(side[i] >> 16));
+    compute_delta_bias(nd, j.bias[0], j.bias[1]);
+    // MvCodedBlock assembly (enc/encoder.rs:774-818)
+    std::vector<MvCodedBlock>& blocks = j.mv_blocks;
+    blocks.resize(N);
+    for (int i = 0; i < N; i++) {
+        uint32_t v = side[i];
+        MvCodedBlock& b = blocks[i];
+        b.mode = (uint8_t)(v & 7);
+        b.new_base = (uint8_t)((v >> 3) & 7);
+        b.skip = (v >> 24) & 1;
+        b.dx = b.dy = 0;
+        b.spx = b.spy = SP_ZERO;
+        if (b.mode == M_NEW) {
+            const int rdx = (int8_t)(v >> 8), rdy = (int8_t)(v >> 16);
+            b.dx = (int8_t)std::min(std::max(rdx - j.bias[0], -128), 127);
+            b.dy = (int8_t)std::min(std::max(rdy - j.bias[1], -128), 127);
+            b.spx = ((v >> 6) & 1) ? SP_PLUS : SP_ZERO;
+            b.spy = ((v >> 7) & 1) ? SP_PLUS : SP_ZERO;
+            S.mv_new_blocks++;
+            S.mv_new_base_counts[std::min<int>(b.new_base, 4)]++;
+            // delta statistics before and after the bias (enc/encoder.rs:768-800, 873-884)
+            if (rdx == 0 && rdy == 0) {
+                S.mv_new_zero_pre_bias++;
+                S.mv_zero_delta_blocks++;
+            }
+            const double fx = (double)b.dx, fy = (double)b.dy, mag = std::sqrt(fx * fx + fy * fy);
+            S.mv_new_delta_mag_sum += mag;
+            S.mv_new_delta_mag_sq_sum += mag * mag;
+            S.mv_class_histogram[mv_class_of(std::abs((int)b.dx))]++;
+            S.mv_class_histogram[mv_class_of(std::abs((int)b.dy))]++;
+            if (b.dx == 0) S.mv_new_zero_axes_x++;
+            if (b.dy == 0) S.mv_new_zero_axes_y++;
+            if (b.dx == 0 && b.dy == 0) S.mv_new_zero_post_bias++;
+        } else {
+            S.mv_zero_delta_blocks++;
+        }
+        S.mv_mode_counts[b.mode]++;
+        if (b.skip) S.blocks_skipped++;
+    }
+    S.mv_new_delta_count = S.mv_new_blocks;
+    S.mv_raw_bytes = (uint32_t)(2 * N + 2 * S.mv_new_blocks);
+    S.resi_raw = (int64_t)(N - (int)S.blocks_skipped) * 384 * 2;
+    if (mbh) search_stats(e, mbh->data(), prevh ? prevh->data() : nullptr, S);
+    S.mv_bias_dx = j.bias[0];
+    S.mv_bias_dy = j.bias[1];
+    S.rdo_lambda = e->L.lambda;
+    j.tr[2] = now_ms();
+    double dt = j.tr[2] - m0;
+    std::lock_guard<std::mutex> g(e->stat_mu);
+    e->host_ms[2] += dt;
+}
+
 static riv_status retire(riv_encoder* e, Job& j) {
     Slot& s = e->slots[j.slot];
     double t0 = now_ms();
@@ -1160,69 +1253,34 @@ static riv_status retire(riv_encoder* e, Job& j) {
         }
     }
     if (j.type == 2) {
-        j.fut_mv = e->mv_exec->submit([ep, jp, side, N, mbh, prevh] {
+        // The MV coder's two stages, each on its own thread and in frame order, so that frame
+        // t + 1's input is assembled and its symbols listed while frame t's are coded (same
+        // bytes as one thread).
+        j.fut_prep = e->mv_prep->submit([ep, jp, side, N, mbh, prevh] {
+            assemble_mv(ep, *jp, side, N, mbh.get(), prevh.get());
             double m0 = now_ms();
-            riv_frame_stats& S = jp->stats;
-            std::vector<std::pair<int8_t, int8_t>> nd;
-            nd.reserve(N);
-            for (int i = 0; i < N; i++)
-                if ((side[i] & 7) == M_NEW) nd.emplace_back((int8_t)(side[i] >> 8), (int8_t)(side[i] >> 16));
-            compute_delta_bias(nd, jp->bias[0], jp->bias[1]);
-            // MvCodedBlock assembly (enc/encoder.rs:774-818)
-            std::vector<MvCodedBlock> blocks(N);
-            for (int i = 0; i < N; i++) {
-                uint32_t v = side[i];
-                MvCodedBlock& b = blocks[i];
-                b.mode = (uint8_t)(v & 7);
-                b.new_base = (uint8_t)((v >> 3) & 7);
-                b.skip = (v >> 24) & 1;
-                b.dx = b.dy = 0;
-                b.spx = b.spy = SP_ZERO;
-                if (b.mode == M_NEW) {
-                    const int rdx = (int8_t)(v >> 8), rdy = (int8_t)(v >> 16);
-                    b.dx = (int8_t)std::min(std::max(rdx - jp->bias[0], -128), 127);
-                    b.dy = (int8_t)std::min(std::max(rdy - jp->bias[1], -128), 127);
-                    b.spx = ((v >> 6) & 1) ? SP_PLUS : SP_ZERO;
-                    b.spy = ((v >> 7) & 1) ? SP_PLUS : SP_ZERO;
-                    S.mv_new_blocks++;
-                    S.mv_new_base_counts[std::min<int>(b.new_base, 4)]++;
-                    // delta statistics before and after the bias (enc/encoder.rs:768-800, 873-884)
-                    if (rdx == 0 && rdy == 0) {
-                        S.mv_new_zero_pre_bias++;
-                        S.mv_zero_delta_blocks++;
-                    }
-                    const double fx = (double)b.dx, fy = (double)b.dy, mag = std::sqrt(fx * fx + fy * fy);
-                    S.mv_new_delta_mag_sum += mag;
-                    S.mv_new_delta_mag_sq_sum += mag * mag;
-                    S.mv_class_histogram[mv_class_of(std::abs((int)b.dx))]++;
-                    S.mv_class_histogram[mv_class_of(std::abs((int)b.dy))]++;
-                    if (b.dx == 0) S.mv_new_zero_axes_x++;
-                    if (b.dy == 0) S.mv_new_zero_axes_y++;
-                    if (b.dx == 0 && b.dy == 0) S.mv_new_zero_post_bias++;
-                } else {
-                    S.mv_zero_delta_blocks++;
-                }
-                S.mv_mode_counts[b.mode]++;
-                if (b.skip) S.blocks_skipped++;
-            }
-            S.mv_new_delta_count = S.mv_new_blocks;
-            S.mv_raw_bytes = (uint32_t)(2 * N + 2 * S.mv_new_blocks);
-            S.resi_raw = (int64_t)(N - (int)S.blocks_skipped) * 384 * 2;
-            if (mbh) search_stats(ep, mbh->data(), prevh ? prevh->data() : nullptr, S);
-            // the MV coder's modelling split mv_parts ways when set (same bytes; shorter on
-            // the ordered thread, which is serial across frames)
-            if (ep->mv_parts > 1) ep->mvc.encode_frame_parallel(blocks, ep->BW, jp->mv_bytes, ep->rans_submit, ep->mv_parts);
-            else ep->mvc.encode_frame(blocks, ep->BW, jp->mv_bytes, &ep->rans_submit);
-            S.mv_bias_dx = jp->bias[0];
-            S.mv_bias_dy = jp->bias[1];
-            S.rdo_lambda = ep->L.lambda;
-            double dt = now_ms() - m0;
+            jp->tr[3] = m0;
+            ep->mvc.prepare(jp->mv_blocks, ep->BW, jp->mv_syms);
+            jp->tr[4] = now_ms();
+            double dt = jp->tr[4] - m0;
+            std::lock_guard<std::mutex> g(ep->stat_mu);
+            ep->host_ms[2] += dt;
+        });
+        j.fut_mv = e->mv_exec->submit([ep, jp] {
+            jp->fut_prep.get();
+            double m0 = now_ms();
+            jp->tr[5] = m0;
+            ep->mvc.code(jp->mv_syms, jp->mv_bytes, &ep->mv_submit);
+            jp->tr[6] = now_ms();
+            double dt = jp->tr[6] - m0;
             std::lock_guard<std::mutex> g(ep->stat_mu);
             ep->host_ms[2] += dt;
         });
     } else {
-        // key frame: MV entropy contexts restart (enc/encoder.rs:335-337), in frame order
-        j.fut_mv = e->mv_exec->submit([ep] { ep->mvc.reset(); });
+        // key frame: MV entropy contexts restart (enc/encoder.rs:335-337), in frame order on
+        // both stages
+        j.fut_prep = e->mv_prep->submit([ep] { ep->mvc.reset_history(); });
+        j.fut_mv = e->mv_exec->submit([ep] { ep->mvc.reset_models(); });
     }
     const int16_t* packed = s.packed.as<int16_t>();
     const uint8_t* peobs = s.peobs.as<uint8_t>();
@@ -1230,12 +1288,16 @@ static riv_status retire(riv_encoder* e, Job& j) {
     bool intra = j.type == 1;
     // The newest frame of a drain is coded by all of rans_pool's threads (no later frame will
     // be coded beside it); the others model on one pool thread and hand their full rANS
-    // batches to rans_pool, which keeps the CPU cost per frame lowest while frames overlap.
+    // batches to rans_pool, which keeps the CPU cost per frame lowest while frames overlap
+    // (splitting every drained frame measured slower on a 16-core host: the split coder's
+    // extra work then competes with the frames beside it).
     const int parts = e->draining && &j == &e->jobs.back() ? e->rans_parts : 1;
     j.fut = e->pool->submit([jp, ep, packed, peobs, count, intra, parts] {
         double d0 = now_ms();
+        jp->tr[7] = d0;
         encode_residual_frame(packed, peobs, (int)count, intra, jp->res_bytes, &ep->rans_submit, parts);
-        double dt = now_ms() - d0;
+        jp->tr[8] = now_ms();
+        double dt = jp->tr[8] - d0;
         std::lock_guard<std::mutex> g(ep->stat_mu);
         ep->host_ms[3] += dt;
     });
@@ -1278,6 +1340,13 @@ static riv_status write_job(riv_encoder* e, Job& j) {
     if (j.type != 2) j.stats.resi_raw = -1;
     if (e->wr.write(e->wr.user, rec.data(), rec.size()) != 0) return fail(e, RIV_ERR_IO, "writer.write failed");
     e->host_ms[4] += now_ms() - w0;
+    if (!e->trace_path.empty()) {
+        j.tr[9] = now_ms();
+        std::array<double, 11> row;
+        row[0] = (double)j.index;
+        for (int k = 0; k < 10; k++) row[k + 1] = j.tr[k];
+        e->trace.push_back(row);
+    }
     e->frame_count++;
     if (j.timed) {
         memcpy(e->last_times, j.times, sizeof(j.times));
@@ -1290,7 +1359,9 @@ static riv_status write_job(riv_encoder* e, Job& j) {
 // Advance the pipeline.  Frames are retired strictly in order (the MV coder's contexts
 // carry across frames) and written strictly in order.  With `block_front` the oldest
 // frame is driven to completion; everything else only advances if already possible.
-static riv_status pump(riv_encoder* e, bool block_front) {
+static riv_status pump(riv_encoder* e, bool block_front, bool block_write);
+static riv_status pump(riv_encoder* e, bool block_front) { return pump(e, block_front, block_front); }
+static riv_status pump(riv_encoder* e, bool block_front, bool block_write) {
     bool block = block_front;
     for (auto& j : e->jobs) {
         if (j.state != 0) continue;
@@ -1309,7 +1380,7 @@ static riv_status pump(riv_encoder* e, bool block_front) {
         if (st) return st;
         block = false;
     }
-    block = block_front;
+    block = block_write;
     while (!e->jobs.empty()) {
         Job& f = e->jobs.front();
         if (f.state != 1) break;
@@ -1337,9 +1408,29 @@ static riv_status drain_all(riv_encoder* e) {
     // A record the writer refuses is dropped (pump pops it) and the drain goes on, so that
     // every later record is still written and the header can be patched; the refusal is
     // reported once the queue is empty.
+    // Frames are retired as soon as their GPU work is done, not after the front frame's record
+    // is written, so that their host coding starts at once; the front frame's coding is
+    // waited for in short slices in between.
     riv_status io = RIV_OK;
+    auto retired = [e] {
+        size_t n = 0;
+        for (const Job& j : e->jobs) n += j.state == 1;
+        return n;
+    };
     while (!e->jobs.empty()) {
-        riv_status st = pump(e, true);
+        const size_t n0 = e->jobs.size(), r0 = retired();
+        riv_status st = pump(e, false, false);
+        if (st == RIV_ERR_IO) {
+            io = st;
+            continue;
+        }
+        if (st) return st;
+        if (e->jobs.empty() || e->jobs.size() != n0 || retired() != r0) continue;  // progress
+        Job& f = e->jobs.front();
+        const bool later_unretired = retired() < e->jobs.size();
+        if (f.state == 0) st = pump(e, true, false);          // block on the front frame's GPU work
+        else if (!later_unretired) st = pump(e, false, true);  // nothing else to retire: block on its record
+        else f.fut.wait_for(std::chrono::microseconds(20));
         if (st == RIV_ERR_IO) {
             io = st;
             continue;
@@ -1384,6 +1475,7 @@ static riv_status encode_common(riv_encoder* e, int src, const void* a, const vo
         Job& j = e->jobs.back();
         j.index = n;
         j.ts = ts;
+        if (!e->trace_path.empty()) j.tr[0] = now_ms();
         j.type = intra ? 1 : 2;
         j.slot = (int)(n % cap);
         j.timed = e->cfg.pipeline_depth == 0 || stats != nullptr || n % TIMING_SAMPLE == 0;
@@ -1576,9 +1668,22 @@ void riv_encoder_free(riv_encoder* e) {
     for (auto& j : e->jobs) {
         if (j.fut.valid()) j.fut.wait();
         if (j.fut_mv.valid()) j.fut_mv.wait();
+        if (j.fut_prep.valid()) j.fut_prep.wait();
+    }
+    if (!e->trace_path.empty() && !e->trace.empty()) {
+        if (FILE* f = fopen(e->trace_path.c_str(), "a")) {
+            for (const auto& r : e->trace) {
+                fprintf(f, "%.0f", r[0]);
+                for (int k = 1; k < 11; k++) fprintf(f, ",%.4f", r[k]);
+                fprintf(f, "\n");
+            }
+            fclose(f);
+        }
     }
     e->pool.reset();
     e->mv_exec.reset();
+    e->mv_prep.reset();
+    e->mv_pool.reset();
     e->rans_pool.reset();
     if (e->S) cudaStreamSynchronize(e->S);
     if (e->C) cudaStreamSynchronize(e->C);
@@ -2612,7 +2717,7 @@ constexpr int TUNE_ROUNDS = 2;  // all-P-frame steps measured per candidate
 struct riv_batch {
     int device = 0;
     std::vector<riv_encoder*> clips;
-    std::shared_ptr<ThreadPool> pool, rans_pool;
+    std::shared_ptr<ThreadPool> pool, rans_pool, mv_pool;
     cudaStream_t B = nullptr, Hs = nullptr, C = nullptr;  // GPU chain, host->device, device->host
     cudaEvent_t ev_h2d = nullptr, ev_gpu = nullptr;
     std::vector<cudaEvent_t> ev_step;  // per step in flight: its GPU work and copies done
@@ -3070,8 +3175,9 @@ riv_status riv_batch_new(const riv_config* cfgs, const riv_writer_vtable* writer
     try {
         CK(cudaSetDevice(b->device));
         const unsigned hw = std::max(2u, std::thread::hardware_concurrency());
-        b->pool = std::make_shared<ThreadPool>(hw - 1);
-        b->rans_pool = std::make_shared<ThreadPool>(std::max(2u, hw / 2));
+        b->pool = std::make_shared<ThreadPool>(hw - 1, BULK_NICE);
+        b->rans_pool = std::make_shared<ThreadPool>(std::max(2u, hw / 2), BULK_NICE);
+        b->mv_pool = std::make_shared<ThreadPool>(std::max(2u, hw / 4));
         size_t maxcap = 1;
         for (uint32_t i = 0; i < n; i++) {
             riv_config c = cfgs[i];
@@ -3087,8 +3193,11 @@ riv_status riv_batch_new(const riv_config* cfgs, const riv_writer_vtable* writer
             e->defer_ok = false;  // each step reconstructs its frames itself
             e->pool = b->pool;
             e->rans_pool = b->rans_pool;
-            ThreadPool* rp = b->rans_pool.get();
+            e->mv_pool = b->mv_pool;
+            ThreadPool* rp = b->rans_pool.get();  // both submit paths onto the shared pools
             e->rans_submit = [rp](std::function<void()> f) { return rp->submit(std::move(f)); };
+            ThreadPool* mp = b->mv_pool.get();
+            e->mv_submit = [mp](std::function<void()> f) { return mp->submit(std::move(f)); };
             e->rans_parts = (int)std::max(2u, hw / 2) + 1;
             b->clips.push_back(e);
             b->max_sr = std::max(b->max_sr, (int)c.search_range);
@@ -3185,6 +3294,7 @@ void riv_batch_free(riv_batch* b) {
     b->clips.clear();
     b->pool.reset();
     b->rans_pool.reset();
+    b->mv_pool.reset();
     for (auto& ev : b->ev_step)
         if (ev) cudaEventDestroy(ev);
     for (int q = 0; q < 2; q++)

@@ -2723,6 +2723,59 @@ __device__ __forceinline__ unsigned ls_sad_hp(const uint8_t* win, int ws, int ox
     return __reduce_add_sync(0xffffffffu, s);
 }
 
+// Four positions at once: lane group g (lanes 8g .. 8g + 7) scores its own position, lane i of
+// the group rows 2i and 2i + 1 (16 samples each, current samples in cw: row 2i in cw[0..3], row
+// 2i + 1 in cw[4..7]); the group's sum ends in every lane of the group.  Five aligned words per
+// row cover the 16 unaligned bytes; `w(k, sh)` is the word at byte 4k + sh / 8 of them.
+__device__ __forceinline__ uint32_t ls_word(const uint32_t (&w)[5], int k, uint32_t sh) {
+    return sh >= 32u ? w[k + 1] : __funnelshift_r(w[k], w[k + 1], sh);
+}
+__device__ __forceinline__ void ls_row5(const uint8_t* win, int off, uint32_t (&w)[5], uint32_t& sh) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(win + off);
+    const uint32_t b = a & ~3u;
+    sh = (a & 3u) * 8u;
+#pragma unroll
+    for (int k = 0; k < 5; k++) asm volatile("ld.shared.u32 %0, [%1];" : "=r"(w[k]) : "r"(b + 4u * k));
+}
+__device__ __forceinline__ unsigned group_sum8(unsigned s) {
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    s += __shfl_xor_sync(0xffffffffu, s, 4);
+    return s;
+}
+// whole-pixel offset (dx, dy)
+__device__ __forceinline__ unsigned ls_sad_g(const uint8_t* win, int ws, int ox, int oy, int dx, int dy, int li,
+                                             const uint32_t (&cw)[8]) {
+    unsigned s = 0;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        uint32_t w[5], sh;
+        ls_row5(win, (oy + 2 * li + h + dy) * ws + ox + dx, w, sh);
+#pragma unroll
+        for (int k = 0; k < 4; k++) s += __vsadu4(ls_word(w, k, sh), cw[4 * h + k]);
+    }
+    return group_sum8(s);
+}
+// half-pel offset (hx, hy), floor-averaged samples (the same rule as ls_sad_hp)
+__device__ __forceinline__ unsigned ls_sad_hp_g(const uint8_t* win, int ws, int ox, int oy, int hx, int hy, int li,
+                                                const uint32_t (&cw)[8]) {
+    const int ix = hx >> 1, iy = hy >> 1, fx = hx & 1, fy = hy & 1;
+    uint32_t w[3][5], sh[3];
+#pragma unroll
+    for (int r = 0; r < 3; r++) ls_row5(win, (oy + 2 * li + r + iy) * ws + ox + ix, w[r], sh[r]);
+    unsigned s = 0;
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const uint32_t a = ls_word(w[h], k, sh[h]), b = ls_word(w[h], k, sh[h] + 8u);
+            const uint32_t c = ls_word(w[h + 1], k, sh[h + 1]), d = ls_word(w[h + 1], k, sh[h + 1] + 8u);
+            const uint32_t v = fx && fy ? favg4(a, b, c, d) : fx ? favg(a, b) : fy ? favg(a, c) : a;
+            s += __vsadu4(v, cw[4 * h + k]);
+        }
+    return group_sum8(s);
+}
+
 __global__ void __launch_bounds__(32 * LS_MBS) k_learned_search(LearnedParams lp) {
     const SearchParams& p = lp.sp;
     extern __shared__ __align__(16) uint8_t lsm[];
@@ -2760,9 +2813,15 @@ __global__ void __launch_bounds__(32 * LS_MBS) k_learned_search(LearnedParams lp
     const int bx = bx0 + w, mb = by * p.BW + bx;
     const int x0 = bx * 16, y0 = by * 16;
     const int ox = x0 - wx0, oy = y0 - wy0;
-    // this lane's 8 current samples
-    const uint8_t* cp = p.cur_y + (size_t)(y0 + (lane >> 1)) * p.W + x0 + (lane & 1) * 8;
-    const uint32_t c0 = *(const uint32_t*)cp, c1 = *(const uint32_t*)(cp + 4);
+    // this lane's group (g) and its place in it (li): rows 2 li, 2 li + 1 of the block
+    const int g = lane >> 3, li = lane & 7;
+    uint32_t cw[8];
+    {
+        const uint8_t* cp = p.cur_y + (size_t)(y0 + 2 * li) * p.W + x0;
+        const uint4 r0 = *(const uint4*)cp, r1 = *(const uint4*)(cp + p.W);
+        cw[0] = r0.x; cw[1] = r0.y; cw[2] = r0.z; cw[3] = r0.w;
+        cw[4] = r1.x; cw[5] = r1.y; cw[6] = r1.z; cw[7] = r1.w;
+    }
     // predictors from the previous P-frame's coded MVs (whole-pixel parts, within +-sr)
     int px[7] = {0, 0, 0, 0, 0, 0, 0}, py[7] = {0, 0, 0, 0, 0, 0, 0};
     bool av[5] = {false, false, false, false, false};
@@ -2791,88 +2850,172 @@ __global__ void __launch_bounds__(32 * LS_MBS) k_learned_search(LearnedParams lp
         }
     }
     auto cost = [&](int dx, int dy, unsigned sad) { return (long long)sad + mv_cost<false>(dx, dy, cc, p, p.mvbits, nullptr); };
-    // candidates: 4 proposals, then the 7 predictors
-    int cx[11], cy[11];
-    int ncand = 0;
+    // One batch: group g scores position (gx, gy) if `act` (a group-uniform flag; inactive groups
+    // score a valid dummy position), and every lane then takes the group results in group order,
+    // so the first strictly better position wins, as in a one-at-a-time walk.
+    auto batch = [&](bool act, int gx, int gy, bool hp, unsigned& sad_out, long long& c_out) {
+        const unsigned sad = hp ? ls_sad_hp_g(lsm, ws, ox, oy, gx, gy, li, cw) : ls_sad_g(lsm, ws, ox, oy, gx, gy, li, cw);
+        sad_out = sad;
+        c_out = act ? (hp ? (long long)sad : cost(gx, gy, sad)) : LLONG_MAX;
+    };
+    auto from_group = [&](int src, unsigned sad, long long c, unsigned& s2, long long& c2) {
+        s2 = __shfl_sync(0xffffffffu, sad, 8 * src);
+        c2 = (long long)__shfl_sync(0xffffffffu, (unsigned long long)c, 8 * src);
+    };
+    // candidates: 4 proposals (slots 0-3, absent without a network), then the 7 predictors
+    // (slots 4-10); a position already scored in the same group (proposals / predictors) changes
+    // neither that group's minimum SAD nor, with the strict `<`, the best, so the list keeps the
+    // first of each (the candidates are the same in every lane)
+    __shared__ int clist[LS_MBS][12];
+    int cx[11] = {0, 0, 0, 0}, cy[11] = {0, 0, 0, 0};
     bool shortcut = false;
-    if (lp.net) {
-        const float* o = lp.net + (size_t)mb * 16;
+    const bool has_net = lp.net != nullptr;
+    if (has_net) {
+        const float4* o4 = (const float4*)(lp.net + (size_t)mb * 16);
+        const float4 q0 = o4[0], q1 = o4[1], q2 = o4[2];
+        const float o[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             const float hx = o[2 * k] * 32.0f, hy = o[2 * k + 1] * 32.0f;  // half-pel units
             cx[k] = min(max(__float2int_rn(hx * 0.5f), -sr), sr);
             cy[k] = min(max(__float2int_rn(hy * 0.5f), -sr), sr);
         }
-        ncand = 4;
-        shortcut = o[8] > lp.skip_logit;
+        shortcut = q2.x > lp.skip_logit;
     }
-    const int npro = ncand;
 #pragma unroll
-    for (int k = 0; k < 7; k++) { cx[ncand + k] = px[k]; cy[ncand + k] = py[k]; }
-    ncand += 7;
-    long long best = LLONG_MAX, bestp = LLONG_MAX, bestq = LLONG_MAX;
+    for (int k = 0; k < 7; k++) { cx[4 + k] = px[k]; cy[4 + k] = py[k]; }
+    int nlist = 0;
+#pragma unroll
+    for (int k = 0; k < 11; k++) {
+        if (k < 4 && !has_net) continue;
+        bool seen = false;
+#pragma unroll
+        for (int j = 0; j < k; j++) seen |= cx[j] == cx[k] && cy[j] == cy[k] && ((j < 4) == (k < 4));
+        if (seen) continue;
+        if (lane == 0) clist[w][nlist] = (k << 16) | ((cy[k] & 0xFF) << 8) | (cx[k] & 0xFF);
+        nlist++;
+    }
+    __syncwarp();
+    long long best = LLONG_MAX;
     unsigned bsad = 0, bsp = 0xffffffffu, bsq = 0xffffffffu;
     int bdx = 0, bdy = 0;
-    for (int k = 0; k < ncand; k++) {
-        const unsigned sad = ls_sad(lsm, ws, ox, oy, cx[k], cy[k], lane, c0, c1);
-        const long long c = cost(cx[k], cy[k], sad);
-        if (k < npro) bsp = min(bsp, sad); else bsq = min(bsq, sad);
-        if (c < best) { best = c; bsad = sad; bdx = cx[k]; bdy = cy[k]; }
+    for (int b0 = 0; b0 < nlist; b0 += 4) {
+        const int e = clist[w][b0 + g < nlist ? b0 + g : b0];
+        unsigned sad;
+        long long c;
+        batch(b0 + g < nlist, (int)(int8_t)(e & 0xFF), (int)(int8_t)((e >> 8) & 0xFF), false, sad, c);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            unsigned s2;
+            long long c2;
+            from_group(q, sad, c, s2, c2);
+            if (b0 + q >= nlist) continue;
+            const int eq = clist[w][b0 + q];
+            if ((eq >> 16) < 4) bsp = min(bsp, s2); else bsq = min(bsq, s2);
+            if (c2 < best) { best = c2; bsad = s2; bdx = (int)(int8_t)(eq & 0xFF); bdy = (int)(int8_t)((eq >> 8) & 0xFF); }
+        }
     }
-    (void)bestp; (void)bestq;
     const bool fallback = !lp.net || bsp > bsq + (unsigned)lp.margin;
     if (fallback) shortcut = false;
     if (!shortcut) {
-        // whole-pixel refinement: hexagon rounds (fallback) then small-diamond rounds
-        const int HX[6] = {2, 1, -1, -2, -1, 1}, HY[6] = {0, 2, 2, 0, -2, -2};
-        const int DX[4] = {1, -1, 0, 0}, DY[4] = {0, 0, 1, -1};
+        // whole-pixel refinement: hexagon rounds (fallback) then small-diamond rounds.  After a
+        // move in direction m, the points a round would evaluate again (the previous centre,
+        // and for the hexagon its two neighbours of m, which are the new centre's points m + 2 ..
+        // m + 4) all cost at least the new centre's cost, so under the strict `<` they can never
+        // be taken: they are skipped, and the walk is unchanged.
+        // hexagon directions (2,0) (1,2) (-1,2) (-2,0) (-1,-2) (1,-2); diamond (1,0) (-1,0) (0,1) (0,-1)
+        // (selects, not tables: the direction is a per-lane value)
+        auto HX = [](int k) { return k == 0 ? 2 : k == 1 ? 1 : k == 2 ? -1 : k == 3 ? -2 : k == 4 ? -1 : 1; };
+        auto HY = [](int k) { return k == 0 || k == 3 ? 0 : k <= 2 ? 2 : -2; };
+        auto DX = [](int k) { return k == 0 ? 1 : k == 1 ? -1 : 0; };
+        auto DY = [](int k) { return k == 2 ? 1 : k == 3 ? -1 : 0; };
+        auto in_range = [&](int dx, int dy) { return dx >= -sr && dx <= sr && dy >= -sr && dy <= sr; };
         if (fallback) {
+            int moved = -1;
             for (int round = 0; round < 16; round++) {  // a bounded hexagon walk (+-32 pixels)
-                int nbx = bdx, nby = bdy;
+                // this round's directions in increasing order: all six, or m - 1, m, m + 1
+                int dirs[6] = {0, 1, 2, 3, 4, 5}, nd = 6;
+                if (moved >= 0) {
+                    const int d0 = (moved + 5) % 6, d2 = (moved + 1) % 6;
+                    const int lo = min(min(d0, moved), d2), hi = max(max(d0, moved), d2);
+                    dirs[0] = lo; dirs[1] = d0 + moved + d2 - lo - hi; dirs[2] = hi;
+                    nd = 3;
+                }
+                auto pick = [&](int i) {
+                    return i == 0 ? dirs[0] : i == 1 ? dirs[1] : i == 2 ? dirs[2] : i == 3 ? dirs[3] : i == 4 ? dirs[4] : dirs[5];
+                };
+                int nbx = bdx, nby = bdy, nk = -1;
                 long long nb = best;
                 unsigned ns = bsad;
 #pragma unroll
-                for (int k = 0; k < 6; k++) {
-                    const int dx = bdx + HX[k], dy = bdy + HY[k];
-                    if (dx < -sr || dx > sr || dy < -sr || dy > sr) continue;
-                    const unsigned sad = ls_sad(lsm, ws, ox, oy, dx, dy, lane, c0, c1);
-                    const long long c = cost(dx, dy, sad);
-                    if (c < nb) { nb = c; ns = sad; nbx = dx; nby = dy; }
+                for (int b0 = 0; b0 < 8; b0 += 4) {
+                    if (b0 >= nd) break;
+                    const int kg = pick(b0 + g < nd ? b0 + g : b0);
+                    const int dx = bdx + HX(kg), dy = bdy + HY(kg);
+                    const bool act = b0 + g < nd && in_range(dx, dy);
+                    unsigned sad;
+                    long long c;
+                    batch(act, act ? dx : bdx, act ? dy : bdy, false, sad, c);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        unsigned s2;
+                        long long c2;
+                        from_group(q, sad, c, s2, c2);
+                        if (b0 + q >= nd) continue;
+                        const int kq = pick(b0 + q);
+                        if (c2 < nb) { nb = c2; ns = s2; nbx = bdx + HX(kq); nby = bdy + HY(kq); nk = kq; }
+                    }
                 }
-                if (nbx == bdx && nby == bdy) break;
-                best = nb; bsad = ns; bdx = nbx; bdy = nby;
+                if (nk < 0) break;
+                best = nb; bsad = ns; bdx = nbx; bdy = nby; moved = nk;
             }
         }
+        int moved = -1;
         for (int round = 0; round < (fallback ? 16 : 8); round++) {
-            int nbx = bdx, nby = bdy;
+            const int dx = bdx + DX(g), dy = bdy + DY(g);
+            const bool act = in_range(dx, dy) && !(moved >= 0 && g == (moved ^ 1));  // not the previous centre
+            unsigned sad;
+            long long c;
+            batch(act, act ? dx : bdx, act ? dy : bdy, false, sad, c);
+            int nbx = bdx, nby = bdy, nk = -1;
             long long nb = best;
             unsigned ns = bsad;
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const int dx = bdx + DX[k], dy = bdy + DY[k];
-                if (dx < -sr || dx > sr || dy < -sr || dy > sr) continue;
-                const unsigned sad = ls_sad(lsm, ws, ox, oy, dx, dy, lane, c0, c1);
-                const long long c = cost(dx, dy, sad);
-                if (c < nb) { nb = c; ns = sad; nbx = dx; nby = dy; }
+            for (int q = 0; q < 4; q++) {
+                unsigned s2;
+                long long c2;
+                from_group(q, sad, c, s2, c2);
+                if (c2 < nb) { nb = c2; ns = s2; nbx = bdx + DX(q); nby = bdy + DY(q); nk = q; }
             }
-            if (nbx == bdx && nby == bdy) break;
-            best = nb; bsad = ns; bdx = nbx; bdy = nby;
+            if (nk < 0) break;
+            best = nb; bsad = ns; bdx = nbx; bdy = nby; moved = nk;
         }
     }
-    // half-pel refinement around the whole-pixel best (the centre with no penalty)
+    // half-pel refinement around the whole-pixel best: the centre (no penalty) first, then the
+    // eight neighbours row by row, each with the fractional penalty c15
     int hx = 2 * bdx, hy = 2 * bdy;
     unsigned hsad = bsad;
     if (!shortcut) {
-        hsad = ls_sad_hp(lsm, ws, ox, oy, hx, hy, lane, c0, c1);
-        long long hbest = hsad;
+        long long hbest = LLONG_MAX;
         int bhx = hx, bhy = hy;
-        for (int sy = -1; sy <= 1; sy++)
-            for (int sx = -1; sx <= 1; sx++) {
-                if (!sx && !sy) continue;
-                const unsigned sad = ls_sad_hp(lsm, ws, ox, oy, hx + sx, hy + sy, lane, c0, c1);
-                const long long c = (long long)sad + p.c15;
-                if (c < hbest) { hbest = c; bhx = hx + sx; bhy = hy + sy; hsad = sad; }
+        for (int b0 = 0; b0 < 9; b0 += 4) {
+            const int i = b0 + g < 9 ? b0 + g : 0;  // 0: centre, 1..8: (sy, sx) in row order without the centre
+            const int n = i == 0 ? 4 : i <= 4 ? i - 1 : i;  // 3x3 index (sy + 1) * 3 + sx + 1
+            const int gx = hx + n % 3 - 1, gy = hy + n / 3 - 1;
+            unsigned sad;
+            long long c;
+            batch(true, gx, gy, true, sad, c);
+            if (i != 0) c += p.c15;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                unsigned s2;
+                long long c2;
+                from_group(q, sad, c, s2, c2);
+                if (b0 + q >= 9) continue;
+                const int iq = b0 + q, nq = iq == 0 ? 4 : iq <= 4 ? iq - 1 : iq;
+                if (c2 < hbest) { hbest = c2; bhx = hx + nq % 3 - 1; bhy = hy + nq / 3 - 1; hsad = s2; }
             }
+        }
         hx = bhx;
         hy = bhy;
     }

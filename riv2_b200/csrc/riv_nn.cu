@@ -755,6 +755,7 @@ int nn_conv(int layer, const void* in, int in_mb, const void* W, const float* bi
 __device__ __forceinline__ int med3(int a, int b, int c) { return max(min(a, b), min(max(a, b), c)); }
 
 constexpr int PF_MBS = 4;               // MBs of a row per CTA
+constexpr int PF_WARPS = 6, PF_THREADS = 32 * PF_WARPS;
 constexpr int PF_WW = 16 * PF_MBS + 48;  // window width shared by them (full resolution)
 
 // bf16 tensor-core product of one 16x16 A fragment and one 16x8 B fragment, f32 accumulate
@@ -775,19 +776,21 @@ __device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a
 // 16 output positions at a time: A rows = positions, the fragment's k pairs = one tap's two
 // channels (one 32-bit word of the shared input), B = W1 (32 x 32, bf16), f32 accumulation.
 template <bool FRONT>
-__global__ void __launch_bounds__(256, 4) k_prop_input(const uint8_t* __restrict__ cur, const uint8_t* __restrict__ ref,
+__global__ void __launch_bounds__(PF_THREADS, 5) k_prop_input(const uint8_t* __restrict__ cur, const uint8_t* __restrict__ ref,
                                                     int W, int H, const int8_t* __restrict__ prev_coded, int mb0,
                                                     int nmb, __nv_bfloat16* __restrict__ feat,
                                                     __nv_bfloat16* __restrict__ x1,
                                                     const __nv_bfloat16* __restrict__ w1, const float* __restrict__ b1,
                                                     __nv_bfloat16* __restrict__ a1) {
-    constexpr int NF = nn::FEAT * nn::FEAT;
-    __shared__ __align__(16) uint32_t F[FRONT ? PF_MBS * NF : 1];      // the input, one word per pixel
-    __shared__ __align__(16) uint32_t O[FRONT ? 8 * 16 * 16 : 1];      // per warp: 16 output rows of 64 bytes
+    // the input, one word per pixel, behind a leading row and column of zeros (conv1's padding)
+    constexpr int FP = nn::FEAT + 1, NF = FP * FP;
+    __shared__ __align__(16) uint32_t F[FRONT ? PF_MBS * NF : 1];
+    __shared__ __align__(16) uint32_t O[FRONT ? PF_WARPS * 16 * 16 : 1];  // per warp: 16 output rows of 64 bytes
     __shared__ __align__(16) uint32_t win[64][PF_WW / 4];   // reference window, 4 MBs wide
     __shared__ __align__(16) uint32_t R[32][PF_WW / 8 + 1];  // its 2x2 averages (+ a word of slack)
     __shared__ __align__(16) uint32_t Cb[PF_MBS][8][2];     // the current blocks' 2x2 averages
-    __shared__ int pu[PF_MBS][nn::NPRED], pv[PF_MBS][nn::NPRED], ph[PF_MBS][2 * nn::NPRED];
+    __shared__ uint32_t mark[PF_MBS][nn::FEAT];              // per volume row: bit u = a predictor's offset
+    __shared__ int ph[PF_MBS][2 * nn::NPRED];
     const int BW = W / 16, BH = H / 16;
     const int t = threadIdx.x;
     // the CTA's MBs: PF_MBS consecutive MBs of one row, starting at raster index first
@@ -798,12 +801,12 @@ __global__ void __launch_bounds__(256, 4) k_prop_input(const uint8_t* __restrict
     if (first + nhere <= mb0 || first >= mb0 + nmb) return;
     const int wx = bx0 * 16 - nn::WIN_OFF, wy = by * 16 - nn::WIN_OFF;
     if (wx >= 0 && wy >= 0 && wx + PF_WW <= W && wy + 64 <= H) {  // inside the frame: word loads
-        for (int k = t; k < 64 * (PF_WW / 4); k += 256) {
+        for (int k = t; k < 64 * (PF_WW / 4); k += PF_THREADS) {
             const int r = k / (PF_WW / 4), c = k % (PF_WW / 4);
             win[r][c] = *(const uint32_t*)(ref + (size_t)(wy + r) * W + wx + 4 * c);
         }
     } else {  // at a border: coordinates clamped per sample
-        for (int k = t; k < 64 * (PF_WW / 4); k += 256) {
+        for (int k = t; k < 64 * (PF_WW / 4); k += PF_THREADS) {
             const int r = k / (PF_WW / 4), c = k % (PF_WW / 4);
             const int yy = min(max(wy + r, 0), H - 1);
             uint32_t v = 0;
@@ -815,11 +818,13 @@ __global__ void __launch_bounds__(256, 4) k_prop_input(const uint8_t* __restrict
             win[r][c] = v;
         }
     }
-    if (t < 64 * nhere) {
-        const int m = t >> 6, j = (t >> 3) & 7, c = t & 7;
+    for (int k = t; k < 64 * nhere; k += PF_THREADS) {
+        const int m = k >> 6, j = (k >> 3) & 7, c = k & 7;
         const uint8_t* p = cur + (size_t)(by * 16 + 2 * j) * W + (bx0 + m) * 16 + 2 * c;
         ((uint8_t*)Cb[m])[j * 8 + c] = (uint8_t)((p[0] + p[1] + p[W] + p[W + 1] + 2) >> 2);
     }
+    if (t < PF_MBS * nn::FEAT) mark[t / nn::FEAT][t % nn::FEAT] = 0u;
+    __syncthreads();
     if (t < nhere) {
         const int bx = bx0 + t;
         int px[nn::NPRED] = {0}, py[nn::NPRED] = {0};
@@ -840,15 +845,14 @@ __global__ void __launch_bounds__(256, 4) k_prop_input(const uint8_t* __restrict
         }
         for (int k = 0; k < nn::NPRED; k++) {
             // nearest half-resolution offset of the MV (half-pel units / 4, rounded half up)
-            pu[t][k] = ((px[k] + 2) >> 2) + 12;
-            pv[t][k] = ((py[k] + 2) >> 2) + 12;
+            const int u = ((px[k] + 2) >> 2) + 12, v = ((py[k] + 2) >> 2) + 12;
+            if (u >= 0 && u < nn::FEAT && v >= 0 && v < nn::FEAT) atomicOr(&mark[t][v], 1u << u);
             ph[t][2 * k] = px[k];
             ph[t][2 * k + 1] = py[k];
         }
     }
-    __syncthreads();
     // 2x2 rounded averages of the window, four output bytes per step
-    for (int k = t; k < 32 * (PF_WW / 8); k += 256) {
+    for (int k = t; k < 32 * (PF_WW / 8); k += PF_THREADS) {
         const int j = k / (PF_WW / 8), c = k % (PF_WW / 8);  // output row j, output word c
         const uint32_t a0 = win[2 * j][2 * c], a1 = win[2 * j][2 * c + 1];
         const uint32_t b0 = win[2 * j + 1][2 * c], b1 = win[2 * j + 1][2 * c + 1];
@@ -860,40 +864,73 @@ __global__ void __launch_bounds__(256, 4) k_prop_input(const uint8_t* __restrict
                   (((s1 >> 18) & 0xFFu) << 24);
     }
     if (t < 32) R[t][PF_WW / 8] = 0u;
+    if (FRONT)  // the padding row and column of each MB's input
+        for (int k = t; k < PF_MBS * (2 * FP - 1); k += PF_THREADS) {
+            const int m = k / (2 * FP - 1), j = k % (2 * FP - 1);
+            F[m * NF + (j < FP ? j : (j - FP + 1) * FP)] = 0u;
+        }
     __syncthreads();
-    // four horizontally adjacent offsets per item: they share the reference words of each row
-    // (shifted by 0, 8, 16, 24 bits) and the current block's words
-    constexpr int NG = nn::FEAT / 4;  // groups of four offsets per row of the volume
-    for (int k = t; k < nhere * nn::FEAT * NG; k += 256) {
-        const int m = k / (nn::FEAT * NG), kg = k % (nn::FEAT * NG);
+    // the volume in blocks of 4 horizontally adjacent x 3 vertically adjacent offsets per item:
+    // each reference row's words and their byte shifts (0, 8, 16, 24 bits) are loaded once and
+    // serve the three offset rows that use them; the current block stays in registers
+    constexpr int UB = 4, VB = 3, NUG = nn::FEAT / UB, NVG = nn::FEAT / VB;
+    for (int k = t; k < nhere * NUG * NVG; k += PF_THREADS) {
+        const int m = k / (NUG * NVG), kg = k % (NUG * NVG);
         const int mb = first + m;
         if (mb < mb0 || mb >= mb0 + nmb) continue;
-        const int v = kg / NG, u0 = 4 * (kg % NG);
+        const int v0 = VB * (kg / NUG), u0 = UB * (kg % NUG);
         const int wq = (8 * m + u0) >> 2;  // 8 m + u0 is a multiple of 4
-        unsigned sad[4] = {0u, 0u, 0u, 0u};
+        uint32_t cw[8][2];
 #pragma unroll
         for (int j = 0; j < 8; j++) {
-            const uint32_t* row = R[v + j];
+            const uint2 c = *(const uint2*)Cb[m][j];
+            cw[j][0] = c.x;
+            cw[j][1] = c.y;
+        }
+        unsigned sad[VB][UB];
+#pragma unroll
+        for (int dv = 0; dv < VB; dv++)
+#pragma unroll
+            for (int q = 0; q < UB; q++) sad[dv][q] = 0u;
+#pragma unroll
+        for (int rr = 0; rr < 8 + VB - 1; rr++) {
+            const uint32_t* row = R[v0 + rr];
             const uint32_t w0 = row[wq], w1 = row[wq + 1], w2 = row[wq + 2];
-            const uint32_t c0 = Cb[m][j][0], c1 = Cb[m][j][1];
-            sad[0] += __vsadu4(w0, c0) + __vsadu4(w1, c1);
+            uint32_t lo[UB], hi[UB];
+            lo[0] = w0;
+            hi[0] = w1;
 #pragma unroll
-            for (int q = 1; q < 4; q++)
-                sad[q] += __vsadu4(__funnelshift_r(w0, w1, 8 * q), c0) + __vsadu4(__funnelshift_r(w1, w2, 8 * q), c1);
+            for (int q = 1; q < UB; q++) {
+                lo[q] = __funnelshift_r(w0, w1, 8 * q);
+                hi[q] = __funnelshift_r(w1, w2, 8 * q);
+            }
+#pragma unroll
+            for (int dv = 0; dv < VB; dv++) {
+                const int j = rr - dv;  // row of the current block against this reference row
+                if (j < 0 || j >= 8) continue;
+#pragma unroll
+                for (int q = 0; q < UB; q++) sad[dv][q] += __vsadu4(lo[q], cw[j][0]) + __vsadu4(hi[q], cw[j][1]);
+            }
         }
-        uint32_t o[4];
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const float f0 = 1.0f - (float)min((int)sad[q], 2048) * (1.0f / 1024.0f);
-            float f1 = 0.0f;
+        for (int dv = 0; dv < VB; dv++) {
+            const int v = v0 + dv;
+            const uint32_t mk = mark[m][v] >> u0;
+            uint32_t o[UB];
 #pragma unroll
-            for (int pq = 0; pq < nn::NPRED; pq++)
-                if (pu[m][pq] == u0 + q && pv[m][pq] == v) f1 = 1.0f;
-            o[q] = pack_bf16(f0, f1);
+            for (int q = 0; q < UB; q++) {
+                const float f0 = 1.0f - (float)min((int)sad[dv][q], 2048) * (1.0f / 1024.0f);
+                o[q] = pack_bf16(f0, ((mk >> q) & 1u) ? 1.0f : 0.0f);
+            }
+            if (FRONT) {
+                uint32_t* f = F + m * NF + (v + 1) * FP + u0 + 1;
+#pragma unroll
+                for (int q = 0; q < UB; q++) f[q] = o[q];
+            } else {
+                const int kk = v * nn::FEAT + u0;  // 16-byte aligned word index
+                *(uint4*)(feat + (size_t)(mb - mb0) * (nn::FEAT * nn::FEAT * 2) + 2 * kk) = make_uint4(o[0], o[1], o[2], o[3]);
+            }
         }
-        const int kk = v * nn::FEAT + u0;  // 16-byte aligned word index
-        if (FRONT) *(uint4*)(F + m * NF + kk) = make_uint4(o[0], o[1], o[2], o[3]);
-        else *(uint4*)(feat + (size_t)(mb - mb0) * (nn::FEAT * nn::FEAT * 2) + 2 * kk) = make_uint4(o[0], o[1], o[2], o[3]);
     }
     if (t < 16 * nhere) {
         const int m = t >> 4, q = t & 15, mb = first + m;
@@ -922,21 +959,20 @@ __global__ void __launch_bounds__(256, 4) k_prop_input(const uint8_t* __restrict
             bias[nt][0] = __ldg(b1 + 8 * nt + 2 * tig);
             bias[nt][1] = __ldg(b1 + 8 * nt + 2 * tig + 1);
         }
-        uint32_t* ob = O + warp * 256;
-        // 9 tiles of 16 positions per MB; warp w takes tiles w, w + 8, ...
-        for (int tile = warp; tile < nhere * 9; tile += 8) {
+        uint32_t* ob = O + warp * 256;  // 16 rows x 16 words
+        // the word of output position (oy, ox) at tap (ky, kx) is F[(2 oy + ky) * FP + 2 ox + kx]
+        // (stride 2: only the leading padding row and column are ever read); this thread's
+        // taps are tig, tig + 4 and, for tig 0, tap 8
+        const int oa = (tig / 3) * FP + tig % 3, ob4 = ((tig + 4) / 3) * FP + (tig + 4) % 3, o8 = 2 * FP + 2;
+        // 9 tiles of 16 positions per MB; warp w takes tiles w, w + PF_WARPS, ...
+        for (int tile = warp; tile < nhere * 9; tile += PF_WARPS) {
             const int m = tile / 9, p0 = (tile % 9) * 16, mb = first + m;
             if (mb < mb0 || mb >= mb0 + nmb) continue;  // warp-uniform
-            const uint32_t* fm = F + m * NF;
-            // the input word of position p (row of A) at tap: zero outside the 24x24 input
-            auto px = [&](int p, int tap) -> uint32_t {
-                const int oy = p / 12, ox = p % 12;
-                const int y = 2 * oy + tap / 3 - 1, x = 2 * ox + tap % 3 - 1;
-                return (y >= 0 && y < nn::FEAT && x >= 0 && x < nn::FEAT) ? fm[y * nn::FEAT + x] : 0u;
-            };
             const int r0 = p0 + g, r1 = p0 + g + 8;
-            const uint32_t a0[4] = {px(r0, tig), px(r1, tig), px(r0, tig + 4), px(r1, tig + 4)};
-            const uint32_t a1f[4] = {tig == 0 ? px(r0, 8) : 0u, tig == 0 ? px(r1, 8) : 0u, 0u, 0u};
+            const uint32_t* f0 = F + m * NF + 2 * (r0 / 12) * FP + 2 * (r0 % 12);
+            const uint32_t* f1 = F + m * NF + 2 * (r1 / 12) * FP + 2 * (r1 % 12);
+            const uint32_t a0[4] = {f0[oa], f1[oa], f0[ob4], f1[ob4]};
+            const uint32_t a1f[4] = {tig == 0 ? f0[o8] : 0u, tig == 0 ? f1[o8] : 0u, 0u, 0u};
 #pragma unroll
             for (int nt = 0; nt < 4; nt++) {
                 float d[4] = {0.0f, 0.0f, 0.0f, 0.0f};
@@ -1146,7 +1182,7 @@ int riv_nn_features(const uint8_t* cur_y, const uint8_t* ref_y, int W, int H, co
         return (int)cudaErrorInvalidValue;
     // CTAs over groups of PF_MBS MBs of a row; those outside mb0 .. mb0+nmb-1 return at once
     const int BW = W / 16, groups = (BW + PF_MBS - 1) / PF_MBS * (H / 16);
-    k_prop_input<false><<<groups, 256, 0, (cudaStream_t)stream>>>(cur_y, ref_y, W, H, prev_coded, mb0, nmb,
+    k_prop_input<false><<<groups, PF_THREADS, 0, (cudaStream_t)stream>>>(cur_y, ref_y, W, H, prev_coded, mb0, nmb,
                                                                   (__nv_bfloat16*)feat, (__nv_bfloat16*)x1, nullptr,
                                                                   nullptr, nullptr);
     return (int)cudaGetLastError();
@@ -1158,7 +1194,7 @@ int riv_nn_front(const uint8_t* cur_y, const uint8_t* ref_y, int W, int H, const
         ((uintptr_t)a1 & 15) || ((uintptr_t)w1 & 3))
         return (int)cudaErrorInvalidValue;
     const int BW = W / 16, groups = (BW + PF_MBS - 1) / PF_MBS * (H / 16);
-    k_prop_input<true><<<groups, 256, 0, (cudaStream_t)stream>>>(cur_y, ref_y, W, H, prev_coded, mb0, nmb, nullptr,
+    k_prop_input<true><<<groups, PF_THREADS, 0, (cudaStream_t)stream>>>(cur_y, ref_y, W, H, prev_coded, mb0, nmb, nullptr,
                                                                  (__nv_bfloat16*)x1, (const __nv_bfloat16*)w1, b1,
                                                                  (__nv_bfloat16*)a1);
     return (int)cudaGetLastError();
