@@ -15,8 +15,9 @@ namespace riv {
 // BinProb state by one multiply (exact for dividends below 2^16, checked for all 65536 states
 // by entropy_init)
 static uint32_t g_div_m[512];
-static uint64_t g_rcp_m[256];
-static uint32_t g_rcp_s[256];
+// ceil(2^64 / f) for f = 2 .. 255: floor(r / f) is the high half of r * g_rcp64[f] for every
+// r < 2^32 (the rounding error r * (ceil - exact) stays below 2^64 / f); f = 1 divides trivially
+static uint64_t g_rcp64[256];
 static std::once_flag g_once;
 
 // BinProb update after one bit (com/rans.rs:73-84).  Computed, not tabulated: a state moves
@@ -51,15 +52,12 @@ void entropy_init() {
             b.packed = (uint16_t)i;
             if (prob_zero(b) != want) std::abort();  // cannot happen: the reciprocals are exact here
         }
-        // Exact reciprocals for r / f, f in [1,255], r < 2^32 (round-up multiplier with
-        // s = 32 + ceil(log2 f) fraction bits).
-        for (uint32_t f = 1; f < 256; f++) {
-            uint32_t l = 0;
-            while ((1u << l) < f) l++;
-            uint32_t s = 32 + l;
-            unsigned __int128 one = (unsigned __int128)1 << s;
-            g_rcp_m[f] = (uint64_t)((one + f - 1) / f);
-            g_rcp_s[f] = s;
+        for (uint32_t f = 2; f < 256; f++) {
+            g_rcp64[f] = (uint64_t)((((unsigned __int128)1 << 64) + f - 1) / f);
+            // spot checks at the quotient steps and the top of the range
+            const uint32_t rs[6] = {0u, f - 1, f, 0xFFFFFFFFu, 0xFFFFFFFFu - 0xFFFFFFFFu % f, 0xFFFFFFFFu - 0xFFFFFFFFu % f - 1};
+            for (uint32_t r : rs)
+                if ((uint32_t)(((unsigned __int128)r * g_rcp64[f]) >> 64) != r / f) std::abort();
         }
     });
 }
@@ -92,12 +90,13 @@ static inline void enc_sym(uint32_t& r, uint16_t* words, int& wp, uint16_t e) {
     if (p == 0) p = 1;
     bool bit = (e >> 8) & 1;
     uint32_t start = bit ? p : 0, freq = bit ? 256u - p : p;
-    uint32_t xmax = freq << 24;
-    if (r >= xmax) {
-        words[--wp] = (uint16_t)r;
-        r >>= 16;
-    }
-    uint32_t q = (uint32_t)(((unsigned __int128)r * g_rcp_m[freq]) >> g_rcp_s[freq]);
+    // renormalisation without a branch: the low word is stored at the next free slot either way
+    // (the buffer has room for one word per symbol) and kept only when r is at or above xmax
+    const uint32_t xmax = freq << 24, out = r >= xmax ? 1u : 0u;
+    words[wp - 1] = (uint16_t)r;
+    wp -= (int)out;
+    r >>= 16 * out;
+    const uint32_t q = freq == 1 ? r : (uint32_t)(((unsigned __int128)r * g_rcp64[freq]) >> 64);
     r = (q << 8) | (r - q * freq + start);
 }
 
@@ -151,6 +150,22 @@ void RansWriter::drain() {
 RansWriter::~RansWriter() {
     for (Batch& b : batches_)
         if (b.done.valid()) b.done.wait();
+}
+
+void RansWriter::finish_async() {
+    if (submit_ == nullptr) {
+        finish();
+        return;
+    }
+    drain();  // the partial batch as one more job
+}
+
+void RansWriter::collect() {
+    for (Batch& b : batches_) {
+        b.done.get();
+        sink_->insert(sink_->end(), b.bytes.begin(), b.bytes.end());
+    }
+    batches_.clear();
 }
 
 void RansWriter::finish() {
@@ -708,12 +723,16 @@ void MvCoder::prepare(const std::vector<MvCodedBlock>& blocks, int bw, MvSymbols
     update(blocks);
 }
 
-void MvCoder::code(const MvSymbols& syms, std::vector<uint8_t>& out, const BatchSubmit* submit) {
-    out.clear();
-    RansWriter w(&out, submit);
+void MvCoder::model(const MvSymbols& syms, RansWriter& w) {
     BinProb* m = &c_.skip;
     const uint16_t* s = syms.s.get();
     for (size_t i = 0; i < syms.n; i++) w.put((s[i] >> 15) != 0, m[s[i] & 0x7fff]);
+}
+
+void MvCoder::code(const MvSymbols& syms, std::vector<uint8_t>& out, const BatchSubmit* submit) {
+    out.clear();
+    RansWriter w(&out, submit);
+    model(syms, w);
     w.finish();
 }
 

@@ -37,6 +37,10 @@ public:
     inline void put(bool bit, BinProb& ctx);
     inline void put_bypass(bool bit);
     void finish();
+    // finish in two halves (with submit only): the last batch goes to submit as well, and
+    // collect() later waits for every batch and appends the words in order
+    void finish_async();
+    void collect();
 
 private:
     // out of line and cold: inlined into put it costs the symbol loop its registers
@@ -114,6 +118,9 @@ public:
     // frame order give encode_frame's bytes.  prepare throws where encode_frame does.
     void prepare(const std::vector<MvCodedBlock>& blocks, int bw, MvSymbols& syms);
     void code(const MvSymbols& syms, std::vector<uint8_t>& out, const BatchSubmit* submit = nullptr);
+    // code's modelling only, into w (its batches coded wherever w sends them; the caller
+    // finishes w)
+    void model(const MvSymbols& syms, RansWriter& w);
     void reset_history();  // prepare's state, as reset() leaves it
     void reset_models();   // code's state, as reset() leaves it
     // Throws std::runtime_error on a NEW block with a raw -1/2 subpel (the reference panics).

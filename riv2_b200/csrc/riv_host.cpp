@@ -362,6 +362,7 @@ struct Job {
     // coding started / done; written
     double tr[10] = {0};
     MvSymbols mv_syms;
+    std::unique_ptr<RansWriter> mv_writer;  // the MV bytes' rANS batches, collected when written
     int8_t bias[2] = {0, 0};
     riv_frame_stats stats{};
     float times[NSTAGE + 1] = {0};
@@ -424,6 +425,7 @@ struct riv_encoder {
     std::shared_ptr<ThreadPool> mv_pool;    // rANS batches of the MV coder (shared by the clips of a batch)
     std::shared_ptr<ThreadPool> rans_pool;  // coefficient-coder jobs (never wait)
     BatchSubmit rans_submit;
+    BatchSubmit rans_submit_urgent;  // rans_pool, ahead of queued batches (a drain's last frame)
     BatchSubmit mv_submit;  // mv_pool: the MV coder is serial across frames, its batches wait for no bulk work
     int rans_parts = 1;  // threads that code one frame's coefficients: rans_pool's and the caller
     bool draining = false;  // inside drain_all: the newest frame is coded by rans_parts threads
@@ -671,18 +673,22 @@ static void setup_device(riv_encoder* e) {
     e->lcoffset.alloc((size_t)N * 4);
     if (e->table_ok)
         e->sadtab.alloc((size_t)N * sad_table_stride(c.search_range) * sizeof(uint16_t));
+    // default: half the host's threads model coefficients (a frame models on one, so this is
+    // several frames at once) and as many code their rANS batches; both run below the serial
+    // stages (submission, MV listing and coding)
     unsigned nt = c.entropy_threads;
-    if (nt == 0) nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency() > 1 ? std::thread::hardware_concurrency() - 1 : 1u));
+    if (nt == 0) nt = std::max(2u, std::min(16u, std::thread::hardware_concurrency() / 2));
     e->pool.reset(new ThreadPool(nt, BULK_NICE));
     e->mv_exec.reset(new ThreadPool(1));
     e->mv_prep.reset(new ThreadPool(1));
     e->mv_pool.reset(new ThreadPool(2));
-    e->rans_pool.reset(new ThreadPool(std::max(2u, nt / 2), BULK_NICE));
-    e->rans_parts = (int)std::max(2u, nt / 2) + 1;
+    e->rans_pool.reset(new ThreadPool(nt, BULK_NICE));
+    e->rans_parts = (int)nt + 1;
     if (const char* v = getenv("RIV_TRACE")) e->trace_path = v;
     {
         ThreadPool* rp = e->rans_pool.get();
         e->rans_submit = [rp](std::function<void()> f) { return rp->submit(std::move(f)); };
+        e->rans_submit_urgent = [rp](std::function<void()> f) { return rp->submit(std::move(f), true); };
         ThreadPool* mp = e->mv_pool.get();
         e->mv_submit = [mp](std::function<void()> f) { return mp->submit(std::move(f)); };
     }
@@ -1270,7 +1276,12 @@ static riv_status retire(riv_encoder* e, Job& j) {
             jp->fut_prep.get();
             double m0 = now_ms();
             jp->tr[5] = m0;
-            ep->mvc.code(jp->mv_syms, jp->mv_bytes, &ep->mv_submit);
+            // modelling only on this thread; every rANS batch is coded on mv_pool and the
+            // bytes are collected when the record is written
+            jp->mv_bytes.clear();
+            jp->mv_writer.reset(new RansWriter(&jp->mv_bytes, &ep->mv_submit));
+            ep->mvc.model(jp->mv_syms, *jp->mv_writer);
+            jp->mv_writer->finish_async();
             jp->tr[6] = now_ms();
             double dt = jp->tr[6] - m0;
             std::lock_guard<std::mutex> g(ep->stat_mu);
@@ -1295,7 +1306,8 @@ static riv_status retire(riv_encoder* e, Job& j) {
     j.fut = e->pool->submit([jp, ep, packed, peobs, count, intra, parts] {
         double d0 = now_ms();
         jp->tr[7] = d0;
-        encode_residual_frame(packed, peobs, (int)count, intra, jp->res_bytes, &ep->rans_submit, parts);
+        encode_residual_frame(packed, peobs, (int)count, intra, jp->res_bytes,
+                              parts > 1 ? &ep->rans_submit_urgent : &ep->rans_submit, parts);
         jp->tr[8] = now_ms();
         double dt = jp->tr[8] - d0;
         std::lock_guard<std::mutex> g(ep->stat_mu);
@@ -1310,6 +1322,10 @@ static riv_status retire(riv_encoder* e, Job& j) {
 static riv_status write_job(riv_encoder* e, Job& j) {
     double b0 = now_ms();
     j.fut_mv.get();
+    if (j.mv_writer) {
+        j.mv_writer->collect();
+        j.mv_writer.reset();
+    }
     j.fut.get();
     double w0 = now_ms();
     e->host_ms[5] += w0 - b0;
@@ -3196,6 +3212,7 @@ riv_status riv_batch_new(const riv_config* cfgs, const riv_writer_vtable* writer
             e->mv_pool = b->mv_pool;
             ThreadPool* rp = b->rans_pool.get();  // both submit paths onto the shared pools
             e->rans_submit = [rp](std::function<void()> f) { return rp->submit(std::move(f)); };
+            e->rans_submit_urgent = [rp](std::function<void()> f) { return rp->submit(std::move(f), true); };
             ThreadPool* mp = b->mv_pool.get();
             e->mv_submit = [mp](std::function<void()> f) { return mp->submit(std::move(f)); };
             e->rans_parts = (int)std::max(2u, hw / 2) + 1;
