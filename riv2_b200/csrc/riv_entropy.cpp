@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <exception>
 #include <stdexcept>
 #include <cstdlib>
@@ -158,6 +159,12 @@ void RansWriter::finish_async() {
         return;
     }
     drain();  // the partial batch as one more job
+}
+
+bool RansWriter::ready() {
+    for (Batch& b : batches_)
+        if (b.done.wait_for(std::chrono::seconds(0)) != std::future_status::ready) return false;
+    return true;
 }
 
 void RansWriter::collect() {
@@ -497,6 +504,20 @@ void encode_residual_frame(const int16_t* packed, const uint8_t* eobs, int nbloc
     blocks_syms(sink, prev_dc, packed, eobs, 0, nblocks, intra);
     if (sink.bad) throw std::runtime_error(MAG_CLASS_ERROR);
     w.finish();
+}
+
+std::unique_ptr<RansWriter> encode_residual_frame_async(const int16_t* packed, const uint8_t* eobs, int nblocks,
+                                                       bool intra, std::vector<uint8_t>& out, const BatchSubmit& submit) {
+    out.clear();
+    if (nblocks == 0) return nullptr;  // the reference never instantiates the coder
+    std::unique_ptr<RansWriter> w(new RansWriter(&out, &submit));
+    std::vector<BinProb> cx(CX_COUNT);
+    int16_t prev_dc[3] = {0, 0, 0};
+    ModelSink sink{*w, cx.data()};
+    blocks_syms(sink, prev_dc, packed, eobs, 0, nblocks, intra);
+    if (sink.bad) throw std::runtime_error(MAG_CLASS_ERROR);
+    w->finish_async();
+    return w;
 }
 
 static inline unsigned get_class_value(RansReader& r, BinProb* ctx, int nctx) {

@@ -41,6 +41,7 @@ public:
     // collect() later waits for every batch and appends the words in order
     void finish_async();
     void collect();
+    bool ready();  // every handed-off batch coded (collect() would not wait)
 
 private:
     // out of line and cold: inlined into put it costs the symbol loop its registers
@@ -91,6 +92,12 @@ bool decode_residual_frame(const uint8_t* data, size_t len, const uint8_t* coded
 // Throws std::runtime_error where the reference encoder panics (a magnitude class above 13).
 void encode_residual_frame(const int16_t* packed, const uint8_t* eobs, int nblocks, bool intra,
                            std::vector<uint8_t>& out, const BatchSubmit* submit = nullptr, int parts = 0);
+// The one-thread form of encode_residual_frame with every rANS batch, the last one included,
+// handed to submit: the returned writer's collect() appends the bytes to out (nullptr: no coded
+// block, out empty).  The modelling thread does not wait for the batches.
+std::unique_ptr<class RansWriter> encode_residual_frame_async(const int16_t* packed, const uint8_t* eobs, int nblocks,
+                                                             bool intra, std::vector<uint8_t>& out,
+                                                             const BatchSubmit& submit);
 
 enum MvMode { M_ZERO = 0, M_NEAREST = 1, M_NEAR = 2, M_TOPRIGHT = 3, M_TOPLEFT = 4, M_NEW = 5, M_TEMPORAL = 6 };
 enum Subpel { SP_ZERO = 0, SP_PLUS = 1, SP_MINUS = 2 };

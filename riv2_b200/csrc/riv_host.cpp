@@ -354,7 +354,7 @@ struct Job {
     int prev_buf = 0;
     int ck = 0;             // double-buffer parity of the frame's buffers
     uint32_t count = 0;
-    std::future<void> fut, fut_mv, fut_prep;
+    std::future<void> fut, fut_mv, fut_prep, fut_asm;
     std::vector<uint8_t> res_bytes, mv_bytes;
     std::vector<MvCodedBlock> mv_blocks;  // the P-frame's MV coder input
     // host timeline (milliseconds, steady clock), kept when the encoder traces: submitted; MV
@@ -363,6 +363,7 @@ struct Job {
     double tr[10] = {0};
     MvSymbols mv_syms;
     std::unique_ptr<RansWriter> mv_writer;  // the MV bytes' rANS batches, collected when written
+    std::unique_ptr<RansWriter> res_writer;  // the coefficient bytes' rANS batches, likewise
     int8_t bias[2] = {0, 0};
     riv_frame_stats stats{};
     float times[NSTAGE + 1] = {0};
@@ -422,6 +423,7 @@ struct riv_encoder {
     std::shared_ptr<ThreadPool> pool;       // coefficient modelling (shared by the clips of a batch)
     std::unique_ptr<ThreadPool> mv_exec;    // one thread: MV coding strictly in frame order
     std::unique_ptr<ThreadPool> mv_prep;    // one thread: MV symbol listing strictly in frame order
+    std::unique_ptr<ThreadPool> mv_asm;     // one thread: the MV coder's input of each P-frame
     std::shared_ptr<ThreadPool> mv_pool;    // rANS batches of the MV coder (shared by the clips of a batch)
     std::shared_ptr<ThreadPool> rans_pool;  // coefficient-coder jobs (never wait)
     BatchSubmit rans_submit;
@@ -681,6 +683,7 @@ static void setup_device(riv_encoder* e) {
     e->pool.reset(new ThreadPool(nt, BULK_NICE));
     e->mv_exec.reset(new ThreadPool(1));
     e->mv_prep.reset(new ThreadPool(1));
+    e->mv_asm.reset(new ThreadPool(1));
     e->mv_pool.reset(new ThreadPool(2));
     e->rans_pool.reset(new ThreadPool(nt, BULK_NICE));
     e->rans_parts = (int)nt + 1;
@@ -1259,11 +1262,13 @@ static riv_status retire(riv_encoder* e, Job& j) {
         }
     }
     if (j.type == 2) {
-        // The MV coder's two stages, each on its own thread and in frame order, so that frame
-        // t + 1's input is assembled and its symbols listed while frame t's are coded (same
-        // bytes as one thread).
-        j.fut_prep = e->mv_prep->submit([ep, jp, side, N, mbh, prevh] {
-            assemble_mv(ep, *jp, side, N, mbh.get(), prevh.get());
+        // Three stages, each on its own thread: the coder's input (which needs nothing of the
+        // coder's state), then the coder's two stages in frame order, so that frame t + 2 is
+        // assembled and frame t + 1's symbols listed while frame t's are coded (same bytes as
+        // one thread).
+        j.fut_asm = e->mv_asm->submit([ep, jp, side, N, mbh, prevh] { assemble_mv(ep, *jp, side, N, mbh.get(), prevh.get()); });
+        j.fut_prep = e->mv_prep->submit([ep, jp] {
+            jp->fut_asm.get();
             double m0 = now_ms();
             jp->tr[3] = m0;
             ep->mvc.prepare(jp->mv_blocks, ep->BW, jp->mv_syms);
@@ -1306,8 +1311,8 @@ static riv_status retire(riv_encoder* e, Job& j) {
     j.fut = e->pool->submit([jp, ep, packed, peobs, count, intra, parts] {
         double d0 = now_ms();
         jp->tr[7] = d0;
-        encode_residual_frame(packed, peobs, (int)count, intra, jp->res_bytes,
-                              parts > 1 ? &ep->rans_submit_urgent : &ep->rans_submit, parts);
+        if (parts > 1) encode_residual_frame(packed, peobs, (int)count, intra, jp->res_bytes, &ep->rans_submit_urgent, parts);
+        else jp->res_writer = encode_residual_frame_async(packed, peobs, (int)count, intra, jp->res_bytes, ep->rans_submit);
         jp->tr[8] = now_ms();
         double dt = jp->tr[8] - d0;
         std::lock_guard<std::mutex> g(ep->stat_mu);
@@ -1327,6 +1332,10 @@ static riv_status write_job(riv_encoder* e, Job& j) {
         j.mv_writer.reset();
     }
     j.fut.get();
+    if (j.res_writer) {
+        j.res_writer->collect();
+        j.res_writer.reset();
+    }
     double w0 = now_ms();
     e->host_ms[5] += w0 - b0;
     const riv_config& c = e->cfg;
@@ -1401,7 +1410,8 @@ static riv_status pump(riv_encoder* e, bool block_front, bool block_write) {
         Job& f = e->jobs.front();
         if (f.state != 1) break;
         if (!block && (f.fut.wait_for(std::chrono::seconds(0)) != std::future_status::ready ||
-                       f.fut_mv.wait_for(std::chrono::seconds(0)) != std::future_status::ready))
+                       f.fut_mv.wait_for(std::chrono::seconds(0)) != std::future_status::ready ||
+                       (f.res_writer && !f.res_writer->ready()) || (f.mv_writer && !f.mv_writer->ready())))
             break;
         riv_status st = write_job(e, f);
         // a record the writer refused is lost and not counted, as when the reference's
@@ -1446,7 +1456,8 @@ static riv_status drain_all(riv_encoder* e) {
         const bool later_unretired = retired() < e->jobs.size();
         if (f.state == 0) st = pump(e, true, false);          // block on the front frame's GPU work
         else if (!later_unretired) st = pump(e, false, true);  // nothing else to retire: block on its record
-        else f.fut.wait_for(std::chrono::microseconds(20));
+        else if (f.fut.wait_for(std::chrono::microseconds(20)) == std::future_status::ready)
+            std::this_thread::sleep_for(std::chrono::microseconds(20));  // its batches are still being coded
         if (st == RIV_ERR_IO) {
             io = st;
             continue;
@@ -1685,6 +1696,7 @@ void riv_encoder_free(riv_encoder* e) {
         if (j.fut.valid()) j.fut.wait();
         if (j.fut_mv.valid()) j.fut_mv.wait();
         if (j.fut_prep.valid()) j.fut_prep.wait();
+        if (j.fut_asm.valid()) j.fut_asm.wait();
     }
     if (!e->trace_path.empty() && !e->trace.empty()) {
         if (FILE* f = fopen(e->trace_path.c_str(), "a")) {
@@ -1699,6 +1711,7 @@ void riv_encoder_free(riv_encoder* e) {
     e->pool.reset();
     e->mv_exec.reset();
     e->mv_prep.reset();
+    e->mv_asm.reset();
     e->mv_pool.reset();
     e->rans_pool.reset();
     if (e->S) cudaStreamSynchronize(e->S);
