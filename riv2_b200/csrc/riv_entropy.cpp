@@ -17,7 +17,8 @@ namespace riv {
 // by entropy_init)
 static uint32_t g_div_m[512];
 // ceil(2^64 / f) for f = 2 .. 255: floor(r / f) is the high half of r * g_rcp64[f] for every
-// r < 2^32 (the rounding error r * (ceil - exact) stays below 2^64 / f); f = 1 divides trivially
+// r < 2^32 (the rounding error r * (ceil - exact) stays below 2^64 / f); f = 1: 2^64 - 1, whose
+// product's high half is r - 1 for r > 0
 static uint64_t g_rcp64[256];
 static std::once_flag g_once;
 
@@ -53,6 +54,7 @@ void entropy_init() {
             b.packed = (uint16_t)i;
             if (prob_zero(b) != want) std::abort();  // cannot happen: the reciprocals are exact here
         }
+        g_rcp64[1] = ~0ull;
         for (uint32_t f = 2; f < 256; f++) {
             g_rcp64[f] = (uint64_t)((((unsigned __int128)1 << 64) + f - 1) / f);
             // spot checks at the quotient steps and the top of the range
@@ -88,16 +90,19 @@ inline void RansWriter::put_bypass(bool bit) {
 
 static inline void enc_sym(uint32_t& r, uint16_t* words, int& wp, uint16_t e) {
     uint32_t p = e & 0xff;
-    if (p == 0) p = 1;
-    bool bit = (e >> 8) & 1;
-    uint32_t start = bit ? p : 0, freq = bit ? 256u - p : p;
+    p += p == 0 ? 1u : 0u;
+    // bit 1: start p, frequency 256 - p; bit 0: start 0, frequency p (masks, not a branch: the
+    // bits are the data)
+    const uint32_t m = 0u - ((uint32_t)(e >> 8) & 1u);
+    const uint32_t start = p & m, freq = (p ^ m) + (m & 257u);
     // renormalisation without a branch: the low word is stored at the next free slot either way
     // (the buffer has room for one word per symbol) and kept only when r is at or above xmax
     const uint32_t xmax = freq << 24, out = r >= xmax ? 1u : 0u;
     words[wp - 1] = (uint16_t)r;
     wp -= (int)out;
     r >>= 16 * out;
-    const uint32_t q = freq == 1 ? r : (uint32_t)(((unsigned __int128)r * g_rcp64[freq]) >> 64);
+    // frequency 1: the multiplier 2^64 - 1 gives r - 1 (r > 0 here), and the comparison adds the 1
+    const uint32_t q = (uint32_t)(((unsigned __int128)r * g_rcp64[freq]) >> 64) + (freq == 1 ? 1u : 0u);
     r = (q << 8) | (r - q * freq + start);
 }
 
