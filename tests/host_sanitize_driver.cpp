@@ -127,12 +127,18 @@ int main(int argc, char** argv) {
         const int n = t < 2 ? 40 : 700 + 400 * t;  // below and above the parallel form's minimum
         const std::vector<int16_t> b = random_blocks(rng, n, t < 4 ? 0.3 : 0.6);
         compact(b, n, intra, packed, eobs);
-        std::vector<uint8_t> inline_bytes, pooled, parallel;
+        std::vector<uint8_t> inline_bytes, pooled, parallel, async_bytes;
         riv::encode_residual_frame(packed.data(), eobs.data(), n, intra, inline_bytes);
         riv::encode_residual_frame(packed.data(), eobs.data(), n, intra, pooled, &submit);
         riv::encode_residual_frame(packed.data(), eobs.data(), n, intra, parallel, &submit, 4);
+        {  // every batch handed off, joined later (the encoder joins at the record write)
+            std::unique_ptr<riv::RansWriter> w =
+                riv::encode_residual_frame_async(packed.data(), eobs.data(), n, intra, async_bytes, submit);
+            if (w) w->collect();
+        }
         if (pooled != inline_bytes) return fail("pooled batches differ from the inline coder", t);
         if (parallel != inline_bytes) return fail("parallel coder differs from the inline coder", t);
+        if (async_bytes != inline_bytes) return fail("handed-off batches differ from the inline coder", t);
         std::vector<uint8_t> coded((size_t)n, 1);
         std::vector<int16_t> back((size_t)n * 384);
         if (!riv::decode_residual_frame(inline_bytes.data(), inline_bytes.size(), coded.data(), n, intra, back.data()))
@@ -143,22 +149,28 @@ int main(int argc, char** argv) {
     std::vector<int16_t> b = random_blocks(rng, 900, 0.4);
     b[(size_t)300 * 384 + 7] = 9000;
     compact(b, 900, false, packed, eobs);
-    for (int form = 0; form < 3; form++) {
+    for (int form = 0; form < 4; form++) {
         std::vector<uint8_t> out;
         bool threw = false;
         try {
             if (form == 0) riv::encode_residual_frame(packed.data(), eobs.data(), 900, false, out);
             else if (form == 1) riv::encode_residual_frame(packed.data(), eobs.data(), 900, false, out, &submit);
-            else riv::encode_residual_frame(packed.data(), eobs.data(), 900, false, out, &submit, 4);
+            else if (form == 2) riv::encode_residual_frame(packed.data(), eobs.data(), 900, false, out, &submit, 4);
+            else riv::encode_residual_frame_async(packed.data(), eobs.data(), 900, false, out, submit);
         } catch (const std::runtime_error&) {
             threw = true;
         }
         if (!threw) return fail("magnitude class 14 did not fail", form);
     }
     // the MV coder: frames of every mode with a candidate history, encoded by one coder and
-    // decoded by another that follows it
+    // decoded by another that follows it; and the same frames through the encoder's pipeline
+    // (symbol listing and modelling of consecutive frames on two threads at once, every rANS
+    // batch on the pool), which must give the same bytes
     {
-        riv::MvCoder enc, dec;
+        riv::MvCoder enc, dec, staged;
+        Pool list_thread(1), model_thread(1);
+        std::vector<std::vector<riv::MvCodedBlock>> frames;
+        std::vector<std::vector<uint8_t>> seq_bytes;
         std::uniform_int_distribution<int> mode(0, 6), base(0, 4), delta(-128, 127), sub(0, 1), few(0, 3);
         std::bernoulli_distribution coin(0.5);
         const int bw = 24, bh = 16;
@@ -179,6 +191,8 @@ int main(int argc, char** argv) {
             }
             std::vector<uint8_t> bytes;
             enc.encode_frame(v, bw, bytes);
+            frames.push_back(v);
+            seq_bytes.push_back(bytes);
             if (!dec.decode_frame(bytes.data(), bytes.size(), bw, bh, back)) return fail("MV decoder: malformed", f);
             for (size_t i = 0; i < v.size(); i++) {
                 const riv::MvCodedBlock &a = v[i], &c = back[i];
@@ -186,6 +200,27 @@ int main(int argc, char** argv) {
                     a.spy != c.spy || a.skip != c.skip)
                     return fail("MV decoder does not invert the coder", f);
             }
+        }
+        const size_t nf = frames.size();
+        std::vector<riv::MvSymbols> syms(nf);
+        std::vector<std::vector<uint8_t>> out(nf);
+        std::vector<std::unique_ptr<riv::RansWriter>> writers(nf);
+        std::vector<std::shared_future<void>> listed(nf);
+        std::vector<std::future<void>> modelled(nf);
+        for (size_t f = 0; f < nf; f++) {
+            listed[f] = list_thread.submit([&, f] { staged.prepare(frames[f], bw, syms[f]); }).share();
+            std::shared_future<void> lf = listed[f];
+            modelled[f] = model_thread.submit([&, f, lf] {
+                lf.get();
+                writers[f].reset(new riv::RansWriter(&out[f], &submit));
+                staged.model(syms[f], *writers[f]);
+                writers[f]->finish_async();
+            });
+        }
+        for (size_t f = 0; f < nf; f++) {
+            modelled[f].get();
+            writers[f]->collect();
+            if (out[f] != seq_bytes[f]) return fail("pipelined MV coder differs from the sequential coder", (int)f);
         }
     }
     std::printf("host entropy sanitizer driver: ok\n");

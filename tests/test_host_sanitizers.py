@@ -1,7 +1,9 @@
 """The host entropy stage (riv2_b200/csrc/riv_entropy.cpp) built with the compiler's
 sanitizers and driven by tests/host_sanitize_driver.cpp on CPU: AddressSanitizer with
 UndefinedBehaviorSanitizer (out-of-bounds accesses, use after free, bad shifts) and
-ThreadSanitizer (data races in the pooled and parallel coefficient coders).  The oracle, the
+ThreadSanitizer (data races in the pooled, parallel and handed-off coefficient coders, and in
+the MV coder's pipeline: symbol listing and modelling of consecutive frames on two threads at
+once, every rANS batch on a pool, as the encoder runs them).  The oracle, the
 checker of every parity test, runs small clips under AddressSanitizer and
 UndefinedBehaviorSanitizer too (tests/oracle_sanitize_driver.cpp).  The device code cannot run
 under a sanitizer here; its kernels bound their own indexes and waits."""
