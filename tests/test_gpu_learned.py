@@ -69,6 +69,25 @@ def test_stream_decodes_to_the_encoder_reconstruction(form, preset, w, h, n):
 
 
 @pytest.mark.parametrize("form", [1, 2])
+def test_1080p_stream_with_the_trained_network_decodes(form):
+    """The bench's size and network: every kernel of the form at 8160 MBs (convolution tiles
+    that cross MB boundaries, four-position search steps at the frame's borders)."""
+    import os
+    from riv2_b200 import proposal as P
+    from riv2_b200.synth import SynthClip
+    clip = SynthClip("1080p", seed=2026)
+    frames = [clip.frame(t) for t in range(4)]
+    weights = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "riv2_b200", "weights",
+                           "proposal.bin")
+    params = P.load_params(weights) if form == 1 else None
+    stream, recons, c = _encode(frames, _cfg(1920, 1080, form), params)
+    _decodes_to(stream, recons)
+    assert c["mbs"] == 8160 * 3
+    if form == 1:
+        assert c["fallbacks"] < c["mbs"] // 2  # the trained network's proposals are mostly taken
+
+
+@pytest.mark.parametrize("form", [1, 2])
 def test_pipelined_stream_equals_synchronous(form):
     from riv2_b200.synth import SynthClip
     clip = SynthClip("cif", seed=43)
