@@ -67,6 +67,7 @@ void entropy_init() {
 
 
 static const int BATCH = 16386;  // com/rans.rs:201
+static_assert(BATCH == RansWriter::BATCH_SYMS, "the writer's stack depth is the reference's batch");
 // The parallel coefficient coder takes frames of 16K to 2M coded coefficients: below, its
 // fork and join cost more than they save; above, its symbol lists (up to about 26 symbols per
 // coefficient) would take hundreds of MB.
@@ -164,6 +165,12 @@ void RansWriter::finish_async() {
         return;
     }
     drain();  // the partial batch as one more job
+}
+
+uint16_t* RansWriter::refill() {
+    sp_ = 0;
+    drain();
+    return stack_.data();
 }
 
 bool RansWriter::ready() {
@@ -264,7 +271,7 @@ constexpr int CX_SIG_Y = 0, CX_SIG_C = 256, CX_MAG_Y = 320, CX_MAG_C = 372, CX_E
 // bits and no stop bit, as the reference does; above it the reference indexes past its
 // models and panics, so the sink is marked bad and the frame fails.
 template <class W>
-static inline void class_value_syms(W& w, unsigned value, int cx0, int nctx) {
+__attribute__((always_inline)) static inline void class_value_syms(W& w, unsigned value, int cx0, int nctx) {
     int maxc = nctx - 1, cls = bit_len(value);
     if (cls > nctx) {
         w.bad = true;
@@ -281,7 +288,8 @@ static inline void class_value_syms(W& w, unsigned value, int cx0, int nctx) {
 // and magnitude class (res/rans.rs:250-278); intra DC values are coded against the previous
 // block's (prev_dc, per plane) ...
 template <class W>
-static void plane_syms(W& w, int16_t* prev_dc, const int16_t* pl, int last, bool luma, int pi, bool dcp) {
+__attribute__((always_inline)) static inline void plane_syms(W& w, int16_t* prev_dc, const int16_t* pl, int last,
+                                                             bool luma, int pi, bool dcp) {
     int16_t dcv = pl[0];
     if (dcp) {
         dcv = (int16_t)(pl[0] - prev_dc[pi]);
@@ -301,7 +309,8 @@ static void plane_syms(W& w, int16_t* prev_dc, const int16_t* pl, int last, bool
 }
 // ... and blocks [b0, b1) of the compact layout starting at p (Y, U, V per MB).
 template <class W>
-static void blocks_syms(W& w, int16_t* prev_dc, const int16_t* p, const uint8_t* eobs, int b0, int b1, bool intra) {
+__attribute__((always_inline)) static inline void blocks_syms(W& w, int16_t* prev_dc, const int16_t* p,
+                                                              const uint8_t* eobs, int b0, int b1, bool intra) {
     for (int b = b0; b < b1; b++) {
         const uint8_t* e = eobs + 3 * b;
         plane_syms(w, prev_dc, p, e[0], true, 0, intra);
@@ -318,13 +327,31 @@ struct DctContexts {
     int16_t prev_dc[3] = {0, 0, 0};
 };
 
-// Sequential sink: models the symbols into a RansWriter.
+// Sequential sink: models the symbols into a RansWriter, with the writer's stack pointer and
+// depth in locals (registers) between its drains, not loaded and stored per symbol; finish()
+// hands the depth back to the writer.
 struct ModelSink {
     RansWriter& w;
     BinProb* cx;
     bool bad = false;
-    void put(bool bit, int id) { w.put(bit, cx[id]); }
-    void bypass(bool bit) { w.put_bypass(bit); }
+    uint16_t* st;
+    int sp;
+    ModelSink(RansWriter& w_, BinProb* cx_) : w(w_), cx(cx_), st(w_.stack()), sp(w_.depth()) {}
+    inline void push(uint16_t e) {
+        if (__builtin_expect(sp == 0, 0)) {
+            st = w.refill();
+            sp = BATCH;
+        }
+        st[--sp] = e;
+    }
+    void put(bool bit, int id) {
+        BinProb& m = cx[id];
+        const uint8_t p = prob_zero(m);
+        observe(m, bit);
+        push((uint16_t)(p | (bit ? 0x100 : 0)));
+    }
+    void bypass(bool bit) { push((uint16_t)(128 | (bit ? 0x100 : 0))); }
+    void finish() { w.commit(sp); }
 };
 // Enumerating sink: model id | bit << 15 per symbol, and how often each model is used.
 struct SymList {
@@ -507,6 +534,7 @@ void encode_residual_frame(const int16_t* packed, const uint8_t* eobs, int nbloc
     int16_t prev_dc[3] = {0, 0, 0};
     ModelSink sink{w, cx.data()};
     blocks_syms(sink, prev_dc, packed, eobs, 0, nblocks, intra);
+    sink.finish();
     if (sink.bad) throw std::runtime_error(MAG_CLASS_ERROR);
     w.finish();
 }
@@ -520,6 +548,7 @@ std::unique_ptr<RansWriter> encode_residual_frame_async(const int16_t* packed, c
     int16_t prev_dc[3] = {0, 0, 0};
     ModelSink sink{*w, cx.data()};
     blocks_syms(sink, prev_dc, packed, eobs, 0, nblocks, intra);
+    sink.finish();
     if (sink.bad) throw std::runtime_error(MAG_CLASS_ERROR);
     w->finish_async();
     return w;
@@ -750,9 +779,10 @@ void MvCoder::prepare(const std::vector<MvCodedBlock>& blocks, int bw, MvSymbols
 }
 
 void MvCoder::model(const MvSymbols& syms, RansWriter& w) {
-    BinProb* m = &c_.skip;
+    ModelSink sink{w, &c_.skip};
     const uint16_t* s = syms.s.get();
-    for (size_t i = 0; i < syms.n; i++) w.put((s[i] >> 15) != 0, m[s[i] & 0x7fff]);
+    for (size_t i = 0; i < syms.n; i++) sink.put((s[i] >> 15) != 0, s[i] & 0x7fff);
+    sink.finish();
 }
 
 void MvCoder::code(const MvSymbols& syms, std::vector<uint8_t>& out, const BatchSubmit* submit) {

@@ -43,6 +43,16 @@ public:
     void collect();
     bool ready();  // every handed-off batch coded (collect() would not wait)
 
+    // The stack in a caller's registers, for symbol loops: start from stack() and depth(),
+    // push downwards (stack()[--depth] = entry), call refill() at depth 0 (it hands the full
+    // stack off and returns the fresh one, depth BATCH_SYMS again) and commit(depth) before any
+    // other call on the writer.
+    static constexpr int BATCH_SYMS = 16386;  // com/rans.rs:201
+    uint16_t* stack() { return stack_.data(); }
+    int depth() const { return sp_; }
+    __attribute__((noinline)) uint16_t* refill();
+    void commit(int depth) { sp_ = depth; }
+
 private:
     // out of line and cold: inlined into put it costs the symbol loop its registers
     __attribute__((noinline, cold)) void drain();
