@@ -8,10 +8,12 @@
 //  * k_nn_gemm: D = A . B^T with both operands staged by TMA (cp.async.bulk.tensor) through a
 //    four-deep ring: warp 0 issues the copies, warp 1 the MMAs, all four warps run the
 //    epilogue (warp w owns accumulator rows 32w .. 32w+31, the TMEM lanes it may read).
-//  * k_nn_conv: implicit-GEMM 3x3 convolution.  The weights come in once by TMA and stay in
-//    shared memory; each 128-row tile of output positions is gathered (im2col) by the CTA's
-//    threads straight into the swizzled operand layout, one k-block per ring stage, while the
-//    tensor core consumes the previous stage.  Persistent CTAs, one per SM.
+//  * k_nn_conv_i2c: implicit-GEMM 3x3 convolution (32 input channels: conv2-4).  The weights
+//    come in once by TMA and stay in shared memory; each 128-row tile of output positions is
+//    loaded by the TMA's im2col mode, one 128 x 32-channel load per filter tap, while the
+//    tensor core consumes earlier taps.  Persistent CTAs, two per SM.
+//  * k_nn_conv: the same GEMM with the operand gathered by the CTA's threads (cp.async straight
+//    into the swizzled layout): conv1 of the training path, and conv2-4 when RIV_CONV_GATHER=1.
 //
 // Every wait is bounded; an expired wait sets bit 0 of *err and the kernel runs to its end
 // without waiting again (tensor memory is always released).
@@ -712,7 +714,7 @@ int nn_conv(int layer, const void* in, int in_mb, const void* W, const float* bi
     a.err = err;
     const long long rows = (long long)nmb * a.hout * a.hout;
     const int ntiles = (int)((rows + 127) / 128);
-    const char* gv = getenv("RIV_CONV_GATHER");
+    const char* gv = getenv("RIV_CONV_GATHER");  // read per call: a test switches it between calls
     if (cin == 32 && !(gv && gv[0] == '1')) {
         CUtensorMap tin;
         if (!make_im2col_map(&tin, in, a.hin, in_mb, nmb, a.stride)) return (int)cudaErrorInvalidValue;
