@@ -180,11 +180,21 @@ def make_frames(n: int, seed: int, clip: int) -> np.ndarray:
     return SynthClip("1080p", seed=seed, clip=clip).frames(n)
 
 
+def entropy_threads() -> int:
+    """Host threads per entropy pool of one encoder: the encoder's default (half the host) for
+    one rank; with several ranks on the node each takes its share, so that N replicas do not
+    oversubscribe the host N times."""
+    local = int(os.environ.get("LOCAL_WORLD_SIZE", "1"))
+    if local <= 1:
+        return 0
+    return max(2, min(16, (os.cpu_count() or 2) // (2 * local)))
+
+
 def config(iq: int, pq: int, depth: int, device: int, form: int = 0, margin: int = 256):
     from riv2_b200 import encoder as E
     return (E.EncoderConfig.new(W_DISP, H_DISP, FPS).with_intra_quality(iq).with_inter_quality(pq)
             .with_keyframe_interval(E.KeyframeInterval.fixed(1 << 40)).with_pipeline_depth(depth).with_device(device)
-            .with_encode_form(form).with_proposal_margin(margin))
+            .with_encode_form(form).with_proposal_margin(margin).with_entropy_threads(entropy_threads()))
 
 
 def psnr_y_of_stream(stream: bytes, src_y, dev_index: int):

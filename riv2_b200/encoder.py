@@ -270,6 +270,7 @@ class EncoderConfig:
     def with_encode_form(self, v: int): return self._with(encode_form=v)
     def with_proposal_margin(self, v: int): return self._with(proposal_margin=v)
     def with_device(self, v: int): return self._with(device=v)
+    def with_entropy_threads(self, v: int): return self._with(entropy_threads=v)
 
     def validate(self) -> None:
         """EncoderConfig::validate (enc/config.rs:129-164)."""
